@@ -1,0 +1,304 @@
+"""Benchmark of the B200 GBDT engine.
+
+Workload (one GPU): binary logistic GBDT on a 1,000,000 x 100 f32 matrix
+(even columns N(0,1), odd U(0,1), 10% NaN on 20 columns, label from 10
+pairwise products), depth 8, 256 bins, lr 0.1, FP32 grad/hess — the
+reference's plain-GBDT GPU configuration. Data are seeded synthetic.
+
+A step is one boosting round (one tree) on the GPU-resident binned matrix;
+`value` is seconds per 100 trees over the whole job (all GPUs). `e2e` is the
+same metric through the public C-ABI train call from host buffers (dataset
+copy, H2D, binning, 100 trees, D2H of the training predictions).
+With --gpus N (torchrun) every rank trains an independent replica on its own
+row stream (training does not shard; no collective on the data path).
+
+--impl reference times the CPU restatement of the reference's path (the Rust
+crate cannot be built here) with all host threads, rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "train s/100 trees, predict rows/s, p99 serve ms vs plain GPU at equal loss"
+UNIT = "s/100 trees"
+N_ROWS, N_FEAT, N_NAN, SEED = 1_000_000, 100, 20, 2
+WORKLOAD = "binary-logistic GBDT 1,000,000x100 f32 (20 NaN cols), depth 8, 256 bins, lr 0.1, FP32 grad/hess"
+
+
+def cfg_kwargs():
+    import boosters_b200 as bst
+    return dict(objective=bst.Objective.logistic(), n_estimators=500, learning_rate=0.1, max_depth=8, max_bins=256,
+                metric=bst.Metric.none())
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def reduce_max(world, v):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(n_rounds, n_threads, x, y):
+    """The CPU restatement on the same workload: per-tree seconds (binning excluded)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import boosters_b200 as bst
+    import oracle_bridge as ob
+    cfg = bst.GBDTConfig(**cfg_kwargs()).to_c()
+    m = ob.OracleModel(x, y, cfg, n_threads=0, record_leaves=False, omp_threads=n_threads, max_trees=n_rounds)
+    return [ob.lib.orc_model_tree_seconds(m._h, t) for t in range(m.n_trees)]
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import boosters_b200 as bst
+    x, y = bst.synth.binary(N_ROWS, N_FEAT, N_NAN, seed=SEED, stream=0)
+    cores = os.cpu_count() or 1
+    secs = cpu_baseline(args.warmup + args.steps, cores, x, y)
+    timed = secs[args.warmup:]
+    v = 100.0 * sum(timed) / len(timed)
+    sample = f"{args.warmup}+{args.steps} boosting rounds of the {N_ROWS}x{N_FEAT} workload (binning excluded)"
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * sum(timed) / len(timed), 3),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": "cpu threads"},
+            "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import ctypes
+
+    import boosters_b200 as bst
+    from boosters_b200 import _native as n
+    import torch
+
+    torch.cuda.set_device(local)
+    kw = cfg_kwargs()
+    cfg = bst.GBDTConfig(device=local, **kw)
+    x, y = bst.synth.binary(N_ROWS, N_FEAT, N_NAN, seed=SEED, stream=rank)
+    ds = bst.Dataset.from_feature_major(x, y)
+    t_bin0 = time.perf_counter()
+    booster = bst.Booster(ds, cfg, n_threads=0)
+    binning_s = time.perf_counter() - t_bin0
+    booster.update(args.warmup)
+    t0_stats, c0 = booster.stats()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    # update() returns after its stream is idle, so events on this stream
+    # bracket the device work of the timed rounds
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        booster.update(1)
+    ev1.record()
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    clk = clocks.stop()
+    barrier(world)
+    t1_stats, c1 = booster.stats()
+    # device time of the timed rounds (sum of CUDA-event phases; host gaps included in elapsed)
+    elapsed_max = reduce_max(world, elapsed)
+    value = 100.0 * elapsed_max / (args.steps * world)
+    ms_per_step = 1000.0 * elapsed_max / args.steps
+
+    hist_ms = t1_stats["histograms"] - t0_stats["histograms"]
+    hist_bytes = c1["hist_bytes"] - c0["hist_bytes"]
+    hist_launches = max(1, c1["hist_launches"] - c0["hist_launches"])
+    launches = c1["launches"] - c0["launches"]
+    peak, peak_kind = peaks()
+    achieved = hist_bytes / (hist_ms / 1e3) / 1e9 if hist_ms > 0 else 0.0
+    traffic = None
+    tr_file = os.path.join(ROOT, "profiles", "hist_build_traffic.json")
+    if os.path.exists(tr_file):
+        with open(tr_file) as f:
+            tr = json.load(f)
+        # ncu DRAM bytes per algorithmic byte, scaled to this run's average launch
+        traffic = round(tr["dram_bytes_per_algorithmic_byte"] * hist_bytes / hist_launches)
+
+    # held-out loss of the model after warmup + steps rounds
+    model = booster.model()
+    xv, yv = bst.synth.binary(200_000, N_FEAT, N_NAN, seed=SEED, stream=1000 + rank)
+    pv = model.predict_group_major(bst.Dataset.from_feature_major(xv))
+    heldout = bst.metric("logloss", pv, yv)
+
+    # predict throughput on device-resident rows (serving kernel), rows/s
+    rows_pred = None
+    try:
+        xs = torch.from_numpy(np.ascontiguousarray(xv.T)).cuda()
+        out = torch.empty((1, xs.shape[0]), dtype=torch.float32, device="cuda")
+        st = torch.cuda.current_stream()
+        for _ in range(2):
+            n.check(n.lib.bst_gbdt_predict_device(model._h, ctypes.c_void_p(xs.data_ptr()), xs.shape[0], N_FEAT, 1,
+                                                  ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(st.cuda_stream)))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        reps = 5
+        for _ in range(reps):
+            n.check(n.lib.bst_gbdt_predict_device(model._h, ctypes.c_void_p(xs.data_ptr()), xs.shape[0], N_FEAT, 1,
+                                                  ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(st.cuda_stream)))
+        e1.record(st)
+        e1.synchronize()
+        rows_pred = xs.shape[0] * reps / (e0.elapsed_time(e1) / 1e3)
+    except Exception as ex:  # reported, not fatal
+        rows_pred = f"error: {ex}"
+
+    # e2e through the public API from pinned host buffers: 100 trees per step
+    e2e_cfg = bst.GBDTConfig(device=local, **dict(kw, n_estimators=100))
+    xh = torch.from_numpy(x).pin_memory().numpy()
+    yh = torch.from_numpy(y).pin_memory().numpy()
+    e2e_steps = max(1, min(args.steps, 2))
+    bst.GBDTModel.train(bst.Dataset.from_feature_major(xh, yh), e2e_cfg)  # warm-up call
+    barrier(world)
+    te0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        dsh = bst.Dataset.from_feature_major(xh, yh)
+        mh = bst.GBDTModel.train(dsh, e2e_cfg)
+        _ = mh.train_predictions()
+    te = reduce_max(world, time.perf_counter() - te0)
+    e2e_value = te / (e2e_steps * world)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        secs = cpu_baseline(2, cores, x, y)
+        cpu = {"value": round(100.0 * sum(secs) / len(secs), 3), "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"2 boosting rounds of the {N_ROWS}x{N_FEAT} workload, binning excluded"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 grad/hess, int64 fixed-point histograms",
+            "data": "synthetic (seeded counter-based generator)",
+            "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (128 MB binned rows + 8 MB grad/hess per round)",
+                       "binning_s": round(binning_s, 3), "heldout_logloss": round(heldout, 6),
+                       "trees_trained": booster.n_rounds},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_hist_build", "launches": hist_launches,
+                         "avg_launch_ms": round(hist_ms / hist_launches, 5),
+                         "algorithmic_bytes_per_launch": round(hist_bytes / hist_launches)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_value, 4), "unit": "s/100 trees (host buffers, binning + H2D + D2H included)",
+                    "h2d_bytes_per_step": int(x.nbytes + y.nbytes), "d2h_bytes_per_step": int(N_ROWS * 4)},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "predict_rows_per_s": rows_pred,
+            "phase_ms_per_step": {k: round((t1_stats[k] - t0_stats[k]) / args.steps, 4)
+                                  for k in ("gradients", "histograms", "split_scan", "partition", "leaf_update",
+                                            "other")},
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

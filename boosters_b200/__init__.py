@@ -1,0 +1,548 @@
+"""boosters_b200 — B200-native GBDT engine with the API of egordm/boosters.
+
+The Python surface mirrors ``boosters`` (packages/boosters-python:
+``Dataset``, ``GBDTConfig``, ``GBDTModel``, ``Objective``, ``Metric``,
+``GrowthStrategy``); every call goes through the C ABI of
+``libboosters_b200.so`` (include/boosters_c.h), whose hot path runs as
+sm_100a CUDA kernels. There is no CPU fallback.
+"""
+import ctypes
+import enum
+
+import numpy as np
+
+from . import _native as _n
+from ._native import BoostersError
+
+__all__ = ["Dataset", "GBDTConfig", "GBDTModel", "Objective", "Metric", "GrowthStrategy",
+           "BoostersError", "BinnedDataset", "synth", "metric"]
+__version__ = _n.lib.bst_version().decode()
+
+
+class GrowthStrategy(enum.Enum):
+    """Tree growth policy (training/gbdt/expansion.rs:46-57)."""
+
+    Depthwise = 0
+    Leafwise = 1
+
+
+class Objective:
+    """Loss functions (training/objectives/mod.rs:196-219) the engine trains."""
+
+    class Squared:
+        code = _n.OBJ_SQUARED
+        n_outputs = 1
+
+        def __repr__(self):
+            return "Objective.Squared()"
+
+    class Logistic:
+        code = _n.OBJ_LOGISTIC
+        n_outputs = 1
+
+        def __repr__(self):
+            return "Objective.Logistic()"
+
+    class Softmax:
+        code = _n.OBJ_SOFTMAX
+
+        def __init__(self, n_classes):
+            if int(n_classes) < 2:
+                raise ValueError("n_classes must be >= 2")
+            self.n_classes = int(n_classes)
+            self.n_outputs = self.n_classes
+
+        def __repr__(self):
+            return f"Objective.Softmax(n_classes={self.n_classes})"
+
+    @staticmethod
+    def squared():
+        return Objective.Squared()
+
+    @staticmethod
+    def logistic():
+        return Objective.Logistic()
+
+    @staticmethod
+    def softmax(n_classes):
+        return Objective.Softmax(n_classes)
+
+
+class Metric:
+    """Evaluation metrics (training/metrics/mod.rs)."""
+
+    class Rmse:
+        code = _n.METRIC_RMSE
+
+    class LogLoss:
+        code = _n.METRIC_LOGLOSS
+
+    class MultiLogLoss:
+        code = _n.METRIC_MLOGLOSS
+
+    class NoMetric:
+        code = _n.METRIC_NONE
+
+    @staticmethod
+    def rmse():
+        return Metric.Rmse()
+
+    @staticmethod
+    def logloss():
+        return Metric.LogLoss()
+
+    @staticmethod
+    def mlogloss():
+        return Metric.MultiLogLoss()
+
+    @staticmethod
+    def none():
+        return Metric.NoMetric()
+
+
+_PRECISION = {"fp32": _n.PRECISION_FP32, "q16": _n.PRECISION_Q16, "q8": _n.PRECISION_Q8}
+
+
+class GBDTConfig:
+    """GBDT configuration with the reference's names and defaults
+    (packages/boosters-python/src/config.rs:160-560, model/gbdt/config.rs:111-226),
+    plus GPU options (precision, cuda_graph, device)."""
+
+    def __init__(self, n_estimators=100, learning_rate=0.3, objective=None, metric=None,
+                 growth_strategy=GrowthStrategy.Depthwise, max_depth=6, n_leaves=31,
+                 max_onehot_cats=4, l1=0.0, l2=1.0, min_gain_to_split=0.0, min_child_weight=1.0,
+                 min_samples_leaf=1, subsample=1.0, colsample_bytree=1.0, colsample_bylevel=1.0,
+                 max_bins=256, enable_bundling=True, sparsity_threshold=0.9,
+                 max_categorical_cardinality=0, binning_sample_cnt=200000, cache_size=8,
+                 early_stopping_rounds=None, seed=42, verbosity=0, precision="fp32",
+                 cuda_graph=False, device=0):
+        self.n_estimators = n_estimators
+        self.learning_rate = learning_rate
+        self.objective = objective if objective is not None else Objective.Squared()
+        self.metric = metric
+        self.growth_strategy = growth_strategy
+        self.max_depth = max_depth
+        self.n_leaves = n_leaves
+        self.max_onehot_cats = max_onehot_cats
+        self.l1 = l1
+        self.l2 = l2
+        self.min_gain_to_split = min_gain_to_split
+        self.min_child_weight = min_child_weight
+        self.min_samples_leaf = min_samples_leaf
+        self.subsample = subsample
+        self.colsample_bytree = colsample_bytree
+        self.colsample_bylevel = colsample_bylevel
+        self.max_bins = max_bins
+        self.enable_bundling = enable_bundling
+        self.sparsity_threshold = sparsity_threshold
+        self.max_categorical_cardinality = max_categorical_cardinality
+        self.binning_sample_cnt = binning_sample_cnt
+        self.cache_size = cache_size
+        self.early_stopping_rounds = early_stopping_rounds
+        self.seed = seed
+        self.verbosity = verbosity
+        if precision not in _PRECISION:
+            raise ValueError(f"precision must be one of {sorted(_PRECISION)}")
+        self.precision = precision
+        self.cuda_graph = cuda_graph
+        self.device = device
+        _n.check(_n.lib.bst_config_validate(ctypes.byref(self.to_c())))
+
+    def to_c(self, record_leaves=False):
+        c = _n.Config()
+        _n.lib.bst_config_default(ctypes.byref(c))
+        c.objective = self.objective.code
+        c.n_classes = getattr(self.objective, "n_classes", 0)
+        c.metric = _n.METRIC_DEFAULT if self.metric is None else self.metric.code
+        c.n_trees = int(self.n_estimators)
+        c.learning_rate = float(self.learning_rate)
+        c.growth_strategy = GrowthStrategy(self.growth_strategy).value
+        c.max_depth = int(self.max_depth)
+        c.max_leaves = int(self.n_leaves)
+        c.max_onehot_cats = int(self.max_onehot_cats)
+        c.lambda_ = float(self.l2)
+        c.alpha = float(self.l1)
+        c.min_child_weight = float(self.min_child_weight)
+        c.min_gain = float(self.min_gain_to_split)
+        c.min_samples_leaf = int(self.min_samples_leaf)
+        c.subsample = float(self.subsample)
+        c.colsample_bytree = float(self.colsample_bytree)
+        c.colsample_bylevel = float(self.colsample_bylevel)
+        c.max_bins = int(self.max_bins)
+        c.sparsity_threshold = float(self.sparsity_threshold)
+        c.enable_bundling = 1 if self.enable_bundling else 0
+        c.max_categorical_cardinality = int(self.max_categorical_cardinality)
+        c.binning_sample_cnt = int(self.binning_sample_cnt)
+        c.early_stopping_rounds = -1 if self.early_stopping_rounds is None else int(self.early_stopping_rounds)
+        c.cache_size = int(self.cache_size)
+        c.seed = int(self.seed)
+        c.verbosity = int(self.verbosity)
+        c.precision = _PRECISION[self.precision]
+        c.cuda_graph = 1 if self.cuda_graph else 0
+        c.device = int(self.device)
+        c.record_leaves = 1 if record_leaves else 0
+        return c
+
+    def __repr__(self):
+        return (f"GBDTConfig(n_estimators={self.n_estimators}, learning_rate={self.learning_rate}, "
+                f"objective={self.objective!r}, growth_strategy={self.growth_strategy}, "
+                f"max_depth={self.max_depth}, n_leaves={self.n_leaves})")
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Dataset:
+    """Training / prediction data (packages/boosters-python/src/data.rs:252-294).
+
+    ``features`` is sample-major ``(n_samples, n_features)`` like the
+    reference's Python Dataset; use :meth:`from_feature_major` to pass the
+    core library's feature-major ``[n_features, n_samples]`` layout directly.
+    ``labels`` is ``(n_samples,)`` or ``(n_outputs, n_samples)``.
+    """
+
+    def __init__(self, features, labels=None, weights=None, feature_names=None,
+                 categorical_features=None, _feature_major=False):
+        x = np.asarray(features)
+        if x.ndim != 2:
+            raise ValueError("features must be 2-D")
+        xfm = _f32(x if _feature_major else x.T)
+        n_features, n_samples = xfm.shape
+        y = None
+        n_outputs = 0
+        if labels is not None:
+            y = _f32(labels)
+            if y.ndim == 1:
+                y = y.reshape(1, -1)
+            if y.shape[1] != n_samples:
+                raise ValueError("labels must have one value per sample")
+            n_outputs = y.shape[0]
+        w = None
+        if weights is not None:
+            w = _f32(weights).reshape(-1)
+            if w.shape[0] != n_samples:
+                raise ValueError("weights must have one value per sample")
+        cats = np.ascontiguousarray(sorted(set(categorical_features or [])), dtype=np.uint32)
+        h = ctypes.c_void_p()
+        _n.check(_n.lib.bst_dataset_create(
+            _n.ptr(xfm, ctypes.c_float), n_features, n_samples, _n.ptr(y, ctypes.c_float), n_outputs,
+            _n.ptr(w, ctypes.c_float), _n.ptr(cats, ctypes.c_uint32) if len(cats) else None, len(cats),
+            ctypes.byref(h)))
+        self._h = h
+        self.n_samples = int(n_samples)
+        self.n_features = int(n_features)
+        self.has_labels = y is not None
+        self.has_weights = w is not None
+        self.feature_names = list(feature_names) if feature_names is not None else None
+        self.categorical_features = [int(c) for c in cats]
+
+    @classmethod
+    def from_feature_major(cls, features, labels=None, weights=None, categorical_features=None):
+        """Dataset::from_array layout (data/raw/dataset.rs:139): ``[n_features, n_samples]``."""
+        return cls(features, labels, weights, None, categorical_features, _feature_major=True)
+
+    @property
+    def shape(self):
+        return (self.n_samples, self.n_features)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _n.lib.bst_dataset_free(h)
+            self._h = None
+
+    def __repr__(self):
+        return f"Dataset(n_samples={self.n_samples}, n_features={self.n_features})"
+
+
+class BinnedDataset:
+    """GPU-resident binned dataset (data/binned/dataset.rs:207 from_dataset)."""
+
+    def __init__(self, dataset, config=None):
+        cfg = (config or GBDTConfig()).to_c()
+        h = ctypes.c_void_p()
+        _n.check(_n.lib.bst_binned_create(dataset._h, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self.n_samples = dataset.n_samples
+
+    @property
+    def n_columns(self):
+        return int(_n.lib.bst_binned_n_columns(self._h))
+
+    def column_info(self, col):
+        f, nb, dflt = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        cat, miss = ctypes.c_int32(), ctypes.c_int32()
+        _n.check(_n.lib.bst_binned_column_info(self._h, col, ctypes.byref(f), ctypes.byref(nb), ctypes.byref(cat),
+                                               ctypes.byref(miss), ctypes.byref(dflt)))
+        return {"feature": f.value, "n_bins": nb.value, "is_categorical": bool(cat.value),
+                "has_missing": bool(miss.value), "default_bin": dflt.value}
+
+    def column_bounds(self, col):
+        nb = self.column_info(col)["n_bins"]
+        out = np.zeros(nb, dtype=np.float64)
+        _n.check(_n.lib.bst_binned_column_bounds(self._h, col, _n.ptr(out, ctypes.c_double)))
+        return out
+
+    def column_bins(self, col):
+        out = np.zeros(self.n_samples, dtype=np.uint16)
+        _n.check(_n.lib.bst_binned_column_bins(self._h, col, _n.ptr(out, ctypes.c_uint16)))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _n.lib.bst_binned_free(h)
+            self._h = None
+
+
+class GBDTModel:
+    """Gradient-boosted trees (model/gbdt/model.rs:115-258)."""
+
+    def __init__(self, handle, config):
+        self._h = handle
+        self.config = config
+
+    @staticmethod
+    def train(train, config=None, val_set=None, n_threads=0, record_leaves=False):
+        """GBDTModel::train. ``n_threads`` keeps the reference's split tie-break
+        semantics: 1 = sequential, otherwise the rayon reduction order."""
+        config = config or GBDTConfig()
+        c = config.to_c(record_leaves=record_leaves)
+        h = ctypes.c_void_p()
+        _n.check(_n.lib.bst_gbdt_train(train._h, val_set._h if val_set is not None else None, ctypes.byref(c),
+                                       int(n_threads), ctypes.byref(h)))
+        m = GBDTModel(h, config)
+        m._rows = train.n_samples
+        return m
+
+    @staticmethod
+    def grow_tree(dataset, grad, hess, config=None, n_threads=0):
+        """TreeGrower::grow on given gradients: a one-tree model."""
+        config = config or GBDTConfig()
+        c = config.to_c(record_leaves=True)
+        g, h = _f32(grad), _f32(hess)
+        hd = ctypes.c_void_p()
+        _n.check(_n.lib.bst_tree_grow(dataset._h, _n.ptr(g, ctypes.c_float), _n.ptr(h, ctypes.c_float),
+                                      ctypes.byref(c), int(n_threads), ctypes.byref(hd)))
+        m = GBDTModel(hd, config)
+        m._rows = dataset.n_samples
+        return m
+
+    @staticmethod
+    def from_trees(n_features, trees, objective=None, base_scores=(0.0,)):
+        """Model from explicit tree arrays (dicts with the keys of :meth:`tree`)."""
+        objective = objective or Objective.Squared()
+        b = _f32(base_scores)
+        hd = ctypes.c_void_p()
+        _n.check(_n.lib.bst_model_create(len(b), n_features, objective.code, _n.ptr(b, ctypes.c_float),
+                                         ctypes.byref(hd)))
+        m = GBDTModel(hd, None)
+        m._rows = 0
+        P = _n.ptr
+        for t in trees:
+            a = {k: np.ascontiguousarray(v) for k, v in t.items() if isinstance(v, (list, tuple, np.ndarray))}
+            u32 = lambda k: np.ascontiguousarray(a[k], dtype=np.uint32)
+            u8 = lambda k: np.ascontiguousarray(a[k], dtype=np.uint8)
+            keep = [u32("split_index"), _f32(a["threshold"]), u32("left"), u32("right"), u8("default_left"),
+                    u8("is_leaf"), _f32(a["leaf_value"]),
+                    u8("split_type") if "split_type" in a else None,
+                    u32("seg_start") if "seg_start" in a else None,
+                    u32("seg_size") if "seg_size" in a else None,
+                    u32("cat_words") if len(a.get("cat_words", [])) else None]
+            nw = 0 if keep[10] is None else len(keep[10])
+            _n.check(_n.lib.bst_model_add_tree(
+                hd, int(t.get("group", 0)), len(keep[0]), P(keep[0], ctypes.c_uint32), P(keep[1], ctypes.c_float),
+                P(keep[2], ctypes.c_uint32), P(keep[3], ctypes.c_uint32), P(keep[4], ctypes.c_uint8),
+                P(keep[5], ctypes.c_uint8), P(keep[6], ctypes.c_float), P(keep[7], ctypes.c_uint8),
+                P(keep[8], ctypes.c_uint32), P(keep[9], ctypes.c_uint32), P(keep[10], ctypes.c_uint32), nw))
+        return m
+
+    @property
+    def n_trees(self):
+        return int(_n.lib.bst_model_n_trees(self._h))
+
+    @property
+    def n_groups(self):
+        return int(_n.lib.bst_model_n_groups(self._h))
+
+    @property
+    def n_features(self):
+        return int(_n.lib.bst_model_n_features(self._h))
+
+    @property
+    def is_fitted(self):
+        return True
+
+    def _predict(self, data, raw):
+        out = np.zeros((self.n_groups, data.n_samples), dtype=np.float32)
+        fn = _n.lib.bst_gbdt_predict_raw if raw else _n.lib.bst_gbdt_predict
+        _n.check(fn(self._h, data._h, 0, _n.ptr(out, ctypes.c_float)))
+        return out
+
+    def predict(self, data, n_threads=0):
+        """Transformed predictions, shape ``(n_samples, n_outputs)``."""
+        return self._predict(data, False).T.copy()
+
+    def predict_raw(self, data, n_threads=0):
+        """Raw margins, shape ``(n_samples, n_outputs)``."""
+        return self._predict(data, True).T.copy()
+
+    def predict_group_major(self, data, raw=False):
+        """Predictions in the core library's ``[n_groups, n_samples]`` layout."""
+        return self._predict(data, raw)
+
+    def base_scores(self):
+        out = np.zeros(self.n_groups, dtype=np.float32)
+        _n.check(_n.lib.bst_model_base_scores(self._h, _n.ptr(out, ctypes.c_float)))
+        return out
+
+    def train_predictions(self):
+        """Raw training predictions ``[n_groups, n_samples]`` after the last round."""
+        n = self._n_train_rows()
+        out = np.zeros((self.n_groups, n), dtype=np.float32)
+        _n.check(_n.lib.bst_model_train_predictions(self._h, _n.ptr(out, ctypes.c_float)))
+        return out
+
+    def _n_train_rows(self):
+        return int(self._rows)
+
+    def tree(self, i):
+        """SoA arrays of tree ``i`` (repr/gbdt/tree.rs:32-47) plus training detail."""
+        nn, grp, nw = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        _n.check(_n.lib.bst_model_tree_info(self._h, i, ctypes.byref(nn), ctypes.byref(grp), ctypes.byref(nw)))
+        n = nn.value
+        t = {"n_nodes": n, "group": grp.value,
+             "split_index": np.zeros(n, np.uint32), "threshold": np.zeros(n, np.float32),
+             "left": np.zeros(n, np.uint32), "right": np.zeros(n, np.uint32),
+             "default_left": np.zeros(n, np.uint8), "is_leaf": np.zeros(n, np.uint8),
+             "leaf_value": np.zeros(n, np.float32), "split_type": np.zeros(n, np.uint8),
+             "gain": np.zeros(n, np.float32), "cover": np.zeros(n, np.float32),
+             "seg_start": np.zeros(n, np.uint32), "seg_size": np.zeros(n, np.uint32),
+             "cat_words": np.zeros(nw.value, np.uint32), "split_bin": np.zeros(n, np.uint32),
+             "grad_sum": np.zeros(n, np.float64), "hess_sum": np.zeros(n, np.float64)}
+        P = _n.ptr
+        _n.check(_n.lib.bst_model_tree_nodes(
+            self._h, i, P(t["split_index"], ctypes.c_uint32), P(t["threshold"], ctypes.c_float),
+            P(t["left"], ctypes.c_uint32), P(t["right"], ctypes.c_uint32), P(t["default_left"], ctypes.c_uint8),
+            P(t["is_leaf"], ctypes.c_uint8), P(t["leaf_value"], ctypes.c_float), P(t["split_type"], ctypes.c_uint8),
+            P(t["gain"], ctypes.c_float), P(t["cover"], ctypes.c_float)))
+        _n.check(_n.lib.bst_model_tree_categories(self._h, i, P(t["seg_start"], ctypes.c_uint32),
+                                                  P(t["seg_size"], ctypes.c_uint32),
+                                                  P(t["cat_words"], ctypes.c_uint32) if nw.value else None))
+        _n.check(_n.lib.bst_model_tree_train_info(self._h, i, P(t["split_bin"], ctypes.c_uint32),
+                                                  P(t["grad_sum"], ctypes.c_double), P(t["hess_sum"], ctypes.c_double)))
+        return t
+
+    def tree_row_leaves(self, i, n_rows):
+        out = np.zeros(n_rows, dtype=np.uint32)
+        _n.check(_n.lib.bst_model_tree_row_leaves(self._h, i, _n.ptr(out, ctypes.c_uint32)))
+        return out
+
+    def train_timings(self):
+        """Device milliseconds per phase of the training call."""
+        out = np.zeros(8, dtype=np.float64)
+        _n.check(_n.lib.bst_model_train_timings(self._h, _n.ptr(out, ctypes.c_double)))
+        keys = ["binning", "gradients", "histograms", "split_scan", "partition", "leaf_update", "other", "total"]
+        return dict(zip(keys, out.tolist()))
+
+    def train_counters(self):
+        out = np.zeros(6, dtype=np.uint64)
+        _n.check(_n.lib.bst_model_train_counters(self._h, _n.ptr(out, ctypes.c_uint64), 6))
+        keys = ["launches", "hist_launches", "hist_rows", "hist_bytes", "scan_launches", "partition_rows"]
+        return dict(zip(keys, (int(v) for v in out)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _n.lib.bst_model_free(h)
+            self._h = None
+
+    def __repr__(self):
+        return f"GBDTModel(n_trees={self.n_trees}, n_features={self.n_features})"
+
+
+_TIMING_KEYS = ["binning", "gradients", "histograms", "split_scan", "partition", "leaf_update", "other", "total"]
+_COUNTER_KEYS = ["launches", "hist_launches", "hist_rows", "hist_bytes", "scan_launches", "partition_rows"]
+
+
+class Booster:
+    """Incremental training on a GPU-resident binned dataset: the boosting loop
+    of GBDTTrainer::train (training/gbdt/trainer.rs:242-401), ``update(k)``
+    runs k more rounds."""
+
+    def __init__(self, train, config=None, n_threads=0):
+        self.config = config or GBDTConfig()
+        c = self.config.to_c()
+        h = ctypes.c_void_p()
+        _n.check(_n.lib.bst_booster_create(train._h, ctypes.byref(c), int(n_threads), ctypes.byref(h)))
+        self._h = h
+        self._rows = train.n_samples
+
+    def update(self, n_rounds=1):
+        _n.check(_n.lib.bst_booster_update(self._h, int(n_rounds)))
+
+    @property
+    def n_rounds(self):
+        return int(_n.lib.bst_booster_n_rounds(self._h))
+
+    def model(self):
+        h = ctypes.c_void_p()
+        _n.check(_n.lib.bst_booster_model(self._h, ctypes.byref(h)))
+        m = GBDTModel(h, self.config)
+        m._rows = self._rows
+        return m
+
+    def stats(self):
+        t = np.zeros(8, np.float64)
+        c = np.zeros(6, np.uint64)
+        _n.check(_n.lib.bst_booster_stats(self._h, _n.ptr(t, ctypes.c_double), _n.ptr(c, ctypes.c_uint64), 6))
+        return dict(zip(_TIMING_KEYS, t.tolist())), dict(zip(_COUNTER_KEYS, (int(v) for v in c)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _n.lib.bst_booster_free(h)
+            self._h = None
+
+
+def metric(kind, preds_group_major, labels, weights=None):
+    """Metric value (training/metrics): kind in {'rmse', 'logloss', 'mlogloss'}."""
+    codes = {"rmse": _n.METRIC_RMSE, "logloss": _n.METRIC_LOGLOSS, "mlogloss": _n.METRIC_MLOGLOSS}
+    p = _f32(preds_group_major)
+    if p.ndim == 1:
+        p = p.reshape(1, -1)
+    y = _f32(labels).reshape(-1)
+    w = None if weights is None else _f32(weights).reshape(-1)
+    out = ctypes.c_double()
+    _n.check(_n.lib.bst_metric(codes[kind], _n.ptr(p, ctypes.c_float), p.shape[0], p.shape[1],
+                               _n.ptr(y, ctypes.c_float), _n.ptr(w, ctypes.c_float), ctypes.byref(out)))
+    return out.value
+
+
+class synth:
+    """Seeded synthetic workloads; every array is feature-major ``[F, n]``."""
+
+    @staticmethod
+    def regression(n, n_features, n_informative=20, seed=1, stream=0):
+        x = np.empty((n_features, n), dtype=np.float32)
+        y = np.empty(n, dtype=np.float32)
+        _n.check(_n.lib.bst_synth_regression(n, n_features, n_informative, seed, stream,
+                                             _n.ptr(x, ctypes.c_float), _n.ptr(y, ctypes.c_float)))
+        return x, y
+
+    @staticmethod
+    def binary(n, n_features, n_nan_cols=20, seed=2, stream=0):
+        x = np.empty((n_features, n), dtype=np.float32)
+        y = np.empty(n, dtype=np.float32)
+        _n.check(_n.lib.bst_synth_binary(n, n_features, n_nan_cols, seed, stream,
+                                         _n.ptr(x, ctypes.c_float), _n.ptr(y, ctypes.c_float)))
+        return x, y
+
+    @staticmethod
+    def multiclass(n, n_numeric=40, n_categorical=10, n_classes=10, seed=4, stream=0):
+        x = np.empty((n_numeric + n_categorical, n), dtype=np.float32)
+        y = np.empty(n, dtype=np.float32)
+        _n.check(_n.lib.bst_synth_multiclass(n, n_numeric, n_categorical, n_classes, seed, stream,
+                                             _n.ptr(x, ctypes.c_float), _n.ptr(y, ctypes.c_float)))
+        return x, y

@@ -1,0 +1,294 @@
+// binning.cpp — per-feature analysis and bin bounds on the host.
+//
+// Semantics follow data/binned/feature_analysis.rs:313-569 (analysis and
+// grouping) and data/binned/dataset.rs:592-750 (bin mappers). Features are
+// processed in parallel; each feature's result depends only on its column.
+#include "binning.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <unordered_set>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace bst {
+
+namespace {
+
+// `f64 as f32` with IEEE overflow to infinity.
+float to_f32(double d) {
+    const double lim = 0x1.ffffffp127;
+    const double fmax = (double)std::numeric_limits<float>::max();
+    if (d >= lim) return std::numeric_limits<float>::infinity();
+    if (d <= -lim) return -std::numeric_limits<float>::infinity();
+    if (d > fmax) return std::numeric_limits<float>::max();
+    if (d < -fmax) return -std::numeric_limits<float>::max();
+    return (float)d;
+}
+
+int32_t trunc_i32(double v) {  // `as i32`: truncate and saturate, NaN -> 0
+    if (std::isnan(v)) return 0;
+    if (v >= 2147483647.0) return 2147483647;
+    if (v <= -2147483648.0) return (int32_t)(-2147483647 - 1);
+    return (int32_t)v;
+}
+
+// Small open-addressing set of distinct f32 values (+0.0 and -0.0 are one
+// value), tracking at most `limit` members like FeatureStats (feature_analysis.rs:296-346).
+struct DistinctFloats {
+    std::vector<uint32_t> slots;  // key bits + 1 (0 = empty)
+    uint32_t mask = 0;
+    size_t size = 0;
+    float first = 0.0f;
+    explicit DistinctFloats(size_t limit) {
+        size_t cap = 16;
+        while (cap < limit * 4) cap <<= 1;
+        slots.assign(cap, 0);
+        mask = (uint32_t)cap - 1;
+    }
+    static uint32_t key(float v) {
+        if (v == 0.0f) v = 0.0f;
+        uint32_t b;
+        std::memcpy(&b, &v, 4);
+        return b;
+    }
+    // returns true if v is new (and inserts it when `insert`)
+    bool probe(float v, bool insert) {
+        uint32_t k = key(v);
+        uint32_t h = (k * 0x9E3779B1u) & mask;
+        while (true) {
+            uint32_t s = slots[h];
+            if (s == 0) {
+                if (insert) {
+                    slots[h] = k + 1;
+                    if (size == 0) first = v;
+                    ++size;
+                }
+                return true;
+            }
+            if (s == k + 1) return false;
+            h = (h + 1) & mask;
+        }
+    }
+};
+
+struct FeatureFacts {
+    bool trivial = true, numeric = true, sparse = false, bundle_candidate = false;
+    uint64_t n_nan = 0;
+};
+
+FeatureFacts analyze(const float* col, uint64_t n, const bst_config& cfg, bool user_cat) {
+    const size_t limit = std::max<size_t>(cfg.max_categorical_cardinality, cfg.max_bins) + 10;
+    DistinctFloats uniq(limit);
+    bool exceeded = false, all_int = true;
+    uint64_t nan = 0, valid = 0, nonzero = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const float v = col[i];
+        if (std::isnan(v)) {
+            ++nan;
+            continue;
+        }
+        ++valid;
+        nonzero += (v != 0.0f);
+        if (all_int && !(v - std::trunc(v) == 0.0f)) all_int = false;
+        if (!exceeded && uniq.probe(v, false)) {
+            if (uniq.size >= limit)
+                exceeded = true;
+            else
+                uniq.probe(v, true);
+        }
+    }
+    FeatureFacts f;
+    const size_t n_unique = uniq.size;
+    f.n_nan = nan;
+    f.trivial = valid == 0 || (n_unique == 1 && uniq.first == 0.0f) || n_unique == 0;
+    const bool binary = n_unique == 2;
+    const bool auto_cat = !user_cat && all_int && n_unique <= cfg.max_categorical_cardinality;
+    f.numeric = user_cat ? false : (binary ? true : !auto_cat);
+    const float density = n == 0 ? 0.0f : (float)nonzero / (float)n;
+    f.sparse = density <= (1.0f - cfg.sparsity_threshold);
+    const double density64 = n == 0 ? 0.0 : (double)nonzero / (double)n;
+    f.bundle_candidate = !f.numeric && density64 <= 1.0 - (double)cfg.sparsity_threshold;
+    return f;
+}
+
+// dataset.rs:598-633: deterministic splitmix64 row sample used for bounds.
+std::vector<uint32_t> binning_sample(uint64_t n, uint64_t k) {
+    std::vector<uint32_t> out;
+    if (n <= k) return out;
+    out.reserve(k);
+    std::unordered_set<uint32_t> seen;
+    seen.reserve(k * 2);
+    uint64_t s = 0xD1B54A32D192ED03ULL ^ n;
+    while (out.size() < k) {
+        s += 0x9E3779B97F4A7C15ULL;
+        uint64_t z = s;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        z ^= z >> 31;
+        const uint32_t r = (uint32_t)(z % n);
+        if (seen.insert(r).second) out.push_back(r);
+    }
+    std::sort(out.begin(), out.end());
+    return out;
+}
+
+// dataset.rs:683-750: quantile midpoints over the distinct finite values.
+Mapper numeric_mapper(std::vector<float>& vals, uint32_t max_bins, bool has_nan) {
+    float lo = std::numeric_limits<float>::max(), hi = -std::numeric_limits<float>::max();
+    size_t w = 0;
+    for (size_t i = 0; i < vals.size(); ++i) {
+        const float v = vals[i];
+        if (std::isfinite(v)) {
+            lo = std::min(lo, v);
+            hi = std::max(hi, v);
+            vals[w++] = v;
+        }
+    }
+    vals.resize(w);
+    Mapper m;
+    if (w == 0 || lo >= hi) {
+        m.bounds = {std::numeric_limits<double>::max()};
+        m.n_bins = 1;
+        return m;
+    }
+    const uint32_t nb = (uint32_t)std::min<uint64_t>(max_bins, w);
+    std::sort(vals.begin(), vals.end());
+    vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+    const size_t u = vals.size();
+    if (u <= nb) {
+        for (size_t i = 0; i + 1 < u; ++i) m.bounds.push_back(((double)vals[i] + (double)vals[i + 1]) / 2.0);
+    } else {
+        for (uint32_t i = 1; i < nb; ++i) {
+            const double q = (double)i / (double)nb;
+            const size_t idx = std::min<size_t>((size_t)std::floor(q * (double)(u - 1)), u - 2);
+            const double b = ((double)vals[idx] + (double)vals[idx + 1]) / 2.0;
+            if (m.bounds.empty() || b > m.bounds.back()) m.bounds.push_back(b);
+        }
+    }
+    m.bounds.push_back(std::numeric_limits<double>::max());
+    if (has_nan) m.bounds.push_back(std::numeric_limits<double>::max());
+    m.n_bins = (uint32_t)m.bounds.size();
+    m.missing = has_nan ? MISSING_NAN : MISSING_NONE;
+    m.default_bin = has_nan ? m.n_bins - 1 : 0;
+    return m;
+}
+
+}  // namespace
+
+float f32_round_down(double d) {
+    float r = to_f32(d);
+    if (std::isnan(d)) return r;
+    if ((double)r > d) r = std::nextafter(r, -std::numeric_limits<float>::infinity());
+    return r;
+}
+
+bst_status plan_binning(const float* x, uint64_t F, uint64_t n,
+                        const std::vector<uint8_t>& user_cat, const bst_config& cfg,
+                        BinPlan& plan, std::string& err) {
+    if (n == 0 || F == 0) {
+        err = "dataset is empty";
+        return BST_ERR_EMPTY_DATASET;
+    }
+    if (n > 0xFFFFFFF0ull) {
+        err = "more than 2^32-16 rows are not supported";
+        return BST_ERR_UNSUPPORTED;
+    }
+    plan = BinPlan();
+    plan.n = n;
+    plan.n_features = (uint32_t)F;
+    plan.mappers.resize(F);
+    plan.trivial.assign(F, 0);
+    std::vector<FeatureFacts> facts(F);
+    const std::vector<uint32_t> sample = binning_sample(n, cfg.binning_sample_cnt);
+
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t f = 0; f < (int64_t)F; ++f) {
+        const float* col = x + (uint64_t)f * n;
+        const bool uc = (size_t)f < user_cat.size() && user_cat[f];
+        FeatureFacts ff = analyze(col, n, cfg, uc);
+        facts[f] = ff;
+        if (ff.trivial) continue;
+        if (ff.numeric) {
+            std::vector<float> vals;
+            if (sample.empty())
+                vals.assign(col, col + n);
+            else {
+                vals.resize(sample.size());
+                for (size_t i = 0; i < sample.size(); ++i) vals[i] = col[sample[i]];
+            }
+            plan.mappers[f] = numeric_mapper(vals, cfg.max_bins, ff.n_nan > 0);
+        } else {
+            // every finite value's category, not a sample (dataset.rs:655-672)
+            std::vector<int32_t> c;
+            c.reserve(1024);
+            std::unordered_set<int32_t> seen;
+            for (uint64_t i = 0; i < n; ++i)
+                if (std::isfinite(col[i])) {
+                    const int32_t k = trunc_i32((double)col[i]);
+                    if (seen.insert(k).second) c.push_back(k);
+                }
+            std::sort(c.begin(), c.end());
+            if (c.empty()) c.push_back(0);
+            Mapper m;
+            m.categorical = true;
+            m.n_bins = (uint32_t)c.size();
+            m.cats = std::move(c);
+            plan.mappers[f] = std::move(m);
+        }
+    }
+
+    for (uint64_t f = 0; f < F; ++f) {
+        if (facts[f].trivial) {
+            plan.trivial[f] = 1;
+            continue;
+        }
+        // compute_groups (feature_analysis.rs:655-751) sends these to sparse
+        // storage / EFB bundles, which the GPU engine does not implement.
+        if (facts[f].sparse || (cfg.enable_bundling && facts[f].bundle_candidate)) {
+            err = "feature " + std::to_string(f) +
+                  " has density <= 1 - sparsity_threshold and would use sparse storage, "
+                  "which the GPU engine does not support";
+            return BST_ERR_UNSUPPORTED;
+        }
+        const Mapper& m = plan.mappers[f];
+        if (m.categorical && m.n_bins > 256) {
+            err = "categorical feature " + std::to_string(f) + " has more than 256 categories";
+            return BST_ERR_UNSUPPORTED;
+        }
+        if (m.n_bins > 4096) {
+            err = "feature " + std::to_string(f) + " has more than 4096 bins";
+            return BST_ERR_UNSUPPORTED;
+        }
+    }
+
+    uint32_t off = 0;
+    for (uint64_t f = 0; f < F; ++f) {
+        if (plan.trivial[f]) continue;
+        const Mapper& m = plan.mappers[f];
+        plan.col_feature.push_back((uint32_t)f);
+        plan.col_nbins.push_back(m.n_bins);
+        plan.col_hist_off.push_back(off);
+        plan.col_default.push_back(m.default_bin);
+        plan.col_cat.push_back(m.categorical ? 1 : 0);
+        plan.col_missing.push_back(m.missing != MISSING_NONE ? 1 : 0);
+        if (m.n_bins <= 256) {
+            plan.col_matrix.push_back(0);
+            plan.col_pos.push_back(plan.f8++);
+        } else {
+            plan.col_matrix.push_back(1);
+            plan.col_pos.push_back(plan.f16++);
+        }
+        off += m.n_bins;
+    }
+    plan.total_bins = off;
+    plan.s8 = (plan.f8 + 15) / 16 * 16;
+    plan.s16 = (plan.f16 + 7) / 8 * 8;
+    return BST_OK;
+}
+
+}  // namespace bst

@@ -1,0 +1,812 @@
+// capi.cpp — the extern "C" boundary (include/boosters_c.h).
+// Every entry point catches engine errors and returns a status code; the
+// message of the last failure is kept per thread.
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+
+#include "../../include/boosters_c.h"
+#include "engine.h"
+
+struct bst_dataset {
+    bst::HostDataset d;
+};
+struct bst_binned {
+    bst::DeviceBinned b;
+    int device = 0;
+};
+struct bst_model {
+    std::unique_ptr<bst::Model> m;
+};
+struct bst_booster {
+    std::unique_ptr<bst::Booster> b;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+bst_status fail(bst_status code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+template <class F>
+bst_status guarded(F&& f) {
+    try {
+        g_err.clear();
+        return f();
+    } catch (const bst::Error& e) {
+        return fail(e.code, e.msg);
+    } catch (const std::bad_alloc&) {
+        return fail(BST_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(BST_ERR_INVALID_ARGUMENT, e.what());
+    }
+}
+
+bool ratio_ok(float v) { return v > 0.0f && v <= 1.0f; }
+
+template <class T>
+void copy_out(T* dst, const std::vector<T>& src) {
+    if (dst && !src.empty()) std::memcpy(dst, src.data(), sizeof(T) * src.size());
+}
+
+std::string fmt(float v) {
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%g", (double)v);
+    return buf;
+}
+
+// GBDTConfig::validate (model/gbdt/config.rs:252-310) and engine limits.
+bst_status check_config(const bst_config* c, bool for_training) {
+    if (!c) return fail(BST_ERR_INVALID_ARGUMENT, "config is NULL");
+    if (!(c->learning_rate > 0.0f)) return fail(BST_ERR_CONFIG, "learning_rate must be positive, got " + fmt(c->learning_rate));
+    if (c->n_trees == 0) return fail(BST_ERR_CONFIG, "n_trees must be at least 1");
+    const float* r[3] = {&c->subsample, &c->colsample_bytree, &c->colsample_bylevel};
+    const char* rn[3] = {"subsample", "colsample_bytree", "colsample_bylevel"};
+    for (int i = 0; i < 3; ++i)
+        if (!ratio_ok(*r[i])) return fail(BST_ERR_CONFIG, std::string(rn[i]) + " must be in (0, 1], got " + fmt(*r[i]));
+    const float* g[4] = {&c->lambda, &c->alpha, &c->min_child_weight, &c->min_gain};
+    const char* gn[4] = {"lambda", "alpha", "min_child_weight", "min_gain"};
+    for (int i = 0; i < 4; ++i)
+        if (*g[i] < 0.0f) return fail(BST_ERR_CONFIG, std::string(gn[i]) + " must be non-negative, got " + fmt(*g[i]));
+    if (!for_training) return BST_OK;
+    if (c->objective < BST_OBJ_SQUARED || c->objective > BST_OBJ_SOFTMAX)
+        return fail(BST_ERR_UNSUPPORTED, "objective not supported by the GPU engine");
+    if (c->objective == BST_OBJ_SOFTMAX && c->n_classes < 2) return fail(BST_ERR_CONFIG, "softmax needs n_classes >= 2");
+    if (c->subsample != 1.0f || c->colsample_bytree != 1.0f || c->colsample_bylevel != 1.0f)
+        return fail(BST_ERR_UNSUPPORTED, "row/column subsampling is not supported by the GPU engine");
+    if (c->early_stopping_rounds >= 0)
+        return fail(BST_ERR_UNSUPPORTED, "early stopping is not supported by the GPU engine");
+    if (c->growth_strategy != BST_GROWTH_DEPTHWISE && c->growth_strategy != BST_GROWTH_LEAFWISE)
+        return fail(BST_ERR_CONFIG, "unknown growth strategy");
+    if (c->growth_strategy == BST_GROWTH_DEPTHWISE && c->max_depth > 24)
+        return fail(BST_ERR_UNSUPPORTED, "max_depth > 24 is not supported by the GPU engine");
+    if (c->growth_strategy == BST_GROWTH_LEAFWISE && c->max_leaves < 1)
+        return fail(BST_ERR_CONFIG, "max_leaves must be at least 1");
+    if (c->max_bins < 1) return fail(BST_ERR_CONFIG, "max_bins must be at least 1");
+    if (c->precision != BST_PRECISION_FP32)
+        return fail(BST_ERR_UNSUPPORTED, "only FP32 histogram precision is available in this build");
+    return BST_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bst_last_error(void) { return g_err.c_str(); }
+const char* bst_version(void) { return "boosters-b200 0.1.0 (sm_100a)"; }
+
+void bst_config_default(bst_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->objective = BST_OBJ_SQUARED;
+    c->n_classes = 0;
+    c->metric = BST_METRIC_DEFAULT;
+    c->n_trees = 100;
+    c->learning_rate = 0.3f;
+    c->growth_strategy = BST_GROWTH_DEPTHWISE;
+    c->max_depth = 6;
+    c->max_leaves = 31;
+    c->max_onehot_cats = 4;
+    c->lambda = 1.0f;
+    c->alpha = 0.0f;
+    c->min_child_weight = 1.0f;
+    c->min_gain = 0.0f;
+    c->min_samples_leaf = 1;
+    c->subsample = 1.0f;
+    c->colsample_bytree = 1.0f;
+    c->colsample_bylevel = 1.0f;
+    c->max_bins = 256;
+    c->sparsity_threshold = 0.9f;
+    c->enable_bundling = 1;
+    c->max_categorical_cardinality = 0;
+    c->binning_sample_cnt = 200000;
+    c->early_stopping_rounds = -1;
+    c->cache_size = 8;
+    c->seed = 42;
+    c->verbosity = 0;
+    c->precision = BST_PRECISION_FP32;
+    c->batched = 1;
+    c->cuda_graph = 0;
+    c->device = 0;
+    c->record_leaves = 0;
+}
+
+bst_status bst_config_validate(const bst_config* c) {
+    g_err.clear();
+    return check_config(c, false);
+}
+
+bst_status bst_dataset_create(const float* x, uint64_t F, uint64_t n, const float* y, uint32_t n_outputs,
+                              const float* w, const uint32_t* cat, uint32_t n_cat, bst_dataset** out) {
+    return guarded([&]() -> bst_status {
+        if (!out) return fail(BST_ERR_INVALID_ARGUMENT, "out is NULL");
+        *out = nullptr;
+        if (F == 0) return fail(BST_ERR_EMPTY_DATASET, "features cannot be empty");
+        if (n > 0 && !x) return fail(BST_ERR_INVALID_ARGUMENT, "features is NULL");
+        if (y && n_outputs == 0) return fail(BST_ERR_INVALID_ARGUMENT, "targets given with n_outputs == 0");
+        for (uint32_t i = 0; i < n_cat; ++i)
+            if (!cat || cat[i] >= F) return fail(BST_ERR_INVALID_ARGUMENT, "categorical feature index out of range");
+        auto* ds = new bst_dataset();
+        bst::HostDataset& d = ds->d;
+        d.n = n;
+        d.F = F;
+        d.x.assign(x, x + F * n);
+        if (y) {
+            d.n_outputs = n_outputs;
+            d.y.assign(y, y + (size_t)n_outputs * n);
+        }
+        if (w) {
+            d.has_w = true;
+            d.w.assign(w, w + n);
+        }
+        d.user_cat.assign(F, 0);
+        for (uint32_t i = 0; i < n_cat; ++i) d.user_cat[cat[i]] = 1;
+        *out = ds;
+        return BST_OK;
+    });
+}
+
+void bst_dataset_free(bst_dataset* ds) { delete ds; }
+uint64_t bst_dataset_n_samples(const bst_dataset* ds) { return ds ? ds->d.n : 0; }
+uint64_t bst_dataset_n_features(const bst_dataset* ds) { return ds ? ds->d.F : 0; }
+
+bst_status bst_binned_create(const bst_dataset* ds, const bst_config* cfg, bst_binned** out) {
+    return guarded([&]() -> bst_status {
+        if (!ds || !cfg || !out) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+        *out = nullptr;
+        BST_CK(cudaSetDevice(cfg->device));
+        auto* b = new bst_binned();
+        b->device = cfg->device;
+        cudaStream_t st;
+        BST_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        try {
+            bst::make_binned(ds->d, *cfg, st, b->b);
+        } catch (...) {
+            cudaStreamDestroy(st);
+            delete b;
+            throw;
+        }
+        cudaStreamDestroy(st);
+        *out = b;
+        return BST_OK;
+    });
+}
+
+void bst_binned_free(bst_binned* b) { delete b; }
+uint32_t bst_binned_n_columns(const bst_binned* b) { return b ? b->b.plan.n_cols() : 0; }
+
+bst_status bst_binned_column_info(const bst_binned* b, uint32_t col, uint32_t* feature, uint32_t* n_bins,
+                                  int32_t* is_cat, int32_t* has_missing, uint32_t* default_bin) {
+    if (!b || col >= b->b.plan.n_cols()) return fail(BST_ERR_INVALID_ARGUMENT, "column out of range");
+    const bst::BinPlan& p = b->b.plan;
+    if (feature) *feature = p.col_feature[col];
+    if (n_bins) *n_bins = p.col_nbins[col];
+    if (is_cat) *is_cat = p.col_cat[col];
+    if (has_missing) *has_missing = p.col_missing[col];
+    if (default_bin) *default_bin = p.col_default[col];
+    return BST_OK;
+}
+
+bst_status bst_binned_column_bounds(const bst_binned* b, uint32_t col, double* out) {
+    if (!b || !out || col >= b->b.plan.n_cols()) return fail(BST_ERR_INVALID_ARGUMENT, "column out of range");
+    const bst::Mapper& m = b->b.plan.mappers[b->b.plan.col_feature[col]];
+    for (uint32_t i = 0; i < m.n_bins; ++i) out[i] = m.bin_to_value(i);
+    return BST_OK;
+}
+
+bst_status bst_binned_column_bins(const bst_binned* b, uint32_t col, uint16_t* out) {
+    return guarded([&]() -> bst_status {
+        if (!b || !out || col >= b->b.plan.n_cols()) return fail(BST_ERR_INVALID_ARGUMENT, "column out of range");
+        BST_CK(cudaSetDevice(b->device));
+        const bst::BinPlan& p = b->b.plan;
+        const uint64_t n = p.n;
+        if (p.col_matrix[col] == 0) {
+            std::vector<uint8_t> tmp(n);
+            BST_CK(cudaMemcpy2D(tmp.data(), 1, b->b.bins8.p + p.col_pos[col], p.s8, 1, n, cudaMemcpyDeviceToHost));
+            for (uint64_t i = 0; i < n; ++i) out[i] = tmp[i];
+        } else {
+            BST_CK(cudaMemcpy2D(out, 2, b->b.bins16.p + p.col_pos[col], (size_t)p.s16 * 2, 2, n, cudaMemcpyDeviceToHost));
+        }
+        return BST_OK;
+    });
+}
+
+bst_status bst_gbdt_train(const bst_dataset* train, const bst_dataset* val, const bst_config* cfg,
+                          uint32_t n_threads, bst_model** out) {
+    (void)val;  // only used by metrics / early stopping in the reference
+    return guarded([&]() -> bst_status {
+        if (!out) return fail(BST_ERR_INVALID_ARGUMENT, "out is NULL");
+        *out = nullptr;
+        if (!train) return fail(BST_ERR_INVALID_ARGUMENT, "train dataset is NULL");
+        bst_status rc = check_config(cfg, true);
+        if (rc != BST_OK) return rc;
+        if (train->d.n == 0) return fail(BST_ERR_EMPTY_DATASET, "dataset is empty");
+        if (train->d.y.empty()) return fail(BST_ERR_MISSING_TARGETS, "dataset must have targets for training");
+        auto m = bst::train_model(train->d, *cfg, n_threads);
+        *out = new bst_model{std::move(m)};
+        return BST_OK;
+    });
+}
+
+static bst_status predict_common(const bst_model* m, const bst_dataset* ds, bool raw, float* out) {
+    return guarded([&]() -> bst_status {
+        if (!m || !ds || !out) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+        if (ds->d.F < m->m->n_features)
+            return fail(BST_ERR_INVALID_ARGUMENT, "dataset has fewer features than the model");
+        bst::predict_host(*m->m, ds->d, raw, out);
+        return BST_OK;
+    });
+}
+
+bst_status bst_gbdt_predict(const bst_model* m, const bst_dataset* ds, uint32_t n_threads, float* out) {
+    (void)n_threads;
+    return predict_common(m, ds, false, out);
+}
+bst_status bst_gbdt_predict_raw(const bst_model* m, const bst_dataset* ds, uint32_t n_threads, float* out) {
+    (void)n_threads;
+    return predict_common(m, ds, true, out);
+}
+
+bst_status bst_gbdt_predict_device(const bst_model* m, const float* x, uint64_t n, uint64_t F, int32_t raw,
+                                   float* out, void* stream) {
+    return guarded([&]() -> bst_status {
+        if (!m || (n && (!x || !out))) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+        if (F < m->m->n_features) return fail(BST_ERR_INVALID_ARGUMENT, "fewer features than the model");
+        bst::predict_device(*m->m, x, n, F, raw != 0, out, (cudaStream_t)stream);
+        return BST_OK;
+    });
+}
+
+void bst_model_free(bst_model* m) { delete m; }
+uint32_t bst_model_n_trees(const bst_model* m) { return m ? (uint32_t)m->m->trees.size() : 0; }
+uint32_t bst_model_n_groups(const bst_model* m) { return m ? m->m->n_groups : 0; }
+uint32_t bst_model_n_features(const bst_model* m) { return m ? m->m->n_features : 0; }
+
+bst_status bst_model_base_scores(const bst_model* m, float* out) {
+    if (!m || !out) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::memcpy(out, m->m->base.data(), sizeof(float) * m->m->base.size());
+    return BST_OK;
+}
+
+bst_status bst_model_train_predictions(const bst_model* m, float* out) {
+    if (!m || !out) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::memcpy(out, m->m->train_pred.data(), sizeof(float) * m->m->train_pred.size());
+    return BST_OK;
+}
+
+static const bst::HostTree* tree_at(const bst_model* m, uint32_t t) {
+    if (!m || t >= m->m->trees.size()) {
+        g_err = "tree index out of range";
+        return nullptr;
+    }
+    return &m->m->trees[t];
+}
+
+bst_status bst_model_tree_info(const bst_model* m, uint32_t t, uint32_t* n_nodes, uint32_t* group,
+                               uint32_t* n_words) {
+    const bst::HostTree* tr = tree_at(m, t);
+    if (!tr) return BST_ERR_INVALID_ARGUMENT;
+    if (n_nodes) *n_nodes = (uint32_t)tr->split_index.size();
+    if (group) *group = tr->group;
+    if (n_words) *n_words = (uint32_t)tr->cat_words.size();
+    return BST_OK;
+}
+
+bst_status bst_model_tree_nodes(const bst_model* m, uint32_t t, uint32_t* si, float* thr, uint32_t* l, uint32_t* r,
+                                uint8_t* dl, uint8_t* il, float* lv, uint8_t* st, float* gain, float* cover) {
+    const bst::HostTree* tr = tree_at(m, t);
+    if (!tr) return BST_ERR_INVALID_ARGUMENT;
+    copy_out(si, tr->split_index);
+    copy_out(thr, tr->threshold);
+    copy_out(l, tr->left);
+    copy_out(r, tr->right);
+    copy_out(dl, tr->default_left);
+    copy_out(il, tr->is_leaf);
+    copy_out(lv, tr->leaf);
+    copy_out(st, tr->split_type);
+    copy_out(gain, tr->gain);
+    copy_out(cover, tr->cover);
+    return BST_OK;
+}
+
+bst_status bst_model_tree_categories(const bst_model* m, uint32_t t, uint32_t* ss, uint32_t* sz, uint32_t* words) {
+    const bst::HostTree* tr = tree_at(m, t);
+    if (!tr) return BST_ERR_INVALID_ARGUMENT;
+    copy_out(ss, tr->seg_start);
+    copy_out(sz, tr->seg_size);
+    copy_out(words, tr->cat_words);
+    return BST_OK;
+}
+
+bst_status bst_model_tree_train_info(const bst_model* m, uint32_t t, uint32_t* sb, double* gs, double* hs) {
+    const bst::HostTree* tr = tree_at(m, t);
+    if (!tr) return BST_ERR_INVALID_ARGUMENT;
+    copy_out(sb, tr->split_bin);
+    copy_out(gs, tr->grad_sum);
+    copy_out(hs, tr->hess_sum);
+    return BST_OK;
+}
+
+bst_status bst_model_tree_row_leaves(const bst_model* m, uint32_t t, uint32_t* out) {
+    const bst::HostTree* tr = tree_at(m, t);
+    if (!tr) return BST_ERR_INVALID_ARGUMENT;
+    if (tr->row_leaf.empty()) return fail(BST_ERR_INVALID_ARGUMENT, "model was trained without record_leaves");
+    copy_out(out, tr->row_leaf);
+    return BST_OK;
+}
+
+bst_status bst_model_train_timings(const bst_model* m, double* out8) {
+    if (!m || !out8) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    for (int i = 0; i < 8; ++i) out8[i] = m->m->timings[i];
+    return BST_OK;
+}
+
+bst_status bst_model_train_counters(const bst_model* m, uint64_t* out, uint32_t n) {
+    if (!m || !out) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    const bst::Counters& c = m->m->counters;
+    const uint64_t v[6] = {c.launches, c.hist_launches, c.hist_rows, c.hist_bytes, c.scan_launches, c.partition_rows};
+    for (uint32_t i = 0; i < n && i < 6; ++i) out[i] = v[i];
+    return BST_OK;
+}
+
+bst_status bst_booster_create(const bst_dataset* train, const bst_config* cfg, uint32_t n_threads,
+                              bst_booster** out) {
+    return guarded([&]() -> bst_status {
+        if (!out || !train) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+        *out = nullptr;
+        bst_status rc = check_config(cfg, true);
+        if (rc != BST_OK) return rc;
+        if (train->d.n == 0) return fail(BST_ERR_EMPTY_DATASET, "dataset is empty");
+        if (train->d.y.empty()) return fail(BST_ERR_MISSING_TARGETS, "dataset must have targets for training");
+        *out = new bst_booster{std::make_unique<bst::Booster>(train->d, *cfg, n_threads)};
+        return BST_OK;
+    });
+}
+
+bst_status bst_booster_update(bst_booster* b, uint32_t n_rounds) {
+    return guarded([&]() -> bst_status {
+        if (!b) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+        b->b->update(n_rounds);
+        return BST_OK;
+    });
+}
+
+uint32_t bst_booster_n_rounds(const bst_booster* b) { return b ? b->b->rounds_done() : 0; }
+
+bst_status bst_booster_model(const bst_booster* b, bst_model** out) {
+    return guarded([&]() -> bst_status {
+        if (!b || !out) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+        *out = new bst_model{b->b->snapshot()};
+        return BST_OK;
+    });
+}
+
+bst_status bst_booster_stats(const bst_booster* b, double* t8, uint64_t* c, uint32_t nc) {
+    if (!b) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    const bst::Model& m = b->b->model();
+    if (t8)
+        for (int i = 0; i < 8; ++i) t8[i] = m.timings[i];
+    if (c) {
+        const bst::Counters& k = m.counters;
+        const uint64_t v[6] = {k.launches, k.hist_launches, k.hist_rows, k.hist_bytes, k.scan_launches, k.partition_rows};
+        for (uint32_t i = 0; i < nc && i < 6; ++i) c[i] = v[i];
+    }
+    return BST_OK;
+}
+
+void bst_booster_free(bst_booster* b) { delete b; }
+
+bst_status bst_tree_grow(const bst_dataset* ds, const float* g, const float* h, const bst_config* cfg,
+                         uint32_t n_threads, bst_model** out) {
+    return guarded([&]() -> bst_status {
+        if (!ds || !g || !h || !out) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+        *out = nullptr;
+        bst_status rc = check_config(cfg, false);
+        if (rc != BST_OK) return rc;
+        if (cfg->growth_strategy != BST_GROWTH_DEPTHWISE && cfg->growth_strategy != BST_GROWTH_LEAFWISE)
+            return fail(BST_ERR_CONFIG, "unknown growth strategy");
+        if (ds->d.n == 0) return fail(BST_ERR_EMPTY_DATASET, "dataset is empty");
+        auto m = bst::grow_one_tree(ds->d, g, h, *cfg, n_threads);
+        *out = new bst_model{std::move(m)};
+        return BST_OK;
+    });
+}
+
+bst_status bst_model_create(uint32_t G, uint32_t F, int32_t objective, const float* base, bst_model** out) {
+    return guarded([&]() -> bst_status {
+        if (!out || G == 0 || !base) return fail(BST_ERR_INVALID_ARGUMENT, "bad argument");
+        if (objective < BST_OBJ_SQUARED || objective > BST_OBJ_SOFTMAX) return fail(BST_ERR_INVALID_ARGUMENT, "bad objective");
+        auto m = std::make_unique<bst::Model>();
+        m->n_groups = G;
+        m->n_features = F;
+        m->objective = objective;
+        m->base.assign(base, base + G);
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaGetLastError();
+        m->device = dev;
+        *out = new bst_model{std::move(m)};
+        return BST_OK;
+    });
+}
+
+bst_status bst_model_add_tree(bst_model* mh, uint32_t group, uint32_t nn, const uint32_t* si, const float* thr,
+                              const uint32_t* l, const uint32_t* r, const uint8_t* dl, const uint8_t* il,
+                              const float* lv, const uint8_t* st, const uint32_t* ss, const uint32_t* sz,
+                              const uint32_t* words, uint32_t n_words) {
+    return guarded([&]() -> bst_status {
+        if (!mh || nn == 0 || !si || !thr || !l || !r || !dl || !il || !lv)
+            return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+        bst::Model& m = *mh->m;
+        if (group >= m.n_groups) return fail(BST_ERR_INVALID_ARGUMENT, "group out of range");
+        // validate: children in range and strictly after their parent (no cycles)
+        for (uint32_t i = 0; i < nn; ++i) {
+            if (il[i]) continue;
+            if (l[i] >= nn || r[i] >= nn || l[i] <= i || r[i] <= i)
+                return fail(BST_ERR_INVALID_ARGUMENT, "child index out of range or not after its parent");
+            if (si[i] >= m.n_features) return fail(BST_ERR_INVALID_ARGUMENT, "split feature out of range");
+            if (st && st[i] == 1 && ss && sz && (uint64_t)ss[i] + sz[i] > n_words)
+                return fail(BST_ERR_INVALID_ARGUMENT, "category segment out of range");
+        }
+        bst::HostTree t;
+        for (uint32_t i = 0; i < nn; ++i) t.alloc();
+        for (uint32_t i = 0; i < nn; ++i) {
+            t.split_index[i] = si[i];
+            t.threshold[i] = thr[i];
+            t.left[i] = l[i];
+            t.right[i] = r[i];
+            t.default_left[i] = dl[i] ? 1 : 0;
+            t.is_leaf[i] = il[i] ? 1 : 0;
+            t.leaf[i] = lv[i];
+            t.split_type[i] = st ? st[i] : 0;
+        }
+        t.seg_start.assign(nn, 0);
+        t.seg_size.assign(nn, 0);
+        if (ss && sz) {
+            t.seg_start.assign(ss, ss + nn);
+            t.seg_size.assign(sz, sz + nn);
+        }
+        if (words && n_words) t.cat_words.assign(words, words + n_words);
+        t.group = group;
+        std::lock_guard<std::mutex> lk(m.mu);
+        m.trees.push_back(std::move(t));
+        m.dev.reset();  // rebuild the device forest on next use
+        return BST_OK;
+    });
+}
+
+// ---- component entry points ------------------------------------------------
+
+bst_status bst_bin_values(const double* bounds, uint32_t n_bounds, int32_t missing, uint32_t default_bin,
+                          int32_t is_cat, const int32_t* cats, uint32_t n_cats, const float* values,
+                          uint64_t n, uint32_t* out) {
+    return guarded([&]() -> bst_status {
+        if ((n && (!values || !out)) || (is_cat && n_cats && !cats) || (!is_cat && n_bounds && !bounds))
+            return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+        if (n == 0) return BST_OK;
+        bst::Mapper m;
+        m.categorical = is_cat != 0;
+        m.missing = missing;
+        m.default_bin = default_bin;
+        if (m.categorical) {
+            m.cats.assign(cats, cats + n_cats);
+            m.n_bins = n_cats;
+        } else {
+            m.bounds.assign(bounds, bounds + n_bounds);
+            m.n_bins = n_bounds;
+        }
+        const bool wide = m.n_bins > 256;
+        bst::BinColumn bc;
+        bc.matrix = wide ? 1 : 0;
+        bc.pos = 0;
+        bc.is_cat = m.categorical;
+        bc.nan_bin = m.missing == bst::MISSING_NAN ? (m.n_bins ? m.n_bins - 1 : 0) : m.default_bin;
+        bc.zero_bin = m.missing == bst::MISSING_ZERO ? m.default_bin : 0xFFFFFFFFu;
+        std::vector<float> thr;
+        std::vector<int32_t> cv;
+        bc.off = 0;
+        if (m.categorical) {
+            std::vector<int32_t> sorted(m.cats);
+            for (size_t i = 1; i < sorted.size(); ++i)
+                if (sorted[i] <= sorted[i - 1]) return fail(BST_ERR_INVALID_ARGUMENT, "categories must be strictly increasing");
+            cv = sorted;
+            bc.n_cats = n_cats;
+            bc.n_search = 0;
+        } else {
+            bc.n_cats = 0;
+            bc.n_search = m.n_search();
+            for (uint32_t j = 0; j < bc.n_search; ++j) thr.push_back(bst::f32_round_down(m.bounds[j]));
+        }
+        cudaStream_t st = nullptr;
+        bst::DevArray<float> dx, dthr;
+        bst::DevArray<int32_t> dc;
+        bst::DevArray<bst::BinColumn> dcol;
+        bst::DevArray<uint8_t> b8;
+        bst::DevArray<uint16_t> b16;
+        dx.alloc(n);
+        BST_CK(cudaMemcpy(dx.p, values, sizeof(float) * n, cudaMemcpyHostToDevice));
+        dthr.alloc(std::max<size_t>(1, thr.size()));
+        if (!thr.empty()) BST_CK(cudaMemcpy(dthr.p, thr.data(), sizeof(float) * thr.size(), cudaMemcpyHostToDevice));
+        dc.alloc(std::max<size_t>(1, cv.size()));
+        if (!cv.empty()) BST_CK(cudaMemcpy(dc.p, cv.data(), sizeof(int32_t) * cv.size(), cudaMemcpyHostToDevice));
+        dcol.alloc(1);
+        BST_CK(cudaMemcpy(dcol.p, &bc, sizeof(bc), cudaMemcpyHostToDevice));
+        const uint32_t s8 = wide ? 0 : 16, s16 = wide ? 8 : 0;
+        if (s8) b8.alloc(n * s8);
+        if (s16) b16.alloc(n * s16);
+        bst::launch_bin_assign(dx.p, n, dcol.p, 1, dthr.p, dc.p, b8.p, s8, b16.p, s16, st);
+        BST_CK(cudaGetLastError());
+        BST_CK(cudaDeviceSynchronize());
+        if (!wide) {
+            std::vector<uint8_t> t(n);
+            BST_CK(cudaMemcpy2D(t.data(), 1, b8.p, s8, 1, n, cudaMemcpyDeviceToHost));
+            for (uint64_t i = 0; i < n; ++i) out[i] = t[i];
+        } else {
+            std::vector<uint16_t> t(n);
+            BST_CK(cudaMemcpy2D(t.data(), 2, b16.p, (size_t)s16 * 2, 2, n, cudaMemcpyDeviceToHost));
+            for (uint64_t i = 0; i < n; ++i) out[i] = t[i];
+        }
+        return BST_OK;
+    });
+}
+
+// Power-of-two fixed-point scale with bound * 2^k < 2^62 (as k_fixed_scales).
+static double fixed_scale(double bound) {
+    if (!(bound > 0.0)) return 1.0;
+    int e;
+    std::frexp(bound, &e);
+    int k = 62 - e;
+    k = std::max(-1000, std::min(1000, k));
+    return std::ldexp(1.0, k);
+}
+
+static bst::BinPlan plan_from_counts(const uint32_t* n_bins, uint32_t F, uint64_t n) {
+    bst::BinPlan p;
+    p.n = n;
+    p.n_features = F;
+    uint32_t off = 0;
+    for (uint32_t f = 0; f < F; ++f) {
+        p.col_feature.push_back(f);
+        p.col_nbins.push_back(n_bins[f]);
+        p.col_hist_off.push_back(off);
+        p.col_default.push_back(0);
+        p.col_cat.push_back(0);
+        p.col_missing.push_back(0);
+        if (n_bins[f] <= 256) {
+            p.col_matrix.push_back(0);
+            p.col_pos.push_back(p.f8++);
+        } else {
+            p.col_matrix.push_back(1);
+            p.col_pos.push_back(p.f16++);
+        }
+        off += n_bins[f];
+    }
+    p.total_bins = off;
+    p.s8 = (p.f8 + 15) / 16 * 16;
+    p.s16 = (p.f16 + 7) / 8 * 8;
+    return p;
+}
+
+bst_status bst_histogram_build(const uint16_t* bins, const uint32_t* n_bins, uint32_t F, uint64_t n,
+                               const float* grad, const float* hess, const uint32_t* rows, uint64_t n_rows,
+                               double* out) {
+    return guarded([&]() -> bst_status {
+        if (!bins || !n_bins || !grad || !hess || !out || F == 0) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+        if (n > 0xFFFFFFF0ull) return fail(BST_ERR_UNSUPPORTED, "too many rows");
+        for (uint32_t f = 0; f < F; ++f)
+            if (n_bins[f] == 0 || n_bins[f] > 4096) return fail(BST_ERR_UNSUPPORTED, "bins per feature must be in 1..4096");
+        bst::BinPlan p = plan_from_counts(n_bins, F, n);
+        const uint64_t cnt = rows ? n_rows : n;
+        for (uint64_t i = 0; rows && i < n_rows; ++i)
+            if (rows[i] >= n) return fail(BST_ERR_INVALID_ARGUMENT, "row index out of range");
+        for (uint32_t f = 0; f < F; ++f)
+            for (uint64_t i = 0; i < n; ++i)
+                if (bins[(uint64_t)f * n + i] >= n_bins[f]) return fail(BST_ERR_INVALID_ARGUMENT, "bin out of range");
+        std::vector<uint8_t> m8((size_t)n * p.s8, 0);
+        std::vector<uint16_t> m16((size_t)n * p.s16, 0);
+        for (uint32_t f = 0; f < F; ++f) {
+            const uint16_t* src = bins + (uint64_t)f * n;
+            if (p.col_matrix[f] == 0)
+                for (uint64_t i = 0; i < n; ++i) m8[i * p.s8 + p.col_pos[f]] = (uint8_t)src[i];
+            else
+                for (uint64_t i = 0; i < n; ++i) m16[i * p.s16 + p.col_pos[f]] = src[i];
+        }
+        std::vector<float2> gh(n);
+        float mg = 0.0f, mh = 0.0f;
+        for (uint64_t i = 0; i < n; ++i) {
+            gh[i] = make_float2(grad[i], hess[i]);
+            if (std::fabs(grad[i]) <= 3.4e38f) mg = std::max(mg, std::fabs(grad[i]));
+            if (std::fabs(hess[i]) <= 3.4e38f) mh = std::max(mh, std::fabs(hess[i]));
+        }
+        const double scale[4] = {fixed_scale((double)n * mg), fixed_scale((double)n * mh), 0, 0};
+        std::vector<bst::HistTile> tiles;
+        uint32_t max_smem = 0;
+        bst::build_hist_tiles(p, tiles, max_smem);
+        std::vector<bst::HistChunk> ch;
+        for (uint64_t s = 0; s < cnt; s += 4096)
+            ch.push_back(bst::HistChunk{0, (uint32_t)s, (uint32_t)std::min<uint64_t>(4096, cnt - s), rows ? 0u : 1u});
+        bst::DevArray<uint8_t> d8;
+        bst::DevArray<uint16_t> d16;
+        bst::DevArray<float2> dgh;
+        bst::DevArray<double> dsc;
+        bst::DevArray<uint32_t> dr;
+        bst::DevArray<bst::HistTile> dt;
+        bst::DevArray<bst::HistChunk> dch;
+        bst::DevArray<bst::HBin> dh;
+        if (p.s8) {
+            d8.alloc(m8.size());
+            BST_CK(cudaMemcpy(d8.p, m8.data(), m8.size(), cudaMemcpyHostToDevice));
+        }
+        if (p.s16) {
+            d16.alloc(m16.size());
+            BST_CK(cudaMemcpy(d16.p, m16.data(), m16.size() * 2, cudaMemcpyHostToDevice));
+        }
+        dgh.alloc(std::max<uint64_t>(1, n));
+        if (n) BST_CK(cudaMemcpy(dgh.p, gh.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+        dsc.alloc(4);
+        BST_CK(cudaMemcpy(dsc.p, scale, sizeof(scale), cudaMemcpyHostToDevice));
+        dr.alloc(std::max<uint64_t>(1, cnt));
+        if (rows && cnt) BST_CK(cudaMemcpy(dr.p, rows, sizeof(uint32_t) * cnt, cudaMemcpyHostToDevice));
+        dt.alloc(tiles.size());
+        BST_CK(cudaMemcpy(dt.p, tiles.data(), sizeof(bst::HistTile) * tiles.size(), cudaMemcpyHostToDevice));
+        dch.alloc(std::max<size_t>(1, ch.size()));
+        if (!ch.empty()) BST_CK(cudaMemcpy(dch.p, ch.data(), sizeof(bst::HistChunk) * ch.size(), cudaMemcpyHostToDevice));
+        dh.alloc(p.total_bins);
+        BST_CK(cudaMemset(dh.p, 0, sizeof(bst::HBin) * p.total_bins));
+        bst::launch_hist_build(dch.p, (uint32_t)ch.size(), dt.p, (uint32_t)tiles.size(), max_smem, dr.p, dgh.p, dsc.p,
+                               d8.p, p.s8, d16.p, p.s16, dh.p, p.total_bins, nullptr);
+        BST_CK(cudaGetLastError());
+        std::vector<bst::HBin> h(p.total_bins);
+        BST_CK(cudaMemcpy(h.data(), dh.p, sizeof(bst::HBin) * p.total_bins, cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < p.total_bins; ++i) {
+            out[2 * i] = (double)h[i].g / scale[0];
+            out[2 * i + 1] = (double)h[i].h / scale[1];
+        }
+        return BST_OK;
+    });
+}
+
+bst_status bst_find_split(const double* hist, const uint32_t* n_bins, const int32_t* is_cat, const int32_t* has_missing,
+                          uint32_t F, double pg, double ph, uint32_t pc, const bst_config* cfg, uint32_t n_threads,
+                          bst_split* out) {
+    return guarded([&]() -> bst_status {
+        if (!hist || !n_bins || !is_cat || !has_missing || !cfg || !out) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+        bst_status rc = check_config(cfg, false);
+        if (rc != BST_OK) return rc;
+        std::memset(out, 0, sizeof(*out));
+        out->gain = -std::numeric_limits<float>::infinity();
+        if (F == 0) return BST_OK;
+        uint64_t total = 0;
+        for (uint32_t f = 0; f < F; ++f) {
+            if (is_cat[f] && n_bins[f] > 256) return fail(BST_ERR_UNSUPPORTED, "categorical features need <= 256 bins");
+            total += n_bins[f];
+        }
+        double ag = std::fabs(pg), ah = std::fabs(ph);
+        for (uint64_t i = 0; i < total; ++i) {
+            ag += std::fabs(hist[2 * i]);
+            ah += std::fabs(hist[2 * i + 1]);
+        }
+        const double sg = fixed_scale(ag), sh = fixed_scale(ah);
+        std::vector<bst::HBin> h(total);
+        for (uint64_t i = 0; i < total; ++i) {
+            h[i].g = std::llrint(hist[2 * i] * sg);
+            h[i].h = std::llrint(hist[2 * i + 1] * sh);
+        }
+        std::vector<bst::ScanColumn> cols(F);
+        uint32_t off = 0;
+        for (uint32_t f = 0; f < F; ++f) {
+            cols[f] = bst::ScanColumn{n_bins[f], off, is_cat[f] ? 1u : 0u, has_missing[f] ? 1u : 0u};
+            off += n_bins[f];
+        }
+        bst::ScanNode node{0, pc, 1u, 0u, std::llrint(pg * sg), std::llrint(ph * sh)};
+        const double scale[4] = {sg, sh, 1.0 / sg, 1.0 / sh};
+        bst::GainParamsDev gp;
+        gp.lambda = (double)cfg->lambda;
+        gp.min_gain = (double)cfg->min_gain;
+        gp.min_child_weight = (double)cfg->min_child_weight;
+        gp.min_samples_leaf = cfg->min_samples_leaf;
+        gp.max_onehot_cats = cfg->max_onehot_cats;
+        bst::DevArray<bst::HBin> dh;
+        bst::DevArray<bst::ScanColumn> dc;
+        bst::DevArray<bst::ScanNode> dn;
+        bst::DevArray<double> ds;
+        bst::DevArray<bst::ColCand> dcand;
+        bst::DevArray<long long> dtot;
+        bst::DevArray<bst::NodeSplit> dout;
+        dh.alloc(total);
+        BST_CK(cudaMemcpy(dh.p, h.data(), sizeof(bst::HBin) * total, cudaMemcpyHostToDevice));
+        dc.alloc(F);
+        BST_CK(cudaMemcpy(dc.p, cols.data(), sizeof(bst::ScanColumn) * F, cudaMemcpyHostToDevice));
+        dn.alloc(1);
+        BST_CK(cudaMemcpy(dn.p, &node, sizeof(node), cudaMemcpyHostToDevice));
+        ds.alloc(4);
+        BST_CK(cudaMemcpy(ds.p, scale, sizeof(scale), cudaMemcpyHostToDevice));
+        dcand.alloc(F);
+        dtot.alloc(2);
+        dout.alloc(1);
+        bst::launch_split_scan(dn.p, 1, dc.p, F, dh.p, total, ds.p, gp, dcand.p, dtot.p, nullptr);
+        bst::launch_split_reduce(dcand.p, dtot.p, 1, F, (n_threads != 1 && F >= 16) ? 1 : 0, dout.p, nullptr);
+        BST_CK(cudaGetLastError());
+        bst::NodeSplit s;
+        BST_CK(cudaMemcpy(&s, dout.p, sizeof(s), cudaMemcpyDeviceToHost));
+        if (s.flags & 4u) {
+            out->feature = s.col;
+            out->gain = s.gain;
+            out->default_left = (s.flags & 1u) ? 1 : 0;
+            out->is_categorical = (s.flags & 2u) ? 1 : 0;
+            out->bin = s.bin;
+            for (int q = 0; q < 4; ++q) out->left_cats[q] = s.cats[q];
+        }
+        return BST_OK;
+    });
+}
+
+bst_status bst_metric(int32_t metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w,
+                      double* out) {
+    if (!out || (n && (!p || !y))) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = 0.0;
+    if (n == 0) return BST_OK;
+    const double EPS = 1e-15;
+    auto wv = [&](uint64_t i) { return w ? (double)w[i] : 1.0; };
+    auto clampd = [](double v, double lo, double hi) { return v < lo ? lo : (v > hi ? hi : v); };
+    if (metric == BST_METRIC_RMSE) {  // metrics/regression.rs:17-45
+        double sum = 0.0;
+        for (uint32_t g = 0; g < G; ++g) {
+            double ss = 0, sw = 0;
+            for (uint64_t i = 0; i < n; ++i) {
+                const double d = (double)p[(uint64_t)g * n + i] - (double)y[i];
+                ss = ss + wv(i) * d * d;
+                sw = sw + wv(i);
+            }
+            sum += sw > 0.0 ? std::sqrt(ss / sw) : 0.0;
+        }
+        *out = sum / (double)G;
+    } else if (metric == BST_METRIC_LOGLOSS) {  // metrics/classification.rs:13-40
+        double sl = 0, sw = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const double pp = clampd((double)p[i], EPS, 1.0 - EPS), l = (double)y[i];
+            sl = sl + wv(i) * -(l * std::log(pp) + (1.0 - l) * std::log(1.0 - pp));
+            sw = sw + wv(i);
+        }
+        *out = sw > 0.0 ? sl / sw : 0.0;
+    } else if (metric == BST_METRIC_MLOGLOSS) {  // metrics/classification.rs:332-360
+        double sl = 0, sw = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const float r = std::round(y[i]);
+            const uint64_t c = r > 0.0f ? (uint64_t)r : 0;
+            const double pp = clampd(c < G ? (double)p[c * n + i] : EPS, EPS, 1.0 - EPS);
+            sl = sl + wv(i) * -std::log(pp);
+            sw = sw + wv(i);
+        }
+        *out = sw > 0.0 ? sl / sw : 0.0;
+    } else {
+        return fail(BST_ERR_INVALID_ARGUMENT, "unknown metric");
+    }
+    return BST_OK;
+}
+
+}  // extern "C"

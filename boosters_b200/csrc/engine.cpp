@@ -1,0 +1,1118 @@
+// engine.cpp — GBDT training and prediction on one B200.
+//
+// The tree-growth control flow follows boosters' TreeGrower
+// (training/gbdt/grower.rs:265-514) and growth policies
+// (training/gbdt/expansion.rs:87-320); every data-parallel step runs as a
+// kernel from kernels.cu on device-resident data. The host keeps only the
+// tree under construction (a few hundred nodes) and reads back, per level,
+// the partition counts and the chosen splits.
+#include "engine.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+namespace bst {
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error{e == cudaErrorMemoryAllocation ? BST_ERR_OUT_OF_MEMORY : BST_ERR_CUDA,
+                    std::string(what) + ": " + cudaGetErrorString(e)};
+    }
+}
+
+// Column tiles of the histogram kernel: lanes of one 16-byte row vector
+// whose bins fit one shared-memory histogram (<= 4096 bins = 64 KiB).
+void build_hist_tiles(const BinPlan& p, std::vector<HistTile>& tiles, uint32_t& max_smem) {
+    const uint32_t kMaxSmemBins = 4096;
+    tiles.clear();
+    const uint32_t nc = p.n_cols();
+    std::vector<int> col_of8(p.s8, -1), col_of16(p.s16, -1);
+    for (uint32_t c = 0; c < nc; ++c) {
+        if (p.col_matrix[c] == 0)
+            col_of8[p.col_pos[c]] = (int)c;
+        else
+            col_of16[p.col_pos[c]] = (int)c;
+    }
+    auto emit = [&](uint32_t matrix, uint32_t lanes, const std::vector<int>& col_of, uint32_t nvec) {
+        for (uint32_t v = 0; v < nvec; ++v) {
+            HistTile t;
+            std::memset(&t, 0, sizeof(t));
+            t.matrix = matrix;
+            t.vec = v;
+            bool open = false;
+            for (uint32_t l = 0; l < lanes; ++l) {
+                const int c = col_of[v * lanes + l];
+                if (c < 0) continue;
+                const uint32_t nb = p.col_nbins[c];
+                if (open && t.smem_bins + nb > kMaxSmemBins) {
+                    tiles.push_back(t);
+                    std::memset(&t, 0, sizeof(t));
+                    t.matrix = matrix;
+                    t.vec = v;
+                    open = false;
+                }
+                if (!open) {
+                    t.c0 = l;
+                    open = true;
+                }
+                t.lane_smem[l] = t.smem_bins;
+                t.lane_hist[l] = p.col_hist_off[c];
+                t.lane_nbins[l] = nb;
+                t.smem_bins += nb;
+                t.c1 = l + 1;
+            }
+            if (open) tiles.push_back(t);
+        }
+    };
+    emit(0, 16, col_of8, p.s8 / 16);
+    emit(1, 8, col_of16, p.s16 / 8);
+    max_smem = 0;
+    for (auto& t : tiles) max_smem = std::max(max_smem, t.smem_bins);
+}
+
+namespace {
+
+constexpr uint32_t HIST_CHUNK_ROWS = 4096;
+constexpr uint32_t PART_CHUNK_ROWS = 4096;
+constexpr uint32_t SUM_CHUNK_ROWS = 8192;
+
+float to_f32(double d) {
+    const double lim = 0x1.ffffffp127;
+    const double fmax = (double)std::numeric_limits<float>::max();
+    if (d >= lim) return std::numeric_limits<float>::infinity();
+    if (d <= -lim) return -std::numeric_limits<float>::infinity();
+    if (d > fmax) return std::numeric_limits<float>::max();
+    if (d < -fmax) return -std::numeric_limits<float>::max();
+    return (float)d;
+}
+
+// f32::next_up as used for split thresholds (grower.rs:543-556).
+float next_up(float x) {
+    if (std::isnan(x) || x == std::numeric_limits<float>::infinity()) return x;
+    uint32_t b;
+    if (x == 0.0f) {
+        b = 1;
+    } else {
+        std::memcpy(&b, &x, 4);
+        b = x > 0.0f ? b + 1 : b - 1;
+    }
+    float r;
+    std::memcpy(&r, &b, 4);
+    return r;
+}
+
+// GainParams::compute_leaf_weight (training/gbdt/split/gain.rs:151-168).
+float leaf_weight(double g, double h, const bst_config& c) {
+    const double lambda = (double)c.lambda, alpha = (double)c.alpha;
+    if (alpha == 0.0) return to_f32(-g / (h + lambda));
+    const double ag = std::fabs(g);
+    if (ag <= alpha) return 0.0f;
+    const double sign = g > 0.0 ? -1.0 : 1.0;
+    return to_f32(sign * (ag - alpha) / (h + lambda));
+}
+
+std::vector<uint32_t> bitset_words(const unsigned long long cats[4]) {  // categories.rs:145
+    uint32_t mx = 0;
+    bool any = false;
+    for (uint32_t c = 0; c < 256; ++c)
+        if ((cats[c >> 6] >> (c & 63)) & 1ull) {
+            mx = c;
+            any = true;
+        }
+    if (!any) return {};
+    std::vector<uint32_t> w((mx >> 5) + 1, 0);
+    for (uint32_t c = 0; c <= mx; ++c)
+        if ((cats[c >> 6] >> (c & 63)) & 1ull) w[c >> 5] |= 1u << (c & 31);
+    return w;
+}
+
+// Pinned staging area for per-level work lists.
+struct Staging {
+    char* p = nullptr;
+    size_t cap = 0, off = 0;
+    ~Staging() {
+        if (p) cudaFreeHost(p);
+    }
+    void reserve(size_t bytes) {
+        if (bytes <= cap) return;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        BST_CK(cudaMallocHost(&p, bytes));
+        cap = bytes;
+        off = 0;
+    }
+    template <class T>
+    T* take(size_t count) {
+        size_t a = (off + 63) & ~size_t(63);
+        size_t need = a + count * sizeof(T);
+        if (need > cap) throw Error{BST_ERR_OUT_OF_MEMORY, "staging area exhausted"};
+        off = need;
+        return reinterpret_cast<T*>(p + a);
+    }
+    void reset() { off = 0; }
+};
+
+struct Timer {
+    std::vector<cudaEvent_t> evs;
+    std::vector<std::pair<int, size_t>> marks;  // (phase, first event index)
+    size_t used = 0;
+    cudaStream_t st = nullptr;
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    ~Timer() {
+        for (auto e : evs) cudaEventDestroy(e);
+    }
+    cudaEvent_t next() {
+        if (used == evs.size()) {
+            cudaEvent_t e;
+            BST_CK(cudaEventCreate(&e));
+            evs.push_back(e);
+        }
+        return evs[used++];
+    }
+    size_t begin(int phase) {
+        size_t i = used;
+        BST_CK(cudaEventRecord(next(), st));
+        marks.push_back({phase, i});
+        return i;
+    }
+    void end() { BST_CK(cudaEventRecord(next(), st)); }
+    // stream must be idle
+    void collect() {
+        for (auto& m : marks) {
+            float ms = 0;
+            BST_CK(cudaEventElapsedTime(&ms, evs[m.second], evs[m.second + 1]));
+            acc[m.first] += ms;
+        }
+        marks.clear();
+        used = 0;
+    }
+};
+
+enum Phase { PH_BIN = 0, PH_GRAD = 1, PH_HIST = 2, PH_SCAN = 3, PH_PART = 4, PH_LEAF = 5, PH_OTHER = 6 };
+
+struct PNode {
+    uint32_t begin = 0, count = 0;
+};
+
+struct Cand {
+    uint32_t node, tree_node, depth;
+    NodeSplit split;
+    long long G, H;
+    uint32_t count;
+};
+
+class Trainer {
+  public:
+    Trainer(const HostDataset& ds, const DeviceBinned& b, const bst_config& cfg, uint32_t n_threads,
+            cudaStream_t st, Model& model)
+        : ds_(ds), b_(b), p_(b.plan), cfg_(cfg), st_(st), m_(model) {
+        n_ = p_.n;
+        G_ = model.n_groups;
+        n_cols_ = p_.n_cols();
+        last_wins_ = (n_threads != 1) && n_cols_ >= 16;  // find.rs:125-129, utils.rs:152
+        leafwise_ = cfg.growth_strategy == BST_GROWTH_LEAFWISE;
+        const uint32_t max_leaves = leafwise_ ? cfg.max_leaves : (1u << std::min<uint32_t>(cfg.max_depth, 31));
+        max_pnodes_ = std::max<uint32_t>(1, max_leaves);
+        timer_.st = st;
+        gp_.lambda = (double)cfg.lambda;
+        gp_.min_gain = (double)cfg.min_gain;
+        gp_.min_child_weight = (double)cfg.min_child_weight;
+        gp_.min_samples_leaf = cfg.min_samples_leaf;
+        gp_.max_onehot_cats = cfg.max_onehot_cats;
+    }
+
+    void start() { setup(); }
+
+    // One tree on caller-given gradients (TreeGrower::grow, grower.rs:265).
+    HostTree run_external(const float* g, const float* h) {
+        setup_common();
+        const uint64_t n = n_;
+        pred_.alloc(n);
+        BST_CK(cudaMemsetAsync(pred_.p, 0, sizeof(float) * n, st_));
+        gh_.alloc(n);
+        maxabs_.alloc(2);
+        scales_.alloc(4);
+        h_scales_.assign(4, 1.0);
+        std::vector<float2> gh(n);
+        float mg = 0.0f, mh = 0.0f;
+        for (uint64_t i = 0; i < n; ++i) {
+            gh[i] = make_float2(g[i], h[i]);
+            if (std::fabs(g[i]) <= 3.4e38f) mg = std::max(mg, std::fabs(g[i]));
+            if (std::fabs(h[i]) <= 3.4e38f) mh = std::max(mh, std::fabs(h[i]));
+        }
+        unsigned bits[2];
+        std::memcpy(&bits[0], &mg, 4);
+        std::memcpy(&bits[1], &mh, 4);
+        BST_CK(cudaMemcpyAsync(gh_.p, gh.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, st_));
+        BST_CK(cudaMemcpyAsync(maxabs_.p, bits, sizeof(bits), cudaMemcpyHostToDevice, st_));
+        launch_fixed_scales(maxabs_.p, 1, n_, scales_.p, st_);
+        BST_CK(cudaMemcpyAsync(h_scales_.data(), scales_.p, sizeof(double) * 4, cudaMemcpyDeviceToHost, st_));
+        BST_CK(cudaStreamSynchronize(st_));
+        HostTree t = grow(0);
+        m_.train_pred.resize(n);
+        BST_CK(cudaMemcpy(m_.train_pred.data(), pred_.p, sizeof(float) * n, cudaMemcpyDeviceToHost));
+        return t;
+    }
+
+    void run() {
+        setup();
+        rounds(cfg_.n_trees);
+        finish();
+    }
+
+    // Boosting rounds (trainer.rs:242-335): gradients of every output, then
+    // one tree per output.
+    void rounds(uint32_t k) {
+        const int obj = cfg_.objective;
+        for (uint32_t round = 0; round < k; ++round) {
+            timer_.begin(PH_GRAD);
+            BST_CK(cudaMemsetAsync(maxabs_.p, 0, sizeof(unsigned) * 2 * G_, st_));
+            launch_gradients(obj, G_, pred_.p, y_.p, w_.p, n_, gh_.p, maxabs_.p, st_);
+            launch_fixed_scales(maxabs_.p, G_, n_, scales_.p, st_);
+            m_.counters.launches += 2;
+            timer_.end();
+            BST_CK(cudaMemcpyAsync(h_scales_.data(), scales_.p, sizeof(double) * 4 * G_, cudaMemcpyDeviceToHost, st_));
+            BST_CK(cudaStreamSynchronize(st_));
+            for (uint32_t o = 0; o < G_; ++o) {
+                HostTree t = grow(o);
+                t.group = o;
+                std::lock_guard<std::mutex> lk(m_.mu);
+                m_.trees.push_back(std::move(t));
+                m_.dev.reset();
+            }
+        }
+        BST_CK(cudaStreamSynchronize(st_));
+        timer_.collect();
+        for (int i = 1; i < 7; ++i) {
+            m_.timings[i] += timer_.acc[i];
+            timer_.acc[i] = 0.0;
+        }
+        m_.counters.hist_ms = m_.timings[PH_HIST];
+    }
+
+    // Training predictions back to the model.
+    void finish() {
+        m_.train_pred.resize((size_t)G_ * n_);
+        BST_CK(cudaMemcpy(m_.train_pred.data(), pred_.p, sizeof(float) * G_ * n_, cudaMemcpyDeviceToHost));
+    }
+
+  private:
+    const HostDataset& ds_;
+    const DeviceBinned& b_;
+    const BinPlan& p_;
+    const bst_config& cfg_;
+    cudaStream_t st_;
+    Model& m_;
+    uint64_t n_ = 0;
+    uint32_t G_ = 1, n_cols_ = 0, max_pnodes_ = 1;
+    bool last_wins_ = false, leafwise_ = false;
+    GainParamsDev gp_{};
+    Timer timer_;
+    Staging stage_;
+
+    DevArray<float> pred_, y_, w_;
+    DevArray<float2> gh_;
+    DevArray<unsigned> maxabs_;
+    DevArray<double> scales_;
+    std::vector<double> h_scales_;
+    DevArray<uint32_t> ridx_, tmp_, row_leaf_;
+    DevArray<HBin> hist_;
+    uint64_t slot_bins_ = 0;
+    DevArray<HistTile> tiles_;
+    uint32_t n_tiles_ = 0, tile_smem_ = 0;
+    DevArray<ScanColumn> scan_cols_;
+    DevArray<HistChunk> d_hchunks_, d_schunks_;
+    DevArray<FinishWork> d_finish_;
+    DevArray<ScanNode> d_scan_nodes_;
+    DevArray<ColCand> d_cand_;
+    DevArray<long long> d_node_tot_, d_sums_;
+    DevArray<NodeSplit> d_splits_;
+    DevArray<PartWork> d_pworks_;
+    DevArray<PartChunk> d_pchunks_;
+    DevArray<unsigned> d_cursors_;
+    DevArray<LeafSeg> d_leaves_;
+
+    // per-tree state
+    std::vector<PNode> pn_;
+    uint32_t n_pnodes_ = 0;
+    HostTree tree_;
+    std::vector<uint32_t> leaf_tree_node_;  // by partition node
+    std::vector<float> leaf_value_;
+    const float2* gh_o_ = nullptr;
+    const double* scale_o_ = nullptr;
+    double inv_g_ = 1.0, inv_h_ = 1.0;
+
+    void setup() {
+        setup_common();
+        const uint64_t n = n_;
+        pred_.alloc((size_t)G_ * n);
+        y_.alloc(n);
+        if (ds_.has_w) w_.alloc(n);
+        gh_.alloc((size_t)G_ * n);
+        maxabs_.alloc(2 * G_);
+        scales_.alloc(4 * G_);
+        h_scales_.assign(4 * G_, 1.0);
+        // targets: first output row (targets.output(0) in every objective)
+        BST_CK(cudaMemcpyAsync(y_.p, ds_.y.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st_));
+        if (ds_.has_w) BST_CK(cudaMemcpyAsync(w_.p, ds_.w.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st_));
+        std::vector<float> init((size_t)G_ * n);
+        for (uint32_t g = 0; g < G_; ++g) std::fill(init.begin() + (size_t)g * n, init.begin() + (size_t)(g + 1) * n, m_.base[g]);
+        BST_CK(cudaMemcpyAsync(pred_.p, init.data(), sizeof(float) * init.size(), cudaMemcpyHostToDevice, st_));
+        BST_CK(cudaStreamSynchronize(st_));
+    }
+
+    void setup_common() {
+        const uint64_t n = n_;
+        ridx_.alloc(n);
+        tmp_.alloc(n);
+        if (cfg_.record_leaves) row_leaf_.alloc(n);
+        slot_bins_ = p_.total_bins;
+        if (n_cols_) {
+            // one histogram per partition node (the reference's LRU pool is
+            // unnecessary with 180 GB of HBM); refuse sizes that cannot fit
+            size_t free_b = 0, total_b = 0;
+            BST_CK(cudaMemGetInfo(&free_b, &total_b));
+            const double need = (double)max_pnodes_ * (double)slot_bins_ * sizeof(HBin);
+            if (need > 0.6 * (double)free_b)
+                throw Error{BST_ERR_UNSUPPORTED, "node histograms need " + std::to_string((uint64_t)need) +
+                                                     " bytes; reduce max_depth / max_leaves or max_bins"};
+            hist_.alloc((size_t)max_pnodes_ * slot_bins_);
+        }
+        build_tiles();
+        std::vector<ScanColumn> sc(n_cols_);
+        for (uint32_t c = 0; c < n_cols_; ++c)
+            sc[c] = ScanColumn{p_.col_nbins[c], p_.col_hist_off[c], p_.col_cat[c], p_.col_missing[c]};
+        scan_cols_.alloc(std::max<uint32_t>(1, n_cols_));
+        if (n_cols_) BST_CK(cudaMemcpy(scan_cols_.p, sc.data(), sizeof(ScanColumn) * n_cols_, cudaMemcpyHostToDevice));
+
+        const size_t max_chunks = (size_t)(n / 1024 + 2 * (size_t)max_pnodes_ + 16);
+        d_hchunks_.alloc(max_chunks);
+        d_schunks_.alloc(max_chunks);
+        d_pchunks_.alloc(max_chunks);
+        d_finish_.alloc(max_pnodes_ + 1);
+        d_scan_nodes_.alloc(2 * (size_t)max_pnodes_ + 2);
+        d_cand_.alloc((2 * (size_t)max_pnodes_ + 2) * std::max<uint32_t>(1, n_cols_));
+        d_node_tot_.alloc(2 * (2 * (size_t)max_pnodes_ + 2));
+        d_splits_.alloc(2 * (size_t)max_pnodes_ + 2);
+        d_pworks_.alloc(max_pnodes_ + 1);
+        d_cursors_.alloc(2 * ((size_t)max_pnodes_ + 1));
+        d_sums_.alloc(2 * ((size_t)max_pnodes_ + 1));
+        d_leaves_.alloc(max_pnodes_ + 1);
+        stage_.reserve(max_chunks * 48 + (size_t)(max_pnodes_ + 4) * 256 + (1 << 20));
+    }
+
+    void build_tiles() {
+        std::vector<HistTile> tiles;
+        build_hist_tiles(p_, tiles, tile_smem_);
+        n_tiles_ = (uint32_t)tiles.size();
+        if (n_tiles_) {
+            tiles_.alloc(n_tiles_);
+            BST_CK(cudaMemcpy(tiles_.p, tiles.data(), sizeof(HistTile) * n_tiles_, cudaMemcpyHostToDevice));
+        }
+    }
+
+    template <class T>
+    T* upload(const T* host, size_t count, DevArray<T>& dst) {
+        if (count == 0) return dst.p;
+        if (count > dst.n) throw Error{BST_ERR_INVALID_ARGUMENT, "work list exceeds its device buffer"};
+        BST_CK(cudaMemcpyAsync(dst.p, host, sizeof(T) * count, cudaMemcpyHostToDevice, st_));
+        return dst.p;
+    }
+
+    // ---- histograms -----------------------------------------------------------
+    // Builds the histogram of the rows pn[node] into slot `slot` (zeroed by caller).
+    void hist_chunks_for(uint32_t slot, const PNode& pn, bool identity, std::vector<HistChunk>& out) {
+        for (uint32_t s = 0; s < pn.count; s += HIST_CHUNK_ROWS)
+            out.push_back(HistChunk{slot, pn.begin + s, std::min(HIST_CHUNK_ROWS, pn.count - s), identity ? 1u : 0u});
+    }
+
+    void launch_hist(const std::vector<HistChunk>& chunks) {
+        if (chunks.empty() || n_tiles_ == 0) return;
+        HistChunk* h = stage_.take<HistChunk>(chunks.size());
+        std::copy(chunks.begin(), chunks.end(), h);
+        upload(h, chunks.size(), d_hchunks_);
+        timer_.begin(PH_HIST);
+        launch_hist_build(d_hchunks_.p, (uint32_t)chunks.size(), tiles_.p, n_tiles_, tile_smem_, ridx_.p, gh_o_,
+                          scale_o_, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, hist_.p, slot_bins_, st_);
+        timer_.end();
+        uint64_t rows = 0;
+        for (auto& c : chunks) rows += c.count;
+        m_.counters.launches += 1;
+        m_.counters.hist_launches += 1;
+        m_.counters.hist_rows += rows;
+        m_.counters.hist_bytes += rows * ((uint64_t)p_.f8 + 2ull * p_.f16 + 12ull);
+    }
+
+    // ---- split scan ---------------------------------------------------------------
+    void scan(const std::vector<ScanNode>& nodes, std::vector<NodeSplit>& out) {
+        out.resize(nodes.size());
+        if (nodes.empty()) return;
+        ScanNode* h = stage_.take<ScanNode>(nodes.size());
+        std::copy(nodes.begin(), nodes.end(), h);
+        upload(h, nodes.size(), d_scan_nodes_);
+        timer_.begin(PH_SCAN);
+        launch_split_scan(d_scan_nodes_.p, (uint32_t)nodes.size(), scan_cols_.p, n_cols_, hist_.p, slot_bins_,
+                          scale_o_, gp_, d_cand_.p, d_node_tot_.p, st_);
+        launch_split_reduce(d_cand_.p, d_node_tot_.p, (uint32_t)nodes.size(), n_cols_, last_wins_ ? 1 : 0,
+                            d_splits_.p, st_);
+        timer_.end();
+        m_.counters.launches += 2;
+        m_.counters.scan_launches += 1;
+        NodeSplit* hs = stage_.take<NodeSplit>(nodes.size());
+        BST_CK(cudaMemcpyAsync(hs, d_splits_.p, sizeof(NodeSplit) * nodes.size(), cudaMemcpyDeviceToHost, st_));
+        BST_CK(cudaStreamSynchronize(st_));
+        std::copy(hs, hs + nodes.size(), out.begin());
+    }
+
+    // Exact fixed-point sums of the rows of each node (no histogram).
+    void node_sums(const std::vector<PNode>& nodes, std::vector<std::pair<long long, long long>>& out) {
+        out.assign(nodes.size(), {0, 0});
+        if (nodes.empty()) return;
+        std::vector<HistChunk> ch;
+        for (uint32_t j = 0; j < nodes.size(); ++j)
+            for (uint32_t s = 0; s < nodes[j].count; s += SUM_CHUNK_ROWS)
+                ch.push_back(HistChunk{j, nodes[j].begin + s, std::min(SUM_CHUNK_ROWS, nodes[j].count - s), 0u});
+        BST_CK(cudaMemsetAsync(d_sums_.p, 0, sizeof(long long) * 2 * nodes.size(), st_));
+        if (!ch.empty()) {
+            HistChunk* h = stage_.take<HistChunk>(ch.size());
+            std::copy(ch.begin(), ch.end(), h);
+            upload(h, ch.size(), d_schunks_);
+            timer_.begin(PH_OTHER);
+            launch_node_sums(d_schunks_.p, (uint32_t)ch.size(), ridx_.p, gh_o_, scale_o_, d_sums_.p, st_);
+            timer_.end();
+            m_.counters.launches += 1;
+        }
+        long long* hs = stage_.take<long long>(2 * nodes.size());
+        BST_CK(cudaMemcpyAsync(hs, d_sums_.p, sizeof(long long) * 2 * nodes.size(), cudaMemcpyDeviceToHost, st_));
+        BST_CK(cudaStreamSynchronize(st_));
+        for (size_t j = 0; j < nodes.size(); ++j) out[j] = {hs[2 * j], hs[2 * j + 1]};
+    }
+
+    // ---- tree bookkeeping (grower.rs:484-514, 576-650) -----------------------------
+    void make_leaf(const Cand& c) {
+        const double g = (double)c.G * inv_g_, h = (double)c.H * inv_h_;
+        const float w = leaf_weight(g, h, cfg_);
+        const float v = w * cfg_.learning_rate;  // apply_learning_rate (mutable_tree.rs:258)
+        tree_.is_leaf[c.tree_node] = 1;
+        tree_.leaf[c.tree_node] = v;
+        tree_.cover[c.tree_node] = to_f32(h);
+        tree_.grad_sum[c.tree_node] = g;
+        tree_.hess_sum[c.tree_node] = h;
+        if (c.node >= leaf_tree_node_.size()) {
+            leaf_tree_node_.resize(c.node + 1, 0xFFFFFFFFu);
+            leaf_value_.resize(c.node + 1, 0.0f);
+        }
+        leaf_tree_node_[c.node] = c.tree_node;
+        leaf_value_[c.node] = v;
+    }
+
+    // returns (tree node of the training-left child, tree node of the training-right child)
+    std::pair<uint32_t, uint32_t> apply_split(const Cand& c) {
+        const NodeSplit& s = c.split;
+        const uint32_t col = s.col;
+        const uint32_t feat = p_.col_feature[col];
+        const Mapper& m = p_.mappers[feat];
+        const uint32_t nd = c.tree_node;
+        const double g = (double)c.G * inv_g_, h = (double)c.H * inv_h_;
+        tree_.gain[nd] = s.gain;
+        tree_.cover[nd] = to_f32(h);
+        tree_.grad_sum[nd] = g;
+        tree_.hess_sum[nd] = h;
+        const uint32_t l = tree_.alloc(), r = tree_.alloc();
+        tree_.split_index[nd] = feat;
+        tree_.left[nd] = l;
+        tree_.right[nd] = r;
+        tree_.is_leaf[nd] = 0;
+        const bool dl = s.flags & 1u;
+        if (!(s.flags & 2u)) {
+            tree_.threshold[nd] = next_up(to_f32(m.bin_to_value(s.bin)));
+            tree_.default_left[nd] = dl;
+            tree_.split_type[nd] = 0;
+            tree_.split_bin[nd] = s.bin;
+            return {l, r};
+        }
+        // categorical: stored bitset = categories going right at inference,
+        // children swapped and default inverted (grower.rs:612-647)
+        tree_.threshold[nd] = 0.0f;
+        tree_.default_left[nd] = dl ? 0 : 1;
+        tree_.split_type[nd] = 1;
+        cat_nodes_.push_back({nd, bitset_words(s.cats)});
+        return {r, l};
+    }
+
+    std::vector<std::pair<uint32_t, std::vector<uint32_t>>> cat_nodes_;
+
+    void freeze_categories() {  // mutable_tree.rs:299-335
+        const size_t nn = tree_.split_index.size();
+        tree_.seg_start.assign(nn, 0);
+        tree_.seg_size.assign(nn, 0);
+        tree_.cat_words.clear();
+        std::sort(cat_nodes_.begin(), cat_nodes_.end(),
+                  [](const auto& a, const auto& b) { return a.first < b.first; });
+        for (auto& cn : cat_nodes_) {
+            tree_.seg_start[cn.first] = (uint32_t)tree_.cat_words.size();
+            tree_.seg_size[cn.first] = (uint32_t)cn.second.size();
+            tree_.cat_words.insert(tree_.cat_words.end(), cn.second.begin(), cn.second.end());
+        }
+        cat_nodes_.clear();
+    }
+
+    static bool expands(const Cand& c, float min_gain) {  // grower.rs:530-539
+        const bool valid = (c.split.flags & 4u) && c.split.gain > -std::numeric_limits<float>::infinity();
+        return valid && !(c.split.gain <= min_gain);
+    }
+
+    // Splits every parent in `par` (already accepted): partition, child
+    // histograms (smaller child built, larger by subtraction) and child splits.
+    void expand(std::vector<Cand>& par, const std::vector<std::pair<uint32_t, uint32_t>>& tree_children,
+                const std::vector<uint32_t>& right_ids, bool need_split, std::vector<Cand>& children) {
+        const size_t k = par.size();
+        stage_.reset();
+        // 1. partition (partition.rs:296-382)
+        std::vector<PartChunk> pch;
+        PartWork* pw = stage_.take<PartWork>(k);
+        unsigned* cur = stage_.take<unsigned>(2 * k);
+        uint64_t prow = 0;
+        for (size_t j = 0; j < k; ++j) {
+            const Cand& c = par[j];
+            const PNode& pn = pn_[c.node];
+            const uint32_t col = c.split.col;
+            PartWork w;
+            std::memset(&w, 0, sizeof(w));
+            w.begin = pn.begin;
+            w.count = pn.count;
+            w.matrix = p_.col_matrix[col];
+            w.pos = p_.col_pos[col];
+            w.thr_bin = c.split.bin;
+            w.flags = (c.split.flags & 1u) | (p_.col_missing[col] ? 2u : 0u) | ((c.split.flags & 2u) ? 4u : 0u);
+            w.default_bin = p_.col_default[col];
+            for (int q = 0; q < 4; ++q) w.cats[q] = c.split.cats[q];
+            pw[j] = w;
+            cur[2 * j] = pn.begin;
+            cur[2 * j + 1] = pn.begin + pn.count;
+            for (uint32_t s = 0; s < pn.count; s += PART_CHUNK_ROWS)
+                pch.push_back(PartChunk{(uint32_t)j, pn.begin + s, std::min(PART_CHUNK_ROWS, pn.count - s), 0});
+            prow += pn.count;
+        }
+        upload(pw, k, d_pworks_);
+        upload(cur, 2 * k, d_cursors_);
+        PartChunk* hpc = stage_.take<PartChunk>(std::max<size_t>(1, pch.size()));
+        std::copy(pch.begin(), pch.end(), hpc);
+        upload(hpc, pch.size(), d_pchunks_);
+        timer_.begin(PH_PART);
+        launch_partition(d_pworks_.p, d_pchunks_.p, (uint32_t)pch.size(), ridx_.p, tmp_.p, d_cursors_.p, b_.bins8.p,
+                         p_.s8, b_.bins16.p, p_.s16, st_);
+        launch_copy_chunks(d_pchunks_.p, d_pworks_.p, (uint32_t)pch.size(), tmp_.p, ridx_.p, st_);
+        timer_.end();
+        m_.counters.launches += pch.empty() ? 0 : 2;
+        m_.counters.partition_rows += prow;
+        unsigned* hc = stage_.take<unsigned>(2 * k);
+        BST_CK(cudaMemcpyAsync(hc, d_cursors_.p, sizeof(unsigned) * 2 * k, cudaMemcpyDeviceToHost, st_));
+        BST_CK(cudaStreamSynchronize(st_));
+        std::vector<uint32_t> lc(k), rc(k);
+        for (size_t j = 0; j < k; ++j) {
+            const PNode pn = pn_[par[j].node];
+            lc[j] = hc[2 * j] - pn.begin;
+            rc[j] = pn.count - lc[j];
+            pn_[par[j].node] = PNode{pn.begin, lc[j]};
+            pn_[right_ids[j]] = PNode{pn.begin + lc[j], rc[j]};
+        }
+        stage_.reset();
+        children.clear();
+        children.reserve(2 * k);
+        if (need_split && n_cols_ > 0) {
+            // 2. smaller child into the right slot, then subtract (pool.rs:414-432)
+            const uint32_t r_lo = *std::min_element(right_ids.begin(), right_ids.end());
+            const uint32_t r_hi = *std::max_element(right_ids.begin(), right_ids.end());
+            BST_CK(cudaMemsetAsync(hist_.p + (size_t)r_lo * slot_bins_, 0,
+                                   sizeof(HBin) * slot_bins_ * (size_t)(r_hi - r_lo + 1), st_));
+            std::vector<HistChunk> hch;
+            FinishWork* fw = stage_.take<FinishWork>(k);
+            for (size_t j = 0; j < k; ++j) {
+                const bool left_small = lc[j] <= rc[j];  // grower.rs:398-402
+                const uint32_t small = left_small ? par[j].node : right_ids[j];
+                hist_chunks_for(right_ids[j], pn_[small], false, hch);
+                fw[j] = FinishWork{par[j].node, right_ids[j], left_small ? 1u : 0u, 0u};
+            }
+            launch_hist(hch);
+            upload(fw, k, d_finish_);
+            timer_.begin(PH_OTHER);
+            launch_hist_finish(d_finish_.p, (uint32_t)k, hist_.p, slot_bins_, p_.total_bins, st_);
+            timer_.end();
+            m_.counters.launches += 1;
+            // 3. child splits (left, right per parent)
+            std::vector<ScanNode> sn;
+            sn.reserve(2 * k);
+            for (size_t j = 0; j < k; ++j) {
+                sn.push_back(ScanNode{par[j].node, lc[j], 0u, 0u, 0, 0});
+                sn.push_back(ScanNode{right_ids[j], rc[j], 0u, 0u, 0, 0});
+            }
+            std::vector<NodeSplit> res;
+            scan(sn, res);
+            for (size_t j = 0; j < k; ++j) {
+                const uint32_t d = par[j].depth + 1;
+                children.push_back(Cand{par[j].node, tree_children[j].first, d, res[2 * j], res[2 * j].tot_g,
+                                        res[2 * j].tot_h, lc[j]});
+                children.push_back(Cand{right_ids[j], tree_children[j].second, d, res[2 * j + 1],
+                                        res[2 * j + 1].tot_g, res[2 * j + 1].tot_h, rc[j]});
+            }
+        } else {
+            // children will not be split: only their sums are needed
+            std::vector<PNode> smalls(k);
+            for (size_t j = 0; j < k; ++j)
+                smalls[j] = lc[j] <= rc[j] ? pn_[par[j].node] : pn_[right_ids[j]];
+            std::vector<std::pair<long long, long long>> sums;
+            node_sums(smalls, sums);
+            for (size_t j = 0; j < k; ++j) {
+                const bool left_small = lc[j] <= rc[j];
+                const long long sg = sums[j].first, sh = sums[j].second;
+                const long long lg = left_small ? sg : par[j].G - sg, lh = left_small ? sh : par[j].H - sh;
+                const long long rg = par[j].G - lg, rh = par[j].H - lh;
+                NodeSplit inv;
+                std::memset(&inv, 0, sizeof(inv));
+                inv.gain = -std::numeric_limits<float>::infinity();
+                const uint32_t d = par[j].depth + 1;
+                children.push_back(Cand{par[j].node, tree_children[j].first, d, inv, lg, lh, lc[j]});
+                children.push_back(Cand{right_ids[j], tree_children[j].second, d, inv, rg, rh, rc[j]});
+            }
+        }
+    }
+
+    HostTree grow(uint32_t o) {
+        gh_o_ = gh_.p + (size_t)o * n_;
+        scale_o_ = scales_.p + 4 * (size_t)o;
+        inv_g_ = h_scales_[4 * o + 2];
+        inv_h_ = h_scales_[4 * o + 3];
+        tree_ = HostTree();
+        cat_nodes_.clear();
+        leaf_tree_node_.assign(max_pnodes_, 0xFFFFFFFFu);
+        leaf_value_.assign(max_pnodes_, 0.0f);
+        pn_.assign(max_pnodes_ + 1, PNode{});
+        pn_[0] = PNode{0, (uint32_t)n_};
+        n_pnodes_ = 1;
+        stage_.reset();
+        timer_.begin(PH_OTHER);
+        launch_iota(ridx_.p, n_, st_);
+        timer_.end();
+        m_.counters.launches += 1;
+        tree_.alloc();  // root (mutable_tree.rs:80 init_root)
+
+        // root histogram, sums and split (grower.rs:288-308)
+        Cand root;
+        root.node = 0;
+        root.tree_node = 0;
+        root.depth = 0;
+        root.count = (uint32_t)n_;
+        if (n_cols_ > 0) {
+            BST_CK(cudaMemsetAsync(hist_.p, 0, sizeof(HBin) * slot_bins_, st_));
+            std::vector<HistChunk> ch;
+            hist_chunks_for(0, pn_[0], true, ch);
+            launch_hist(ch);
+            std::vector<NodeSplit> res;
+            scan({ScanNode{0, (uint32_t)n_, 0u, 0u, 0, 0}}, res);
+            root.split = res[0];
+            root.G = res[0].tot_g;
+            root.H = res[0].tot_h;
+        } else {
+            std::vector<std::pair<long long, long long>> sums;
+            node_sums({pn_[0]}, sums);
+            std::memset(&root.split, 0, sizeof(root.split));
+            root.split.gain = -std::numeric_limits<float>::infinity();
+            root.G = sums[0].first;
+            root.H = sums[0].second;
+        }
+
+        const float min_gain = cfg_.min_gain;
+        if (!leafwise_) {
+            // depth-wise (expansion.rs:137-196)
+            std::vector<Cand> cur{root}, next;
+            uint32_t depth = 0;
+            while (depth < cfg_.max_depth && !cur.empty()) {
+                std::vector<Cand> par;
+                std::vector<std::pair<uint32_t, uint32_t>> tch;
+                std::vector<uint32_t> rid;
+                for (const Cand& c : cur) {
+                    if (!expands(c, min_gain)) {
+                        make_leaf(c);
+                        continue;
+                    }
+                    tch.push_back(apply_split(c));
+                    rid.push_back(n_pnodes_++);
+                    par.push_back(c);
+                }
+                next.clear();
+                if (!par.empty()) {
+                    const bool need_split = depth + 1 < cfg_.max_depth;
+                    expand(par, tch, rid, need_split, next);
+                }
+                cur.swap(next);
+                ++depth;
+            }
+            for (const Cand& c : cur) make_leaf(c);
+        } else {
+            // leaf-wise (expansion.rs:137-166): max-heap by (gain, node id)
+            std::vector<Cand> heap{root};
+            uint32_t n_leaves = 1;
+            auto pop = [&]() {
+                size_t bi = 0;
+                for (size_t i = 1; i < heap.size(); ++i) {
+                    const float a = heap[i].split.gain, b = heap[bi].split.gain;
+                    if (a > b || (a == b && heap[i].node > heap[bi].node)) bi = i;
+                }
+                Cand c = heap[bi];
+                heap.erase(heap.begin() + bi);
+                return c;
+            };
+            while (n_leaves < cfg_.max_leaves && !heap.empty()) {
+                Cand c = pop();
+                n_leaves += 1;
+                if (!expands(c, min_gain)) {
+                    make_leaf(c);
+                    continue;
+                }
+                std::vector<Cand> par{c}, kids;
+                std::vector<std::pair<uint32_t, uint32_t>> tch{apply_split(c)};
+                std::vector<uint32_t> rid{n_pnodes_++};
+                expand(par, tch, rid, n_leaves < cfg_.max_leaves, kids);
+                for (auto& k : kids) heap.push_back(k);
+            }
+            while (!heap.empty()) make_leaf(pop());
+        }
+        freeze_categories();
+
+        // prediction update from the partition (grower.rs:208-219)
+        std::vector<LeafSeg> segs;
+        for (uint32_t pnode = 0; pnode < n_pnodes_; ++pnode) {
+            if (pn_[pnode].count == 0) continue;
+            segs.push_back(LeafSeg{pn_[pnode].begin, pn_[pnode].count, leaf_value_[pnode], leaf_tree_node_[pnode]});
+        }
+        std::sort(segs.begin(), segs.end(), [](const LeafSeg& a, const LeafSeg& b) { return a.begin < b.begin; });
+        stage_.reset();
+        LeafSeg* hl = stage_.take<LeafSeg>(std::max<size_t>(1, segs.size()));
+        std::copy(segs.begin(), segs.end(), hl);
+        upload(hl, segs.size(), d_leaves_);
+        timer_.begin(PH_LEAF);
+        launch_leaf_update(d_leaves_.p, (uint32_t)segs.size(), ridx_.p, n_, pred_.p + (size_t)o * n_,
+                           cfg_.record_leaves ? row_leaf_.p : nullptr, st_);
+        timer_.end();
+        m_.counters.launches += 1;
+        if (cfg_.record_leaves) {
+            tree_.row_leaf.resize(n_);
+            BST_CK(cudaMemcpyAsync(tree_.row_leaf.data(), row_leaf_.p, sizeof(uint32_t) * n_, cudaMemcpyDeviceToHost, st_));
+        }
+        BST_CK(cudaStreamSynchronize(st_));
+        BST_CK(cudaGetLastError());
+        timer_.collect();
+        return std::move(tree_);
+    }
+};
+
+// Objective::compute_base_score (objectives/mod.rs:278-298).
+void base_scores(const HostDataset& ds, const bst_config& cfg, uint32_t G, std::vector<float>& out) {
+    const uint64_t n = ds.n;
+    const float* y = ds.y.data();
+    out.assign(G, 0.0f);
+    if (n == 0) return;
+    auto wv = [&](uint64_t i) { return ds.has_w ? (double)ds.w[i] : 1.0; };
+    if (cfg.objective == BST_OBJ_SQUARED) {  // regression.rs:45-69
+        double sw = 0, swy = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            sw = sw + wv(i);
+            swy = swy + wv(i) * (double)y[i];
+        }
+        out[0] = sw > 0.0 ? to_f32(swy / sw) : 0.0f;
+    } else if (cfg.objective == BST_OBJ_LOGISTIC) {  // classification.rs:54-76
+        double pos = 0, tot = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            pos = pos + wv(i) * (double)y[i];
+            tot = tot + wv(i);
+        }
+        double p = pos / tot;
+        p = p < 1e-7 ? 1e-7 : (p > 1.0 - 1e-7 ? 1.0 - 1e-7 : p);
+        out[0] = to_f32(std::log(p / (1.0 - p)));
+    } else {  // classification.rs:189-222
+        std::vector<double> cw(G, 0.0);
+        double tot = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const float yi = y[i];
+            const uint64_t label = (yi > 0.0f) ? (uint64_t)yi : 0;
+            if (label < G) cw[label] += wv(i);
+            tot += wv(i);
+        }
+        for (uint32_t g = 0; g < G; ++g) {
+            double p = cw[g] / tot;
+            p = p < 1e-7 ? 1e-7 : (p > 1.0 - 1e-7 ? 1.0 - 1e-7 : p);
+            out[g] = to_f32(std::log(p));
+        }
+    }
+}
+
+struct StreamGuard {
+    cudaStream_t s = nullptr;
+    StreamGuard() { BST_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+    ~StreamGuard() {
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+}  // namespace
+
+int transform_of(int objective) {
+    return objective == BST_OBJ_LOGISTIC ? 1 : (objective == BST_OBJ_SOFTMAX ? 2 : 0);
+}
+
+uint32_t HostTree::alloc() {
+    split_index.push_back(0);
+    threshold.push_back(0.0f);
+    left.push_back(0);
+    right.push_back(0);
+    default_left.push_back(0);
+    is_leaf.push_back(0);
+    leaf.push_back(0.0f);
+    split_type.push_back(0);
+    gain.push_back(0.0f);
+    cover.push_back(0.0f);
+    split_bin.push_back(0xFFFFFFFFu);
+    grad_sum.push_back(0.0);
+    hess_sum.push_back(0.0);
+    return (uint32_t)split_index.size() - 1;
+}
+
+void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, DeviceBinned& out) {
+    std::string err;
+    const auto t0 = std::chrono::steady_clock::now();
+    bst_status rc = plan_binning(ds.x.data(), ds.F, ds.n, ds.user_cat, cfg, out.plan, err);
+    if (rc != BST_OK) throw Error{rc, err};
+    const BinPlan& p = out.plan;
+    const uint32_t nc = p.n_cols();
+    const uint64_t n = p.n;
+    if (nc == 0) {
+        out.binning_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return;
+    }
+    if (bin_assign_rows(p.s8, p.s16) == 0) throw Error{BST_ERR_UNSUPPORTED, "too many features for one row tile"};
+    std::vector<BinColumn> cols(nc);
+    std::vector<float> thr;
+    std::vector<int32_t> cats;
+    for (uint32_t c = 0; c < nc; ++c) {
+        const Mapper& m = p.mappers[p.col_feature[c]];
+        BinColumn bc;
+        bc.matrix = p.col_matrix[c];
+        bc.pos = p.col_pos[c];
+        bc.is_cat = m.categorical;
+        bc.nan_bin = m.missing == MISSING_NAN ? m.n_bins - 1 : m.default_bin;
+        bc.zero_bin = m.missing == MISSING_ZERO ? m.default_bin : 0xFFFFFFFFu;
+        if (m.categorical) {
+            bc.off = (uint32_t)cats.size();
+            bc.n_cats = (uint32_t)m.cats.size();
+            bc.n_search = 0;
+            cats.insert(cats.end(), m.cats.begin(), m.cats.end());
+        } else {
+            bc.off = (uint32_t)thr.size();
+            bc.n_cats = 0;
+            bc.n_search = m.n_search();
+            for (uint32_t j = 0; j < bc.n_search; ++j) thr.push_back(f32_round_down(m.bounds[j]));
+        }
+        cols[c] = bc;
+    }
+    DevArray<float> x, d_thr;
+    DevArray<int32_t> d_cats;
+    DevArray<BinColumn> d_cols;
+    x.alloc((size_t)nc * n);
+    for (uint32_t c = 0; c < nc; ++c)
+        BST_CK(cudaMemcpyAsync(x.p + (size_t)c * n, ds.x.data() + (size_t)p.col_feature[c] * n, sizeof(float) * n,
+                               cudaMemcpyHostToDevice, st));
+    d_cols.alloc(nc);
+    BST_CK(cudaMemcpyAsync(d_cols.p, cols.data(), sizeof(BinColumn) * nc, cudaMemcpyHostToDevice, st));
+    d_thr.alloc(std::max<size_t>(1, thr.size()));
+    if (!thr.empty()) BST_CK(cudaMemcpyAsync(d_thr.p, thr.data(), sizeof(float) * thr.size(), cudaMemcpyHostToDevice, st));
+    d_cats.alloc(std::max<size_t>(1, cats.size()));
+    if (!cats.empty())
+        BST_CK(cudaMemcpyAsync(d_cats.p, cats.data(), sizeof(int32_t) * cats.size(), cudaMemcpyHostToDevice, st));
+    if (p.s8) out.bins8.alloc((size_t)n * p.s8);
+    if (p.s16) out.bins16.alloc((size_t)n * p.s16);
+    launch_bin_assign(x.p, n, d_cols.p, nc, d_thr.p, d_cats.p, out.bins8.p, p.s8, out.bins16.p, p.s16, st);
+    BST_CK(cudaGetLastError());
+    BST_CK(cudaStreamSynchronize(st));
+    out.binning_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+std::unique_ptr<Model> grow_one_tree(const HostDataset& ds, const float* g, const float* h, const bst_config& cfg,
+                                     uint32_t n_threads) {
+    BST_CK(cudaSetDevice(cfg.device));
+    StreamGuard sg;
+    auto model = std::make_unique<Model>();
+    model->device = cfg.device;
+    model->objective = BST_OBJ_SQUARED;
+    model->n_groups = 1;
+    model->n_features = (uint32_t)ds.F;
+    model->base = {0.0f};
+    DeviceBinned binned;
+    make_binned(ds, cfg, sg.s, binned);
+    Trainer tr(ds, binned, cfg, n_threads, sg.s, *model);
+    HostTree t = tr.run_external(g, h);
+    model->trees.push_back(std::move(t));
+    return model;
+}
+
+std::unique_ptr<Model> train_model(const HostDataset& ds, const bst_config& cfg, uint32_t n_threads) {
+    BST_CK(cudaSetDevice(cfg.device));
+    StreamGuard sg;
+    auto model = std::make_unique<Model>();
+    model->device = cfg.device;
+    model->objective = cfg.objective;
+    model->n_groups = cfg.objective == BST_OBJ_SOFTMAX ? cfg.n_classes : 1;
+    model->n_features = (uint32_t)ds.F;
+    DeviceBinned binned;
+    make_binned(ds, cfg, sg.s, binned);
+    model->timings[PH_BIN] = binned.binning_ms;
+    base_scores(ds, cfg, model->n_groups, model->base);
+    const auto t0 = std::chrono::steady_clock::now();
+    Trainer tr(ds, binned, cfg, n_threads, sg.s, *model);
+    tr.run();
+    model->timings[7] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return model;
+}
+
+struct Booster::Impl {
+    StreamGuard sg;
+    DeviceBinned binned;
+    std::unique_ptr<Model> model;
+    std::unique_ptr<Trainer> tr;
+    bst_config cfg;
+    uint32_t done = 0;
+};
+
+Booster::Booster(const HostDataset& ds, const bst_config& cfg, uint32_t n_threads) {
+    BST_CK(cudaSetDevice(cfg.device));
+    impl_ = std::make_unique<Impl>();
+    Impl& b = *impl_;
+    b.cfg = cfg;
+    b.model = std::make_unique<Model>();
+    Model& m = *b.model;
+    m.device = cfg.device;
+    m.objective = cfg.objective;
+    m.n_groups = cfg.objective == BST_OBJ_SOFTMAX ? cfg.n_classes : 1;
+    m.n_features = (uint32_t)ds.F;
+    make_binned(ds, cfg, b.sg.s, b.binned);
+    m.timings[PH_BIN] = b.binned.binning_ms;
+    base_scores(ds, cfg, m.n_groups, m.base);
+    b.tr = std::make_unique<Trainer>(ds, b.binned, b.cfg, n_threads, b.sg.s, m);
+    b.tr->start();
+}
+
+Booster::~Booster() = default;
+
+void Booster::update(uint32_t rounds) {
+    BST_CK(cudaSetDevice(impl_->cfg.device));
+    const auto t0 = std::chrono::steady_clock::now();
+    impl_->tr->rounds(rounds);
+    impl_->done += rounds;
+    impl_->model->timings[7] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+uint32_t Booster::rounds_done() const { return impl_->done; }
+const Model& Booster::model() const { return *impl_->model; }
+
+std::unique_ptr<Model> Booster::snapshot() const {
+    BST_CK(cudaSetDevice(impl_->cfg.device));
+    impl_->tr->finish();
+    const Model& s = *impl_->model;
+    auto m = std::make_unique<Model>();
+    m->n_groups = s.n_groups;
+    m->n_features = s.n_features;
+    m->objective = s.objective;
+    m->base = s.base;
+    m->trees = s.trees;
+    m->train_pred = s.train_pred;
+    for (int i = 0; i < 8; ++i) m->timings[i] = s.timings[i];
+    m->counters = s.counters;
+    m->device = s.device;
+    return m;
+}
+
+const DeviceForest& Model::device_forest() const {
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev) return *dev;
+    BST_CK(cudaSetDevice(device));
+    auto f = std::make_unique<DeviceForest>();
+    std::vector<ForestNode> nodes;
+    std::vector<uint32_t> roots, cat_seg, cat_words, gt, goff(n_groups + 1, 0);
+    for (const HostTree& t : trees) {
+        const uint32_t base_idx = (uint32_t)nodes.size();
+        const uint32_t wbase = (uint32_t)cat_words.size();
+        roots.push_back(base_idx);
+        for (size_t i = 0; i < t.split_index.size(); ++i) {
+            ForestNode fn;
+            fn.word = (t.split_index[i] & 0x1FFFFFFFu) | ((uint32_t)t.is_leaf[i] << 31) |
+                      ((uint32_t)t.default_left[i] << 30) | ((uint32_t)(t.split_type[i] == 1) << 29);
+            fn.value = t.is_leaf[i] ? t.leaf[i] : t.threshold[i];
+            fn.left = base_idx + t.left[i];
+            fn.right = base_idx + t.right[i];
+            nodes.push_back(fn);
+            const uint32_t ss = t.seg_size.empty() ? 0 : t.seg_size[i];
+            cat_seg.push_back(ss ? wbase + t.seg_start[i] : 0);
+            cat_seg.push_back(ss);
+        }
+        cat_words.insert(cat_words.end(), t.cat_words.begin(), t.cat_words.end());
+    }
+    for (uint32_t g = 0; g < n_groups; ++g) {
+        goff[g] = (uint32_t)gt.size();
+        for (uint32_t t = 0; t < trees.size(); ++t)
+            if (trees[t].group == g) gt.push_back(t);
+    }
+    goff[n_groups] = (uint32_t)gt.size();
+    auto up = [](auto& dst, const auto& src) {
+        dst.alloc(std::max<size_t>(1, src.size()));
+        if (!src.empty())
+            BST_CK(cudaMemcpy(dst.p, src.data(), sizeof(src[0]) * src.size(), cudaMemcpyHostToDevice));
+    };
+    up(f->nodes, nodes);
+    up(f->roots, roots);
+    up(f->group_trees, gt);
+    up(f->group_off, goff);
+    up(f->cat_seg, cat_seg);
+    up(f->cat_words, cat_words);
+    up(f->base, base);
+    f->view.nodes = f->nodes.p;
+    f->view.roots = f->roots.p;
+    f->view.group_trees = f->group_trees.p;
+    f->view.group_off = f->group_off.p;
+    f->view.cat_seg = f->cat_seg.p;
+    f->view.cat_words = f->cat_words.p;
+    f->view.base = f->base.p;
+    f->view.n_trees = (uint32_t)trees.size();
+    f->view.n_groups = n_groups;
+    dev = std::move(f);
+    return *dev;
+}
+
+void predict_device(const Model& m, const float* x, uint64_t n, uint64_t F, bool raw, float* out, cudaStream_t st) {
+    const DeviceForest& f = m.device_forest();
+    launch_predict(f.view, x, n, (uint32_t)F, 0, out, st);
+    if (!raw) launch_transform(transform_of(m.objective), out, m.n_groups, n, st);
+    BST_CK(cudaGetLastError());
+}
+
+void predict_host(const Model& m, const HostDataset& ds, bool raw, float* out) {
+    BST_CK(cudaSetDevice(m.device));
+    const DeviceForest& f = m.device_forest();
+    StreamGuard sg;
+    const uint64_t n = ds.n;
+    if (n == 0) return;
+    DevArray<float> x, o;
+    x.alloc((size_t)n * ds.F);
+    o.alloc((size_t)n * m.n_groups);
+    BST_CK(cudaMemcpyAsync(x.p, ds.x.data(), sizeof(float) * n * ds.F, cudaMemcpyHostToDevice, sg.s));
+    launch_predict(f.view, x.p, n, (uint32_t)ds.F, 1, o.p, sg.s);
+    if (!raw) launch_transform(transform_of(m.objective), o.p, m.n_groups, n, sg.s);
+    BST_CK(cudaGetLastError());
+    BST_CK(cudaMemcpyAsync(out, o.p, sizeof(float) * n * m.n_groups, cudaMemcpyDeviceToHost, sg.s));
+    BST_CK(cudaStreamSynchronize(sg.s));
+}
+
+}  // namespace bst

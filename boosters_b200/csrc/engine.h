@@ -1,0 +1,140 @@
+// engine.h — training and prediction orchestration of the B200 GBDT engine.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/boosters_c.h"
+#include "binning.h"
+#include "kernels.h"
+
+namespace bst {
+
+struct Error {
+    bst_status code;
+    std::string msg;
+};
+
+void cuda_check(cudaError_t e, const char* what);
+#define BST_CK(x) ::bst::cuda_check((x), #x)
+
+template <class T>
+struct DevArray {
+    T* p = nullptr;
+    size_t n = 0;
+    DevArray() = default;
+    DevArray(const DevArray&) = delete;
+    DevArray& operator=(const DevArray&) = delete;
+    ~DevArray() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t k) {
+        if (k <= n && p) return;
+        release();
+        if (k == 0) return;
+        cudaError_t e = cudaMalloc(&p, k * sizeof(T));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            throw Error{e == cudaErrorMemoryAllocation ? BST_ERR_OUT_OF_MEMORY : BST_ERR_CUDA,
+                        std::string("cudaMalloc of ") + std::to_string(k * sizeof(T)) +
+                            " bytes failed: " + cudaGetErrorString(e)};
+        }
+        n = k;
+    }
+};
+
+// Host copy of a feature-major dataset (data/raw/dataset.rs:139).
+struct HostDataset {
+    uint64_t n = 0, F = 0;
+    std::vector<float> x;  // [F][n]
+    std::vector<float> y;  // [n_outputs][n]
+    uint32_t n_outputs = 0;
+    std::vector<float> w;
+    bool has_w = false;
+    std::vector<uint8_t> user_cat;  // per feature
+};
+
+// Binned dataset resident on the GPU.
+struct DeviceBinned {
+    BinPlan plan;
+    DevArray<uint8_t> bins8;
+    DevArray<uint16_t> bins16;
+    double binning_ms = 0.0;
+};
+
+// Host tree (repr/gbdt/tree.rs:32-47) plus training detail.
+struct HostTree {
+    std::vector<uint32_t> split_index, left, right, seg_start, seg_size, cat_words, split_bin;
+    std::vector<float> threshold, leaf, gain, cover;
+    std::vector<uint8_t> default_left, is_leaf, split_type;
+    std::vector<double> grad_sum, hess_sum;
+    std::vector<uint32_t> row_leaf;
+    uint32_t group = 0;
+    uint32_t alloc();
+};
+
+struct DeviceForest {
+    DevArray<ForestNode> nodes;
+    DevArray<uint32_t> roots, group_trees, group_off, cat_seg, cat_words;
+    DevArray<float> base;
+    ForestDev view{};
+};
+
+struct Counters {
+    uint64_t launches = 0;
+    uint64_t hist_launches = 0, hist_rows = 0, hist_bytes = 0;
+    uint64_t scan_launches = 0, partition_rows = 0;
+    double hist_ms = 0;
+};
+
+struct Model {
+    uint32_t n_groups = 1, n_features = 0;
+    int objective = 0;
+    std::vector<float> base;
+    std::vector<HostTree> trees;
+    std::vector<float> train_pred;
+    double timings[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    Counters counters;
+    int device = 0;
+    mutable std::mutex mu;
+    mutable std::unique_ptr<DeviceForest> dev;
+    const DeviceForest& device_forest() const;
+};
+
+// Incremental training on a GPU-resident binned dataset: the boosting loop of
+// GBDTTrainer::train (training/gbdt/trainer.rs:242-401), a batch of rounds
+// per update().
+class Booster {
+  public:
+    Booster(const HostDataset& ds, const bst_config& cfg, uint32_t n_threads);
+    ~Booster();
+    void update(uint32_t rounds);
+    uint32_t rounds_done() const;
+    const Model& model() const;
+    std::unique_ptr<Model> snapshot() const;
+
+  private:
+    struct Impl;
+    std::unique_ptr<Impl> impl_;
+};
+
+void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, DeviceBinned& out);
+std::unique_ptr<Model> train_model(const HostDataset& ds, const bst_config& cfg, uint32_t n_threads);
+std::unique_ptr<Model> grow_one_tree(const HostDataset& ds, const float* grad, const float* hess,
+                                     const bst_config& cfg, uint32_t n_threads);
+void predict_host(const Model& m, const HostDataset& ds, bool raw, float* out);
+void predict_device(const Model& m, const float* x_dev_sm, uint64_t n, uint64_t F, bool raw,
+                    float* out_dev, cudaStream_t st);
+int transform_of(int objective);
+void build_hist_tiles(const BinPlan& p, std::vector<HistTile>& tiles, uint32_t& max_smem);
+
+}  // namespace bst

@@ -1,0 +1,941 @@
+// kernels.cu — sm_100a kernels of the B200 GBDT engine.
+//
+// Every kernel here is HBM- or latency-bound integer/byte work with a little
+// f32/f64 arithmetic; none is a dense contraction, so none uses tensor cores.
+// Floating-point expressions are written in the reference's evaluation order
+// and the file is compiled with -fmad=false so that no a*b+c is fused: f32
+// and f64 results round exactly as the Rust CPU path does.
+#include <math.h>
+
+#include "kernels.h"
+
+namespace bst {
+
+namespace {
+
+constexpr unsigned FULL = 0xFFFFFFFFu;
+
+__device__ __forceinline__ int32_t sat_i32(double v) {
+    if (v != v) return 0;
+    if (v >= 2147483647.0) return 2147483647;
+    if (v <= -2147483648.0) return (int32_t)(-2147483647 - 1);
+    return (int32_t)v;
+}
+
+__device__ __forceinline__ uint32_t sat_u32(float v) {
+    if (!(v > 0.0f)) return 0u;
+    if (v >= 4294967295.0f) return 0xFFFFFFFFu;
+    return (uint32_t)v;
+}
+
+// f32 exp of an f32 argument. Computed in f64 and rounded once, so the result
+// is the correctly rounded expf in all but a vanishing fraction of inputs
+// (the CPU reference calls the platform libm expf).
+__device__ __forceinline__ float exp_f32(float x) { return (float)exp((double)x); }
+
+__device__ __forceinline__ long long quantize(float v, double scale) {
+    return __double2ll_rn((double)v * scale);
+}
+
+__device__ __forceinline__ long long shfl_up_ll(long long v, int d) {
+    return __shfl_up_sync(FULL, v, d);
+}
+
+}  // namespace
+
+// ============================================================================
+// K1: bin assignment (BinMapper::value_to_bin, data/binned/bin_mapper.rs:210)
+// Reads the feature-major f32 matrix coalesced, writes row-major bins.
+// ============================================================================
+
+__global__ void __launch_bounds__(128)
+k_bin_assign(const float* __restrict__ x, uint64_t n, const BinColumn* __restrict__ cols,
+             uint32_t n_cols, const float* __restrict__ thr, const int32_t* __restrict__ cats,
+             uint8_t* __restrict__ bins8, uint32_t s8, uint16_t* __restrict__ bins16,
+             uint32_t s16) {
+    // one thread per row of a tile of blockDim.x rows
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t rows = blockDim.x;
+    uint8_t* t8 = smem;
+    uint16_t* t16 = reinterpret_cast<uint16_t*>(smem + (size_t)rows * s8);
+    const uint64_t r0 = (uint64_t)blockIdx.x * rows;
+    const uint64_t rem = n - r0;
+    const uint32_t valid = rem < (uint64_t)rows ? (uint32_t)rem : rows;
+    const uint32_t tile_bytes = rows * s8 + rows * s16 * 2u;
+    for (uint32_t i = threadIdx.x * 16u; i < tile_bytes; i += rows * 16u)
+        *reinterpret_cast<uint4*>(smem + i) = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    const uint32_t t = threadIdx.x;
+    if (t < valid) {
+        const uint64_t row = r0 + t;
+        for (uint32_t c = 0; c < n_cols; ++c) {
+            const BinColumn col = cols[c];
+            const float v = x[(uint64_t)c * n + row];
+            uint32_t bin;
+            if (v != v) {
+                bin = col.nan_bin;
+            } else if (v == 0.0f && col.zero_bin != 0xFFFFFFFFu) {
+                bin = col.zero_bin;
+            } else if (col.is_cat) {
+                const int32_t key = sat_i32((double)v);
+                const int32_t* cs = cats + col.off;
+                uint32_t lo = 0, hi = col.n_cats;
+                while (lo < hi) {
+                    uint32_t mid = (lo + hi) >> 1;
+                    if (cs[mid] < key)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                bin = (lo < col.n_cats && cs[lo] == key) ? lo : 0u;
+            } else {
+                const float* th = thr + col.off;
+                uint32_t lo = 0, hi = col.n_search;
+                while (lo < hi) {
+                    uint32_t mid = lo + ((hi - lo) >> 1);
+                    if (v <= th[mid])
+                        hi = mid;
+                    else
+                        lo = mid + 1;
+                }
+                bin = lo;
+            }
+            if (col.matrix == 0)
+                t8[t * s8 + col.pos] = (uint8_t)bin;
+            else
+                t16[t * s16 + col.pos] = (uint16_t)bin;
+        }
+    }
+    __syncthreads();
+    if (s8) {
+        const uint32_t nvec = valid * s8 / 16u;
+        uint4* dst = reinterpret_cast<uint4*>(bins8 + r0 * s8);
+        const uint4* src = reinterpret_cast<const uint4*>(t8);
+        for (uint32_t i = threadIdx.x; i < nvec; i += rows) dst[i] = src[i];
+    }
+    if (s16) {
+        const uint32_t nvec = valid * s16 * 2u / 16u;
+        uint4* dst = reinterpret_cast<uint4*>(bins16 + r0 * s16);
+        const uint4* src = reinterpret_cast<const uint4*>(t16);
+        for (uint32_t i = threadIdx.x; i < nvec; i += rows) dst[i] = src[i];
+    }
+}
+
+int bin_assign_rows(uint32_t s8, uint32_t s16) {
+    const size_t per_row = (size_t)s8 + (size_t)s16 * 2;
+    for (int rows = 128; rows >= 32; rows -= 32)
+        if ((size_t)rows * per_row <= 160 * 1024) return rows;
+    return 0;
+}
+
+void launch_bin_assign(const float* x_fm, uint64_t n, const BinColumn* cols, uint32_t n_cols,
+                       const float* thr, const int32_t* cats, uint8_t* bins8, uint32_t s8,
+                       uint16_t* bins16, uint32_t s16, cudaStream_t st) {
+    if (n == 0 || n_cols == 0) return;
+    const int rows = bin_assign_rows(s8, s16);
+    if (rows == 0) return;
+    const uint64_t blocks = (n + rows - 1) / rows;
+    const size_t smem = (size_t)rows * s8 + (size_t)rows * s16 * 2;
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_bin_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    k_bin_assign<<<(unsigned)blocks, rows, smem, st>>>(x_fm, n, cols, n_cols, thr, cats, bins8, s8,
+                                                     bins16, s16);
+}
+
+// ============================================================================
+// K3: gradients (training/objectives/regression.rs:20, classification.rs:24,141)
+// ============================================================================
+
+__device__ __forceinline__ void warp_max_atomic(unsigned* dst, float v) {
+    unsigned b = __float_as_uint(fabsf(v));
+    if (!(fabsf(v) <= 3.4e38f)) b = 0;  // ignore NaN / inf for the scale
+    for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(FULL, b, o));
+    if ((threadIdx.x & 31) == 0 && b) atomicMax(dst, b);
+}
+
+__global__ void k_gradients(int objective, uint32_t G, const float* __restrict__ pred,
+                            const float* __restrict__ y, const float* __restrict__ w, uint64_t n,
+                            float2* __restrict__ gh, unsigned* __restrict__ maxabs) {
+    const float HESS_MIN = 1e-6f;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    // loop trip count is warp-uniform so that the shuffles below are safe
+    const uint64_t n_round = (n + 31) & ~uint64_t(31);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += stride) {
+        const bool ok = i < n;
+        const float wi = (ok && w) ? w[i] : 1.0f;
+        const float yi = ok ? y[i] : 0.0f;
+        if (objective == 0) {  // squared
+            const float p = ok ? pred[i] : 0.0f;
+            const float g = wi * (p - yi);
+            if (ok) gh[i] = make_float2(g, wi);
+            warp_max_atomic(&maxabs[0], ok ? g : 0.0f);
+            warp_max_atomic(&maxabs[1], ok ? wi : 0.0f);
+        } else if (objective == 1) {  // logistic
+            const float x = ok ? pred[i] : 0.0f;
+            const float p = 1.0f / (1.0f + exp_f32(-x));
+            const float g = wi * (p - yi);
+            const float h = fmaxf(wi * p * (1.0f - p), HESS_MIN);
+            if (ok) gh[i] = make_float2(g, h);
+            warp_max_atomic(&maxabs[0], ok ? g : 0.0f);
+            warp_max_atomic(&maxabs[1], ok ? h : 0.0f);
+        } else {  // softmax
+            uint64_t label = 0;
+            if (ok && yi > 0.0f) label = (uint64_t)yi;  // `f32 as usize`
+            float mx = -INFINITY;
+            for (uint32_t c = 0; c < G; ++c) mx = fmaxf(mx, ok ? pred[(uint64_t)c * n + i] : 0.0f);
+            float sum = -0.0f;
+            for (uint32_t c = 0; c < G; ++c) sum = sum + exp_f32((ok ? pred[(uint64_t)c * n + i] : 0.0f) - mx);
+            for (uint32_t c = 0; c < G; ++c) {
+                const float pc = ok ? pred[(uint64_t)c * n + i] : 0.0f;
+                const float p = exp_f32(pc - mx) / sum;
+                const float ind = (c == label) ? 1.0f : 0.0f;
+                const float g = wi * (p - ind);
+                const float h = fmaxf(wi * p * (1.0f - p), HESS_MIN);
+                if (ok) gh[(uint64_t)c * n + i] = make_float2(g, h);
+                warp_max_atomic(&maxabs[2 * c], ok ? g : 0.0f);
+                warp_max_atomic(&maxabs[2 * c + 1], ok ? h : 0.0f);
+            }
+        }
+    }
+}
+
+void launch_gradients(int objective, uint32_t G, const float* pred, const float* y,
+                      const float* w, uint64_t n, float2* gh, unsigned* maxabs,
+                      cudaStream_t st) {
+    if (n == 0) return;
+    uint64_t blocks = (n + 255) / 256;
+    if (blocks > 148ull * 16) blocks = 148ull * 16;
+    k_gradients<<<(unsigned)blocks, 256, 0, st>>>(objective, G, pred, y, w, n, gh, maxabs);
+}
+
+__global__ void k_fixed_scales(const unsigned* __restrict__ maxabs, uint32_t G, uint64_t n,
+                               double* __restrict__ scales) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 2 * G) return;
+    const float m = __uint_as_float(maxabs[i]);
+    int k = 0;
+    if (m > 0.0f) {
+        int e;
+        frexp((double)n * (double)m, &e);  // n*m < 2^e
+        k = 62 - e;
+        if (k > 1000) k = 1000;
+        if (k < -1000) k = -1000;
+    }
+    const uint32_t o = i >> 1, which = i & 1;
+    scales[4 * o + which] = ldexp(1.0, k);
+    scales[4 * o + 2 + which] = ldexp(1.0, -k);
+}
+
+void launch_fixed_scales(const unsigned* maxabs, uint32_t G, uint64_t n, double* scales,
+                         cudaStream_t st) {
+    k_fixed_scales<<<(2 * G + 63) / 64, 64, 0, st>>>(maxabs, G, n, scales);
+}
+
+// ============================================================================
+// K4: histogram build (HistogramBuilder, training/gbdt/histograms/ops.rs:79-127)
+// Shared-memory privatised 64-bit fixed-point histograms over a tile of
+// columns; 128-bit row loads; one global atomic flush per non-empty bin.
+// ============================================================================
+
+constexpr int HIST_THREADS = 256;
+
+__global__ void __launch_bounds__(HIST_THREADS)
+k_hist_build(const HistChunk* __restrict__ chunks, const HistTile* __restrict__ tiles,
+             const uint32_t* __restrict__ ridx, const float2* __restrict__ gh,
+             const double* __restrict__ scale, const uint8_t* __restrict__ bins8, uint32_t s8,
+             const uint16_t* __restrict__ bins16, uint32_t s16, HBin* __restrict__ hist,
+             uint64_t slot_bins) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    HBin* sm = reinterpret_cast<HBin*>(smem_raw);
+    __shared__ HistTile tile;
+    const HistChunk chunk = chunks[blockIdx.y];
+    if (threadIdx.x == 0) tile = tiles[blockIdx.x];
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < tile.smem_bins; i += HIST_THREADS)
+        reinterpret_cast<uint4*>(sm)[i] = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+
+    const double sg = scale[0], sh = scale[1];
+    const uint32_t c0 = tile.c0, c1 = tile.c1;
+    uint32_t loff[16], lnb[16];
+#pragma unroll
+    for (int l = 0; l < 16; ++l) {
+        loff[l] = tile.lane_smem[l];
+        lnb[l] = tile.lane_nbins[l];
+    }
+    const bool ident = chunk.flags & 1u;
+    if (tile.matrix == 0) {
+        const uint8_t* base = bins8 + (size_t)tile.vec * 16u;
+        for (uint32_t i = threadIdx.x; i < chunk.count; i += HIST_THREADS) {
+            const uint32_t p = chunk.begin + i;
+            const uint32_t row = ident ? p : ridx[p];
+            const float2 v = gh[row];
+            const unsigned long long qg = (unsigned long long)quantize(v.x, sg);
+            const unsigned long long qh = (unsigned long long)quantize(v.y, sh);
+            const uint4 b = *reinterpret_cast<const uint4*>(base + (size_t)row * s8);
+            const uint32_t words[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int l = 0; l < 16; ++l) {
+                if (l >= (int)c0 && l < (int)c1) {
+                    const uint32_t bin = (words[l >> 2] >> ((l & 3) * 8)) & 0xFFu;
+                    if (bin < lnb[l]) {
+                        HBin* d = sm + loff[l] + bin;
+                        atomicAdd(reinterpret_cast<unsigned long long*>(&d->g), qg);
+                        atomicAdd(reinterpret_cast<unsigned long long*>(&d->h), qh);
+                    }
+                }
+            }
+        }
+    } else {
+        const uint16_t* base = bins16 + (size_t)tile.vec * 8u;
+        for (uint32_t i = threadIdx.x; i < chunk.count; i += HIST_THREADS) {
+            const uint32_t p = chunk.begin + i;
+            const uint32_t row = ident ? p : ridx[p];
+            const float2 v = gh[row];
+            const unsigned long long qg = (unsigned long long)quantize(v.x, sg);
+            const unsigned long long qh = (unsigned long long)quantize(v.y, sh);
+            const uint4 b = *reinterpret_cast<const uint4*>(base + (size_t)row * s16);
+            const uint32_t words[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int l = 0; l < 8; ++l) {
+                if (l >= (int)c0 && l < (int)c1) {
+                    const uint32_t bin = (words[l >> 1] >> ((l & 1) * 16)) & 0xFFFFu;
+                    if (bin < lnb[l]) {
+                        HBin* d = sm + loff[l] + bin;
+                        atomicAdd(reinterpret_cast<unsigned long long*>(&d->g), qg);
+                        atomicAdd(reinterpret_cast<unsigned long long*>(&d->h), qh);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    HBin* out = hist + (size_t)chunk.slot * slot_bins;
+    for (uint32_t l = c0; l < c1; ++l) {
+        const uint32_t so = tile.lane_smem[l], go = tile.lane_hist[l], nb = tile.lane_nbins[l];
+        for (uint32_t b = threadIdx.x; b < nb; b += HIST_THREADS) {
+            const HBin s = sm[so + b];
+            if (s.g | s.h) {
+                atomicAdd(reinterpret_cast<unsigned long long*>(&out[go + b].g), (unsigned long long)s.g);
+                atomicAdd(reinterpret_cast<unsigned long long*>(&out[go + b].h), (unsigned long long)s.h);
+            }
+        }
+    }
+}
+
+void launch_hist_build(const HistChunk* chunks, uint32_t n_chunks, const HistTile* tiles,
+                       uint32_t n_tiles, uint32_t max_smem_bins, const uint32_t* ridx,
+                       const float2* gh, const double* scale, const uint8_t* bins8, uint32_t s8,
+                       const uint16_t* bins16, uint32_t s16, HBin* hist, uint64_t slot_bins,
+                       cudaStream_t st) {
+    if (n_chunks == 0 || n_tiles == 0) return;
+    const size_t smem = (size_t)max_smem_bins * sizeof(HBin);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_hist_build, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr_set = true;
+    }
+    dim3 grid(n_tiles, n_chunks);
+    k_hist_build<<<grid, HIST_THREADS, smem, st>>>(chunks, tiles, ridx, gh, scale, bins8, s8,
+                                                   bins16, s16, hist, slot_bins);
+}
+
+__global__ void k_hist_finish(const FinishWork* __restrict__ works, HBin* __restrict__ hist,
+                              uint64_t slot_bins, uint32_t total_bins) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total_bins) return;
+    const FinishWork w = works[blockIdx.y];
+    HBin* L = hist + (size_t)w.left * slot_bins + i;
+    HBin* R = hist + (size_t)w.right * slot_bins + i;
+    const HBin p = *L, s = *R;
+    HBin d;
+    d.g = p.g - s.g;
+    d.h = p.h - s.h;
+    if (w.flags & 1u) {  // left child was built (smaller): parent - left -> right
+        *L = s;
+        *R = d;
+    } else {
+        *L = d;
+    }
+}
+
+void launch_hist_finish(const FinishWork* w, uint32_t n_work, HBin* hist, uint64_t slot_bins,
+                        uint32_t total_bins, cudaStream_t st) {
+    if (n_work == 0 || total_bins == 0) return;
+    dim3 grid((total_bins + 255) / 256, n_work);
+    k_hist_finish<<<grid, 256, 0, st>>>(w, hist, slot_bins, total_bins);
+}
+
+__global__ void k_node_sums(const HistChunk* __restrict__ chunks, const uint32_t* __restrict__ ridx,
+                            const float2* __restrict__ gh, const double* __restrict__ scale,
+                            long long* __restrict__ sums) {
+    const HistChunk c = chunks[blockIdx.x];
+    const double sg = scale[0], sh = scale[1];
+    long long ag = 0, ah = 0;
+    for (uint32_t i = threadIdx.x; i < c.count; i += blockDim.x) {
+        const uint32_t p = c.begin + i;
+        const uint32_t row = (c.flags & 1u) ? p : ridx[p];
+        const float2 v = gh[row];
+        ag += quantize(v.x, sg);
+        ah += quantize(v.y, sh);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        ag += __shfl_xor_sync(FULL, ag, o);
+        ah += __shfl_xor_sync(FULL, ah, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(&sums[2 * c.slot]), (unsigned long long)ag);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&sums[2 * c.slot + 1]), (unsigned long long)ah);
+    }
+}
+
+void launch_node_sums(const HistChunk* chunks, uint32_t n_chunks, const uint32_t* ridx,
+                      const float2* gh, const double* scale, long long* sums, cudaStream_t st) {
+    if (n_chunks == 0) return;
+    k_node_sums<<<n_chunks, 256, 0, st>>>(chunks, ridx, gh, scale, sums);
+}
+
+// ============================================================================
+// K6: split scan (GreedySplitter, training/gbdt/split/find.rs:113-644)
+// One warp per (node, column); exact int64 prefix sums, f64 gain cast to f32,
+// ties resolved by the reference's scan order.
+// ============================================================================
+
+namespace {
+
+struct Best {
+    float gain;
+    uint32_t order;
+    uint32_t bin;
+    uint32_t flags;
+};
+
+__device__ __forceinline__ bool better(float g, uint32_t o, float bg, uint32_t bo) {
+    // candidates: larger gain wins, equal gain -> earlier scan position wins
+    return g > bg || (g == bg && o < bo);
+}
+
+__device__ __forceinline__ Best warp_best(Best b) {
+    for (int off = 16; off > 0; off >>= 1) {
+        Best o;
+        o.gain = __shfl_xor_sync(FULL, b.gain, off);
+        o.order = __shfl_xor_sync(FULL, b.order, off);
+        o.bin = __shfl_xor_sync(FULL, b.bin, off);
+        o.flags = __shfl_xor_sync(FULL, b.flags, off);
+        if (better(o.gain, o.order, b.gain, b.order)) b = o;
+    }
+    return b;
+}
+
+__device__ __forceinline__ long long warp_incl_scan(long long v, int lane) {
+    for (int d = 1; d < 32; d <<= 1) {
+        long long t = shfl_up_ll(v, d);
+        if (lane >= d) v += t;
+    }
+    return v;
+}
+
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+struct GainCtx {
+    double lambda, offset, mcw;
+    uint32_t msl;
+    __device__ float gain(double gl, double hl, double gr, double hr) const {
+        const double sl = gl * gl / (hl + lambda);
+        const double sr = gr * gr / (hr + lambda);
+        return __double2float_rn(0.5 * (sl + sr) - offset);
+    }
+    __device__ bool valid(double hl, double hr, uint32_t cl, uint32_t cr) const {
+        return hl >= mcw && hr >= mcw && cl >= msl && cr >= msl;
+    }
+};
+
+__device__ __forceinline__ uint32_t sat_sub(uint32_t a, uint32_t b) { return a > b ? a - b : 0u; }
+
+constexpr int SCAN_WARPS = 8;
+constexpr int SORT_N = 256;  // categorical columns with <= 256 bins
+
+}  // namespace
+
+__global__ void __launch_bounds__(SCAN_WARPS * 32)
+k_split_scan(const ScanNode* __restrict__ nodes, const ScanColumn* __restrict__ cols,
+             uint32_t n_cols, const HBin* __restrict__ hist, uint64_t slot_bins,
+             const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
+             long long* __restrict__ node_tot) {
+    __shared__ double s_key[SCAN_WARPS][SORT_N];
+    __shared__ uint32_t s_cat[SCAN_WARPS][SORT_N];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t col = blockIdx.x * SCAN_WARPS + warp;
+    const uint32_t node = blockIdx.y;
+    if (col >= n_cols) return;
+    const ScanColumn cm = cols[col];
+    const ScanNode nd = nodes[node];
+    const HBin* h = hist + (size_t)nd.slot * slot_bins + cm.hist_off;
+    const double ig = scale[2], ih = scale[3];
+    const uint32_t nb = cm.n_bins;
+    const uint32_t pc = nd.count;
+
+    // node totals (every column's bins sum to the same exact total)
+    long long tg = 0, th = 0;
+    for (uint32_t b = lane; b < nb; b += 32) {
+        tg += h[b].g;
+        th += h[b].h;
+    }
+    tg = warp_sum_ll(tg);
+    th = warp_sum_ll(th);
+    if (nd.flags & 1u) {
+        tg = nd.pg;
+        th = nd.ph;
+    }
+    if (col == 0 && lane == 0) {
+        node_tot[2 * node] = tg;
+        node_tot[2 * node + 1] = th;
+    }
+    const double pg = (double)tg * ig, ph = (double)th * ih;
+    GainCtx ctx;
+    ctx.lambda = gp.lambda;
+    ctx.offset = 0.5 * (pg * pg / (ph + gp.lambda)) + gp.min_gain;
+    ctx.mcw = gp.min_child_weight;
+    ctx.msl = gp.min_samples_leaf;
+
+    Best best{-INFINITY, 0xFFFFFFFFu, 0u, 0u};
+    ColCand* out = cand + (size_t)node * n_cols + col;
+
+    if (!cm.is_cat) {
+        if (nb >= 2) {
+            // find.rs:286-407: forward scan (missing right), backward scan
+            // (missing left) when the column has a NaN bin (the last bin).
+            const bool hm = cm.has_missing != 0;
+            const long long pm_g = tg - h[nb - 1].g, pm_h = th - h[nb - 1].h;  // P[nb-2]
+            long long carry_g = 0, carry_h = 0;
+            for (uint32_t base = 0; base < nb; base += 32) {
+                const uint32_t b = base + lane;
+                long long vg = 0, vh = 0;
+                if (b < nb) {
+                    vg = h[b].g;
+                    vh = h[b].h;
+                }
+                const long long Pg = warp_incl_scan(vg, lane) + carry_g;
+                const long long Ph = warp_incl_scan(vh, lane) + carry_h;
+                carry_g = __shfl_sync(FULL, Pg, 31);
+                carry_h = __shfl_sync(FULL, Ph, 31);
+                if (b + 1 < nb) {  // forward candidate: bins <= b go left
+                    const double lg = (double)Pg * ig, lh = (double)Ph * ih;
+                    const double rg = (double)(tg - Pg) * ig, rh = (double)(th - Ph) * ih;
+                    const uint32_t lc = b + 1, rc = sat_sub(pc, lc);
+                    if (ctx.valid(lh, rh, lc, rc)) {
+                        const float g = ctx.gain(lg, lh, rg, rh);
+                        if (better(g, b, best.gain, best.order)) best = Best{g, b, b, 0u};
+                    }
+                }
+                if (hm && b + 2 < nb) {  // backward candidate: bins b+1..nb-2 go right
+                    const long long Rg = pm_g - Pg, Rh = pm_h - Ph;
+                    const double rg = (double)Rg * ig, rh = (double)Rh * ih;
+                    const double lg = (double)(tg - Rg) * ig, lh = (double)(th - Rh) * ih;
+                    const uint32_t rc = nb - 2 - b, lc = sat_sub(pc, rc);
+                    if (ctx.valid(lh, rh, lc, rc)) {
+                        const float g = ctx.gain(lg, lh, rg, rh);
+                        const uint32_t ord = 2 * nb - 3 - b;
+                        if (better(g, ord, best.gain, best.order)) best = Best{g, ord, b, 1u};
+                    }
+                }
+            }
+        }
+        best = warp_best(best);
+        if (lane == 0) {
+            out->gain = best.gain;
+            out->order = best.order;
+            out->bin = best.bin;
+            out->flags = best.flags;
+            out->cats[0] = out->cats[1] = out->cats[2] = out->cats[3] = 0ull;
+        }
+        return;
+    }
+
+    // categorical (find.rs:426-573)
+    unsigned long long cats[4] = {0ull, 0ull, 0ull, 0ull};
+    if (nb >= 2 && nb <= gp.max_onehot_cats) {
+        for (uint32_t c = lane; c < nb; c += 32) {  // one category left (find.rs:472)
+            const double lg = (double)h[c].g * ig, lh = (double)h[c].h * ih;
+            const double rg = (double)(tg - h[c].g) * ig, rh = (double)(th - h[c].h) * ih;
+            const uint32_t lc = 1, rc = sat_sub(pc, 1);
+            if (ctx.valid(lh, rh, lc, rc)) {
+                const float g = ctx.gain(lg, lh, rg, rh);
+                if (better(g, c, best.gain, best.order)) best = Best{g, c, c, 2u};
+            }
+        }
+        best = warp_best(best);
+        if (best.gain > -INFINITY && best.bin < 256) cats[best.bin >> 6] = 1ull << (best.bin & 63);
+    } else if (nb > gp.max_onehot_cats && nb <= SORT_N) {
+        // sorted partition (find.rs:511-573): categories with hess > 1e-10
+        // ordered by -g/(h+1e-6) ascending, ties by category (stable sort)
+        double* key = s_key[warp];
+        uint32_t* cat = s_cat[warp];
+        uint32_t m = 0;
+        for (uint32_t base = 0; base < nb; base += 32) {
+            const uint32_t c = base + lane;
+            bool ok = false;
+            double r = 0.0;
+            if (c < nb) {
+                const double gg = (double)h[c].g * ig, hh = (double)h[c].h * ih;
+                ok = hh > 1e-10;
+                r = -gg / (hh + 1e-6);
+            }
+            const unsigned bal = __ballot_sync(FULL, ok);
+            const uint32_t pos = m + __popc(bal & ((1u << lane) - 1u));
+            if (ok) {
+                key[pos] = r;
+                cat[pos] = c;
+            }
+            m += __popc(bal);
+        }
+        for (uint32_t i = m + lane; i < SORT_N; i += 32) {
+            key[i] = INFINITY;
+            cat[i] = 0xFFFFFFFFu;
+        }
+        __syncwarp();
+        if (m >= 2) {
+            // bitonic sort of (key, cat) over SORT_N entries
+            for (uint32_t k = 2; k <= SORT_N; k <<= 1) {
+                for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                    for (uint32_t i = lane; i < SORT_N; i += 32) {
+                        const uint32_t ixj = i ^ j;
+                        if (ixj > i) {
+                            const bool up = (i & k) == 0;
+                            const double a = key[i], b = key[ixj];
+                            const uint32_t ca = cat[i], cb = cat[ixj];
+                            const bool a_gt_b = a > b || (a == b && ca > cb);
+                            if (a_gt_b == up) {
+                                key[i] = b;
+                                key[ixj] = a;
+                                cat[i] = cb;
+                                cat[ixj] = ca;
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+            long long carry_g = 0, carry_h = 0;
+            for (uint32_t base = 0; base + 1 < m; base += 32) {
+                const uint32_t i = base + lane;
+                long long vg = 0, vh = 0;
+                if (i + 1 < m) {
+                    const uint32_t c = cat[i];
+                    vg = h[c].g;
+                    vh = h[c].h;
+                }
+                const long long Pg = warp_incl_scan(vg, lane) + carry_g;
+                const long long Ph = warp_incl_scan(vh, lane) + carry_h;
+                carry_g = __shfl_sync(FULL, Pg, 31);
+                carry_h = __shfl_sync(FULL, Ph, 31);
+                if (i + 1 < m) {
+                    const double lg = (double)Pg * ig, lh = (double)Ph * ih;
+                    const double rg = (double)(tg - Pg) * ig, rh = (double)(th - Ph) * ih;
+                    const uint32_t lc = i + 1, rc = sat_sub(pc, lc);
+                    if (ctx.valid(lh, rh, lc, rc)) {
+                        const float g = ctx.gain(lg, lh, rg, rh);
+                        if (better(g, i, best.gain, best.order)) best = Best{g, i, i, 2u};
+                    }
+                }
+            }
+            best = warp_best(best);
+            if (best.gain > -INFINITY) {
+                unsigned long long part[4] = {0ull, 0ull, 0ull, 0ull};
+                for (uint32_t i = lane; i <= best.order && i < m; i += 32) {
+                    const uint32_t c = cat[i];
+                    if (c < 256) part[c >> 6] |= 1ull << (c & 63);
+                }
+                for (int q = 0; q < 4; ++q) {
+                    unsigned long long v = part[q];
+                    for (int o = 16; o > 0; o >>= 1) v |= __shfl_xor_sync(FULL, v, o);
+                    cats[q] = v;
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        out->gain = best.gain;
+        out->order = best.order;
+        out->bin = best.bin;
+        out->flags = best.gain > -INFINITY ? best.flags : 0u;
+        for (int q = 0; q < 4; ++q) out->cats[q] = cats[q];
+    }
+}
+
+void launch_split_scan(const ScanNode* nodes, uint32_t n_nodes, const ScanColumn* cols,
+                       uint32_t n_cols, const HBin* hist, uint64_t slot_bins,
+                       const double* scale, GainParamsDev gp, ColCand* cand,
+                       long long* node_tot, cudaStream_t st) {
+    if (n_nodes == 0 || n_cols == 0) return;
+    dim3 grid((n_cols + SCAN_WARPS - 1) / SCAN_WARPS, n_nodes);
+    k_split_scan<<<grid, SCAN_WARPS * 32, 0, st>>>(nodes, cols, n_cols, hist, slot_bins, scale,
+                                                    gp, cand, node_tot);
+}
+
+// Across columns (find.rs:180-212 sequential; :219-270 rayon reduce).
+__global__ void k_split_reduce(const ColCand* __restrict__ cand, const long long* __restrict__ node_tot,
+                               uint32_t n_cols, int last_wins, NodeSplit* __restrict__ out) {
+    const uint32_t node = blockIdx.x;
+    const int lane = threadIdx.x;
+    float bg = -INFINITY;
+    uint32_t bc = 0xFFFFFFFFu;
+    const ColCand* c = cand + (size_t)node * n_cols;
+    for (uint32_t i = lane; i < n_cols; i += 32) {
+        const float g = c[i].gain;
+        if (!(g > -INFINITY)) continue;
+        if (bc == 0xFFFFFFFFu || g > bg || (last_wins && g == bg)) {
+            bg = g;
+            bc = i;
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        const float og = __shfl_xor_sync(FULL, bg, off);
+        const uint32_t oc = __shfl_xor_sync(FULL, bc, off);
+        bool take;
+        if (oc == 0xFFFFFFFFu)
+            take = false;
+        else if (bc == 0xFFFFFFFFu)
+            take = true;
+        else if (og != bg)
+            take = og > bg;
+        else
+            take = last_wins ? oc > bc : oc < bc;
+        if (take) {
+            bg = og;
+            bc = oc;
+        }
+    }
+    if (lane == 0) {
+        NodeSplit s;
+        s.tot_g = node_tot[2 * node];
+        s.tot_h = node_tot[2 * node + 1];
+        if (bc == 0xFFFFFFFFu) {
+            s.gain = -INFINITY;
+            s.col = 0;
+            s.bin = 0;
+            s.flags = 0;
+            s.cats[0] = s.cats[1] = s.cats[2] = s.cats[3] = 0ull;
+        } else {
+            const ColCand& w = c[bc];
+            s.gain = w.gain;
+            s.col = bc;
+            s.bin = w.bin;
+            s.flags = (w.flags & 3u) | 4u;
+            for (int q = 0; q < 4; ++q) s.cats[q] = w.cats[q];
+        }
+        out[node] = s;
+    }
+}
+
+void launch_split_reduce(const ColCand* cand, const long long* node_tot, uint32_t n_nodes,
+                         uint32_t n_cols, int last_wins, NodeSplit* out, cudaStream_t st) {
+    if (n_nodes == 0) return;
+    k_split_reduce<<<n_nodes, 32, 0, st>>>(cand, node_tot, n_cols, last_wins, out);
+}
+
+// ============================================================================
+// K7: row partition (RowPartitioner::split, training/gbdt/partition.rs:296-382)
+// Left rows fill the node's range from the front, right rows from the back.
+// ============================================================================
+
+__global__ void k_partition(const PartWork* __restrict__ works, const PartChunk* __restrict__ chunks,
+                            const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp,
+                            unsigned* __restrict__ cursors, const uint8_t* __restrict__ bins8,
+                            uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16) {
+    const PartChunk ch = chunks[blockIdx.x];
+    __shared__ PartWork w;
+    if (threadIdx.x == 0) w = works[ch.work];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    for (uint32_t base = 0; base < ch.len; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const bool ok = i < ch.len;
+        uint32_t row = 0;
+        bool left = false;
+        if (ok) {
+            row = ridx[ch.start + i];
+            const uint32_t bin = w.matrix == 0 ? (uint32_t)bins8[(size_t)row * s8 + w.pos]
+                                               : (uint32_t)bins16[(size_t)row * s16 + w.pos];
+            if ((w.flags & 2u) && bin == w.default_bin)
+                left = (w.flags & 1u) != 0;
+            else if (w.flags & 4u)
+                left = bin < 256 && ((w.cats[bin >> 6] >> (bin & 63)) & 1ull);
+            else
+                left = bin <= w.thr_bin;
+        }
+        const unsigned act = __ballot_sync(FULL, ok);
+        const unsigned lm = __ballot_sync(FULL, ok && left);
+        const unsigned rm = act & ~lm;
+        unsigned lbase = 0, rbase = 0;
+        if (lane == 0) {
+            if (lm) lbase = atomicAdd(&cursors[2 * ch.work], (unsigned)__popc(lm));
+            if (rm) rbase = atomicSub(&cursors[2 * ch.work + 1], (unsigned)__popc(rm)) - (unsigned)__popc(rm);
+        }
+        lbase = __shfl_sync(FULL, lbase, 0);
+        rbase = __shfl_sync(FULL, rbase, 0);
+        if (ok) {
+            if (left)
+                tmp[lbase + __popc(lm & lt)] = row;
+            else
+                tmp[rbase + __popc(rm & lt)] = row;
+        }
+    }
+}
+
+void launch_partition(const PartWork* works, const PartChunk* chunks, uint32_t n_chunks,
+                      const uint32_t* ridx, uint32_t* tmp, unsigned* cursors,
+                      const uint8_t* bins8, uint32_t s8, const uint16_t* bins16, uint32_t s16,
+                      cudaStream_t st) {
+    if (n_chunks == 0) return;
+    k_partition<<<n_chunks, 256, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16, s16);
+}
+
+__global__ void k_copy_chunks(const PartChunk* __restrict__ chunks, const uint32_t* __restrict__ src,
+                              uint32_t* __restrict__ dst) {
+    const PartChunk ch = chunks[blockIdx.x];
+    for (uint32_t i = threadIdx.x; i < ch.len; i += blockDim.x) dst[ch.start + i] = src[ch.start + i];
+}
+
+void launch_copy_chunks(const PartChunk* chunks, const PartWork* works, uint32_t n_chunks,
+                        const uint32_t* src, uint32_t* dst, cudaStream_t st) {
+    (void)works;
+    if (n_chunks == 0) return;
+    k_copy_chunks<<<n_chunks, 256, 0, st>>>(chunks, src, dst);
+}
+
+__global__ void k_iota(uint32_t* __restrict__ r, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        r[i] = (uint32_t)i;
+}
+
+void launch_iota(uint32_t* ridx, uint64_t n, cudaStream_t st) {
+    if (n == 0) return;
+    uint64_t blocks = (n + 255) / 256;
+    if (blocks > 148ull * 16) blocks = 148ull * 16;
+    k_iota<<<(unsigned)blocks, 256, 0, st>>>(ridx, n);
+}
+
+// ============================================================================
+// K8: leaf values -> predictions (grower.rs:208-219)
+// ============================================================================
+
+__global__ void k_leaf_update(const LeafSeg* __restrict__ leaves, uint32_t n_leaves,
+                              const uint32_t* __restrict__ ridx, uint64_t n, float* __restrict__ pred,
+                              uint32_t* __restrict__ row_leaf) {
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = n_leaves;  // last leaf with begin <= p
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (leaves[mid].begin <= p)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const LeafSeg L = leaves[lo];
+        if (p >= L.begin && p < (uint64_t)L.begin + L.count) {
+            const uint32_t row = ridx[p];
+            pred[row] = pred[row] + L.value;
+            if (row_leaf) row_leaf[row] = L.tree_node;
+        }
+    }
+}
+
+void launch_leaf_update(const LeafSeg* leaves, uint32_t n_leaves, const uint32_t* ridx,
+                        uint64_t n, float* pred, uint32_t* row_leaf, cudaStream_t st) {
+    if (n == 0 || n_leaves == 0) return;
+    uint64_t blocks = (n + 255) / 256;
+    if (blocks > 148ull * 16) blocks = 148ull * 16;
+    k_leaf_update<<<(unsigned)blocks, 256, 0, st>>>(leaves, n_leaves, ridx, n, pred, row_leaf);
+}
+
+// ============================================================================
+// K9: forest traversal (tree_view.rs:119-160, predictor.rs:271-302)
+// One thread per row; trees summed in forest order per group in f32.
+// ============================================================================
+
+__global__ void k_predict(ForestDev f, const float* __restrict__ x,
+                          uint64_t n, uint32_t n_features, int feature_major, float* __restrict__ out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t fstride = feature_major ? n : 1;
+    const float* xr = feature_major ? x + i : x + i * n_features;
+    for (uint32_t g = 0; g < f.n_groups; ++g) {
+        float acc = f.base[g];
+        for (uint32_t k = f.group_off[g]; k < f.group_off[g + 1]; ++k) {
+            uint32_t nd = f.roots[f.group_trees[k]];
+            for (int step = 0; step < 65536; ++step) {
+                const ForestNode fn = f.nodes[nd];
+                if (fn.word >> 31) {
+                    acc = acc + fn.value;
+                    break;
+                }
+                const uint32_t feat = fn.word & 0x1FFFFFFFu;
+                const float v = feat < n_features ? xr[(uint64_t)feat * fstride] : NAN;
+                bool left;
+                if (v != v) {
+                    left = (fn.word >> 30) & 1u;
+                } else if ((fn.word >> 29) & 1u) {
+                    const uint32_t cat = sat_u32(v);
+                    const uint32_t start = f.cat_seg[2 * nd], size = f.cat_seg[2 * nd + 1];
+                    const uint32_t wi = cat >> 5;
+                    const bool right = wi < size && ((f.cat_words[start + wi] >> (cat & 31)) & 1u);
+                    left = !right;
+                } else {
+                    left = v < fn.value;
+                }
+                nd = left ? fn.left : fn.right;
+            }
+        }
+        out[(uint64_t)g * n + i] = acc;
+    }
+}
+
+void launch_predict(const ForestDev& f, const float* x, uint64_t n, uint32_t n_features,
+                    int feature_major, float* out, cudaStream_t st) {
+    if (n == 0) return;
+    k_predict<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(f, x, n, n_features, feature_major, out);
+}
+
+__global__ void k_transform(int t, float* __restrict__ p, uint32_t G, uint64_t n) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 1) {
+        if (i >= (uint64_t)G * n) return;
+        const float x = p[i];
+        const float c = x < -500.0f ? -500.0f : (x > 500.0f ? 500.0f : x);
+        float r;
+        if (c >= 0.0f) {
+            r = 1.0f / (1.0f + exp_f32(-c));
+        } else {
+            const float e = exp_f32(c);
+            r = e / (1.0f + e);
+        }
+        p[i] = r;
+    } else if (t == 2) {
+        if (i >= n) return;
+        float mx = -INFINITY;
+        for (uint32_t g = 0; g < G; ++g) mx = fmaxf(mx, p[(uint64_t)g * n + i]);
+        float sum = 0.0f;
+        for (uint32_t g = 0; g < G; ++g) {
+            const float e = exp_f32(p[(uint64_t)g * n + i] - mx);
+            p[(uint64_t)g * n + i] = e;
+            sum = sum + e;
+        }
+        if (sum > 0.0f)
+            for (uint32_t g = 0; g < G; ++g) p[(uint64_t)g * n + i] = p[(uint64_t)g * n + i] / sum;
+    }
+}
+
+void launch_transform(int transform, float* out, uint32_t G, uint64_t n, cudaStream_t st) {
+    if (transform == 0 || n == 0) return;
+    const uint64_t total = transform == 1 ? (uint64_t)G * n : n;
+    k_transform<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(transform, out, G, n);
+}
+
+}  // namespace bst

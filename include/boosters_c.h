@@ -1,0 +1,343 @@
+/*
+ * boosters_c.h — C ABI of the B200-native GBDT engine (libboosters_b200.so).
+ *
+ * The entry points are the drop-in replacement for the Rust API of
+ * egordm/boosters on its GBDT hot path (binning, training, prediction).
+ * Every function that can fail returns a bst_status; the thread-local
+ * message of the last failure is available from bst_last_error().
+ * Handles are opaque, created and freed by the library. Output buffers are
+ * owned by the caller. No function aborts the process.
+ *
+ * Array layouts follow the reference:
+ *   features  feature-major  [n_features, n_samples]  f32 (NaN = missing)
+ *   targets   output-major   [n_outputs,  n_samples]  f32
+ *   weights                  [n_samples]              f32
+ *   predictions group-major  [n_groups,   n_samples]  f32
+ *
+ * Reference interfaces are cited as crates/boosters/src/<file>:<line>.
+ */
+#ifndef BOOSTERS_C_H
+#define BOOSTERS_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                             */
+/* ------------------------------------------------------------------------ */
+
+typedef int32_t bst_status;
+#define BST_OK 0
+#define BST_ERR_INVALID_ARGUMENT 1 /* null pointer, shape mismatch          */
+#define BST_ERR_CONFIG 2           /* model/gbdt/config.rs:39 ConfigError   */
+#define BST_ERR_EMPTY_DATASET 3    /* data/binned/dataset.rs:29 EmptyDataset */
+#define BST_ERR_MISSING_TARGETS 4  /* model/gbdt/model.rs:127 (panics there) */
+#define BST_ERR_UNSUPPORTED 5      /* feature outside the GPU engine's scope */
+#define BST_ERR_CUDA 6             /* CUDA runtime error / no device        */
+#define BST_ERR_OUT_OF_MEMORY 7
+#define BST_ERR_TIMEOUT 8
+#define BST_ERR_FORMAT 9 /* malformed model bytes                           */
+
+/* Message of the last failure on the calling thread ("" if none). */
+const char* bst_last_error(void);
+/* Library version string. */
+const char* bst_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Configuration  (model/gbdt/config.rs:111-226 GBDTConfig,                 */
+/*                 data/binned/feature_analysis.rs:29-63 BinningConfig)     */
+/* ------------------------------------------------------------------------ */
+
+#define BST_OBJ_SQUARED 0  /* training/objectives/regression.rs:20       */
+#define BST_OBJ_LOGISTIC 1 /* training/objectives/classification.rs:24   */
+#define BST_OBJ_SOFTMAX 2  /* training/objectives/classification.rs:141  */
+
+#define BST_METRIC_DEFAULT -1 /* derived from the objective (training/metrics/mod.rs) */
+#define BST_METRIC_NONE 0
+#define BST_METRIC_RMSE 1
+#define BST_METRIC_LOGLOSS 2
+#define BST_METRIC_MLOGLOSS 3
+
+#define BST_GROWTH_DEPTHWISE 0 /* training/gbdt/expansion.rs:46 DepthWise */
+#define BST_GROWTH_LEAFWISE 1  /* training/gbdt/expansion.rs:51 LeafWise  */
+
+/* GPU extension: histogram accumulation precision.
+ * FP32: f32 grad/hess accumulated exactly in 64-bit fixed point (the
+ *       reference's f64 histograms, training/gbdt/histograms/ops.rs:42).
+ * Q16 / Q8: grad/hess quantised per round to int16 / int8 with stochastic
+ *       rounding, histograms accumulated exactly in int32. */
+#define BST_PRECISION_FP32 0
+#define BST_PRECISION_Q16 1
+#define BST_PRECISION_Q8 2
+
+typedef struct bst_config {
+    /* objective & metric */
+    int32_t objective;    /* BST_OBJ_*                                      */
+    uint32_t n_classes;   /* softmax only                                   */
+    int32_t metric;       /* BST_METRIC_*                                   */
+    /* boosting */
+    uint32_t n_trees;     /* default 100                                    */
+    float learning_rate;  /* default 0.3                                    */
+    /* tree */
+    int32_t growth_strategy; /* BST_GROWTH_*, default depth-wise            */
+    uint32_t max_depth;      /* depth-wise, default 6                       */
+    uint32_t max_leaves;     /* leaf-wise, default 31                       */
+    uint32_t max_onehot_cats; /* default 4                                  */
+    /* regularisation (training/gbdt/split/gain.rs:60-86 GainParams) */
+    float lambda;           /* default 1.0                                  */
+    float alpha;            /* default 0.0                                  */
+    float min_child_weight; /* default 1.0                                  */
+    float min_gain;         /* default 0.0                                  */
+    uint32_t min_samples_leaf; /* default 1                                 */
+    /* sampling (only 1.0 is supported by the GPU engine)                   */
+    float subsample;
+    float colsample_bytree;
+    float colsample_bylevel;
+    /* binning */
+    uint32_t max_bins;                   /* default 256                     */
+    float sparsity_threshold;            /* default 0.9                     */
+    int32_t enable_bundling;             /* default 1                       */
+    uint32_t max_categorical_cardinality; /* default 0 (no auto-detect)     */
+    uint64_t binning_sample_cnt;         /* default 200000                  */
+    /* early stopping: < 0 means None */
+    int32_t early_stopping_rounds;
+    /* resources / reproducibility */
+    uint64_t cache_size; /* default 8 (host histogram LRU of the reference) */
+    uint64_t seed;       /* default 42                                      */
+    int32_t verbosity;   /* default 0 (silent)                              */
+    /* GPU extensions */
+    int32_t precision;     /* BST_PRECISION_*, default FP32                 */
+    int32_t batched;       /* 1: device-side frontier batching (default 1)  */
+    int32_t cuda_graph;    /* 1: capture each boosting round in a CUDA graph */
+    int32_t device;        /* CUDA device ordinal, default 0                */
+    int32_t record_leaves; /* 1: keep per-tree row->leaf arrays (tests)     */
+} bst_config;
+
+/* Fill *cfg with the reference defaults (GBDTConfig::default(),
+ * model/gbdt/config.rs:316). */
+void bst_config_default(bst_config* cfg);
+
+/* GBDTConfig::validate (model/gbdt/config.rs:252-310): returns BST_OK or
+ * BST_ERR_CONFIG with the reference's message. */
+bst_status bst_config_validate(const bst_config* cfg);
+
+/* ------------------------------------------------------------------------ */
+/* Dataset  (data/raw/dataset.rs:139 Dataset::from_array,                   */
+/*           data/raw/dataset.rs:635 DatasetBuilder::add_categorical)       */
+/* ------------------------------------------------------------------------ */
+
+typedef struct bst_dataset bst_dataset;
+
+/* Copies the host arrays. targets may be NULL (n_outputs ignored), weights
+ * may be NULL (uniform), categorical_features lists feature indices that
+ * the schema marks categorical. */
+bst_status bst_dataset_create(const float* features, uint64_t n_features, uint64_t n_samples,
+                              const float* targets, uint32_t n_outputs, const float* weights,
+                              const uint32_t* categorical_features, uint32_t n_categorical,
+                              bst_dataset** out);
+void bst_dataset_free(bst_dataset* ds);
+uint64_t bst_dataset_n_samples(const bst_dataset* ds);
+uint64_t bst_dataset_n_features(const bst_dataset* ds);
+
+/* ------------------------------------------------------------------------ */
+/* Binned dataset  (data/binned/dataset.rs:207 BinnedDataset::from_dataset) */
+/* ------------------------------------------------------------------------ */
+
+typedef struct bst_binned bst_binned;
+
+/* Feature analysis and bin bounds on the host, bin assignment on the GPU
+ * (data/binned/dataset.rs:592-842). */
+bst_status bst_binned_create(const bst_dataset* ds, const bst_config* cfg, bst_binned** out);
+void bst_binned_free(bst_binned* b);
+/* Effective columns (data/binned/dataset.rs:460 feature_views). */
+uint32_t bst_binned_n_columns(const bst_binned* b);
+/* Per effective column: source feature, bin count, categorical flag,
+ * has-missing flag, default (missing) bin. Any pointer may be NULL. */
+bst_status bst_binned_column_info(const bst_binned* b, uint32_t col, uint32_t* feature,
+                                  uint32_t* n_bins, int32_t* is_categorical,
+                                  int32_t* has_missing, uint32_t* default_bin);
+/* Numeric upper bounds of a column (n_bins doubles; bin_mapper.rs:57). */
+bst_status bst_binned_column_bounds(const bst_binned* b, uint32_t col, double* out);
+/* Logical bin of every row of a column, copied back from the GPU. */
+bst_status bst_binned_column_bins(const bst_binned* b, uint32_t col, uint16_t* out);
+
+/* ------------------------------------------------------------------------ */
+/* Training and prediction  (model/gbdt/model.rs:115 GBDTModel::train,      */
+/*                           :217 predict, :238 predict_raw)                */
+/* ------------------------------------------------------------------------ */
+
+typedef struct bst_model bst_model;
+
+/* n_threads keeps the reference's meaning for split tie-breaking:
+ * 1 = sequential (first maximal feature wins), otherwise the rayon
+ * reduction order (last maximal feature wins when >= 16 features,
+ * training/gbdt/split/find.rs:125-129,266-269). val may be NULL. */
+bst_status bst_gbdt_train(const bst_dataset* train, const bst_dataset* val,
+                          const bst_config* cfg, uint32_t n_threads, bst_model** out);
+
+/* out: caller-owned [n_groups, n_samples]. Transformed (sigmoid/softmax). */
+bst_status bst_gbdt_predict(const bst_model* m, const bst_dataset* ds, uint32_t n_threads,
+                            float* out);
+/* out: caller-owned [n_groups, n_samples]. Raw margins. */
+bst_status bst_gbdt_predict_raw(const bst_model* m, const bst_dataset* ds, uint32_t n_threads,
+                                float* out);
+
+/* Device-pointer prediction: features_dev is sample-major [n_rows,
+ * n_features] f32 in device memory, out_dev is [n_groups, n_rows] f32 in
+ * device memory; runs on `stream` (cudaStream_t, NULL = legacy stream)
+ * without synchronising. raw != 0 skips the output transform. */
+bst_status bst_gbdt_predict_device(const bst_model* m, const float* features_dev,
+                                   uint64_t n_rows, uint64_t n_features, int32_t raw,
+                                   float* out_dev, void* stream);
+
+void bst_model_free(bst_model* m);
+uint32_t bst_model_n_trees(const bst_model* m);
+uint32_t bst_model_n_groups(const bst_model* m);
+uint32_t bst_model_n_features(const bst_model* m);
+/* Base scores, one per group. */
+bst_status bst_model_base_scores(const bst_model* m, float* out);
+/* Training predictions [n_groups, n_samples] left after the last round. */
+bst_status bst_model_train_predictions(const bst_model* m, float* out);
+
+/* Tree introspection (repr/gbdt/tree.rs:32-47 Tree SoA). */
+bst_status bst_model_tree_info(const bst_model* m, uint32_t tree, uint32_t* n_nodes,
+                               uint32_t* group, uint32_t* n_category_words);
+/* Any pointer may be NULL; arrays have n_nodes entries. */
+bst_status bst_model_tree_nodes(const bst_model* m, uint32_t tree, uint32_t* split_index,
+                                float* threshold, uint32_t* left, uint32_t* right,
+                                uint8_t* default_left, uint8_t* is_leaf, float* leaf_value,
+                                uint8_t* split_type, float* gain, float* cover);
+/* Categorical bitsets (repr/gbdt/categories.rs:29 CategoriesStorage). */
+bst_status bst_model_tree_categories(const bst_model* m, uint32_t tree, uint32_t* seg_start,
+                                     uint32_t* seg_size, uint32_t* words);
+/* Training-time detail per node: the bin threshold chosen by the split scan
+ * (0xFFFFFFFF for leaves / categorical) and the node's gradient and hessian
+ * sums (f64). Any pointer may be NULL. */
+bst_status bst_model_tree_train_info(const bst_model* m, uint32_t tree, uint32_t* split_bin,
+                                     double* grad_sum, double* hess_sum);
+/* With cfg.record_leaves: the tree node (leaf) each training row reached in
+ * the row partition of that tree (training/gbdt/partition.rs:296). */
+bst_status bst_model_tree_row_leaves(const bst_model* m, uint32_t tree, uint32_t* out);
+
+/* Per-phase device timings of the last training call, in milliseconds:
+ * [binning, gradients, histograms, split scan, partition, leaf update,
+ *  other, total]. */
+bst_status bst_model_train_timings(const bst_model* m, double* out8);
+/* Work counters of the last training call: [kernel launches, histogram
+ * launches, histogram row visits, histogram algorithmic bytes (rows x
+ * (bin bytes per row + 12)), split-scan launches, partitioned rows]. */
+bst_status bst_model_train_counters(const bst_model* m, uint64_t* out, uint32_t n);
+
+/* ------------------------------------------------------------------------ */
+/* Component entry points (the reference's public building blocks)         */
+/* ------------------------------------------------------------------------ */
+
+/* BinMapper::value_to_bin (data/binned/bin_mapper.rs:210) on the GPU for one
+ * mapper. missing_type: 0 None, 1 Zero, 2 NaN. For categorical mappers
+ * pass the sorted category values in cats (bounds ignored). */
+bst_status bst_bin_values(const double* bounds, uint32_t n_bounds, int32_t missing_type,
+                          uint32_t default_bin, int32_t is_categorical, const int32_t* cats,
+                          uint32_t n_cats, const float* values, uint64_t n_values,
+                          uint32_t* out);
+
+/* HistogramBuilder::build_gathered / build_contiguous
+ * (training/gbdt/histograms/ops.rs:79,105) on the GPU. bins is
+ * feature-major [n_features, n_samples] logical bins; rows selects the node
+ * (NULL = all rows); out receives [sum(n_bins)][2] f64 (grad, hess). */
+bst_status bst_histogram_build(const uint16_t* bins, const uint32_t* n_bins,
+                               uint32_t n_features, uint64_t n_samples, const float* grad,
+                               const float* hess, const uint32_t* rows, uint64_t n_rows,
+                               double* out);
+
+/* Incremental training: the boosting loop of GBDTTrainer::train
+ * (training/gbdt/trainer.rs:242-401) over a GPU-resident binned copy of
+ * `train`, a caller-chosen number of rounds per update. cfg.n_trees is
+ * ignored; bst_booster_model snapshots the trees trained so far. */
+typedef struct bst_booster bst_booster;
+bst_status bst_booster_create(const bst_dataset* train, const bst_config* cfg, uint32_t n_threads,
+                              bst_booster** out);
+bst_status bst_booster_update(bst_booster* b, uint32_t n_rounds);
+uint32_t bst_booster_n_rounds(const bst_booster* b);
+bst_status bst_booster_model(const bst_booster* b, bst_model** out);
+/* Cumulative timings (as bst_model_train_timings) and counters (as
+ * bst_model_train_counters) of every update so far. */
+bst_status bst_booster_stats(const bst_booster* b, double* timings8, uint64_t* counters,
+                             uint32_t n_counters);
+void bst_booster_free(bst_booster* b);
+
+/* TreeGrower::grow (training/gbdt/grower.rs:265) on caller-given gradients:
+ * bins ds, grows one tree on the GPU and returns it as a one-tree model (base
+ * score 0, identity transform). grad / hess have n_samples entries. */
+bst_status bst_tree_grow(const bst_dataset* ds, const float* grad, const float* hess,
+                         const bst_config* cfg, uint32_t n_threads, bst_model** out);
+
+/* Model from explicit SoA trees (repr/gbdt/tree.rs:62 Tree::new and
+ * repr/gbdt/forest.rs:31 Forest::push_tree). objective selects the output
+ * transform. Child indices are local to the tree; the arrays are validated. */
+bst_status bst_model_create(uint32_t n_groups, uint32_t n_features, int32_t objective,
+                            const float* base_scores, bst_model** out);
+bst_status bst_model_add_tree(bst_model* m, uint32_t group, uint32_t n_nodes,
+                              const uint32_t* split_index, const float* threshold,
+                              const uint32_t* left, const uint32_t* right,
+                              const uint8_t* default_left, const uint8_t* is_leaf,
+                              const float* leaf_value, const uint8_t* split_type,
+                              const uint32_t* seg_start, const uint32_t* seg_size,
+                              const uint32_t* words, uint32_t n_words);
+
+/* A split as chosen by the split scan (training/gbdt/split/types.rs:34). */
+typedef struct bst_split {
+    uint32_t feature;      /* effective column                             */
+    float gain;            /* -inf when invalid                            */
+    int32_t default_left;
+    int32_t is_categorical;
+    uint32_t bin;          /* numerical: bins <= bin go left               */
+    uint64_t left_cats[4]; /* categorical: bins going left (<= 256 bins)   */
+} bst_split;
+
+/* GreedySplitter::find_split (training/gbdt/split/find.rs:113) on the GPU
+ * over a host histogram [sum(n_bins)][2] f64. */
+bst_status bst_find_split(const double* histogram, const uint32_t* n_bins,
+                          const int32_t* is_categorical, const int32_t* has_missing,
+                          uint32_t n_features, double parent_grad, double parent_hess,
+                          uint32_t parent_count, const bst_config* cfg, uint32_t n_threads,
+                          bst_split* out);
+
+/* ------------------------------------------------------------------------ */
+/* Seeded synthetic workloads (host, counter-based; identical bytes for any */
+/* consumer). Feature-major x [n_features, n_samples], y [n_samples].       */
+/* ------------------------------------------------------------------------ */
+
+/* Regression: x ~ N(0,1); y = x.w + 0.1 N(0,1), w ~ N(0,1) on the first
+ * n_informative features and 0 elsewhere. */
+bst_status bst_synth_regression(uint64_t n_samples, uint64_t n_features,
+                                uint64_t n_informative, uint64_t seed, uint64_t stream,
+                                float* x, float* y);
+/* Binary: even columns N(0,1), odd U(0,1); columns < n_nan_cols get 10% NaN;
+ * y ~ Bernoulli(sigmoid(sum of 10 pairwise products + N(0,0.5))), NaN->0 in
+ * the label formula. */
+bst_status bst_synth_binary(uint64_t n_samples, uint64_t n_features, uint64_t n_nan_cols,
+                            uint64_t seed, uint64_t stream, float* x, float* y);
+/* Multiclass with categoricals: n_numeric N(0,1) columns then n_categorical
+ * columns with cardinality U{4..64} and Zipf(1.2) frequencies (values
+ * 0..K-1); y = argmax_c(W_c.x_num + E_c[j][x_cat_j] + Gumbel). */
+bst_status bst_synth_multiclass(uint64_t n_samples, uint64_t n_numeric, uint64_t n_categorical,
+                                uint64_t n_classes, uint64_t seed, uint64_t stream, float* x,
+                                float* y);
+
+/* ------------------------------------------------------------------------ */
+/* Metrics (training/metrics/regression.rs:17, classification.rs:13,332)    */
+/* ------------------------------------------------------------------------ */
+
+/* preds [n_groups, n_samples] (probabilities for logloss/mlogloss). */
+bst_status bst_metric(int32_t metric, const float* preds, uint32_t n_groups, uint64_t n_samples,
+                      const float* targets, const float* weights, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BOOSTERS_C_H */

@@ -1,0 +1,129 @@
+/*
+ * oracle.h — CPU restatement of egordm/boosters' GBDT hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is the checker that the tests,
+ * the smoke check and the CPU-baseline leg of bench.py compare the CUDA
+ * engine against. The engine never links, loads or calls it.
+ *
+ * It follows the Rust CPU path with sequential (n_threads = 1) arithmetic:
+ * f64 histogram sums in partition order, the exact LRU histogram pool,
+ * the stable row partition and glibc expf. The rayon tie-breaking of the
+ * parallel split search is emulated when n_threads != 1, and the histogram
+ * build / split search can use OpenMP threads without changing any result.
+ */
+#ifndef BST_ORACLE_H
+#define BST_ORACLE_H
+
+#include <stdint.h>
+
+#include "../include/boosters_c.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_model orc_model;
+typedef struct orc_binned orc_binned;
+
+/* ---- binning (data/binned/dataset.rs:207) ---- */
+int orc_bin(const float* x_fm, uint64_t n_features, uint64_t n_samples,
+            const uint32_t* cat_idx, uint32_t n_cat, const bst_config* cfg, orc_binned** out);
+void orc_binned_free(orc_binned* b);
+uint32_t orc_binned_n_columns(const orc_binned* b);
+void orc_binned_column_info(const orc_binned* b, uint32_t col, uint32_t* feature,
+                            uint32_t* n_bins, int32_t* is_cat, int32_t* has_missing,
+                            uint32_t* default_bin);
+void orc_binned_column_bounds(const orc_binned* b, uint32_t col, double* out);
+void orc_binned_column_bins(const orc_binned* b, uint32_t col, uint16_t* out);
+
+/* BinMapper::value_to_bin for an explicit mapper (bin_mapper.rs:210). */
+uint32_t orc_value_to_bin(const double* bounds, uint32_t n_bounds, int32_t missing_type,
+                          uint32_t default_bin, int32_t is_cat, const int32_t* cats,
+                          uint32_t n_cats, double value);
+
+/* ---- components ---- */
+double orc_gain_full(double gl, double hl, double gr, double hr, double gp, double hp,
+                     float lambda, float min_gain); /* gain.rs:102 (returns the f32 value) */
+float orc_leaf_weight(double g, double h, float lambda, float alpha); /* gain.rs:151 */
+int orc_is_valid_split(double hl, double hr, uint32_t cl, uint32_t cr, float min_child_weight,
+                       uint32_t min_samples_leaf); /* gain.rs:123 */
+/* HistogramBuilder (ops.rs:79-127): bins feature-major u16; rows may be NULL. */
+void orc_histogram_build(const uint16_t* bins, const uint32_t* n_bins, uint32_t n_features,
+                         uint64_t n_samples, const float* grad, const float* hess,
+                         const uint32_t* rows, uint64_t n_rows, double* out);
+/* GreedySplitter::find_split (find.rs:113). */
+void orc_find_split(const double* hist, const uint32_t* n_bins, const int32_t* is_cat,
+                    const int32_t* has_missing, uint32_t n_features, double pg, double ph,
+                    uint32_t pc, const bst_config* cfg, uint32_t n_threads, bst_split* out);
+/* Objective gradients (objectives/mod.rs:236) for [n_outputs, n] preds. */
+void orc_gradients(int32_t objective, uint32_t n_outputs, const float* preds, const float* y,
+                   const float* w, uint64_t n, float* grad, float* hess);
+void orc_base_score(int32_t objective, uint32_t n_outputs, const float* y, const float* w,
+                    uint64_t n, float* out);
+/* OutputTransform::transform_inplace (transform.rs:61); transform: 0 id, 1 sigmoid, 2 softmax */
+void orc_transform(int32_t transform, float* preds, uint32_t n_groups, uint64_t n);
+double orc_metric(int32_t metric, const float* preds, uint32_t n_groups, uint64_t n,
+                  const float* y, const float* w);
+
+/* ---- training (model/gbdt/model.rs:115) ---- */
+/* Returns 0 on success, else a bst_status code. record_leaves keeps per-tree
+ * row->leaf arrays. omp_threads = threads the histogram build / split search
+ * may use (results are identical for any value). */
+int orc_train(const float* x_fm, uint64_t n_features, uint64_t n_samples, const float* y,
+              uint32_t y_rows, const float* w, const uint32_t* cat_idx, uint32_t n_cat,
+              const bst_config* cfg, uint32_t n_threads, int record_leaves, int omp_threads,
+              orc_model** out);
+/* Same, but stop after max_trees trees (bounded CPU-baseline samples). */
+int orc_train_limited(const float* x_fm, uint64_t n_features, uint64_t n_samples,
+                      const float* y, uint32_t y_rows, const float* w, const uint32_t* cat_idx,
+                      uint32_t n_cat, const bst_config* cfg, uint32_t n_threads,
+                      int record_leaves, int omp_threads, uint32_t max_trees, orc_model** out);
+void orc_model_free(orc_model* m);
+uint32_t orc_model_n_trees(const orc_model* m);
+uint32_t orc_model_n_groups(const orc_model* m);
+void orc_model_base_scores(const orc_model* m, float* out);
+void orc_model_train_predictions(const orc_model* m, float* out);
+void orc_tree_info(const orc_model* m, uint32_t t, uint32_t* n_nodes, uint32_t* group,
+                   uint32_t* n_cat_words);
+void orc_tree_nodes(const orc_model* m, uint32_t t, uint32_t* split_index, float* threshold,
+                    uint32_t* left, uint32_t* right, uint8_t* default_left, uint8_t* is_leaf,
+                    float* leaf_value, uint8_t* split_type, float* gain, float* cover);
+void orc_tree_categories(const orc_model* m, uint32_t t, uint32_t* seg_start,
+                         uint32_t* seg_size, uint32_t* words);
+void orc_tree_train_info(const orc_model* m, uint32_t t, uint32_t* split_bin, double* grad_sum,
+                         double* hess_sum);
+void orc_tree_row_leaves(const orc_model* m, uint32_t t, uint32_t* out);
+/* Seconds spent in tree growth + prediction updates (binning excluded). */
+double orc_model_train_seconds(const orc_model* m);
+double orc_model_binning_seconds(const orc_model* m);
+/* Seconds of tree t: its growth and prediction update (the first tree of a
+ * round also carries that round's gradient computation). */
+double orc_model_tree_seconds(const orc_model* m, uint32_t t);
+
+/* ---- prediction (model/gbdt/model.rs:217-258) ---- */
+int orc_predict(const orc_model* m, const float* x_fm, uint64_t n_features, uint64_t n_samples,
+                int raw, float* out);
+/* Sample-major rows [n, F] (the serving layout). */
+int orc_predict_rows(const orc_model* m, const float* x_sm, uint64_t n_features,
+                     uint64_t n_samples, int raw, int omp_threads, float* out);
+
+/* TreeGrower::grow (training/gbdt/grower.rs:265) on given gradients: one
+ * tree, returned as a one-tree model (base score 0, identity transform). */
+int orc_grow_tree(const float* x_fm, uint64_t n_features, uint64_t n_samples, const float* grad,
+                  const float* hess, const bst_config* cfg, uint32_t n_threads, orc_model** out);
+/* Model from explicit SoA trees (repr/gbdt/tree.rs:62 Tree::new, forest.rs push_tree). */
+int orc_model_create(uint32_t n_groups, uint32_t n_features, int32_t objective, const float* base,
+                     orc_model** out);
+int orc_model_add_tree(orc_model* m, uint32_t group, uint32_t n_nodes, const uint32_t* split_index,
+                       const float* threshold, const uint32_t* left, const uint32_t* right,
+                       const uint8_t* default_left, const uint8_t* is_leaf, const float* leaf_value,
+                       const uint8_t* split_type, const uint32_t* seg_start, const uint32_t* seg_size,
+                       const uint32_t* words, uint32_t n_words);
+
+const char* orc_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
