@@ -758,7 +758,7 @@ bst_status bst_find_split(const double* hist, const uint32_t* n_bins, const int3
             out->gain = s.gain;
             out->default_left = (s.flags & 1u) ? 1 : 0;
             out->is_categorical = (s.flags & 2u) ? 1 : 0;
-            out->bin = s.bin;
+            out->bin = (s.flags & 2u) ? 0u : s.bin;  // SplitType::Categorical has no bin
             for (int q = 0; q < 4; ++q) out->left_cats[q] = s.cats[q];
         }
         return BST_OK;

@@ -244,12 +244,14 @@ k_hist_build(const HistChunk* __restrict__ chunks, const HistTile* __restrict__ 
              const uint32_t* __restrict__ ridx, const float2* __restrict__ gh,
              const double* __restrict__ scale, const uint8_t* __restrict__ bins8, uint32_t s8,
              const uint16_t* __restrict__ bins16, uint32_t s16, HBin* __restrict__ hist,
-             uint64_t slot_bins) {
+             uint64_t slot_bins, uint32_t n_tiles) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     HBin* sm = reinterpret_cast<HBin*>(smem_raw);
     __shared__ HistTile tile;
-    const HistChunk chunk = chunks[blockIdx.y];
-    if (threadIdx.x == 0) tile = tiles[blockIdx.x];
+    // tiles vary fastest so the blocks of one row chunk run together and
+    // share its grad/hess and row ids in L2
+    const HistChunk chunk = chunks[blockIdx.x / n_tiles];
+    if (threadIdx.x == 0) tile = tiles[blockIdx.x % n_tiles];
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < tile.smem_bins; i += HIST_THREADS)
         reinterpret_cast<uint4*>(sm)[i] = make_uint4(0, 0, 0, 0);
@@ -335,16 +337,17 @@ void launch_hist_build(const HistChunk* chunks, uint32_t n_chunks, const HistTil
         cudaFuncSetAttribute(k_hist_build, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         attr_set = true;
     }
-    dim3 grid(n_tiles, n_chunks);
-    k_hist_build<<<grid, HIST_THREADS, smem, st>>>(chunks, tiles, ridx, gh, scale, bins8, s8,
-                                                   bins16, s16, hist, slot_bins);
+    const uint64_t blocks = (uint64_t)n_tiles * n_chunks;
+    if (blocks > 0x7FFFFFFFull) return;
+    k_hist_build<<<(unsigned)blocks, HIST_THREADS, smem, st>>>(chunks, tiles, ridx, gh, scale, bins8, s8,
+                                                              bins16, s16, hist, slot_bins, n_tiles);
 }
 
 __global__ void k_hist_finish(const FinishWork* __restrict__ works, HBin* __restrict__ hist,
-                              uint64_t slot_bins, uint32_t total_bins) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+                              uint64_t slot_bins, uint32_t total_bins, uint32_t blocks_per_work) {
+    const uint32_t i = (blockIdx.x % blocks_per_work) * blockDim.x + threadIdx.x;
     if (i >= total_bins) return;
-    const FinishWork w = works[blockIdx.y];
+    const FinishWork w = works[blockIdx.x / blocks_per_work];
     HBin* L = hist + (size_t)w.left * slot_bins + i;
     HBin* R = hist + (size_t)w.right * slot_bins + i;
     const HBin p = *L, s = *R;
@@ -362,8 +365,10 @@ __global__ void k_hist_finish(const FinishWork* __restrict__ works, HBin* __rest
 void launch_hist_finish(const FinishWork* w, uint32_t n_work, HBin* hist, uint64_t slot_bins,
                         uint32_t total_bins, cudaStream_t st) {
     if (n_work == 0 || total_bins == 0) return;
-    dim3 grid((total_bins + 255) / 256, n_work);
-    k_hist_finish<<<grid, 256, 0, st>>>(w, hist, slot_bins, total_bins);
+    const uint32_t per = (total_bins + 255) / 256;
+    const uint64_t blocks = (uint64_t)per * n_work;
+    if (blocks > 0x7FFFFFFFull) return;
+    k_hist_finish<<<(unsigned)blocks, 256, 0, st>>>(w, hist, slot_bins, total_bins, per);
 }
 
 __global__ void k_node_sums(const HistChunk* __restrict__ chunks, const uint32_t* __restrict__ ridx,
@@ -464,12 +469,12 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32)
 k_split_scan(const ScanNode* __restrict__ nodes, const ScanColumn* __restrict__ cols,
              uint32_t n_cols, const HBin* __restrict__ hist, uint64_t slot_bins,
              const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
-             long long* __restrict__ node_tot) {
+             long long* __restrict__ node_tot, uint32_t col_blocks) {
     __shared__ double s_key[SCAN_WARPS][SORT_N];
     __shared__ uint32_t s_cat[SCAN_WARPS][SORT_N];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t col = blockIdx.x * SCAN_WARPS + warp;
-    const uint32_t node = blockIdx.y;
+    const uint32_t col = (blockIdx.x % col_blocks) * SCAN_WARPS + warp;
+    const uint32_t node = blockIdx.x / col_blocks;
     if (col >= n_cols) return;
     const ScanColumn cm = cols[col];
     const ScanNode nd = nodes[node];
@@ -671,9 +676,11 @@ void launch_split_scan(const ScanNode* nodes, uint32_t n_nodes, const ScanColumn
                        const double* scale, GainParamsDev gp, ColCand* cand,
                        long long* node_tot, cudaStream_t st) {
     if (n_nodes == 0 || n_cols == 0) return;
-    dim3 grid((n_cols + SCAN_WARPS - 1) / SCAN_WARPS, n_nodes);
-    k_split_scan<<<grid, SCAN_WARPS * 32, 0, st>>>(nodes, cols, n_cols, hist, slot_bins, scale,
-                                                    gp, cand, node_tot);
+    const uint32_t per = (n_cols + SCAN_WARPS - 1) / SCAN_WARPS;
+    const uint64_t blocks = (uint64_t)per * n_nodes;
+    if (blocks > 0x7FFFFFFFull) return;
+    k_split_scan<<<(unsigned)blocks, SCAN_WARPS * 32, 0, st>>>(nodes, cols, n_cols, hist, slot_bins, scale,
+                                                              gp, cand, node_tot, per);
 }
 
 // Across columns (find.rs:180-212 sequential; :219-270 rayon reduce).
