@@ -584,6 +584,18 @@ static double fixed_scale(double bound) {
     return std::ldexp(1.0, k);
 }
 
+// The rule of k_fixed_scales: |q| <= 2^HIST_QBITS and n * 2^k * max < 2^62.
+static double hist_scale(float m, uint64_t n) {
+    if (!(m > 0.0f)) return 1.0;
+    int e, en;
+    std::frexp((double)m, &e);
+    std::frexp((double)n, &en);
+    int B = bst::HIST_QBITS;
+    if (61 - en < B) B = 61 - en;
+    int k = std::max(-1000, std::min(1000, B - e));
+    return std::ldexp(1.0, k);
+}
+
 static bst::BinPlan plan_from_counts(const uint32_t* n_bins, uint32_t F, uint64_t n) {
     bst::BinPlan p;
     p.n = n;
@@ -642,7 +654,7 @@ bst_status bst_histogram_build(const uint16_t* bins, const uint32_t* n_bins, uin
             if (std::fabs(grad[i]) <= 3.4e38f) mg = std::max(mg, std::fabs(grad[i]));
             if (std::fabs(hess[i]) <= 3.4e38f) mh = std::max(mh, std::fabs(hess[i]));
         }
-        const double scale[4] = {fixed_scale((double)n * mg), fixed_scale((double)n * mh), 0, 0};
+        const double scale[4] = {hist_scale(mg, n), hist_scale(mh, n), 0, 0};
         std::vector<bst::HistTile> tiles;
         uint32_t max_smem = 0;
         bst::build_hist_tiles(p, tiles, max_smem);

@@ -215,9 +215,15 @@ __global__ void k_fixed_scales(const unsigned* __restrict__ maxabs, uint32_t G, 
     const float m = __uint_as_float(maxabs[i]);
     int k = 0;
     if (m > 0.0f) {
-        int e;
-        frexp((double)n * (double)m, &e);  // n*m < 2^e
-        k = 62 - e;
+        int e, en;
+        frexp((double)m, &e);  // max|v| < 2^e
+        frexp((double)n, &en);  // n < 2^en
+        // |q| <= 2^B: 4096-row shared-memory partial sums fit the 32-bit
+        // hi/lo split of k_hist_build, and n * 2^B < 2^62 keeps every int64
+        // sum exact
+        int B = HIST_QBITS;
+        if (61 - en < B) B = 61 - en;
+        k = B - e;
         if (k > 1000) k = 1000;
         if (k < -1000) k = -1000;
     }
@@ -233,27 +239,40 @@ void launch_fixed_scales(const unsigned* maxabs, uint32_t G, uint64_t n, double*
 
 // ============================================================================
 // K4: histogram build (HistogramBuilder, training/gbdt/histograms/ops.rs:79-127)
-// Shared-memory privatised 64-bit fixed-point histograms over a tile of
-// columns; 128-bit row loads; one global atomic flush per non-empty bin.
+// Shared-memory privatised fixed-point histograms over a tile of columns,
+// 128-bit row loads, one global atomic flush per non-empty bin.
+// Each int64 value q (|q| <= 2^38) is split exactly into lo = q mod 2^20 and
+// hi = q >> 20, accumulated with 32-bit shared atomics (several times the
+// throughput of 64-bit shared atomics on B200); a block covers at most 4096
+// rows, so 4096 * 2^20 < 2^32 and 4096 * 2^18 < 2^31 and the recombined
+// sums hi * 2^20 + lo are exact.
 // ============================================================================
 
 constexpr int HIST_THREADS = 256;
+
+__device__ __forceinline__ void hist_add(uint32_t* s, uint32_t S, uint32_t idx, long long qg, long long qh) {
+    const uint32_t lo_mask = (1u << HIST_LO_BITS) - 1u;
+    atomicAdd(&s[idx], (uint32_t)qg & lo_mask);
+    atomicAdd(&s[S + idx], (uint32_t)(qg >> HIST_LO_BITS));
+    atomicAdd(&s[2 * S + idx], (uint32_t)qh & lo_mask);
+    atomicAdd(&s[3 * S + idx], (uint32_t)(qh >> HIST_LO_BITS));
+}
 
 __global__ void __launch_bounds__(HIST_THREADS)
 k_hist_build(const HistChunk* __restrict__ chunks, const HistTile* __restrict__ tiles,
              const uint32_t* __restrict__ ridx, const float2* __restrict__ gh,
              const double* __restrict__ scale, const uint8_t* __restrict__ bins8, uint32_t s8,
              const uint16_t* __restrict__ bins16, uint32_t s16, HBin* __restrict__ hist,
-             uint64_t slot_bins, uint32_t n_tiles) {
+             uint64_t slot_bins, uint32_t n_tiles, uint32_t S) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    HBin* sm = reinterpret_cast<HBin*>(smem_raw);
+    uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);  // [lo_g | hi_g | lo_h | hi_h] x S
     __shared__ HistTile tile;
     // tiles vary fastest so the blocks of one row chunk run together and
     // share its grad/hess and row ids in L2
     const HistChunk chunk = chunks[blockIdx.x / n_tiles];
     if (threadIdx.x == 0) tile = tiles[blockIdx.x % n_tiles];
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < tile.smem_bins; i += HIST_THREADS)
+    for (uint32_t i = threadIdx.x; i < S; i += HIST_THREADS)  // S is a multiple of 4
         reinterpret_cast<uint4*>(sm)[i] = make_uint4(0, 0, 0, 0);
     __syncthreads();
 
@@ -266,47 +285,38 @@ k_hist_build(const HistChunk* __restrict__ chunks, const HistTile* __restrict__ 
         lnb[l] = tile.lane_nbins[l];
     }
     const bool ident = chunk.flags & 1u;
+    const uint32_t count = min(chunk.count, (uint32_t)HIST_CHUNK_MAX);
     if (tile.matrix == 0) {
         const uint8_t* base = bins8 + (size_t)tile.vec * 16u;
-        for (uint32_t i = threadIdx.x; i < chunk.count; i += HIST_THREADS) {
+        for (uint32_t i = threadIdx.x; i < count; i += HIST_THREADS) {
             const uint32_t p = chunk.begin + i;
             const uint32_t row = ident ? p : ridx[p];
             const float2 v = gh[row];
-            const unsigned long long qg = (unsigned long long)quantize(v.x, sg);
-            const unsigned long long qh = (unsigned long long)quantize(v.y, sh);
+            const long long qg = quantize(v.x, sg), qh = quantize(v.y, sh);
             const uint4 b = *reinterpret_cast<const uint4*>(base + (size_t)row * s8);
             const uint32_t words[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
             for (int l = 0; l < 16; ++l) {
                 if (l >= (int)c0 && l < (int)c1) {
                     const uint32_t bin = (words[l >> 2] >> ((l & 3) * 8)) & 0xFFu;
-                    if (bin < lnb[l]) {
-                        HBin* d = sm + loff[l] + bin;
-                        atomicAdd(reinterpret_cast<unsigned long long*>(&d->g), qg);
-                        atomicAdd(reinterpret_cast<unsigned long long*>(&d->h), qh);
-                    }
+                    if (bin < lnb[l]) hist_add(sm, S, loff[l] + bin, qg, qh);
                 }
             }
         }
     } else {
         const uint16_t* base = bins16 + (size_t)tile.vec * 8u;
-        for (uint32_t i = threadIdx.x; i < chunk.count; i += HIST_THREADS) {
+        for (uint32_t i = threadIdx.x; i < count; i += HIST_THREADS) {
             const uint32_t p = chunk.begin + i;
             const uint32_t row = ident ? p : ridx[p];
             const float2 v = gh[row];
-            const unsigned long long qg = (unsigned long long)quantize(v.x, sg);
-            const unsigned long long qh = (unsigned long long)quantize(v.y, sh);
+            const long long qg = quantize(v.x, sg), qh = quantize(v.y, sh);
             const uint4 b = *reinterpret_cast<const uint4*>(base + (size_t)row * s16);
             const uint32_t words[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
             for (int l = 0; l < 8; ++l) {
                 if (l >= (int)c0 && l < (int)c1) {
                     const uint32_t bin = (words[l >> 1] >> ((l & 1) * 16)) & 0xFFFFu;
-                    if (bin < lnb[l]) {
-                        HBin* d = sm + loff[l] + bin;
-                        atomicAdd(reinterpret_cast<unsigned long long*>(&d->g), qg);
-                        atomicAdd(reinterpret_cast<unsigned long long*>(&d->h), qh);
-                    }
+                    if (bin < lnb[l]) hist_add(sm, S, loff[l] + bin, qg, qh);
                 }
             }
         }
@@ -316,10 +326,13 @@ k_hist_build(const HistChunk* __restrict__ chunks, const HistTile* __restrict__ 
     for (uint32_t l = c0; l < c1; ++l) {
         const uint32_t so = tile.lane_smem[l], go = tile.lane_hist[l], nb = tile.lane_nbins[l];
         for (uint32_t b = threadIdx.x; b < nb; b += HIST_THREADS) {
-            const HBin s = sm[so + b];
-            if (s.g | s.h) {
-                atomicAdd(reinterpret_cast<unsigned long long*>(&out[go + b].g), (unsigned long long)s.g);
-                atomicAdd(reinterpret_cast<unsigned long long*>(&out[go + b].h), (unsigned long long)s.h);
+            const uint32_t j = so + b;
+            const uint32_t glo = sm[j], ghi = sm[S + j], hlo = sm[2 * S + j], hhi = sm[3 * S + j];
+            if (glo | ghi | hlo | hhi) {
+                const long long g = (long long)(int32_t)ghi * (1ll << HIST_LO_BITS) + (long long)glo;
+                const long long h = (long long)(int32_t)hhi * (1ll << HIST_LO_BITS) + (long long)hlo;
+                atomicAdd(reinterpret_cast<unsigned long long*>(&out[go + b].g), (unsigned long long)g);
+                atomicAdd(reinterpret_cast<unsigned long long*>(&out[go + b].h), (unsigned long long)h);
             }
         }
     }
@@ -331,7 +344,8 @@ void launch_hist_build(const HistChunk* chunks, uint32_t n_chunks, const HistTil
                        const uint16_t* bins16, uint32_t s16, HBin* hist, uint64_t slot_bins,
                        cudaStream_t st) {
     if (n_chunks == 0 || n_tiles == 0) return;
-    const size_t smem = (size_t)max_smem_bins * sizeof(HBin);
+    const uint32_t S = (max_smem_bins + 3u) & ~3u;
+    const size_t smem = (size_t)S * 4u * sizeof(uint32_t);
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_hist_build, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -340,7 +354,7 @@ void launch_hist_build(const HistChunk* chunks, uint32_t n_chunks, const HistTil
     const uint64_t blocks = (uint64_t)n_tiles * n_chunks;
     if (blocks > 0x7FFFFFFFull) return;
     k_hist_build<<<(unsigned)blocks, HIST_THREADS, smem, st>>>(chunks, tiles, ridx, gh, scale, bins8, s8,
-                                                              bins16, s16, hist, slot_bins, n_tiles);
+                                                              bins16, s16, hist, slot_bins, n_tiles, S);
 }
 
 __global__ void k_hist_finish(const FinishWork* __restrict__ works, HBin* __restrict__ hist,

@@ -46,7 +46,12 @@ void launch_bin_assign(const float* x_fm, uint64_t n, const BinColumn* cols, uin
 void launch_gradients(int objective, uint32_t G, const float* pred, const float* y,
                       const float* w, uint64_t n, float2* gh, unsigned* maxabs,
                       cudaStream_t st);
-// scales [G][4] = (2^kg, 2^kh, 2^-kg, 2^-kh) with n*max*2^k < 2^62.
+// Fixed-point resolution: every grad/hess becomes round(v * 2^k) with
+// |q| <= 2^HIST_QBITS (and n * 2^k * max < 2^62 for the int64 sums).
+constexpr int HIST_QBITS = 38;
+constexpr int HIST_LO_BITS = 20;     // low part of the shared-memory split
+constexpr int HIST_CHUNK_MAX = 4096; // rows per block: 4096 * 2^20 < 2^32, 4096 * 2^18 < 2^31
+// scales [G][4] = (2^kg, 2^kh, 2^-kg, 2^-kh).
 void launch_fixed_scales(const unsigned* maxabs, uint32_t G, uint64_t n, double* scales,
                          cudaStream_t st);
 
