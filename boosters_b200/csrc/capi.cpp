@@ -717,12 +717,14 @@ bst_status bst_find_split(const double* hist, const uint32_t* n_bins, const int3
             if (is_cat[f] && n_bins[f] > 256) return fail(BST_ERR_UNSUPPORTED, "categorical features need <= 256 bins");
             total += n_bins[f];
         }
-        double ag = std::fabs(pg), ah = std::fabs(ph);
+        // bound on every prefix sum: bins x max|bin| + |parent| (order-independent)
+        double mg = 0.0, mh = 0.0;
         for (uint64_t i = 0; i < total; ++i) {
-            ag += std::fabs(hist[2 * i]);
-            ah += std::fabs(hist[2 * i + 1]);
+            mg = std::max(mg, std::fabs(hist[2 * i]));
+            mh = std::max(mh, std::fabs(hist[2 * i + 1]));
         }
-        const double sg = fixed_scale(ag), sh = fixed_scale(ah);
+        const double sg = fixed_scale((double)total * mg + std::fabs(pg));
+        const double sh = fixed_scale((double)total * mh + std::fabs(ph));
         std::vector<bst::HBin> h(total);
         for (uint64_t i = 0; i < total; ++i) {
             h[i].g = std::llrint(hist[2 * i] * sg);

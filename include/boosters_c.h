@@ -306,6 +306,32 @@ bst_status bst_find_split(const double* histogram, const uint32_t* n_bins,
                           uint32_t parent_count, const bst_config* cfg, uint32_t n_threads,
                           bst_split* out);
 
+/* The split search of bst_find_split, for callers that cannot allocate
+ * device memory per call: a process whose device memory is already fully
+ * reserved by another allocator, or latency-critical code that cannot afford
+ * cudaMalloc/cudaFree (cudaFree synchronises the whole device). This entry
+ * point has no counterpart in the reference.
+ *
+ * It allocates nothing. histogram_dev is a DEVICE array [sum(n_bins)][2] f64
+ * (grad, hess); n_bins / is_categorical / has_missing are host arrays; the
+ * result is written to the host struct *out after the work on `stream`
+ * (cudaStream_t, NULL = legacy stream) has finished. Results equal those of
+ * bst_find_split on the same histogram.
+ *
+ * Working memory is one fixed array in device global memory (about 1.1 MiB),
+ * which every GPU that loads the library holds until the process exits.
+ * Limits: n_features <= 1024, sum(n_bins) <= 65536, categorical features <=
+ * 256 bins; larger inputs return BST_ERR_INVALID_ARGUMENT. The first call on
+ * a device looks up that array's device address (once per device); make that
+ * first call before any stream capture. Every call shares the array: calls
+ * that overlap on the GPU (other streams, other host threads) race and must
+ * be serialised by the caller. */
+bst_status bst_find_split_noalloc(const double* histogram_dev, const uint32_t* n_bins,
+                                  const int32_t* is_categorical, const int32_t* has_missing,
+                                  uint32_t n_features, double parent_grad, double parent_hess,
+                                  uint32_t parent_count, const bst_config* cfg, uint32_t n_threads,
+                                  void* stream, bst_split* out);
+
 /* ------------------------------------------------------------------------ */
 /* Seeded synthetic workloads (host, counter-based; identical bytes for any */
 /* consumer). Feature-major x [n_features, n_samples], y [n_samples].       */
