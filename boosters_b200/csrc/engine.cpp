@@ -173,13 +173,23 @@ struct Timer {
         }
         return evs[used++];
     }
+    // in_graph: record as event-record nodes of a stream capture (a plain
+    // record during capture is only an internal dependency, not a timestamp)
+    bool in_graph = false;
+    bool broken = false;
+    void record(cudaEvent_t e) {
+        if (in_graph)
+            BST_CK(cudaEventRecordWithFlags(e, st, cudaEventRecordExternal));
+        else
+            BST_CK(cudaEventRecord(e, st));
+    }
     size_t begin(int phase) {
         size_t i = used;
-        BST_CK(cudaEventRecord(next(), st));
+        record(next());
         marks.push_back({phase, i});
         return i;
     }
-    void end() { BST_CK(cudaEventRecord(next(), st)); }
+    void end() { record(next()); }
     // stream must be idle
     void collect() {
         for (auto& m : marks) {
@@ -189,6 +199,30 @@ struct Timer {
         }
         marks.clear();
         used = 0;
+    }
+    void reserve(size_t k) {
+        while (evs.size() < k) {
+            cudaEvent_t e;
+            BST_CK(cudaEventCreate(&e));
+            evs.push_back(e);
+        }
+    }
+    // For events recorded inside a CUDA graph: accumulate, keep the marks.
+    // Returns false (and stops trying) if the events cannot be timed.
+    bool collect_keep() {
+        if (broken) return false;
+        double tmp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (auto& m : marks) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, evs[m.second], evs[m.second + 1]) != cudaSuccess) {
+                cudaGetLastError();
+                broken = true;
+                return false;
+            }
+            tmp[m.first] += ms;
+        }
+        for (int i = 0; i < 8; ++i) acc[i] += tmp[i];
+        return true;
     }
 };
 
@@ -278,7 +312,7 @@ class Trainer {
             BST_CK(cudaMemcpyAsync(h_scales_.data(), scales_.p, sizeof(double) * 4 * G_, cudaMemcpyDeviceToHost, st_));
             BST_CK(cudaStreamSynchronize(st_));
             for (uint32_t o = 0; o < G_; ++o) {
-                HostTree t = grow(o);
+                HostTree t = use_batched_ ? grow_batched(o) : grow(o);
                 t.group = o;
                 std::lock_guard<std::mutex> lk(m_.mu);
                 m_.trees.push_back(std::move(t));
@@ -403,6 +437,249 @@ class Trainer {
         d_sums_.alloc(2 * ((size_t)max_pnodes_ + 1));
         d_leaves_.alloc(max_pnodes_ + 1);
         stage_.reserve(max_chunks * 48 + (size_t)(max_pnodes_ + 4) * 256 + (1 << 20));
+        use_batched_ = cfg_.batched && !leafwise_ && n_cols_ > 0 && cfg_.max_depth <= 14;
+        if (use_batched_) setup_batched();
+    }
+
+    // ---- device-side level loop, one CUDA graph per output (kernels.h) -------
+    bool use_batched_ = false;
+    BDev bd_{};
+    DevArray<BState> d_bstate_;
+    DevArray<BNode> d_front_[2];
+    DevArray<BExp> d_bexp_;
+    DevArray<BTreeNode> d_btree_;
+    DevArray<BLeaf> d_bleaves_;
+    DevArray<BColumn> d_bcols_;
+    DevArray<HistChunk> d_root_chunks_;
+    DevArray<ScanNode> d_root_scan_;
+    uint32_t n_root_chunks_ = 0, max_tnodes_ = 0;
+    std::vector<cudaGraphExec_t> graphs_;
+    std::vector<std::unique_ptr<Timer>> gtimers_;
+    cudaEvent_t whole_[2] = {nullptr, nullptr};
+    std::vector<uint64_t> graph_launches_, graph_hist_launches_;
+    BTreeNode* h_btree_ = nullptr;
+    BState* h_bstate_ = nullptr;
+
+  public:
+    ~Trainer() {
+        for (auto g : graphs_)
+            if (g) cudaGraphExecDestroy(g);
+        if (h_btree_) cudaFreeHost(h_btree_);
+        if (h_bstate_) cudaFreeHost(h_bstate_);
+        for (auto e : whole_)
+            if (e) cudaEventDestroy(e);
+    }
+
+  private:
+
+    void setup_batched() {
+        init_kernel_attributes();
+        const uint32_t max_front = max_pnodes_;
+        max_tnodes_ = 2 * max_front;
+        d_bstate_.alloc(1);
+        d_front_[0].alloc(max_front);
+        d_front_[1].alloc(max_front);
+        d_bexp_.alloc(max_front / 2 + 1);
+        d_btree_.alloc(max_tnodes_);
+        d_bleaves_.alloc(max_front + 1);
+        std::vector<BColumn> bc(n_cols_);
+        for (uint32_t c = 0; c < n_cols_; ++c)
+            bc[c] = BColumn{p_.col_matrix[c], p_.col_pos[c], p_.col_missing[c], p_.col_default[c]};
+        d_bcols_.alloc(n_cols_);
+        BST_CK(cudaMemcpy(d_bcols_.p, bc.data(), sizeof(BColumn) * n_cols_, cudaMemcpyHostToDevice));
+        std::vector<HistChunk> rc;
+        hist_chunks_for(0, PNode{0, (uint32_t)n_}, true, rc);
+        n_root_chunks_ = (uint32_t)rc.size();
+        d_root_chunks_.alloc(std::max<size_t>(1, rc.size()));
+        BST_CK(cudaMemcpy(d_root_chunks_.p, rc.data(), sizeof(HistChunk) * rc.size(), cudaMemcpyHostToDevice));
+        const ScanNode rs{0, (uint32_t)n_, 0u, 0u, 0, 0};
+        d_root_scan_.alloc(1);
+        BST_CK(cudaMemcpy(d_root_scan_.p, &rs, sizeof(rs), cudaMemcpyHostToDevice));
+        BST_CK(cudaMallocHost(&h_btree_, sizeof(BTreeNode) * max_tnodes_));
+        BST_CK(cudaMallocHost(&h_bstate_, sizeof(BState)));
+        bd_.state = d_bstate_.p;
+        bd_.front[0] = d_front_[0].p;
+        bd_.front[1] = d_front_[1].p;
+        bd_.exp = d_bexp_.p;
+        bd_.tree = d_btree_.p;
+        bd_.leaves = d_bleaves_.p;
+        bd_.pworks = d_pworks_.p;
+        bd_.cursors = d_cursors_.p;
+        bd_.finish = d_finish_.p;
+        bd_.scan_nodes = d_scan_nodes_.p;
+        bd_.sums = d_sums_.p;
+        bd_.bcols = d_bcols_.p;
+        bd_.max_front = max_front;
+        bd_.max_tnodes = max_tnodes_;
+        graphs_.assign(G_, nullptr);
+        gtimers_.resize(G_);
+        graph_launches_.assign(G_, 0);
+        graph_hist_launches_.assign(G_, 0);
+    }
+
+    // The launch sequence of one tree for output o (captured into a graph).
+    void enqueue_tree(uint32_t o, Timer& tm, uint64_t& launches, uint64_t& hist_launches) {
+        const float2* gh = gh_.p + (size_t)o * n_;
+        const double* scale = scales_.p + 4 * (size_t)o;
+        float* pred = pred_.p + (size_t)o * n_;
+        const uint32_t g_wide = 148 * 8, g_hist = 148 * 3;
+        LeafParams lp{(double)cfg_.lambda, (double)cfg_.alpha, (double)cfg_.min_gain, cfg_.learning_rate, 0u};
+        launches = 0;
+        hist_launches = 0;
+        tm.begin(PH_OTHER);
+        launch_iota(ridx_.p, n_, st_);
+        launch_b_root(bd_, n_, st_);
+        BST_CK(cudaMemsetAsync(hist_.p, 0, sizeof(HBin) * slot_bins_, st_));
+        tm.end();
+        tm.begin(PH_HIST);
+        launch_hist_build(d_root_chunks_.p, n_root_chunks_, tiles_.p, n_tiles_, tile_smem_, ridx_.p, gh, scale,
+                          b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, hist_.p, slot_bins_, st_);
+        tm.end();
+        tm.begin(PH_SCAN);
+        launch_split_scan(d_root_scan_.p, 1, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p,
+                          d_node_tot_.p, st_);
+        launch_split_reduce(d_cand_.p, d_node_tot_.p, 1, n_cols_, last_wins_ ? 1 : 0, d_splits_.p, st_);
+        launch_b_root_set(bd_, d_splits_.p, st_);
+        tm.end();
+        launches += 6;
+        hist_launches += 1;
+        for (uint32_t d = 0; d < cfg_.max_depth; ++d) {
+            const int a = (int)(d & 1u);
+            const bool need_split = d + 1 < cfg_.max_depth;
+            tm.begin(PH_OTHER);
+            launch_b_decide(bd_, a, lp, scale, st_);
+            tm.end();
+            tm.begin(PH_PART);
+            launch_b_partition(bd_, ridx_.p, tmp_.p, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, g_wide, st_);
+            launch_b_copy(bd_, tmp_.p, ridx_.p, g_wide, st_);
+            tm.end();
+            tm.begin(PH_OTHER);
+            launch_b_children(bd_, a, need_split ? 1 : 0, st_);
+            tm.end();
+            launches += 4;
+            if (need_split) {
+                tm.begin(PH_OTHER);
+                launch_b_zero_right(bd_, hist_.p, slot_bins_, g_wide, st_);
+                tm.end();
+                tm.begin(PH_HIST);
+                launch_b_hist(bd_, tiles_.p, n_tiles_, tile_smem_, ridx_.p, gh, scale, b_.bins8.p, p_.s8,
+                              b_.bins16.p, p_.s16, hist_.p, slot_bins_, g_hist, st_);
+                tm.end();
+                tm.begin(PH_OTHER);
+                launch_b_finish(bd_, hist_.p, slot_bins_, p_.total_bins, g_wide, st_);
+                tm.end();
+                tm.begin(PH_SCAN);
+                launch_b_scan(bd_, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p,
+                              d_node_tot_.p, g_wide, st_);
+                launch_b_reduce(bd_, a ^ 1, d_cand_.p, d_node_tot_.p, n_cols_, last_wins_ ? 1 : 0, g_wide, st_);
+                tm.end();
+                launches += 5;
+                hist_launches += 1;
+            } else {
+                tm.begin(PH_OTHER);
+                BST_CK(cudaMemsetAsync(d_sums_.p, 0, sizeof(long long) * d_sums_.n, st_));
+                launch_b_sums(bd_, ridx_.p, gh, scale, g_wide, st_);
+                launch_b_children_sums(bd_, a ^ 1, st_);
+                tm.end();
+                launches += 2;
+            }
+        }
+        tm.begin(PH_LEAF);
+        launch_b_finalize(bd_, (int)(cfg_.max_depth & 1u), lp, scale, st_);
+        launch_b_leaf_update(bd_, ridx_.p, pred, cfg_.record_leaves ? row_leaf_.p : nullptr, g_wide, st_);
+        tm.end();
+        launches += 2;
+    }
+
+    HostTree grow_batched(uint32_t o) {
+        if (!graphs_[o]) {
+            gtimers_[o] = std::make_unique<Timer>();
+            gtimers_[o]->st = st_;
+            gtimers_[o]->reserve(16 + 20 * (size_t)cfg_.max_depth);
+            gtimers_[o]->in_graph = true;
+            BST_CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue_tree(o, *gtimers_[o], graph_launches_[o], graph_hist_launches_[o]);
+            } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(st_, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            cudaGraph_t g = nullptr;
+            BST_CK(cudaStreamEndCapture(st_, &g));
+            cudaGraphExec_t ex = nullptr;
+            const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+            cudaGraphDestroy(g);
+            BST_CK(e);
+            graphs_[o] = ex;
+        }
+        if (!whole_[0]) {
+            BST_CK(cudaEventCreate(&whole_[0]));
+            BST_CK(cudaEventCreate(&whole_[1]));
+        }
+        BST_CK(cudaEventRecord(whole_[0], st_));
+        BST_CK(cudaGraphLaunch(graphs_[o], st_));
+        BST_CK(cudaEventRecord(whole_[1], st_));
+        BST_CK(cudaMemcpyAsync(h_bstate_, d_bstate_.p, sizeof(BState), cudaMemcpyDeviceToHost, st_));
+        BST_CK(cudaMemcpyAsync(h_btree_, d_btree_.p, sizeof(BTreeNode) * max_tnodes_, cudaMemcpyDeviceToHost, st_));
+        HostTree t;
+        if (cfg_.record_leaves) {
+            t.row_leaf.resize(n_);
+            BST_CK(cudaMemcpyAsync(t.row_leaf.data(), row_leaf_.p, sizeof(uint32_t) * n_, cudaMemcpyDeviceToHost, st_));
+        }
+        BST_CK(cudaStreamSynchronize(st_));
+        BST_CK(cudaGetLastError());
+        if (!gtimers_[o]->collect_keep()) {
+            // per-phase timestamps unavailable: book the whole tree as "other"
+            float ms = 0;
+            BST_CK(cudaEventElapsedTime(&ms, whole_[0], whole_[1]));
+            timer_.acc[PH_OTHER] += ms;
+        }
+        for (int i = 1; i < 7; ++i) {
+            timer_.acc[i] += gtimers_[o]->acc[i];
+            gtimers_[o]->acc[i] = 0.0;
+        }
+        const uint64_t rows = h_bstate_->hist_rows;
+        m_.counters.launches += graph_launches_[o];
+        m_.counters.hist_launches += graph_hist_launches_[o];
+        m_.counters.hist_rows += rows;
+        m_.counters.hist_bytes += rows * ((uint64_t)p_.f8 + 2ull * p_.f16 + 12ull);
+        m_.counters.scan_launches += graph_hist_launches_[o];
+        // host tree from the device tree (grower.rs:576-650 threshold translation)
+        const uint32_t nt = h_bstate_->n_tnodes;
+        cat_nodes_.clear();
+        for (uint32_t i = 0; i < nt; ++i) t.alloc();
+        for (uint32_t i = 0; i < nt; ++i) {
+            const BTreeNode& b = h_btree_[i];
+            t.grad_sum[i] = b.G;
+            t.hess_sum[i] = b.H;
+            t.cover[i] = to_f32(b.H);
+            if (b.flags & 4u) {
+                t.is_leaf[i] = 1;
+                t.leaf[i] = b.leaf;
+                continue;
+            }
+            const uint32_t feat = p_.col_feature[b.col];
+            t.split_index[i] = feat;
+            t.left[i] = b.left;
+            t.right[i] = b.right;
+            t.gain[i] = b.gain;
+            if (!(b.flags & 2u)) {
+                t.threshold[i] = next_up(to_f32(p_.mappers[feat].bin_to_value(b.bin)));
+                t.default_left[i] = (b.flags & 1u) ? 1 : 0;
+                t.split_type[i] = 0;
+                t.split_bin[i] = b.bin;
+            } else {
+                t.threshold[i] = 0.0f;
+                t.default_left[i] = (b.flags & 1u) ? 0 : 1;
+                t.split_type[i] = 1;
+                cat_nodes_.push_back({i, bitset_words(b.cats)});
+            }
+        }
+        tree_ = std::move(t);
+        freeze_categories();
+        return std::move(tree_);
     }
 
     void build_tiles() {

@@ -258,20 +258,14 @@ __device__ __forceinline__ void hist_add(uint32_t* s, uint32_t S, uint32_t idx, 
     atomicAdd(&s[3 * S + idx], (uint32_t)(qh >> HIST_LO_BITS));
 }
 
-__global__ void __launch_bounds__(HIST_THREADS)
-k_hist_build(const HistChunk* __restrict__ chunks, const HistTile* __restrict__ tiles,
-             const uint32_t* __restrict__ ridx, const float2* __restrict__ gh,
-             const double* __restrict__ scale, const uint8_t* __restrict__ bins8, uint32_t s8,
-             const uint16_t* __restrict__ bins16, uint32_t s16, HBin* __restrict__ hist,
-             uint64_t slot_bins, uint32_t n_tiles, uint32_t S) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);  // [lo_g | hi_g | lo_h | hi_h] x S
-    __shared__ HistTile tile;
-    // tiles vary fastest so the blocks of one row chunk run together and
-    // share its grad/hess and row ids in L2
-    const HistChunk chunk = chunks[blockIdx.x / n_tiles];
-    if (threadIdx.x == 0) tile = tiles[blockIdx.x % n_tiles];
-    __syncthreads();
+// One (row chunk, column tile) item: zero the shared histogram, accumulate,
+// flush to the global histogram of chunk.slot. Block-uniform; `tile` is in
+// shared memory; returns with the shared histogram free for reuse.
+__device__ void hist_item(const HistChunk& chunk, const HistTile& tile, uint32_t* sm, uint32_t S,
+                          const uint32_t* __restrict__ ridx, const float2* __restrict__ gh,
+                          const double* __restrict__ scale, const uint8_t* __restrict__ bins8, uint32_t s8,
+                          const uint16_t* __restrict__ bins16, uint32_t s16, HBin* __restrict__ hist,
+                          uint64_t slot_bins) {
     for (uint32_t i = threadIdx.x; i < S; i += HIST_THREADS)  // S is a multiple of 4
         reinterpret_cast<uint4*>(sm)[i] = make_uint4(0, 0, 0, 0);
     __syncthreads();
@@ -336,6 +330,24 @@ k_hist_build(const HistChunk* __restrict__ chunks, const HistTile* __restrict__ 
             }
         }
     }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(HIST_THREADS)
+k_hist_build(const HistChunk* __restrict__ chunks, const HistTile* __restrict__ tiles,
+             const uint32_t* __restrict__ ridx, const float2* __restrict__ gh,
+             const double* __restrict__ scale, const uint8_t* __restrict__ bins8, uint32_t s8,
+             const uint16_t* __restrict__ bins16, uint32_t s16, HBin* __restrict__ hist,
+             uint64_t slot_bins, uint32_t n_tiles, uint32_t S) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);  // [lo_g | hi_g | lo_h | hi_h] x S
+    __shared__ HistTile tile;
+    // tiles vary fastest so the blocks of one row chunk run together and
+    // share its grad/hess and row ids in L2
+    const HistChunk chunk = chunks[blockIdx.x / n_tiles];
+    if (threadIdx.x == 0) tile = tiles[blockIdx.x % n_tiles];
+    __syncthreads();
+    hist_item(chunk, tile, sm, S, ridx, gh, scale, bins8, s8, bins16, s16, hist, slot_bins);
 }
 
 void launch_hist_build(const HistChunk* chunks, uint32_t n_chunks, const HistTile* tiles,
@@ -479,19 +491,15 @@ constexpr int SORT_N = 256;  // categorical columns with <= 256 bins
 
 }  // namespace
 
-__global__ void __launch_bounds__(SCAN_WARPS * 32)
-k_split_scan(const ScanNode* __restrict__ nodes, const ScanColumn* __restrict__ cols,
-             uint32_t n_cols, const HBin* __restrict__ hist, uint64_t slot_bins,
-             const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
-             long long* __restrict__ node_tot, uint32_t col_blocks) {
-    __shared__ double s_key[SCAN_WARPS][SORT_N];
-    __shared__ uint32_t s_cat[SCAN_WARPS][SORT_N];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t col = (blockIdx.x % col_blocks) * SCAN_WARPS + warp;
-    const uint32_t node = blockIdx.x / col_blocks;
-    if (col >= n_cols) return;
+// One warp: best split of column `col` of node `node` (the node's histogram
+// lives in slot nd.slot); writes cand[node * n_cols + col] and, for column 0,
+// the node totals. key / cat: this warp's SORT_N-entry shared scratch.
+__device__ void scan_item(const ScanNode nd, uint32_t node, uint32_t col, const ScanColumn* __restrict__ cols,
+                          uint32_t n_cols, const HBin* __restrict__ hist, uint64_t slot_bins,
+                          const double* __restrict__ scale, const GainParamsDev& gp, ColCand* __restrict__ cand,
+                          long long* __restrict__ node_tot, double* key, uint32_t* cat) {
+    const int lane = threadIdx.x & 31;
     const ScanColumn cm = cols[col];
-    const ScanNode nd = nodes[node];
     const HBin* h = hist + (size_t)nd.slot * slot_bins + cm.hist_off;
     const double ig = scale[2], ih = scale[3];
     const uint32_t nb = cm.n_bins;
@@ -591,8 +599,6 @@ k_split_scan(const ScanNode* __restrict__ nodes, const ScanColumn* __restrict__ 
     } else if (nb > gp.max_onehot_cats && nb <= SORT_N) {
         // sorted partition (find.rs:511-573): categories with hess > 1e-10
         // ordered by -g/(h+1e-6) ascending, ties by category (stable sort)
-        double* key = s_key[warp];
-        uint32_t* cat = s_cat[warp];
         uint32_t m = 0;
         for (uint32_t base = 0; base < nb; base += 32) {
             const uint32_t c = base + lane;
@@ -683,6 +689,21 @@ k_split_scan(const ScanNode* __restrict__ nodes, const ScanColumn* __restrict__ 
         out->flags = best.gain > -INFINITY ? best.flags : 0u;
         for (int q = 0; q < 4; ++q) out->cats[q] = cats[q];
     }
+}
+
+__global__ void __launch_bounds__(SCAN_WARPS * 32)
+k_split_scan(const ScanNode* __restrict__ nodes, const ScanColumn* __restrict__ cols,
+             uint32_t n_cols, const HBin* __restrict__ hist, uint64_t slot_bins,
+             const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
+             long long* __restrict__ node_tot, uint32_t col_blocks) {
+    __shared__ double s_key[SCAN_WARPS][SORT_N];
+    __shared__ uint32_t s_cat[SCAN_WARPS][SORT_N];
+    const int warp = threadIdx.x >> 5;
+    const uint32_t col = (blockIdx.x % col_blocks) * SCAN_WARPS + warp;
+    const uint32_t node = blockIdx.x / col_blocks;
+    if (col >= n_cols) return;
+    scan_item(nodes[node], node, col, cols, n_cols, hist, slot_bins, scale, gp, cand, node_tot, s_key[warp],
+              s_cat[warp]);
 }
 
 void launch_split_scan(const ScanNode* nodes, uint32_t n_nodes, const ScanColumn* cols,
@@ -874,6 +895,692 @@ void launch_leaf_update(const LeafSeg* leaves, uint32_t n_leaves, const uint32_t
     uint64_t blocks = (n + 255) / 256;
     if (blocks > 148ull * 16) blocks = 148ull * 16;
     k_leaf_update<<<(unsigned)blocks, 256, 0, st>>>(leaves, n_leaves, ridx, n, pred, row_leaf);
+}
+
+// ============================================================================
+// Device-side depth-wise growth: the level loop of TreeGrower::grow
+// (training/gbdt/grower.rs:288-337, expansion.rs:137-196) as a fixed launch
+// sequence whose sizes live in device memory (BState), so one CUDA graph
+// replays a whole tree.
+// ============================================================================
+
+namespace {
+
+// Block-wide exclusive scan (blockDim.x <= 1024); *total gets the block sum.
+__device__ uint32_t block_excl_scan(uint32_t v, uint32_t* sh, uint32_t* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    uint32_t x = v;
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(FULL, x, d);
+        if (lane >= d) x += t;
+    }
+    if (lane == 31) sh[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t y = lane < nw ? sh[lane] : 0u;
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t t = __shfl_up_sync(FULL, y, d);
+            if (lane >= d) y += t;
+        }
+        if (lane < nw) sh[lane] = y;
+    }
+    __syncthreads();
+    const uint32_t r = (warp ? sh[warp - 1] : 0u) + x - v;
+    *total = sh[nw - 1];
+    __syncthreads();
+    return r;
+}
+
+// GainParams::compute_leaf_weight (gain.rs:151-168) x learning rate (mutable_tree.rs:258).
+__device__ float leaf_value_dev(long long G, long long H, const double* scale, const LeafParams& lp) {
+    const double g = (double)G * scale[2], h = (double)H * scale[3];
+    float w;
+    if (lp.alpha == 0.0) {
+        w = __double2float_rn(-g / (h + lp.lambda));
+    } else {
+        const double ag = fabs(g);
+        if (ag <= lp.alpha) {
+            w = 0.0f;
+        } else {
+            const double sign = g > 0.0 ? -1.0 : 1.0;
+            w = __double2float_rn(sign * (ag - lp.alpha) / (h + lp.lambda));
+        }
+    }
+    return w * lp.learning_rate;
+}
+
+// last index i in [0, n) with key(i) <= c (key non-decreasing, key(0) <= c)
+template <class F>
+__device__ __forceinline__ uint32_t last_le(uint32_t n, uint32_t c, F key) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (key(mid) <= c)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ bool goes_left(const PartWork& w, uint32_t bin) {
+    if ((w.flags & 2u) && bin == w.default_bin) return (w.flags & 1u) != 0;
+    if (w.flags & 4u) return bin < 256 && ((w.cats[bin >> 6] >> (bin & 63)) & 1ull);
+    return bin <= w.thr_bin;
+}
+
+__device__ void write_leaf(BTreeNode& t, long long G, long long H, const double* scale, float v) {
+    t.col = 0;
+    t.bin = 0;
+    t.flags = 4u;
+    t.left = 0;
+    t.right = 0;
+    t.gain = 0.0f;
+    t.leaf = v;
+    t.G = (double)G * scale[2];
+    t.H = (double)H * scale[3];
+    t.cats[0] = t.cats[1] = t.cats[2] = t.cats[3] = 0ull;
+}
+
+}  // namespace
+
+__global__ void k_b_root(BDev d, uint64_t n) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    BNode r;
+    r.pnode = 0;
+    r.tnode = 0;
+    r.begin = 0;
+    r.count = (uint32_t)n;
+    r.G = 0;
+    r.H = 0;
+    r.split.gain = -INFINITY;
+    r.split.col = 0;
+    r.split.bin = 0;
+    r.split.flags = 0;
+    r.split.cats[0] = r.split.cats[1] = r.split.cats[2] = r.split.cats[3] = 0ull;
+    r.split.tot_g = 0;
+    r.split.tot_h = 0;
+    d.front[0][0] = r;
+    BState s;
+    s.n_front = 1;
+    s.n_exp = 0;
+    s.n_pnodes = 1;
+    s.n_tnodes = 1;
+    s.part_chunks = 0;
+    s.hist_chunks = 0;
+    s.n_leaves = 0;
+    s.leaf_chunks = 0;
+    s.first_right = 1;
+    s.pad = 0;
+    s.hist_rows = n;
+    s.pad2[0] = s.pad2[1] = s.pad2[2] = s.pad2[3] = 0;
+    *d.state = s;
+}
+
+void launch_b_root(const BDev& d, uint64_t n, cudaStream_t st) { k_b_root<<<1, 32, 0, st>>>(d, n); }
+
+__global__ void k_b_hist(BDev d, const HistTile* __restrict__ tiles, uint32_t n_tiles, uint32_t S,
+                         const uint32_t* __restrict__ ridx, const float2* __restrict__ gh,
+                         const double* __restrict__ scale, const uint8_t* __restrict__ bins8, uint32_t s8,
+                         const uint16_t* __restrict__ bins16, uint32_t s16, HBin* __restrict__ hist,
+                         uint64_t slot_bins);
+
+void init_kernel_attributes() {
+    cudaFuncSetAttribute(k_hist_build, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_b_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_bin_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+}
+
+__global__ void k_b_root_set(BDev d, const NodeSplit* __restrict__ rs) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const NodeSplit s = *rs;
+    BNode& r = d.front[0][0];
+    r.split = s;
+    r.G = s.tot_g;
+    r.H = s.tot_h;
+}
+
+void launch_b_root_set(const BDev& d, const NodeSplit* rs, cudaStream_t st) { k_b_root_set<<<1, 32, 0, st>>>(d, rs); }
+
+// Expansion decisions of one level (grower.rs:353-372, 530-539): leaves for
+// the rest, right-child ids in frontier order (partition.rs:375), tree nodes
+// in allocation order (mutable_tree.rs:105-164), partition work lists.
+__global__ void __launch_bounds__(1024) k_b_decide(BDev d, int a, LeafParams lp, const double* __restrict__ scale) {
+    __shared__ uint32_t sh[33];
+    __shared__ uint32_t base_exp, base_leaf, base_chunk, first_right, tn0, nf;
+    BState* s = d.state;
+    if (threadIdx.x == 0) {
+        nf = s->n_front;
+        base_exp = 0;
+        base_leaf = s->n_leaves;
+        base_chunk = 0;
+        first_right = s->n_pnodes;
+        tn0 = s->n_tnodes;
+    }
+    __syncthreads();
+    const BNode* A = d.front[a];
+    for (uint32_t i0 = 0; i0 < nf; i0 += blockDim.x) {
+        const uint32_t i = i0 + threadIdx.x;
+        const bool valid = i < nf;
+        BNode nd;
+        if (valid) nd = A[i];
+        const bool ex = valid && (nd.split.flags & 4u) && nd.split.gain > -INFINITY &&
+                        !((double)nd.split.gain <= lp.min_gain);
+        uint32_t te, tl, tc;
+        const uint32_t je = block_excl_scan(ex ? 1u : 0u, sh, &te);
+        const uint32_t jl = block_excl_scan((valid && !ex) ? 1u : 0u, sh, &tl);
+        const uint32_t nch = ex ? (nd.count + B_PART_CHUNK - 1) / B_PART_CHUNK : 0u;
+        const uint32_t jc = block_excl_scan(nch, sh, &tc);
+        if (valid && !ex) {
+            const float v = leaf_value_dev(nd.G, nd.H, scale, lp);
+            write_leaf(d.tree[nd.tnode], nd.G, nd.H, scale, v);
+            BLeaf lf;
+            lf.begin = nd.begin;
+            lf.count = nd.count;
+            lf.value = v;
+            lf.tnode = nd.tnode;
+            lf.chunk_off = 0;
+            lf.pad = 0;
+            d.leaves[base_leaf + jl] = lf;
+        }
+        if (ex) {
+            const uint32_t j = base_exp + je;
+            const uint32_t tla = tn0 + 2 * j, tra = tn0 + 2 * j + 1;
+            const bool cat = (nd.split.flags & 2u) != 0;
+            const uint32_t col = nd.split.col;
+            const BColumn bc = d.bcols[col];
+            BTreeNode t;
+            t.col = col;
+            t.bin = nd.split.bin;
+            t.flags = (nd.split.flags & 1u) | (cat ? 2u : 0u);
+            t.left = tla;
+            t.right = tra;
+            t.gain = nd.split.gain;
+            t.leaf = 0.0f;
+            t.G = (double)nd.G * scale[2];
+            t.H = (double)nd.H * scale[3];
+            for (int q = 0; q < 4; ++q) t.cats[q] = nd.split.cats[q];
+            d.tree[nd.tnode] = t;
+            BExp e;
+            e.front = i;
+            e.right_pnode = first_right + j;
+            e.tl = cat ? tra : tla;  // categorical: training-left rows go to the stored right child
+            e.tr = cat ? tla : tra;
+            e.lc = e.rc = e.small_begin = e.small_count = 0;
+            e.part_off = base_chunk + jc;
+            e.hist_off = 0;
+            e.pad0 = e.pad1 = 0;
+            d.exp[j] = e;
+            PartWork w;
+            w.begin = nd.begin;
+            w.count = nd.count;
+            w.matrix = bc.matrix;
+            w.pos = bc.pos;
+            w.thr_bin = nd.split.bin;
+            w.flags = (nd.split.flags & 1u) | (bc.has_missing ? 2u : 0u) | (cat ? 4u : 0u);
+            w.default_bin = bc.default_bin;
+            w.pad = 0;
+            for (int q = 0; q < 4; ++q) w.cats[q] = nd.split.cats[q];
+            d.pworks[j] = w;
+            d.cursors[2 * j] = nd.begin;
+            d.cursors[2 * j + 1] = nd.begin + nd.count;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            base_exp += te;
+            base_leaf += tl;
+            base_chunk += tc;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        s->n_exp = base_exp;
+        s->n_leaves = base_leaf;
+        s->part_chunks = base_chunk;
+        s->first_right = first_right;
+        s->n_pnodes = first_right + base_exp;
+        s->n_tnodes = tn0 + 2 * base_exp;
+    }
+}
+
+void launch_b_decide(const BDev& d, int a, LeafParams lp, const double* scale, cudaStream_t st) {
+    k_b_decide<<<1, 1024, 0, st>>>(d, a, lp, scale);
+}
+
+// Partition of every expanding node (partition.rs:296-382); 2048-row chunks,
+// loads issued ahead of the ballots for memory-level parallelism.
+__global__ void __launch_bounds__(256)
+k_b_partition(BDev d, const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp,
+              const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16) {
+    constexpr int PER = B_PART_CHUNK / 256;
+    const uint32_t total = d.state->part_chunks, n_exp = d.state->n_exp;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+        const uint32_t j = last_le(n_exp, c, [&](uint32_t k) { return d.exp[k].part_off; });
+        const PartWork w = d.pworks[j];
+        const uint32_t start = w.begin + (c - d.exp[j].part_off) * B_PART_CHUNK;
+        const uint32_t end = w.begin + w.count;
+        const uint32_t len = min(B_PART_CHUNK, end - start);
+        uint32_t rows[PER], bins[PER];
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const uint32_t i = k * 256 + threadIdx.x;
+            rows[k] = i < len ? ridx[start + i] : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const uint32_t i = k * 256 + threadIdx.x;
+            bins[k] = 0u;
+            if (i < len)
+                bins[k] = w.matrix == 0 ? (uint32_t)bins8[(size_t)rows[k] * s8 + w.pos]
+                                        : (uint32_t)bins16[(size_t)rows[k] * s16 + w.pos];
+        }
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const uint32_t i = k * 256 + threadIdx.x;
+            const bool ok = i < len;
+            const bool left = ok && goes_left(w, bins[k]);
+            const unsigned act = __ballot_sync(FULL, ok);
+            const unsigned lm = __ballot_sync(FULL, left);
+            const unsigned rm = act & ~lm;
+            unsigned lbase = 0, rbase = 0;
+            if (lane == 0) {
+                if (lm) lbase = atomicAdd(&d.cursors[2 * j], (unsigned)__popc(lm));
+                if (rm) rbase = atomicSub(&d.cursors[2 * j + 1], (unsigned)__popc(rm)) - (unsigned)__popc(rm);
+            }
+            lbase = __shfl_sync(FULL, lbase, 0);
+            rbase = __shfl_sync(FULL, rbase, 0);
+            if (ok) {
+                if (left)
+                    tmp[lbase + __popc(lm & lt)] = rows[k];
+                else
+                    tmp[rbase + __popc(rm & lt)] = rows[k];
+            }
+        }
+    }
+}
+
+void launch_b_partition(const BDev& d, const uint32_t* ridx, uint32_t* tmp, const uint8_t* bins8, uint32_t s8,
+                        const uint16_t* bins16, uint32_t s16, uint32_t grid, cudaStream_t st) {
+    k_b_partition<<<grid, 256, 0, st>>>(d, ridx, tmp, bins8, s8, bins16, s16);
+}
+
+__global__ void k_b_copy(BDev d, const uint32_t* __restrict__ tmp, uint32_t* __restrict__ ridx) {
+    const uint32_t total = d.state->part_chunks, n_exp = d.state->n_exp;
+    for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+        const uint32_t j = last_le(n_exp, c, [&](uint32_t k) { return d.exp[k].part_off; });
+        const PartWork w = d.pworks[j];
+        const uint32_t start = w.begin + (c - d.exp[j].part_off) * B_PART_CHUNK;
+        const uint32_t len = min(B_PART_CHUNK, w.begin + w.count - start);
+        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) ridx[start + i] = tmp[start + i];
+    }
+}
+
+void launch_b_copy(const BDev& d, const uint32_t* tmp, uint32_t* ridx, uint32_t grid, cudaStream_t st) {
+    k_b_copy<<<grid, 256, 0, st>>>(d, tmp, ridx);
+}
+
+// Children of every split: ranges from the partition cursors, smaller child
+// (grower.rs:398-402), next frontier in (left, right) order, histogram or
+// node-sum work over the smaller children.
+__global__ void __launch_bounds__(1024) k_b_children(BDev d, int a, int need_split) {
+    __shared__ uint32_t sh[33];
+    __shared__ uint32_t base, n_exp;
+    __shared__ unsigned long long rows;
+    BState* s = d.state;
+    if (threadIdx.x == 0) {
+        n_exp = s->n_exp;
+        base = 0;
+        rows = 0ull;
+    }
+    __syncthreads();
+    const BNode* A = d.front[a];
+    BNode* B = d.front[a ^ 1];
+    for (uint32_t j0 = 0; j0 < n_exp; j0 += blockDim.x) {
+        const uint32_t j = j0 + threadIdx.x;
+        const bool valid = j < n_exp;
+        uint32_t nch = 0;
+        if (valid) {
+            BExp e = d.exp[j];
+            const BNode nd = A[e.front];
+            const uint32_t lc = d.cursors[2 * j] - nd.begin, rc = nd.count - lc;
+            const bool left_small = lc <= rc;
+            e.lc = lc;
+            e.rc = rc;
+            e.small_begin = left_small ? nd.begin : nd.begin + lc;
+            e.small_count = left_small ? lc : rc;
+            BNode l, r;
+            l.pnode = nd.pnode;
+            l.tnode = e.tl;
+            l.begin = nd.begin;
+            l.count = lc;
+            r.pnode = e.right_pnode;
+            r.tnode = e.tr;
+            r.begin = nd.begin + lc;
+            r.count = rc;
+            l.G = l.H = r.G = r.H = 0;
+            l.split.gain = r.split.gain = -INFINITY;
+            l.split.col = r.split.col = 0;
+            l.split.bin = r.split.bin = 0;
+            l.split.flags = r.split.flags = 0;
+            for (int q = 0; q < 4; ++q) l.split.cats[q] = r.split.cats[q] = 0ull;
+            l.split.tot_g = l.split.tot_h = r.split.tot_g = r.split.tot_h = 0;
+            B[2 * j] = l;
+            B[2 * j + 1] = r;
+            d.finish[j] = FinishWork{nd.pnode, e.right_pnode, left_small ? 1u : 0u, 0u};
+            d.scan_nodes[2 * j] = ScanNode{nd.pnode, lc, 0u, 0u, 0, 0};
+            d.scan_nodes[2 * j + 1] = ScanNode{e.right_pnode, rc, 0u, 0u, 0, 0};
+            nch = (e.small_count + HIST_CHUNK_MAX - 1) / HIST_CHUNK_MAX;
+            d.exp[j] = e;
+            if (need_split) atomicAdd(&rows, (unsigned long long)e.small_count);
+        }
+        uint32_t tc;
+        const uint32_t jc = block_excl_scan(nch, sh, &tc);
+        if (valid) d.exp[j].hist_off = base + jc;
+        __syncthreads();
+        if (threadIdx.x == 0) base += tc;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        s->hist_chunks = base;
+        s->n_front = 2 * n_exp;
+        s->hist_rows += rows;
+    }
+}
+
+void launch_b_children(const BDev& d, int a, int need_split, cudaStream_t st) {
+    k_b_children<<<1, 1024, 0, st>>>(d, a, need_split);
+}
+
+__global__ void k_b_zero_right(BDev d, HBin* __restrict__ hist, uint64_t slot_bins) {
+    const uint64_t n = (uint64_t)d.state->n_exp * slot_bins;
+    uint4* p = reinterpret_cast<uint4*>(hist + (uint64_t)d.state->first_right * slot_bins);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        p[i] = make_uint4(0, 0, 0, 0);
+}
+
+void launch_b_zero_right(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t grid, cudaStream_t st) {
+    k_b_zero_right<<<grid, 256, 0, st>>>(d, hist, slot_bins);
+}
+
+// Histograms of all smaller children of the level (one persistent launch).
+__global__ void __launch_bounds__(HIST_THREADS)
+k_b_hist(BDev d, const HistTile* __restrict__ tiles, uint32_t n_tiles, uint32_t S, const uint32_t* __restrict__ ridx,
+         const float2* __restrict__ gh, const double* __restrict__ scale, const uint8_t* __restrict__ bins8,
+         uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16, HBin* __restrict__ hist, uint64_t slot_bins) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);
+    __shared__ HistTile tile;
+    const uint32_t n_exp = d.state->n_exp;
+    const uint64_t items = (uint64_t)d.state->hist_chunks * n_tiles;
+    for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
+        const uint32_t c = (uint32_t)(it / n_tiles), t = (uint32_t)(it % n_tiles);
+        const uint32_t j = last_le(n_exp, c, [&](uint32_t k) { return d.exp[k].hist_off; });
+        const BExp e = d.exp[j];
+        const uint32_t start = e.small_begin + (c - e.hist_off) * HIST_CHUNK_MAX;
+        HistChunk ch;
+        ch.slot = e.right_pnode;
+        ch.begin = start;
+        ch.count = min((uint32_t)HIST_CHUNK_MAX, e.small_begin + e.small_count - start);
+        ch.flags = 0u;
+        if (threadIdx.x == 0) tile = tiles[t];
+        __syncthreads();
+        hist_item(ch, tile, sm, S, ridx, gh, scale, bins8, s8, bins16, s16, hist, slot_bins);
+    }
+}
+
+void launch_b_hist(const BDev& d, const HistTile* tiles, uint32_t n_tiles, uint32_t max_smem_bins,
+                   const uint32_t* ridx, const float2* gh, const double* scale, const uint8_t* bins8,
+                   uint32_t s8, const uint16_t* bins16, uint32_t s16, HBin* hist, uint64_t slot_bins,
+                   uint32_t grid, cudaStream_t st) {
+    if (n_tiles == 0) return;
+    const uint32_t S = (max_smem_bins + 3u) & ~3u;
+    const size_t smem = (size_t)S * 4u * sizeof(uint32_t);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_b_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr_set = true;
+    }
+    k_b_hist<<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gh, scale, bins8, s8, bins16, s16, hist,
+                                                slot_bins);
+}
+
+__global__ void k_b_finish(BDev d, HBin* __restrict__ hist, uint64_t slot_bins, uint32_t total_bins) {
+    const uint64_t n = (uint64_t)d.state->n_exp * total_bins;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = (uint32_t)(i / total_bins), b = (uint32_t)(i % total_bins);
+        const FinishWork w = d.finish[j];
+        HBin* L = hist + (size_t)w.left * slot_bins + b;
+        HBin* R = hist + (size_t)w.right * slot_bins + b;
+        const HBin p = *L, s = *R;
+        HBin df;
+        df.g = p.g - s.g;
+        df.h = p.h - s.h;
+        if (w.flags & 1u) {
+            *L = s;
+            *R = df;
+        } else {
+            *L = df;
+        }
+    }
+}
+
+void launch_b_finish(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t total_bins, uint32_t grid,
+                     cudaStream_t st) {
+    k_b_finish<<<grid, 256, 0, st>>>(d, hist, slot_bins, total_bins);
+}
+
+__global__ void __launch_bounds__(SCAN_WARPS * 32)
+k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HBin* __restrict__ hist,
+         uint64_t slot_bins, const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
+         long long* __restrict__ node_tot) {
+    __shared__ double s_key[SCAN_WARPS][SORT_N];
+    __shared__ uint32_t s_cat[SCAN_WARPS][SORT_N];
+    const int warp = threadIdx.x >> 5;
+    const uint32_t col_blocks = (n_cols + SCAN_WARPS - 1) / SCAN_WARPS;
+    const uint64_t items = (uint64_t)2 * d.state->n_exp * col_blocks;
+    for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
+        const uint32_t node = (uint32_t)(it / col_blocks);
+        const uint32_t col = (uint32_t)(it % col_blocks) * SCAN_WARPS + warp;
+        if (col < n_cols)
+            scan_item(d.scan_nodes[node], node, col, cols, n_cols, hist, slot_bins, scale, gp, cand, node_tot,
+                      s_key[warp], s_cat[warp]);
+    }
+}
+
+void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const HBin* hist, uint64_t slot_bins,
+                   const double* scale, GainParamsDev gp, ColCand* cand, long long* node_tot, uint32_t grid,
+                   cudaStream_t st) {
+    if (n_cols == 0) return;
+    k_b_scan<<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, hist, slot_bins, scale, gp, cand, node_tot);
+}
+
+// Reduction over columns (find.rs:180-270) straight into the next frontier.
+__global__ void k_b_reduce(BDev d, int b, const ColCand* __restrict__ cand, const long long* __restrict__ node_tot,
+                           uint32_t n_cols, int last_wins) {
+    const uint32_t n_nodes = 2 * d.state->n_exp;
+    BNode* B = d.front[b];
+    const int lane = threadIdx.x;
+    for (uint32_t node = blockIdx.x; node < n_nodes; node += gridDim.x) {
+        float bg = -INFINITY;
+        uint32_t bc = 0xFFFFFFFFu;
+        const ColCand* c = cand + (size_t)node * n_cols;
+        for (uint32_t i = lane; i < n_cols; i += 32) {
+            const float g = c[i].gain;
+            if (!(g > -INFINITY)) continue;
+            if (bc == 0xFFFFFFFFu || g > bg || (last_wins && g == bg)) {
+                bg = g;
+                bc = i;
+            }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            const float og = __shfl_xor_sync(FULL, bg, off);
+            const uint32_t oc = __shfl_xor_sync(FULL, bc, off);
+            bool take;
+            if (oc == 0xFFFFFFFFu)
+                take = false;
+            else if (bc == 0xFFFFFFFFu)
+                take = true;
+            else if (og != bg)
+                take = og > bg;
+            else
+                take = last_wins ? oc > bc : oc < bc;
+            if (take) {
+                bg = og;
+                bc = oc;
+            }
+        }
+        if (lane == 0) {
+            NodeSplit s;
+            s.tot_g = node_tot[2 * node];
+            s.tot_h = node_tot[2 * node + 1];
+            if (bc == 0xFFFFFFFFu) {
+                s.gain = -INFINITY;
+                s.col = 0;
+                s.bin = 0;
+                s.flags = 0;
+                s.cats[0] = s.cats[1] = s.cats[2] = s.cats[3] = 0ull;
+            } else {
+                const ColCand& w = c[bc];
+                s.gain = w.gain;
+                s.col = bc;
+                s.bin = w.bin;
+                s.flags = (w.flags & 3u) | 4u;
+                for (int q = 0; q < 4; ++q) s.cats[q] = w.cats[q];
+            }
+            B[node].split = s;
+            B[node].G = s.tot_g;
+            B[node].H = s.tot_h;
+        }
+    }
+}
+
+void launch_b_reduce(const BDev& d, int b, const ColCand* cand, const long long* node_tot, uint32_t n_cols,
+                     int last_wins, uint32_t grid, cudaStream_t st) {
+    k_b_reduce<<<grid, 32, 0, st>>>(d, b, cand, node_tot, n_cols, last_wins);
+}
+
+// Node sums of the smaller children when the children are not split further.
+__global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, const float2* __restrict__ gh,
+                         const double* __restrict__ scale) {
+    const uint32_t total = d.state->hist_chunks, n_exp = d.state->n_exp;
+    const double sg = scale[0], sh = scale[1];
+    for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+        const uint32_t j = last_le(n_exp, c, [&](uint32_t k) { return d.exp[k].hist_off; });
+        const BExp e = d.exp[j];
+        const uint32_t start = e.small_begin + (c - e.hist_off) * HIST_CHUNK_MAX;
+        const uint32_t len = min((uint32_t)HIST_CHUNK_MAX, e.small_begin + e.small_count - start);
+        long long ag = 0, ah = 0;
+        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+            const float2 v = gh[ridx[start + i]];
+            ag += quantize(v.x, sg);
+            ah += quantize(v.y, sh);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            ag += __shfl_xor_sync(FULL, ag, o);
+            ah += __shfl_xor_sync(FULL, ah, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(&d.sums[2 * j]), (unsigned long long)ag);
+            atomicAdd(reinterpret_cast<unsigned long long*>(&d.sums[2 * j + 1]), (unsigned long long)ah);
+        }
+    }
+}
+
+void launch_b_sums(const BDev& d, const uint32_t* ridx, const float2* gh, const double* scale, uint32_t grid,
+                   cudaStream_t st) {
+    k_b_sums<<<grid, 256, 0, st>>>(d, ridx, gh, scale);
+}
+
+__global__ void k_b_children_sums(BDev d, int b) {
+    const uint32_t n_exp = d.state->n_exp;
+    const BNode* A = d.front[b ^ 1];
+    BNode* B = d.front[b];
+    for (uint32_t j = threadIdx.x; j < n_exp; j += blockDim.x) {
+        const BExp e = d.exp[j];
+        const BNode p = A[e.front];
+        const long long sg = d.sums[2 * j], sh = d.sums[2 * j + 1];
+        const bool left_small = e.lc <= e.rc;
+        const long long lg = left_small ? sg : p.G - sg, lh = left_small ? sh : p.H - sh;
+        B[2 * j].G = lg;
+        B[2 * j].H = lh;
+        B[2 * j + 1].G = p.G - lg;
+        B[2 * j + 1].H = p.H - lh;
+    }
+}
+
+void launch_b_children_sums(const BDev& d, int b, cudaStream_t st) { k_b_children_sums<<<1, 1024, 0, st>>>(d, b); }
+
+// Remaining frontier -> leaves (grower.rs:484-514); leaf row chunks.
+__global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams lp, const double* __restrict__ scale) {
+    __shared__ uint32_t sh[33];
+    __shared__ uint32_t base, nf, n0;
+    BState* s = d.state;
+    if (threadIdx.x == 0) {
+        nf = s->n_front;
+        n0 = s->n_leaves;
+        base = 0;
+    }
+    __syncthreads();
+    const BNode* A = d.front[a];
+    for (uint32_t i = threadIdx.x; i < nf; i += blockDim.x) {
+        const BNode nd = A[i];
+        const float v = leaf_value_dev(nd.G, nd.H, scale, lp);
+        write_leaf(d.tree[nd.tnode], nd.G, nd.H, scale, v);
+        BLeaf lf;
+        lf.begin = nd.begin;
+        lf.count = nd.count;
+        lf.value = v;
+        lf.tnode = nd.tnode;
+        lf.chunk_off = 0;
+        lf.pad = 0;
+        d.leaves[n0 + i] = lf;
+    }
+    __syncthreads();
+    const uint32_t nl = n0 + nf;
+    for (uint32_t l0 = 0; l0 < nl; l0 += blockDim.x) {
+        const uint32_t l = l0 + threadIdx.x;
+        const uint32_t nch = l < nl ? (d.leaves[l].count + B_LEAF_CHUNK - 1) / B_LEAF_CHUNK : 0u;
+        uint32_t tc;
+        const uint32_t jc = block_excl_scan(nch, sh, &tc);
+        if (l < nl) d.leaves[l].chunk_off = base + jc;
+        __syncthreads();
+        if (threadIdx.x == 0) base += tc;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        s->n_leaves = nl;
+        s->leaf_chunks = base;
+        s->n_front = 0;
+    }
+}
+
+void launch_b_finalize(const BDev& d, int a, LeafParams lp, const double* scale, cudaStream_t st) {
+    k_b_finalize<<<1, 1024, 0, st>>>(d, a, lp, scale);
+}
+
+// pred[row] += leaf value over the final partition (grower.rs:208-219).
+__global__ void k_b_leaf_update(BDev d, const uint32_t* __restrict__ ridx, float* __restrict__ pred,
+                                uint32_t* __restrict__ row_leaf) {
+    const uint32_t total = d.state->leaf_chunks, nl = d.state->n_leaves;
+    for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+        const uint32_t l = last_le(nl, c, [&](uint32_t k) { return d.leaves[k].chunk_off; });
+        const BLeaf lf = d.leaves[l];
+        const uint32_t start = lf.begin + (c - lf.chunk_off) * B_LEAF_CHUNK;
+        const uint32_t len = min(B_LEAF_CHUNK, lf.begin + lf.count - start);
+        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+            const uint32_t row = ridx[start + i];
+            pred[row] = pred[row] + lf.value;
+            if (row_leaf) row_leaf[row] = lf.tnode;
+        }
+    }
+}
+
+void launch_b_leaf_update(const BDev& d, const uint32_t* ridx, float* pred, uint32_t* row_leaf, uint32_t grid,
+                          cudaStream_t st) {
+    k_b_leaf_update<<<grid, 256, 0, st>>>(d, ridx, pred, row_leaf);
 }
 
 // ============================================================================

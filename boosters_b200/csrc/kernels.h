@@ -165,6 +165,95 @@ struct LeafSeg {
 void launch_leaf_update(const LeafSeg* leaves, uint32_t n_leaves, const uint32_t* ridx,
                         uint64_t n, float* pred, uint32_t* row_leaf, cudaStream_t st);
 
+// ---- device-side depth-wise growth (one CUDA graph per tree) -----------------
+// The host launches a fixed sequence of kernels per tree; every data-dependent
+// size (frontier, expanding nodes, row chunks) is read from device memory, so
+// the sequence is captured once and replayed for every tree.
+struct BColumn {  // per effective column, for decisions and the partition
+    uint32_t matrix, pos, has_missing, default_bin;
+};
+struct BNode {  // frontier entry
+    uint32_t pnode, tnode, begin, count;
+    long long G, H;
+    NodeSplit split;
+};
+struct BTreeNode {  // tree node as grown (training semantics)
+    uint32_t col, bin, flags;  // flags: bit0 default_left, bit1 categorical, bit2 leaf
+    uint32_t left, right;      // children tree nodes in allocation order
+    float gain, leaf;          // leaf: value x learning rate
+    double G, H;
+    unsigned long long cats[4];
+};
+struct BExp {  // an expanding node of the current level
+    uint32_t front, right_pnode, tl, tr;  // tl/tr: tree nodes of the training-left/right child
+    uint32_t lc, rc, small_begin, small_count;
+    uint32_t part_off, hist_off, pad0, pad1;
+};
+struct BLeaf {
+    uint32_t begin, count;
+    float value;
+    uint32_t tnode;
+    uint32_t chunk_off, pad;
+};
+struct BState {
+    uint32_t n_front, n_exp, n_pnodes, n_tnodes;
+    uint32_t part_chunks, hist_chunks, n_leaves, leaf_chunks;
+    uint32_t first_right, pad;
+    unsigned long long hist_rows;  // rows visited by histogram builds of this tree
+    uint32_t pad2[4];
+};
+struct LeafParams {
+    double lambda, alpha, min_gain;
+    float learning_rate;
+    uint32_t pad;
+};
+struct BDev {  // device buffers of the level loop
+    BState* state;
+    BNode* front[2];
+    BExp* exp;
+    BTreeNode* tree;
+    BLeaf* leaves;
+    PartWork* pworks;
+    unsigned* cursors;
+    FinishWork* finish;
+    ScanNode* scan_nodes;
+    long long* sums;  // [max_exp][2]
+    const BColumn* bcols;
+    uint32_t max_front, max_tnodes;
+};
+constexpr uint32_t B_PART_CHUNK = 2048;
+constexpr uint32_t B_LEAF_CHUNK = 4096;
+
+// Raises the dynamic shared-memory limits of the kernels that need > 48 KiB
+// (call once per device before any stream capture).
+void init_kernel_attributes();
+void launch_b_root(const BDev& d, uint64_t n, cudaStream_t st);
+void launch_b_root_set(const BDev& d, const NodeSplit* root_split, cudaStream_t st);
+// level kernels; `a` is the index of the current frontier buffer
+void launch_b_decide(const BDev& d, int a, LeafParams lp, const double* scale, cudaStream_t st);
+void launch_b_partition(const BDev& d, const uint32_t* ridx, uint32_t* tmp, const uint8_t* bins8, uint32_t s8,
+                        const uint16_t* bins16, uint32_t s16, uint32_t grid, cudaStream_t st);
+void launch_b_copy(const BDev& d, const uint32_t* tmp, uint32_t* ridx, uint32_t grid, cudaStream_t st);
+void launch_b_children(const BDev& d, int a, int need_split, cudaStream_t st);
+void launch_b_zero_right(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t grid, cudaStream_t st);
+void launch_b_hist(const BDev& d, const HistTile* tiles, uint32_t n_tiles, uint32_t max_smem_bins,
+                   const uint32_t* ridx, const float2* gh, const double* scale, const uint8_t* bins8,
+                   uint32_t s8, const uint16_t* bins16, uint32_t s16, HBin* hist, uint64_t slot_bins,
+                   uint32_t grid, cudaStream_t st);
+void launch_b_finish(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t total_bins, uint32_t grid,
+                     cudaStream_t st);
+void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const HBin* hist,
+                   uint64_t slot_bins, const double* scale, GainParamsDev gp, ColCand* cand,
+                   long long* node_tot, uint32_t grid, cudaStream_t st);
+void launch_b_reduce(const BDev& d, int b, const ColCand* cand, const long long* node_tot, uint32_t n_cols,
+                     int last_wins, uint32_t grid, cudaStream_t st);
+void launch_b_sums(const BDev& d, const uint32_t* ridx, const float2* gh, const double* scale, uint32_t grid,
+                   cudaStream_t st);
+void launch_b_children_sums(const BDev& d, int b, cudaStream_t st);
+void launch_b_finalize(const BDev& d, int a, LeafParams lp, const double* scale, cudaStream_t st);
+void launch_b_leaf_update(const BDev& d, const uint32_t* ridx, float* pred, uint32_t* row_leaf, uint32_t grid,
+                          cudaStream_t st);
+
 // ---- K9 forest traversal ----------------------------------------------------
 // Node: word0 = feature | (is_leaf << 31) | (default_left << 30) | (categorical << 29)
 //       value = threshold (split) or leaf value (leaf); left/right absolute indices.
