@@ -32,7 +32,11 @@ sys.path.insert(0, ROOT)
 METRIC = "train s/100 trees, predict rows/s, p99 serve ms vs plain GPU at equal loss"
 UNIT = "s/100 trees"
 N_ROWS, N_FEAT, N_NAN, SEED = 1_000_000, 100, 20, 2
-WORKLOAD = "binary-logistic GBDT 1,000,000x100 f32 (20 NaN cols), depth 8, 256 bins, lr 0.1, FP32 grad/hess"
+WORKLOAD = "binary-logistic GBDT 1,000,000x100 f32 (20 NaN cols), depth 8, 256 bins, lr 0.1, 500 trees"
+DTYPES = {"plain": "f32 grad/hess, int64 fixed-point histograms",
+          "batched_fp32": "f32 grad/hess, int64 fixed-point histograms",
+          "batched_q16": "int16 grad/hess (stochastic rounding), integer histograms, f64 leaf solves",
+          "batched_q8": "int8 grad/hess (stochastic rounding), integer histograms, f64 leaf solves"}
 
 
 def cfg_kwargs():
@@ -149,6 +153,39 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+FORMS = [  # (name, GBDTConfig overrides); "plain" is the reference form on the GPU
+    ("plain", dict(precision="fp32", batched=False)),
+    ("batched_fp32", dict(precision="fp32", batched=True)),
+    ("batched_q16", dict(precision="q16", batched=True)),
+    ("batched_q8", dict(precision="q8", batched=True)),
+]
+EQUAL_LOSS_REL = 1e-3
+
+
+def run_form(bst, torch, ds, xv, yv, cfg, args, world):
+    """W warm-up rounds, K timed rounds (one update call, device events),
+    then the rest of the configured trees; held-out logloss of the result."""
+    booster = bst.Booster(ds, cfg, n_threads=0)
+    booster.update(args.warmup)
+    t0, c0 = booster.stats()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    booster.update(args.steps)  # returns with the engine's stream idle
+    ev1.record()
+    ev1.synchronize()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    t1, c1 = booster.stats()
+    rest = max(0, cfg.n_estimators - args.warmup - args.steps)
+    if rest:
+        booster.update(rest)
+    model = booster.model()
+    pv = model.predict_group_major(bst.Dataset.from_feature_major(xv))
+    return dict(elapsed=elapsed, t0=t0, t1=t1, c0=c0, c1=c1, heldout=bst.metric("logloss", pv, yv),
+                trees=booster.n_rounds, model=model)
+
+
 def run_ours(args, world, rank, local):
     import ctypes
 
@@ -158,41 +195,48 @@ def run_ours(args, world, rank, local):
 
     torch.cuda.set_device(local)
     kw = cfg_kwargs()
-    cfg = bst.GBDTConfig(device=local, **kw)
     x, y = bst.synth.binary(N_ROWS, N_FEAT, N_NAN, seed=SEED, stream=rank)
     ds = bst.Dataset.from_feature_major(x, y)
+    xv, yv = bst.synth.binary(200_000, N_FEAT, N_NAN, seed=SEED, stream=1000 + rank)
     t_bin0 = time.perf_counter()
-    booster = bst.Booster(ds, cfg, n_threads=0)
+    bst.BinnedDataset(ds, bst.GBDTConfig(device=local, **kw))
     binning_s = time.perf_counter() - t_bin0
-    booster.update(args.warmup)
-    t0_stats, c0 = booster.stats()
-    barrier(world)
-    torch.cuda.synchronize()
+
     clocks = ClockSampler(local)
     clocks.start()
-    # update() returns after its stream is idle, so events on this stream
-    # bracket the device work of the timed rounds
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record()
-    for _ in range(args.steps):
-        booster.update(1)
-    ev1.record()
-    ev1.synchronize()
-    torch.cuda.synchronize()
-    elapsed = ev0.elapsed_time(ev1) / 1e3
-    t1_stats, c1 = booster.stats()
-    # a short timed region may fall between two clock samples: keep the same
-    # load running (untimed, same work) until a few samples exist
+    res = {}
+    for name, over in FORMS:
+        res[name] = run_form(bst, torch, ds, xv, yv, bst.GBDTConfig(device=local, **dict(kw, **over)), args, world)
+    # a short timed region may fall between two clock samples: keep training
+    # load running (untimed) until a few samples exist
     t_ext = time.perf_counter()
-    while len(clocks.rows) < 4 and time.perf_counter() - t_ext < 3.0:
-        booster.update(1)
+    if len(clocks.rows) < 4:
+        b = bst.Booster(ds, bst.GBDTConfig(device=local, **kw), n_threads=0)
+        while len(clocks.rows) < 4 and time.perf_counter() - t_ext < 3.0:
+            b.update(10)
     clk = clocks.stop()
     clk["extended_window_s"] = round(time.perf_counter() - t_ext, 3)
     barrier(world)
-    # device time of the timed rounds (sum of CUDA-event phases; host gaps included in elapsed)
-    elapsed_max = reduce_max(world, elapsed)
-    value = 100.0 * elapsed_max / (args.steps * world)
-    ms_per_step = 1000.0 * elapsed_max / args.steps
+
+    # headline: the fastest form whose held-out loss is within 1e-3 relative of
+    # the plain form's at the same number of trees
+    plain_loss = res["plain"]["heldout"]
+    forms = {}
+    for name, r in res.items():
+        el = reduce_max(world, r["elapsed"])
+        r["value"] = 100.0 * el / (args.steps * world)
+        r["ms"] = 1000.0 * el / args.steps
+        r["equal_loss"] = abs(r["heldout"] - plain_loss) <= EQUAL_LOSS_REL * plain_loss
+        forms[name] = {"s_per_100_trees": round(r["value"], 5), "heldout_logloss": round(r["heldout"], 6),
+                       "loss_rel_vs_plain": round((r["heldout"] - plain_loss) / plain_loss, 6),
+                       "equal_loss": r["equal_loss"], "trees": r["trees"]}
+    ok = [k for k, r in res.items() if r["equal_loss"]]
+    head = min(ok, key=lambda k: res[k]["value"])
+    hr = res[head]
+    value, ms_per_step = hr["value"], hr["ms"]
+    t0_stats, t1_stats, c0, c1 = hr["t0"], hr["t1"], hr["c0"], hr["c1"]
+    model = hr["model"]
+    head_over = dict(FORMS)[head]
 
     hist_ms = t1_stats["histograms"] - t0_stats["histograms"]
     hist_bytes = c1["hist_bytes"] - c0["hist_bytes"]
@@ -201,18 +245,12 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = peaks()
     achieved = hist_bytes / (hist_ms / 1e3) / 1e9 if hist_ms > 0 else 0.0
     traffic = None
-    tr_file = os.path.join(ROOT, "profiles", "hist_build_traffic.json")
+    tr_file = os.path.join(ROOT, "profiles", f"hist_build_traffic_{head}.json")
     if os.path.exists(tr_file):
         with open(tr_file) as f:
             tr = json.load(f)
         # ncu DRAM bytes per algorithmic byte, scaled to this run's average launch
         traffic = round(tr["dram_bytes_per_algorithmic_byte"] * hist_bytes / hist_launches)
-
-    # held-out loss of the model after warmup + steps rounds
-    model = booster.model()
-    xv, yv = bst.synth.binary(200_000, N_FEAT, N_NAN, seed=SEED, stream=1000 + rank)
-    pv = model.predict_group_major(bst.Dataset.from_feature_major(xv))
-    heldout = bst.metric("logloss", pv, yv)
 
     # predict throughput on device-resident rows (serving kernel), rows/s
     rows_pred = None
@@ -236,7 +274,7 @@ def run_ours(args, world, rank, local):
         rows_pred = f"error: {ex}"
 
     # e2e through the public API from pinned host buffers: 100 trees per step
-    e2e_cfg = bst.GBDTConfig(device=local, **dict(kw, n_estimators=100))
+    e2e_cfg = bst.GBDTConfig(device=local, **dict(kw, n_estimators=100, **head_over))
     xh = torch.from_numpy(x).pin_memory().numpy()
     yh = torch.from_numpy(y).pin_memory().numpy()
     e2e_steps = max(1, min(args.steps, 2))
@@ -261,15 +299,17 @@ def run_ours(args, world, rank, local):
         line = {
             "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 grad/hess, int64 fixed-point histograms",
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPES[head],
             "data": "synthetic (seeded counter-based generator)",
-            "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "config": {"workload": WORKLOAD, "form": head, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (128 MB binned rows + 8 MB grad/hess per round)",
-                       "binning_s": round(binning_s, 3), "heldout_logloss": round(heldout, 6),
-                       "trees_trained": booster.n_rounds},
+                       "binning_s": round(binning_s, 3), "heldout_logloss": round(hr["heldout"], 6),
+                       "heldout_rows": int(len(yv)), "equal_loss_rule": "within 1e-3 relative of plain",
+                       "speedup_vs_plain": round(res["plain"]["value"] / value, 3)},
+            "forms": forms,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_hist_build", "launches": hist_launches,
+                         "kernel": "k_b_hist" if head != "plain" else "k_hist_build", "launches": hist_launches,
                          "avg_launch_ms": round(hist_ms / hist_launches, 5),
                          "algorithmic_bytes_per_launch": round(hist_bytes / hist_launches)},
             "cpu_baseline": cpu,

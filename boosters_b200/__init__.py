@@ -106,7 +106,9 @@ _PRECISION = {"fp32": _n.PRECISION_FP32, "q16": _n.PRECISION_Q16, "q8": _n.PRECI
 class GBDTConfig:
     """GBDT configuration with the reference's names and defaults
     (packages/boosters-python/src/config.rs:160-560, model/gbdt/config.rs:111-226),
-    plus GPU options (precision, cuda_graph, device)."""
+    plus GPU options: precision ("fp32", "q16", "q8"), batched (depth-wise
+    trees grown by a device-side level loop replayed as one CUDA graph per
+    tree; False selects the host-driven loop), cuda_graph, device."""
 
     def __init__(self, n_estimators=100, learning_rate=0.3, objective=None, metric=None,
                  growth_strategy=GrowthStrategy.Depthwise, max_depth=6, n_leaves=31,
@@ -115,7 +117,7 @@ class GBDTConfig:
                  max_bins=256, enable_bundling=True, sparsity_threshold=0.9,
                  max_categorical_cardinality=0, binning_sample_cnt=200000, cache_size=8,
                  early_stopping_rounds=None, seed=42, verbosity=0, precision="fp32",
-                 cuda_graph=False, device=0):
+                 cuda_graph=False, device=0, batched=True):
         self.n_estimators = n_estimators
         self.learning_rate = learning_rate
         self.objective = objective if objective is not None else Objective.Squared()
@@ -146,6 +148,7 @@ class GBDTConfig:
         self.precision = precision
         self.cuda_graph = cuda_graph
         self.device = device
+        self.batched = batched
         _n.check(_n.lib.bst_config_validate(ctypes.byref(self.to_c())))
 
     def to_c(self, record_leaves=False):
@@ -179,6 +182,7 @@ class GBDTConfig:
         c.verbosity = int(self.verbosity)
         c.precision = _PRECISION[self.precision]
         c.cuda_graph = 1 if self.cuda_graph else 0
+        c.batched = 1 if self.batched else 0
         c.device = int(self.device)
         c.record_leaves = 1 if record_leaves else 0
         return c

@@ -154,6 +154,9 @@ SIGNATURES = [
     ("bst_find_split_noalloc", ctypes.c_int32,
      [ctypes.c_void_p, c_u32p, c_i32p, c_i32p, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
       ctypes.c_uint32, ctypes.POINTER(Config), ctypes.c_uint32, ctypes.c_void_p, ctypes.POINTER(Split)]),
+    ("bst_quantize_gradients", ctypes.c_int32,
+     [c_f32p, c_f32p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+      c_i32p, c_i32p, c_f64p]),
     ("bst_synth_regression", ctypes.c_int32,
      [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, c_f32p, c_f32p]),
     ("bst_synth_binary", ctypes.c_int32,

@@ -87,8 +87,8 @@ bst_status check_config(const bst_config* c, bool for_training) {
     if (c->growth_strategy == BST_GROWTH_LEAFWISE && c->max_leaves < 1)
         return fail(BST_ERR_CONFIG, "max_leaves must be at least 1");
     if (c->max_bins < 1) return fail(BST_ERR_CONFIG, "max_bins must be at least 1");
-    if (c->precision != BST_PRECISION_FP32)
-        return fail(BST_ERR_UNSUPPORTED, "only FP32 histogram precision is available in this build");
+    if (c->precision != BST_PRECISION_FP32 && c->precision != BST_PRECISION_Q16 && c->precision != BST_PRECISION_Q8)
+        return fail(BST_ERR_CONFIG, "unknown histogram precision " + std::to_string(c->precision));
     return BST_OK;
 }
 
@@ -689,8 +689,12 @@ bst_status bst_histogram_build(const uint16_t* bins, const uint32_t* n_bins, uin
         if (!ch.empty()) BST_CK(cudaMemcpy(dch.p, ch.data(), sizeof(bst::HistChunk) * ch.size(), cudaMemcpyHostToDevice));
         dh.alloc(p.total_bins);
         BST_CK(cudaMemset(dh.p, 0, sizeof(bst::HBin) * p.total_bins));
-        bst::launch_hist_build(dch.p, (uint32_t)ch.size(), dt.p, (uint32_t)tiles.size(), max_smem, dr.p, dgh.p, dsc.p,
-                               d8.p, p.s8, d16.p, p.s16, dh.p, p.total_bins, nullptr);
+        bst::GradRef gr{};
+        gr.gh = dgh.p;
+        gr.scale = dsc.p;
+        gr.mode = bst::GRAD_F32;
+        bst::launch_hist_build(dch.p, (uint32_t)ch.size(), dt.p, (uint32_t)tiles.size(), max_smem, dr.p, gr, d8.p,
+                               p.s8, d16.p, p.s16, dh.p, p.total_bins, nullptr);
         BST_CK(cudaGetLastError());
         std::vector<bst::HBin> h(p.total_bins);
         BST_CK(cudaMemcpy(h.data(), dh.p, sizeof(bst::HBin) * p.total_bins, cudaMemcpyDeviceToHost));
@@ -774,6 +778,49 @@ bst_status bst_find_split(const double* hist, const uint32_t* n_bins, const int3
             out->is_categorical = (s.flags & 2u) ? 1 : 0;
             out->bin = (s.flags & 2u) ? 0u : s.bin;  // SplitType::Categorical has no bin
             for (int q = 0; q < 4; ++q) out->left_cats[q] = s.cats[q];
+        }
+        return BST_OK;
+    });
+}
+
+bst_status bst_quantize_gradients(const float* grad, const float* hess, uint64_t n, int32_t precision, uint64_t seed,
+                                  uint32_t round, uint32_t output, int32_t* qg, int32_t* qh, double* steps) {
+    if (!steps || (n && (!grad || !hess || !qg || !qh))) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (precision != BST_PRECISION_Q16 && precision != BST_PRECISION_Q8)
+        return fail(BST_ERR_INVALID_ARGUMENT, "precision must be Q16 or Q8");
+    if (n > 0xFFFFFFFFull) return fail(BST_ERR_INVALID_ARGUMENT, "at most 2^32 - 1 rows");
+    return guarded([&]() -> bst_status {
+        std::vector<float2> gh(n);
+        for (uint64_t i = 0; i < n; ++i) gh[i] = make_float2(grad[i], hess[i]);
+        bst::DevArray<float2> dgh;
+        bst::DevArray<unsigned> dmax;
+        bst::DevArray<double> dsteps;
+        bst::DevArray<uint8_t> dq;
+        const size_t qb = precision == BST_PRECISION_Q8 ? 2 : 4;
+        dgh.alloc(std::max<uint64_t>(1, n));
+        dmax.alloc(2);
+        dsteps.alloc(4);
+        dq.alloc(std::max<uint64_t>(1, n) * qb);
+        if (n) BST_CK(cudaMemcpy(dgh.p, gh.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+        BST_CK(cudaMemset(dmax.p, 0, 2 * sizeof(unsigned)));
+        bst::launch_maxabs(dgh.p, n, dmax.p, nullptr);
+        bst::launch_quantize(precision, 1, dgh.p, n, dmax.p, seed, round, output, dq.p, dsteps.p, nullptr);
+        BST_CK(cudaGetLastError());
+        BST_CK(cudaMemcpy(steps, dsteps.p, 4 * sizeof(double), cudaMemcpyDeviceToHost));
+        if (n == 0) return BST_OK;
+        std::vector<uint8_t> hq(n * qb);
+        BST_CK(cudaMemcpy(hq.data(), dq.p, n * qb, cudaMemcpyDeviceToHost));
+        for (uint64_t i = 0; i < n; ++i) {
+            if (qb == 2) {
+                qg[i] = (int8_t)hq[2 * i];
+                qh[i] = (int8_t)hq[2 * i + 1];
+            } else {
+                int16_t a, b;
+                std::memcpy(&a, &hq[4 * i], 2);
+                std::memcpy(&b, &hq[4 * i + 2], 2);
+                qg[i] = a;
+                qh[i] = b;
+            }
         }
         return BST_OK;
     });

@@ -26,12 +26,15 @@ void cuda_check(cudaError_t e, const char* what) {
 
 // Column tiles of the histogram kernel: lanes of one 16-byte row vector
 // whose bins fit one shared-memory histogram (<= 4096 bins = 64 KiB).
-void build_hist_tiles(const BinPlan& p, std::vector<HistTile>& tiles, uint32_t& max_smem) {
+// only: if given, the columns to cover (others are skipped).
+void build_hist_tiles(const BinPlan& p, std::vector<HistTile>& tiles, uint32_t& max_smem,
+                      const std::vector<uint8_t>* only) {
     const uint32_t kMaxSmemBins = 4096;
     tiles.clear();
     const uint32_t nc = p.n_cols();
     std::vector<int> col_of8(p.s8, -1), col_of16(p.s16, -1);
     for (uint32_t c = 0; c < nc; ++c) {
+        if (only && !(*only)[c]) continue;
         if (p.col_matrix[c] == 0)
             col_of8[p.col_pos[c]] = (int)c;
         else
@@ -74,9 +77,57 @@ void build_hist_tiles(const BinPlan& p, std::vector<HistTile>& tiles, uint32_t& 
     for (auto& t : tiles) max_smem = std::max(max_smem, t.smem_bins);
 }
 
+// Column-lane tiles: aligned 32-byte windows of each matrix row (a 16-byte
+// window for a row tail of 16 bytes). A window holding a column with more
+// than max_bins bins is left to the HistTile kernel: its columns are marked
+// in `rest`.
+void build_lane_tiles(const BinPlan& p, uint32_t max_bins, std::vector<LaneTile>& tiles, uint32_t& tile_bins,
+                      std::vector<uint8_t>& rest) {
+    tiles.clear();
+    tile_bins = 0;
+    const uint32_t nc = p.n_cols();
+    rest.assign(nc, 0);
+    for (uint32_t m = 0; m < 2; ++m) {
+        const uint32_t esize = m == 0 ? 1u : 2u;
+        const uint32_t row_bytes = m == 0 ? p.s8 : p.s16 * 2u;
+        std::vector<int> col_at(row_bytes / esize, -1);
+        for (uint32_t c = 0; c < nc; ++c)
+            if (p.col_matrix[c] == m) col_at[p.col_pos[c]] = (int)c;
+        for (uint32_t off = 0; off < row_bytes;) {
+            const uint32_t width = row_bytes - off >= 32 ? 32u : 16u;
+            LaneTile t;
+            std::memset(&t, 0, sizeof(t));
+            t.esize = esize;
+            t.words = width / 4;
+            t.byte_off = off;
+            bool any = false, big = false;
+            for (uint32_t e = 0; e < width / esize; ++e) {
+                const int c = col_at[off / esize + e];
+                if (c < 0) continue;
+                any = true;
+                const uint32_t nb = p.col_nbins[c];
+                big = big || nb > max_bins;
+                t.col_hist[e] = p.col_hist_off[c];
+                t.col_nbins[e] = nb;
+                t.n_bins = std::max(t.n_bins, nb);
+            }
+            if (any && big) {
+                for (uint32_t e = 0; e < width / esize; ++e) {
+                    const int c = col_at[off / esize + e];
+                    if (c >= 0) rest[c] = 1;
+                }
+            } else if (any) {
+                t.n_bins = std::max<uint32_t>(t.n_bins, 1);
+                tile_bins = std::max(tile_bins, t.n_bins);
+                tiles.push_back(t);
+            }
+            off += width;
+        }
+    }
+}
+
 namespace {
 
-constexpr uint32_t HIST_CHUNK_ROWS = 4096;
 constexpr uint32_t PART_CHUNK_ROWS = 4096;
 constexpr uint32_t SUM_CHUNK_ROWS = 8192;
 
@@ -263,6 +314,7 @@ class Trainer {
 
     // One tree on caller-given gradients (TreeGrower::grow, grower.rs:265).
     HostTree run_external(const float* g, const float* h) {
+        external_ = true;  // caller-given gradients are used as they are (f32)
         setup_common();
         const uint64_t n = n_;
         pred_.alloc(n);
@@ -308,17 +360,34 @@ class Trainer {
             launch_gradients(obj, G_, pred_.p, y_.p, w_.p, n_, gh_.p, maxabs_.p, st_);
             launch_fixed_scales(maxabs_.p, G_, n_, scales_.p, st_);
             m_.counters.launches += 2;
-            timer_.end();
-            BST_CK(cudaMemcpyAsync(h_scales_.data(), scales_.p, sizeof(double) * 4 * G_, cudaMemcpyDeviceToHost, st_));
-            BST_CK(cudaStreamSynchronize(st_));
-            for (uint32_t o = 0; o < G_; ++o) {
-                HostTree t = use_batched_ ? grow_batched(o) : grow(o);
-                t.group = o;
-                std::lock_guard<std::mutex> lk(m_.mu);
-                m_.trees.push_back(std::move(t));
-                m_.dev.reset();
+            if (qmode_ != GRAD_F32) {
+                launch_quantize(qmode_, G_, gh_.p, n_, maxabs_.p, cfg_.seed, round_no_, 0u, gq_.p, qscales_.p, st_);
+                m_.counters.launches += 1;
             }
+            ++round_no_;
+            timer_.end();
+            if (use_batched_) {
+                // device-side trees: no host round trip until a ring slot is reused
+                for (uint32_t o = 0; o < G_; ++o) {
+                    const uint32_t si = (uint32_t)(seq_ % RING);
+                    if (slots_[si].pending) push_tree(collect_batched(si));
+                    launch_batched(o, si);
+                    ++seq_;
+                }
+                continue;
+            }
+            BST_CK(cudaMemcpyAsync(h_scales_.data(), scales_.p, sizeof(double) * 4 * G_, cudaMemcpyDeviceToHost, st_));
+            if (qmode_ != GRAD_F32)
+                BST_CK(cudaMemcpyAsync(h_qscales_.data(), qscales_.p, sizeof(double) * 4 * G_,
+                                       cudaMemcpyDeviceToHost, st_));
+            BST_CK(cudaStreamSynchronize(st_));
+            for (uint32_t o = 0; o < G_; ++o) push_tree(grow(o), o);
         }
+        if (use_batched_)
+            for (uint32_t i = 0; i < RING; ++i) {
+                const uint32_t si = (uint32_t)((seq_ + i) % RING);
+                if (slots_[si].pending) push_tree(collect_batched(si));
+            }
         BST_CK(cudaStreamSynchronize(st_));
         timer_.collect();
         for (int i = 1; i < 7; ++i) {
@@ -326,6 +395,17 @@ class Trainer {
             timer_.acc[i] = 0.0;
         }
         m_.counters.hist_ms = m_.timings[PH_HIST];
+    }
+
+    void push_tree(HostTree&& t, uint32_t o) {
+        t.group = o;
+        std::lock_guard<std::mutex> lk(m_.mu);
+        m_.trees.push_back(std::move(t));
+        m_.dev.reset();
+    }
+    void push_tree(HostTree&& t) {
+        const uint32_t o = t.group;
+        push_tree(std::move(t), o);
     }
 
     // Training predictions back to the model.
@@ -358,9 +438,10 @@ class Trainer {
     uint64_t slot_bins_ = 0;
     DevArray<HistTile> tiles_;
     uint32_t n_tiles_ = 0, tile_smem_ = 0;
+    DevArray<LaneTile> lane_tiles_;
+    uint32_t n_lane_tiles_ = 0, lane_bins_ = 0;
     DevArray<ScanColumn> scan_cols_;
-    DevArray<HistChunk> d_hchunks_, d_schunks_;
-    DevArray<FinishWork> d_finish_;
+    DevArray<HistChunk> d_schunks_;
     DevArray<ScanNode> d_scan_nodes_;
     DevArray<ColCand> d_cand_;
     DevArray<long long> d_node_tot_, d_sums_;
@@ -376,9 +457,37 @@ class Trainer {
     HostTree tree_;
     std::vector<uint32_t> leaf_tree_node_;  // by partition node
     std::vector<float> leaf_value_;
-    const float2* gh_o_ = nullptr;
-    const double* scale_o_ = nullptr;
+    const double* scale_o_ = nullptr;  // units of the histogram sums (scan, node stats)
     double inv_g_ = 1.0, inv_h_ = 1.0;
+    GradRef gr_o_{};  // histogram / node-sum source of the current output
+    GradRef gx_o_{};  // exact f32 source (leaf solves in quantised mode)
+
+    // quantised training (BST_PRECISION_Q16 / Q8)
+    int qmode_ = GRAD_F32;
+    bool external_ = false;
+    DevArray<uint8_t> gq_;
+    DevArray<double> qscales_;
+    std::vector<double> h_qscales_;
+    uint32_t round_no_ = 0;
+
+    uint32_t grad_bytes() const { return qmode_ == GRAD_Q8 ? 2u : (qmode_ == GRAD_Q16 ? 4u : 8u); }
+    GradRef grad_ref(uint32_t o) const {
+        GradRef r{};
+        r.gh = gh_.p + (size_t)o * n_;
+        r.scale = scales_.p + 4 * (size_t)o;
+        r.mode = qmode_;
+        r.gq = qmode_ == GRAD_F32 ? nullptr : (const void*)(gq_.p + (size_t)o * n_ * (grad_bytes()));
+        return r;
+    }
+    GradRef exact_ref(uint32_t o) const {
+        GradRef r = grad_ref(o);
+        r.mode = GRAD_F32;
+        r.gq = nullptr;
+        return r;
+    }
+    const double* unit_scale(uint32_t o) const {
+        return (qmode_ == GRAD_F32 ? scales_.p : qscales_.p) + 4 * (size_t)o;
+    }
 
     void setup() {
         setup_common();
@@ -390,6 +499,11 @@ class Trainer {
         maxabs_.alloc(2 * G_);
         scales_.alloc(4 * G_);
         h_scales_.assign(4 * G_, 1.0);
+        if (qmode_ != GRAD_F32) {
+            gq_.alloc((size_t)G_ * n * grad_bytes());
+            qscales_.alloc(4 * G_);
+            h_qscales_.assign(4 * G_, 1.0);
+        }
         // targets: first output row (targets.output(0) in every objective)
         BST_CK(cudaMemcpyAsync(y_.p, ds_.y.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st_));
         if (ds_.has_w) BST_CK(cudaMemcpyAsync(w_.p, ds_.w.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st_));
@@ -401,6 +515,7 @@ class Trainer {
 
     void setup_common() {
         const uint64_t n = n_;
+        qmode_ = external_ ? GRAD_F32 : cfg_.precision;
         ridx_.alloc(n);
         tmp_.alloc(n);
         if (cfg_.record_leaves) row_leaf_.alloc(n);
@@ -424,10 +539,8 @@ class Trainer {
         if (n_cols_) BST_CK(cudaMemcpy(scan_cols_.p, sc.data(), sizeof(ScanColumn) * n_cols_, cudaMemcpyHostToDevice));
 
         const size_t max_chunks = (size_t)(n / 1024 + 2 * (size_t)max_pnodes_ + 16);
-        d_hchunks_.alloc(max_chunks);
         d_schunks_.alloc(max_chunks);
         d_pchunks_.alloc(max_chunks);
-        d_finish_.alloc(max_pnodes_ + 1);
         d_scan_nodes_.alloc(2 * (size_t)max_pnodes_ + 2);
         d_cand_.alloc((2 * (size_t)max_pnodes_ + 2) * std::max<uint32_t>(1, n_cols_));
         d_node_tot_.alloc(2 * (2 * (size_t)max_pnodes_ + 2));
@@ -437,6 +550,7 @@ class Trainer {
         d_sums_.alloc(2 * ((size_t)max_pnodes_ + 1));
         d_leaves_.alloc(max_pnodes_ + 1);
         stage_.reserve(max_chunks * 48 + (size_t)(max_pnodes_ + 4) * 256 + (1 << 20));
+        if (n_cols_) setup_hist_state();
         use_batched_ = cfg_.batched && !leafwise_ && n_cols_ > 0 && cfg_.max_depth <= 14;
         if (use_batched_) setup_batched();
     }
@@ -450,36 +564,97 @@ class Trainer {
     DevArray<BTreeNode> d_btree_;
     DevArray<BLeaf> d_bleaves_;
     DevArray<BColumn> d_bcols_;
-    DevArray<HistChunk> d_root_chunks_;
+    DevArray<uint32_t> d_seg_exp_;
+    DevArray<uint8_t> d_part_;      // partial histograms of the lane tiles
+    DevArray<uint32_t> d_bin_map_;  // global bin -> (lane tile, partial entry)
+    DevArray<uint2> d_ent_;         // node partial entry -> (global bin, lane tile / offset)
+    uint32_t n_ent_ = 0;
     DevArray<ScanNode> d_root_scan_;
-    uint32_t n_root_chunks_ = 0, max_tnodes_ = 0;
-    std::vector<cudaGraphExec_t> graphs_;
+    uint32_t max_tnodes_ = 0;
+    // Pipelined replay: tree k is read back and converted on the host while
+    // the device grows tree k+1. Each ring slot owns its own graph per output
+    // (its event-record nodes then time only the launch that used the slot).
+    static constexpr uint32_t RING = 2;
+    struct Slot {
+        BTreeNode* tree = nullptr;  // pinned
+        BState* state = nullptr;    // pinned
+        cudaEvent_t done = nullptr, w0 = nullptr, w1 = nullptr;
+        bool pending = false;
+        uint32_t o = 0;
+        std::vector<uint32_t> row_leaf;
+    };
+    Slot slots_[RING];
+    uint64_t seq_ = 0;
+    std::vector<cudaGraphExec_t> graphs_;  // [o * RING + slot]
     std::vector<std::unique_ptr<Timer>> gtimers_;
-    cudaEvent_t whole_[2] = {nullptr, nullptr};
     std::vector<uint64_t> graph_launches_, graph_hist_launches_;
-    BTreeNode* h_btree_ = nullptr;
-    BState* h_bstate_ = nullptr;
 
   public:
     ~Trainer() {
         for (auto g : graphs_)
             if (g) cudaGraphExecDestroy(g);
-        if (h_btree_) cudaFreeHost(h_btree_);
-        if (h_bstate_) cudaFreeHost(h_bstate_);
-        for (auto e : whole_)
-            if (e) cudaEventDestroy(e);
+        for (auto& sl : slots_) {
+            if (sl.tree) cudaFreeHost(sl.tree);
+            if (sl.state) cudaFreeHost(sl.state);
+            for (auto e : {sl.done, sl.w0, sl.w1})
+                if (e) cudaEventDestroy(e);
+        }
     }
 
   private:
+
+    // Level state and buffers of the histogram pipeline (both growth loops).
+    void setup_hist_state() {
+        init_kernel_attributes();
+        const uint32_t max_front = max_pnodes_;
+        d_bstate_.alloc(1);
+        d_bexp_.alloc(max_front / 2 + 1);
+        bd_.state = d_bstate_.p;
+        bd_.exp = d_bexp_.p;
+        // about three row segments x lane tiles per resident histogram block
+        const uint32_t blocks = n_lane_tiles_ ? 148u * lane_blocks_per_sm(qmode_) : 148u * 3u;
+        const uint32_t tiles = std::max<uint32_t>(1, n_lane_tiles_ ? n_lane_tiles_ : n_tiles_);
+        bd_.hist_target = std::max<uint32_t>(1, 3u * blocks / tiles);
+        bd_.hist_seg_max = n_lane_tiles_ ? lane_segment_max(qmode_) : (uint32_t)HIST_CHUNK_MAX;
+        // segments per level <= rows / segment + nodes; the segment is at least
+        // min(1024, seg_max) and at least rows / hist_target rounded up
+        const uint64_t min_seg = std::max<uint64_t>(
+            1024, std::min<uint64_t>(bd_.hist_seg_max, (n_ + bd_.hist_target - 1) / bd_.hist_target));
+        const uint64_t max_segs = n_ / std::min<uint64_t>(min_seg, HIST_CHUNK_MAX) + max_front + 16;
+        d_seg_exp_.alloc(max_segs);
+        bd_.seg_exp = d_seg_exp_.p;
+        bd_.max_segs = (uint32_t)max_segs;
+        if (n_lane_tiles_) {
+            d_part_.alloc(max_segs * n_lane_tiles_ * (size_t)lane_part_stride() * lane_part_entry_bytes(qmode_));
+            std::vector<uint32_t> bm(p_.total_bins, 0xFFFFFFFFu);
+            std::vector<LaneTile> lt(n_lane_tiles_);
+            BST_CK(cudaMemcpy(lt.data(), lane_tiles_.p, sizeof(LaneTile) * n_lane_tiles_, cudaMemcpyDeviceToHost));
+            std::vector<uint2> ent;
+            for (uint32_t t = 0; t < n_lane_tiles_; ++t) {
+                const uint32_t C = lt[t].words * 4 / lt[t].esize, B = lt[t].n_bins;
+                for (uint32_t e = 0; e < C; ++e)
+                    for (uint32_t b = 0; b < lt[t].col_nbins[e]; ++b) {
+                        bm[lt[t].col_hist[e] + b] = (t << 16) | (e * B + b);
+                        ent.push_back(make_uint2(lt[t].col_hist[e] + b, (t << 16) | (e * B + b)));
+                    }
+            }
+            n_ent_ = (uint32_t)ent.size();
+            d_ent_.alloc(std::max<size_t>(1, ent.size()));
+            BST_CK(cudaMemcpy(d_ent_.p, ent.data(), sizeof(uint2) * ent.size(), cudaMemcpyHostToDevice));
+            d_bin_map_.alloc(p_.total_bins);
+            BST_CK(cudaMemcpy(d_bin_map_.p, bm.data(), sizeof(uint32_t) * bm.size(), cudaMemcpyHostToDevice));
+        } else {
+            d_bin_map_.alloc(std::max<uint64_t>(1, p_.total_bins));
+            BST_CK(cudaMemset(d_bin_map_.p, 0xFF, sizeof(uint32_t) * std::max<uint64_t>(1, p_.total_bins)));
+        }
+    }
 
     void setup_batched() {
         init_kernel_attributes();
         const uint32_t max_front = max_pnodes_;
         max_tnodes_ = 2 * max_front;
-        d_bstate_.alloc(1);
         d_front_[0].alloc(max_front);
         d_front_[1].alloc(max_front);
-        d_bexp_.alloc(max_front / 2 + 1);
         d_btree_.alloc(max_tnodes_);
         d_bleaves_.alloc(max_front + 1);
         std::vector<BColumn> bc(n_cols_);
@@ -487,119 +662,153 @@ class Trainer {
             bc[c] = BColumn{p_.col_matrix[c], p_.col_pos[c], p_.col_missing[c], p_.col_default[c]};
         d_bcols_.alloc(n_cols_);
         BST_CK(cudaMemcpy(d_bcols_.p, bc.data(), sizeof(BColumn) * n_cols_, cudaMemcpyHostToDevice));
-        std::vector<HistChunk> rc;
-        hist_chunks_for(0, PNode{0, (uint32_t)n_}, true, rc);
-        n_root_chunks_ = (uint32_t)rc.size();
-        d_root_chunks_.alloc(std::max<size_t>(1, rc.size()));
-        BST_CK(cudaMemcpy(d_root_chunks_.p, rc.data(), sizeof(HistChunk) * rc.size(), cudaMemcpyHostToDevice));
         const ScanNode rs{0, (uint32_t)n_, 0u, 0u, 0, 0};
         d_root_scan_.alloc(1);
         BST_CK(cudaMemcpy(d_root_scan_.p, &rs, sizeof(rs), cudaMemcpyHostToDevice));
-        BST_CK(cudaMallocHost(&h_btree_, sizeof(BTreeNode) * max_tnodes_));
-        BST_CK(cudaMallocHost(&h_bstate_, sizeof(BState)));
-        bd_.state = d_bstate_.p;
+        for (auto& sl : slots_) {
+            BST_CK(cudaMallocHost(&sl.tree, sizeof(BTreeNode) * max_tnodes_));
+            BST_CK(cudaMallocHost(&sl.state, sizeof(BState)));
+            BST_CK(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+            BST_CK(cudaEventCreate(&sl.w0));
+            BST_CK(cudaEventCreate(&sl.w1));
+        }
         bd_.front[0] = d_front_[0].p;
         bd_.front[1] = d_front_[1].p;
-        bd_.exp = d_bexp_.p;
         bd_.tree = d_btree_.p;
         bd_.leaves = d_bleaves_.p;
         bd_.pworks = d_pworks_.p;
         bd_.cursors = d_cursors_.p;
-        bd_.finish = d_finish_.p;
         bd_.scan_nodes = d_scan_nodes_.p;
         bd_.sums = d_sums_.p;
         bd_.bcols = d_bcols_.p;
         bd_.max_front = max_front;
         bd_.max_tnodes = max_tnodes_;
-        graphs_.assign(G_, nullptr);
-        gtimers_.resize(G_);
-        graph_launches_.assign(G_, 0);
-        graph_hist_launches_.assign(G_, 0);
+        graphs_.assign((size_t)G_ * RING, nullptr);
+        gtimers_.resize((size_t)G_ * RING);
+        graph_launches_.assign((size_t)G_ * RING, 0);
+        graph_hist_launches_.assign((size_t)G_ * RING, 0);
+    }
+
+    // Rows per histogram row segment for `rows` rows (the rule of k_b_children).
+    uint32_t chunk_rows(uint64_t rows) const {
+        const uint64_t tgt = std::max<uint32_t>(1, bd_.hist_target);
+        uint64_t want = (rows + tgt - 1) / tgt;
+        want = (want + 255) & ~uint64_t(255);
+        return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(want, 1024), bd_.hist_seg_max);
+    }
+
+    // Histograms of the smaller children described by the level state in bd_
+    // (or of all rows, root): partial histograms of the lane tiles, general
+    // tiles (atomic, into zeroed right slots), then the merge with the
+    // subtraction trick.
+    void enqueue_hist(const GradRef& gr, const uint32_t* ridx, bool root, Timer& tm, uint64_t& launches,
+                      uint64_t& hist_launches) {
+        // resident general-tile blocks per SM: 64 registers x 256 threads
+        // allow 4; the fixed-point form's 16 B/bin shared histograms allow 3
+        const uint32_t g_hist = 148 * (qmode_ == GRAD_F32 ? 3 : 4);
+        tm.begin(PH_HIST);
+        if (n_lane_tiles_)
+            launch_b_hist_part(bd_, lane_tiles_.p, n_lane_tiles_, ridx, gr, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16,
+                               d_part_.p, st_);
+        if (n_tiles_)
+            launch_b_hist(bd_, tiles_.p, n_tiles_, tile_smem_, ridx, gr, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16,
+                          hist_.p, slot_bins_, g_hist, st_);
+        tm.end();
+        tm.begin(PH_OTHER);
+        launch_b_merge(bd_, hist_.p, slot_bins_, p_.total_bins, d_part_.p, n_lane_tiles_, d_ent_.p, n_ent_,
+                       d_bin_map_.p, n_tiles_ > 0, root ? 1 : 0, qmode_, st_);
+        tm.end();
+        const uint32_t hist_kernels = (n_lane_tiles_ ? 1u : 0u) + (n_tiles_ ? 1u : 0u);
+        launches += 2 * hist_kernels;  // builds and merges
+        hist_launches += hist_kernels;
     }
 
     // The launch sequence of one tree for output o (captured into a graph).
     void enqueue_tree(uint32_t o, Timer& tm, uint64_t& launches, uint64_t& hist_launches) {
-        const float2* gh = gh_.p + (size_t)o * n_;
-        const double* scale = scales_.p + 4 * (size_t)o;
+        const GradRef gh = grad_ref(o);
+        const double* scale = unit_scale(o);
         float* pred = pred_.p + (size_t)o * n_;
-        const uint32_t g_wide = 148 * 8, g_hist = 148 * 3;
+        const uint32_t g_wide = 148 * 8;
         LeafParams lp{(double)cfg_.lambda, (double)cfg_.alpha, (double)cfg_.min_gain, cfg_.learning_rate, 0u};
         launches = 0;
         hist_launches = 0;
         tm.begin(PH_OTHER);
         launch_iota(ridx_.p, n_, st_);
         launch_b_root(bd_, n_, st_);
-        BST_CK(cudaMemsetAsync(hist_.p, 0, sizeof(HBin) * slot_bins_, st_));
+        if (n_tiles_) BST_CK(cudaMemsetAsync(hist_.p, 0, sizeof(HBin) * slot_bins_, st_));
+        launch_b_root_hist(bd_, n_, chunk_rows(n_), st_);
         tm.end();
-        tm.begin(PH_HIST);
-        launch_hist_build(d_root_chunks_.p, n_root_chunks_, tiles_.p, n_tiles_, tile_smem_, ridx_.p, gh, scale,
-                          b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, hist_.p, slot_bins_, st_);
-        tm.end();
+        enqueue_hist(gh, ridx_.p, true, tm, launches, hist_launches);
         tm.begin(PH_SCAN);
         launch_split_scan(d_root_scan_.p, 1, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p,
                           d_node_tot_.p, st_);
         launch_split_reduce(d_cand_.p, d_node_tot_.p, 1, n_cols_, last_wins_ ? 1 : 0, d_splits_.p, st_);
-        launch_b_root_set(bd_, d_splits_.p, st_);
         tm.end();
-        launches += 6;
-        hist_launches += 1;
+        tm.begin(PH_OTHER);
+        launch_b_root_set(bd_, d_splits_.p, lp, scale, st_);  // + level-0 decisions
+        tm.end();
+        launches += 5;
+        // row indices: level d partitions R[d & 1] into R[(d + 1) & 1]
+        uint32_t* R[2] = {ridx_.p, tmp_.p};
         for (uint32_t d = 0; d < cfg_.max_depth; ++d) {
             const int a = (int)(d & 1u);
             const bool need_split = d + 1 < cfg_.max_depth;
-            tm.begin(PH_OTHER);
-            launch_b_decide(bd_, a, lp, scale, st_);
-            tm.end();
+            uint32_t* rout = R[(d + 1) & 1u];
             tm.begin(PH_PART);
-            launch_b_partition(bd_, ridx_.p, tmp_.p, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, g_wide, st_);
-            launch_b_copy(bd_, tmp_.p, ridx_.p, g_wide, st_);
+            launch_b_partition(bd_, R[d & 1u], rout, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, a, need_split ? 1 : 0,
+                               g_wide, st_);  // + children
             tm.end();
-            tm.begin(PH_OTHER);
-            launch_b_children(bd_, a, need_split ? 1 : 0, st_);
-            tm.end();
-            launches += 4;
+            launches += 1;
             if (need_split) {
-                tm.begin(PH_OTHER);
-                launch_b_zero_right(bd_, hist_.p, slot_bins_, g_wide, st_);
-                tm.end();
-                tm.begin(PH_HIST);
-                launch_b_hist(bd_, tiles_.p, n_tiles_, tile_smem_, ridx_.p, gh, scale, b_.bins8.p, p_.s8,
-                              b_.bins16.p, p_.s16, hist_.p, slot_bins_, g_hist, st_);
-                tm.end();
-                tm.begin(PH_OTHER);
-                launch_b_finish(bd_, hist_.p, slot_bins_, p_.total_bins, g_wide, st_);
-                tm.end();
+                if (n_tiles_) {  // general tiles add atomically into the zeroed right slots
+                    tm.begin(PH_OTHER);
+                    launch_b_zero_right(bd_, hist_.p, slot_bins_, g_wide, st_);
+                    tm.end();
+                    launches += 1;
+                }
+                enqueue_hist(gh, rout, false, tm, launches, hist_launches);
                 tm.begin(PH_SCAN);
                 launch_b_scan(bd_, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p,
                               d_node_tot_.p, g_wide, st_);
-                launch_b_reduce(bd_, a ^ 1, d_cand_.p, d_node_tot_.p, n_cols_, last_wins_ ? 1 : 0, g_wide, st_);
+                launch_b_reduce(bd_, a ^ 1, d_cand_.p, d_node_tot_.p, n_cols_, last_wins_ ? 1 : 0, 1, lp, scale,
+                                (d + 1) & 1u, g_wide, st_);  // + next level's decisions
                 tm.end();
-                launches += 5;
-                hist_launches += 1;
+                launches += 2;
             } else {
                 tm.begin(PH_OTHER);
                 BST_CK(cudaMemsetAsync(d_sums_.p, 0, sizeof(long long) * d_sums_.n, st_));
-                launch_b_sums(bd_, ridx_.p, gh, scale, g_wide, st_);
+                launch_b_sums(bd_, rout, gh, g_wide, st_);
                 launch_b_children_sums(bd_, a ^ 1, st_);
                 tm.end();
                 launches += 2;
             }
         }
         tm.begin(PH_LEAF);
-        launch_b_finalize(bd_, (int)(cfg_.max_depth & 1u), lp, scale, st_);
-        launch_b_leaf_update(bd_, ridx_.p, pred, cfg_.record_leaves ? row_leaf_.p : nullptr, g_wide, st_);
+        launch_b_finalize(bd_, (int)(cfg_.max_depth & 1u), lp, scale, cfg_.max_depth & 1u, st_);
+        if (qmode_ != GRAD_F32) {
+            // leaves solved from the exact sums of the f32 gradients
+            BST_CK(cudaMemsetAsync(d_sums_.p, 0, sizeof(long long) * d_sums_.n, st_));
+            launch_b_leaf_sums(bd_, R[0], R[1], exact_ref(o), g_wide, st_);
+            launch_b_leaf_values(bd_, lp, scales_.p + 4 * (size_t)o, st_);
+            launches += 2;
+        }
+        launch_b_leaf_update(bd_, R[0], R[1], pred, cfg_.record_leaves ? row_leaf_.p : nullptr, g_wide, st_);
         tm.end();
         launches += 2;
     }
 
-    HostTree grow_batched(uint32_t o) {
-        if (!graphs_[o]) {
-            gtimers_[o] = std::make_unique<Timer>();
-            gtimers_[o]->st = st_;
-            gtimers_[o]->reserve(16 + 20 * (size_t)cfg_.max_depth);
-            gtimers_[o]->in_graph = true;
+    // Enqueues the tree of output o into ring slot `si` (no host wait).
+    void launch_batched(uint32_t o, uint32_t si) {
+        Slot& sl = slots_[si];
+        const size_t gi = (size_t)o * RING + si;
+        if (!graphs_[gi]) {
+            gtimers_[gi] = std::make_unique<Timer>();
+            gtimers_[gi]->st = st_;
+            gtimers_[gi]->reserve(16 + 20 * (size_t)cfg_.max_depth);
+            gtimers_[gi]->in_graph = true;
             BST_CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
             try {
-                enqueue_tree(o, *gtimers_[o], graph_launches_[o], graph_hist_launches_[o]);
+                enqueue_tree(o, *gtimers_[gi], graph_launches_[gi], graph_hist_launches_[gi]);
             } catch (...) {
                 cudaGraph_t g = nullptr;
                 cudaStreamEndCapture(st_, &g);
@@ -612,40 +821,54 @@ class Trainer {
             const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
             cudaGraphDestroy(g);
             BST_CK(e);
-            graphs_[o] = ex;
+            graphs_[gi] = ex;
         }
-        if (!whole_[0]) {
-            BST_CK(cudaEventCreate(&whole_[0]));
-            BST_CK(cudaEventCreate(&whole_[1]));
-        }
-        BST_CK(cudaEventRecord(whole_[0], st_));
-        BST_CK(cudaGraphLaunch(graphs_[o], st_));
-        BST_CK(cudaEventRecord(whole_[1], st_));
-        BST_CK(cudaMemcpyAsync(h_bstate_, d_bstate_.p, sizeof(BState), cudaMemcpyDeviceToHost, st_));
-        BST_CK(cudaMemcpyAsync(h_btree_, d_btree_.p, sizeof(BTreeNode) * max_tnodes_, cudaMemcpyDeviceToHost, st_));
-        HostTree t;
+        BST_CK(cudaEventRecord(sl.w0, st_));
+        BST_CK(cudaGraphLaunch(graphs_[gi], st_));
+        BST_CK(cudaEventRecord(sl.w1, st_));
+        BST_CK(cudaMemcpyAsync(sl.state, d_bstate_.p, sizeof(BState), cudaMemcpyDeviceToHost, st_));
+        BST_CK(cudaMemcpyAsync(sl.tree, d_btree_.p, sizeof(BTreeNode) * max_tnodes_, cudaMemcpyDeviceToHost, st_));
         if (cfg_.record_leaves) {
-            t.row_leaf.resize(n_);
-            BST_CK(cudaMemcpyAsync(t.row_leaf.data(), row_leaf_.p, sizeof(uint32_t) * n_, cudaMemcpyDeviceToHost, st_));
+            sl.row_leaf.resize(n_);
+            BST_CK(cudaMemcpyAsync(sl.row_leaf.data(), row_leaf_.p, sizeof(uint32_t) * n_, cudaMemcpyDeviceToHost,
+                                   st_));
         }
-        BST_CK(cudaStreamSynchronize(st_));
+        BST_CK(cudaEventRecord(sl.done, st_));
+        sl.pending = true;
+        sl.o = o;
+    }
+
+    // Waits for ring slot `si` and converts its device tree to a host tree.
+    HostTree collect_batched(uint32_t si) {
+        Slot& sl = slots_[si];
+        const uint32_t o = sl.o;
+        const size_t gi = (size_t)o * RING + si;
+        BST_CK(cudaEventSynchronize(sl.done));
         BST_CK(cudaGetLastError());
-        if (!gtimers_[o]->collect_keep()) {
+        sl.pending = false;
+        HostTree t;
+        t.group = o;
+        t.row_leaf = std::move(sl.row_leaf);
+        sl.row_leaf = {};
+        Timer& gt = *gtimers_[gi];
+        if (!gt.collect_keep()) {
             // per-phase timestamps unavailable: book the whole tree as "other"
             float ms = 0;
-            BST_CK(cudaEventElapsedTime(&ms, whole_[0], whole_[1]));
+            BST_CK(cudaEventElapsedTime(&ms, sl.w0, sl.w1));
             timer_.acc[PH_OTHER] += ms;
         }
         for (int i = 1; i < 7; ++i) {
-            timer_.acc[i] += gtimers_[o]->acc[i];
-            gtimers_[o]->acc[i] = 0.0;
+            timer_.acc[i] += gt.acc[i];
+            gt.acc[i] = 0.0;
         }
+        const BState* h_bstate_ = sl.state;
+        const BTreeNode* h_btree_ = sl.tree;
         const uint64_t rows = h_bstate_->hist_rows;
-        m_.counters.launches += graph_launches_[o];
-        m_.counters.hist_launches += graph_hist_launches_[o];
+        m_.counters.launches += graph_launches_[gi];
+        m_.counters.hist_launches += graph_hist_launches_[gi];
         m_.counters.hist_rows += rows;
-        m_.counters.hist_bytes += rows * ((uint64_t)p_.f8 + 2ull * p_.f16 + 12ull);
-        m_.counters.scan_launches += graph_hist_launches_[o];
+        m_.counters.hist_bytes += rows * ((uint64_t)p_.f8 + 2ull * p_.f16 + grad_bytes() + 4ull);
+        m_.counters.scan_launches += graph_hist_launches_[gi];
         // host tree from the device tree (grower.rs:576-650 threshold translation)
         const uint32_t nt = h_bstate_->n_tnodes;
         cat_nodes_.clear();
@@ -683,8 +906,16 @@ class Trainer {
     }
 
     void build_tiles() {
+        std::vector<LaneTile> lt;
+        std::vector<uint8_t> rest;
+        build_lane_tiles(p_, lane_tile_max_bins(qmode_), lt, lane_bins_, rest);
+        n_lane_tiles_ = (uint32_t)lt.size();
+        if (n_lane_tiles_) {
+            lane_tiles_.alloc(n_lane_tiles_);
+            BST_CK(cudaMemcpy(lane_tiles_.p, lt.data(), sizeof(LaneTile) * n_lane_tiles_, cudaMemcpyHostToDevice));
+        }
         std::vector<HistTile> tiles;
-        build_hist_tiles(p_, tiles, tile_smem_);
+        build_hist_tiles(p_, tiles, tile_smem_, &rest);
         n_tiles_ = (uint32_t)tiles.size();
         if (n_tiles_) {
             tiles_.alloc(n_tiles_);
@@ -700,28 +931,40 @@ class Trainer {
         return dst.p;
     }
 
-    // ---- histograms -----------------------------------------------------------
-    // Builds the histogram of the rows pn[node] into slot `slot` (zeroed by caller).
-    void hist_chunks_for(uint32_t slot, const PNode& pn, bool identity, std::vector<HistChunk>& out) {
-        for (uint32_t s = 0; s < pn.count; s += HIST_CHUNK_ROWS)
-            out.push_back(HistChunk{slot, pn.begin + s, std::min(HIST_CHUNK_ROWS, pn.count - s), identity ? 1u : 0u});
-    }
-
-    void launch_hist(const std::vector<HistChunk>& chunks) {
-        if (chunks.empty() || n_tiles_ == 0) return;
-        HistChunk* h = stage_.take<HistChunk>(chunks.size());
-        std::copy(chunks.begin(), chunks.end(), h);
-        upload(h, chunks.size(), d_hchunks_);
-        timer_.begin(PH_HIST);
-        launch_hist_build(d_hchunks_.p, (uint32_t)chunks.size(), tiles_.p, n_tiles_, tile_smem_, ridx_.p, gh_o_,
-                          scale_o_, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, hist_.p, slot_bins_, st_);
-        timer_.end();
+    // ---- histograms (host-driven loop) -------------------------------------------
+    // Uploads a level state (expanding nodes with their smaller children)
+    // and runs the device histogram pipeline on it.
+    void host_hist(const std::vector<BExp>& exps, bool root) {
         uint64_t rows = 0;
-        for (auto& c : chunks) rows += c.count;
-        m_.counters.launches += 1;
-        m_.counters.hist_launches += 1;
+        for (auto& e : exps) rows += e.small_count;
+        const uint32_t CH = root ? chunk_rows(n_) : chunk_rows(rows);
+        BExp* he = stage_.take<BExp>(exps.size());
+        std::vector<uint32_t> segs;
+        uint32_t nseg = 0;
+        for (size_t j = 0; j < exps.size(); ++j) {
+            he[j] = exps[j];
+            he[j].hist_off = nseg;
+            const uint32_t nch = (exps[j].small_count + CH - 1) / CH;
+            for (uint32_t q = 0; q < nch; ++q) segs.push_back((uint32_t)j);
+            nseg += nch;
+        }
+        if (nseg > d_seg_exp_.n) throw Error{BST_ERR_INVALID_ARGUMENT, "histogram segment list exceeds its buffer"};
+        BState* hs = stage_.take<BState>(1);
+        std::memset(hs, 0, sizeof(BState));
+        hs->n_exp = (uint32_t)exps.size();
+        hs->hist_chunks = nseg;
+        hs->hist_chunk = CH;
+        uint32_t* hseg = stage_.take<uint32_t>(std::max<size_t>(1, segs.size()));
+        std::copy(segs.begin(), segs.end(), hseg);
+        upload(he, exps.size(), d_bexp_);
+        upload(hs, 1, d_bstate_);
+        upload(hseg, segs.size(), d_seg_exp_);
+        uint64_t launches = 0, hist_launches = 0;
+        enqueue_hist(gr_o_, ridx_.p, root, timer_, launches, hist_launches);
+        m_.counters.launches += launches;
+        m_.counters.hist_launches += hist_launches;
         m_.counters.hist_rows += rows;
-        m_.counters.hist_bytes += rows * ((uint64_t)p_.f8 + 2ull * p_.f16 + 12ull);
+        m_.counters.hist_bytes += rows * ((uint64_t)p_.f8 + 2ull * p_.f16 + grad_bytes() + 4ull);
     }
 
     // ---- split scan ---------------------------------------------------------------
@@ -747,6 +990,10 @@ class Trainer {
 
     // Exact fixed-point sums of the rows of each node (no histogram).
     void node_sums(const std::vector<PNode>& nodes, std::vector<std::pair<long long, long long>>& out) {
+        node_sums(nodes, gr_o_, out);
+    }
+    void node_sums(const std::vector<PNode>& nodes, const GradRef& gr,
+                   std::vector<std::pair<long long, long long>>& out) {
         out.assign(nodes.size(), {0, 0});
         if (nodes.empty()) return;
         std::vector<HistChunk> ch;
@@ -759,7 +1006,7 @@ class Trainer {
             std::copy(ch.begin(), ch.end(), h);
             upload(h, ch.size(), d_schunks_);
             timer_.begin(PH_OTHER);
-            launch_node_sums(d_schunks_.p, (uint32_t)ch.size(), ridx_.p, gh_o_, scale_o_, d_sums_.p, st_);
+            launch_node_sums(d_schunks_.p, (uint32_t)ch.size(), ridx_.p, gr, d_sums_.p, st_);
             timer_.end();
             m_.counters.launches += 1;
         }
@@ -903,24 +1150,27 @@ class Trainer {
         children.reserve(2 * k);
         if (need_split && n_cols_ > 0) {
             // 2. smaller child into the right slot, then subtract (pool.rs:414-432)
-            const uint32_t r_lo = *std::min_element(right_ids.begin(), right_ids.end());
-            const uint32_t r_hi = *std::max_element(right_ids.begin(), right_ids.end());
-            BST_CK(cudaMemsetAsync(hist_.p + (size_t)r_lo * slot_bins_, 0,
-                                   sizeof(HBin) * slot_bins_ * (size_t)(r_hi - r_lo + 1), st_));
-            std::vector<HistChunk> hch;
-            FinishWork* fw = stage_.take<FinishWork>(k);
+            if (n_tiles_) {  // general tiles add atomically into zeroed right slots
+                const uint32_t r_lo = *std::min_element(right_ids.begin(), right_ids.end());
+                const uint32_t r_hi = *std::max_element(right_ids.begin(), right_ids.end());
+                BST_CK(cudaMemsetAsync(hist_.p + (size_t)r_lo * slot_bins_, 0,
+                                       sizeof(HBin) * slot_bins_ * (size_t)(r_hi - r_lo + 1), st_));
+            }
+            std::vector<BExp> exps(k);
             for (size_t j = 0; j < k; ++j) {
                 const bool left_small = lc[j] <= rc[j];  // grower.rs:398-402
                 const uint32_t small = left_small ? par[j].node : right_ids[j];
-                hist_chunks_for(right_ids[j], pn_[small], false, hch);
-                fw[j] = FinishWork{par[j].node, right_ids[j], left_small ? 1u : 0u, 0u};
+                BExp e;
+                std::memset(&e, 0, sizeof(e));
+                e.left_pnode = par[j].node;
+                e.right_pnode = right_ids[j];
+                e.lc = lc[j];
+                e.rc = rc[j];
+                e.small_begin = pn_[small].begin;
+                e.small_count = pn_[small].count;
+                exps[j] = e;
             }
-            launch_hist(hch);
-            upload(fw, k, d_finish_);
-            timer_.begin(PH_OTHER);
-            launch_hist_finish(d_finish_.p, (uint32_t)k, hist_.p, slot_bins_, p_.total_bins, st_);
-            timer_.end();
-            m_.counters.launches += 1;
+            host_hist(exps, false);
             // 3. child splits (left, right per parent)
             std::vector<ScanNode> sn;
             sn.reserve(2 * k);
@@ -959,11 +1209,39 @@ class Trainer {
         }
     }
 
+    // Quantised training: re-solve every leaf from the exact fixed-point sums
+    // of its f32 gradients (the histogram sums only chose the splits).
+    void exact_leaves(uint32_t o) {
+        stage_.reset();  // every earlier staged copy has completed (node_sums / scan synchronise)
+        std::vector<PNode> nodes;
+        std::vector<uint32_t> ids;
+        for (uint32_t pnode = 0; pnode < n_pnodes_; ++pnode)
+            if (leaf_tree_node_[pnode] != 0xFFFFFFFFu) {
+                nodes.push_back(pn_[pnode]);
+                ids.push_back(pnode);
+            }
+        std::vector<std::pair<long long, long long>> sums;
+        node_sums(nodes, gx_o_, sums);
+        const double ig = h_scales_[4 * o + 2], ih = h_scales_[4 * o + 3];
+        for (size_t j = 0; j < ids.size(); ++j) {
+            const double g = (double)sums[j].first * ig, h = (double)sums[j].second * ih;
+            const float v = leaf_weight(g, h, cfg_) * cfg_.learning_rate;
+            const uint32_t tn = leaf_tree_node_[ids[j]];
+            tree_.leaf[tn] = v;
+            tree_.cover[tn] = to_f32(h);
+            tree_.grad_sum[tn] = g;
+            tree_.hess_sum[tn] = h;
+            leaf_value_[ids[j]] = v;
+        }
+    }
+
     HostTree grow(uint32_t o) {
-        gh_o_ = gh_.p + (size_t)o * n_;
-        scale_o_ = scales_.p + 4 * (size_t)o;
-        inv_g_ = h_scales_[4 * o + 2];
-        inv_h_ = h_scales_[4 * o + 3];
+        gr_o_ = grad_ref(o);
+        gx_o_ = exact_ref(o);
+        scale_o_ = unit_scale(o);
+        const std::vector<double>& hs = qmode_ == GRAD_F32 ? h_scales_ : h_qscales_;
+        inv_g_ = hs[4 * o + 2];
+        inv_h_ = hs[4 * o + 3];
         tree_ = HostTree();
         cat_nodes_.clear();
         leaf_tree_node_.assign(max_pnodes_, 0xFFFFFFFFu);
@@ -985,10 +1263,12 @@ class Trainer {
         root.depth = 0;
         root.count = (uint32_t)n_;
         if (n_cols_ > 0) {
-            BST_CK(cudaMemsetAsync(hist_.p, 0, sizeof(HBin) * slot_bins_, st_));
-            std::vector<HistChunk> ch;
-            hist_chunks_for(0, pn_[0], true, ch);
-            launch_hist(ch);
+            if (n_tiles_) BST_CK(cudaMemsetAsync(hist_.p, 0, sizeof(HBin) * slot_bins_, st_));
+            BExp e;
+            std::memset(&e, 0, sizeof(e));
+            e.rc = (uint32_t)n_;
+            e.small_count = (uint32_t)n_;
+            host_hist({e}, true);
             std::vector<NodeSplit> res;
             scan({ScanNode{0, (uint32_t)n_, 0u, 0u, 0, 0}}, res);
             root.split = res[0];
@@ -1059,6 +1339,7 @@ class Trainer {
             }
             while (!heap.empty()) make_leaf(pop());
         }
+        if (qmode_ != GRAD_F32) exact_leaves(o);
         freeze_categories();
 
         // prediction update from the partition (grower.rs:208-219)

@@ -135,6 +135,9 @@ void predict_host(const Model& m, const HostDataset& ds, bool raw, float* out);
 void predict_device(const Model& m, const float* x_dev_sm, uint64_t n, uint64_t F, bool raw,
                     float* out_dev, cudaStream_t st);
 int transform_of(int objective);
-void build_hist_tiles(const BinPlan& p, std::vector<HistTile>& tiles, uint32_t& max_smem);
+void build_hist_tiles(const BinPlan& p, std::vector<HistTile>& tiles, uint32_t& max_smem,
+                      const std::vector<uint8_t>* only = nullptr);
+void build_lane_tiles(const BinPlan& p, uint32_t max_bins, std::vector<LaneTile>& tiles, uint32_t& tile_bins,
+                      std::vector<uint8_t>& rest);
 
 }  // namespace bst

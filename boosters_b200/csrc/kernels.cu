@@ -7,6 +7,9 @@
 // and f64 results round exactly as the Rust CPU path does.
 #include <math.h>
 
+#include <atomic>
+
+
 #include "kernels.h"
 
 namespace bst {
@@ -199,6 +202,23 @@ __global__ void k_gradients(int objective, uint32_t G, const float* __restrict__
     }
 }
 
+__global__ void k_maxabs(const float2* __restrict__ gh, uint64_t n, unsigned* __restrict__ maxabs) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t n_round = (n + 31) & ~uint64_t(31);  // warp-uniform trip count
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += stride) {
+        const float2 v = i < n ? gh[i] : make_float2(0.0f, 0.0f);
+        warp_max_atomic(&maxabs[0], v.x);
+        warp_max_atomic(&maxabs[1], v.y);
+    }
+}
+
+void launch_maxabs(const float2* gh, uint64_t n, unsigned* maxabs, cudaStream_t st) {
+    if (n == 0) return;
+    uint64_t blocks = (n + 255) / 256;
+    if (blocks > 148ull * 8) blocks = 148ull * 8;
+    k_maxabs<<<(unsigned)blocks, 256, 0, st>>>(gh, n, maxabs);
+}
+
 void launch_gradients(int objective, uint32_t G, const float* pred, const float* y,
                       const float* w, uint64_t n, float2* gh, unsigned* maxabs,
                       cudaStream_t st) {
@@ -250,27 +270,73 @@ void launch_fixed_scales(const unsigned* maxabs, uint32_t G, uint64_t n, double*
 
 constexpr int HIST_THREADS = 256;
 
+// Shared-memory words per histogram bin: 4 for the hi/lo split of the 64-bit
+// fixed-point values, 2 for quantised values (one 32-bit sum each for grad
+// and hess: a block covers <= 4096 rows of |q| <= 32767, so 4096 * 32767 <
+// 2^31 and the 32-bit sums are exact).
+__host__ __device__ constexpr uint32_t acc_words(int mode) { return mode == GRAD_F32 ? 4u : 2u; }
+
+template <int MODE>
+struct GradLoad;
+template <>
+struct GradLoad<GRAD_F32> {
+    const float2* __restrict__ gh;
+    double sg, sh;
+    __device__ explicit GradLoad(const GradRef& r) : gh(r.gh), sg(r.scale[0]), sh(r.scale[1]) {}
+    __device__ __forceinline__ void operator()(uint32_t row, long long& g, long long& h) const {
+        const float2 v = gh[row];
+        g = quantize(v.x, sg);
+        h = quantize(v.y, sh);
+    }
+};
+template <>
+struct GradLoad<GRAD_Q16> {
+    const short2* __restrict__ q;
+    __device__ explicit GradLoad(const GradRef& r) : q(static_cast<const short2*>(r.gq)) {}
+    __device__ __forceinline__ void operator()(uint32_t row, long long& g, long long& h) const {
+        const short2 v = q[row];
+        g = v.x;
+        h = v.y;
+    }
+};
+template <>
+struct GradLoad<GRAD_Q8> {
+    const char2* __restrict__ q;
+    __device__ explicit GradLoad(const GradRef& r) : q(static_cast<const char2*>(r.gq)) {}
+    __device__ __forceinline__ void operator()(uint32_t row, long long& g, long long& h) const {
+        const char2 v = q[row];
+        g = v.x;
+        h = v.y;
+    }
+};
+
+template <int MODE>
 __device__ __forceinline__ void hist_add(uint32_t* s, uint32_t S, uint32_t idx, long long qg, long long qh) {
-    const uint32_t lo_mask = (1u << HIST_LO_BITS) - 1u;
-    atomicAdd(&s[idx], (uint32_t)qg & lo_mask);
-    atomicAdd(&s[S + idx], (uint32_t)(qg >> HIST_LO_BITS));
-    atomicAdd(&s[2 * S + idx], (uint32_t)qh & lo_mask);
-    atomicAdd(&s[3 * S + idx], (uint32_t)(qh >> HIST_LO_BITS));
+    if constexpr (MODE == GRAD_F32) {
+        const uint32_t lo_mask = (1u << HIST_LO_BITS) - 1u;
+        atomicAdd(&s[idx], (uint32_t)qg & lo_mask);
+        atomicAdd(&s[S + idx], (uint32_t)(qg >> HIST_LO_BITS));
+        atomicAdd(&s[2 * S + idx], (uint32_t)qh & lo_mask);
+        atomicAdd(&s[3 * S + idx], (uint32_t)(qh >> HIST_LO_BITS));
+    } else {
+        atomicAdd(&s[idx], (uint32_t)(int32_t)qg);
+        atomicAdd(&s[S + idx], (uint32_t)(int32_t)qh);
+    }
 }
 
 // One (row chunk, column tile) item: zero the shared histogram, accumulate,
 // flush to the global histogram of chunk.slot. Block-uniform; `tile` is in
 // shared memory; returns with the shared histogram free for reuse.
+template <int MODE>
 __device__ void hist_item(const HistChunk& chunk, const HistTile& tile, uint32_t* sm, uint32_t S,
-                          const uint32_t* __restrict__ ridx, const float2* __restrict__ gh,
-                          const double* __restrict__ scale, const uint8_t* __restrict__ bins8, uint32_t s8,
-                          const uint16_t* __restrict__ bins16, uint32_t s16, HBin* __restrict__ hist,
-                          uint64_t slot_bins) {
-    for (uint32_t i = threadIdx.x; i < S; i += HIST_THREADS)  // S is a multiple of 4
+                          const uint32_t* __restrict__ ridx, const GradLoad<MODE>& load,
+                          const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16,
+                          uint32_t s16, HBin* __restrict__ hist, uint64_t slot_bins) {
+    constexpr uint32_t NW = acc_words(MODE);
+    for (uint32_t i = threadIdx.x; i < S * NW / 4; i += HIST_THREADS)  // S is a multiple of 4
         reinterpret_cast<uint4*>(sm)[i] = make_uint4(0, 0, 0, 0);
     __syncthreads();
 
-    const double sg = scale[0], sh = scale[1];
     const uint32_t c0 = tile.c0, c1 = tile.c1;
     uint32_t loff[16], lnb[16];
 #pragma unroll
@@ -285,15 +351,15 @@ __device__ void hist_item(const HistChunk& chunk, const HistTile& tile, uint32_t
         for (uint32_t i = threadIdx.x; i < count; i += HIST_THREADS) {
             const uint32_t p = chunk.begin + i;
             const uint32_t row = ident ? p : ridx[p];
-            const float2 v = gh[row];
-            const long long qg = quantize(v.x, sg), qh = quantize(v.y, sh);
+            long long qg, qh;
+            load(row, qg, qh);
             const uint4 b = *reinterpret_cast<const uint4*>(base + (size_t)row * s8);
             const uint32_t words[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
             for (int l = 0; l < 16; ++l) {
                 if (l >= (int)c0 && l < (int)c1) {
                     const uint32_t bin = (words[l >> 2] >> ((l & 3) * 8)) & 0xFFu;
-                    if (bin < lnb[l]) hist_add(sm, S, loff[l] + bin, qg, qh);
+                    if (bin < lnb[l]) hist_add<MODE>(sm, S, loff[l] + bin, qg, qh);
                 }
             }
         }
@@ -302,15 +368,15 @@ __device__ void hist_item(const HistChunk& chunk, const HistTile& tile, uint32_t
         for (uint32_t i = threadIdx.x; i < count; i += HIST_THREADS) {
             const uint32_t p = chunk.begin + i;
             const uint32_t row = ident ? p : ridx[p];
-            const float2 v = gh[row];
-            const long long qg = quantize(v.x, sg), qh = quantize(v.y, sh);
+            long long qg, qh;
+            load(row, qg, qh);
             const uint4 b = *reinterpret_cast<const uint4*>(base + (size_t)row * s16);
             const uint32_t words[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
             for (int l = 0; l < 8; ++l) {
                 if (l >= (int)c0 && l < (int)c1) {
                     const uint32_t bin = (words[l >> 1] >> ((l & 1) * 16)) & 0xFFFFu;
-                    if (bin < lnb[l]) hist_add(sm, S, loff[l] + bin, qg, qh);
+                    if (bin < lnb[l]) hist_add<MODE>(sm, S, loff[l] + bin, qg, qh);
                 }
             }
         }
@@ -321,94 +387,555 @@ __device__ void hist_item(const HistChunk& chunk, const HistTile& tile, uint32_t
         const uint32_t so = tile.lane_smem[l], go = tile.lane_hist[l], nb = tile.lane_nbins[l];
         for (uint32_t b = threadIdx.x; b < nb; b += HIST_THREADS) {
             const uint32_t j = so + b;
-            const uint32_t glo = sm[j], ghi = sm[S + j], hlo = sm[2 * S + j], hhi = sm[3 * S + j];
-            if (glo | ghi | hlo | hhi) {
-                const long long g = (long long)(int32_t)ghi * (1ll << HIST_LO_BITS) + (long long)glo;
-                const long long h = (long long)(int32_t)hhi * (1ll << HIST_LO_BITS) + (long long)hlo;
-                atomicAdd(reinterpret_cast<unsigned long long*>(&out[go + b].g), (unsigned long long)g);
-                atomicAdd(reinterpret_cast<unsigned long long*>(&out[go + b].h), (unsigned long long)h);
+            long long g, h;
+            if constexpr (MODE == GRAD_F32) {
+                const uint32_t glo = sm[j], ghi = sm[S + j], hlo = sm[2 * S + j], hhi = sm[3 * S + j];
+                if (!(glo | ghi | hlo | hhi)) continue;
+                g = (long long)(int32_t)ghi * (1ll << HIST_LO_BITS) + (long long)glo;
+                h = (long long)(int32_t)hhi * (1ll << HIST_LO_BITS) + (long long)hlo;
+            } else {
+                const uint32_t gw = sm[j], hw = sm[S + j];
+                if (!(gw | hw)) continue;
+                g = (int32_t)gw;
+                h = (int32_t)hw;
             }
+            atomicAdd(reinterpret_cast<unsigned long long*>(&out[go + b].g), (unsigned long long)g);
+            atomicAdd(reinterpret_cast<unsigned long long*>(&out[go + b].h), (unsigned long long)h);
         }
     }
     __syncthreads();
 }
 
+// ---- column-lane tiles ------------------------------------------------------
+
+// Shared histogram of a lane tile: LANE_ROWS bins x 32 slots per accumulator
+// plane (fixed height, so plane offsets are immediates).
+constexpr uint32_t LANE_ROWS = 264;
+__host__ __device__ constexpr uint32_t lane_threads(int mode) { return mode == GRAD_F32 ? 512u : 256u; }
+constexpr uint32_t LANE_PART_STRIDE = LANE_ROWS * 32u;  // partial entries per item
+constexpr uint32_t LANE_STAGES = 3;  // cp.async ring depth per warp
+constexpr uint32_t LANE_SLOT = 48;   // bytes per lane per stage (32 + 16 pad: conflict-free 16-byte reads)
+__host__ __device__ constexpr uint32_t lane_smem_bytes(int mode) {
+    return LANE_ROWS * 32u * acc_words(mode) * 4u + (lane_threads(mode) / 32u) * LANE_STAGES * 32u * LANE_SLOT;
+}
+
+uint32_t lane_tile_max_bins(int) { return LANE_ROWS; }
+
+uint32_t lane_blocks_per_sm(int mode) {
+    uint32_t b = (227u * 1024u) / (lane_smem_bytes(mode) + 1024u);
+    const uint32_t by_threads = 2048u / lane_threads(mode);
+    if (b > by_threads) b = by_threads;
+    return b ? b : 1u;
+}
+
+uint32_t lane_segment_max(int mode) { return mode == GRAD_F32 ? (uint32_t)HIST_CHUNK_MAX : 16384u; }
+uint32_t lane_part_entry_bytes(int mode) { return mode == GRAD_F32 ? 16u : 8u; }
+uint32_t lane_part_stride() { return LANE_PART_STRIDE; }
+
+template <int MODE>
+struct LaneAdd;
+template <>
+struct LaneAdd<GRAD_F32> {  // hi/lo split of the 64-bit fixed-point values
+    uint32_t glo, ghi, hlo, hhi;
+    LaneAdd() = default;
+    __device__ LaneAdd(long long qg, long long qh) {
+        const uint32_t lo_mask = (1u << HIST_LO_BITS) - 1u;
+        glo = (uint32_t)qg & lo_mask;
+        ghi = (uint32_t)(qg >> HIST_LO_BITS);
+        hlo = (uint32_t)qh & lo_mask;
+        hhi = (uint32_t)(qh >> HIST_LO_BITS);
+    }
+    __device__ __forceinline__ void add(uint32_t* sm, uint32_t plane, uint32_t idx) const {
+        atomicAdd(&sm[idx], glo);
+        atomicAdd(&sm[plane + idx], ghi);
+        atomicAdd(&sm[2 * plane + idx], hlo);
+        atomicAdd(&sm[3 * plane + idx], hhi);
+    }
+    __device__ static void read(const uint32_t* sm, uint32_t plane, uint32_t idx, long long& g, long long& h) {
+        g += (long long)(int32_t)sm[plane + idx] * (1ll << HIST_LO_BITS) + (long long)sm[idx];
+        h += (long long)(int32_t)sm[3 * plane + idx] * (1ll << HIST_LO_BITS) + (long long)sm[2 * plane + idx];
+    }
+    // 4 consecutive slots (idx % 4 == 0) added into g[4], h[4]
+    __device__ static void read4(const uint32_t* sm, uint32_t plane, uint32_t idx, long long* g, long long* h) {
+        const uint4 glo = *reinterpret_cast<const uint4*>(sm + idx);
+        const uint4 ghi = *reinterpret_cast<const uint4*>(sm + plane + idx);
+        const uint4 hlo = *reinterpret_cast<const uint4*>(sm + 2 * plane + idx);
+        const uint4 hhi = *reinterpret_cast<const uint4*>(sm + 3 * plane + idx);
+        const uint32_t gl[4] = {glo.x, glo.y, glo.z, glo.w}, gh[4] = {ghi.x, ghi.y, ghi.z, ghi.w};
+        const uint32_t hl[4] = {hlo.x, hlo.y, hlo.z, hlo.w}, hh[4] = {hhi.x, hhi.y, hhi.z, hhi.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            g[q] += (long long)(int32_t)gh[q] * (1ll << HIST_LO_BITS) + (long long)gl[q];
+            h[q] += (long long)(int32_t)hh[q] * (1ll << HIST_LO_BITS) + (long long)hl[q];
+        }
+    }
+};
+template <int MODE>
+struct LaneAdd {  // quantised: one 32-bit sum each
+    uint32_t g, h;
+    LaneAdd() = default;
+    __device__ LaneAdd(long long qg, long long qh) : g((uint32_t)(int32_t)qg), h((uint32_t)(int32_t)qh) {}
+    __device__ __forceinline__ void add(uint32_t* sm, uint32_t plane, uint32_t idx) const {
+        atomicAdd(&sm[idx], g);
+        atomicAdd(&sm[plane + idx], h);
+    }
+    __device__ static void read(const uint32_t* sm, uint32_t plane, uint32_t idx, long long& gs, long long& hs) {
+        gs += (int32_t)sm[idx];
+        hs += (int32_t)sm[plane + idx];
+    }
+    __device__ static void read4(const uint32_t* sm, uint32_t plane, uint32_t idx, long long* g, long long* h) {
+        const uint4 a = *reinterpret_cast<const uint4*>(sm + idx);
+        const uint4 b = *reinterpret_cast<const uint4*>(sm + plane + idx);
+        g[0] += (int32_t)a.x;
+        g[1] += (int32_t)a.y;
+        g[2] += (int32_t)a.z;
+        g[3] += (int32_t)a.w;
+        h[0] += (int32_t)b.x;
+        h[1] += (int32_t)b.y;
+        h[2] += (int32_t)b.z;
+        h[3] += (int32_t)b.w;
+    }
+};
+
+// Rows [first, first + count) of a row segment into this block's shared
+// histogram (zeroed by the caller). Each warp streams its rows' bin windows
+// into a LANE_STAGES-deep ring of shared-memory stages with cp.async (issued
+// LANE_STAGES - 1 iterations ahead, so the gathers overlap the atomics);
+// gradients are prefetched into registers the same distance ahead.
+template <int MODE, int ESIZE, int WORDS>
+__device__ void lane_accumulate(uint32_t first, uint32_t count, bool ident, const LaneTile& tile, uint32_t* sm,
+                                uint8_t* stage, const uint32_t* __restrict__ ridx, const GradLoad<MODE>& load,
+                                const uint8_t* __restrict__ matrix, uint32_t stride) {
+    constexpr uint32_t C = WORDS * 4 / ESIZE;  // columns in the window
+    constexpr uint32_t plane = LANE_ROWS * 32u;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t lr = lane % C, slot0 = (lane / C) * C;
+    const uint32_t rb = lr * ESIZE;  // left rotation of the window, bytes
+    const uint32_t rq = rb >> 2, rs = (rb & 3u) * 8u;
+    const uint8_t* base = matrix + tile.byte_off;
+    const uint32_t step = nwarps * 32u;
+    // this lane's slot in stage s: stage + (warp * LANE_STAGES + s) * 32 * LANE_SLOT + lane * LANE_SLOT
+    uint8_t* my = stage + (size_t)warp * LANE_STAGES * 32u * LANE_SLOT + lane * LANE_SLOT;
+    const uint32_t my_s = (uint32_t)__cvta_generic_to_shared(my);
+    auto row_at = [&](uint32_t i) -> uint32_t {
+        const uint32_t p = first + i;
+        return ident ? p : ridx[p];
+    };
+    auto issue = [&](uint32_t row, uint32_t s) {
+        const uint8_t* src = base + (size_t)row * stride;
+        const uint32_t dst = my_s + s * 32u * LANE_SLOT;
+#pragma unroll
+        for (int v = 0; v < WORDS / 4; ++v)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16u * v), "l"(src + 16 * v)
+                         : "memory");
+    };
+    const uint32_t i0 = warp * 32u + lane;
+    // prologue: iterations 0 .. LANE_STAGES - 2
+    LaneAdd<MODE> ring[LANE_STAGES];
+#pragma unroll
+    for (uint32_t k = 0; k < LANE_STAGES - 1; ++k) {
+        const uint32_t i = i0 + k * step;
+        ring[k] = LaneAdd<MODE>(0, 0);
+        if (i < count) {
+            const uint32_t row = row_at(i);
+            issue(row, k);
+            long long qg, qh;
+            load(row, qg, qh);
+            ring[k] = LaneAdd<MODE>(qg, qh);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    uint32_t row_next = 0;  // row id of iteration k + LANE_STAGES - 1
+    {
+        const uint32_t i = i0 + (LANE_STAGES - 1) * step;
+        if (i < count) row_next = row_at(i);
+    }
+    uint32_t s_cur = 0, s_new = LANE_STAGES - 1;
+    for (uint32_t k = 0; warp * 32u + k * step < count; ++k) {
+        // issue iteration k + LANE_STAGES - 1
+        {
+            const uint32_t i = i0 + (k + LANE_STAGES - 1) * step;
+            ring[LANE_STAGES - 1] = LaneAdd<MODE>(0, 0);
+            if (i < count) {
+                issue(row_next, s_new);
+                long long qg, qh;
+                load(row_next, qg, qh);
+                ring[LANE_STAGES - 1] = LaneAdd<MODE>(qg, qh);
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            const uint32_t i2 = i + step;
+            row_next = i2 < count ? row_at(i2) : 0u;
+        }
+        asm volatile("cp.async.wait_group %0;" ::"n"(LANE_STAGES - 1) : "memory");
+        const uint32_t i = i0 + k * step;
+        if (i < count) {
+            uint32_t w[WORDS];
+            const uint4* src = reinterpret_cast<const uint4*>(my + s_cur * 32u * LANE_SLOT);
+#pragma unroll
+            for (int v = 0; v < WORDS / 4; ++v) {
+                const uint4 t = src[v];
+                w[4 * v] = t.x;
+                w[4 * v + 1] = t.y;
+                w[4 * v + 2] = t.z;
+                w[4 * v + 3] = t.w;
+            }
+            // rotate left by rb bytes: whole words by rq, then bytes by rs bits
+#pragma unroll
+            for (int st = 1; st < WORDS; st <<= 1) {
+                const bool take = (rq & (uint32_t)st) != 0u;
+                uint32_t t[WORDS];
+#pragma unroll
+                for (int q = 0; q < WORDS; ++q) t[q] = take ? w[(q + st) % WORDS] : w[q];
+#pragma unroll
+                for (int q = 0; q < WORDS; ++q) w[q] = t[q];
+            }
+            {
+                uint32_t t[WORDS];
+#pragma unroll
+                for (int q = 0; q < WORDS; ++q) t[q] = __funnelshift_r(w[q], w[(q + 1) % WORDS], rs);
+#pragma unroll
+                for (int q = 0; q < WORDS; ++q) w[q] = t[q];
+            }
+            const LaneAdd<MODE> a = ring[0];
+#pragma unroll
+            for (uint32_t j = 0; j < C; ++j) {
+                uint32_t e;
+                if (ESIZE == 1)
+                    e = (w[j >> 2] >> ((j & 3u) * 8u)) & 0xFFu;
+                else
+                    e = (w[j >> 1] >> ((j & 1u) * 16u)) & 0xFFFFu;
+                a.add(sm, plane, e * 32u + slot0 + ((lr + j) & (C - 1u)));
+            }
+        }
+#pragma unroll
+        for (uint32_t q = 0; q + 1 < LANE_STAGES; ++q) ring[q] = ring[q + 1];
+        s_cur = s_cur + 1 == LANE_STAGES ? 0u : s_cur + 1;
+        s_new = s_new + 1 == LANE_STAGES ? 0u : s_new + 1;
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+template <int MODE>
+__device__ __forceinline__ void lane_accumulate_any(uint32_t first, uint32_t count, bool ident, const LaneTile& t,
+                                                    uint32_t* sm, uint8_t* stage, const uint32_t* __restrict__ ridx,
+                                                    const GradLoad<MODE>& load, const uint8_t* __restrict__ bins8,
+                                                    uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16) {
+    if (t.esize == 1) {
+        if (t.words == 8)
+            lane_accumulate<MODE, 1, 8>(first, count, ident, t, sm, stage, ridx, load, bins8, s8);
+        else
+            lane_accumulate<MODE, 1, 4>(first, count, ident, t, sm, stage, ridx, load, bins8, s8);
+    } else {
+        const uint8_t* m = reinterpret_cast<const uint8_t*>(bins16);
+        if (t.words == 8)
+            lane_accumulate<MODE, 2, 8>(first, count, ident, t, sm, stage, ridx, load, m, s16 * 2u);
+        else
+            lane_accumulate<MODE, 2, 4>(first, count, ident, t, sm, stage, ridx, load, m, s16 * 2u);
+    }
+}
+
+__device__ __forceinline__ void load_lane_tile(LaneTile& dst, const LaneTile& src) {
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(&src);
+    uint32_t* d = reinterpret_cast<uint32_t*>(&dst);
+    for (uint32_t i = threadIdx.x; i < sizeof(LaneTile) / 4u; i += blockDim.x) d[i] = s[i];
+}
+
+// ---- row-segment partial histograms and the merge ----------------------------
+// A work item is (row segment c, lane tile t): one block accumulates the
+// segment's rows for the tile's columns in shared memory, then writes the
+// tile's bins, copies summed, as partial[c * n_tiles + t][element * n_bins +
+// bin] (column-major: a column's bins are contiguous, as in the node
+// histogram) with plain stores (no global atomics: each partial has one
+// writer). k_b_merge then sums a node's partials and applies the
+// subtraction trick. Segments come from the level state: segment c belongs
+// to expanding node seg_exp[c] and covers rows small_begin + (c - hist_off) *
+// hist_chunk .. of that node's smaller child.
+
+template <int MODE>
+struct PartEntry;
+template <>
+struct PartEntry<GRAD_F32> {
+    using T = longlong2;
+    __device__ static T make(long long g, long long h) { return make_longlong2(g, h); }
+};
+template <int MODE>
+struct PartEntry {
+    using T = int2;  // per-block sums of <= 16384 quantised values fit int32
+    __device__ static T make(long long g, long long h) { return make_int2((int)g, (int)h); }
+};
+
+template <int MODE>
+__device__ void part_item(uint32_t first, uint32_t count, const LaneTile& tile, uint32_t* sm, uint8_t* stage,
+                          const uint32_t* __restrict__ ridx, const GradLoad<MODE>& load,
+                          const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16,
+                          uint32_t s16, typename PartEntry<MODE>::T* __restrict__ out) {
+    constexpr uint32_t NW = acc_words(MODE);
+    constexpr uint32_t plane = LANE_ROWS * 32u;
+    const uint32_t B = tile.n_bins;  // <= LANE_ROWS
+    for (uint32_t w = 0; w < NW; ++w)
+        for (uint32_t i = threadIdx.x; i < B * 8u; i += blockDim.x)
+            reinterpret_cast<uint4*>(sm + w * plane)[i] = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    lane_accumulate_any<MODE>(first, count, false, tile, sm, stage, ridx, load, bins8, s8, bins16, s16);
+    __syncthreads();
+    // thread -> (bin b, 4 consecutive elements c4..c4+3), copies summed
+    const uint32_t C = tile.words * 4u / tile.esize, K = 32u / C, G4 = C / 4u;
+    for (uint32_t t = threadIdx.x; t < B * G4; t += blockDim.x) {
+        const uint32_t c4 = (t % G4) * 4u, b = t / G4;
+        long long g[4] = {0, 0, 0, 0}, h[4] = {0, 0, 0, 0};
+        for (uint32_t k = 0; k < K; ++k) LaneAdd<MODE>::read4(sm, plane, b * 32u + k * C + c4, g, h);
+        // lanes t..t+G4-1 take 4 columns each of bin b: each store
+        // instruction writes runs of consecutive bins (full 32-byte sectors)
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) out[(c4 + q) * B + b] = PartEntry<MODE>::make(g[q], h[q]);
+    }
+    __syncthreads();  // shared histogram free for the next item
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(lane_threads(MODE))
+k_b_hist_part(BDev d, const LaneTile* __restrict__ tiles, uint32_t n_tiles, const uint32_t* __restrict__ ridx,
+              GradRef gr, const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16,
+              uint32_t s16, void* __restrict__ part) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);
+    uint8_t* stage = smem_raw + acc_words(MODE) * LANE_ROWS * 32u * 4u;
+    __shared__ LaneTile tile;
+    using E = typename PartEntry<MODE>::T;
+    const GradLoad<MODE> load(gr);
+    const uint32_t CH = d.state->hist_chunk;
+    const uint64_t items = (uint64_t)d.state->hist_chunks * n_tiles;
+    for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
+        const uint32_t c = (uint32_t)(it / n_tiles), t = (uint32_t)(it % n_tiles);
+        const BExp e = d.exp[d.seg_exp[c]];
+        const uint32_t start = e.small_begin + (c - e.hist_off) * CH;
+        const uint32_t count = min(CH, e.small_begin + e.small_count - start);
+        load_lane_tile(tile, tiles[t]);
+        __syncthreads();
+        part_item<MODE>(start, count, tile, sm, stage, ridx, load, bins8, s8, bins16, s16,
+                        reinterpret_cast<E*>(part) + (size_t)it * LANE_PART_STRIDE);
+    }
+}
+
+void launch_b_hist_part(const BDev& d, const LaneTile* tiles, uint32_t n_tiles, const uint32_t* ridx,
+                        const GradRef& gr, const uint8_t* bins8, uint32_t s8, const uint16_t* bins16, uint32_t s16,
+                        void* part, cudaStream_t st) {
+    if (n_tiles == 0) return;
+    init_kernel_attributes();
+    const unsigned g = 148u * lane_blocks_per_sm(gr.mode), th = lane_threads(gr.mode);
+    const size_t smem = lane_smem_bytes(gr.mode);
+    if (gr.mode == GRAD_Q16)
+        k_b_hist_part<GRAD_Q16><<<g, th, smem, st>>>(d, tiles, n_tiles, ridx, gr, bins8, s8, bins16, s16, part);
+    else if (gr.mode == GRAD_Q8)
+        k_b_hist_part<GRAD_Q8><<<g, th, smem, st>>>(d, tiles, n_tiles, ridx, gr, bins8, s8, bins16, s16, part);
+    else
+        k_b_hist_part<GRAD_F32><<<g, th, smem, st>>>(d, tiles, n_tiles, ridx, gr, bins8, s8, bins16, s16, part);
+}
+
+// The subtraction trick (pool.rs:414-432) for one global bin of node e:
+// larger = parent - smaller. The parent histogram lives in slot left_pnode,
+// which becomes the left child's; the right child's is right_pnode. root:
+// no parent, the sum goes to right_pnode.
+__device__ __forceinline__ void merge_store(HBin* __restrict__ hist, uint64_t slot_bins, const BExp& e, uint32_t gb,
+                                            HBin sm, int root) {
+    if (root) {
+        hist[(size_t)e.right_pnode * slot_bins + gb] = sm;
+        return;
+    }
+    HBin* L = hist + (size_t)e.left_pnode * slot_bins + gb;
+    HBin* R = hist + (size_t)e.right_pnode * slot_bins + gb;
+    const HBin p = *L;
+    HBin lg;
+    lg.g = p.g - sm.g;
+    lg.h = p.h - sm.h;
+    if (e.lc <= e.rc) {  // left child is the smaller (grower.rs:398-402)
+        *L = sm;
+        *R = lg;
+    } else {
+        *L = lg;
+        *R = sm;
+    }
+}
+
+// Lane-tile bins: one thread per (node, partial entry); ent[r] maps entry r
+// of a node (tiles in order, column-major inside a tile) to its global bin
+// (0xFFFFFFFF: no bin) and (tile << 16 | offset in the tile's partial
+// record). Consecutive threads read consecutive partial entries and touch
+// consecutive bins of the node histograms. Each thread handles MERGE_ILP
+// entries at once so that their dependent loads overlap.
+constexpr uint32_t MERGE_ILP = 4;
+
+template <int MODE>
+__global__ void __launch_bounds__(256, 4)
+k_b_merge(BDev d, HBin* __restrict__ hist, uint64_t slot_bins, const void* __restrict__ part, uint32_t n_tiles,
+          const uint2* __restrict__ ent, uint32_t n_ent, int root) {
+    using E = typename PartEntry<MODE>::T;
+    const E* P = reinterpret_cast<const E*>(part);
+    const uint32_t n_exp = d.state->n_exp, n_seg = d.state->hist_chunks;
+    const uint64_t n = (uint64_t)n_exp * n_ent;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const size_t rec = (size_t)n_tiles * LANE_PART_STRIDE;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += stride * MERGE_ILP) {
+        uint2 m[MERGE_ILP];
+        uint32_t j[MERGE_ILP], c0[MERGE_ILP], c1[MERGE_ILP];
+        bool ok[MERGE_ILP];
+#pragma unroll
+        for (uint32_t u = 0; u < MERGE_ILP; ++u) {
+            const uint64_t i = i0 + u * stride;
+            ok[u] = i < n;
+            j[u] = ok[u] ? (uint32_t)(i / n_ent) : 0u;
+            m[u] = ok[u] ? ent[(uint32_t)(i % n_ent)] : make_uint2(0xFFFFFFFFu, 0u);
+            c0[u] = d.exp[j[u]].hist_off;
+            c1[u] = j[u] + 1 < n_exp ? d.exp[j[u] + 1].hist_off : n_seg;
+            ok[u] = ok[u] && m[u].x != 0xFFFFFFFFu;
+        }
+        long long g[MERGE_ILP], h[MERGE_ILP];
+        HBin par[MERGE_ILP];
+#pragma unroll
+        for (uint32_t u = 0; u < MERGE_ILP; ++u) {
+            g[u] = 0;
+            h[u] = 0;
+            par[u].g = par[u].h = 0;
+            if (!ok[u]) continue;
+            if (!root) par[u] = hist[(size_t)d.exp[j[u]].left_pnode * slot_bins + m[u].x];
+            const E* p = P + (size_t)(m[u].y >> 16) * LANE_PART_STRIDE + (m[u].y & 0xFFFFu);
+            for (uint32_t c = c0[u]; c < c1[u]; ++c) {
+                const E v = p[(size_t)c * rec];
+                g[u] += v.x;
+                h[u] += v.y;
+            }
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < MERGE_ILP; ++u) {
+            if (!ok[u]) continue;
+            const BExp& e = d.exp[j[u]];
+            HBin sm;
+            sm.g = g[u];
+            sm.h = h[u];
+            if (root) {
+                hist[(size_t)e.right_pnode * slot_bins + m[u].x] = sm;
+                continue;
+            }
+            HBin lg;
+            lg.g = par[u].g - sm.g;
+            lg.h = par[u].h - sm.h;
+            const bool left_small = e.lc <= e.rc;  // grower.rs:398-402
+            hist[(size_t)e.left_pnode * slot_bins + m[u].x] = left_small ? sm : lg;
+            hist[(size_t)e.right_pnode * slot_bins + m[u].x] = left_small ? lg : sm;
+        }
+    }
+}
+
+// Bins of general tiles (built atomically into the right slot).
+__global__ void k_b_merge_rest(BDev d, HBin* __restrict__ hist, uint64_t slot_bins, uint32_t total_bins,
+                               const uint32_t* __restrict__ bin_map, int root) {
+    const uint32_t n_exp = d.state->n_exp;
+    const uint64_t n = (uint64_t)n_exp * total_bins;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = (uint32_t)(i / total_bins), gb = (uint32_t)(i % total_bins);
+        if (bin_map[gb] != 0xFFFFFFFFu) continue;
+        const BExp e = d.exp[j];
+        merge_store(hist, slot_bins, e, gb, hist[(size_t)e.right_pnode * slot_bins + gb], root);
+    }
+}
+
+void launch_b_merge(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t total_bins, const void* part,
+                    uint32_t n_lane_tiles, const uint2* ent, uint32_t n_ent, const uint32_t* bin_map, bool has_rest,
+                    int root, int mode, cudaStream_t st) {
+    const unsigned grid = 148u * 8u;
+    if (n_lane_tiles) {
+        if (mode == GRAD_F32)
+            k_b_merge<GRAD_F32><<<grid, 256, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles, ent, n_ent, root);
+        else
+            k_b_merge<GRAD_Q8><<<grid, 256, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles, ent, n_ent, root);
+    }
+    if (has_rest) k_b_merge_rest<<<grid, 256, 0, st>>>(d, hist, slot_bins, total_bins, bin_map, root);
+}
+
+// Level state for the root histogram: one "expanding node" whose smaller
+// child is all n rows (ridx is the identity), segments of `chunk` rows.
+__global__ void k_b_root_hist(BDev d, uint64_t n, uint32_t chunk) {
+    uint32_t nseg = (uint32_t)((n + chunk - 1) / chunk);
+    if (nseg > d.max_segs) nseg = d.max_segs;  // never: the buffer is sized for it
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nseg; c += gridDim.x * blockDim.x) d.seg_exp[c] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        BExp e;
+        e.front = 0;
+        e.right_pnode = 0;
+        e.tl = e.tr = 0;
+        e.lc = 0;
+        e.rc = (uint32_t)n;
+        e.small_begin = 0;
+        e.small_count = (uint32_t)n;
+        e.part_off = 0;
+        e.hist_off = 0;
+        e.left_pnode = 0;
+        e.pad1 = 0;
+        d.exp[0] = e;
+        d.state->n_exp = 1;
+        d.state->hist_chunks = nseg;
+        d.state->hist_chunk = chunk;
+    }
+}
+
+void launch_b_root_hist(const BDev& d, uint64_t n, uint32_t chunk, cudaStream_t st) {
+    k_b_root_hist<<<4, 256, 0, st>>>(d, n, chunk);
+}
+
+template <int MODE>
 __global__ void __launch_bounds__(HIST_THREADS)
 k_hist_build(const HistChunk* __restrict__ chunks, const HistTile* __restrict__ tiles,
-             const uint32_t* __restrict__ ridx, const float2* __restrict__ gh,
-             const double* __restrict__ scale, const uint8_t* __restrict__ bins8, uint32_t s8,
+             const uint32_t* __restrict__ ridx, GradRef gr, const uint8_t* __restrict__ bins8, uint32_t s8,
              const uint16_t* __restrict__ bins16, uint32_t s16, HBin* __restrict__ hist,
              uint64_t slot_bins, uint32_t n_tiles, uint32_t S) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);  // [lo_g | hi_g | lo_h | hi_h] x S
+    uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);
     __shared__ HistTile tile;
     // tiles vary fastest so the blocks of one row chunk run together and
-    // share its grad/hess and row ids in L2
+    // share its gradients and row ids in L2
     const HistChunk chunk = chunks[blockIdx.x / n_tiles];
     if (threadIdx.x == 0) tile = tiles[blockIdx.x % n_tiles];
     __syncthreads();
-    hist_item(chunk, tile, sm, S, ridx, gh, scale, bins8, s8, bins16, s16, hist, slot_bins);
+    const GradLoad<MODE> load(gr);
+    hist_item<MODE>(chunk, tile, sm, S, ridx, load, bins8, s8, bins16, s16, hist, slot_bins);
 }
 
 void launch_hist_build(const HistChunk* chunks, uint32_t n_chunks, const HistTile* tiles,
                        uint32_t n_tiles, uint32_t max_smem_bins, const uint32_t* ridx,
-                       const float2* gh, const double* scale, const uint8_t* bins8, uint32_t s8,
+                       const GradRef& gr, const uint8_t* bins8, uint32_t s8,
                        const uint16_t* bins16, uint32_t s16, HBin* hist, uint64_t slot_bins,
                        cudaStream_t st) {
     if (n_chunks == 0 || n_tiles == 0) return;
     const uint32_t S = (max_smem_bins + 3u) & ~3u;
-    const size_t smem = (size_t)S * 4u * sizeof(uint32_t);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_hist_build, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attr_set = true;
-    }
+    const size_t smem = (size_t)S * acc_words(gr.mode) * sizeof(uint32_t);
+    init_kernel_attributes();
     const uint64_t blocks = (uint64_t)n_tiles * n_chunks;
     if (blocks > 0x7FFFFFFFull) return;
-    k_hist_build<<<(unsigned)blocks, HIST_THREADS, smem, st>>>(chunks, tiles, ridx, gh, scale, bins8, s8,
-                                                              bins16, s16, hist, slot_bins, n_tiles, S);
+    const unsigned g = (unsigned)blocks;
+    if (gr.mode == GRAD_Q16)
+        k_hist_build<GRAD_Q16><<<g, HIST_THREADS, smem, st>>>(chunks, tiles, ridx, gr, bins8, s8, bins16, s16, hist,
+                                                               slot_bins, n_tiles, S);
+    else if (gr.mode == GRAD_Q8)
+        k_hist_build<GRAD_Q8><<<g, HIST_THREADS, smem, st>>>(chunks, tiles, ridx, gr, bins8, s8, bins16, s16, hist,
+                                                              slot_bins, n_tiles, S);
+    else
+        k_hist_build<GRAD_F32><<<g, HIST_THREADS, smem, st>>>(chunks, tiles, ridx, gr, bins8, s8, bins16, s16,
+                                                               hist, slot_bins, n_tiles, S);
 }
 
-__global__ void k_hist_finish(const FinishWork* __restrict__ works, HBin* __restrict__ hist,
-                              uint64_t slot_bins, uint32_t total_bins, uint32_t blocks_per_work) {
-    const uint32_t i = (blockIdx.x % blocks_per_work) * blockDim.x + threadIdx.x;
-    if (i >= total_bins) return;
-    const FinishWork w = works[blockIdx.x / blocks_per_work];
-    HBin* L = hist + (size_t)w.left * slot_bins + i;
-    HBin* R = hist + (size_t)w.right * slot_bins + i;
-    const HBin p = *L, s = *R;
-    HBin d;
-    d.g = p.g - s.g;
-    d.h = p.h - s.h;
-    if (w.flags & 1u) {  // left child was built (smaller): parent - left -> right
-        *L = s;
-        *R = d;
-    } else {
-        *L = d;
-    }
-}
-
-void launch_hist_finish(const FinishWork* w, uint32_t n_work, HBin* hist, uint64_t slot_bins,
-                        uint32_t total_bins, cudaStream_t st) {
-    if (n_work == 0 || total_bins == 0) return;
-    const uint32_t per = (total_bins + 255) / 256;
-    const uint64_t blocks = (uint64_t)per * n_work;
-    if (blocks > 0x7FFFFFFFull) return;
-    k_hist_finish<<<(unsigned)blocks, 256, 0, st>>>(w, hist, slot_bins, total_bins, per);
-}
-
-__global__ void k_node_sums(const HistChunk* __restrict__ chunks, const uint32_t* __restrict__ ridx,
-                            const float2* __restrict__ gh, const double* __restrict__ scale,
+template <int MODE>
+__global__ void k_node_sums(const HistChunk* __restrict__ chunks, const uint32_t* __restrict__ ridx, GradRef gr,
                             long long* __restrict__ sums) {
     const HistChunk c = chunks[blockIdx.x];
-    const double sg = scale[0], sh = scale[1];
+    const GradLoad<MODE> load(gr);
     long long ag = 0, ah = 0;
     for (uint32_t i = threadIdx.x; i < c.count; i += blockDim.x) {
         const uint32_t p = c.begin + i;
         const uint32_t row = (c.flags & 1u) ? p : ridx[p];
-        const float2 v = gh[row];
-        ag += quantize(v.x, sg);
-        ah += quantize(v.y, sh);
+        long long qg, qh;
+        load(row, qg, qh);
+        ag += qg;
+        ah += qh;
     }
     for (int o = 16; o > 0; o >>= 1) {
         ag += __shfl_xor_sync(FULL, ag, o);
@@ -420,10 +947,87 @@ __global__ void k_node_sums(const HistChunk* __restrict__ chunks, const uint32_t
     }
 }
 
-void launch_node_sums(const HistChunk* chunks, uint32_t n_chunks, const uint32_t* ridx,
-                      const float2* gh, const double* scale, long long* sums, cudaStream_t st) {
+void launch_node_sums(const HistChunk* chunks, uint32_t n_chunks, const uint32_t* ridx, const GradRef& gr,
+                      long long* sums, cudaStream_t st) {
     if (n_chunks == 0) return;
-    k_node_sums<<<n_chunks, 256, 0, st>>>(chunks, ridx, gh, scale, sums);
+    if (gr.mode == GRAD_Q16)
+        k_node_sums<GRAD_Q16><<<n_chunks, 256, 0, st>>>(chunks, ridx, gr, sums);
+    else if (gr.mode == GRAD_Q8)
+        k_node_sums<GRAD_Q8><<<n_chunks, 256, 0, st>>>(chunks, ridx, gr, sums);
+    else
+        k_node_sums<GRAD_F32><<<n_chunks, 256, 0, st>>>(chunks, ridx, gr, sums);
+}
+
+// ============================================================================
+// Quantised gradients (int16 / int8 training mode; no counterpart in the
+// reference). Philox4x32-10 as published by Salmon, Moraes, Dror and Shaw,
+// "Parallel Random Numbers: As Easy as 1, 2, 3" (SC 2011), gives each
+// (row, output, round) two uniform words; q = floor(v * Q / max|v| + u).
+// ============================================================================
+
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+        const uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += W0;
+        k.y += W1;
+    }
+    return c;
+}
+
+__device__ __forceinline__ int32_t stochastic_round(float v, double inv, uint32_t r, int32_t Q) {
+    const double u = (double)r * 0x1p-32;
+    double x = (double)v * inv;
+    x = x + u;
+    double f = floor(x);
+    if (!(f >= (double)-Q)) f = (double)-Q;
+    if (f > (double)Q) f = (double)Q;
+    return (int32_t)f;
+}
+
+template <int MODE>
+__global__ void k_quantize(const float2* __restrict__ gh, uint64_t n, uint32_t G, const unsigned* __restrict__ maxabs,
+                           uint2 key, uint32_t round, uint32_t out0, void* __restrict__ gq,
+                           double* __restrict__ qscales) {
+    constexpr int32_t Q = MODE == GRAD_Q8 ? 127 : 32767;
+    const uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i0 < 2ull * G) {
+        const float m = __uint_as_float(maxabs[i0]);
+        const uint32_t o = (uint32_t)(i0 >> 1), which = (uint32_t)(i0 & 1);
+        qscales[4 * o + which] = m > 0.0f ? (double)Q / (double)m : 0.0;
+        qscales[4 * o + 2 + which] = m > 0.0f ? (double)m / (double)Q : 0.0;
+    }
+    const uint64_t total = n * G;
+    for (uint64_t i = i0; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t o = (uint32_t)(i / n), row = (uint32_t)(i % n);
+        const float mg = __uint_as_float(maxabs[2 * o]), mh = __uint_as_float(maxabs[2 * o + 1]);
+        const double ig = mg > 0.0f ? (double)Q / (double)mg : 0.0;
+        const double ih = mh > 0.0f ? (double)Q / (double)mh : 0.0;
+        const uint4 r = philox4x32_10(make_uint4(row, out0 + o, round, QUANT_STREAM), key);
+        const float2 v = gh[i];
+        const int32_t qg = stochastic_round(v.x, ig, r.x, Q), qh = stochastic_round(v.y, ih, r.y, Q);
+        if constexpr (MODE == GRAD_Q8)
+            static_cast<char2*>(gq)[i] = make_char2((signed char)qg, (signed char)qh);
+        else
+            static_cast<short2*>(gq)[i] = make_short2((short)qg, (short)qh);
+    }
+}
+
+void launch_quantize(int mode, uint32_t G, const float2* gh, uint64_t n, const unsigned* maxabs, uint64_t seed,
+                     uint32_t round, uint32_t out0, void* gq, double* qscales, cudaStream_t st) {
+    if (G == 0) return;
+    const uint64_t total = n * G;
+    uint64_t blocks = (total + 255) / 256;
+    if (blocks > 148ull * 16) blocks = 148ull * 16;
+    if (blocks == 0) blocks = 1;
+    const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+    if (mode == GRAD_Q8)
+        k_quantize<GRAD_Q8><<<(unsigned)blocks, 256, 0, st>>>(gh, n, G, maxabs, key, round, out0, gq, qscales);
+    else
+        k_quantize<GRAD_Q16><<<(unsigned)blocks, 256, 0, st>>>(gh, n, G, maxabs, key, round, out0, gq, qscales);
 }
 
 // ============================================================================
@@ -784,49 +1388,97 @@ void launch_split_reduce(const ColCand* cand, const long long* node_tot, uint32_
 // Left rows fill the node's range from the front, right rows from the back.
 // ============================================================================
 
-__global__ void k_partition(const PartWork* __restrict__ works, const PartChunk* __restrict__ chunks,
-                            const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp,
-                            unsigned* __restrict__ cursors, const uint8_t* __restrict__ bins8,
-                            uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16) {
+namespace {
+
+constexpr int PART_THREADS = 256;  // 8 warps
+constexpr int PART_PER = 8;        // rows per thread per pass: 2048-row passes
+
+__device__ __forceinline__ bool part_left(const PartWork& w, uint32_t bin) {
+    if ((w.flags & 2u) && bin == w.default_bin) return (w.flags & 1u) != 0;
+    if (w.flags & 4u) return bin < 256 && ((w.cats[bin >> 6] >> (bin & 63)) & 1ull);
+    return bin <= w.thr_bin;
+}
+
+// Rows ridx[start, start + len) of one node into tmp: left rows at the left
+// cursor cur[0] (growing), right rows below the right cursor cur[1]
+// (shrinking). Ranks come from a block-wide scan of ballots, so each
+// 2048-row pass takes one atomic per side (same-address atomics from every
+// warp serialise in L2). Block-uniform; blockDim.x == PART_THREADS.
+__device__ void part_rows(const PartWork& w, uint32_t start, uint32_t len, unsigned* cur,
+                          const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp,
+                          const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16,
+                          uint32_t s16) {
+    __shared__ uint32_t s_l[PART_PER][PART_THREADS / 32], s_r[PART_PER][PART_THREADS / 32];
+    __shared__ uint32_t s_base[2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    for (uint32_t b0 = 0; b0 < len; b0 += PART_THREADS * PART_PER) {
+        uint32_t rows[PART_PER], bins[PART_PER];
+        unsigned lm[PART_PER], rm[PART_PER];
+#pragma unroll
+        for (int k = 0; k < PART_PER; ++k) {
+            const uint32_t i = b0 + k * PART_THREADS + threadIdx.x;
+            rows[k] = i < len ? ridx[start + i] : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < PART_PER; ++k) {
+            const uint32_t i = b0 + k * PART_THREADS + threadIdx.x;
+            bins[k] = 0u;
+            if (i < len)
+                bins[k] = w.matrix == 0 ? (uint32_t)bins8[(size_t)rows[k] * s8 + w.pos]
+                                        : (uint32_t)bins16[(size_t)rows[k] * s16 + w.pos];
+        }
+#pragma unroll
+        for (int k = 0; k < PART_PER; ++k) {
+            const uint32_t i = b0 + k * PART_THREADS + threadIdx.x;
+            const bool ok = i < len;
+            const unsigned act = __ballot_sync(FULL, ok);
+            lm[k] = __ballot_sync(FULL, ok && part_left(w, bins[k]));
+            rm[k] = act & ~lm[k];
+            if (lane == 0) {
+                s_l[k][warp] = (uint32_t)__popc(lm[k]);
+                s_r[k][warp] = (uint32_t)__popc(rm[k]);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t L = 0, R = 0;
+            for (int k = 0; k < PART_PER; ++k)
+                for (int q = 0; q < PART_THREADS / 32; ++q) {
+                    const uint32_t a = s_l[k][q], c = s_r[k][q];
+                    s_l[k][q] = L;
+                    s_r[k][q] = R;
+                    L += a;
+                    R += c;
+                }
+            s_base[0] = L ? atomicAdd(&cur[0], L) : 0u;
+            s_base[1] = R ? atomicSub(&cur[1], R) - R : 0u;
+        }
+        __syncthreads();
+        const uint32_t lb = s_base[0], rbs = s_base[1];
+#pragma unroll
+        for (int k = 0; k < PART_PER; ++k) {
+            const unsigned bit = 1u << lane;
+            if (lm[k] & bit)
+                tmp[lb + s_l[k][warp] + __popc(lm[k] & lt)] = rows[k];
+            else if (rm[k] & bit)
+                tmp[rbs + s_r[k][warp] + __popc(rm[k] & lt)] = rows[k];
+        }
+        __syncthreads();  // s_l / s_r / s_base are reused by the next pass
+    }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(PART_THREADS)
+k_partition(const PartWork* __restrict__ works, const PartChunk* __restrict__ chunks,
+            const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp, unsigned* __restrict__ cursors,
+            const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16) {
     const PartChunk ch = chunks[blockIdx.x];
     __shared__ PartWork w;
     if (threadIdx.x == 0) w = works[ch.work];
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    for (uint32_t base = 0; base < ch.len; base += blockDim.x) {
-        const uint32_t i = base + threadIdx.x;
-        const bool ok = i < ch.len;
-        uint32_t row = 0;
-        bool left = false;
-        if (ok) {
-            row = ridx[ch.start + i];
-            const uint32_t bin = w.matrix == 0 ? (uint32_t)bins8[(size_t)row * s8 + w.pos]
-                                               : (uint32_t)bins16[(size_t)row * s16 + w.pos];
-            if ((w.flags & 2u) && bin == w.default_bin)
-                left = (w.flags & 1u) != 0;
-            else if (w.flags & 4u)
-                left = bin < 256 && ((w.cats[bin >> 6] >> (bin & 63)) & 1ull);
-            else
-                left = bin <= w.thr_bin;
-        }
-        const unsigned act = __ballot_sync(FULL, ok);
-        const unsigned lm = __ballot_sync(FULL, ok && left);
-        const unsigned rm = act & ~lm;
-        unsigned lbase = 0, rbase = 0;
-        if (lane == 0) {
-            if (lm) lbase = atomicAdd(&cursors[2 * ch.work], (unsigned)__popc(lm));
-            if (rm) rbase = atomicSub(&cursors[2 * ch.work + 1], (unsigned)__popc(rm)) - (unsigned)__popc(rm);
-        }
-        lbase = __shfl_sync(FULL, lbase, 0);
-        rbase = __shfl_sync(FULL, rbase, 0);
-        if (ok) {
-            if (left)
-                tmp[lbase + __popc(lm & lt)] = row;
-            else
-                tmp[rbase + __popc(rm & lt)] = row;
-        }
-    }
+    part_rows(w, ch.start, ch.len, cursors + 2 * ch.work, ridx, tmp, bins8, s8, bins16, s16);
 }
 
 void launch_partition(const PartWork* works, const PartChunk* chunks, uint32_t n_chunks,
@@ -834,7 +1486,7 @@ void launch_partition(const PartWork* works, const PartChunk* chunks, uint32_t n
                       const uint8_t* bins8, uint32_t s8, const uint16_t* bins16, uint32_t s16,
                       cudaStream_t st) {
     if (n_chunks == 0) return;
-    k_partition<<<n_chunks, 256, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16, s16);
+    k_partition<<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16, s16);
 }
 
 __global__ void k_copy_chunks(const PartChunk* __restrict__ chunks, const uint32_t* __restrict__ src,
@@ -964,12 +1616,6 @@ __device__ __forceinline__ uint32_t last_le(uint32_t n, uint32_t c, F key) {
     return lo;
 }
 
-__device__ __forceinline__ bool goes_left(const PartWork& w, uint32_t bin) {
-    if ((w.flags & 2u) && bin == w.default_bin) return (w.flags & 1u) != 0;
-    if (w.flags & 4u) return bin < 256 && ((w.cats[bin >> 6] >> (bin & 63)) & 1ull);
-    return bin <= w.thr_bin;
-}
-
 __device__ void write_leaf(BTreeNode& t, long long G, long long H, const double* scale, float v) {
     t.col = 0;
     t.bin = 0;
@@ -1012,41 +1658,23 @@ __global__ void k_b_root(BDev d, uint64_t n) {
     s.n_leaves = 0;
     s.leaf_chunks = 0;
     s.first_right = 1;
-    s.pad = 0;
+    s.hist_chunk = HIST_CHUNK_MAX;
     s.hist_rows = n;
-    s.pad2[0] = s.pad2[1] = s.pad2[2] = s.pad2[3] = 0;
+    s.done = 0;
+    s.pad2[0] = s.pad2[1] = s.pad2[2] = 0;
     *d.state = s;
 }
 
 void launch_b_root(const BDev& d, uint64_t n, cudaStream_t st) { k_b_root<<<1, 32, 0, st>>>(d, n); }
 
-__global__ void k_b_hist(BDev d, const HistTile* __restrict__ tiles, uint32_t n_tiles, uint32_t S,
-                         const uint32_t* __restrict__ ridx, const float2* __restrict__ gh,
-                         const double* __restrict__ scale, const uint8_t* __restrict__ bins8, uint32_t s8,
-                         const uint16_t* __restrict__ bins16, uint32_t s16, HBin* __restrict__ hist,
-                         uint64_t slot_bins);
 
-void init_kernel_attributes() {
-    cudaFuncSetAttribute(k_hist_build, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_b_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_bin_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-}
-
-__global__ void k_b_root_set(BDev d, const NodeSplit* __restrict__ rs) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const NodeSplit s = *rs;
-    BNode& r = d.front[0][0];
-    r.split = s;
-    r.G = s.tot_g;
-    r.H = s.tot_h;
-}
-
-void launch_b_root_set(const BDev& d, const NodeSplit* rs, cudaStream_t st) { k_b_root_set<<<1, 32, 0, st>>>(d, rs); }
 
 // Expansion decisions of one level (grower.rs:353-372, 530-539): leaves for
 // the rest, right-child ids in frontier order (partition.rs:375), tree nodes
 // in allocation order (mutable_tree.rs:105-164), partition work lists.
-__global__ void __launch_bounds__(1024) k_b_decide(BDev d, int a, LeafParams lp, const double* __restrict__ scale) {
+// buf: which row-index buffer holds the rows of this level's nodes (the
+// leaves made here keep their rows there).
+__device__ void decide_body(BDev d, int a, LeafParams lp, const double* __restrict__ scale, uint32_t buf) {
     __shared__ uint32_t sh[33];
     __shared__ uint32_t base_exp, base_leaf, base_chunk, first_right, tn0, nf;
     BState* s = d.state;
@@ -1081,7 +1709,7 @@ __global__ void __launch_bounds__(1024) k_b_decide(BDev d, int a, LeafParams lp,
             lf.value = v;
             lf.tnode = nd.tnode;
             lf.chunk_off = 0;
-            lf.pad = 0;
+            lf.buf = buf;
             d.leaves[base_leaf + jl] = lf;
         }
         if (ex) {
@@ -1110,7 +1738,8 @@ __global__ void __launch_bounds__(1024) k_b_decide(BDev d, int a, LeafParams lp,
             e.lc = e.rc = e.small_begin = e.small_count = 0;
             e.part_off = base_chunk + jc;
             e.hist_off = 0;
-            e.pad0 = e.pad1 = 0;
+            e.left_pnode = nd.pnode;
+            e.pad1 = 0;
             d.exp[j] = e;
             PartWork w;
             w.begin = nd.begin;
@@ -1144,90 +1773,88 @@ __global__ void __launch_bounds__(1024) k_b_decide(BDev d, int a, LeafParams lp,
     }
 }
 
-void launch_b_decide(const BDev& d, int a, LeafParams lp, const double* scale, cudaStream_t st) {
-    k_b_decide<<<1, 1024, 0, st>>>(d, a, lp, scale);
+__global__ void __launch_bounds__(1024) k_b_decide(BDev d, int a, LeafParams lp, const double* __restrict__ scale,
+                                                  uint32_t buf) {
+    decide_body(d, a, lp, scale, buf);
 }
 
-// Partition of every expanding node (partition.rs:296-382); 2048-row chunks,
-// loads issued ahead of the ballots for memory-level parallelism.
-__global__ void __launch_bounds__(256)
-k_b_partition(BDev d, const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp,
-              const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16) {
-    constexpr int PER = B_PART_CHUNK / 256;
-    const uint32_t total = d.state->part_chunks, n_exp = d.state->n_exp;
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
-        const uint32_t j = last_le(n_exp, c, [&](uint32_t k) { return d.exp[k].part_off; });
-        const PartWork w = d.pworks[j];
-        const uint32_t start = w.begin + (c - d.exp[j].part_off) * B_PART_CHUNK;
-        const uint32_t end = w.begin + w.count;
-        const uint32_t len = min(B_PART_CHUNK, end - start);
-        uint32_t rows[PER], bins[PER];
-#pragma unroll
-        for (int k = 0; k < PER; ++k) {
-            const uint32_t i = k * 256 + threadIdx.x;
-            rows[k] = i < len ? ridx[start + i] : 0u;
-        }
-#pragma unroll
-        for (int k = 0; k < PER; ++k) {
-            const uint32_t i = k * 256 + threadIdx.x;
-            bins[k] = 0u;
-            if (i < len)
-                bins[k] = w.matrix == 0 ? (uint32_t)bins8[(size_t)rows[k] * s8 + w.pos]
-                                        : (uint32_t)bins16[(size_t)rows[k] * s16 + w.pos];
-        }
-#pragma unroll
-        for (int k = 0; k < PER; ++k) {
-            const uint32_t i = k * 256 + threadIdx.x;
-            const bool ok = i < len;
-            const bool left = ok && goes_left(w, bins[k]);
-            const unsigned act = __ballot_sync(FULL, ok);
-            const unsigned lm = __ballot_sync(FULL, left);
-            const unsigned rm = act & ~lm;
-            unsigned lbase = 0, rbase = 0;
-            if (lane == 0) {
-                if (lm) lbase = atomicAdd(&d.cursors[2 * j], (unsigned)__popc(lm));
-                if (rm) rbase = atomicSub(&d.cursors[2 * j + 1], (unsigned)__popc(rm)) - (unsigned)__popc(rm);
-            }
-            lbase = __shfl_sync(FULL, lbase, 0);
-            rbase = __shfl_sync(FULL, rbase, 0);
-            if (ok) {
-                if (left)
-                    tmp[lbase + __popc(lm & lt)] = rows[k];
-                else
-                    tmp[rbase + __popc(rm & lt)] = rows[k];
-            }
-        }
+void launch_b_decide(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st) {
+    k_b_decide<<<1, 1024, 0, st>>>(d, a, lp, scale, buf);
+}
+
+// Root split into the frontier, then the level-0 decisions.
+__global__ void __launch_bounds__(1024) k_b_root_set(BDev d, const NodeSplit* __restrict__ rs, LeafParams lp,
+                                                    const double* __restrict__ scale) {
+    if (threadIdx.x == 0) {
+        const NodeSplit s = *rs;
+        BNode& r = d.front[0][0];
+        r.split = s;
+        r.G = s.tot_g;
+        r.H = s.tot_h;
     }
+    __syncthreads();
+    decide_body(d, 0, lp, scale, 0u);
 }
 
-void launch_b_partition(const BDev& d, const uint32_t* ridx, uint32_t* tmp, const uint8_t* bins8, uint32_t s8,
-                        const uint16_t* bins16, uint32_t s16, uint32_t grid, cudaStream_t st) {
-    k_b_partition<<<grid, 256, 0, st>>>(d, ridx, tmp, bins8, s8, bins16, s16);
+void launch_b_root_set(const BDev& d, const NodeSplit* rs, LeafParams lp, const double* scale, cudaStream_t st) {
+    k_b_root_set<<<1, 1024, 0, st>>>(d, rs, lp, scale);
 }
 
-__global__ void k_b_copy(BDev d, const uint32_t* __restrict__ tmp, uint32_t* __restrict__ ridx) {
+// "Last block" hand-off: every block of the launch counts itself in
+// state->done after a fence; the block that completes the count returns true
+// (with the count reset) and may read everything the others wrote.
+__device__ bool last_block(BState* s) {
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(&s->done, 1u) == gridDim.x - 1u;
+        if (last) s->done = 0u;
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+__device__ void children_body(BDev d, int a, int need_split);
+
+// Partition of every expanding node (partition.rs:296-382) over 2048-row
+// chunks (one atomic per side per chunk, part_rows) from row-index buffer
+// rin into rout; the last block then derives the children (children_body).
+__global__ void __launch_bounds__(PART_THREADS)
+k_b_partition(BDev d, const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp,
+              const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16,
+              int a, int need_split) {
+    __shared__ PartWork w;
+    __shared__ uint32_t s_j;
     const uint32_t total = d.state->part_chunks, n_exp = d.state->n_exp;
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
-        const uint32_t j = last_le(n_exp, c, [&](uint32_t k) { return d.exp[k].part_off; });
-        const PartWork w = d.pworks[j];
+        if (threadIdx.x == 0) {
+            const uint32_t j = last_le(n_exp, c, [&](uint32_t k) { return d.exp[k].part_off; });
+            s_j = j;
+            w = d.pworks[j];
+        }
+        __syncthreads();
+        const uint32_t j = s_j;
         const uint32_t start = w.begin + (c - d.exp[j].part_off) * B_PART_CHUNK;
         const uint32_t len = min(B_PART_CHUNK, w.begin + w.count - start);
-        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) ridx[start + i] = tmp[start + i];
+        part_rows(w, start, len, d.cursors + 2 * j, ridx, tmp, bins8, s8, bins16, s16);
     }
+    if (last_block(d.state)) children_body(d, a, need_split);
 }
 
-void launch_b_copy(const BDev& d, const uint32_t* tmp, uint32_t* ridx, uint32_t grid, cudaStream_t st) {
-    k_b_copy<<<grid, 256, 0, st>>>(d, tmp, ridx);
+void launch_b_partition(const BDev& d, const uint32_t* rin, uint32_t* rout, const uint8_t* bins8, uint32_t s8,
+                        const uint16_t* bins16, uint32_t s16, int a, int need_split, uint32_t grid,
+                        cudaStream_t st) {
+    k_b_partition<<<grid, PART_THREADS, 0, st>>>(d, rin, rout, bins8, s8, bins16, s16, a, need_split);
 }
 
 // Children of every split: ranges from the partition cursors, smaller child
 // (grower.rs:398-402), next frontier in (left, right) order, histogram or
 // node-sum work over the smaller children.
-__global__ void __launch_bounds__(1024) k_b_children(BDev d, int a, int need_split) {
+__device__ void children_body(BDev d, int a, int need_split) {
     __shared__ uint32_t sh[33];
-    __shared__ uint32_t base, n_exp;
+    __shared__ uint32_t base, n_exp, chunk;
     __shared__ unsigned long long rows;
     BState* s = d.state;
     if (threadIdx.x == 0) {
@@ -1241,7 +1868,6 @@ __global__ void __launch_bounds__(1024) k_b_children(BDev d, int a, int need_spl
     for (uint32_t j0 = 0; j0 < n_exp; j0 += blockDim.x) {
         const uint32_t j = j0 + threadIdx.x;
         const bool valid = j < n_exp;
-        uint32_t nch = 0;
         if (valid) {
             BExp e = d.exp[j];
             const BNode nd = A[e.front];
@@ -1269,30 +1895,52 @@ __global__ void __launch_bounds__(1024) k_b_children(BDev d, int a, int need_spl
             l.split.tot_g = l.split.tot_h = r.split.tot_g = r.split.tot_h = 0;
             B[2 * j] = l;
             B[2 * j + 1] = r;
-            d.finish[j] = FinishWork{nd.pnode, e.right_pnode, left_small ? 1u : 0u, 0u};
             d.scan_nodes[2 * j] = ScanNode{nd.pnode, lc, 0u, 0u, 0, 0};
             d.scan_nodes[2 * j + 1] = ScanNode{e.right_pnode, rc, 0u, 0u, 0, 0};
-            nch = (e.small_count + HIST_CHUNK_MAX - 1) / HIST_CHUNK_MAX;
             d.exp[j] = e;
-            if (need_split) atomicAdd(&rows, (unsigned long long)e.small_count);
+            atomicAdd(&rows, (unsigned long long)e.small_count);
         }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // rows per histogram row segment: about hist_target segments (a
+        // multiple of 256 rows in [1024, hist_seg_max]), so that the
+        // persistent histogram launch has a few equal items per block; node
+        // sums (last level) use HIST_CHUNK_MAX-row chunks
+        uint32_t c = HIST_CHUNK_MAX;
+        if (need_split) {
+            const uint32_t tgt = d.hist_target ? d.hist_target : 1u;
+            unsigned long long want = (rows + tgt - 1) / tgt;
+            want = (want + 255ull) & ~255ull;
+            c = (uint32_t)(want < 1024ull ? 1024ull : (want > d.hist_seg_max ? d.hist_seg_max : want));
+        }
+        chunk = c;
+    }
+    __syncthreads();
+    for (uint32_t j0 = 0; j0 < n_exp; j0 += blockDim.x) {
+        const uint32_t j = j0 + threadIdx.x;
+        const bool valid = j < n_exp;
+        const uint32_t nch = valid ? (d.exp[j].small_count + chunk - 1) / chunk : 0u;
         uint32_t tc;
         const uint32_t jc = block_excl_scan(nch, sh, &tc);
-        if (valid) d.exp[j].hist_off = base + jc;
+        if (valid) {
+            d.exp[j].hist_off = base + jc;
+            for (uint32_t q = 0; q < nch; ++q)  // segment -> expansion (the buffer bound always holds)
+                if (base + jc + q < d.max_segs) d.seg_exp[base + jc + q] = j;
+        }
         __syncthreads();
         if (threadIdx.x == 0) base += tc;
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        s->hist_chunks = base;
+        s->hist_chunks = base < d.max_segs ? base : d.max_segs;
+        s->hist_chunk = chunk;
         s->n_front = 2 * n_exp;
-        s->hist_rows += rows;
+        if (need_split) s->hist_rows += rows;
     }
 }
 
-void launch_b_children(const BDev& d, int a, int need_split, cudaStream_t st) {
-    k_b_children<<<1, 1024, 0, st>>>(d, a, need_split);
-}
+
 
 __global__ void k_b_zero_right(BDev d, HBin* __restrict__ hist, uint64_t slot_bins) {
     const uint64_t n = (uint64_t)d.state->n_exp * slot_bins;
@@ -1306,71 +1954,55 @@ void launch_b_zero_right(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t
 }
 
 // Histograms of all smaller children of the level (one persistent launch).
+template <int MODE>
 __global__ void __launch_bounds__(HIST_THREADS)
 k_b_hist(BDev d, const HistTile* __restrict__ tiles, uint32_t n_tiles, uint32_t S, const uint32_t* __restrict__ ridx,
-         const float2* __restrict__ gh, const double* __restrict__ scale, const uint8_t* __restrict__ bins8,
-         uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16, HBin* __restrict__ hist, uint64_t slot_bins) {
+         GradRef gr, const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16,
+         HBin* __restrict__ hist, uint64_t slot_bins) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);
     __shared__ HistTile tile;
-    const uint32_t n_exp = d.state->n_exp;
+    const GradLoad<MODE> load(gr);
+    const uint32_t n_exp = d.state->n_exp, CH = d.state->hist_chunk;
     const uint64_t items = (uint64_t)d.state->hist_chunks * n_tiles;
     for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
         const uint32_t c = (uint32_t)(it / n_tiles), t = (uint32_t)(it % n_tiles);
-        const uint32_t j = last_le(n_exp, c, [&](uint32_t k) { return d.exp[k].hist_off; });
+        const uint32_t j = d.seg_exp[c];
         const BExp e = d.exp[j];
-        const uint32_t start = e.small_begin + (c - e.hist_off) * HIST_CHUNK_MAX;
-        HistChunk ch;
-        ch.slot = e.right_pnode;
-        ch.begin = start;
-        ch.count = min((uint32_t)HIST_CHUNK_MAX, e.small_begin + e.small_count - start);
-        ch.flags = 0u;
+        const uint32_t start = e.small_begin + (c - e.hist_off) * CH;
+        const uint32_t seg_count = min(CH, e.small_begin + e.small_count - start);
         if (threadIdx.x == 0) tile = tiles[t];
         __syncthreads();
-        hist_item(ch, tile, sm, S, ridx, gh, scale, bins8, s8, bins16, s16, hist, slot_bins);
-    }
-}
-
-void launch_b_hist(const BDev& d, const HistTile* tiles, uint32_t n_tiles, uint32_t max_smem_bins,
-                   const uint32_t* ridx, const float2* gh, const double* scale, const uint8_t* bins8,
-                   uint32_t s8, const uint16_t* bins16, uint32_t s16, HBin* hist, uint64_t slot_bins,
-                   uint32_t grid, cudaStream_t st) {
-    if (n_tiles == 0) return;
-    const uint32_t S = (max_smem_bins + 3u) & ~3u;
-    const size_t smem = (size_t)S * 4u * sizeof(uint32_t);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_b_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attr_set = true;
-    }
-    k_b_hist<<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gh, scale, bins8, s8, bins16, s16, hist,
-                                                slot_bins);
-}
-
-__global__ void k_b_finish(BDev d, HBin* __restrict__ hist, uint64_t slot_bins, uint32_t total_bins) {
-    const uint64_t n = (uint64_t)d.state->n_exp * total_bins;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t j = (uint32_t)(i / total_bins), b = (uint32_t)(i % total_bins);
-        const FinishWork w = d.finish[j];
-        HBin* L = hist + (size_t)w.left * slot_bins + b;
-        HBin* R = hist + (size_t)w.right * slot_bins + b;
-        const HBin p = *L, s = *R;
-        HBin df;
-        df.g = p.g - s.g;
-        df.h = p.h - s.h;
-        if (w.flags & 1u) {
-            *L = s;
-            *R = df;
-        } else {
-            *L = df;
+        for (uint32_t off = 0; off < seg_count; off += HIST_CHUNK_MAX) {  // block-uniform
+            HistChunk ch;
+            ch.slot = e.right_pnode;
+            ch.begin = start + off;
+            ch.count = min((uint32_t)HIST_CHUNK_MAX, seg_count - off);
+            ch.flags = 0u;
+            hist_item<MODE>(ch, tile, sm, S, ridx, load, bins8, s8, bins16, s16, hist, slot_bins);
         }
     }
 }
 
-void launch_b_finish(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t total_bins, uint32_t grid,
-                     cudaStream_t st) {
-    k_b_finish<<<grid, 256, 0, st>>>(d, hist, slot_bins, total_bins);
+void launch_b_hist(const BDev& d, const HistTile* tiles, uint32_t n_tiles, uint32_t max_smem_bins,
+                   const uint32_t* ridx, const GradRef& gr, const uint8_t* bins8, uint32_t s8,
+                   const uint16_t* bins16, uint32_t s16, HBin* hist, uint64_t slot_bins, uint32_t grid,
+                   cudaStream_t st) {
+    if (n_tiles == 0) return;
+    const uint32_t S = (max_smem_bins + 3u) & ~3u;
+    const size_t smem = (size_t)S * acc_words(gr.mode) * sizeof(uint32_t);
+    init_kernel_attributes();
+    if (gr.mode == GRAD_Q16)
+        k_b_hist<GRAD_Q16><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16, s16,
+                                                              hist, slot_bins);
+    else if (gr.mode == GRAD_Q8)
+        k_b_hist<GRAD_Q8><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16, s16,
+                                                             hist, slot_bins);
+    else
+        k_b_hist<GRAD_F32><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16, s16,
+                                                              hist, slot_bins);
 }
+
 
 __global__ void __launch_bounds__(SCAN_WARPS * 32)
 k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HBin* __restrict__ hist,
@@ -1399,7 +2031,8 @@ void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const
 
 // Reduction over columns (find.rs:180-270) straight into the next frontier.
 __global__ void k_b_reduce(BDev d, int b, const ColCand* __restrict__ cand, const long long* __restrict__ node_tot,
-                           uint32_t n_cols, int last_wins) {
+                           uint32_t n_cols, int last_wins, int decide, LeafParams lp,
+                           const double* __restrict__ scale, uint32_t buf) {
     const uint32_t n_nodes = 2 * d.state->n_exp;
     BNode* B = d.front[b];
     const int lane = threadIdx.x;
@@ -1455,28 +2088,32 @@ __global__ void k_b_reduce(BDev d, int b, const ColCand* __restrict__ cand, cons
             B[node].H = s.tot_h;
         }
     }
+    // the next level's decisions once every node of the frontier is final
+    if (decide && last_block(d.state)) decide_body(d, b, lp, scale, buf);
 }
 
 void launch_b_reduce(const BDev& d, int b, const ColCand* cand, const long long* node_tot, uint32_t n_cols,
-                     int last_wins, uint32_t grid, cudaStream_t st) {
-    k_b_reduce<<<grid, 32, 0, st>>>(d, b, cand, node_tot, n_cols, last_wins);
+                     int last_wins, int decide, LeafParams lp, const double* scale, uint32_t buf, uint32_t grid,
+                     cudaStream_t st) {
+    k_b_reduce<<<grid, 32, 0, st>>>(d, b, cand, node_tot, n_cols, last_wins, decide, lp, scale, buf);
 }
 
 // Node sums of the smaller children when the children are not split further.
-__global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, const float2* __restrict__ gh,
-                         const double* __restrict__ scale) {
-    const uint32_t total = d.state->hist_chunks, n_exp = d.state->n_exp;
-    const double sg = scale[0], sh = scale[1];
+template <int MODE>
+__global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, GradRef gr) {
+    const uint32_t total = d.state->hist_chunks, n_exp = d.state->n_exp, CH = d.state->hist_chunk;
+    const GradLoad<MODE> load(gr);
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
-        const uint32_t j = last_le(n_exp, c, [&](uint32_t k) { return d.exp[k].hist_off; });
+        const uint32_t j = d.seg_exp[c];
         const BExp e = d.exp[j];
-        const uint32_t start = e.small_begin + (c - e.hist_off) * HIST_CHUNK_MAX;
-        const uint32_t len = min((uint32_t)HIST_CHUNK_MAX, e.small_begin + e.small_count - start);
+        const uint32_t start = e.small_begin + (c - e.hist_off) * CH;
+        const uint32_t len = min(CH, e.small_begin + e.small_count - start);
         long long ag = 0, ah = 0;
         for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
-            const float2 v = gh[ridx[start + i]];
-            ag += quantize(v.x, sg);
-            ah += quantize(v.y, sh);
+            long long qg, qh;
+            load(ridx[start + i], qg, qh);
+            ag += qg;
+            ah += qh;
         }
         for (int o = 16; o > 0; o >>= 1) {
             ag += __shfl_xor_sync(FULL, ag, o);
@@ -1489,9 +2126,13 @@ __global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, const float2
     }
 }
 
-void launch_b_sums(const BDev& d, const uint32_t* ridx, const float2* gh, const double* scale, uint32_t grid,
-                   cudaStream_t st) {
-    k_b_sums<<<grid, 256, 0, st>>>(d, ridx, gh, scale);
+void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, uint32_t grid, cudaStream_t st) {
+    if (gr.mode == GRAD_Q16)
+        k_b_sums<GRAD_Q16><<<grid, 256, 0, st>>>(d, ridx, gr);
+    else if (gr.mode == GRAD_Q8)
+        k_b_sums<GRAD_Q8><<<grid, 256, 0, st>>>(d, ridx, gr);
+    else
+        k_b_sums<GRAD_F32><<<grid, 256, 0, st>>>(d, ridx, gr);
 }
 
 __global__ void k_b_children_sums(BDev d, int b) {
@@ -1514,7 +2155,8 @@ __global__ void k_b_children_sums(BDev d, int b) {
 void launch_b_children_sums(const BDev& d, int b, cudaStream_t st) { k_b_children_sums<<<1, 1024, 0, st>>>(d, b); }
 
 // Remaining frontier -> leaves (grower.rs:484-514); leaf row chunks.
-__global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams lp, const double* __restrict__ scale) {
+__global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams lp, const double* __restrict__ scale,
+                                                    uint32_t buf) {
     __shared__ uint32_t sh[33];
     __shared__ uint32_t base, nf, n0;
     BState* s = d.state;
@@ -1535,7 +2177,7 @@ __global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams l
         lf.value = v;
         lf.tnode = nd.tnode;
         lf.chunk_off = 0;
-        lf.pad = 0;
+        lf.buf = buf;
         d.leaves[n0 + i] = lf;
     }
     __syncthreads();
@@ -1557,19 +2199,68 @@ __global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams l
     }
 }
 
-void launch_b_finalize(const BDev& d, int a, LeafParams lp, const double* scale, cudaStream_t st) {
-    k_b_finalize<<<1, 1024, 0, st>>>(d, a, lp, scale);
+void launch_b_finalize(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st) {
+    k_b_finalize<<<1, 1024, 0, st>>>(d, a, lp, scale, buf);
+}
+
+// Quantised training: every leaf is solved from the exact fixed-point sums
+// of the f32 gradients over its rows (d.sums[leaf][2], zeroed by the caller).
+__global__ void k_b_leaf_sums(BDev d, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1, GradRef gr) {
+    const uint32_t total = d.state->leaf_chunks, nl = d.state->n_leaves;
+    const GradLoad<GRAD_F32> load(gr);
+    for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+        const uint32_t l = last_le(nl, c, [&](uint32_t k) { return d.leaves[k].chunk_off; });
+        const BLeaf lf = d.leaves[l];
+        const uint32_t start = lf.begin + (c - lf.chunk_off) * B_LEAF_CHUNK;
+        const uint32_t len = min(B_LEAF_CHUNK, lf.begin + lf.count - start);
+        const uint32_t* ridx = lf.buf ? r1 : r0;
+        long long ag = 0, ah = 0;
+        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+            long long qg, qh;
+            load(ridx[start + i], qg, qh);
+            ag += qg;
+            ah += qh;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            ag += __shfl_xor_sync(FULL, ag, o);
+            ah += __shfl_xor_sync(FULL, ah, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(&d.sums[2 * l]), (unsigned long long)ag);
+            atomicAdd(reinterpret_cast<unsigned long long*>(&d.sums[2 * l + 1]), (unsigned long long)ah);
+        }
+    }
+}
+
+void launch_b_leaf_sums(const BDev& d, const uint32_t* r0, const uint32_t* r1, const GradRef& gr, uint32_t grid,
+                        cudaStream_t st) {
+    k_b_leaf_sums<<<grid, 256, 0, st>>>(d, r0, r1, gr);
+}
+
+__global__ void k_b_leaf_values(BDev d, LeafParams lp, const double* __restrict__ scale) {
+    const uint32_t nl = d.state->n_leaves;
+    for (uint32_t l = threadIdx.x; l < nl; l += blockDim.x) {
+        const long long G = d.sums[2 * l], H = d.sums[2 * l + 1];
+        const float v = leaf_value_dev(G, H, scale, lp);
+        d.leaves[l].value = v;
+        write_leaf(d.tree[d.leaves[l].tnode], G, H, scale, v);
+    }
+}
+
+void launch_b_leaf_values(const BDev& d, LeafParams lp, const double* scale, cudaStream_t st) {
+    k_b_leaf_values<<<1, 1024, 0, st>>>(d, lp, scale);
 }
 
 // pred[row] += leaf value over the final partition (grower.rs:208-219).
-__global__ void k_b_leaf_update(BDev d, const uint32_t* __restrict__ ridx, float* __restrict__ pred,
-                                uint32_t* __restrict__ row_leaf) {
+__global__ void k_b_leaf_update(BDev d, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1,
+                                float* __restrict__ pred, uint32_t* __restrict__ row_leaf) {
     const uint32_t total = d.state->leaf_chunks, nl = d.state->n_leaves;
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
         const uint32_t l = last_le(nl, c, [&](uint32_t k) { return d.leaves[k].chunk_off; });
         const BLeaf lf = d.leaves[l];
         const uint32_t start = lf.begin + (c - lf.chunk_off) * B_LEAF_CHUNK;
         const uint32_t len = min(B_LEAF_CHUNK, lf.begin + lf.count - start);
+        const uint32_t* ridx = lf.buf ? r1 : r0;
         for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
             const uint32_t row = ridx[start + i];
             pred[row] = pred[row] + lf.value;
@@ -1578,9 +2269,9 @@ __global__ void k_b_leaf_update(BDev d, const uint32_t* __restrict__ ridx, float
     }
 }
 
-void launch_b_leaf_update(const BDev& d, const uint32_t* ridx, float* pred, uint32_t* row_leaf, uint32_t grid,
-                          cudaStream_t st) {
-    k_b_leaf_update<<<grid, 256, 0, st>>>(d, ridx, pred, row_leaf);
+void launch_b_leaf_update(const BDev& d, const uint32_t* r0, const uint32_t* r1, float* pred, uint32_t* row_leaf,
+                          uint32_t grid, cudaStream_t st) {
+    k_b_leaf_update<<<grid, 256, 0, st>>>(d, r0, r1, pred, row_leaf);
 }
 
 // ============================================================================
@@ -1664,6 +2355,27 @@ void launch_transform(int transform, float* out, uint32_t G, uint64_t n, cudaStr
     if (transform == 0 || n == 0) return;
     const uint64_t total = transform == 1 ? (uint64_t)G * n : n;
     k_transform<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(transform, out, G, n);
+}
+
+void init_kernel_attributes() {
+    static std::atomic<unsigned long long> done{0ull};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    const unsigned long long bit = dev < 64 ? (1ull << dev) : 0ull;
+    if (bit && (done.load() & bit)) return;
+    const int hist_smem = 200 * 1024;
+    cudaFuncSetAttribute(k_hist_build<GRAD_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
+    cudaFuncSetAttribute(k_hist_build<GRAD_Q16>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
+    cudaFuncSetAttribute(k_hist_build<GRAD_Q8>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
+    cudaFuncSetAttribute(k_b_hist<GRAD_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
+    cudaFuncSetAttribute(k_b_hist<GRAD_Q16>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
+    cudaFuncSetAttribute(k_b_hist<GRAD_Q8>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
+    cudaFuncSetAttribute(k_bin_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    const int lane_smem = (int)lane_smem_bytes(GRAD_F32);
+    cudaFuncSetAttribute(k_b_hist_part<GRAD_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, lane_smem);
+    cudaFuncSetAttribute(k_b_hist_part<GRAD_Q16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lane_smem);
+    cudaFuncSetAttribute(k_b_hist_part<GRAD_Q8>, cudaFuncAttributeMaxDynamicSharedMemorySize, lane_smem);
+    done.fetch_or(bit);
 }
 
 }  // namespace bst

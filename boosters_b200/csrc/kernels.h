@@ -55,6 +55,29 @@ constexpr int HIST_CHUNK_MAX = 4096; // rows per block: 4096 * 2^20 < 2^32, 4096
 void launch_fixed_scales(const unsigned* maxabs, uint32_t G, uint64_t n, double* scales,
                          cudaStream_t st);
 
+// Gradient source of the histogram and node-sum kernels (values = BST_PRECISION_*):
+//   GRAD_F32  gh (f32 pairs) as fixed point round(v * scale[0..1]), exact int64 sums
+//   GRAD_Q16  gq short2 [G][n] quantised integers (|q| <= 32767)
+//   GRAD_Q8   gq char2  [G][n] quantised integers (|q| <= 127)
+constexpr int GRAD_F32 = 0, GRAD_Q16 = 1, GRAD_Q8 = 2;
+struct GradRef {
+    const float2* gh;
+    const void* gq;
+    const double* scale;  // GRAD_F32: the fixed-point scales of this output
+    int mode;
+};
+// Stochastic rounding of every (output, row): q = floor(v * Q / max|v| + u),
+// u from Philox4x32-10 with counter (row, output, round, QUANT_STREAM) and key
+// (seed lo, seed hi); word 0 rounds grad, word 1 hess.
+// qscales [G][4] = (Q / max|g|, Q / max|h|, max|g| / Q, max|h| / Q): the last
+// two turn integer histogram sums into gradient units.
+constexpr uint32_t QUANT_STREAM = 0x51A7E5EDu;
+// maxabs[2] = bit patterns of max|grad|, max|hess| over finite values (atomicMax; zero it first)
+void launch_maxabs(const float2* gh, uint64_t n, unsigned* maxabs, cudaStream_t st);
+// (outputs are numbered from out0 in the counter)
+void launch_quantize(int mode, uint32_t G, const float2* gh, uint64_t n, const unsigned* maxabs,
+                     uint64_t seed, uint32_t round, uint32_t out0, void* gq, double* qscales, cudaStream_t st);
+
 // ---- K4 histogram build -----------------------------------------------------
 struct HistChunk {
     uint32_t slot;   // destination histogram slot
@@ -73,22 +96,42 @@ struct HistTile {
 };
 void launch_hist_build(const HistChunk* chunks, uint32_t n_chunks, const HistTile* tiles,
                        uint32_t n_tiles, uint32_t max_smem_bins, const uint32_t* ridx,
-                       const float2* gh, const double* scale, const uint8_t* bins8, uint32_t s8,
+                       const GradRef& gr, const uint8_t* bins8, uint32_t s8,
                        const uint16_t* bins16, uint32_t s16, HBin* hist, uint64_t slot_bins,
                        cudaStream_t st);
 
-// Subtraction trick: the parent histogram lives in slot `left`, the smaller
-// child was built into slot `right`. flags bit0 = left child is the smaller.
-struct FinishWork {
-    uint32_t left, right, flags, pad;
+// Column-lane histogram tiles (bank-conflict-free form of K4). A tile is a
+// 16- or 32-byte aligned window of a row-major bin matrix holding C = bytes /
+// esize columns. Each lane of a warp takes one row, rotates the row's window
+// by (lane mod C) elements and at step j adds its gradient pair to column
+// (lane + j) mod C; the shared histogram keeps K = 32 / C copies of every
+// column at word bin * 32 + copy * C + column, so the 32 lanes of every
+// atomic hit 32 distinct banks. Columns with more than the tile's n_bins
+// bins never share a window with these tiles (they use HistTile).
+struct LaneTile {
+    uint32_t esize;     // 1 (u8 matrix) or 2 (u16 matrix)
+    uint32_t words;     // window width in 32-bit words: 4 or 8
+    uint32_t byte_off;  // window start inside the row, bytes (multiple of 16)
+    uint32_t n_bins;    // largest bin count of the window's columns
+    uint32_t col_hist[32];   // per window element: global histogram bin offset
+    uint32_t col_nbins[32];  // per window element: bins (0 = no column)
 };
-void launch_hist_finish(const FinishWork* w, uint32_t n_work, HBin* hist, uint64_t slot_bins,
-                        uint32_t total_bins, cudaStream_t st);
+// Largest n_bins of a lane tile (shared-memory height).
+uint32_t lane_tile_max_bins(int mode);
+// Rows of a row segment at most: what one block may sum exactly in 32-bit
+// shared counters (4096 for the hi/lo fixed-point split, 16384 quantised).
+uint32_t lane_segment_max(int mode);
+uint32_t lane_blocks_per_sm(int mode);
+// Partial histograms: one record of lane_part_stride() entries per (segment,
+// lane tile) item, entries of lane_part_entry_bytes(mode) bytes, column-major
+// (entry = element * n_bins + bin).
+uint32_t lane_part_stride();
+uint32_t lane_part_entry_bytes(int mode);
 
 // Exact node sums (sum of the same fixed-point values) for nodes whose
 // histogram is not needed. Uses HistChunk.slot as the output index.
 void launch_node_sums(const HistChunk* chunks, uint32_t n_chunks, const uint32_t* ridx,
-                      const float2* gh, const double* scale, long long* sums, cudaStream_t st);
+                      const GradRef& gr, long long* sums, cudaStream_t st);
 
 // ---- K6 split scan ----------------------------------------------------------
 struct ScanColumn {
@@ -187,20 +230,25 @@ struct BTreeNode {  // tree node as grown (training semantics)
 struct BExp {  // an expanding node of the current level
     uint32_t front, right_pnode, tl, tr;  // tl/tr: tree nodes of the training-left/right child
     uint32_t lc, rc, small_begin, small_count;
-    uint32_t part_off, hist_off, pad0, pad1;
+    uint32_t part_off, hist_off;
+    uint32_t left_pnode;  // the node's own slot: parent histogram, then its left child's
+    uint32_t pad1;
 };
 struct BLeaf {
     uint32_t begin, count;
     float value;
     uint32_t tnode;
-    uint32_t chunk_off, pad;
+    uint32_t chunk_off;
+    uint32_t buf;  // row-index buffer (0 / 1) holding the leaf's rows
 };
 struct BState {
     uint32_t n_front, n_exp, n_pnodes, n_tnodes;
     uint32_t part_chunks, hist_chunks, n_leaves, leaf_chunks;
-    uint32_t first_right, pad;
+    uint32_t first_right;
+    uint32_t hist_chunk;           // rows per histogram work item of the level
     unsigned long long hist_rows;  // rows visited by histogram builds of this tree
-    uint32_t pad2[4];
+    uint32_t done;                 // last-block hand-off counter (zero between launches)
+    uint32_t pad2[3];
 };
 struct LeafParams {
     double lambda, alpha, min_gain;
@@ -215,11 +263,14 @@ struct BDev {  // device buffers of the level loop
     BLeaf* leaves;
     PartWork* pworks;
     unsigned* cursors;
-    FinishWork* finish;
     ScanNode* scan_nodes;
     long long* sums;  // [max_exp][2]
+    uint32_t* seg_exp;  // histogram row segment -> expanding node of the level
+    uint32_t max_segs;  // capacity of seg_exp (and of the partial-histogram buffer)
     const BColumn* bcols;
     uint32_t max_front, max_tnodes;
+    uint32_t hist_target;   // desired histogram row segments per level
+    uint32_t hist_seg_max;  // largest row segment (lane_segment_max)
 };
 constexpr uint32_t B_PART_CHUNK = 2048;
 constexpr uint32_t B_LEAF_CHUNK = 4096;
@@ -228,31 +279,56 @@ constexpr uint32_t B_LEAF_CHUNK = 4096;
 // (call once per device before any stream capture).
 void init_kernel_attributes();
 void launch_b_root(const BDev& d, uint64_t n, cudaStream_t st);
-void launch_b_root_set(const BDev& d, const NodeSplit* root_split, cudaStream_t st);
+// Row indices alternate between two buffers: level d partitions buffer d & 1
+// into buffer (d + 1) & 1; a leaf records the buffer that holds its rows.
+// Root split into the frontier, then the level-0 decisions (rows in buffer 0).
+void launch_b_root_set(const BDev& d, const NodeSplit* root_split, LeafParams lp, const double* scale,
+                       cudaStream_t st);
 // level kernels; `a` is the index of the current frontier buffer
-void launch_b_decide(const BDev& d, int a, LeafParams lp, const double* scale, cudaStream_t st);
-void launch_b_partition(const BDev& d, const uint32_t* ridx, uint32_t* tmp, const uint8_t* bins8, uint32_t s8,
-                        const uint16_t* bins16, uint32_t s16, uint32_t grid, cudaStream_t st);
-void launch_b_copy(const BDev& d, const uint32_t* tmp, uint32_t* ridx, uint32_t grid, cudaStream_t st);
-void launch_b_children(const BDev& d, int a, int need_split, cudaStream_t st);
+void launch_b_decide(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st);
+// partition rin -> rout, then (last block) the children of every split
+void launch_b_partition(const BDev& d, const uint32_t* rin, uint32_t* rout, const uint8_t* bins8, uint32_t s8,
+                        const uint16_t* bins16, uint32_t s16, int a, int need_split, uint32_t grid,
+                        cudaStream_t st);
 void launch_b_zero_right(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t grid, cudaStream_t st);
 void launch_b_hist(const BDev& d, const HistTile* tiles, uint32_t n_tiles, uint32_t max_smem_bins,
-                   const uint32_t* ridx, const float2* gh, const double* scale, const uint8_t* bins8,
-                   uint32_t s8, const uint16_t* bins16, uint32_t s16, HBin* hist, uint64_t slot_bins,
-                   uint32_t grid, cudaStream_t st);
-void launch_b_finish(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t total_bins, uint32_t grid,
-                     cudaStream_t st);
+                   const uint32_t* ridx, const GradRef& gr, const uint8_t* bins8, uint32_t s8,
+                   const uint16_t* bins16, uint32_t s16, HBin* hist, uint64_t slot_bins, uint32_t grid,
+                   cudaStream_t st);
+// Partial histograms of every (row segment, lane tile) item of the level
+// (state: n_exp, hist_chunks, hist_chunk; exp[].small_begin/small_count/
+// hist_off; seg_exp).
+void launch_b_hist_part(const BDev& d, const LaneTile* tiles, uint32_t n_tiles, const uint32_t* ridx,
+                        const GradRef& gr, const uint8_t* bins8, uint32_t s8, const uint16_t* bins16, uint32_t s16,
+                        void* part, cudaStream_t st);
+// Sums each node's partials and applies the subtraction trick into slots
+// left_pnode / right_pnode (root: one node, the sum goes to right_pnode).
+// has_rest: bins of general tiles (bin_map[global bin] == 0xFFFFFFFF) were
+// built atomically into the right slots.
+// ent [n_ent]: per partial entry of a node (lane tiles in order, column-major
+// inside each tile): (global bin or 0xFFFFFFFF, tile << 16 | offset).
+void launch_b_merge(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t total_bins, const void* part,
+                    uint32_t n_lane_tiles, const uint2* ent, uint32_t n_ent, const uint32_t* bin_map, bool has_rest,
+                    int root, int mode, cudaStream_t st);
+// Level state of the root histogram: all n rows as one segment list.
+void launch_b_root_hist(const BDev& d, uint64_t n, uint32_t chunk, cudaStream_t st);
 void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const HBin* hist,
                    uint64_t slot_bins, const double* scale, GainParamsDev gp, ColCand* cand,
                    long long* node_tot, uint32_t grid, cudaStream_t st);
+// column reduction into frontier b; decide != 0: then (last block) the
+// decisions of the next level, whose rows are in buffer buf
 void launch_b_reduce(const BDev& d, int b, const ColCand* cand, const long long* node_tot, uint32_t n_cols,
-                     int last_wins, uint32_t grid, cudaStream_t st);
-void launch_b_sums(const BDev& d, const uint32_t* ridx, const float2* gh, const double* scale, uint32_t grid,
-                   cudaStream_t st);
+                     int last_wins, int decide, LeafParams lp, const double* scale, uint32_t buf, uint32_t grid,
+                     cudaStream_t st);
+void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, uint32_t grid, cudaStream_t st);
 void launch_b_children_sums(const BDev& d, int b, cudaStream_t st);
-void launch_b_finalize(const BDev& d, int a, LeafParams lp, const double* scale, cudaStream_t st);
-void launch_b_leaf_update(const BDev& d, const uint32_t* ridx, float* pred, uint32_t* row_leaf, uint32_t grid,
-                          cudaStream_t st);
+void launch_b_finalize(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st);
+// quantised training: exact leaf solves from the f32 gradients (gr: GRAD_F32)
+void launch_b_leaf_sums(const BDev& d, const uint32_t* r0, const uint32_t* r1, const GradRef& gr, uint32_t grid,
+                        cudaStream_t st);
+void launch_b_leaf_values(const BDev& d, LeafParams lp, const double* scale, cudaStream_t st);
+void launch_b_leaf_update(const BDev& d, const uint32_t* r0, const uint32_t* r1, float* pred, uint32_t* row_leaf,
+                          uint32_t grid, cudaStream_t st);
 
 // ---- K9 forest traversal ----------------------------------------------------
 // Node: word0 = feature | (is_leaf << 31) | (default_left << 30) | (categorical << 29)

@@ -68,8 +68,13 @@ const char* bst_version(void);
 /* GPU extension: histogram accumulation precision.
  * FP32: f32 grad/hess accumulated exactly in 64-bit fixed point (the
  *       reference's f64 histograms, training/gbdt/histograms/ops.rs:42).
- * Q16 / Q8: grad/hess quantised per round to int16 / int8 with stochastic
- *       rounding, histograms accumulated exactly in int32. */
+ * Q16 / Q8: grad/hess quantised per round and output to int16 / int8 with
+ *       stochastic rounding (q = floor(v * Q / max|v| + u), Q = 32767 / 127,
+ *       u from Philox4x32-10 keyed by `seed`, counter (row, output, round));
+ *       histograms hold exact integer sums (32-bit per block, 64-bit per
+ *       node), so the subtraction trick stays exact; splits are searched on
+ *       the integer sums times max|v| / Q, and every leaf is solved in f64
+ *       from the exact sums of its f32 grad/hess. Depth-wise and leaf-wise. */
 #define BST_PRECISION_FP32 0
 #define BST_PRECISION_Q16 1
 #define BST_PRECISION_Q8 2
@@ -331,6 +336,16 @@ bst_status bst_find_split_noalloc(const double* histogram_dev, const uint32_t* n
                                   uint32_t n_features, double parent_grad, double parent_hess,
                                   uint32_t parent_count, const bst_config* cfg, uint32_t n_threads,
                                   void* stream, bst_split* out);
+
+/* The quantisation step of the Q16 / Q8 training modes, on the GPU, for one
+ * output's host gradients (no counterpart in the reference, which trains on
+ * f32 gradients only): q = floor(v * Q / max|v| + u) as documented at
+ * BST_PRECISION_Q16, with max|v| over the finite values (|v| <= 3.4e38).
+ * qg / qh [n] receive the integers; steps [4] = (Q / max|g|, Q / max|h|,
+ * max|g| / Q, max|h| / Q), zeros for an all-zero input. */
+bst_status bst_quantize_gradients(const float* grad, const float* hess, uint64_t n, int32_t precision,
+                                  uint64_t seed, uint32_t round, uint32_t output, int32_t* qg,
+                                  int32_t* qh, double* steps);
 
 /* ------------------------------------------------------------------------ */
 /* Seeded synthetic workloads (host, counter-based; identical bytes for any */

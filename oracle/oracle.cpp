@@ -377,6 +377,16 @@ namespace {
 
 inline float w_at(const float* w, uint64_t i) { return w ? w[i] : 1.0f; }
 
+}  // namespace
+
+// f32 exp as the correctly rounded value: glibc's f64 exp rounded once to
+// f32. The reference calls the platform's expf (f32::exp); glibc's expf has a
+// 0.502 ULP bound, so the two can differ in the last bit for rare inputs, and
+// the reference's own tests compare exp-derived values with tolerances.
+inline float exp_f32(float x) { return (float)std::exp((double)x); }
+
+namespace {
+
 // regression.rs:20-43, classification.rs:19-52, classification.rs:141-187
 void gradients(int obj, uint32_t G, const float* preds, const float* y, const float* w, uint64_t n,
                float* grad, float* hess) {
@@ -392,7 +402,7 @@ void gradients(int obj, uint32_t G, const float* preds, const float* y, const fl
         for (uint32_t o = 0; o < G; ++o)
             for (uint64_t i = 0; i < n; ++i) {
                 float wi = w_at(w, i);
-                float p = 1.0f / (1.0f + std::exp(-preds[o * n + i]));
+                float p = 1.0f / (1.0f + exp_f32(-preds[o * n + i]));
                 grad[o * n + i] = wi * (p - y[i]);
                 hess[o * n + i] = std::fmax(wi * p * (1.0f - p), HESS_MIN);
             }
@@ -403,9 +413,9 @@ void gradients(int obj, uint32_t G, const float* preds, const float* y, const fl
             float mx = -std::numeric_limits<float>::infinity();
             for (uint32_t c = 0; c < G; ++c) mx = std::fmax(mx, preds[c * n + i]);
             float sum = -0.0f;
-            for (uint32_t c = 0; c < G; ++c) sum += std::exp(preds[c * n + i] - mx);
+            for (uint32_t c = 0; c < G; ++c) sum += exp_f32(preds[c * n + i] - mx);
             for (uint32_t c = 0; c < G; ++c) {
-                float p = std::exp(preds[c * n + i] - mx) / sum;
+                float p = exp_f32(preds[c * n + i] - mx) / sum;
                 float ind = (c == label) ? 1.0f : 0.0f;
                 grad[c * n + i] = wi * (p - ind);
                 hess[c * n + i] = std::fmax(wi * p * (1.0f - p), HESS_MIN);
@@ -459,6 +469,10 @@ void base_score(int obj, uint32_t G, const float* y, const float* w, uint64_t n,
 struct GainParams {
     float lambda = 1.0f, alpha = 0.0f, min_gain = 0.0f, min_child_weight = 1.0f;
     uint32_t min_samples_leaf = 1;
+    // Units of the histogram sums: 1.0 for f32 gradients; the quantisation
+    // steps when the histograms hold exact integer sums of quantised values
+    // (every prefix / difference stays an exact integer, converted at use).
+    double sg = 1.0, sh = 1.0;
 };
 
 struct NodeGainContext {  // gain.rs:16-52
@@ -521,8 +535,8 @@ Split find_numerical(const HBin* bins, uint32_t n_bins, uint32_t feature, double
         lc += 1;
         double rg = pg - lg, rh = ph - lh;
         uint32_t rc = sat_sub(pc, lc);
-        if (is_valid_split(gp, lh, rh, lc, rc)) {
-            float g = ctx.gain(lg, lh, rg, rh);
+        if (is_valid_split(gp, lh * gp.sh, rh * gp.sh, lc, rc)) {
+            float g = ctx.gain(lg * gp.sg, lh * gp.sh, rg * gp.sg, rh * gp.sh);
             if (g > best.gain) {
                 best.feature = feature;
                 best.gain = g;
@@ -542,8 +556,8 @@ Split find_numerical(const HBin* bins, uint32_t n_bins, uint32_t feature, double
             rc += 1;
             double lg2 = pg - rg, lh2 = ph - rh;
             uint32_t lc2 = sat_sub(pc, rc);
-            if (is_valid_split(gp, lh2, rh, lc2, rc)) {
-                float g = ctx.gain(lg2, lh2, rg, rh);
+            if (is_valid_split(gp, lh2 * gp.sh, rh * gp.sh, lc2, rc)) {
+                float g = ctx.gain(lg2 * gp.sg, lh2 * gp.sh, rg * gp.sg, rh * gp.sh);
                 if (g > best.gain) {
                     best.feature = feature;
                     best.gain = g;
@@ -566,8 +580,8 @@ Split find_onehot(const HBin* bins, uint32_t n_cats, uint32_t feature, double pg
         uint32_t lc = 1;
         double rg = pg - lg, rh = ph - lh;
         uint32_t rc = sat_sub(pc, lc);
-        if (is_valid_split(gp, lh, rh, lc, rc)) {
-            float g = ctx.gain(lg, lh, rg, rh);
+        if (is_valid_split(gp, lh * gp.sh, rh * gp.sh, lc, rc)) {
+            float g = ctx.gain(lg * gp.sg, lh * gp.sh, rg * gp.sg, rh * gp.sh);
             if (g > best.gain) {
                 best.feature = feature;
                 best.gain = g;
@@ -585,8 +599,10 @@ Split find_sorted(const HBin* bins, uint32_t n_cats, uint32_t feature, double pg
                   uint32_t pc, const GainParams& gp, const NodeGainContext& ctx) {
     Split best;
     std::vector<std::pair<uint32_t, double>> s;
-    for (uint32_t c = 0; c < n_cats; ++c)
-        if (bins[c].second > 1e-10) s.push_back({c, -bins[c].first / (bins[c].second + 1e-6)});
+    for (uint32_t c = 0; c < n_cats; ++c) {
+        const double gg = bins[c].first * gp.sg, hh = bins[c].second * gp.sh;
+        if (hh > 1e-10) s.push_back({c, -gg / (hh + 1e-6)});
+    }
     if (s.size() < 2) return best;
     std::stable_sort(s.begin(), s.end(),
                      [](const std::pair<uint32_t, double>& a, const std::pair<uint32_t, double>& b) {
@@ -603,8 +619,8 @@ Split find_sorted(const HBin* bins, uint32_t n_cats, uint32_t feature, double pg
         lc += 1;
         double rg = pg - lg, rh = ph - lh;
         uint32_t rc = sat_sub(pc, lc);
-        if (is_valid_split(gp, lh, rh, lc, rc)) {
-            float g = ctx.gain(lg, lh, rg, rh);
+        if (is_valid_split(gp, lh * gp.sh, rh * gp.sh, lc, rc)) {
+            float g = ctx.gain(lg * gp.sg, lh * gp.sh, rg * gp.sg, rh * gp.sh);
             if (g > best.gain) {
                 best.feature = feature;
                 best.gain = g;
@@ -629,7 +645,7 @@ struct SplitterCfg {
 Split find_split(const HBin* hist, const uint32_t* offs, const uint32_t* nb, const uint8_t* is_cat,
                  const uint8_t* has_missing, uint32_t n_feat, double pg, double ph, uint32_t pc,
                  const SplitterCfg& sc) {
-    NodeGainContext ctx(pg, ph, sc.gp);
+    NodeGainContext ctx(pg * sc.gp.sg, ph * sc.gp.sh, sc.gp);
     bool par = sc.parallel && n_feat >= 16;  // MIN_FEATURES_PARALLEL (find.rs:18)
     std::vector<Split> per(n_feat);
     auto eval = [&](uint32_t f) {
@@ -963,6 +979,11 @@ struct Grower {
     Tree tree;
     const float* grad = nullptr;
     const float* hess = nullptr;
+    // Quantised training: grad/hess above are the quantised integers (as
+    // floats), histogram sums are exact integers, and leaves are solved from
+    // the f32 gradients rgrad/rhess summed in f64 over the leaf's rows.
+    const float* rgrad = nullptr;
+    const float* rhess = nullptr;
 
     void init(const orc_binned* b, const TrainCfg& cfg) {
         ds = b;
@@ -1029,13 +1050,30 @@ struct Grower {
         leaf_map.push_back({tree_node, pnode});
     }
 
+    // Quantised mode: leaf totals are exact, order-independent sums of the f32
+    // gradients on the fixed-point grid 2^-k (k from max|v| and the row count:
+    // |round(v 2^k)| <= 2^38 and n 2^k max|v| < 2^62), then scaled back.
+    int kg = 0, kh = 0;
     void make_leaf(const Candidate& c) {
-        float w = leaf_weight(tc.sc.gp, c.g, c.h);
+        double g = c.g, h = c.h;
+        if (rgrad) {
+            long long sg = 0, sh = 0;
+            const double fg = std::ldexp(1.0, kg), fh = std::ldexp(1.0, kh);
+            const uint32_t b = part.begin[c.node], cnt = part.count[c.node];
+            for (uint32_t i = 0; i < cnt; ++i) {
+                const uint32_t row = part.indices[b + i];
+                sg += std::llrint((double)rgrad[row] * fg);
+                sh += std::llrint((double)rhess[row] * fh);
+            }
+            g = (double)sg * std::ldexp(1.0, -kg);
+            h = (double)sh * std::ldexp(1.0, -kh);
+        }
+        float w = leaf_weight(tc.sc.gp, g, h);
         tree.is_leaf[c.tree_node] = 1;
         tree.leaf[c.tree_node] = w;
-        tree.cover[c.tree_node] = f64_to_f32(c.h);
-        tree.grad_sum[c.tree_node] = c.g;
-        tree.hess_sum[c.tree_node] = c.h;
+        tree.cover[c.tree_node] = f64_to_f32(h);
+        tree.grad_sum[c.tree_node] = g;
+        tree.hess_sum[c.tree_node] = h;
         record_leaf(c.tree_node, c.node, w);
         pool.release(c.node);
     }
@@ -1109,9 +1147,9 @@ struct Grower {
                 return;
             }
             tree.gain[c.tree_node] = c.split.gain;
-            tree.cover[c.tree_node] = f64_to_f32(c.h);
-            tree.grad_sum[c.tree_node] = c.g;
-            tree.hess_sum[c.tree_node] = c.h;
+            tree.cover[c.tree_node] = f64_to_f32(c.h * tc.sc.gp.sh);
+            tree.grad_sum[c.tree_node] = c.g * tc.sc.gp.sg;
+            tree.hess_sum[c.tree_node] = c.h * tc.sc.gp.sh;
             auto lr = apply_split(c.tree_node, c.split);
             // partition (partition.rs:296-382)
             uint32_t col = c.split.feature;
@@ -1199,6 +1237,90 @@ struct Grower {
     }
 };
 
+// ---------------------------------------------------------------------------
+// Quantised gradients (not in the reference: the int8 / int16 training mode of
+// the GPU engine). Philox4x32-10 counter-based generator as published by
+// Salmon, Moraes, Dror and Shaw, "Parallel Random Numbers: As Easy as 1, 2, 3"
+// (SC 2011); stochastic rounding q = floor(v * Q / max|v| + u), u in [0, 1).
+// ---------------------------------------------------------------------------
+
+void philox4x32_10(const uint32_t in[4], const uint32_t key[2], uint32_t out[4]) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+    uint32_t c0 = in[0], c1 = in[1], c2 = in[2], c3 = in[3], k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)M0 * c0, p1 = (uint64_t)M1 * c2;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+        k0 += W0;
+        k1 += W1;
+    }
+    out[0] = c0;
+    out[1] = c1;
+    out[2] = c2;
+    out[3] = c3;
+}
+
+const uint32_t QUANT_STREAM = 0x51A7E5EDu;  // fourth counter word of the rounding stream
+
+inline int32_t quant_max(int precision) { return precision == BST_PRECISION_Q8 ? 127 : 32767; }
+
+inline float max_abs_finite(const float* v, uint64_t n) {
+    float m = 0.0f;
+    for (uint64_t i = 0; i < n; ++i) {
+        const float a = std::fabs(v[i]);
+        if (a <= 3.4e38f && a > m) m = a;  // the engine's scale ignores |v| > 3.4e38
+    }
+    return m;
+}
+
+int fixed_point_k(float m, uint64_t n) {
+    if (!(m > 0.0f)) return 0;
+    int e, en;
+    std::frexp((double)m, &e);
+    std::frexp((double)n, &en);
+    int B = 38;
+    if (61 - en < B) B = 61 - en;
+    int k = B - e;
+    return k > 1000 ? 1000 : (k < -1000 ? -1000 : k);
+}
+
+// steps = (Q / max|g|, Q / max|h|, max|g| / Q, max|h| / Q); all zero for a
+// zero (or non-finite) maximum
+void quantize(const float* g, const float* h, uint64_t n, int precision, uint64_t seed, uint32_t round,
+              uint32_t output, int32_t* qg, int32_t* qh, double* steps) {
+    const int32_t Q = quant_max(precision);
+    const float mg = max_abs_finite(g, n), mh = max_abs_finite(h, n);
+    const double ig = mg > 0.0f ? (double)Q / (double)mg : 0.0;
+    const double ih = mh > 0.0f ? (double)Q / (double)mh : 0.0;
+    steps[0] = ig;
+    steps[1] = ih;
+    steps[2] = mg > 0.0f ? (double)mg / (double)Q : 0.0;
+    steps[3] = mh > 0.0f ? (double)mh / (double)Q : 0.0;
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint32_t ctr[4] = {(uint32_t)i, output, round, QUANT_STREAM};
+        uint32_t r[4];
+        philox4x32_10(ctr, key, r);
+        const double ug = (double)r[0] * 0x1p-32, uh = (double)r[1] * 0x1p-32;
+        double xg = (double)g[i] * ig;
+        xg = xg + ug;
+        double xh = (double)h[i] * ih;
+        xh = xh + uh;
+        double fg = std::floor(xg), fh = std::floor(xh);
+        if (!(fg >= -Q)) fg = -Q;  // also maps NaN to -Q
+        if (fg > Q) fg = Q;
+        if (!(fh >= -Q)) fh = -Q;
+        if (fh > Q) fh = Q;
+        qg[i] = (int32_t)fg;
+        qh[i] = (int32_t)fh;
+    }
+}
+
 }  // namespace
 
 struct orc_model {
@@ -1220,8 +1342,8 @@ namespace {
 
 inline float sigmoid_t(float x) {  // transform.rs:106-115
     float c = x < -500.0f ? -500.0f : (x > 500.0f ? 500.0f : x);
-    if (c >= 0.0f) return 1.0f / (1.0f + std::exp(-c));
-    float e = std::exp(c);
+    if (c >= 0.0f) return 1.0f / (1.0f + exp_f32(-c));
+    float e = exp_f32(c);
     return e / (1.0f + e);
 }
 
@@ -1234,7 +1356,7 @@ void transform(int t, float* p, uint32_t G, uint64_t n) {
             for (uint32_t g = 0; g < G; ++g) mx = std::fmax(mx, p[g * n + i]);
             float sum = 0.0f;
             for (uint32_t g = 0; g < G; ++g) {
-                float e = std::exp(p[g * n + i] - mx);
+                float e = exp_f32(p[g * n + i] - mx);
                 p[g * n + i] = e;
                 sum += e;
             }
@@ -1470,6 +1592,13 @@ void orc_transform(int32_t t, float* p, uint32_t G, uint64_t n) { transform(t, p
 double orc_metric(int32_t metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w) {
     return metric_impl(metric, p, G, n, y, w);
 }
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    philox4x32_10(ctr, key, out);
+}
+void orc_quantize(const float* g, const float* h, uint64_t n, int32_t precision, uint64_t seed, uint32_t round,
+                  uint32_t output, int32_t* qg, int32_t* qh, double* steps) {
+    quantize(g, h, n, precision, seed, round, output, qg, qh, steps);
+}
 
 int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, uint32_t y_rows,
                       const float* w, const uint32_t* cat_idx, uint32_t n_cat, const bst_config* cfgp,
@@ -1519,11 +1648,38 @@ int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, ui
     gr.init(&b, tc);
     uint32_t n_rounds = cfg.n_trees;
     uint32_t built = 0;
+    const bool quant = cfg.precision != BST_PRECISION_FP32;
+    std::vector<int32_t> qg, qh;
+    std::vector<float> fqg, fqh;
+    if (quant) {
+        qg.resize(n);
+        qh.resize(n);
+        fqg.resize(n);
+        fqh.resize(n);
+    }
     for (uint32_t round = 0; round < n_rounds && built < max_trees; ++round) {
         auto tr0 = std::chrono::steady_clock::now();
         gradients(cfg.objective, G, m->train_pred.data(), y, w, n, grad.data(), hess.data());
         for (uint32_t o = 0; o < G && built < max_trees; ++o) {
-            gr.grow(grad.data() + (size_t)o * n, hess.data() + (size_t)o * n, record_leaves != 0);
+            const float* go = grad.data() + (size_t)o * n;
+            const float* ho = hess.data() + (size_t)o * n;
+            if (quant) {
+                double steps[4];
+                quantize(go, ho, n, cfg.precision, cfg.seed, round, o, qg.data(), qh.data(), steps);
+                for (uint64_t i = 0; i < n; ++i) {
+                    fqg[i] = (float)qg[i];
+                    fqh[i] = (float)qh[i];
+                }
+                gr.tc.sc.gp.sg = steps[2];
+                gr.tc.sc.gp.sh = steps[3];
+                gr.kg = fixed_point_k(max_abs_finite(go, n), n);
+                gr.kh = fixed_point_k(max_abs_finite(ho, n), n);
+                gr.rgrad = go;
+                gr.rhess = ho;
+                gr.grow(fqg.data(), fqh.data(), record_leaves != 0);
+            } else {
+                gr.grow(go, ho, record_leaves != 0);
+            }
             gr.update_predictions(m->train_pred.data() + (size_t)o * n);
             gr.tree.group = o;
             m->trees.push_back(std::move(gr.tree));

@@ -6,8 +6,10 @@
  * engine against. The engine never links, loads or calls it.
  *
  * It follows the Rust CPU path with sequential (n_threads = 1) arithmetic:
- * f64 histogram sums in partition order, the exact LRU histogram pool,
- * the stable row partition and glibc expf. The rayon tie-breaking of the
+ * f64 histogram sums in partition order, the exact LRU histogram pool and
+ * the stable row partition. f32 exp is the correctly rounded value (glibc's
+ * f64 exp rounded once); the reference calls the platform expf, which glibc
+ * bounds by 0.502 ULP, so the two may differ in the last bit for rare inputs. The rayon tie-breaking of the
  * parallel split search is emulated when n_threads != 1, and the histogram
  * build / split search can use OpenMP threads without changing any result.
  */
@@ -64,6 +66,16 @@ void orc_base_score(int32_t objective, uint32_t n_outputs, const float* y, const
 void orc_transform(int32_t transform, float* preds, uint32_t n_groups, uint64_t n);
 double orc_metric(int32_t metric, const float* preds, uint32_t n_groups, uint64_t n,
                   const float* y, const float* w);
+
+/* ---- quantised gradients (the engine's int8 / int16 mode; no reference
+ * counterpart). Philox4x32-10 (Salmon et al., SC 2011) and the stochastic
+ * rounding q = floor(v * Q / max|v| + u), Q = 127 (Q8) or 32767 (Q16),
+ * u = word / 2^32 of philox(ctr = (row, output, round, 0x51A7E5ED),
+ * key = (seed lo, seed hi)): word 0 for grad, word 1 for hess.
+ * steps = (Q / max|g|, Q / max|h|, max|g| / Q, max|h| / Q). */
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+void orc_quantize(const float* grad, const float* hess, uint64_t n, int32_t precision, uint64_t seed,
+                  uint32_t round, uint32_t output, int32_t* qg, int32_t* qh, double* steps);
 
 /* ---- training (model/gbdt/model.rs:115) ---- */
 /* Returns 0 on success, else a bst_status code. record_leaves keeps per-tree

@@ -68,6 +68,8 @@ _SIGS = [
     ("orc_model_add_tree", ctypes.c_int,
      [vp, u32, u32, u32p, f32p, u32p, u32p, u8p, u8p, f32p, u8p, u32p, u32p, u32p, u32]),
     ("orc_predict_rows", ctypes.c_int, [vp, f32p, u64, u64, ctypes.c_int, ctypes.c_int, f32p]),
+    ("orc_philox4x32_10", None, [u32p, u32p, u32p]),
+    ("orc_quantize", None, [f32p, f32p, u64, ctypes.c_int32, u64, u32, u32, i32p, i32p, f64p]),
 ]
 
 
@@ -324,3 +326,23 @@ def metric(kind, preds_gm, y, w=None):
         p = p.reshape(1, -1)
     return lib.orc_metric(kind, P(p, ctypes.c_float), p.shape[0], p.shape[1], P(f32(y), ctypes.c_float),
                           P(None if w is None else f32(w), ctypes.c_float))
+
+
+def philox4x32_10(ctr, key):
+    c = np.asarray(ctr, np.uint32)
+    k = np.asarray(key, np.uint32)
+    out = np.zeros(4, np.uint32)
+    lib.orc_philox4x32_10(P(c, ctypes.c_uint32), P(k, ctypes.c_uint32), P(out, ctypes.c_uint32))
+    return out
+
+
+def quantize(grad, hess, precision, seed, rnd, output=0):
+    """Quantised (qg, qh, steps) of one output's gradients (int32 arrays)."""
+    g, h = f32(grad), f32(hess)
+    n = len(g)
+    qg = np.zeros(n, np.int32)
+    qh = np.zeros(n, np.int32)
+    steps = np.zeros(4, np.float64)
+    lib.orc_quantize(P(g, ctypes.c_float), P(h, ctypes.c_float), n, precision, seed, rnd, output,
+                     P(qg, ctypes.c_int32), P(qh, ctypes.c_int32), P(steps, ctypes.c_double))
+    return qg, qh, steps

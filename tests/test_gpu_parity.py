@@ -218,16 +218,34 @@ def test_train_parity_regression_5k(n_threads):
     np.testing.assert_allclose(gm.predict_group_major(ds, raw=True), om.predict(x, raw=True), rtol=REL, atol=1e-6)
 
 
-def test_train_parity_logistic_nan():
+@pytest.mark.parametrize("batched", [True, False])
+def test_train_parity_logistic_nan(batched):
+    # batched: device-side level loop in a CUDA graph; else the host-driven loop
     x, y = bst.synth.binary(40_000, 40, n_nan_cols=10, seed=2)
     gm, om, ds = train_both(x, y, objective=bst.Objective.logistic(), n_estimators=15, learning_rate=0.1,
-                            max_depth=8)
+                            max_depth=8, batched=batched)
     compare_trees(gm, om, 40_000, sum_rtol=1e-6, sum_atol=1e-6)
     xv, yv = bst.synth.binary(8_000, 40, n_nan_cols=10, seed=2, stream=1)
     pg = gm.predict_group_major(bst.Dataset.from_feature_major(xv))
     po = om.predict(xv)
     np.testing.assert_allclose(pg, po, rtol=REL, atol=1e-6)
     assert abs(bst.metric("logloss", pg, yv) - bst.metric("logloss", po, yv)) < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp32", "q16"])
+@pytest.mark.parametrize("batched", [True, False])
+def test_train_parity_mixed_bin_counts(precision, batched):
+    # columns with up to 1024 bins (u16 rows, general shared-memory tiles)
+    # beside low-cardinality u8 columns (column-lane tiles)
+    rng = np.random.default_rng(12)
+    n = 12_000
+    x = rng.normal(size=(24, n)).astype(np.float32)
+    x[:12] = np.round(x[:12] * 8.0)  # ~60 distinct values
+    x[3, rng.random(n) < 0.1] = np.nan
+    y = (x[0] * 0.5 + np.nan_to_num(x[3]) + x[15] * x[16] + rng.normal(size=n)).astype(np.float32)
+    gm, om, _ = train_both(x, y, n_estimators=8, learning_rate=0.3, max_depth=6, max_bins=1024,
+                           precision=precision, batched=batched)
+    compare_trees(gm, om, n)
 
 
 def test_train_parity_leafwise():
