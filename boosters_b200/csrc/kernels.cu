@@ -1441,18 +1441,31 @@ __device__ void part_rows(const PartWork& w, uint32_t start, uint32_t len, unsig
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t L = 0, R = 0;
-            for (int k = 0; k < PART_PER; ++k)
-                for (int q = 0; q < PART_THREADS / 32; ++q) {
-                    const uint32_t a = s_l[k][q], c = s_r[k][q];
-                    s_l[k][q] = L;
-                    s_r[k][q] = R;
-                    L += a;
-                    R += c;
+        if (warp == 0) {
+            // exclusive scan of the PART_PER x 8 counts in (k, warp) order:
+            // lane q holds entries 2q and 2q + 1
+            static_assert(PART_PER * (PART_THREADS / 32) == 64, "two counts per lane");
+            uint32_t* fl = &s_l[0][0];
+            uint32_t* fr = &s_r[0][0];
+            const uint32_t l0 = fl[2 * lane], l1 = fl[2 * lane + 1], r0 = fr[2 * lane], r1 = fr[2 * lane + 1];
+            uint32_t xl = l0 + l1, xr = r0 + r1;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t tl = __shfl_up_sync(FULL, xl, o), tr = __shfl_up_sync(FULL, xr, o);
+                if (lane >= o) {
+                    xl += tl;
+                    xr += tr;
                 }
-            s_base[0] = L ? atomicAdd(&cur[0], L) : 0u;
-            s_base[1] = R ? atomicSub(&cur[1], R) - R : 0u;
+            }
+            const uint32_t L = __shfl_sync(FULL, xl, 31), R = __shfl_sync(FULL, xr, 31);
+            const uint32_t el = xl - l0 - l1, er = xr - r0 - r1;
+            fl[2 * lane] = el;
+            fl[2 * lane + 1] = el + l0;
+            fr[2 * lane] = er;
+            fr[2 * lane + 1] = er + r0;
+            if (lane == 0) {
+                s_base[0] = L ? atomicAdd(&cur[0], L) : 0u;
+                s_base[1] = R ? atomicSub(&cur[1], R) - R : 0u;
+            }
         }
         __syncthreads();
         const uint32_t lb = s_base[0], rbs = s_base[1];
@@ -1923,14 +1936,16 @@ __device__ void children_body(BDev d, int a, int need_split) {
         const uint32_t nch = valid ? (d.exp[j].small_count + chunk - 1) / chunk : 0u;
         uint32_t tc;
         const uint32_t jc = block_excl_scan(nch, sh, &tc);
-        if (valid) {
-            d.exp[j].hist_off = base + jc;
-            for (uint32_t q = 0; q < nch; ++q)  // segment -> expansion (the buffer bound always holds)
-                if (base + jc + q < d.max_segs) d.seg_exp[base + jc + q] = j;
-        }
+        if (valid) d.exp[j].hist_off = base + jc;
         __syncthreads();
         if (threadIdx.x == 0) base += tc;
         __syncthreads();
+    }
+    // segment -> expansion, all threads (the buffer bound always holds)
+    {
+        const uint32_t total = base < d.max_segs ? base : d.max_segs;
+        for (uint32_t c = threadIdx.x; c < total; c += blockDim.x)
+            d.seg_exp[c] = last_le(n_exp, c, [&](uint32_t k) { return d.exp[k].hist_off; });
     }
     if (threadIdx.x == 0) {
         s->hist_chunks = base < d.max_segs ? base : d.max_segs;
