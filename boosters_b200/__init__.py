@@ -524,6 +524,80 @@ def metric(kind, preds_group_major, labels, weights=None):
     return out.value
 
 
+class Ticket:
+    """A queued prediction request of :class:`PredictionServer`."""
+
+    __slots__ = ("id", "rows", "out", "submit_ns", "done_ns")
+
+    def __init__(self, tid, rows, out):
+        self.id = tid
+        self.rows = rows  # kept alive until the request completes
+        self.out = out
+        self.submit_ns = 0
+        self.done_ns = 0
+
+
+class PredictionServer:
+    """Continuous-batching prediction over a device-resident forest.
+
+    Requests queue FIFO; a dispatcher coalesces waiting requests into one
+    traversal launch per batch (bounded by ``mem_budget_bytes`` over three
+    in-flight batches) while earlier batches run. ``submit`` returns at once;
+    ``wait`` returns the ``(n_groups, n_rows)`` predictions. Row buffers from
+    pinned memory (e.g. ``torch.empty(..., pin_memory=True).numpy()``) give
+    asynchronous host-device copies. The model must stay alive.
+    """
+
+    def __init__(self, model, mem_budget_bytes=1 << 30, max_batch_rows=0, raw=False):
+        self.model = model
+        self.n_features = model.n_features
+        self.n_groups = model.n_groups
+        h = ctypes.c_void_p()
+        _n.check(_n.lib.bst_server_create(model._h, int(mem_budget_bytes), int(max_batch_rows), 1 if raw else 0,
+                                          ctypes.byref(h)))
+        self._h = h
+
+    def submit(self, rows, out=None):
+        """Queue sample-major rows ``(n, n_features)`` float32 (C order)."""
+        rows = np.asarray(rows)
+        if rows.dtype != np.float32 or not rows.flags.c_contiguous:
+            rows = np.ascontiguousarray(rows, dtype=np.float32)
+        if rows.ndim != 2 or rows.shape[1] != self.n_features:
+            raise ValueError(f"rows must have shape (n, {self.n_features})")
+        n = rows.shape[0]
+        if out is None:
+            out = np.empty((self.n_groups, n), dtype=np.float32)
+        elif out.dtype != np.float32 or out.shape != (self.n_groups, n) or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float32 array of shape ({self.n_groups}, {n})")
+        t = ctypes.c_uint64()
+        _n.check(_n.lib.bst_server_submit(self._h, ctypes.c_void_p(rows.ctypes.data), n,
+                                          ctypes.c_void_p(out.ctypes.data), ctypes.byref(t)))
+        return Ticket(t.value, rows, out)
+
+    def wait(self, ticket, timeout_ms=-1):
+        """Predictions ``(n_groups, n_rows)`` of a ticket; raises on timeout."""
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        _n.check(_n.lib.bst_server_wait(self._h, ticket.id, int(timeout_ms), ctypes.byref(a), ctypes.byref(b)))
+        ticket.submit_ns, ticket.done_ns = a.value, b.value
+        return ticket.out
+
+    def stats(self):
+        st = _n.ServerStats()
+        _n.check(_n.lib.bst_server_stats_get(self._h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in _n.ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _n.lib.bst_server_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class synth:
     """Seeded synthetic workloads; every array is feature-major ``[F, n]``."""
 

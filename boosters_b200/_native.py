@@ -87,6 +87,11 @@ class Split(ctypes.Structure):
 
 
 # (name, restype, argtypes) of every exported entry point
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("rows", ctypes.c_uint64), ("max_rows_seen", ctypes.c_uint64), ("max_batch_rows", ctypes.c_uint64)]
+
+
 SIGNATURES = [
     ("bst_last_error", ctypes.c_char_p, []),
     ("bst_version", ctypes.c_char_p, []),
@@ -157,6 +162,15 @@ SIGNATURES = [
     ("bst_quantize_gradients", ctypes.c_int32,
      [c_f32p, c_f32p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
       c_i32p, c_i32p, c_f64p]),
+    ("bst_server_create", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+    ("bst_server_submit", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    ("bst_server_wait", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64),
+      ctypes.POINTER(ctypes.c_uint64)]),
+    ("bst_server_stats_get", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
+    ("bst_server_free", None, [ctypes.c_void_p]),
     ("bst_synth_regression", ctypes.c_int32,
      [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, c_f32p, c_f32p]),
     ("bst_synth_binary", ctypes.c_int32,

@@ -22,6 +22,10 @@ struct bst_model {
 struct bst_booster {
     std::unique_ptr<bst::Booster> b;
 };
+struct bst_server {
+    bst::Server* s = nullptr;
+    ~bst_server() { bst::server_destroy(s); }
+};
 
 namespace {
 
@@ -825,6 +829,43 @@ bst_status bst_quantize_gradients(const float* grad, const float* hess, uint64_t
         return BST_OK;
     });
 }
+
+bst_status bst_server_create(const bst_model* model, uint64_t mem_budget_bytes, uint64_t max_batch_rows,
+                             int32_t raw, bst_server** out) {
+    if (!model || !out) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    return guarded([&]() -> bst_status {
+        std::unique_ptr<bst_server> h(new bst_server());
+        h->s = bst::server_create(*model->m, mem_budget_bytes, max_batch_rows, raw != 0);
+        *out = h.release();
+        return BST_OK;
+    });
+}
+
+bst_status bst_server_submit(bst_server* server, const float* rows, uint64_t n_rows, float* out, uint64_t* ticket) {
+    if (!server || !ticket || (n_rows && (!rows || !out))) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    return guarded([&]() -> bst_status {
+        *ticket = bst::server_submit(*server->s, rows, n_rows, out);
+        return BST_OK;
+    });
+}
+
+bst_status bst_server_wait(bst_server* server, uint64_t ticket, int64_t timeout_ms, uint64_t* submit_ns,
+                           uint64_t* done_ns) {
+    if (!server) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    return guarded([&]() -> bst_status {
+        std::string err;
+        const int st = bst::server_wait(*server->s, ticket, timeout_ms, submit_ns, done_ns, &err);
+        return st == BST_OK ? BST_OK : fail((bst_status)st, err);
+    });
+}
+
+bst_status bst_server_stats_get(bst_server* server, bst_server_stats* out) {
+    if (!server || !out) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    bst::server_stats(*server->s, out);
+    return BST_OK;
+}
+
+void bst_server_free(bst_server* server) { delete server; }
 
 bst_status bst_metric(int32_t metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w,
                       double* out) {

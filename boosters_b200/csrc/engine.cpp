@@ -9,6 +9,7 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -1645,13 +1646,87 @@ const DeviceForest& Model::device_forest() const {
     f->view.base = f->base.p;
     f->view.n_trees = (uint32_t)trees.size();
     f->view.n_groups = n_groups;
+    build_heap_forest(*f);
     dev = std::move(f);
     return *dev;
 }
 
+// Heap-ordered copy of the forest (1-based: children of heap node h at 2h,
+// 2h + 1), trees grouped by output group in forest order, when every leaf is
+// at depth <= HEAP_DEPTH and every feature index fits 16 bits.
+void Model::build_heap_forest(DeviceForest& f) const {
+    std::vector<uint2> hn, cat;
+    std::vector<uint32_t> goff(n_groups + 1, 0), words;
+    uint32_t placed = 0;
+    for (uint32_t g = 0; g < n_groups; ++g) {
+        goff[g] = placed;
+        for (const HostTree& t : trees) {
+            if (t.group != g) continue;
+            const size_t base = hn.size();
+            hn.resize(base + HEAP_NODES, make_uint2(0u, 0u));
+            const uint32_t wbase = (uint32_t)words.size();
+            words.insert(words.end(), t.cat_words.begin(), t.cat_words.end());
+            // (tree node, heap index, depth)
+            std::vector<std::array<uint32_t, 3>> stack{{0u, 1u, 0u}};
+            while (!stack.empty()) {
+                const auto it = stack.back();
+                stack.pop_back();
+                const uint32_t i = it[0], h = it[1], d = it[2];
+                if (h >= HEAP_NODES || d > (uint32_t)HEAP_DEPTH) return;  // too deep: no heap copy
+                uint2 nd;
+                if (t.is_leaf[i]) {
+                    nd.x = 1u << 31;
+                    std::memcpy(&nd.y, &t.leaf[i], 4);
+                } else {
+                    if (t.split_index[i] > 0xFFFFu) return;
+                    nd.x = t.split_index[i] | ((uint32_t)t.default_left[i] << 30) |
+                           ((uint32_t)(t.split_type[i] == 1) << 29);
+                    if (t.split_type[i] == 1) {
+                        const uint32_t ss = t.seg_size.empty() ? 0 : t.seg_size[i];
+                        nd.y = (uint32_t)cat.size();
+                        cat.push_back(make_uint2(ss ? wbase + t.seg_start[i] : 0u, ss));
+                    } else {
+                        std::memcpy(&nd.y, &t.threshold[i], 4);
+                    }
+                    stack.push_back({t.left[i], 2 * h, d + 1});
+                    stack.push_back({t.right[i], 2 * h + 1, d + 1});
+                }
+                hn[base + h] = nd;
+            }
+            ++placed;
+        }
+    }
+    goff[n_groups] = placed;
+    auto up = [](auto& dst, const auto& src) {
+        dst.alloc(std::max<size_t>(1, src.size()));
+        if (!src.empty())
+            BST_CK(cudaMemcpy(dst.p, src.data(), sizeof(src[0]) * src.size(), cudaMemcpyHostToDevice));
+    };
+    up(f.heap_nodes, hn);
+    up(f.heap_goff, goff);
+    up(f.heap_cat, cat);
+    up(f.heap_words, words);
+    f.heap.nodes = f.heap_nodes.p;
+    f.heap.group_off = f.heap_goff.p;
+    f.heap.cat = f.heap_cat.p;
+    f.heap.cat_words = f.heap_words.p;
+    f.heap.base = f.base.p;
+    f.heap.n_trees = placed;
+    f.heap.n_groups = n_groups;
+    f.heap.has_cat = cat.empty() ? 0 : 1;
+    f.heap_ok = true;
+}
+
+void forest_predict_rows(const DeviceForest& f, const float* x, uint64_t n, uint64_t F, float* out, cudaStream_t st) {
+    if (f.heap_ok && predict_heap_rows((uint32_t)F) > 0)
+        launch_predict_heap(f.heap, x, n, (uint32_t)F, out, st);
+    else
+        launch_predict(f.view, x, n, (uint32_t)F, 0, out, st);
+}
+
 void predict_device(const Model& m, const float* x, uint64_t n, uint64_t F, bool raw, float* out, cudaStream_t st) {
     const DeviceForest& f = m.device_forest();
-    launch_predict(f.view, x, n, (uint32_t)F, 0, out, st);
+    forest_predict_rows(f, x, n, F, out, st);
     if (!raw) launch_transform(transform_of(m.objective), out, m.n_groups, n, st);
     BST_CK(cudaGetLastError());
 }

@@ -87,7 +87,15 @@ struct DeviceForest {
     DevArray<uint32_t> roots, group_trees, group_off, cat_seg, cat_words;
     DevArray<float> base;
     ForestDev view{};
+    // heap-ordered copy for the shared-memory traversal (trees of leaf depth
+    // <= HEAP_DEPTH, features < 65536)
+    bool heap_ok = false;
+    DevArray<uint2> heap_nodes, heap_cat;
+    DevArray<uint32_t> heap_goff, heap_words;
+    HeapForest heap{};
 };
+// out [n_groups][n] raw margins of sample-major rows x [n][F] (device).
+void forest_predict_rows(const DeviceForest& f, const float* x, uint64_t n, uint64_t F, float* out, cudaStream_t st);
 
 struct Counters {
     uint64_t launches = 0;
@@ -108,6 +116,7 @@ struct Model {
     mutable std::mutex mu;
     mutable std::unique_ptr<DeviceForest> dev;
     const DeviceForest& device_forest() const;
+    void build_heap_forest(DeviceForest& f) const;
 };
 
 // Incremental training on a GPU-resident binned dataset: the boosting loop of
@@ -135,6 +144,16 @@ void predict_host(const Model& m, const HostDataset& ds, bool raw, float* out);
 void predict_device(const Model& m, const float* x_dev_sm, uint64_t n, uint64_t F, bool raw,
                     float* out_dev, cudaStream_t st);
 int transform_of(int objective);
+
+// Continuous-batching prediction server (server.cpp). The model must outlive
+// the server.
+struct Server;
+Server* server_create(const Model& m, uint64_t mem_budget_bytes, uint64_t max_batch_rows, bool raw);
+void server_destroy(Server* s);
+uint64_t server_submit(Server& s, const float* rows, uint64_t n, float* out);
+int server_wait(Server& s, uint64_t id, int64_t timeout_ms, uint64_t* submit_ns, uint64_t* done_ns,
+                std::string* err);
+void server_stats(Server& s, bst_server_stats* out);
 void build_hist_tiles(const BinPlan& p, std::vector<HistTile>& tiles, uint32_t& max_smem,
                       const std::vector<uint8_t>* only = nullptr);
 void build_lane_tiles(const BinPlan& p, uint32_t max_bins, std::vector<LaneTile>& tiles, uint32_t& tile_bins,

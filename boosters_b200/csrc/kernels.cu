@@ -2337,6 +2337,160 @@ void launch_predict(const ForestDev& f, const float* x, uint64_t n, uint32_t n_f
     k_predict<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(f, x, n, n_features, feature_major, out);
 }
 
+// ---- shared-memory traversal (heap-ordered trees of depth <= HEAP_DEPTH) ------
+// One block holds a tile of R rows in shared memory and streams the trees of
+// each output group through a double-buffered shared-memory ring of
+// PREDICT_CHUNK trees (cp.async); each thread sums its row's leaves in forest
+// order (the same f32 additions as k_predict), walking PREDICT_IL trees at a
+// time as independent chains. The forest is read once per row tile from L2
+// instead of once per row.
+constexpr uint32_t PREDICT_CHUNK = 8;
+constexpr uint32_t PREDICT_IL = 4;
+constexpr uint32_t PREDICT_SMEM = 220u * 1024u;
+constexpr uint32_t PREDICT_TREE_BYTES = HEAP_NODES * 8u;
+
+uint32_t predict_heap_rows(uint32_t F) {
+    const uint32_t trees = 2u * PREDICT_CHUNK * PREDICT_TREE_BYTES;
+    if (F == 0 || F > 0xFFFFu) return 0;
+    uint32_t r = (PREDICT_SMEM - trees) / (F * 4u);
+    if (r > 384u) r = 384u;
+    r &= ~31u;
+    return r >= 64u ? r : 0u;
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+// One tree step for a row: node nd at heap index i; children 2i, 2i + 1 in
+// one aligned 16-byte load issued with the feature load. True at a leaf.
+template <bool CAT>
+__device__ __forceinline__ bool heap_step(const uint2* __restrict__ tree, const float* xr, const HeapForest& f,
+                                          uint32_t& i, uint2& nd) {
+    if (nd.x >> 31) return true;
+    const float v = xr[nd.x & 0xFFFFu];
+    const uint4 ch = *reinterpret_cast<const uint4*>(tree + 2u * i);  // (left child, right child)
+    bool left;
+    if (CAT && ((nd.x >> 29) & 1u) && v == v) {
+        const uint2 cs = f.cat[nd.y];
+        const uint32_t cat = sat_u32(v);
+        const uint32_t wi = cat >> 5;
+        left = !(wi < cs.y && ((f.cat_words[cs.x + wi] >> (cat & 31)) & 1u));
+    } else {
+        // NaN compares false: it goes left only by default_left
+        left = (v < __uint_as_float(nd.y)) | ((v != v) & (((nd.x >> 30) & 1u) != 0u));
+    }
+    i = 2u * i + (left ? 0u : 1u);
+    nd = left ? make_uint2(ch.x, ch.y) : make_uint2(ch.z, ch.w);
+    return false;
+}
+
+template <bool CAT>
+__global__ void __launch_bounds__(384, 1)
+k_predict_heap(HeapForest f, const float* __restrict__ x, uint64_t n, uint32_t F, uint32_t R,
+               float* __restrict__ out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint2* ring = reinterpret_cast<uint2*>(smem_raw);  // [2][PREDICT_CHUNK][HEAP_NODES]
+    float* rows = reinterpret_cast<float*>(smem_raw + 2u * PREDICT_CHUNK * PREDICT_TREE_BYTES);
+    const uint32_t tid = threadIdx.x;
+    const uint64_t n_tiles = (n + R - 1) / R;
+    for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const uint64_t r0 = tile * R;
+        const uint32_t nr = (uint32_t)((uint64_t)R < n - r0 ? (uint64_t)R : n - r0);
+        {  // row tile: nr * F floats, contiguous in x
+            const float* src = x + r0 * F;
+            const uint32_t words = nr * F;
+            const bool vec = ((reinterpret_cast<uintptr_t>(src) & 15u) == 0) && (words % 4u == 0);
+            if (vec) {
+                for (uint32_t i = tid; i < words / 4u; i += blockDim.x) cp_async16(rows + 4u * i, src + 4u * i);
+            } else {
+                for (uint32_t i = tid; i < words; i += blockDim.x) rows[i] = src[i];
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        }
+        const bool ok = tid < nr;
+        const float* xr = rows + (size_t)(ok ? tid : 0) * F;
+        for (uint32_t g = 0; g < f.n_groups; ++g) {
+            const uint32_t t0 = f.group_off[g], t1 = f.group_off[g + 1];
+            float acc = f.base[g];
+            auto issue = [&](uint32_t c, uint32_t buf) {  // chunk starting at tree t0 + c * CHUNK
+                const uint32_t ta = t0 + c * PREDICT_CHUNK;
+                const uint32_t nt = min(PREDICT_CHUNK, t1 - ta);
+                const uint4* src = reinterpret_cast<const uint4*>(f.nodes + (size_t)ta * HEAP_NODES);
+                uint4* dst = reinterpret_cast<uint4*>(ring + (size_t)buf * PREDICT_CHUNK * HEAP_NODES);
+                for (uint32_t i = tid; i < nt * (PREDICT_TREE_BYTES / 16u); i += blockDim.x) cp_async16(dst + i, src + i);
+                asm volatile("cp.async.commit_group;" ::: "memory");
+            };
+            const uint32_t n_chunks = (t1 - t0 + PREDICT_CHUNK - 1) / PREDICT_CHUNK;
+            if (n_chunks) issue(0, 0);
+            for (uint32_t c = 0; c < n_chunks; ++c) {
+                if (c + 1 < n_chunks) {
+                    issue(c + 1, (c + 1) & 1u);
+                    asm volatile("cp.async.wait_group 1;" ::: "memory");
+                } else {
+                    asm volatile("cp.async.wait_group 0;" ::: "memory");
+                }
+                __syncthreads();
+                const uint2* tb = ring + (size_t)(c & 1u) * PREDICT_CHUNK * HEAP_NODES;
+                const uint32_t nt = min(PREDICT_CHUNK, t1 - (t0 + c * PREDICT_CHUNK));
+                if (ok) {
+                    uint32_t q = 0;
+                    for (; q + PREDICT_IL <= nt; q += PREDICT_IL) {
+                        uint32_t ii[PREDICT_IL];
+                        uint2 nn[PREDICT_IL];
+                        bool dd[PREDICT_IL];
+#pragma unroll
+                        for (uint32_t u = 0; u < PREDICT_IL; ++u) {
+                            ii[u] = 1;
+                            nn[u] = tb[(q + u) * HEAP_NODES + 1];
+                            dd[u] = false;
+                        }
+#pragma unroll
+                        for (int step = 0; step <= HEAP_DEPTH; ++step) {
+#pragma unroll
+                            for (uint32_t u = 0; u < PREDICT_IL; ++u)
+                                if (!dd[u]) dd[u] = heap_step<CAT>(tb + (q + u) * HEAP_NODES, xr, f, ii[u], nn[u]);
+                        }
+#pragma unroll
+                        for (uint32_t u = 0; u < PREDICT_IL; ++u) acc = acc + __uint_as_float(nn[u].y);
+                    }
+                    for (; q < nt; ++q) {
+                        const uint2* ta = tb + q * HEAP_NODES;
+                        uint32_t ia = 1;
+                        uint2 na = ta[1];
+#pragma unroll
+                        for (int step = 0; step <= HEAP_DEPTH; ++step)
+                            if (heap_step<CAT>(ta, xr, f, ia, na)) break;
+                        acc = acc + __uint_as_float(na.y);
+                    }
+                }
+                __syncthreads();  // ring buffer (c & 1) free for chunk c + 2
+            }
+            if (ok) out[(uint64_t)g * n + r0 + tid] = acc;
+        }
+        __syncthreads();  // row tile free
+    }
+}
+
+void launch_predict_heap(const HeapForest& f, const float* x, uint64_t n, uint32_t F, float* out, cudaStream_t st) {
+    if (n == 0) return;
+    const uint32_t R = predict_heap_rows(F);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_predict_heap<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
+        cudaFuncSetAttribute(k_predict_heap<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
+        attr = true;
+    }
+    const size_t smem = 2u * PREDICT_CHUNK * PREDICT_TREE_BYTES + (size_t)R * F * 4u;
+    const uint64_t tiles = (n + R - 1) / R;
+    const unsigned grid = (unsigned)(tiles < 148u ? tiles : 148u);
+    if (f.has_cat)
+        k_predict_heap<true><<<grid, R, smem, st>>>(f, x, n, F, R, out);
+    else
+        k_predict_heap<false><<<grid, R, smem, st>>>(f, x, n, F, R, out);
+}
+
 __global__ void k_transform(int t, float* __restrict__ p, uint32_t G, uint64_t n) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t == 1) {

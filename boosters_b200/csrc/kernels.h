@@ -352,6 +352,30 @@ struct ForestDev {
 // out [n_groups][n] raw margins (base score + trees in forest order, f32).
 void launch_predict(const ForestDev& f, const float* x, uint64_t n, uint32_t n_features,
                     int feature_major, float* out, cudaStream_t st);
+// Heap-ordered forest for the shared-memory traversal (trees with leaves at
+// depth <= HEAP_DEPTH): tree t's node i at nodes[t * HEAP_NODES + i], 1-based
+// (root 1, children 2i (left) and 2i + 1 (right), one aligned 16-byte pair;
+// entry 0 unused). Node = (word, value): word = feature (bits 0-15) |
+// leaf << 31 | default_left << 30 | categorical << 29; value = threshold or
+// leaf value (f32 bits), or for a categorical split an index into cat
+// (start, size) pairs over cat_words. Trees are stored grouped by output
+// group in forest order (group_off[g] .. group_off[g + 1]).
+constexpr int HEAP_DEPTH = 8;
+constexpr uint32_t HEAP_NODES = 512;  // entries 1 .. 2^(HEAP_DEPTH + 1) - 1
+struct HeapForest {
+    const uint2* nodes;
+    const uint32_t* group_off;  // [n_groups + 1]
+    const uint2* cat;
+    const uint32_t* cat_words;
+    const float* base;
+    uint32_t n_trees, n_groups;
+    int has_cat;  // any categorical split
+};
+// Rows per block of the shared-memory traversal for F features (0: unusable).
+uint32_t predict_heap_rows(uint32_t n_features);
+// x sample-major [n][n_features]; out [n_groups][n] raw margins.
+void launch_predict_heap(const HeapForest& f, const float* x, uint64_t n, uint32_t n_features, float* out,
+                         cudaStream_t st);
 // transform: 1 sigmoid, 2 softmax over [G][n]
 void launch_transform(int transform, float* out, uint32_t G, uint64_t n, cudaStream_t st);
 

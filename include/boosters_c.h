@@ -348,6 +348,46 @@ bst_status bst_quantize_gradients(const float* grad, const float* hess, uint64_t
                                   int32_t* qh, double* steps);
 
 /* ------------------------------------------------------------------------ */
+/* Serving: continuous batching over a device-resident forest (the engine's  */
+/* serving loop; the reference predicts one call at a time through          */
+/* Predictor::predict_into, inference/gbdt/predictor.rs:197).                */
+/* ------------------------------------------------------------------------ */
+
+typedef struct bst_server bst_server;
+
+typedef struct bst_server_stats {
+    uint64_t submitted;      /* requests accepted                            */
+    uint64_t completed;      /* requests finished                            */
+    uint64_t batches;        /* traversal launches                           */
+    uint64_t rows;           /* rows predicted                               */
+    uint64_t max_rows_seen;  /* largest batch                                */
+    uint64_t max_batch_rows; /* batch capacity from the memory budget        */
+} bst_server_stats;
+
+/* The model stays device-resident and must outlive the server. The device
+ * memory of the in-flight batches (3 slots of input + output rows) is bounded
+ * by mem_budget_bytes; max_batch_rows (0 = no extra cap) further caps a
+ * batch. raw != 0: margins; else the objective's transform. */
+bst_status bst_server_create(const bst_model* model, uint64_t mem_budget_bytes, uint64_t max_batch_rows,
+                             int32_t raw, bst_server** out);
+/* Queues n_rows sample-major rows [n_rows, n_features] f32 for prediction
+ * into out [n_groups, n_rows]; both buffers are the caller's and must stay
+ * valid until bst_server_wait returns for the ticket (pinned host memory
+ * gives asynchronous copies). Requests larger than one batch are rejected
+ * with BST_ERR_INVALID_ARGUMENT. Returns at once. */
+bst_status bst_server_submit(bst_server* server, const float* rows, uint64_t n_rows, float* out,
+                             uint64_t* ticket);
+/* Waits for a ticket (timeout_ms < 0: no limit; BST_ERR_TIMEOUT leaves the
+ * ticket valid). On return the ticket is retired; submit_ns / done_ns (may
+ * be NULL) receive the server's steady-clock times of submission and of
+ * completion of the request's batch. One waiter per ticket. */
+bst_status bst_server_wait(bst_server* server, uint64_t ticket, int64_t timeout_ms, uint64_t* submit_ns,
+                           uint64_t* done_ns);
+bst_status bst_server_stats_get(bst_server* server, bst_server_stats* out);
+/* Completes every queued request, then frees the server. */
+void bst_server_free(bst_server* server);
+
+/* ------------------------------------------------------------------------ */
 /* Seeded synthetic workloads (host, counter-based; identical bytes for any */
 /* consumer). Feature-major x [n_features, n_samples], y [n_samples].       */
 /* ------------------------------------------------------------------------ */

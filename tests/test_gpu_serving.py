@@ -1,0 +1,149 @@
+"""The continuous-batching prediction server: every request's result equals
+the plain per-request predict bit for bit, whether it ran alone or coalesced
+with concurrent requests; admission respects the memory budget. The served
+forests go through the shared-memory heap traversal (depth <= 8) or, for
+deeper trees, the node-list traversal; both must match the plain predict."""
+import threading
+
+import numpy as np
+import pytest
+
+import boosters_b200 as bst
+from boosters_b200 import _native as n
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def model():
+    x, y = bst.synth.binary(30_000, 24, n_nan_cols=6, seed=7)
+    cfg = bst.GBDTConfig(objective=bst.Objective.logistic(), n_estimators=60, learning_rate=0.2, max_depth=6)
+    return bst.GBDTModel.train(bst.Dataset.from_feature_major(x, y), cfg)
+
+
+def plain_predict(model, rows, raw=False):
+    return model.predict_group_major(bst.Dataset(rows), raw=raw)
+
+
+def request_rows(rng, n_rows, F):
+    r = rng.normal(size=(n_rows, F)).astype(np.float32)
+    r[rng.random(size=r.shape) < 0.05] = np.nan
+    return r
+
+
+@pytest.mark.parametrize("raw", [False, True])
+def test_alone_and_in_the_mix_are_identical(model, raw):
+    rng = np.random.default_rng(1)
+    F = model.n_features
+    sizes = [1, 2, 7, 100, 1000, 4096, 33, 65536, 5, 777]
+    reqs = [request_rows(rng, s, F) for s in sizes]
+    want = [plain_predict(model, r, raw) for r in reqs]
+    srv = bst.PredictionServer(model, mem_budget_bytes=64 << 20, raw=raw)
+    try:
+        # alone: submit and wait one at a time
+        alone = [srv.wait(srv.submit(r)).copy() for r in reqs]
+        # in the mix: everything queued at once from several threads
+        tickets = [None] * len(reqs)
+
+        def go(k0):
+            for k in range(k0, len(reqs), 3):
+                tickets[k] = srv.submit(reqs[k])
+
+        th = [threading.Thread(target=go, args=(k,)) for k in range(3)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        mixed = [srv.wait(t) for t in tickets]
+        st = srv.stats()
+    finally:
+        srv.close()
+    for a, b, w in zip(alone, mixed, want):
+        np.testing.assert_array_equal(a, w)
+        np.testing.assert_array_equal(b, w)
+    assert st["completed"] == 2 * len(reqs)
+    assert st["batches"] < 2 * len(reqs)  # concurrent requests were coalesced
+
+
+def test_many_small_requests_stream(model):
+    rng = np.random.default_rng(2)
+    F = model.n_features
+    pool = request_rows(rng, 20_000, F)
+    want = plain_predict(model, pool)
+    srv = bst.PredictionServer(model, mem_budget_bytes=16 << 20)
+    try:
+        ts, spans = [], []
+        for _ in range(400):
+            a = int(rng.integers(0, 20_000))
+            b = min(20_000, a + int(np.exp(rng.uniform(0, np.log(2000)))))
+            ts.append(srv.submit(pool[a:b]))
+            spans.append((a, b))
+        for t, (a, b) in zip(ts, spans):
+            np.testing.assert_array_equal(srv.wait(t), want[:, a:b])
+            assert t.done_ns >= t.submit_ns > 0
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert st["submitted"] == st["completed"] == 400
+    assert st["max_rows_seen"] <= st["max_batch_rows"]
+
+
+def test_softmax_groups_and_categorical_splits():
+    x, y = bst.synth.multiclass(8_000, 10, 3, 4, seed=4)
+    m = bst.GBDTModel.train(bst.Dataset.from_feature_major(x, y, categorical_features=[10, 11, 12]),
+                            bst.GBDTConfig(objective=bst.Objective.softmax(4), n_estimators=5, max_depth=4))
+    rows = np.ascontiguousarray(x[:, :3000].T)
+    srv = bst.PredictionServer(m)
+    try:
+        out = srv.wait(srv.submit(rows))
+    finally:
+        srv.close()
+    np.testing.assert_array_equal(out, m.predict_group_major(bst.Dataset(rows)))
+
+
+def test_budget_admission_limits(model):
+    F = model.n_features
+    per_row = (F + model.n_groups) * 4
+    srv = bst.PredictionServer(model, mem_budget_bytes=3 * per_row * 100)  # 100-row batches
+    try:
+        assert srv.stats()["max_batch_rows"] == 100
+        with pytest.raises(n.BoostersError, match="exceeds"):
+            srv.submit(np.zeros((101, F), np.float32))
+        rng = np.random.default_rng(3)
+        rows = [request_rows(rng, 60, F) for _ in range(10)]
+        ts = [srv.submit(r) for r in rows]
+        outs = [srv.wait(t) for t in ts]
+        st = srv.stats()
+    finally:
+        srv.close()
+    for r, o in zip(rows, outs):
+        np.testing.assert_array_equal(o, plain_predict(model, r))
+    assert st["max_rows_seen"] <= 100  # two 60-row requests never share a batch
+    with pytest.raises(n.BoostersError, match="budget"):
+        bst.PredictionServer(model, mem_budget_bytes=per_row)
+
+
+def test_wait_errors(model):
+    srv = bst.PredictionServer(model)
+    try:
+        t = srv.submit(np.zeros((10, model.n_features), np.float32))
+        srv.wait(t)
+        with pytest.raises(n.BoostersError, match="ticket"):
+            srv.wait(t)  # already retired
+    finally:
+        srv.close()
+
+
+def test_deep_trees_use_the_node_list_traversal():
+    # leaves deeper than the heap's 8 levels: the node-list kernel serves them
+    x, y = bst.synth.binary(20_000, 16, n_nan_cols=4, seed=9)
+    m = bst.GBDTModel.train(bst.Dataset.from_feature_major(x, y),
+                            bst.GBDTConfig(objective=bst.Objective.logistic(), n_estimators=8, max_depth=11,
+                                           growth_strategy=bst.GrowthStrategy.Leafwise, n_leaves=200))
+    rows = np.ascontiguousarray(x[:, :5000].T)
+    srv = bst.PredictionServer(m)
+    try:
+        out = srv.wait(srv.submit(rows))
+    finally:
+        srv.close()
+    np.testing.assert_array_equal(out, m.predict_group_major(bst.Dataset(rows)))
