@@ -1651,51 +1651,120 @@ const DeviceForest& Model::device_forest() const {
     return *dev;
 }
 
-// Heap-ordered copy of the forest (1-based: children of heap node h at 2h,
-// 2h + 1), trees grouped by output group in forest order, when every leaf is
-// at depth <= HEAP_DEPTH and every feature index fits 16 bits.
+// Heap-ordered copy of the forest (1-based: children of heap position h at
+// 2h, 2h + 1), every tree padded to a complete tree of depth HEAP_DEPTH,
+// trees grouped by output group in forest order, with the bin columns its
+// splits read (the word and column formats are those of HeapForest). A leaf
+// at depth d < HEAP_DEPTH sits at its leftmost descendant's position,
+// reached through padding splits (K = 0xFFFF on a NaN-as-0 column) that
+// always go left. Leaves deeper than HEAP_DEPTH, a feature split both
+// numerically and categorically, a NaN threshold whose split sends missing
+// values left, more than 65534 distinct thresholds of one feature, more than
+// HEAP_MAX_COLS columns or 65536 categorical splits, or a category set
+// reaching category 65504 leave the forest on the node-list traversal.
 void Model::build_heap_forest(DeviceForest& f) const {
-    std::vector<uint2> hn, cat;
-    std::vector<uint32_t> goff(n_groups + 1, 0), words;
+    const uint32_t NF = n_features;
+    if (NF == 0) return;
+    std::vector<std::vector<float>> thr(NF);
+    std::vector<uint8_t> fcat(NF, 0), fnum0(NF, 0), fnum1(NF, 0);
+    uint32_t min_F = 1;  // padding splits may read feature 0
+    for (const HostTree& t : trees)
+        for (size_t i = 0; i < t.is_leaf.size(); ++i) {
+            if (t.is_leaf[i]) continue;
+            const uint32_t ft = t.split_index[i];
+            if (ft >= NF) return;
+            min_F = std::max(min_F, ft + 1);
+            if (t.split_type[i] == 1) {
+                fcat[ft] = 1;
+                if (!t.seg_size.empty() && t.seg_size[i] > 2047u) return;
+            } else {
+                const float th = t.threshold[i];
+                if (th == th)
+                    thr[ft].push_back(th);
+                else if (t.default_left[i])
+                    return;
+                (t.default_left[i] ? fnum1 : fnum0)[ft] = 1;
+            }
+        }
+    std::vector<float> thr_flat;
+    std::vector<uint32_t> thr_off(NF + 1, 0);
+    size_t max_thr = 0;
+    bool any_cat = false;
+    for (uint32_t ft = 0; ft < NF; ++ft) {
+        if (fcat[ft] && (fnum0[ft] || fnum1[ft])) return;
+        any_cat |= fcat[ft] != 0;
+        auto& v = thr[ft];
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end(), [](float a, float b) { return a == b; }), v.end());
+        if (v.size() > 65534u) return;
+        max_thr = std::max(max_thr, v.size());
+        thr_off[ft] = (uint32_t)thr_flat.size();
+        thr_flat.insert(thr_flat.end(), v.begin(), v.end());
+    }
+    thr_off[NF] = (uint32_t)thr_flat.size();
+    // bin columns: NaN-as-largest (numeric, default right) or categorical,
+    // and NaN-as-0 (numeric, default left); padding needs one NaN-as-0 column
+    std::vector<int32_t> fcol(2 * (size_t)NF, -1);
+    int32_t n_cols = 0, pad_col = -1;
+    for (uint32_t ft = 0; ft < NF; ++ft) {
+        if (fcat[ft] || fnum0[ft]) fcol[2 * ft] = n_cols++;
+        if (fnum1[ft]) {
+            fcol[2 * ft + 1] = n_cols++;
+            if (pad_col < 0) pad_col = fcol[2 * ft + 1];
+        }
+    }
+    if (pad_col < 0) pad_col = fcol[1] = n_cols++;
+    if ((uint32_t)n_cols > HEAP_MAX_COLS) return;
+    const uint32_t pad_word = 0xFFFF0000u | (uint32_t)pad_col;
+
+    std::vector<uint32_t> hn, goff(n_groups + 1, 0), words;
+    std::vector<uint2> cat;
     uint32_t placed = 0;
     for (uint32_t g = 0; g < n_groups; ++g) {
         goff[g] = placed;
         for (const HostTree& t : trees) {
             if (t.group != g) continue;
             const size_t base = hn.size();
-            hn.resize(base + HEAP_NODES, make_uint2(0u, 0u));
+            hn.resize(base + HEAP_NODES, pad_word);
+            hn[base] = 0;
             const uint32_t wbase = (uint32_t)words.size();
             words.insert(words.end(), t.cat_words.begin(), t.cat_words.end());
-            // (tree node, heap index, depth)
+            // (tree node, heap position, depth)
             std::vector<std::array<uint32_t, 3>> stack{{0u, 1u, 0u}};
             while (!stack.empty()) {
                 const auto it = stack.back();
                 stack.pop_back();
                 const uint32_t i = it[0], h = it[1], d = it[2];
-                if (h >= HEAP_NODES || d > (uint32_t)HEAP_DEPTH) return;  // too deep: no heap copy
-                uint2 nd;
                 if (t.is_leaf[i]) {
-                    nd.x = 1u << 31;
-                    std::memcpy(&nd.y, &t.leaf[i], 4);
-                } else {
-                    if (t.split_index[i] > 0xFFFFu) return;
-                    nd.x = t.split_index[i] | ((uint32_t)t.default_left[i] << 30) |
-                           ((uint32_t)(t.split_type[i] == 1) << 29);
-                    if (t.split_type[i] == 1) {
-                        const uint32_t ss = t.seg_size.empty() ? 0 : t.seg_size[i];
-                        nd.y = (uint32_t)cat.size();
-                        cat.push_back(make_uint2(ss ? wbase + t.seg_start[i] : 0u, ss));
-                    } else {
-                        std::memcpy(&nd.y, &t.threshold[i], 4);
-                    }
-                    stack.push_back({t.left[i], 2 * h, d + 1});
-                    stack.push_back({t.right[i], 2 * h + 1, d + 1});
+                    uint32_t bits;
+                    std::memcpy(&bits, &t.leaf[i], 4);
+                    hn[base + (h << (HEAP_DEPTH - d))] = bits;  // padding splits lead left to here
+                    continue;
                 }
-                hn[base + h] = nd;
+                if (d >= (uint32_t)HEAP_DEPTH) return;  // too deep: no heap copy
+                const uint32_t ft = t.split_index[i];
+                uint32_t w;
+                if (t.split_type[i] == 1) {
+                    if (cat.size() >= 65536u) return;
+                    const uint32_t ss = t.seg_size.empty() ? 0 : t.seg_size[i];
+                    w = ((uint32_t)cat.size() << 16) | 0x8000u | (uint32_t)fcol[2 * ft];
+                    cat.push_back(make_uint2(ss ? wbase + t.seg_start[i] : 0u,
+                                             ss | ((uint32_t)(t.default_left[i] != 0) << 31)));
+                } else {
+                    const float th = t.threshold[i];
+                    const auto& v = thr[ft];
+                    const uint32_t K =
+                        th == th ? (uint32_t)(std::lower_bound(v.begin(), v.end(), th) - v.begin()) + 1u : 0u;
+                    w = (K << 16) | (uint32_t)fcol[2 * ft + (t.default_left[i] ? 1 : 0)];
+                }
+                hn[base + h] = w;
+                stack.push_back({t.left[i], 2 * h, d + 1});
+                stack.push_back({t.right[i], 2 * h + 1, d + 1});
             }
             ++placed;
         }
     }
+    static_assert(HEAP_NODES == 2u << HEAP_DEPTH, "complete tree of HEAP_DEPTH levels");
     goff[n_groups] = placed;
     auto up = [](auto& dst, const auto& src) {
         dst.alloc(std::max<size_t>(1, src.size()));
@@ -1706,19 +1775,31 @@ void Model::build_heap_forest(DeviceForest& f) const {
     up(f.heap_goff, goff);
     up(f.heap_cat, cat);
     up(f.heap_words, words);
+    up(f.heap_thr, thr_flat);
+    up(f.heap_thr_off, thr_off);
+    up(f.heap_fcol, fcol);
+    up(f.heap_fcat, fcat);
     f.heap.nodes = f.heap_nodes.p;
     f.heap.group_off = f.heap_goff.p;
     f.heap.cat = f.heap_cat.p;
     f.heap.cat_words = f.heap_words.p;
+    f.heap.thr = f.heap_thr.p;
+    f.heap.thr_off = f.heap_thr_off.p;
+    f.heap.feat_col = f.heap_fcol.p;
+    f.heap.feat_cat = f.heap_fcat.p;
     f.heap.base = f.base.p;
     f.heap.n_trees = placed;
     f.heap.n_groups = n_groups;
-    f.heap.has_cat = cat.empty() ? 0 : 1;
+    f.heap.n_features = NF;
+    f.heap.n_cols = (uint32_t)n_cols;
+    f.heap.has_cat = any_cat ? 1 : 0;
+    f.heap.bins16 = (any_cat || max_thr > 255) ? 1 : 0;
+    f.heap_min_F = min_F;
     f.heap_ok = true;
 }
 
 void forest_predict_rows(const DeviceForest& f, const float* x, uint64_t n, uint64_t F, float* out, cudaStream_t st) {
-    if (f.heap_ok && predict_heap_rows((uint32_t)F) > 0)
+    if (f.heap_ok && F >= f.heap_min_F && F <= 0xFFFFFFFFull && predict_heap_rows(f.heap, (uint32_t)F, n) > 0)
         launch_predict_heap(f.heap, x, n, (uint32_t)F, out, st);
     else
         launch_predict(f.view, x, n, (uint32_t)F, 0, out, st);

@@ -88,10 +88,15 @@ struct DeviceForest {
     DevArray<float> base;
     ForestDev view{};
     // heap-ordered copy for the shared-memory traversal (trees of leaf depth
-    // <= HEAP_DEPTH, features < 65536)
+    // <= HEAP_DEPTH, features < 65536, rows binned against the forest's own
+    // thresholds)
     bool heap_ok = false;
-    DevArray<uint2> heap_nodes, heap_cat;
-    DevArray<uint32_t> heap_goff, heap_words;
+    uint32_t heap_min_F = 0;  // rows need at least this many features
+    DevArray<uint2> heap_cat;
+    DevArray<uint32_t> heap_nodes, heap_goff, heap_words, heap_thr_off;
+    DevArray<float> heap_thr;
+    DevArray<int32_t> heap_fcol;
+    DevArray<uint8_t> heap_fcat;
     HeapForest heap{};
 };
 // out [n_groups][n] raw margins of sample-major rows x [n][F] (device).

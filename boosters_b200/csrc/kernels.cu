@@ -1978,7 +1978,7 @@ k_b_hist(BDev d, const HistTile* __restrict__ tiles, uint32_t n_tiles, uint32_t 
     uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);
     __shared__ HistTile tile;
     const GradLoad<MODE> load(gr);
-    const uint32_t n_exp = d.state->n_exp, CH = d.state->hist_chunk;
+    const uint32_t CH = d.state->hist_chunk;
     const uint64_t items = (uint64_t)d.state->hist_chunks * n_tiles;
     for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
         const uint32_t c = (uint32_t)(it / n_tiles), t = (uint32_t)(it % n_tiles);
@@ -2116,7 +2116,7 @@ void launch_b_reduce(const BDev& d, int b, const ColCand* cand, const long long*
 // Node sums of the smaller children when the children are not split further.
 template <int MODE>
 __global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, GradRef gr) {
-    const uint32_t total = d.state->hist_chunks, n_exp = d.state->n_exp, CH = d.state->hist_chunk;
+    const uint32_t total = d.state->hist_chunks, CH = d.state->hist_chunk;
     const GradLoad<MODE> load(gr);
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
         const uint32_t j = d.seg_exp[c];
@@ -2338,24 +2338,49 @@ void launch_predict(const ForestDev& f, const float* x, uint64_t n, uint32_t n_f
 }
 
 // ---- shared-memory traversal (heap-ordered trees of depth <= HEAP_DEPTH) ------
-// One block holds a tile of R rows in shared memory and streams the trees of
-// each output group through a double-buffered shared-memory ring of
-// PREDICT_CHUNK trees (cp.async); each thread sums its row's leaves in forest
-// order (the same f32 additions as k_predict), walking PREDICT_IL trees at a
-// time as independent chains. The forest is read once per row tile from L2
-// instead of once per row.
-constexpr uint32_t PREDICT_CHUNK = 8;
+// One block bins a tile of R rows into shared-memory bin columns (against the
+// forest's thresholds) and streams the trees of each output group through a
+// double-buffered shared-memory ring of PREDICT_CHUNK trees (cp.async); each
+// thread walks its row through PREDICT_IL trees at a time as independent
+// chains of exactly HEAP_DEPTH steps and sums the leaves in forest order (the
+// same f32 additions as k_predict). The forest is read once per row tile from
+// L2 instead of once per row.
+//
+// Bin columns are R entries long. Row r of a u8 column sits at byte
+// (r / 128) * 128 + 4 * (r % 32) + (r / 32) % 4, of a u16 column at byte
+// (r / 64) * 128 + 4 * (r % 32) + 2 * ((r / 32) % 2): with R a multiple of
+// 128, lane l of any warp reads bank l whatever column each lane asks for,
+// so the bin fetch of a step is one conflict-free wavefront.
+constexpr uint32_t PREDICT_CHUNK = 16;
 constexpr uint32_t PREDICT_IL = 4;
-constexpr uint32_t PREDICT_SMEM = 220u * 1024u;
-constexpr uint32_t PREDICT_TREE_BYTES = HEAP_NODES * 8u;
+constexpr uint32_t PREDICT_SMEM = 227u * 1024u;
+constexpr uint32_t PREDICT_TREE_BYTES = HEAP_NODES * 4u;
+constexpr uint32_t PREDICT_RING = 2u * PREDICT_CHUNK * PREDICT_TREE_BYTES;
+constexpr uint32_t PREDICT_MAX_ROWS = 768;
+constexpr uint32_t PREDICT_MIN_ROWS = 128;
+constexpr uint32_t PREDICT_SPL_MAX_F = 256;  // splitter table up to this many features (16 KB)
+constexpr uint32_t PREDICT_STAGE_LD = 34;    // halfwords per staged row: odd word stride
+constexpr uint32_t PREDICT_STAGE = 32u * PREDICT_STAGE_LD * 2u;
+constexpr uint32_t BIN_NAN = 0xFFFFu;
+static_assert(PREDICT_MAX_ROWS / 32u * PREDICT_STAGE <= PREDICT_RING, "binning stage lives in the tree ring");
 
-uint32_t predict_heap_rows(uint32_t F) {
-    const uint32_t trees = 2u * PREDICT_CHUNK * PREDICT_TREE_BYTES;
-    if (F == 0 || F > 0xFFFFu) return 0;
-    uint32_t r = (PREDICT_SMEM - trees) / (F * 4u);
-    if (r > 384u) r = 384u;
-    r &= ~31u;
-    return r >= 64u ? r : 0u;
+__host__ __device__ inline uint32_t predict_spl_bytes(uint32_t F) {
+    return F <= PREDICT_SPL_MAX_F ? F * HEAP_SPLITTERS * 4u : 0u;
+}
+
+uint32_t predict_heap_rows(const HeapForest& f, uint32_t F, uint64_t n) {
+    if (F == 0 || f.n_cols == 0 || f.n_cols > HEAP_MAX_COLS) return 0;
+    const uint64_t fixed = PREDICT_RING + predict_spl_bytes(F);
+    const uint64_t per_row = (uint64_t)f.n_cols * (f.bins16 ? 2u : 1u);
+    uint64_t r = (PREDICT_SMEM - fixed) / per_row;
+    if (r > PREDICT_MAX_ROWS) r = PREDICT_MAX_ROWS;
+    r &= ~(uint64_t)(PREDICT_MIN_ROWS - 1);
+    if (r < PREDICT_MIN_ROWS) return 0;
+    // spread a small batch over every SM: about n / 148 rows per block
+    uint64_t want = (n + 147) / 148;
+    want = (want + PREDICT_MIN_ROWS - 1) / PREDICT_MIN_ROWS * PREDICT_MIN_ROWS;
+    if (want < PREDICT_MIN_ROWS) want = PREDICT_MIN_ROWS;
+    return (uint32_t)(want < r ? want : r);
 }
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
@@ -2363,54 +2388,135 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
 }
 
-// One tree step for a row: node nd at heap index i; children 2i, 2i + 1 in
-// one aligned 16-byte load issued with the feature load. True at a leaf.
-template <bool CAT>
-__device__ __forceinline__ bool heap_step(const uint2* __restrict__ tree, const float* xr, const HeapForest& f,
-                                          uint32_t& i, uint2& nd) {
-    if (nd.x >> 31) return true;
-    const float v = xr[nd.x & 0xFFFFu];
-    const uint4 ch = *reinterpret_cast<const uint4*>(tree + 2u * i);  // (left child, right child)
-    bool left;
-    if (CAT && ((nd.x >> 29) & 1u) && v == v) {
-        const uint2 cs = f.cat[nd.y];
-        const uint32_t cat = sat_u32(v);
-        const uint32_t wi = cat >> 5;
-        left = !(wi < cs.y && ((f.cat_words[cs.x + wi] >> (cat & 31)) & 1u));
-    } else {
-        // NaN compares false: it goes left only by default_left
-        left = (v < __uint_as_float(nd.y)) | ((v != v) & (((nd.x >> 30) & 1u) != 0u));
-    }
-    i = 2u * i + (left ? 0u : 1u);
-    nd = left ? make_uint2(ch.x, ch.y) : make_uint2(ch.z, ch.w);
-    return false;
+// Thresholds of one feature as the binning search sees them.
+struct BinFeat {
+    uint32_t off, n, blk, ns;  // threshold range; splitter block size and count
+    bool cat;
+};
+
+__device__ __forceinline__ BinFeat bin_feat(const HeapForest& f, uint32_t feat) {
+    BinFeat b;
+    b.off = f.thr_off[feat];
+    b.n = f.thr_off[feat + 1] - b.off;
+    b.blk = b.n > HEAP_SPLITTERS ? (b.n + HEAP_SPLITTERS - 1) / HEAP_SPLITTERS : 1u;
+    b.ns = (b.n + b.blk - 1) / b.blk;
+    b.cat = f.feat_cat[feat] != 0;
+    return b;
 }
 
-template <bool CAT>
-__global__ void __launch_bounds__(384, 1)
+// bin of value v (see HeapForest); NaN -> BIN_NAN. spl: the feature's
+// splitters thr[off + k * blk] (k < ns) in shared memory, or null.
+__device__ __forceinline__ uint32_t heap_bin(const HeapForest& f, const BinFeat& bf, const float* spl, float v) {
+    if (v != v) return BIN_NAN;
+    if (bf.cat) {
+        const uint32_t c = sat_u32(v);
+        return c < 65534u ? c : 65534u;
+    }
+    uint32_t lo = 0, hi = bf.n;
+    if (spl) {  // block of the first splitter > v, then search inside the block before it
+        uint32_t a = 0, b = bf.ns;
+        while (a < b) {
+            const uint32_t m = (a + b) >> 1;
+            if (spl[m] <= v)
+                a = m + 1;
+            else
+                b = m;
+        }
+        if (a == 0) return 0;
+        lo = (a - 1) * bf.blk;
+        hi = min(a * bf.blk, bf.n);
+    }
+    const float* t = f.thr + bf.off;
+    while (lo < hi) {  // first threshold > v
+        const uint32_t m = (lo + hi) >> 1;
+        if (t[m] <= v)
+            lo = m + 1;
+        else
+            hi = m;
+    }
+    return lo;
+}
+
+// One split step: from heap position h of tree to its chosen child. cb: this
+// thread's row in bin column 0 (byte address); Rb: column stride in bytes.
+template <bool CAT, typename BinT>
+__device__ __forceinline__ uint32_t heap_step(const uint32_t* tree, const unsigned char* cb, uint32_t Rb,
+                                              const HeapForest& f, uint32_t h) {
+    const uint32_t w = tree[h];
+    const uint32_t b = *reinterpret_cast<const BinT*>(cb + (w & 0x7FFFu) * Rb);
+    bool left;
+    if (CAT && (w & 0x8000u)) {
+        const uint2 cs = f.cat[w >> 16];
+        if (b == BIN_NAN) {
+            left = (cs.y >> 31) != 0u;
+        } else {
+            const uint32_t wi = b >> 5;
+            left = !(wi < (cs.y & 0x7FFFFFFFu) && ((f.cat_words[cs.x + wi] >> (b & 31u)) & 1u));
+        }
+    } else {
+        left = b * 65536u + 65535u < w;  // bin < K (K: the word's upper half)
+    }
+    return 2u * h + (left ? 0u : 1u);
+}
+
+template <bool CAT, typename BinT>
+__global__ void __launch_bounds__(PREDICT_MAX_ROWS, 1)
 k_predict_heap(HeapForest f, const float* __restrict__ x, uint64_t n, uint32_t F, uint32_t R,
                float* __restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint2* ring = reinterpret_cast<uint2*>(smem_raw);  // [2][PREDICT_CHUNK][HEAP_NODES]
-    float* rows = reinterpret_cast<float*>(smem_raw + 2u * PREDICT_CHUNK * PREDICT_TREE_BYTES);
-    const uint32_t tid = threadIdx.x;
+    uint32_t* ring = reinterpret_cast<uint32_t*>(smem_raw);  // [2][PREDICT_CHUNK][HEAP_NODES]
+    const uint32_t spl_bytes = predict_spl_bytes(F);
+    float* spl = reinterpret_cast<float*>(smem_raw + PREDICT_RING);
+    unsigned char* bins = smem_raw + PREDICT_RING + spl_bytes;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t Rb = R * (uint32_t)sizeof(BinT);
+    const uint32_t roff = sizeof(BinT) == 1 ? (tid >> 7) * 128u + 4u * lane + ((tid >> 5) & 3u)
+                                            : (tid >> 6) * 128u + 4u * lane + 2u * ((tid >> 5) & 1u);
+    const unsigned char* cb = bins + roff;
+    uint16_t* stage = reinterpret_cast<uint16_t*>(smem_raw) + (size_t)warp * (PREDICT_STAGE / 2u);
+    const uint32_t NF = F < f.n_features ? F : f.n_features;  // features any split reads
+    if (spl_bytes) {
+        for (uint32_t i = tid; i < NF * HEAP_SPLITTERS; i += blockDim.x) {
+            const BinFeat bf = bin_feat(f, i / HEAP_SPLITTERS);
+            const uint32_t k = i % HEAP_SPLITTERS;
+            spl[i] = k < bf.ns ? f.thr[bf.off + k * bf.blk] : 0.0f;
+        }
+    }
+    __syncthreads();
     const uint64_t n_tiles = (n + R - 1) / R;
     for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const uint64_t r0 = tile * R;
         const uint32_t nr = (uint32_t)((uint64_t)R < n - r0 ? (uint64_t)R : n - r0);
-        {  // row tile: nr * F floats, contiguous in x
-            const float* src = x + r0 * F;
-            const uint32_t words = nr * F;
-            const bool vec = ((reinterpret_cast<uintptr_t>(src) & 15u) == 0) && (words % 4u == 0);
-            if (vec) {
-                for (uint32_t i = tid; i < words / 4u; i += blockDim.x) cp_async16(rows + 4u * i, src + 4u * i);
-            } else {
-                for (uint32_t i = tid; i < words; i += blockDim.x) rows[i] = src[i];
+        // bin: each warp its 32 rows, 32 features at a time; coalesced reads
+        // of the sample-major rows (lanes over features), transposed through
+        // the warp's stage (lanes over rows) into the bin columns
+        const uint32_t rb = warp * 32u;
+        for (uint32_t fc = 0; fc < NF; fc += 32u) {
+            const uint32_t fl = fc + lane;
+            const bool has = fl < NF && (f.feat_col[2 * fl] >= 0 || f.feat_col[2 * fl + 1] >= 0);
+            BinFeat bf{};
+            if (has) bf = bin_feat(f, fl);
+            const float* fs = spl_bytes && has ? spl + fl * HEAP_SPLITTERS : nullptr;
+#pragma unroll 8
+            for (uint32_t i = 0; i < 32u; ++i) {
+                const uint32_t r = rb + i;
+                uint32_t b = 0;
+                if (has && r < nr) b = heap_bin(f, bf, fs, x[(r0 + r) * F + fl]);
+                stage[i * PREDICT_STAGE_LD + lane] = (uint16_t)b;
             }
-            asm volatile("cp.async.commit_group;" ::: "memory");
+            __syncwarp();
+            const uint32_t nf = NF - fc < 32u ? NF - fc : 32u;
+            for (uint32_t j = 0; j < nf; ++j) {
+                const int32_t c0 = f.feat_col[2 * (fc + j)], c1 = f.feat_col[2 * (fc + j) + 1];
+                const uint32_t b = stage[lane * PREDICT_STAGE_LD + j];
+                if (c0 >= 0)  // NaN -> the largest bin
+                    *reinterpret_cast<BinT*>(bins + (uint32_t)c0 * Rb + roff) = (BinT)(b == BIN_NAN ? (BinT)~(BinT)0 : b);
+                if (c1 >= 0)  // NaN -> 0
+                    *reinterpret_cast<BinT*>(bins + (uint32_t)c1 * Rb + roff) = (BinT)(b == BIN_NAN ? 0u : b);
+            }
+            __syncwarp();
         }
-        const bool ok = tid < nr;
-        const float* xr = rows + (size_t)(ok ? tid : 0) * F;
+        __syncthreads();  // bins complete; the stage (ring) is free
         for (uint32_t g = 0; g < f.n_groups; ++g) {
             const uint32_t t0 = f.group_off[g], t1 = f.group_off[g + 1];
             float acc = f.base[g];
@@ -2431,64 +2537,57 @@ k_predict_heap(HeapForest f, const float* __restrict__ x, uint64_t n, uint32_t F
                 } else {
                     asm volatile("cp.async.wait_group 0;" ::: "memory");
                 }
-                __syncthreads();
-                const uint2* tb = ring + (size_t)(c & 1u) * PREDICT_CHUNK * HEAP_NODES;
+                __syncthreads();  // chunk c landed
+                const uint32_t* tb = ring + (size_t)(c & 1u) * PREDICT_CHUNK * HEAP_NODES;
                 const uint32_t nt = min(PREDICT_CHUNK, t1 - (t0 + c * PREDICT_CHUNK));
-                if (ok) {
-                    uint32_t q = 0;
-                    for (; q + PREDICT_IL <= nt; q += PREDICT_IL) {
-                        uint32_t ii[PREDICT_IL];
-                        uint2 nn[PREDICT_IL];
-                        bool dd[PREDICT_IL];
+                uint32_t q = 0;
+                for (; q + PREDICT_IL <= nt; q += PREDICT_IL) {
+                    uint32_t h[PREDICT_IL];
 #pragma unroll
-                        for (uint32_t u = 0; u < PREDICT_IL; ++u) {
-                            ii[u] = 1;
-                            nn[u] = tb[(q + u) * HEAP_NODES + 1];
-                            dd[u] = false;
-                        }
+                    for (uint32_t u = 0; u < PREDICT_IL; ++u) h[u] = 1u;
 #pragma unroll
-                        for (int step = 0; step <= HEAP_DEPTH; ++step) {
+                    for (int step = 0; step < HEAP_DEPTH; ++step) {
 #pragma unroll
-                            for (uint32_t u = 0; u < PREDICT_IL; ++u)
-                                if (!dd[u]) dd[u] = heap_step<CAT>(tb + (q + u) * HEAP_NODES, xr, f, ii[u], nn[u]);
-                        }
-#pragma unroll
-                        for (uint32_t u = 0; u < PREDICT_IL; ++u) acc = acc + __uint_as_float(nn[u].y);
+                        for (uint32_t u = 0; u < PREDICT_IL; ++u)
+                            h[u] = heap_step<CAT, BinT>(tb + (q + u) * HEAP_NODES, cb, Rb, f, h[u]);
                     }
-                    for (; q < nt; ++q) {
-                        const uint2* ta = tb + q * HEAP_NODES;
-                        uint32_t ia = 1;
-                        uint2 na = ta[1];
 #pragma unroll
-                        for (int step = 0; step <= HEAP_DEPTH; ++step)
-                            if (heap_step<CAT>(ta, xr, f, ia, na)) break;
-                        acc = acc + __uint_as_float(na.y);
-                    }
+                    for (uint32_t u = 0; u < PREDICT_IL; ++u) acc = acc + __uint_as_float(tb[(q + u) * HEAP_NODES + h[u]]);
+                }
+                for (; q < nt; ++q) {
+                    const uint32_t* t = tb + q * HEAP_NODES;
+                    uint32_t h1 = 1u;
+#pragma unroll
+                    for (int step = 0; step < HEAP_DEPTH; ++step) h1 = heap_step<CAT, BinT>(t, cb, Rb, f, h1);
+                    acc = acc + __uint_as_float(t[h1]);
                 }
                 __syncthreads();  // ring buffer (c & 1) free for chunk c + 2
             }
-            if (ok) out[(uint64_t)g * n + r0 + tid] = acc;
+            if (tid < nr) out[(uint64_t)g * n + r0 + tid] = acc;
         }
-        __syncthreads();  // row tile free
+        __syncthreads();  // bins and stage free for the next tile
     }
 }
 
 void launch_predict_heap(const HeapForest& f, const float* x, uint64_t n, uint32_t F, float* out, cudaStream_t st) {
     if (n == 0) return;
-    const uint32_t R = predict_heap_rows(F);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_predict_heap<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
-        cudaFuncSetAttribute(k_predict_heap<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
-        attr = true;
-    }
-    const size_t smem = 2u * PREDICT_CHUNK * PREDICT_TREE_BYTES + (size_t)R * F * 4u;
+    const uint32_t R = predict_heap_rows(f, F, n);
+    const size_t smem = PREDICT_RING + predict_spl_bytes(F) + (size_t)R * f.n_cols * (f.bins16 ? 2u : 1u);
     const uint64_t tiles = (n + R - 1) / R;
     const unsigned grid = (unsigned)(tiles < 148u ? tiles : 148u);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_predict_heap<true, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
+        cudaFuncSetAttribute(k_predict_heap<false, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
+        cudaFuncSetAttribute(k_predict_heap<false, uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
+        attr = true;
+    }
     if (f.has_cat)
-        k_predict_heap<true><<<grid, R, smem, st>>>(f, x, n, F, R, out);
+        k_predict_heap<true, uint16_t><<<grid, R, smem, st>>>(f, x, n, F, R, out);
+    else if (f.bins16)
+        k_predict_heap<false, uint16_t><<<grid, R, smem, st>>>(f, x, n, F, R, out);
     else
-        k_predict_heap<false><<<grid, R, smem, st>>>(f, x, n, F, R, out);
+        k_predict_heap<false, uint8_t><<<grid, R, smem, st>>>(f, x, n, F, R, out);
 }
 
 __global__ void k_transform(int t, float* __restrict__ p, uint32_t G, uint64_t n) {

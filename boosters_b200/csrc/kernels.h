@@ -352,28 +352,48 @@ struct ForestDev {
 // out [n_groups][n] raw margins (base score + trees in forest order, f32).
 void launch_predict(const ForestDev& f, const float* x, uint64_t n, uint32_t n_features,
                     int feature_major, float* out, cudaStream_t st);
-// Heap-ordered forest for the shared-memory traversal (trees with leaves at
-// depth <= HEAP_DEPTH): tree t's node i at nodes[t * HEAP_NODES + i], 1-based
-// (root 1, children 2i (left) and 2i + 1 (right), one aligned 16-byte pair;
-// entry 0 unused). Node = (word, value): word = feature (bits 0-15) |
-// leaf << 31 | default_left << 30 | categorical << 29; value = threshold or
-// leaf value (f32 bits), or for a categorical split an index into cat
-// (start, size) pairs over cat_words. Trees are stored grouped by output
-// group in forest order (group_off[g] .. group_off[g + 1]).
+// Heap-ordered forest for the shared-memory traversal: every tree padded to a
+// complete tree of depth HEAP_DEPTH, HEAP_NODES 32-bit words per tree,
+// 1-based (root 1, children 2h (left) and 2h + 1 (right)). Words 1 ..
+// 2^HEAP_DEPTH - 1 are splits, words 2^HEAP_DEPTH .. HEAP_NODES - 1 the f32
+// leaf values reached after exactly HEAP_DEPTH steps; a leaf shallower than
+// that is reached through padding splits that always go left.
+//
+// Rows are binned against the forest's own sorted distinct thresholds
+// thr[thr_off[f] .. thr_off[f + 1]): bin(x) = #{t <= x}, so x < t_k exactly
+// when bin(x) < k + 1. A split reads one bin column of the row tile: each
+// feature has up to two numeric columns, one per missing-value direction
+// (feat_col[2f]: NaN stored as the largest bin, which no split sends left;
+// feat_col[2f + 1]: NaN stored as 0, which every split of that column sends
+// left), or one categorical column (feat_col[2f]: min(category, 65534), NaN
+// 0xFFFF). A numeric split word is K << 16 | column with K = rank + 1 of its
+// threshold: left exactly when bin < K, i.e. bin * 65536 + 65535 < word. A
+// categorical split word is index << 16 | 0x8000 | column, index into cat
+// (start, size | default_left << 31) pairs over cat_words. Bins are u8 when
+// no feature has more than 255 thresholds and nothing is categorical, else
+// u16. Trees are grouped by output group in forest order (group_off[g] ..
+// group_off[g + 1]).
 constexpr int HEAP_DEPTH = 8;
-constexpr uint32_t HEAP_NODES = 512;  // entries 1 .. 2^(HEAP_DEPTH + 1) - 1
+constexpr uint32_t HEAP_NODES = 512;
+constexpr uint32_t HEAP_MAX_COLS = 0x7FFFu;
+constexpr uint32_t HEAP_SPLITTERS = 16;  // per feature, for the binning search
 struct HeapForest {
-    const uint2* nodes;
+    const uint32_t* nodes;
     const uint32_t* group_off;  // [n_groups + 1]
     const uint2* cat;
     const uint32_t* cat_words;
+    const float* thr;           // distinct split thresholds per feature, ascending
+    const uint32_t* thr_off;    // [n_features + 1]
+    const int32_t* feat_col;    // [2 * n_features], -1: no column
+    const uint8_t* feat_cat;    // [n_features]: used by categorical splits
     const float* base;
-    uint32_t n_trees, n_groups;
+    uint32_t n_trees, n_groups, n_features, n_cols;
     int has_cat;  // any categorical split
+    int bins16;   // u16 bin columns (else u8)
 };
-// Rows per block of the shared-memory traversal for F features (0: unusable).
-uint32_t predict_heap_rows(uint32_t n_features);
-// x sample-major [n][n_features]; out [n_groups][n] raw margins.
+// Rows per block of the shared-memory traversal for n rows of F features (0:
+// the forest does not fit; use the node-list traversal).
+uint32_t predict_heap_rows(const HeapForest& f, uint32_t n_features, uint64_t n);
 void launch_predict_heap(const HeapForest& f, const float* x, uint64_t n, uint32_t n_features, float* out,
                          cudaStream_t st);
 // transform: 1 sigmoid, 2 softmax over [G][n]

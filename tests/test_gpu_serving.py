@@ -147,3 +147,66 @@ def test_deep_trees_use_the_node_list_traversal():
     finally:
         srv.close()
     np.testing.assert_array_equal(out, m.predict_group_major(bst.Dataset(rows)))
+
+
+def test_values_on_the_thresholds(model):
+    # the served traversal bins rows against the forest's own thresholds:
+    # values equal to a threshold, one ulp either side, signed zeros,
+    # infinities and NaN must all go the way x < threshold sends them
+    F = model.n_features
+    thr = [[] for _ in range(F)]
+    for i in range(model.n_trees):
+        t = model.tree(i)
+        for k in np.flatnonzero(t["is_leaf"] == 0):
+            thr[t["split_index"][k]].append(t["threshold"][k])
+    rng = np.random.default_rng(5)
+    cols = []
+    for f in range(F):
+        v = np.asarray(thr[f] or [0.0], np.float32)
+        cand = np.concatenate([v, np.nextafter(v, np.float32(-np.inf)), np.nextafter(v, np.float32(np.inf)),
+                               np.array([0.0, -0.0, np.inf, -np.inf, np.nan], np.float32)])
+        cols.append(rng.choice(cand, size=5000))
+    rows = np.ascontiguousarray(np.stack(cols, axis=1).astype(np.float32))
+    srv = bst.PredictionServer(model, raw=True)
+    try:
+        out = srv.wait(srv.submit(rows))
+    finally:
+        srv.close()
+    np.testing.assert_array_equal(out, plain_predict(model, rows, raw=True))
+
+
+def test_large_category_ids():
+    x, y = bst.synth.multiclass(6_000, 6, 2, 3, seed=8)
+    m = bst.GBDTModel.train(bst.Dataset.from_feature_major(x, y, categorical_features=[6, 7]),
+                            bst.GBDTConfig(objective=bst.Objective.softmax(3), n_estimators=4, max_depth=5))
+    rows = np.ascontiguousarray(x[:, :2000].T).copy()
+    rng = np.random.default_rng(6)
+    rows[rng.random(2000) < 0.2, 6] = 70000.0   # beyond any category set
+    rows[rng.random(2000) < 0.2, 7] = -3.0      # negative category -> 0
+    rows[rng.random(2000) < 0.1, 7] = 2.7       # fractional category truncates
+    srv = bst.PredictionServer(m, raw=True)
+    try:
+        out = srv.wait(srv.submit(rows))
+    finally:
+        srv.close()
+    np.testing.assert_array_equal(out, m.predict_group_major(bst.Dataset(rows), raw=True))
+
+
+def test_u16_bin_columns():
+    # more than 255 distinct thresholds on a feature: the traversal bins rows
+    # into u16 columns; both missing-value directions occur
+    x, y = bst.synth.binary(40_000, 12, n_nan_cols=6, seed=10)
+    m = bst.GBDTModel.train(bst.Dataset.from_feature_major(x, y),
+                            bst.GBDTConfig(objective=bst.Objective.logistic(), n_estimators=120, max_depth=7,
+                                           max_bins=1024, learning_rate=0.3))
+    n_thr = max(len(np.unique(np.concatenate(
+        [m.tree(i)["threshold"][(m.tree(i)["is_leaf"] == 0) & (m.tree(i)["split_index"] == f)]
+         for i in range(m.n_trees)]))) for f in range(12))
+    assert n_thr > 255
+    rows = np.ascontiguousarray(x[:, :20_000].T)
+    srv = bst.PredictionServer(m, raw=True)
+    try:
+        out = srv.wait(srv.submit(rows))
+    finally:
+        srv.close()
+    np.testing.assert_array_equal(out, m.predict_group_major(bst.Dataset(rows), raw=True))
