@@ -252,7 +252,7 @@ class Dataset:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and _n is not None and _n.lib is not None:  # not at interpreter exit
             _n.lib.bst_dataset_free(h)
             self._h = None
 
@@ -295,7 +295,7 @@ class BinnedDataset:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and _n is not None and _n.lib is not None:  # not at interpreter exit
             _n.lib.bst_binned_free(h)
             self._h = None
 
@@ -458,7 +458,7 @@ class GBDTModel:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and _n is not None and _n.lib is not None:  # not at interpreter exit
             _n.lib.bst_model_free(h)
             self._h = None
 
@@ -505,7 +505,7 @@ class Booster:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and _n is not None and _n.lib is not None:  # not at interpreter exit
             _n.lib.bst_booster_free(h)
             self._h = None
 
@@ -580,6 +580,38 @@ class PredictionServer:
         _n.check(_n.lib.bst_server_wait(self._h, ticket.id, int(timeout_ms), ctypes.byref(a), ctypes.byref(b)))
         ticket.submit_ns, ticket.done_ns = a.value, b.value
         return ticket.out
+
+    def replay(self, pool, arrival_s, row_off, n_rows, ring=256):
+        """Replays a request schedule from a native thread: request ``i`` is
+        rows ``pool[row_off[i]:row_off[i] + n_rows[i]]`` arriving ``arrival_s[i]``
+        seconds after the start. Returns ``(latency_s, span_s, out)``: each
+        request's completion minus its scheduled arrival, the span from the
+        first arrival to the last completion, and the output ring
+        ``(ring, n_groups, max_rows)`` (request ``i`` in slot ``i % ring``)."""
+        pool = np.asarray(pool)
+        if pool.dtype != np.float32 or not pool.flags.c_contiguous or pool.ndim != 2 \
+                or pool.shape[1] != self.n_features:
+            raise ValueError(f"pool must be a C-contiguous float32 array (rows, {self.n_features})")
+        arr = np.ascontiguousarray(np.round(np.asarray(arrival_s, np.float64) * 1e9), dtype=np.uint64)
+        off = np.ascontiguousarray(row_off, dtype=np.uint64)
+        cnt = np.ascontiguousarray(n_rows, dtype=np.uint64)
+        n_req = len(arr)
+        if len(off) != n_req or len(cnt) != n_req:
+            raise ValueError("arrival_s, row_off and n_rows must have the same length")
+        width = int(cnt.max()) if n_req else 1
+        try:
+            import torch
+            out = torch.empty((ring, self.n_groups, width), dtype=torch.float32).pin_memory().numpy()
+        except Exception:
+            out = np.empty((ring, self.n_groups, width), dtype=np.float32)
+        lat = np.zeros(n_req, np.uint64)
+        span = ctypes.c_uint64()
+        _n.check(_n.lib.bst_server_replay(self._h, ctypes.c_void_p(pool.ctypes.data), pool.shape[0], n_req,
+                                          ctypes.c_void_p(arr.ctypes.data), ctypes.c_void_p(off.ctypes.data),
+                                          ctypes.c_void_p(cnt.ctypes.data), ctypes.c_void_p(out.ctypes.data),
+                                          ring, self.n_groups * width, ctypes.c_void_p(lat.ctypes.data),
+                                          ctypes.byref(span)))
+        return lat.astype(np.float64) / 1e9, span.value / 1e9, out
 
     def stats(self):
         st = _n.ServerStats()

@@ -170,6 +170,9 @@ SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64),
       ctypes.POINTER(ctypes.c_uint64)]),
     ("bst_server_stats_get", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
+    ("bst_server_replay", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
     ("bst_server_free", None, [ctypes.c_void_p]),
     ("bst_synth_regression", ctypes.c_int32,
      [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, c_f32p, c_f32p]),

@@ -865,6 +865,18 @@ bst_status bst_server_stats_get(bst_server* server, bst_server_stats* out) {
     return BST_OK;
 }
 
+bst_status bst_server_replay(bst_server* server, const float* pool, uint64_t pool_rows, uint64_t n_req,
+                             const uint64_t* arrival_ns, const uint64_t* row_off, const uint64_t* n_rows, float* out,
+                             uint64_t ring, uint64_t ring_stride, uint64_t* latency_ns, uint64_t* span_ns) {
+    if (!server || (n_req && (!pool || !arrival_ns || !row_off || !n_rows || !out || !latency_ns)))
+        return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    return guarded([&]() -> bst_status {
+        bst::server_replay(*server->s, pool, pool_rows, n_req, arrival_ns, row_off, n_rows, out, ring, ring_stride,
+                           latency_ns, span_ns);
+        return BST_OK;
+    });
+}
+
 void bst_server_free(bst_server* server) { delete server; }
 
 bst_status bst_metric(int32_t metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w,

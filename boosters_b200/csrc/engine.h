@@ -159,6 +159,9 @@ uint64_t server_submit(Server& s, const float* rows, uint64_t n, float* out);
 int server_wait(Server& s, uint64_t id, int64_t timeout_ms, uint64_t* submit_ns, uint64_t* done_ns,
                 std::string* err);
 void server_stats(Server& s, bst_server_stats* out);
+void server_replay(Server& s, const float* pool, uint64_t pool_rows, uint64_t n_req, const uint64_t* arrival_ns,
+                   const uint64_t* row_off, const uint64_t* n_rows, float* out, uint64_t ring, uint64_t ring_stride,
+                   uint64_t* latency_ns, uint64_t* span_ns);
 void build_hist_tiles(const BinPlan& p, std::vector<HistTile>& tiles, uint32_t& max_smem,
                       const std::vector<uint8_t>* only = nullptr);
 void build_lane_tiles(const BinPlan& p, uint32_t max_bins, std::vector<LaneTile>& tiles, uint32_t& tile_bins,

@@ -2368,20 +2368,38 @@ __host__ __device__ inline uint32_t predict_spl_bytes(uint32_t F) {
     return F <= PREDICT_SPL_MAX_F ? F * HEAP_SPLITTERS * 4u : 0u;
 }
 
-uint32_t predict_heap_rows(const HeapForest& f, uint32_t F, uint64_t n) {
-    if (F == 0 || f.n_cols == 0 || f.n_cols > HEAP_MAX_COLS) return 0;
+// Launch shape of the traversal: R rows per tile, the trees of each chunk
+// split over S thread groups of R threads (S > 1 for small batches: each
+// group walks its share of the chunk's trees and leaves the values in
+// shared memory, where the row's group-0 thread adds them in forest order).
+struct HeapPlan {
+    uint32_t R = 0, S = 1;
+    size_t smem = 0;
+};
+
+static HeapPlan heap_plan(const HeapForest& f, uint32_t F, uint64_t n) {
+    HeapPlan p;
+    if (F == 0 || f.n_cols == 0 || f.n_cols > HEAP_MAX_COLS) return p;
     const uint64_t fixed = PREDICT_RING + predict_spl_bytes(F);
     const uint64_t per_row = (uint64_t)f.n_cols * (f.bins16 ? 2u : 1u);
-    uint64_t r = (PREDICT_SMEM - fixed) / per_row;
-    if (r > PREDICT_MAX_ROWS) r = PREDICT_MAX_ROWS;
-    r &= ~(uint64_t)(PREDICT_MIN_ROWS - 1);
-    if (r < PREDICT_MIN_ROWS) return 0;
+    if (fixed + per_row * PREDICT_MIN_ROWS > PREDICT_SMEM) return p;
+    uint64_t rmax = (PREDICT_SMEM - fixed) / per_row;
+    if (rmax > PREDICT_MAX_ROWS) rmax = PREDICT_MAX_ROWS;
+    rmax &= ~(uint64_t)(PREDICT_MIN_ROWS - 1);
     // spread a small batch over every SM: about n / 148 rows per block
-    uint64_t want = (n + 147) / 148;
-    want = (want + PREDICT_MIN_ROWS - 1) / PREDICT_MIN_ROWS * PREDICT_MIN_ROWS;
-    if (want < PREDICT_MIN_ROWS) want = PREDICT_MIN_ROWS;
-    return (uint32_t)(want < r ? want : r);
+    uint64_t r = (n + 147) / 148;
+    r = (r + PREDICT_MIN_ROWS - 1) / PREDICT_MIN_ROWS * PREDICT_MIN_ROWS;
+    if (r < PREDICT_MIN_ROWS) r = PREDICT_MIN_ROWS;
+    if (r > rmax) r = rmax;
+    uint32_t S = r <= 128 ? 4u : (r <= 384 ? 2u : 1u);
+    if (S > 1 && fixed + r * (per_row + PREDICT_CHUNK * 4u) > PREDICT_SMEM) S = 1;
+    p.R = (uint32_t)r;
+    p.S = S;
+    p.smem = fixed + (S > 1 ? (size_t)PREDICT_CHUNK * 4u * r : 0) + (size_t)r * per_row;
+    return p;
 }
+
+uint32_t predict_heap_rows(const HeapForest& f, uint32_t F, uint64_t n) { return heap_plan(f, F, n).R; }
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
@@ -2459,19 +2477,48 @@ __device__ __forceinline__ uint32_t heap_step(const uint32_t* tree, const unsign
     return 2u * h + (left ? 0u : 1u);
 }
 
+// Leaf values of trees [q0, q1) of the chunk at tb for this thread's row,
+// PREDICT_IL chains at a time; emit(q, value) in tree order.
+template <bool CAT, typename BinT, typename Emit>
+__device__ __forceinline__ void heap_walk(const uint32_t* tb, uint32_t q0, uint32_t q1, const unsigned char* cb,
+                                          uint32_t Rb, const HeapForest& f, Emit emit) {
+    uint32_t q = q0;
+    for (; q + PREDICT_IL <= q1; q += PREDICT_IL) {
+        uint32_t h[PREDICT_IL];
+#pragma unroll
+        for (uint32_t u = 0; u < PREDICT_IL; ++u) h[u] = 1u;
+#pragma unroll
+        for (int step = 0; step < HEAP_DEPTH; ++step) {
+#pragma unroll
+            for (uint32_t u = 0; u < PREDICT_IL; ++u) h[u] = heap_step<CAT, BinT>(tb + (q + u) * HEAP_NODES, cb, Rb, f, h[u]);
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < PREDICT_IL; ++u) emit(q + u, __uint_as_float(tb[(q + u) * HEAP_NODES + h[u]]));
+    }
+    for (; q < q1; ++q) {
+        const uint32_t* t = tb + q * HEAP_NODES;
+        uint32_t h1 = 1u;
+#pragma unroll
+        for (int step = 0; step < HEAP_DEPTH; ++step) h1 = heap_step<CAT, BinT>(t, cb, Rb, f, h1);
+        emit(q, __uint_as_float(t[h1]));
+    }
+}
+
 template <bool CAT, typename BinT>
 __global__ void __launch_bounds__(PREDICT_MAX_ROWS, 1)
-k_predict_heap(HeapForest f, const float* __restrict__ x, uint64_t n, uint32_t F, uint32_t R,
+k_predict_heap(HeapForest f, const float* __restrict__ x, uint64_t n, uint32_t F, uint32_t R, uint32_t S,
                float* __restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* ring = reinterpret_cast<uint32_t*>(smem_raw);  // [2][PREDICT_CHUNK][HEAP_NODES]
     const uint32_t spl_bytes = predict_spl_bytes(F);
     float* spl = reinterpret_cast<float*>(smem_raw + PREDICT_RING);
-    unsigned char* bins = smem_raw + PREDICT_RING + spl_bytes;
+    float* lv = reinterpret_cast<float*>(smem_raw + PREDICT_RING + spl_bytes);  // [PREDICT_CHUNK][R] when S > 1
+    unsigned char* bins = smem_raw + PREDICT_RING + spl_bytes + (S > 1 ? PREDICT_CHUNK * 4u * R : 0u);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t rg = tid % R, sg = tid / R;  // row in the tile, tree group
     const uint32_t Rb = R * (uint32_t)sizeof(BinT);
-    const uint32_t roff = sizeof(BinT) == 1 ? (tid >> 7) * 128u + 4u * lane + ((tid >> 5) & 3u)
-                                            : (tid >> 6) * 128u + 4u * lane + 2u * ((tid >> 5) & 1u);
+    const uint32_t roff = sizeof(BinT) == 1 ? (rg >> 7) * 128u + 4u * lane + ((rg >> 5) & 3u)
+                                            : (rg >> 6) * 128u + 4u * lane + 2u * ((rg >> 5) & 1u);
     const unsigned char* cb = bins + roff;
     uint16_t* stage = reinterpret_cast<uint16_t*>(smem_raw) + (size_t)warp * (PREDICT_STAGE / 2u);
     const uint32_t NF = F < f.n_features ? F : f.n_features;  // features any split reads
@@ -2487,11 +2534,12 @@ k_predict_heap(HeapForest f, const float* __restrict__ x, uint64_t n, uint32_t F
     for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const uint64_t r0 = tile * R;
         const uint32_t nr = (uint32_t)((uint64_t)R < n - r0 ? (uint64_t)R : n - r0);
-        // bin: each warp its 32 rows, 32 features at a time; coalesced reads
-        // of the sample-major rows (lanes over features), transposed through
-        // the warp's stage (lanes over rows) into the bin columns
-        const uint32_t rb = warp * 32u;
-        for (uint32_t fc = 0; fc < NF; fc += 32u) {
+        // bin: each warp 32 rows, 32 features at a time (the tree groups take
+        // turns over the feature chunks); coalesced reads of the sample-major
+        // rows (lanes over features), transposed through the warp's stage
+        // (lanes over rows) into the bin columns
+        const uint32_t rb = rg & ~31u;
+        for (uint32_t fc = sg * 32u; fc < NF; fc += 32u * S) {
             const uint32_t fl = fc + lane;
             const bool has = fl < NF && (f.feat_col[2 * fl] >= 0 || f.feat_col[2 * fl + 1] >= 0);
             BinFeat bf{};
@@ -2537,33 +2585,22 @@ k_predict_heap(HeapForest f, const float* __restrict__ x, uint64_t n, uint32_t F
                 } else {
                     asm volatile("cp.async.wait_group 0;" ::: "memory");
                 }
-                __syncthreads();  // chunk c landed
+                __syncthreads();  // chunk c landed; the previous chunk's leaf values are summed
                 const uint32_t* tb = ring + (size_t)(c & 1u) * PREDICT_CHUNK * HEAP_NODES;
                 const uint32_t nt = min(PREDICT_CHUNK, t1 - (t0 + c * PREDICT_CHUNK));
-                uint32_t q = 0;
-                for (; q + PREDICT_IL <= nt; q += PREDICT_IL) {
-                    uint32_t h[PREDICT_IL];
-#pragma unroll
-                    for (uint32_t u = 0; u < PREDICT_IL; ++u) h[u] = 1u;
-#pragma unroll
-                    for (int step = 0; step < HEAP_DEPTH; ++step) {
-#pragma unroll
-                        for (uint32_t u = 0; u < PREDICT_IL; ++u)
-                            h[u] = heap_step<CAT, BinT>(tb + (q + u) * HEAP_NODES, cb, Rb, f, h[u]);
-                    }
-#pragma unroll
-                    for (uint32_t u = 0; u < PREDICT_IL; ++u) acc = acc + __uint_as_float(tb[(q + u) * HEAP_NODES + h[u]]);
-                }
-                for (; q < nt; ++q) {
-                    const uint32_t* t = tb + q * HEAP_NODES;
-                    uint32_t h1 = 1u;
-#pragma unroll
-                    for (int step = 0; step < HEAP_DEPTH; ++step) h1 = heap_step<CAT, BinT>(t, cb, Rb, f, h1);
-                    acc = acc + __uint_as_float(t[h1]);
+                if (S == 1) {
+                    heap_walk<CAT, BinT>(tb, 0, nt, cb, Rb, f, [&](uint32_t, float v) { acc = acc + v; });
+                } else {
+                    const uint32_t per = PREDICT_CHUNK / S;  // S divides the chunk
+                    const uint32_t q0 = min(sg * per, nt), q1 = min(q0 + per, nt);
+                    heap_walk<CAT, BinT>(tb, q0, q1, cb, Rb, f, [&](uint32_t q, float v) { lv[q * R + rg] = v; });
+                    __syncthreads();
+                    if (sg == 0)
+                        for (uint32_t q = 0; q < nt; ++q) acc = acc + lv[q * R + rg];
                 }
                 __syncthreads();  // ring buffer (c & 1) free for chunk c + 2
             }
-            if (tid < nr) out[(uint64_t)g * n + r0 + tid] = acc;
+            if (sg == 0 && rg < nr) out[(uint64_t)g * n + r0 + rg] = acc;
         }
         __syncthreads();  // bins and stage free for the next tile
     }
@@ -2571,23 +2608,17 @@ k_predict_heap(HeapForest f, const float* __restrict__ x, uint64_t n, uint32_t F
 
 void launch_predict_heap(const HeapForest& f, const float* x, uint64_t n, uint32_t F, float* out, cudaStream_t st) {
     if (n == 0) return;
-    const uint32_t R = predict_heap_rows(f, F, n);
-    const size_t smem = PREDICT_RING + predict_spl_bytes(F) + (size_t)R * f.n_cols * (f.bins16 ? 2u : 1u);
-    const uint64_t tiles = (n + R - 1) / R;
+    const HeapPlan p = heap_plan(f, F, n);
+    const uint64_t tiles = (n + p.R - 1) / p.R;
     const unsigned grid = (unsigned)(tiles < 148u ? tiles : 148u);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_predict_heap<true, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
-        cudaFuncSetAttribute(k_predict_heap<false, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
-        cudaFuncSetAttribute(k_predict_heap<false, uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
-        attr = true;
-    }
+    const unsigned threads = p.R * p.S;
+    init_kernel_attributes();  // per device: the traversal's shared-memory opt-in
     if (f.has_cat)
-        k_predict_heap<true, uint16_t><<<grid, R, smem, st>>>(f, x, n, F, R, out);
+        k_predict_heap<true, uint16_t><<<grid, threads, p.smem, st>>>(f, x, n, F, p.R, p.S, out);
     else if (f.bins16)
-        k_predict_heap<false, uint16_t><<<grid, R, smem, st>>>(f, x, n, F, R, out);
+        k_predict_heap<false, uint16_t><<<grid, threads, p.smem, st>>>(f, x, n, F, p.R, p.S, out);
     else
-        k_predict_heap<false, uint8_t><<<grid, R, smem, st>>>(f, x, n, F, R, out);
+        k_predict_heap<false, uint8_t><<<grid, threads, p.smem, st>>>(f, x, n, F, p.R, p.S, out);
 }
 
 __global__ void k_transform(int t, float* __restrict__ p, uint32_t G, uint64_t n) {
@@ -2631,6 +2662,9 @@ void init_kernel_attributes() {
     if (cudaGetDevice(&dev) != cudaSuccess) return;
     const unsigned long long bit = dev < 64 ? (1ull << dev) : 0ull;
     if (bit && (done.load() & bit)) return;
+    cudaFuncSetAttribute(k_predict_heap<true, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
+    cudaFuncSetAttribute(k_predict_heap<false, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
+    cudaFuncSetAttribute(k_predict_heap<false, uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
     const int hist_smem = 200 * 1024;
     cudaFuncSetAttribute(k_hist_build<GRAD_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
     cudaFuncSetAttribute(k_hist_build<GRAD_Q16>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);

@@ -3,17 +3,17 @@
 // at a time through Predictor::predict_into, inference/gbdt/predictor.rs:197).
 //
 // Requests (sample-major f32 rows, caller-owned input and output buffers)
-// queue FIFO. A dispatcher thread coalesces the queue head into a batch that
-// fits one of SLOTS in-flight slots (device input / output buffers sized by
-// the memory budget), copies each request's rows straight from the caller's
-// buffer into the slot's device input, runs ONE traversal launch over the
-// whole batch and copies each request's outputs straight back, all on the
-// slot's stream. While batch k runs, batch k + 1 forms from requests that
-// arrived meanwhile and is issued on the next slot's stream, so copies and
-// traversals of consecutive batches overlap on the device. A completion
-// thread retires slots in order and wakes the waiters. A row's prediction
-// depends on that row alone (trees summed in forest order per row), so every
-// result is identical whatever batch it shares.
+// are admitted FIFO into a device row ring as soon as it has room: the
+// admission issues the request's host-to-device copy at once on the copy
+// stream, so copies proceed while earlier batches traverse. A dispatcher
+// coalesces admitted requests that sit contiguously in the ring into one
+// batch per free slot (SLOTS batches in flight), makes the slot's stream
+// wait for the batch's last copy, runs ONE traversal launch over the ring
+// span and copies each request's outputs straight back to the caller. A
+// completion thread retires batches in order, frees their ring span, admits
+// waiting requests and wakes the waiters. A row's prediction depends on that
+// row alone (trees summed in forest order per row), so every result is
+// identical whatever batch it shares.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -40,6 +40,10 @@ uint64_t now_ns() {
 
 struct Server {
     static constexpr int SLOTS = 3;
+    // Coalescing stops at one full wave of the traversal (148 SMs x 768-row
+    // tiles) unless the caller caps batches explicitly: a larger batch runs
+    // in two waves and holds every request in it for both.
+    static constexpr uint64_t COALESCE_ROWS = 148ull * 768ull;
 
     struct Req {
         uint64_t id = 0;
@@ -47,26 +51,33 @@ struct Server {
         uint64_t n = 0;
         float* out = nullptr;
         uint64_t submit_ns = 0, done_ns = 0;
-        int status = -1;  // -1 pending, else bst_status
+        int status = -1;      // -1 pending, else bst_status
+        uint64_t pos = 0;     // first ring row, once admitted
+        cudaEvent_t copied = nullptr;  // recorded after the request's copy
     };
     struct Slot {
-        DevArray<float> d_in, d_out;
+        DevArray<float> d_out;
         cudaStream_t st = nullptr;
         cudaEvent_t done = nullptr;
-        std::vector<uint64_t> reqs;  // ticket ids
+        std::vector<uint64_t> reqs;  // ticket ids, in ring order
         bool busy = false;
     };
 
     const Model& m;
-    uint64_t F = 0, G = 1, max_rows = 0;
+    uint64_t F = 0, G = 1, max_rows = 0, coalesce_rows = 0, ring_rows = 0;
     bool raw = false;
     int device = 0;
 
     std::mutex mu;
-    std::condition_variable cv_submit, cv_slot, cv_done, cv_inflight;
-    std::deque<uint64_t> queue;
+    std::condition_variable cv_work, cv_done, cv_inflight;
     std::unordered_map<uint64_t, Req> reqs;
-    std::deque<int> inflight;  // slot indices in issue order
+    std::deque<uint64_t> pending;   // waiting for ring room
+    std::deque<uint64_t> admitted;  // copy issued, not yet in a batch
+    std::deque<std::pair<uint64_t, uint64_t>> live;  // ring spans (start, n) of admitted requests, in order
+    std::deque<int> inflight;       // slot indices in issue order
+    std::vector<cudaEvent_t> events;  // free copy events
+    DevArray<float> ring;
+    cudaStream_t cst = nullptr;     // host-to-device copies
     Slot slots[SLOTS];
     uint64_t next_id = 1;
     bool stop = false;
@@ -86,9 +97,12 @@ struct Server {
         if (max_rows == 0)
             throw Error{BST_ERR_INVALID_ARGUMENT, "memory budget below one row per in-flight slot"};
         if (max_rows > 0xFFFFFFFFull) max_rows = 0xFFFFFFFFull;
+        coalesce_rows = cap ? max_rows : std::min(max_rows, COALESCE_ROWS);
+        ring_rows = (uint64_t)SLOTS * max_rows;  // the slots' input share of the budget
         (void)m.device_forest();  // forest resident before the first request
+        ring.alloc((size_t)ring_rows * std::max<uint64_t>(1, F));
+        BST_CK(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking));
         for (auto& s : slots) {
-            s.d_in.alloc((size_t)max_rows * std::max<uint64_t>(1, F));
             s.d_out.alloc((size_t)max_rows * G);
             BST_CK(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
             BST_CK(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
@@ -104,24 +118,84 @@ struct Server {
             std::unique_lock<std::mutex> lk(mu);
             cv_done.wait(lk, [&] {
                 if (error != BST_OK) return true;
-                if (!queue.empty() || !inflight.empty()) return false;
+                if (!pending.empty() || !admitted.empty() || !inflight.empty()) return false;
                 for (auto& s : slots)
                     if (s.busy) return false;
                 return true;
             });
             stop = true;
         }
-        cv_submit.notify_all();
-        cv_slot.notify_all();
+        cv_work.notify_all();
         cv_inflight.notify_all();
         if (dispatcher.joinable()) dispatcher.join();
         if (completer.joinable()) completer.join();
         cudaSetDevice(device);
+        if (cst) cudaStreamSynchronize(cst);
         for (auto& s : slots) {
             if (s.st) cudaStreamSynchronize(s.st);
             if (s.done) cudaEventDestroy(s.done);
             if (s.st) cudaStreamDestroy(s.st);
         }
+        for (auto& kv : reqs)
+            if (kv.second.copied) cudaEventDestroy(kv.second.copied);
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+        if (cst) cudaStreamDestroy(cst);
+    }
+
+    // Ring room for n rows after the live spans (contiguous; wraps to row 0).
+    bool ring_alloc(uint64_t n, uint64_t* pos) const {
+        if (live.empty()) {
+            *pos = 0;
+            return n <= ring_rows;
+        }
+        const uint64_t tail = live.front().first;
+        const uint64_t head = live.back().first + live.back().second;
+        // wrapped when the newest span starts before the oldest: the free
+        // room is then [head, tail) alone (empty when head == tail)
+        if (live.back().first >= tail) {
+            if (n <= ring_rows - head) {
+                *pos = head;
+                return true;
+            }
+            if (n <= tail) {
+                *pos = 0;
+                return true;
+            }
+            return false;
+        }
+        if (n <= tail - head) {
+            *pos = head;
+            return true;
+        }
+        return false;
+    }
+
+    // Admits waiting requests while the ring has room: issues their copies.
+    // Caller holds mu.
+    void admit_locked() {
+        bool any = false;
+        while (!pending.empty() && error == BST_OK) {
+            Req& r = reqs[pending.front()];
+            uint64_t pos;
+            if (!ring_alloc(r.n, &pos)) break;
+            cudaEvent_t ev;
+            if (!events.empty()) {
+                ev = events.back();
+                events.pop_back();
+            } else {
+                BST_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            }
+            r.copied = ev;
+            r.pos = pos;
+            if (F)
+                BST_CK(cudaMemcpyAsync(ring.p + pos * F, r.rows, sizeof(float) * r.n * F, cudaMemcpyHostToDevice, cst));
+            BST_CK(cudaEventRecord(ev, cst));
+            live.emplace_back(pos, r.n);
+            admitted.push_back(r.id);
+            pending.pop_front();
+            any = true;
+        }
+        if (any) cv_work.notify_one();
     }
 
     uint64_t submit(const float* rows, uint64_t n, float* out) {
@@ -137,10 +211,22 @@ struct Server {
         r.n = n;
         r.out = out;
         r.submit_ns = now_ns();
-        reqs.emplace(r.id, r);
-        queue.push_back(r.id);
         stats.submitted += 1;
-        cv_submit.notify_one();
+        if (n == 0) {  // nothing to predict: complete at once
+            r.status = BST_OK;
+            r.done_ns = r.submit_ns;
+            stats.completed += 1;
+            reqs.emplace(r.id, r);
+            return r.id;
+        }
+        reqs.emplace(r.id, r);
+        pending.push_back(r.id);
+        try {
+            BST_CK(cudaSetDevice(device));
+            admit_locked();
+        } catch (const Error& e) {
+            fail_all(e.code, e.msg);
+        }
         return r.id;
     }
 
@@ -154,6 +240,7 @@ struct Server {
             return BST_ERR_TIMEOUT;
         const Req r = reqs[id];
         reqs.erase(id);
+        if (r.copied && r.status != BST_OK) cudaEventDestroy(r.copied);  // never returned to the pool
         if (submit_ns) *submit_ns = r.submit_ns;
         if (done_ns) *done_ns = r.done_ns;
         return r.status;
@@ -164,14 +251,17 @@ struct Server {
             error = code;
             error_msg = msg;
         }
+        if (cst) cudaStreamSynchronize(cst);  // no copy still reads a caller's rows
         const uint64_t t = now_ns();
         for (auto& kv : reqs)
             if (kv.second.status < 0) {
                 kv.second.status = code;
                 kv.second.done_ns = t;
             }
-        queue.clear();
+        pending.clear();
+        admitted.clear();
         cv_done.notify_all();
+        cv_work.notify_all();
     }
 
     void dispatch_loop() {
@@ -184,10 +274,9 @@ struct Server {
             uint64_t rows = 0;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_submit.wait(lk, [&] { return stop || !queue.empty(); });
-                if (stop) return;
-                cv_slot.wait(lk, [&] {
+                cv_work.wait(lk, [&] {
                     if (stop) return true;
+                    if (admitted.empty()) return false;
                     for (int i = 0; i < SLOTS; ++i)
                         if (!slots[i].busy) return true;
                     return false;
@@ -198,13 +287,15 @@ struct Server {
                         si = i;
                         break;
                     }
-                // admission: the queue head while the batch fits the slot
-                while (!queue.empty()) {
-                    const Req& r = reqs[queue.front()];
-                    if (rows + r.n > max_rows) break;
+                // the admitted head while contiguous in the ring and within
+                // the coalescing limit (a single request up to the capacity)
+                while (!admitted.empty()) {
+                    const Req& r = reqs[admitted.front()];
+                    if (!batch.empty() && (rows + r.n > coalesce_rows || r.pos != batch.back().pos + batch.back().n))
+                        break;
                     batch.push_back(r);
                     rows += r.n;
-                    queue.pop_front();
+                    admitted.pop_front();
                 }
                 Slot& s = slots[si];
                 s.busy = true;
@@ -216,19 +307,13 @@ struct Server {
             }
             Slot& s = slots[si];
             try {
-                uint64_t off = 0;
-                for (auto& r : batch) {
-                    if (r.n && F)
-                        BST_CK(cudaMemcpyAsync(s.d_in.p + off * F, r.rows, sizeof(float) * r.n * F,
-                                               cudaMemcpyHostToDevice, s.st));
-                    off += r.n;
-                }
-                forest_predict_rows(f, s.d_in.p, rows, F, s.d_out.p, s.st);
+                BST_CK(cudaStreamWaitEvent(s.st, batch.back().copied, 0));  // copies are in order on cst
+                forest_predict_rows(f, ring.p + batch.front().pos * F, rows, F, s.d_out.p, s.st);
                 if (!raw) launch_transform(tr, s.d_out.p, (uint32_t)G, rows, s.st);
                 BST_CK(cudaGetLastError());
-                off = 0;
+                uint64_t off = 0;
                 for (auto& r : batch) {
-                    for (uint64_t g = 0; g < G && r.n; ++g)
+                    for (uint64_t g = 0; g < G; ++g)
                         BST_CK(cudaMemcpyAsync(r.out + g * r.n, s.d_out.p + g * rows + off, sizeof(float) * r.n,
                                                cudaMemcpyDeviceToHost, s.st));
                     off += r.n;
@@ -238,7 +323,6 @@ struct Server {
                 std::lock_guard<std::mutex> lk(mu);
                 fail_all(e.code, e.msg);
                 s.busy = false;
-                cv_slot.notify_one();
                 continue;
             }
             {
@@ -273,15 +357,114 @@ struct Server {
                     if (it == reqs.end()) continue;
                     it->second.status = BST_OK;
                     it->second.done_ns = t;
+                    if (it->second.copied) {
+                        events.push_back(it->second.copied);
+                        it->second.copied = nullptr;
+                    }
+                    if (!live.empty()) live.pop_front();  // batches retire in admission order
                 }
                 stats.completed += s.reqs.size();
+                try {
+                    admit_locked();
+                } catch (const Error& err) {
+                    fail_all(err.code, err.msg);
+                }
             }
             s.busy = false;
             cv_done.notify_all();
-            cv_slot.notify_one();
+            cv_work.notify_one();
         }
     }
 };
+
+// Load replay: requests submitted from this thread at scheduled steady-clock
+// times, completions collected by a second thread, latency counted from the
+// scheduled arrival (a late submission counts against the server).
+void server_replay(Server& s, const float* pool, uint64_t pool_rows, uint64_t n_req, const uint64_t* arrival_ns,
+                   const uint64_t* row_off, const uint64_t* n_rows, float* out, uint64_t ring, uint64_t ring_stride,
+                   uint64_t* latency_ns, uint64_t* span_ns) {
+    if (ring == 0) throw Error{BST_ERR_INVALID_ARGUMENT, "replay ring must hold at least one request"};
+    for (uint64_t i = 0; i < n_req; ++i) {
+        if (row_off[i] > pool_rows || n_rows[i] > pool_rows - row_off[i])
+            throw Error{BST_ERR_INVALID_ARGUMENT, "replay request " + std::to_string(i) + " outside the row pool"};
+        if (n_rows[i] * s.G > ring_stride)
+            throw Error{BST_ERR_INVALID_ARGUMENT, "replay ring slot smaller than a request's output"};
+        if (i && arrival_ns[i] < arrival_ns[i - 1])
+            throw Error{BST_ERR_INVALID_ARGUMENT, "replay arrivals must be non-decreasing"};
+    }
+    std::vector<uint64_t> ticket(n_req, 0);
+    std::mutex mu;
+    std::condition_variable cv;
+    uint64_t published = 0, completed = 0, last_done = 0;
+    bool submit_done = false, wait_failed = false;
+    int err = BST_OK;
+    std::string err_msg;
+    const uint64_t start = now_ns() + 1000000ull;  // 1 ms lead
+    // the waiter retires every published ticket in order (the server holds
+    // the caller's ring slots until then)
+    std::thread waiter([&] {
+        for (uint64_t i = 0;; ++i) {
+            uint64_t id;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv.wait(lk, [&] { return published > i || submit_done; });
+                if (published <= i) return;
+                id = ticket[i];
+            }
+            uint64_t sub = 0, done = 0;
+            std::string msg;
+            const int st = server_wait(s, id, -1, &sub, &done, &msg);
+            std::lock_guard<std::mutex> lk(mu);
+            if (st != BST_OK && !wait_failed) {
+                wait_failed = true;
+                err = st;
+                err_msg = msg;
+            }
+            const uint64_t due = start + arrival_ns[i];
+            latency_ns[i] = done > due ? done - due : 0;
+            last_done = std::max(last_done, done);
+            completed = i + 1;
+            cv.notify_all();
+        }
+    });
+    for (uint64_t i = 0; i < n_req; ++i) {
+        const uint64_t due = start + arrival_ns[i];
+        const uint64_t now = now_ns();
+        if (due > now + 200000ull)  // sleep to 200 us before, then spin
+            std::this_thread::sleep_for(std::chrono::nanoseconds(due - now - 200000ull));
+        while (now_ns() < due) {
+        }
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv.wait(lk, [&] { return wait_failed || i < ring || completed > i - ring; });  // output slot free
+            if (wait_failed) break;
+        }
+        uint64_t id = 0;
+        try {
+            id = server_submit(s, pool + row_off[i] * s.F, n_rows[i], out + (i % ring) * ring_stride);
+        } catch (const Error& e) {
+            std::lock_guard<std::mutex> lk(mu);
+            if (err == BST_OK) {
+                err = e.code;
+                err_msg = e.msg;
+            }
+            break;
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        ticket[i] = id;
+        published = i + 1;
+        cv.notify_all();
+    }
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        submit_done = true;
+        cv.notify_all();
+    }
+    waiter.join();
+    if (err != BST_OK) throw Error{(bst_status)err, err_msg};
+    const uint64_t first = start + (n_req ? arrival_ns[0] : 0);
+    if (span_ns) *span_ns = last_done > first ? last_done - first : 0;
+}
 
 Server* server_create(const Model& m, uint64_t mem_budget_bytes, uint64_t max_batch_rows, bool raw) {
     return new Server(m, mem_budget_bytes, max_batch_rows, raw);

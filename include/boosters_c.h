@@ -366,8 +366,10 @@ typedef struct bst_server_stats {
 
 /* The model stays device-resident and must outlive the server. The device
  * memory of the in-flight batches (3 slots of input + output rows) is bounded
- * by mem_budget_bytes; max_batch_rows (0 = no extra cap) further caps a
- * batch. raw != 0: margins; else the objective's transform. */
+ * by mem_budget_bytes; max_batch_rows caps a batch further (0: requests
+ * coalesce up to one full wave of the traversal, 113,664 rows, and a single
+ * request may fill a whole slot). raw != 0: margins; else the objective's
+ * transform. */
 bst_status bst_server_create(const bst_model* model, uint64_t mem_budget_bytes, uint64_t max_batch_rows,
                              int32_t raw, bst_server** out);
 /* Queues n_rows sample-major rows [n_rows, n_features] f32 for prediction
@@ -384,6 +386,17 @@ bst_status bst_server_submit(bst_server* server, const float* rows, uint64_t n_r
 bst_status bst_server_wait(bst_server* server, uint64_t ticket, int64_t timeout_ms, uint64_t* submit_ns,
                            uint64_t* done_ns);
 bst_status bst_server_stats_get(bst_server* server, bst_server_stats* out);
+/* Load replay (capacity planning and latency measurement): submits n_req
+ * requests from a native thread at steady-clock offsets arrival_ns[i]
+ * (non-decreasing, from a start 1 ms after the call), request i being rows
+ * [row_off[i], row_off[i] + n_rows[i]) of the sample-major pool, its
+ * predictions written to out + (i % ring) * ring_stride (a slot is reused
+ * once the request ring positions earlier has completed). latency_ns[i] =
+ * completion of the request's batch - its scheduled arrival; *span_ns (may
+ * be NULL) = last completion - first scheduled arrival. */
+bst_status bst_server_replay(bst_server* server, const float* pool, uint64_t pool_rows, uint64_t n_req,
+                             const uint64_t* arrival_ns, const uint64_t* row_off, const uint64_t* n_rows, float* out,
+                             uint64_t ring, uint64_t ring_stride, uint64_t* latency_ns, uint64_t* span_ns);
 /* Completes every queued request, then frees the server. */
 void bst_server_free(bst_server* server);
 

@@ -210,3 +210,49 @@ def test_u16_bin_columns():
     finally:
         srv.close()
     np.testing.assert_array_equal(out, m.predict_group_major(bst.Dataset(rows), raw=True))
+
+
+def test_replay_schedule(model):
+    rng = np.random.default_rng(12)
+    F = model.n_features
+    pool = request_rows(rng, 50_000, F)
+    n_req = 300
+    sizes = np.clip(np.floor(np.exp(rng.uniform(0, np.log(4097), n_req))).astype(np.int64), 1, 4096)
+    offs = rng.integers(0, 50_000 - 4096, n_req)
+    arrival = np.cumsum(rng.exponential(1 / 20_000, n_req))
+    want = plain_predict(model, pool, raw=True)
+    srv = bst.PredictionServer(model, raw=True)
+    try:
+        lat, span, out = srv.replay(pool, arrival, offs, sizes, ring=n_req)
+        with pytest.raises(n.BoostersError, match="pool"):
+            srv.replay(pool, [0.0], [49_999], [2])
+        st = srv.stats()
+    finally:
+        srv.close()
+    for i in range(n_req):
+        np.testing.assert_array_equal(out[i, :, :sizes[i]], want[:, offs[i]:offs[i] + sizes[i]])
+    assert (lat > 0).all() and span >= arrival[-1] - arrival[0]
+    assert st["completed"] == n_req
+
+
+def test_small_ring_wraps(model):
+    # a 300-row input ring (100-row batches): requests of random sizes wrap
+    # around it many times while earlier batches are still in flight
+    F = model.n_features
+    per_row = (F + model.n_groups) * 4
+    rng = np.random.default_rng(13)
+    pool = request_rows(rng, 20_000, F)
+    want = plain_predict(model, pool)
+    srv = bst.PredictionServer(model, mem_budget_bytes=3 * per_row * 100)
+    try:
+        spans, ts = [], []
+        for _ in range(300):
+            k = int(rng.integers(1, 101))
+            a = int(rng.integers(0, 20_000 - k))
+            ts.append(srv.submit(pool[a:a + k]))
+            spans.append((a, k))
+        outs = [srv.wait(t) for t in ts]
+    finally:
+        srv.close()
+    for (a, k), o in zip(spans, outs):
+        np.testing.assert_array_equal(o, want[:, a:a + k])
