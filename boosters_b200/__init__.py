@@ -557,21 +557,37 @@ class PredictionServer:
                                           ctypes.byref(h)))
         self._h = h
 
+    @staticmethod
+    def _buffer(a, shape, what):
+        """(pointer, keep-alive) of a C-contiguous float32 array: numpy (host)
+        or a CUDA tensor (device; the server copies by unified addressing)."""
+        if hasattr(a, "data_ptr") and getattr(a, "is_cuda", False):
+            import torch
+            if a.dtype != torch.float32 or not a.is_contiguous() or tuple(a.shape) != tuple(shape):
+                raise ValueError(f"{what} must be a contiguous float32 tensor of shape {tuple(shape)}")
+            return a.data_ptr(), a
+        if not isinstance(a, np.ndarray) or a.dtype != np.float32 or not a.flags.c_contiguous \
+                or a.shape != tuple(shape):
+            raise ValueError(f"{what} must be a C-contiguous float32 array of shape {tuple(shape)}")
+        return a.ctypes.data, a
+
     def submit(self, rows, out=None):
-        """Queue sample-major rows ``(n, n_features)`` float32 (C order)."""
-        rows = np.asarray(rows)
-        if rows.dtype != np.float32 or not rows.flags.c_contiguous:
-            rows = np.ascontiguousarray(rows, dtype=np.float32)
-        if rows.ndim != 2 or rows.shape[1] != self.n_features:
+        """Queue sample-major rows ``(n, n_features)`` float32 (C order): a
+        numpy array (pinned memory copies asynchronously) or a CUDA tensor on
+        the model's GPU. ``out``: ``(n_groups, n)`` float32, numpy or CUDA."""
+        if not (hasattr(rows, "data_ptr") and getattr(rows, "is_cuda", False)):
+            rows = np.asarray(rows)
+            if rows.dtype != np.float32 or not rows.flags.c_contiguous:
+                rows = np.ascontiguousarray(rows, dtype=np.float32)
+        if len(rows.shape) != 2 or rows.shape[1] != self.n_features:
             raise ValueError(f"rows must have shape (n, {self.n_features})")
         n = rows.shape[0]
+        rp, rows = self._buffer(rows, (n, self.n_features), "rows")
         if out is None:
             out = np.empty((self.n_groups, n), dtype=np.float32)
-        elif out.dtype != np.float32 or out.shape != (self.n_groups, n) or not out.flags.c_contiguous:
-            raise ValueError(f"out must be a C-contiguous float32 array of shape ({self.n_groups}, {n})")
+        op, out = self._buffer(out, (self.n_groups, n), "out")
         t = ctypes.c_uint64()
-        _n.check(_n.lib.bst_server_submit(self._h, ctypes.c_void_p(rows.ctypes.data), n,
-                                          ctypes.c_void_p(out.ctypes.data), ctypes.byref(t)))
+        _n.check(_n.lib.bst_server_submit(self._h, ctypes.c_void_p(rp), n, ctypes.c_void_p(op), ctypes.byref(t)))
         return Ticket(t.value, rows, out)
 
     def wait(self, ticket, timeout_ms=-1):
@@ -583,15 +599,17 @@ class PredictionServer:
 
     def replay(self, pool, arrival_s, row_off, n_rows, ring=256):
         """Replays a request schedule from a native thread: request ``i`` is
-        rows ``pool[row_off[i]:row_off[i] + n_rows[i]]`` arriving ``arrival_s[i]``
+        rows ``pool[row_off[i]:row_off[i] + n_rows[i]]`` (pool: numpy, or a
+        CUDA tensor for device-resident requests) arriving ``arrival_s[i]``
         seconds after the start. Returns ``(latency_s, span_s, out)``: each
         request's completion minus its scheduled arrival, the span from the
         first arrival to the last completion, and the output ring
         ``(ring, n_groups, max_rows)`` (request ``i`` in slot ``i % ring``)."""
-        pool = np.asarray(pool)
-        if pool.dtype != np.float32 or not pool.flags.c_contiguous or pool.ndim != 2 \
-                or pool.shape[1] != self.n_features:
-            raise ValueError(f"pool must be a C-contiguous float32 array (rows, {self.n_features})")
+        if not (hasattr(pool, "data_ptr") and getattr(pool, "is_cuda", False)):
+            pool = np.asarray(pool)
+        if len(pool.shape) != 2 or pool.shape[1] != self.n_features:
+            raise ValueError(f"pool must have shape (rows, {self.n_features})")
+        pp, pool = self._buffer(pool, tuple(pool.shape), "pool")
         arr = np.ascontiguousarray(np.round(np.asarray(arrival_s, np.float64) * 1e9), dtype=np.uint64)
         off = np.ascontiguousarray(row_off, dtype=np.uint64)
         cnt = np.ascontiguousarray(n_rows, dtype=np.uint64)
@@ -606,7 +624,7 @@ class PredictionServer:
             out = np.empty((ring, self.n_groups, width), dtype=np.float32)
         lat = np.zeros(n_req, np.uint64)
         span = ctypes.c_uint64()
-        _n.check(_n.lib.bst_server_replay(self._h, ctypes.c_void_p(pool.ctypes.data), pool.shape[0], n_req,
+        _n.check(_n.lib.bst_server_replay(self._h, ctypes.c_void_p(pp), pool.shape[0], n_req,
                                           ctypes.c_void_p(arr.ctypes.data), ctypes.c_void_p(off.ctypes.data),
                                           ctypes.c_void_p(cnt.ctypes.data), ctypes.c_void_p(out.ctypes.data),
                                           ring, self.n_groups * width, ctypes.c_void_p(lat.ctypes.data),

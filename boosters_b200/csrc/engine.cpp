@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <map>
 
 namespace bst {
 
@@ -1686,8 +1687,13 @@ void Model::build_heap_forest(DeviceForest& f) const {
                 (t.default_left[i] ? fnum1 : fnum0)[ft] = 1;
             }
         }
-    std::vector<float> thr_flat;
+    // per feature: thresholds in NaN-padded blocks of blk = 2^lb entries
+    // (the smallest power of two with n <= HEAP_SPLITTERS blk) and the
+    // splitters (first threshold of blocks 1 ..)
+    const float qnan = std::numeric_limits<float>::quiet_NaN();
+    std::vector<float> thr_flat, spl((size_t)NF * HEAP_SPLITTERS, qnan);
     std::vector<uint32_t> thr_off(NF + 1, 0);
+    std::vector<uint8_t> finfo(NF, 0);
     size_t max_thr = 0;
     bool any_cat = false;
     for (uint32_t ft = 0; ft < NF; ++ft) {
@@ -1698,8 +1704,15 @@ void Model::build_heap_forest(DeviceForest& f) const {
         v.erase(std::unique(v.begin(), v.end(), [](float a, float b) { return a == b; }), v.end());
         if (v.size() > 65534u) return;
         max_thr = std::max(max_thr, v.size());
-        thr_off[ft] = (uint32_t)thr_flat.size();
+        uint32_t lb = 4;  // blocks of at least one 16-entry window
+        while (((size_t)HEAP_SPLITTERS << lb) < v.size()) ++lb;
+        const size_t blk = (size_t)1 << lb;
+        const size_t ns = std::max<size_t>(1, (v.size() + blk - 1) / blk);
+        thr_off[ft] = (uint32_t)thr_flat.size();  // a multiple of 16 floats: aligned windows
         thr_flat.insert(thr_flat.end(), v.begin(), v.end());
+        thr_flat.resize(thr_off[ft] + ns * blk, qnan);
+        for (size_t j = 0; j + 1 < ns; ++j) spl[(size_t)ft * HEAP_SPLITTERS + j] = v[(j + 1) * blk];
+        finfo[ft] = (uint8_t)(lb | (fcat[ft] ? 0x80u : 0u));
     }
     thr_off[NF] = (uint32_t)thr_flat.size();
     // bin columns: NaN-as-largest (numeric, default right) or categorical,
@@ -1777,16 +1790,18 @@ void Model::build_heap_forest(DeviceForest& f) const {
     up(f.heap_words, words);
     up(f.heap_thr, thr_flat);
     up(f.heap_thr_off, thr_off);
+    up(f.heap_spl, spl);
     up(f.heap_fcol, fcol);
-    up(f.heap_fcat, fcat);
+    up(f.heap_finfo, finfo);
     f.heap.nodes = f.heap_nodes.p;
     f.heap.group_off = f.heap_goff.p;
     f.heap.cat = f.heap_cat.p;
     f.heap.cat_words = f.heap_words.p;
     f.heap.thr = f.heap_thr.p;
     f.heap.thr_off = f.heap_thr_off.p;
+    f.heap.spl = f.heap_spl.p;
     f.heap.feat_col = f.heap_fcol.p;
-    f.heap.feat_cat = f.heap_fcat.p;
+    f.heap.feat_info = f.heap_finfo.p;
     f.heap.base = f.base.p;
     f.heap.n_trees = placed;
     f.heap.n_groups = n_groups;
@@ -1798,11 +1813,56 @@ void Model::build_heap_forest(DeviceForest& f) const {
     f.heap_ok = true;
 }
 
-void forest_predict_rows(const DeviceForest& f, const float* x, uint64_t n, uint64_t F, float* out, cudaStream_t st) {
-    if (f.heap_ok && F >= f.heap_min_F && F <= 0xFFFFFFFFull && predict_heap_rows(f.heap, (uint32_t)F, n) > 0)
-        launch_predict_heap(f.heap, x, n, (uint32_t)F, out, st);
-    else
+// Stream-ordered device memory for the traversal's bin tiles when the caller
+// brings none: one pool per device, kept warm up to 1 GiB between calls.
+static cudaMemPool_t scratch_pool() {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    int dev = 0;
+    BST_CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(dev);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    BST_CK(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = 1ull << 30;
+    BST_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    pools[dev] = pool;
+    return pool;
+}
+
+bool forest_uses_heap(const DeviceForest& f, uint64_t n, uint64_t F) {
+    return f.heap_ok && F >= f.heap_min_F && F <= 0xFFFFFFFFull && predict_heap_rows(f.heap, (uint32_t)F, n) > 0;
+}
+
+size_t forest_bin_bytes_per_row(const DeviceForest& f, uint64_t F) {
+    return f.heap_ok && F <= 0xFFFFFFFFull ? predict_heap_scratch_max(f.heap, (uint32_t)F, 1) / (1 + PREDICT_TILE_MAX)
+                                           : 0;
+}
+
+size_t forest_scratch_max(const DeviceForest& f, uint64_t n_max, uint64_t F) {
+    return f.heap_ok && F <= 0xFFFFFFFFull ? predict_heap_scratch_max(f.heap, (uint32_t)F, n_max) : 0;
+}
+
+void forest_predict_rows(const DeviceForest& f, const float* x, uint64_t n, uint64_t F, float* out, cudaStream_t st,
+                         void* scratch, size_t scratch_bytes) {
+    if (!forest_uses_heap(f, n, F)) {
         launch_predict(f.view, x, n, (uint32_t)F, 0, out, st);
+        return;
+    }
+    const size_t need = predict_heap_scratch(f.heap, (uint32_t)F, n);
+    if (scratch && scratch_bytes >= need) {
+        launch_predict_heap(f.heap, x, n, (uint32_t)F, out, scratch, st);
+        return;
+    }
+    void* tmp = nullptr;
+    BST_CK(cudaMallocFromPoolAsync(&tmp, std::max<size_t>(need, 16), scratch_pool(), st));
+    launch_predict_heap(f.heap, x, n, (uint32_t)F, out, tmp, st);
+    BST_CK(cudaFreeAsync(tmp, st));
 }
 
 void predict_device(const Model& m, const float* x, uint64_t n, uint64_t F, bool raw, float* out, cudaStream_t st) {

@@ -94,13 +94,20 @@ struct DeviceForest {
     uint32_t heap_min_F = 0;  // rows need at least this many features
     DevArray<uint2> heap_cat;
     DevArray<uint32_t> heap_nodes, heap_goff, heap_words, heap_thr_off;
-    DevArray<float> heap_thr;
+    DevArray<float> heap_thr, heap_spl;
     DevArray<int32_t> heap_fcol;
-    DevArray<uint8_t> heap_fcat;
+    DevArray<uint8_t> heap_finfo;
     HeapForest heap{};
 };
-// out [n_groups][n] raw margins of sample-major rows x [n][F] (device).
-void forest_predict_rows(const DeviceForest& f, const float* x, uint64_t n, uint64_t F, float* out, cudaStream_t st);
+// out [n_groups][n] raw margins of sample-major rows x [n][F] (device). The
+// shared-memory traversal bins the rows into scratch first: the caller's
+// (scratch_bytes >= what n rows need) or stream-ordered pool memory.
+void forest_predict_rows(const DeviceForest& f, const float* x, uint64_t n, uint64_t F, float* out, cudaStream_t st,
+                         void* scratch = nullptr, size_t scratch_bytes = 0);
+bool forest_uses_heap(const DeviceForest& f, uint64_t n, uint64_t F);
+// Scratch bytes enough for any batch of up to n_max rows; bin bytes per row.
+size_t forest_scratch_max(const DeviceForest& f, uint64_t n_max, uint64_t F);
+size_t forest_bin_bytes_per_row(const DeviceForest& f, uint64_t F);
 
 struct Counters {
     uint64_t launches = 0;

@@ -2338,34 +2338,38 @@ void launch_predict(const ForestDev& f, const float* x, uint64_t n, uint32_t n_f
 }
 
 // ---- shared-memory traversal (heap-ordered trees of depth <= HEAP_DEPTH) ------
-// One block bins a tile of R rows into shared-memory bin columns (against the
-// forest's thresholds) and streams the trees of each output group through a
-// double-buffered shared-memory ring of PREDICT_CHUNK trees (cp.async); each
-// thread walks its row through PREDICT_IL trees at a time as independent
-// chains of exactly HEAP_DEPTH steps and sums the leaves in forest order (the
-// same f32 additions as k_predict). The forest is read once per row tile from
-// L2 instead of once per row.
+// Two launches. k_bin_rows bins the rows against the forest's thresholds into
+// tiles of R rows in global scratch, each tile's bin columns laid out as the
+// traversal reads them from shared memory. k_predict_heap copies a tile's
+// columns into shared memory (cp.async) and streams the trees of each output
+// group through a double-buffered shared-memory ring of PREDICT_CHUNK trees;
+// each thread walks its row through PREDICT_IL trees at a time as
+// independent chains of exactly HEAP_DEPTH steps and sums the leaves in
+// forest order (the same f32 additions as k_predict). The forest is read
+// once per row tile from L2 instead of once per row.
 //
 // Bin columns are R entries long. Row r of a u8 column sits at byte
 // (r / 128) * 128 + 4 * (r % 32) + (r / 32) % 4, of a u16 column at byte
 // (r / 64) * 128 + 4 * (r % 32) + 2 * ((r / 32) % 2): with R a multiple of
 // 128, lane l of any warp reads bank l whatever column each lane asks for,
-// so the bin fetch of a step is one conflict-free wavefront.
+// so the bin fetch of a step is one conflict-free wavefront; and one 32-bit
+// word holds rows r, r + 32 (, r + 64, r + 96) of a column, so the binning
+// pass writes whole 128-byte lines.
 constexpr uint32_t PREDICT_CHUNK = 16;
 constexpr uint32_t PREDICT_IL = 4;
 constexpr uint32_t PREDICT_SMEM = 227u * 1024u;
 constexpr uint32_t PREDICT_TREE_BYTES = HEAP_NODES * 4u;
 constexpr uint32_t PREDICT_RING = 2u * PREDICT_CHUNK * PREDICT_TREE_BYTES;
-constexpr uint32_t PREDICT_MAX_ROWS = 768;
+constexpr uint32_t PREDICT_MAX_ROWS = PREDICT_TILE_MAX;
 constexpr uint32_t PREDICT_MIN_ROWS = 128;
-constexpr uint32_t PREDICT_SPL_MAX_F = 256;  // splitter table up to this many features (16 KB)
-constexpr uint32_t PREDICT_STAGE_LD = 34;    // halfwords per staged row: odd word stride
-constexpr uint32_t PREDICT_STAGE = 32u * PREDICT_STAGE_LD * 2u;
+constexpr uint32_t PREDICT_SPL_MAX_F = 256;  // splitter table in shared memory up to this many features
 constexpr uint32_t BIN_NAN = 0xFFFFu;
-static_assert(PREDICT_MAX_ROWS / 32u * PREDICT_STAGE <= PREDICT_RING, "binning stage lives in the tree ring");
+constexpr uint32_t BIN_THREADS = 256;         // binning pass: 8 warps per block
+constexpr uint32_t BIN_F = 8;                 // features staged per step of the binning pass
+constexpr uint32_t BIN_XS_LD = BIN_F + 1;     // floats per staged row: odd stride
 
-__host__ __device__ inline uint32_t predict_spl_bytes(uint32_t F) {
-    return F <= PREDICT_SPL_MAX_F ? F * HEAP_SPLITTERS * 4u : 0u;
+__host__ __device__ inline uint32_t predict_spl_floats(uint32_t NF) {
+    return NF <= PREDICT_SPL_MAX_F ? NF * HEAP_SPLITTERS : 0u;
 }
 
 // Launch shape of the traversal: R rows per tile, the trees of each chunk
@@ -2374,85 +2378,155 @@ __host__ __device__ inline uint32_t predict_spl_bytes(uint32_t F) {
 // shared memory, where the row's group-0 thread adds them in forest order).
 struct HeapPlan {
     uint32_t R = 0, S = 1;
-    size_t smem = 0;
+    size_t smem = 0, col_bytes = 0;  // col_bytes: one tile's bin columns
 };
 
 static HeapPlan heap_plan(const HeapForest& f, uint32_t F, uint64_t n) {
     HeapPlan p;
     if (F == 0 || f.n_cols == 0 || f.n_cols > HEAP_MAX_COLS) return p;
-    const uint64_t fixed = PREDICT_RING + predict_spl_bytes(F);
     const uint64_t per_row = (uint64_t)f.n_cols * (f.bins16 ? 2u : 1u);
-    if (fixed + per_row * PREDICT_MIN_ROWS > PREDICT_SMEM) return p;
-    uint64_t rmax = (PREDICT_SMEM - fixed) / per_row;
+    if (PREDICT_RING + per_row * PREDICT_MIN_ROWS > PREDICT_SMEM) return p;
+    uint64_t rmax = (PREDICT_SMEM - PREDICT_RING) / per_row;
     if (rmax > PREDICT_MAX_ROWS) rmax = PREDICT_MAX_ROWS;
     rmax &= ~(uint64_t)(PREDICT_MIN_ROWS - 1);
-    // spread a small batch over every SM: about n / 148 rows per block
-    uint64_t r = (n + 147) / 148;
+    // whole waves of 148 tiles: as few waves as the largest tile allows, the
+    // rows spread evenly over them (a small batch over every SM)
+    const uint64_t waves = n ? (n + 148 * rmax - 1) / (148 * rmax) : 1;
+    uint64_t r = (n + 148 * waves - 1) / (148 * waves);
     r = (r + PREDICT_MIN_ROWS - 1) / PREDICT_MIN_ROWS * PREDICT_MIN_ROWS;
     if (r < PREDICT_MIN_ROWS) r = PREDICT_MIN_ROWS;
     if (r > rmax) r = rmax;
     uint32_t S = r <= 128 ? 4u : (r <= 384 ? 2u : 1u);
-    if (S > 1 && fixed + r * (per_row + PREDICT_CHUNK * 4u) > PREDICT_SMEM) S = 1;
+    if (S > 1 && PREDICT_RING + r * (per_row + PREDICT_CHUNK * 4u) > PREDICT_SMEM) S = 1;
     p.R = (uint32_t)r;
     p.S = S;
-    p.smem = fixed + (S > 1 ? (size_t)PREDICT_CHUNK * 4u * r : 0) + (size_t)r * per_row;
+    p.col_bytes = (size_t)r * per_row;
+    p.smem = PREDICT_RING + (S > 1 ? (size_t)PREDICT_CHUNK * 4u * r : 0) + p.col_bytes;
     return p;
 }
 
 uint32_t predict_heap_rows(const HeapForest& f, uint32_t F, uint64_t n) { return heap_plan(f, F, n).R; }
+
+size_t predict_heap_scratch(const HeapForest& f, uint32_t F, uint64_t n) {
+    const HeapPlan p = heap_plan(f, F, n);
+    return p.R ? (size_t)((n + p.R - 1) / p.R) * p.col_bytes : 0;
+}
+
+size_t predict_heap_scratch_max(const HeapForest& f, uint32_t F, uint64_t n_max) {
+    return (size_t)(n_max + PREDICT_MAX_ROWS) * f.n_cols * (f.bins16 ? 2u : 1u);
+}
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
 }
 
-// Thresholds of one feature as the binning search sees them.
-struct BinFeat {
-    uint32_t off, n, blk, ns;  // threshold range; splitter block size and count
-    bool cat;
-};
-
-__device__ __forceinline__ BinFeat bin_feat(const HeapForest& f, uint32_t feat) {
-    BinFeat b;
-    b.off = f.thr_off[feat];
-    b.n = f.thr_off[feat + 1] - b.off;
-    b.blk = b.n > HEAP_SPLITTERS ? (b.n + HEAP_SPLITTERS - 1) / HEAP_SPLITTERS : 1u;
-    b.ns = (b.n + b.blk - 1) / b.blk;
-    b.cat = f.feat_cat[feat] != 0;
-    return b;
+// Bin of v for one numeric feature (see HeapForest) once the splitters have
+// picked block c: lb branchless steps count the block's first blk - 1
+// entries <= v, one more compare the last. NaN padding is never <= v, so no
+// search leaves the feature's blocks.
+__device__ __forceinline__ uint32_t heap_bin_block(const float* __restrict__ t, uint32_t lb, uint32_t c, float v) {
+    uint32_t k = c << lb;  // block start
+    for (uint32_t s = (1u << lb) >> 1; s >= 1u; s >>= 1) k += t[k + s - 1] <= v ? s : 0u;
+    return k + (t[k] <= v ? 1u : 0u);
 }
 
-// bin of value v (see HeapForest); NaN -> BIN_NAN. spl: the feature's
-// splitters thr[off + k * blk] (k < ns) in shared memory, or null.
-__device__ __forceinline__ uint32_t heap_bin(const HeapForest& f, const BinFeat& bf, const float* spl, float v) {
-    if (v != v) return BIN_NAN;
-    if (bf.cat) {
-        const uint32_t c = sat_u32(v);
-        return c < 65534u ? c : 65534u;
-    }
-    uint32_t lo = 0, hi = bf.n;
-    if (spl) {  // block of the first splitter > v, then search inside the block before it
-        uint32_t a = 0, b = bf.ns;
-        while (a < b) {
-            const uint32_t m = (a + b) >> 1;
-            if (spl[m] <= v)
-                a = m + 1;
-            else
-                b = m;
+// Binning pass: one warp bins 32 * RPL rows (lane l: rows l + 32 i), all
+// features, PREDICT_BIN_F at a time staged through shared memory (coalesced
+// loads), into the tile layout; the RPL rows of a lane fill one 32-bit word
+// per column.
+template <typename BinT>
+__global__ void __launch_bounds__(BIN_THREADS)
+k_bin_rows(HeapForest f, const float* __restrict__ x, uint64_t n, uint32_t F, uint32_t R, uint32_t FC,
+           uint32_t* __restrict__ bins_g) {
+    constexpr uint32_t RPL = 4u / (uint32_t)sizeof(BinT);
+    constexpr uint32_t WR = 32u * RPL;  // rows per warp
+    constexpr uint32_t BITS = 8u * (uint32_t)sizeof(BinT);
+    extern __shared__ __align__(16) float bsm[];
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarps = BIN_THREADS / 32u;
+    const uint32_t NF = F < f.n_features ? F : f.n_features;
+    const uint32_t spl_n = predict_spl_floats(NF);
+    float* spl = bsm;
+    float* xs = bsm + spl_n + (size_t)warp * WR * BIN_XS_LD;
+    for (uint32_t i = tid; i < spl_n; i += BIN_THREADS) spl[i] = f.spl[i];
+    __syncthreads();
+    const uint32_t col_words = R * (uint32_t)sizeof(BinT) / 4u;
+    const uint64_t n_groups = (n + WR - 1) / WR;
+    const uint32_t n_fc = (NF + FC - 1) / FC;  // feature chunks: more warps for a small batch
+    const uint64_t items = n_groups * n_fc;
+    for (uint64_t it = (uint64_t)blockIdx.x * nwarps + warp; it < items; it += (uint64_t)gridDim.x * nwarps) {
+        const uint64_t gi = it / n_fc;
+        const uint32_t f0 = (uint32_t)(it - gi * n_fc) * FC, f1 = f0 + FC < NF ? f0 + FC : NF;
+        const uint64_t row0 = gi * WR;
+        const uint64_t tile = row0 / R;
+        const uint32_t rg0 = (uint32_t)(row0 - tile * R);  // a multiple of WR
+        const uint32_t nr = (uint32_t)(n - row0 < WR ? n - row0 : WR);
+        uint32_t* tw = bins_g + (size_t)tile * f.n_cols * col_words + (rg0 / WR) * 32u + lane;
+        for (uint32_t fg = f0; fg < f1; fg += BIN_F) {
+            const uint32_t fj = fg + lane % BIN_F;
+#pragma unroll 8
+            for (uint32_t k = 0; k < WR * BIN_F / 32u; ++k) {
+                const uint32_t row = lane / BIN_F + k * (32u / BIN_F);
+                xs[row * BIN_XS_LD + lane % BIN_F] = row < nr && fj < f1 ? x[(row0 + row) * F + fj] : 0.0f;
+            }
+            __syncwarp();
+            const uint32_t nf = f1 - fg < BIN_F ? f1 - fg : BIN_F;
+            for (uint32_t j = 0; j < nf; ++j) {
+                const uint32_t ft = fg + j;  // the same feature in every lane
+                const int32_t c0 = f.feat_col[2 * ft], c1 = f.feat_col[2 * ft + 1];
+                if (c0 < 0 && c1 < 0) continue;
+                const uint32_t info = f.feat_info[ft];
+                const uint32_t lb = info & 31u;
+                const float* sp = spl_n ? spl + ft * HEAP_SPLITTERS : f.spl + (size_t)ft * HEAP_SPLITTERS;
+                const float* t = f.thr + f.thr_off[ft];
+                float v[RPL];
+                uint32_t b[RPL];
+#pragma unroll
+                for (uint32_t i = 0; i < RPL; ++i) {
+                    v[i] = xs[(lane + 32u * i) * BIN_XS_LD + j];
+                    b[i] = 0;
+                }
+                if (!(info >> 7)) {
+#pragma unroll
+                    for (uint32_t s = HEAP_SPLITTERS / 2; s >= 1; s >>= 1) {
+#pragma unroll
+                        for (uint32_t i = 0; i < RPL; ++i) b[i] += sp[b[i] + s - 1] <= v[i] ? s : 0u;
+                    }
+                    if (lb == 4) {  // 16-entry blocks: fixed steps, the rows interleaved
+#pragma unroll
+                        for (uint32_t i = 0; i < RPL; ++i) b[i] <<= 4;
+#pragma unroll
+                        for (uint32_t s = 8; s >= 1; s >>= 1) {
+#pragma unroll
+                            for (uint32_t i = 0; i < RPL; ++i) b[i] += t[b[i] + s - 1] <= v[i] ? s : 0u;
+                        }
+#pragma unroll
+                        for (uint32_t i = 0; i < RPL; ++i) b[i] += t[b[i]] <= v[i] ? 1u : 0u;
+                    } else {
+#pragma unroll
+                        for (uint32_t i = 0; i < RPL; ++i) b[i] = heap_bin_block(t, lb, b[i], v[i]);
+                    }
+                }
+                uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+                for (uint32_t i = 0; i < RPL; ++i) {
+                    uint32_t bb = b[i];
+                    if (v[i] != v[i]) {
+                        bb = BIN_NAN;
+                    } else if (info >> 7) {
+                        const uint32_t cv = sat_u32(v[i]);
+                        bb = cv < 65534u ? cv : 65534u;
+                    }
+                    const uint32_t mask = (1u << BITS) - 1u;  // NaN: largest bin / 0
+                    w0 |= (bb == BIN_NAN ? mask : bb & mask) << (BITS * i);
+                    w1 |= (bb == BIN_NAN ? 0u : bb & mask) << (BITS * i);
+                }
+                if (c0 >= 0) tw[(size_t)c0 * col_words] = w0;
+                if (c1 >= 0) tw[(size_t)c1 * col_words] = w1;
+            }
+            __syncwarp();
         }
-        if (a == 0) return 0;
-        lo = (a - 1) * bf.blk;
-        hi = min(a * bf.blk, bf.n);
     }
-    const float* t = f.thr + bf.off;
-    while (lo < hi) {  // first threshold > v
-        const uint32_t m = (lo + hi) >> 1;
-        if (t[m] <= v)
-            lo = m + 1;
-        else
-            hi = m;
-    }
-    return lo;
 }
 
 // One split step: from heap position h of tree to its chosen child. cb: this
@@ -2506,65 +2580,29 @@ __device__ __forceinline__ void heap_walk(const uint32_t* tb, uint32_t q0, uint3
 
 template <bool CAT, typename BinT>
 __global__ void __launch_bounds__(PREDICT_MAX_ROWS, 1)
-k_predict_heap(HeapForest f, const float* __restrict__ x, uint64_t n, uint32_t F, uint32_t R, uint32_t S,
+k_predict_heap(HeapForest f, const unsigned char* __restrict__ bins_g, uint64_t n, uint32_t R, uint32_t S,
                float* __restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* ring = reinterpret_cast<uint32_t*>(smem_raw);  // [2][PREDICT_CHUNK][HEAP_NODES]
-    const uint32_t spl_bytes = predict_spl_bytes(F);
-    float* spl = reinterpret_cast<float*>(smem_raw + PREDICT_RING);
-    float* lv = reinterpret_cast<float*>(smem_raw + PREDICT_RING + spl_bytes);  // [PREDICT_CHUNK][R] when S > 1
-    unsigned char* bins = smem_raw + PREDICT_RING + spl_bytes + (S > 1 ? PREDICT_CHUNK * 4u * R : 0u);
-    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    float* lv = reinterpret_cast<float*>(smem_raw + PREDICT_RING);  // [PREDICT_CHUNK][R] when S > 1
+    unsigned char* bins = smem_raw + PREDICT_RING + (S > 1 ? PREDICT_CHUNK * 4u * R : 0u);
+    const uint32_t tid = threadIdx.x, lane = tid & 31u;
     const uint32_t rg = tid % R, sg = tid / R;  // row in the tile, tree group
     const uint32_t Rb = R * (uint32_t)sizeof(BinT);
+    const uint32_t col_bytes = f.n_cols * Rb;
     const uint32_t roff = sizeof(BinT) == 1 ? (rg >> 7) * 128u + 4u * lane + ((rg >> 5) & 3u)
                                             : (rg >> 6) * 128u + 4u * lane + 2u * ((rg >> 5) & 1u);
     const unsigned char* cb = bins + roff;
-    uint16_t* stage = reinterpret_cast<uint16_t*>(smem_raw) + (size_t)warp * (PREDICT_STAGE / 2u);
-    const uint32_t NF = F < f.n_features ? F : f.n_features;  // features any split reads
-    if (spl_bytes) {
-        for (uint32_t i = tid; i < NF * HEAP_SPLITTERS; i += blockDim.x) {
-            const BinFeat bf = bin_feat(f, i / HEAP_SPLITTERS);
-            const uint32_t k = i % HEAP_SPLITTERS;
-            spl[i] = k < bf.ns ? f.thr[bf.off + k * bf.blk] : 0.0f;
-        }
-    }
-    __syncthreads();
     const uint64_t n_tiles = (n + R - 1) / R;
     for (uint64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const uint64_t r0 = tile * R;
         const uint32_t nr = (uint32_t)((uint64_t)R < n - r0 ? (uint64_t)R : n - r0);
-        // bin: each warp 32 rows, 32 features at a time (the tree groups take
-        // turns over the feature chunks); coalesced reads of the sample-major
-        // rows (lanes over features), transposed through the warp's stage
-        // (lanes over rows) into the bin columns
-        const uint32_t rb = rg & ~31u;
-        for (uint32_t fc = sg * 32u; fc < NF; fc += 32u * S) {
-            const uint32_t fl = fc + lane;
-            const bool has = fl < NF && (f.feat_col[2 * fl] >= 0 || f.feat_col[2 * fl + 1] >= 0);
-            BinFeat bf{};
-            if (has) bf = bin_feat(f, fl);
-            const float* fs = spl_bytes && has ? spl + fl * HEAP_SPLITTERS : nullptr;
-#pragma unroll 8
-            for (uint32_t i = 0; i < 32u; ++i) {
-                const uint32_t r = rb + i;
-                uint32_t b = 0;
-                if (has && r < nr) b = heap_bin(f, bf, fs, x[(r0 + r) * F + fl]);
-                stage[i * PREDICT_STAGE_LD + lane] = (uint16_t)b;
-            }
-            __syncwarp();
-            const uint32_t nf = NF - fc < 32u ? NF - fc : 32u;
-            for (uint32_t j = 0; j < nf; ++j) {
-                const int32_t c0 = f.feat_col[2 * (fc + j)], c1 = f.feat_col[2 * (fc + j) + 1];
-                const uint32_t b = stage[lane * PREDICT_STAGE_LD + j];
-                if (c0 >= 0)  // NaN -> the largest bin
-                    *reinterpret_cast<BinT*>(bins + (uint32_t)c0 * Rb + roff) = (BinT)(b == BIN_NAN ? (BinT)~(BinT)0 : b);
-                if (c1 >= 0)  // NaN -> 0
-                    *reinterpret_cast<BinT*>(bins + (uint32_t)c1 * Rb + roff) = (BinT)(b == BIN_NAN ? 0u : b);
-            }
-            __syncwarp();
+        {  // the tile's bin columns; the first chunk wait below covers them
+            const uint4* src = reinterpret_cast<const uint4*>(bins_g + tile * col_bytes);
+            uint4* dst = reinterpret_cast<uint4*>(bins);
+            for (uint32_t i = tid; i < col_bytes / 16u; i += blockDim.x) cp_async16(dst + i, src + i);
+            asm volatile("cp.async.commit_group;" ::: "memory");
         }
-        __syncthreads();  // bins complete; the stage (ring) is free
         for (uint32_t g = 0; g < f.n_groups; ++g) {
             const uint32_t t0 = f.group_off[g], t1 = f.group_off[g + 1];
             float acc = f.base[g];
@@ -2585,7 +2623,7 @@ k_predict_heap(HeapForest f, const float* __restrict__ x, uint64_t n, uint32_t F
                 } else {
                     asm volatile("cp.async.wait_group 0;" ::: "memory");
                 }
-                __syncthreads();  // chunk c landed; the previous chunk's leaf values are summed
+                __syncthreads();  // chunk c (and the tile's bins) landed; the previous chunk's leaf values are summed
                 const uint32_t* tb = ring + (size_t)(c & 1u) * PREDICT_CHUNK * HEAP_NODES;
                 const uint32_t nt = min(PREDICT_CHUNK, t1 - (t0 + c * PREDICT_CHUNK));
                 if (S == 1) {
@@ -2602,23 +2640,46 @@ k_predict_heap(HeapForest f, const float* __restrict__ x, uint64_t n, uint32_t F
             }
             if (sg == 0 && rg < nr) out[(uint64_t)g * n + r0 + rg] = acc;
         }
-        __syncthreads();  // bins and stage free for the next tile
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();  // bins free for the next tile
     }
 }
 
-void launch_predict_heap(const HeapForest& f, const float* x, uint64_t n, uint32_t F, float* out, cudaStream_t st) {
+void launch_predict_heap(const HeapForest& f, const float* x, uint64_t n, uint32_t F, float* out, void* scratch,
+                         cudaStream_t st) {
     if (n == 0) return;
+    init_kernel_attributes();  // per device: the kernels' shared-memory opt-in
     const HeapPlan p = heap_plan(f, F, n);
+    const uint32_t NF = F < f.n_features ? F : f.n_features;
     const uint64_t tiles = (n + p.R - 1) / p.R;
+    {
+        // warp items: row groups x feature chunks, about 32 warps per SM
+        const uint32_t wr = f.bins16 ? 64u : 128u;
+        const uint64_t groups = (n + wr - 1) / wr;
+        const uint64_t want = 148u * 32u;
+        const uint64_t fgs = (NF + BIN_F - 1) / BIN_F;
+        uint64_t n_fc = groups >= want ? 1 : (want + groups - 1) / groups;
+        if (n_fc > fgs) n_fc = fgs;
+        if (n_fc < 1) n_fc = 1;
+        const uint32_t FC = (uint32_t)((fgs + n_fc - 1) / n_fc) * BIN_F;
+        const uint64_t items = groups * ((NF + FC - 1) / FC);
+        const uint64_t blocks = (items + BIN_THREADS / 32u - 1) / (BIN_THREADS / 32u);
+        const unsigned grid = (unsigned)(blocks < 148u * 4u ? blocks : 148u * 4u);
+        const size_t smem = (predict_spl_floats(NF) + (size_t)(BIN_THREADS / 32u) * wr * BIN_XS_LD) * sizeof(float);
+        if (f.bins16)
+            k_bin_rows<uint16_t><<<grid, BIN_THREADS, smem, st>>>(f, x, n, F, p.R, FC, static_cast<uint32_t*>(scratch));
+        else
+            k_bin_rows<uint8_t><<<grid, BIN_THREADS, smem, st>>>(f, x, n, F, p.R, FC, static_cast<uint32_t*>(scratch));
+    }
     const unsigned grid = (unsigned)(tiles < 148u ? tiles : 148u);
     const unsigned threads = p.R * p.S;
-    init_kernel_attributes();  // per device: the traversal's shared-memory opt-in
+    const unsigned char* bg = static_cast<const unsigned char*>(scratch);
     if (f.has_cat)
-        k_predict_heap<true, uint16_t><<<grid, threads, p.smem, st>>>(f, x, n, F, p.R, p.S, out);
+        k_predict_heap<true, uint16_t><<<grid, threads, p.smem, st>>>(f, bg, n, p.R, p.S, out);
     else if (f.bins16)
-        k_predict_heap<false, uint16_t><<<grid, threads, p.smem, st>>>(f, x, n, F, p.R, p.S, out);
+        k_predict_heap<false, uint16_t><<<grid, threads, p.smem, st>>>(f, bg, n, p.R, p.S, out);
     else
-        k_predict_heap<false, uint8_t><<<grid, threads, p.smem, st>>>(f, x, n, F, p.R, p.S, out);
+        k_predict_heap<false, uint8_t><<<grid, threads, p.smem, st>>>(f, bg, n, p.R, p.S, out);
 }
 
 __global__ void k_transform(int t, float* __restrict__ p, uint32_t G, uint64_t n) {
@@ -2662,6 +2723,8 @@ void init_kernel_attributes() {
     if (cudaGetDevice(&dev) != cudaSuccess) return;
     const unsigned long long bit = dev < 64 ? (1ull << dev) : 0ull;
     if (bit && (done.load() & bit)) return;
+    cudaFuncSetAttribute(k_bin_rows<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_bin_rows<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_predict_heap<true, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
     cudaFuncSetAttribute(k_predict_heap<false, uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);
     cudaFuncSetAttribute(k_predict_heap<false, uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PREDICT_SMEM);

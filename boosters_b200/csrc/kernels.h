@@ -359,9 +359,13 @@ void launch_predict(const ForestDev& f, const float* x, uint64_t n, uint32_t n_f
 // leaf values reached after exactly HEAP_DEPTH steps; a leaf shallower than
 // that is reached through padding splits that always go left.
 //
-// Rows are binned against the forest's own sorted distinct thresholds
-// thr[thr_off[f] .. thr_off[f + 1]): bin(x) = #{t <= x}, so x < t_k exactly
-// when bin(x) < k + 1. A split reads one bin column of the row tile: each
+// Rows are binned against the forest's own sorted distinct thresholds of
+// each feature: bin(x) = #{t <= x}, so x < t_k exactly when bin(x) < k + 1.
+// Feature f's n thresholds sit at thr + thr_off[f] (a multiple of 16
+// floats), padded with NaN (never <= x) to whole blocks of blk =
+// 2^(feat_info[f] & 31) entries, blk the smallest power of two >= 16 with
+// n <= 16 blk; spl[16 f + j] is the first threshold of block j + 1 (NaN past
+// the last block), so that the bin search is a fixed sequence of compares. A split reads one bin column of the row tile: each
 // feature has up to two numeric columns, one per missing-value direction
 // (feat_col[2f]: NaN stored as the largest bin, which no split sends left;
 // feat_col[2f + 1]: NaN stored as 0, which every split of that column sends
@@ -382,10 +386,11 @@ struct HeapForest {
     const uint32_t* group_off;  // [n_groups + 1]
     const uint2* cat;
     const uint32_t* cat_words;
-    const float* thr;           // distinct split thresholds per feature, ascending
+    const float* thr;           // per feature: distinct split thresholds, ascending, NaN-padded blocks
     const uint32_t* thr_off;    // [n_features + 1]
+    const float* spl;           // [n_features][HEAP_SPLITTERS]
     const int32_t* feat_col;    // [2 * n_features], -1: no column
-    const uint8_t* feat_cat;    // [n_features]: used by categorical splits
+    const uint8_t* feat_info;   // [n_features]: log2(block) | categorical << 7
     const float* base;
     uint32_t n_trees, n_groups, n_features, n_cols;
     int has_cat;  // any categorical split
@@ -394,8 +399,15 @@ struct HeapForest {
 // Rows per block of the shared-memory traversal for n rows of F features (0:
 // the forest does not fit; use the node-list traversal).
 uint32_t predict_heap_rows(const HeapForest& f, uint32_t n_features, uint64_t n);
+// Bytes of bin-tile scratch the traversal of n rows needs; an upper bound for
+// any n <= n_max.
+size_t predict_heap_scratch(const HeapForest& f, uint32_t n_features, uint64_t n);
+size_t predict_heap_scratch_max(const HeapForest& f, uint32_t n_features, uint64_t n_max);
+constexpr uint32_t PREDICT_TILE_MAX = 768;  // largest traversal tile (rows)
+// out [n_groups][n] raw margins of sample-major rows x [n][n_features];
+// scratch: predict_heap_scratch bytes of device memory (16-byte aligned).
 void launch_predict_heap(const HeapForest& f, const float* x, uint64_t n, uint32_t n_features, float* out,
-                         cudaStream_t st);
+                         void* scratch, cudaStream_t st);
 // transform: 1 sigmoid, 2 softmax over [G][n]
 void launch_transform(int transform, float* out, uint32_t G, uint64_t n, cudaStream_t st);
 

@@ -2,8 +2,9 @@
 // forest (the serving pattern of the engine; the reference predicts one call
 // at a time through Predictor::predict_into, inference/gbdt/predictor.rs:197).
 //
-// Requests (sample-major f32 rows, caller-owned input and output buffers)
-// are admitted FIFO into a device row ring as soon as it has room: the
+// Requests (sample-major f32 rows, caller-owned input and output buffers in
+// host or device memory: the copies go by unified addressing) are admitted
+// FIFO into a device row ring as soon as it has room: the
 // admission issues the request's host-to-device copy at once on the copy
 // stream, so copies proceed while earlier batches traverse. A dispatcher
 // coalesces admitted requests that sit contiguously in the ring into one
@@ -57,6 +58,7 @@ struct Server {
     };
     struct Slot {
         DevArray<float> d_out;
+        DevArray<unsigned char> scratch;  // the traversal's bin tiles
         cudaStream_t st = nullptr;
         cudaEvent_t done = nullptr;
         std::vector<uint64_t> reqs;  // ticket ids, in ring order
@@ -91,7 +93,9 @@ struct Server {
         BST_CK(cudaSetDevice(device));
         F = m.n_features;
         G = m.n_groups;
-        const uint64_t per_row = (F + G) * sizeof(float);
+        const DeviceForest& df = m.device_forest();  // forest resident before the first request
+        // per row and slot: its input rows (in the ring), outputs and bin tiles
+        const uint64_t per_row = (F + G) * sizeof(float) + forest_bin_bytes_per_row(df, F);
         max_rows = budget / ((uint64_t)SLOTS * std::max<uint64_t>(1, per_row));
         if (cap) max_rows = std::min(max_rows, cap);
         if (max_rows == 0)
@@ -99,11 +103,12 @@ struct Server {
         if (max_rows > 0xFFFFFFFFull) max_rows = 0xFFFFFFFFull;
         coalesce_rows = cap ? max_rows : std::min(max_rows, COALESCE_ROWS);
         ring_rows = (uint64_t)SLOTS * max_rows;  // the slots' input share of the budget
-        (void)m.device_forest();  // forest resident before the first request
         ring.alloc((size_t)ring_rows * std::max<uint64_t>(1, F));
         BST_CK(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking));
+        const size_t scratch = forest_scratch_max(df, max_rows, F);
         for (auto& s : slots) {
             s.d_out.alloc((size_t)max_rows * G);
+            if (scratch) s.scratch.alloc(scratch);
             BST_CK(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
             BST_CK(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
         }
@@ -188,7 +193,7 @@ struct Server {
             r.copied = ev;
             r.pos = pos;
             if (F)
-                BST_CK(cudaMemcpyAsync(ring.p + pos * F, r.rows, sizeof(float) * r.n * F, cudaMemcpyHostToDevice, cst));
+                BST_CK(cudaMemcpyAsync(ring.p + pos * F, r.rows, sizeof(float) * r.n * F, cudaMemcpyDefault, cst));
             BST_CK(cudaEventRecord(ev, cst));
             live.emplace_back(pos, r.n);
             admitted.push_back(r.id);
@@ -308,14 +313,15 @@ struct Server {
             Slot& s = slots[si];
             try {
                 BST_CK(cudaStreamWaitEvent(s.st, batch.back().copied, 0));  // copies are in order on cst
-                forest_predict_rows(f, ring.p + batch.front().pos * F, rows, F, s.d_out.p, s.st);
+                forest_predict_rows(f, ring.p + batch.front().pos * F, rows, F, s.d_out.p, s.st, s.scratch.p,
+                                    s.scratch.n);
                 if (!raw) launch_transform(tr, s.d_out.p, (uint32_t)G, rows, s.st);
                 BST_CK(cudaGetLastError());
                 uint64_t off = 0;
                 for (auto& r : batch) {
                     for (uint64_t g = 0; g < G; ++g)
                         BST_CK(cudaMemcpyAsync(r.out + g * r.n, s.d_out.p + g * rows + off, sizeof(float) * r.n,
-                                               cudaMemcpyDeviceToHost, s.st));
+                                               cudaMemcpyDefault, s.st));
                     off += r.n;
                 }
                 BST_CK(cudaEventRecord(s.done, s.st));

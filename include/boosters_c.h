@@ -373,10 +373,12 @@ typedef struct bst_server_stats {
 bst_status bst_server_create(const bst_model* model, uint64_t mem_budget_bytes, uint64_t max_batch_rows,
                              int32_t raw, bst_server** out);
 /* Queues n_rows sample-major rows [n_rows, n_features] f32 for prediction
- * into out [n_groups, n_rows]; both buffers are the caller's and must stay
- * valid until bst_server_wait returns for the ticket (pinned host memory
- * gives asynchronous copies). Requests larger than one batch are rejected
- * with BST_ERR_INVALID_ARGUMENT. Returns at once. */
+ * into out [n_groups, n_rows]; both buffers are the caller's, in host or
+ * device memory of the model's GPU (unified addressing tells them apart),
+ * and must stay valid until bst_server_wait returns for the ticket (host
+ * buffers should be pinned for asynchronous copies; device rows skip the
+ * PCIe transfer). Requests larger than one batch are rejected with
+ * BST_ERR_INVALID_ARGUMENT. Returns at once. */
 bst_status bst_server_submit(bst_server* server, const float* rows, uint64_t n_rows, float* out,
                              uint64_t* ticket);
 /* Waits for a ticket (timeout_ms < 0: no limit; BST_ERR_TIMEOUT leaves the

@@ -104,13 +104,15 @@ def test_softmax_groups_and_categorical_splits():
 def test_budget_admission_limits(model):
     F = model.n_features
     per_row = (F + model.n_groups) * 4
-    srv = bst.PredictionServer(model, mem_budget_bytes=3 * per_row * 100)  # 100-row batches
+    srv = bst.PredictionServer(model, mem_budget_bytes=3 * per_row * 100)  # under 100-row batches
     try:
-        assert srv.stats()["max_batch_rows"] == 100
+        cap = srv.stats()["max_batch_rows"]
+        assert 20 <= cap <= 100  # input, output and bin-tile bytes per row share the budget
         with pytest.raises(n.BoostersError, match="exceeds"):
-            srv.submit(np.zeros((101, F), np.float32))
+            srv.submit(np.zeros((cap + 1, F), np.float32))
         rng = np.random.default_rng(3)
-        rows = [request_rows(rng, 60, F) for _ in range(10)]
+        k = cap // 2 + 1
+        rows = [request_rows(rng, k, F) for _ in range(10)]
         ts = [srv.submit(r) for r in rows]
         outs = [srv.wait(t) for t in ts]
         st = srv.stats()
@@ -118,7 +120,7 @@ def test_budget_admission_limits(model):
         srv.close()
     for r, o in zip(rows, outs):
         np.testing.assert_array_equal(o, plain_predict(model, r))
-    assert st["max_rows_seen"] <= 100  # two 60-row requests never share a batch
+    assert st["max_rows_seen"] <= cap  # two requests of over half a batch never share one
     with pytest.raises(n.BoostersError, match="budget"):
         bst.PredictionServer(model, mem_budget_bytes=per_row)
 
@@ -236,7 +238,7 @@ def test_replay_schedule(model):
 
 
 def test_small_ring_wraps(model):
-    # a 300-row input ring (100-row batches): requests of random sizes wrap
+    # an input ring of three small batches: requests of random sizes wrap
     # around it many times while earlier batches are still in flight
     F = model.n_features
     per_row = (F + model.n_groups) * 4
@@ -245,9 +247,10 @@ def test_small_ring_wraps(model):
     want = plain_predict(model, pool)
     srv = bst.PredictionServer(model, mem_budget_bytes=3 * per_row * 100)
     try:
+        cap = srv.stats()["max_batch_rows"]
         spans, ts = [], []
         for _ in range(300):
-            k = int(rng.integers(1, 101))
+            k = int(rng.integers(1, cap + 1))
             a = int(rng.integers(0, 20_000 - k))
             ts.append(srv.submit(pool[a:a + k]))
             spans.append((a, k))
@@ -256,3 +259,31 @@ def test_small_ring_wraps(model):
         srv.close()
     for (a, k), o in zip(spans, outs):
         np.testing.assert_array_equal(o, want[:, a:a + k])
+
+
+def test_device_resident_requests(model):
+    # rows already in device memory: same results, no host copy of the rows
+    import torch
+    rng = np.random.default_rng(14)
+    F = model.n_features
+    host = request_rows(rng, 30_000, F)
+    dev = torch.from_numpy(host).cuda()
+    want = plain_predict(model, host, raw=True)
+    srv = bst.PredictionServer(model, raw=True)
+    try:
+        spans = [(0, 1), (5, 700), (1000, 25_000), (29_000, 1000)]
+        ts = [srv.submit(dev[a:a + k]) for a, k in spans]
+        outs = [srv.wait(t).copy() for t in ts]
+        dout = torch.empty((model.n_groups, 500), dtype=torch.float32, device="cuda")
+        srv.wait(srv.submit(dev[100:600], out=dout))
+        n_req = 200
+        sizes = rng.integers(1, 3000, n_req)
+        offs = rng.integers(0, 27_000, n_req)
+        lat, span, ring = srv.replay(dev, np.cumsum(rng.exponential(1 / 20_000, n_req)), offs, sizes, ring=n_req)
+    finally:
+        srv.close()
+    for (a, k), o in zip(spans, outs):
+        np.testing.assert_array_equal(o, want[:, a:a + k])
+    np.testing.assert_array_equal(dout.cpu().numpy(), want[:, 100:600])
+    for i in range(n_req):
+        np.testing.assert_array_equal(ring[i, :, :sizes[i]], want[:, offs[i]:offs[i] + sizes[i]])
