@@ -372,7 +372,7 @@ def run_ours(args, world, rank, local):
             "forms": forms,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_b_hist" if head != "plain" else "k_hist_build", "launches": hist_launches,
+                         "kernel": "k_b_hist_part" if head != "plain" else "k_hist_build", "launches": hist_launches,
                          "avg_launch_ms": round(hist_ms / hist_launches, 5),
                          "algorithmic_bytes_per_launch": round(hist_bytes / hist_launches)},
             "cpu_baseline": cpu,
@@ -389,6 +389,40 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_profile(args):
+    """A small fixed workload for profilers (no JSON line): `train` grows
+    --rounds trees of the 1M x 100 logistic workload in --form; `predict`
+    trains --trees trees (batched_q8) and predicts --rows rows three times."""
+    import ctypes
+    import torch
+    import boosters_b200 as bst
+    from boosters_b200 import _native as n
+    x, y = bst.synth.binary(N_ROWS, N_FEAT, N_NAN, seed=SEED)
+    if args.profile == "train":
+        cfg = bst.GBDTConfig(**dict(cfg_kwargs(), **dict(FORMS)[args.form]))
+        booster = bst.Booster(bst.Dataset.from_feature_major(x, y), cfg, n_threads=0)
+        for r in range(args.rounds):  # per round: the histogram launches' algorithmic bytes
+            c0 = booster.stats()[1]
+            booster.update(1)
+            c1 = booster.stats()[1]
+            print(f"round {r}: hist_launches {c1['hist_launches'] - c0['hist_launches']} "
+                  f"hist_bytes {c1['hist_bytes'] - c0['hist_bytes']}")
+        torch.cuda.synchronize()
+        print(f"profile train: {booster.n_rounds} rounds ({args.form})")
+        return
+    cfg = bst.GBDTConfig(**dict(cfg_kwargs(), n_estimators=args.trees, precision="q8", batched=True))
+    model = bst.GBDTModel.train(bst.Dataset.from_feature_major(x, y), cfg)
+    xv, _ = bst.synth.binary(args.rows, N_FEAT, N_NAN, seed=SEED, stream=9)
+    xs = torch.from_numpy(np.ascontiguousarray(xv.T)).cuda()
+    out = torch.empty((1, args.rows), dtype=torch.float32, device="cuda")
+    st = torch.cuda.current_stream()
+    for _ in range(3):
+        n.check(n.lib.bst_gbdt_predict_device(model._h, ctypes.c_void_p(xs.data_ptr()), args.rows, N_FEAT, 1,
+                                              ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(st.cuda_stream)))
+    torch.cuda.synchronize()
+    print(f"profile predict: {args.trees} trees x {args.rows} rows, 3 launches")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -397,7 +431,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--profile", choices=["train", "predict"], help="run a small workload for a profiler and exit")
+    ap.add_argument("--form", default="batched_q8", choices=[k for k, _ in FORMS])
+    ap.add_argument("--rounds", type=int, default=4)
+    ap.add_argument("--trees", type=int, default=1000)
+    ap.add_argument("--rows", type=int, default=300_000)
     args = ap.parse_args()
+    if args.profile:
+        run_profile(args)
+        return
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_init()
     try:
