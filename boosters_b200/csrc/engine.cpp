@@ -436,6 +436,13 @@ class Trainer {
     DevArray<double> scales_;
     std::vector<double> h_scales_;
     DevArray<uint32_t> ridx_, tmp_, row_leaf_;
+    // the rows' gradient elements in the order of ridx_ / tmp_ (batched form):
+    // the partition moves them with the row ids, the histogram reads them in place
+    DevArray<uint8_t> qpos_[2];
+    // column-major copy of the bins (batched form): the partition's split column
+    DevArray<uint8_t> fm8_;
+    DevArray<uint16_t> fm16_;
+    BinsFM fm_{};
     DevArray<HBin> hist_;
     uint64_t slot_bins_ = 0;
     DevArray<HistTile> tiles_;
@@ -554,7 +561,15 @@ class Trainer {
         stage_.reserve(max_chunks * 48 + (size_t)(max_pnodes_ + 4) * 256 + (1 << 20));
         if (n_cols_) setup_hist_state();
         use_batched_ = cfg_.batched && !leafwise_ && n_cols_ > 0 && cfg_.max_depth <= 14;
-        if (use_batched_) setup_batched();
+        if (use_batched_) {
+            setup_batched();
+            for (auto& q : qpos_) q.alloc((size_t)n_ * grad_bytes());
+            if (p_.s8) fm8_.alloc((size_t)n_ * p_.s8);
+            if (p_.s16) fm16_.alloc((size_t)n_ * p_.s16);
+            launch_transpose_bins(b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, n_, fm8_.p, fm16_.p, st_);
+            BST_CK(cudaGetLastError());
+            fm_ = BinsFM{fm8_.p, fm16_.p, n_};
+        }
     }
 
     // ---- device-side level loop, one CUDA graph per output (kernels.h) -------
@@ -756,19 +771,25 @@ class Trainer {
             const int a = (int)(d & 1u);
             const bool need_split = d + 1 < cfg_.max_depth;
             uint32_t* rout = R[(d + 1) & 1u];
+            // gradient elements move with the row ids: level 0 reads them in
+            // row order (the unpermuted arrays), later levels ping-pong
+            const void* qin = d == 0 ? (qmode_ == GRAD_F32 ? (const void*)gh.gh : gh.gq) : (const void*)qpos_[d & 1u].p;
+            void* qout = need_split ? (void*)qpos_[(d + 1) & 1u].p : nullptr;
             tm.begin(PH_PART);
             launch_b_partition(bd_, R[d & 1u], rout, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, a, need_split ? 1 : 0,
-                               g_wide, st_);  // + children
+                               g_wide, qin, qout, qmode_, fm_, st_);  // + children
             tm.end();
             launches += 1;
             if (need_split) {
+                GradRef gl = gh;
+                gl.qpos = qpos_[(d + 1) & 1u].p;
                 if (n_tiles_) {  // general tiles add atomically into the zeroed right slots
                     tm.begin(PH_OTHER);
                     launch_b_zero_right(bd_, hist_.p, slot_bins_, g_wide, st_);
                     tm.end();
                     launches += 1;
                 }
-                enqueue_hist(gh, rout, false, tm, launches, hist_launches);
+                enqueue_hist(gl, rout, false, tm, launches, hist_launches);
                 tm.begin(PH_SCAN);
                 launch_b_scan(bd_, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p,
                               d_node_tot_.p, g_wide, st_);

@@ -10,6 +10,8 @@
 #include <atomic>
 
 
+#include <type_traits>
+
 #include "kernels.h"
 
 namespace bst {
@@ -149,18 +151,30 @@ void launch_bin_assign(const float* x_fm, uint64_t n, const BinColumn* cols, uin
 // K3: gradients (training/objectives/regression.rs:20, classification.rs:24,141)
 // ============================================================================
 
-__device__ __forceinline__ void warp_max_atomic(unsigned* dst, float v) {
-    unsigned b = __float_as_uint(fabsf(v));
-    if (!(fabsf(v) <= 3.4e38f)) b = 0;  // ignore NaN / inf for the scale
-    for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(FULL, b, o));
-    if ((threadIdx.x & 31) == 0 && b) atomicMax(dst, b);
+// |v| as an order-preserving bit pattern for the scale maxima; NaN and
+// infinities do not set the scale.
+__device__ __forceinline__ unsigned abs_bits(float v) {
+    const float a = fabsf(v);
+    return a <= 3.4e38f ? __float_as_uint(a) : 0u;
 }
 
+__device__ __forceinline__ unsigned warp_max_u32(unsigned b) {
+    for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(FULL, b, o));
+    return b;
+}
+
+// Per-output max |grad| and |hess| go to a per-block shared array (one
+// shared atomic per warp), then one global atomic per block and value: a
+// global atomic per warp on the same two words serialises in L2.
 __global__ void k_gradients(int objective, uint32_t G, const float* __restrict__ pred,
                             const float* __restrict__ y, const float* __restrict__ w, uint64_t n,
                             float2* __restrict__ gh, unsigned* __restrict__ maxabs) {
+    extern __shared__ unsigned smax[];  // [2G]
     const float HESS_MIN = 1e-6f;
+    for (uint32_t i = threadIdx.x; i < 2 * G; i += blockDim.x) smax[i] = 0u;
+    __syncthreads();
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    unsigned m0 = 0u, m1 = 0u;  // squared / logistic: this thread's maxima
     // loop trip count is warp-uniform so that the shuffles below are safe
     const uint64_t n_round = (n + 31) & ~uint64_t(31);
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += stride) {
@@ -170,17 +184,21 @@ __global__ void k_gradients(int objective, uint32_t G, const float* __restrict__
         if (objective == 0) {  // squared
             const float p = ok ? pred[i] : 0.0f;
             const float g = wi * (p - yi);
-            if (ok) gh[i] = make_float2(g, wi);
-            warp_max_atomic(&maxabs[0], ok ? g : 0.0f);
-            warp_max_atomic(&maxabs[1], ok ? wi : 0.0f);
+            if (ok) {
+                gh[i] = make_float2(g, wi);
+                m0 = max(m0, abs_bits(g));
+                m1 = max(m1, abs_bits(wi));
+            }
         } else if (objective == 1) {  // logistic
             const float x = ok ? pred[i] : 0.0f;
             const float p = 1.0f / (1.0f + exp_f32(-x));
             const float g = wi * (p - yi);
             const float h = fmaxf(wi * p * (1.0f - p), HESS_MIN);
-            if (ok) gh[i] = make_float2(g, h);
-            warp_max_atomic(&maxabs[0], ok ? g : 0.0f);
-            warp_max_atomic(&maxabs[1], ok ? h : 0.0f);
+            if (ok) {
+                gh[i] = make_float2(g, h);
+                m0 = max(m0, abs_bits(g));
+                m1 = max(m1, abs_bits(h));
+            }
         } else {  // softmax
             uint64_t label = 0;
             if (ok && yi > 0.0f) label = (uint64_t)yi;  // `f32 as usize`
@@ -195,21 +213,46 @@ __global__ void k_gradients(int objective, uint32_t G, const float* __restrict__
                 const float g = wi * (p - ind);
                 const float h = fmaxf(wi * p * (1.0f - p), HESS_MIN);
                 if (ok) gh[(uint64_t)c * n + i] = make_float2(g, h);
-                warp_max_atomic(&maxabs[2 * c], ok ? g : 0.0f);
-                warp_max_atomic(&maxabs[2 * c + 1], ok ? h : 0.0f);
+                const unsigned bg = warp_max_u32(ok ? abs_bits(g) : 0u), bh = warp_max_u32(ok ? abs_bits(h) : 0u);
+                if ((threadIdx.x & 31) == 0) {
+                    if (bg) atomicMax(&smax[2 * c], bg);
+                    if (bh) atomicMax(&smax[2 * c + 1], bh);
+                }
             }
         }
     }
+    if (objective != 2) {
+        m0 = warp_max_u32(m0);
+        m1 = warp_max_u32(m1);
+        if ((threadIdx.x & 31) == 0) {
+            if (m0) atomicMax(&smax[0], m0);
+            if (m1) atomicMax(&smax[1], m1);
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < 2 * G; i += blockDim.x)
+        if (smax[i]) atomicMax(&maxabs[i], smax[i]);
 }
 
 __global__ void k_maxabs(const float2* __restrict__ gh, uint64_t n, unsigned* __restrict__ maxabs) {
+    __shared__ unsigned smax[2];
+    if (threadIdx.x < 2) smax[threadIdx.x] = 0u;
+    __syncthreads();
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t n_round = (n + 31) & ~uint64_t(31);  // warp-uniform trip count
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += stride) {
-        const float2 v = i < n ? gh[i] : make_float2(0.0f, 0.0f);
-        warp_max_atomic(&maxabs[0], v.x);
-        warp_max_atomic(&maxabs[1], v.y);
+    unsigned m0 = 0u, m1 = 0u;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float2 v = gh[i];
+        m0 = max(m0, abs_bits(v.x));
+        m1 = max(m1, abs_bits(v.y));
     }
+    m0 = warp_max_u32(m0);
+    m1 = warp_max_u32(m1);
+    if ((threadIdx.x & 31) == 0) {
+        if (m0) atomicMax(&smax[0], m0);
+        if (m1) atomicMax(&smax[1], m1);
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 && smax[threadIdx.x]) atomicMax(&maxabs[threadIdx.x], smax[threadIdx.x]);
 }
 
 void launch_maxabs(const float2* gh, uint64_t n, unsigned* maxabs, cudaStream_t st) {
@@ -224,8 +267,8 @@ void launch_gradients(int objective, uint32_t G, const float* pred, const float*
                       cudaStream_t st) {
     if (n == 0) return;
     uint64_t blocks = (n + 255) / 256;
-    if (blocks > 148ull * 16) blocks = 148ull * 16;
-    k_gradients<<<(unsigned)blocks, 256, 0, st>>>(objective, G, pred, y, w, n, gh, maxabs);
+    if (blocks > 148ull * 8) blocks = 148ull * 8;
+    k_gradients<<<(unsigned)blocks, 256, 2 * G * sizeof(unsigned), st>>>(objective, G, pred, y, w, n, gh, maxabs);
 }
 
 __global__ void k_fixed_scales(const unsigned* __restrict__ maxabs, uint32_t G, uint64_t n,
@@ -278,23 +321,37 @@ __host__ __device__ constexpr uint32_t acc_words(int mode) { return mode == GRAD
 
 template <int MODE>
 struct GradLoad;
+// operator()(row): the row's element by row id; at(pos, row): by its
+// position in the row-id buffer when the positional copy exists.
 template <>
 struct GradLoad<GRAD_F32> {
     const float2* __restrict__ gh;
+    const float2* __restrict__ qp;
     double sg, sh;
-    __device__ explicit GradLoad(const GradRef& r) : gh(r.gh), sg(r.scale[0]), sh(r.scale[1]) {}
-    __device__ __forceinline__ void operator()(uint32_t row, long long& g, long long& h) const {
-        const float2 v = gh[row];
+    __device__ explicit GradLoad(const GradRef& r)
+        : gh(r.gh), qp(static_cast<const float2*>(r.qpos)), sg(r.scale[0]), sh(r.scale[1]) {}
+    __device__ __forceinline__ void conv(float2 v, long long& g, long long& h) const {
         g = quantize(v.x, sg);
         h = quantize(v.y, sh);
+    }
+    __device__ __forceinline__ void operator()(uint32_t row, long long& g, long long& h) const { conv(gh[row], g, h); }
+    __device__ __forceinline__ void at(uint32_t pos, uint32_t row, long long& g, long long& h) const {
+        conv(qp ? qp[pos] : gh[row], g, h);
     }
 };
 template <>
 struct GradLoad<GRAD_Q16> {
     const short2* __restrict__ q;
-    __device__ explicit GradLoad(const GradRef& r) : q(static_cast<const short2*>(r.gq)) {}
+    const short2* __restrict__ qp;
+    __device__ explicit GradLoad(const GradRef& r)
+        : q(static_cast<const short2*>(r.gq)), qp(static_cast<const short2*>(r.qpos)) {}
     __device__ __forceinline__ void operator()(uint32_t row, long long& g, long long& h) const {
         const short2 v = q[row];
+        g = v.x;
+        h = v.y;
+    }
+    __device__ __forceinline__ void at(uint32_t pos, uint32_t row, long long& g, long long& h) const {
+        const short2 v = qp ? qp[pos] : q[row];
         g = v.x;
         h = v.y;
     }
@@ -302,9 +359,16 @@ struct GradLoad<GRAD_Q16> {
 template <>
 struct GradLoad<GRAD_Q8> {
     const char2* __restrict__ q;
-    __device__ explicit GradLoad(const GradRef& r) : q(static_cast<const char2*>(r.gq)) {}
+    const char2* __restrict__ qp;
+    __device__ explicit GradLoad(const GradRef& r)
+        : q(static_cast<const char2*>(r.gq)), qp(static_cast<const char2*>(r.qpos)) {}
     __device__ __forceinline__ void operator()(uint32_t row, long long& g, long long& h) const {
         const char2 v = q[row];
+        g = v.x;
+        h = v.y;
+    }
+    __device__ __forceinline__ void at(uint32_t pos, uint32_t row, long long& g, long long& h) const {
+        const char2 v = qp ? qp[pos] : q[row];
         g = v.x;
         h = v.y;
     }
@@ -540,7 +604,7 @@ __device__ void lane_accumulate(uint32_t first, uint32_t count, bool ident, cons
             const uint32_t row = row_at(i);
             issue(row, k);
             long long qg, qh;
-            load(row, qg, qh);
+            load.at(first + i, row, qg, qh);
             ring[k] = LaneAdd<MODE>(qg, qh);
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
@@ -559,7 +623,7 @@ __device__ void lane_accumulate(uint32_t first, uint32_t count, bool ident, cons
             if (i < count) {
                 issue(row_next, s_new);
                 long long qg, qh;
-                load(row_next, qg, qh);
+                load.at(first + i, row_next, qg, qh);
                 ring[LANE_STAGES - 1] = LaneAdd<MODE>(qg, qh);
             }
             asm volatile("cp.async.commit_group;" ::: "memory");
@@ -762,8 +826,9 @@ __device__ __forceinline__ void merge_store(HBin* __restrict__ hist, uint64_t sl
 // (0xFFFFFFFF: no bin) and (tile << 16 | offset in the tile's partial
 // record). Consecutive threads read consecutive partial entries and touch
 // consecutive bins of the node histograms. Each thread handles MERGE_ILP
-// entries at once so that their dependent loads overlap.
-constexpr uint32_t MERGE_ILP = 4;
+// entries at once and loads four segments' partials at a time, so that the
+// dependent loads overlap.
+constexpr uint32_t MERGE_ILP = 2;
 
 template <int MODE>
 __global__ void __launch_bounds__(256, 4)
@@ -799,7 +864,14 @@ k_b_merge(BDev d, HBin* __restrict__ hist, uint64_t slot_bins, const void* __res
             if (!ok[u]) continue;
             if (!root) par[u] = hist[(size_t)d.exp[j[u]].left_pnode * slot_bins + m[u].x];
             const E* p = P + (size_t)(m[u].y >> 16) * LANE_PART_STRIDE + (m[u].y & 0xFFFFu);
-            for (uint32_t c = c0[u]; c < c1[u]; ++c) {
+            uint32_t c = c0[u];
+            for (; c + 4 <= c1[u]; c += 4) {  // four segments' loads in flight
+                const E v0 = p[(size_t)c * rec], v1 = p[(size_t)(c + 1) * rec];
+                const E v2 = p[(size_t)(c + 2) * rec], v3 = p[(size_t)(c + 3) * rec];
+                g[u] += (long long)v0.x + (long long)v1.x + (long long)v2.x + (long long)v3.x;
+                h[u] += (long long)v0.y + (long long)v1.y + (long long)v2.y + (long long)v3.y;
+            }
+            for (; c < c1[u]; ++c) {
                 const E v = p[(size_t)c * rec];
                 g[u] += v.x;
                 h[u] += v.y;
@@ -1404,10 +1476,18 @@ __device__ __forceinline__ bool part_left(const PartWork& w, uint32_t bin) {
 // (shrinking). Ranks come from a block-wide scan of ballots, so each
 // 2048-row pass takes one atomic per side (same-address atomics from every
 // warp serialise in L2). Block-uniform; blockDim.x == PART_THREADS.
+// Q: the type of the gradient element carried with each row id (qin at the
+// source position, qout at the destination), or char for none.
+// fm8 / fm16 (or null): the same bins column-major ([column][n_rows]), so
+// that a node's split column is gathered from one contiguous column.
+template <typename Q = char>
 __device__ void part_rows(const PartWork& w, uint32_t start, uint32_t len, unsigned* cur,
                           const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp,
                           const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16,
-                          uint32_t s16) {
+                          uint32_t s16, const Q* __restrict__ qin = nullptr, Q* __restrict__ qout = nullptr,
+                          const uint8_t* __restrict__ fm8 = nullptr, const uint16_t* __restrict__ fm16 = nullptr,
+                          uint64_t n_rows = 0) {
+    constexpr bool CARRY = !std::is_same<Q, char>::value;
     __shared__ uint32_t s_l[PART_PER][PART_THREADS / 32], s_r[PART_PER][PART_THREADS / 32];
     __shared__ uint32_t s_base[2];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1415,18 +1495,27 @@ __device__ void part_rows(const PartWork& w, uint32_t start, uint32_t len, unsig
     for (uint32_t b0 = 0; b0 < len; b0 += PART_THREADS * PART_PER) {
         uint32_t rows[PART_PER], bins[PART_PER];
         unsigned lm[PART_PER], rm[PART_PER];
+        Q qv[CARRY ? PART_PER : 1];
 #pragma unroll
         for (int k = 0; k < PART_PER; ++k) {
             const uint32_t i = b0 + k * PART_THREADS + threadIdx.x;
             rows[k] = i < len ? ridx[start + i] : 0u;
+            if constexpr (CARRY) {
+                if (i < len) qv[k] = qin[start + i];
+            }
         }
 #pragma unroll
         for (int k = 0; k < PART_PER; ++k) {
             const uint32_t i = b0 + k * PART_THREADS + threadIdx.x;
             bins[k] = 0u;
-            if (i < len)
-                bins[k] = w.matrix == 0 ? (uint32_t)bins8[(size_t)rows[k] * s8 + w.pos]
-                                        : (uint32_t)bins16[(size_t)rows[k] * s16 + w.pos];
+            if (i < len) {
+                if (fm8 || fm16)
+                    bins[k] = w.matrix == 0 ? (uint32_t)fm8[(size_t)w.pos * n_rows + rows[k]]
+                                            : (uint32_t)fm16[(size_t)w.pos * n_rows + rows[k]];
+                else
+                    bins[k] = w.matrix == 0 ? (uint32_t)bins8[(size_t)rows[k] * s8 + w.pos]
+                                            : (uint32_t)bins16[(size_t)rows[k] * s16 + w.pos];
+            }
         }
 #pragma unroll
         for (int k = 0; k < PART_PER; ++k) {
@@ -1472,10 +1561,15 @@ __device__ void part_rows(const PartWork& w, uint32_t start, uint32_t len, unsig
 #pragma unroll
         for (int k = 0; k < PART_PER; ++k) {
             const unsigned bit = 1u << lane;
+            uint32_t dst = 0xFFFFFFFFu;
             if (lm[k] & bit)
-                tmp[lb + s_l[k][warp] + __popc(lm[k] & lt)] = rows[k];
+                dst = lb + s_l[k][warp] + __popc(lm[k] & lt);
             else if (rm[k] & bit)
-                tmp[rbs + s_r[k][warp] + __popc(rm[k] & lt)] = rows[k];
+                dst = rbs + s_r[k][warp] + __popc(rm[k] & lt);
+            if (dst != 0xFFFFFFFFu) {
+                tmp[dst] = rows[k];
+                if constexpr (CARRY) qout[dst] = qv[k];
+            }
         }
         __syncthreads();  // s_l / s_r / s_base are reused by the next pass
     }
@@ -1834,10 +1928,11 @@ __device__ void children_body(BDev d, int a, int need_split);
 // Partition of every expanding node (partition.rs:296-382) over 2048-row
 // chunks (one atomic per side per chunk, part_rows) from row-index buffer
 // rin into rout; the last block then derives the children (children_body).
+template <typename Q>
 __global__ void __launch_bounds__(PART_THREADS)
 k_b_partition(BDev d, const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp,
               const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16,
-              int a, int need_split) {
+              int a, int need_split, const Q* __restrict__ qin, Q* __restrict__ qout, BinsFM fm) {
     __shared__ PartWork w;
     __shared__ uint32_t s_j;
     const uint32_t total = d.state->part_chunks, n_exp = d.state->n_exp;
@@ -1851,15 +1946,58 @@ k_b_partition(BDev d, const uint32_t* __restrict__ ridx, uint32_t* __restrict__ 
         const uint32_t j = s_j;
         const uint32_t start = w.begin + (c - d.exp[j].part_off) * B_PART_CHUNK;
         const uint32_t len = min(B_PART_CHUNK, w.begin + w.count - start);
-        part_rows(w, start, len, d.cursors + 2 * j, ridx, tmp, bins8, s8, bins16, s16);
+        part_rows<Q>(w, start, len, d.cursors + 2 * j, ridx, tmp, bins8, s8, bins16, s16, qin, qout, fm.b8, fm.b16,
+                     fm.n);
     }
     if (last_block(d.state)) children_body(d, a, need_split);
 }
 
 void launch_b_partition(const BDev& d, const uint32_t* rin, uint32_t* rout, const uint8_t* bins8, uint32_t s8,
                         const uint16_t* bins16, uint32_t s16, int a, int need_split, uint32_t grid,
-                        cudaStream_t st) {
-    k_b_partition<<<grid, PART_THREADS, 0, st>>>(d, rin, rout, bins8, s8, bins16, s16, a, need_split);
+                        const void* qin, void* qout, int mode, const BinsFM& fm, cudaStream_t st) {
+    if (!qin || !qout)
+        k_b_partition<char><<<grid, PART_THREADS, 0, st>>>(d, rin, rout, bins8, s8, bins16, s16, a, need_split,
+                                                           nullptr, nullptr, fm);
+    else if (mode == GRAD_Q8)
+        k_b_partition<char2><<<grid, PART_THREADS, 0, st>>>(d, rin, rout, bins8, s8, bins16, s16, a, need_split,
+                                                            static_cast<const char2*>(qin), static_cast<char2*>(qout),
+                                                            fm);
+    else if (mode == GRAD_Q16)
+        k_b_partition<short2><<<grid, PART_THREADS, 0, st>>>(d, rin, rout, bins8, s8, bins16, s16, a, need_split,
+                                                             static_cast<const short2*>(qin),
+                                                             static_cast<short2*>(qout), fm);
+    else
+        k_b_partition<float2><<<grid, PART_THREADS, 0, st>>>(d, rin, rout, bins8, s8, bins16, s16, a, need_split,
+                                                             static_cast<const float2*>(qin),
+                                                             static_cast<float2*>(qout), fm);
+}
+
+// Column-major copy of a row-major bin matrix (s columns): 32 x 32 tiles
+// through shared memory, coalesced on both sides.
+template <typename T>
+__global__ void k_transpose_bins(const T* __restrict__ in, uint32_t s, uint64_t n, T* __restrict__ out) {
+    __shared__ T t[32][33];
+    const uint64_t r0 = (uint64_t)blockIdx.x * 32u;
+    const uint32_t c0 = blockIdx.y * 32u;
+    for (uint32_t k = threadIdx.y; k < 32u; k += blockDim.y) {
+        const uint64_t r = r0 + k;
+        const uint32_t c = c0 + threadIdx.x;
+        if (r < n && c < s) t[k][threadIdx.x] = in[r * s + c];
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.y; k < 32u; k += blockDim.y) {
+        const uint32_t c = c0 + k;
+        const uint64_t r = r0 + threadIdx.x;
+        if (r < n && c < s) out[(uint64_t)c * n + r] = t[threadIdx.x][k];
+    }
+}
+
+void launch_transpose_bins(const uint8_t* b8, uint32_t s8, const uint16_t* b16, uint32_t s16, uint64_t n,
+                           uint8_t* fm8, uint16_t* fm16, cudaStream_t st) {
+    const dim3 blk(32, 8);
+    if (s8 && n) k_transpose_bins<uint8_t><<<dim3((unsigned)((n + 31) / 32), (s8 + 31) / 32), blk, 0, st>>>(b8, s8, n, fm8);
+    if (s16 && n)
+        k_transpose_bins<uint16_t><<<dim3((unsigned)((n + 31) / 32), (s16 + 31) / 32), blk, 0, st>>>(b16, s16, n, fm16);
 }
 
 // Children of every split: ranges from the partition cursors, smaller child

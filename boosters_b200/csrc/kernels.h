@@ -65,7 +65,13 @@ struct GradRef {
     const void* gq;
     const double* scale;  // GRAD_F32: the fixed-point scales of this output
     int mode;
+    // optional: the same elements (float2 / short2 / char2 by mode) permuted
+    // into the order of the row-id buffer the histogram reads, so that the
+    // lane-tile histogram loads them at the row's position (coalesced)
+    // instead of gathering them by row id
+    const void* qpos = nullptr;
 };
+__host__ __device__ constexpr uint32_t grad_elem_bytes(int mode) { return mode == 0 ? 8u : (mode == 1 ? 4u : 2u); }
 // Stochastic rounding of every (output, row): q = floor(v * Q / max|v| + u),
 // u from Philox4x32-10 with counter (row, output, round, QUANT_STREAM) and key
 // (seed lo, seed hi); word 0 rounds grad, word 1 hess.
@@ -286,10 +292,20 @@ void launch_b_root_set(const BDev& d, const NodeSplit* root_split, LeafParams lp
                        cudaStream_t st);
 // level kernels; `a` is the index of the current frontier buffer
 void launch_b_decide(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st);
-// partition rin -> rout, then (last block) the children of every split
+// Column-major copies of the bin matrices ([column][n]), or null pointers.
+struct BinsFM {
+    const uint8_t* b8 = nullptr;
+    const uint16_t* b16 = nullptr;
+    uint64_t n = 0;
+};
+void launch_transpose_bins(const uint8_t* b8, uint32_t s8, const uint16_t* b16, uint32_t s16, uint64_t n,
+                           uint8_t* fm8, uint16_t* fm16, cudaStream_t st);
+// partition rin -> rout, then (last block) the children of every split;
+// qin / qout (grad_elem_bytes(mode) each, or null) move each row's gradient
+// element with its row id; fm: the split columns are read column-major
 void launch_b_partition(const BDev& d, const uint32_t* rin, uint32_t* rout, const uint8_t* bins8, uint32_t s8,
                         const uint16_t* bins16, uint32_t s16, int a, int need_split, uint32_t grid,
-                        cudaStream_t st);
+                        const void* qin, void* qout, int mode, const BinsFM& fm, cudaStream_t st);
 void launch_b_zero_right(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t grid, cudaStream_t st);
 void launch_b_hist(const BDev& d, const HistTile* tiles, uint32_t n_tiles, uint32_t max_smem_bins,
                    const uint32_t* ridx, const GradRef& gr, const uint8_t* bins8, uint32_t s8,
