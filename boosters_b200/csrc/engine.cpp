@@ -436,6 +436,9 @@ class Trainer {
     DevArray<double> scales_;
     std::vector<double> h_scales_;
     DevArray<uint32_t> ridx_, tmp_, row_leaf_;
+    // Q8 node histograms in HBin32 when every sum fits 32 bits (n * 127 < 2^31)
+    bool hist32_ = false;
+    size_t hbytes() const { return hist32_ ? sizeof(HBin32) : sizeof(HBin); }
     // the rows' gradient elements in the order of ridx_ / tmp_ (batched form):
     // the partition moves them with the row ids, the histogram reads them in place
     DevArray<uint8_t> qpos_[2];
@@ -525,6 +528,7 @@ class Trainer {
     void setup_common() {
         const uint64_t n = n_;
         qmode_ = external_ ? GRAD_F32 : cfg_.precision;
+        hist32_ = qmode_ == GRAD_Q8 && (uint64_t)n_ * 127ull <= 0x7FFFFFFFull;
         ridx_.alloc(n);
         tmp_.alloc(n);
         if (cfg_.record_leaves) row_leaf_.alloc(n);
@@ -729,11 +733,11 @@ class Trainer {
                                d_part_.p, st_);
         if (n_tiles_)
             launch_b_hist(bd_, tiles_.p, n_tiles_, tile_smem_, ridx, gr, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16,
-                          hist_.p, slot_bins_, g_hist, st_);
+                          hist_.p, slot_bins_, g_hist, st_, hist32_);
         tm.end();
         tm.begin(PH_OTHER);
         launch_b_merge(bd_, hist_.p, slot_bins_, p_.total_bins, d_part_.p, n_lane_tiles_, d_ent_.p, n_ent_,
-                       d_bin_map_.p, n_tiles_ > 0, root ? 1 : 0, qmode_, st_);
+                       d_bin_map_.p, n_tiles_ > 0, root ? 1 : 0, qmode_, st_, hist32_);
         tm.end();
         const uint32_t hist_kernels = (n_lane_tiles_ ? 1u : 0u) + (n_tiles_ ? 1u : 0u);
         launches += 2 * hist_kernels;  // builds and merges
@@ -752,13 +756,13 @@ class Trainer {
         tm.begin(PH_OTHER);
         launch_iota(ridx_.p, n_, st_);
         launch_b_root(bd_, n_, st_);
-        if (n_tiles_) BST_CK(cudaMemsetAsync(hist_.p, 0, sizeof(HBin) * slot_bins_, st_));
+        if (n_tiles_) BST_CK(cudaMemsetAsync(hist_.p, 0, hbytes() * slot_bins_, st_));
         launch_b_root_hist(bd_, n_, chunk_rows(n_), st_);
         tm.end();
         enqueue_hist(gh, ridx_.p, true, tm, launches, hist_launches);
         tm.begin(PH_SCAN);
         launch_split_scan(d_root_scan_.p, 1, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p,
-                          d_node_tot_.p, st_);
+                          d_node_tot_.p, st_, hist32_);
         launch_split_reduce(d_cand_.p, d_node_tot_.p, 1, n_cols_, last_wins_ ? 1 : 0, d_splits_.p, st_);
         tm.end();
         tm.begin(PH_OTHER);
@@ -785,14 +789,14 @@ class Trainer {
                 gl.qpos = qpos_[(d + 1) & 1u].p;
                 if (n_tiles_) {  // general tiles add atomically into the zeroed right slots
                     tm.begin(PH_OTHER);
-                    launch_b_zero_right(bd_, hist_.p, slot_bins_, g_wide, st_);
+                    launch_b_zero_right(bd_, hist_.p, slot_bins_, g_wide, st_, hist32_);
                     tm.end();
                     launches += 1;
                 }
                 enqueue_hist(gl, rout, false, tm, launches, hist_launches);
                 tm.begin(PH_SCAN);
                 launch_b_scan(bd_, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p,
-                              d_node_tot_.p, g_wide, st_);
+                              d_node_tot_.p, g_wide, st_, hist32_);
                 launch_b_reduce(bd_, a ^ 1, d_cand_.p, d_node_tot_.p, n_cols_, last_wins_ ? 1 : 0, 1, lp, scale,
                                 (d + 1) & 1u, g_wide, st_);  // + next level's decisions
                 tm.end();
@@ -999,7 +1003,7 @@ class Trainer {
         upload(h, nodes.size(), d_scan_nodes_);
         timer_.begin(PH_SCAN);
         launch_split_scan(d_scan_nodes_.p, (uint32_t)nodes.size(), scan_cols_.p, n_cols_, hist_.p, slot_bins_,
-                          scale_o_, gp_, d_cand_.p, d_node_tot_.p, st_);
+                          scale_o_, gp_, d_cand_.p, d_node_tot_.p, st_, hist32_);
         launch_split_reduce(d_cand_.p, d_node_tot_.p, (uint32_t)nodes.size(), n_cols_, last_wins_ ? 1 : 0,
                             d_splits_.p, st_);
         timer_.end();
@@ -1176,8 +1180,8 @@ class Trainer {
             if (n_tiles_) {  // general tiles add atomically into zeroed right slots
                 const uint32_t r_lo = *std::min_element(right_ids.begin(), right_ids.end());
                 const uint32_t r_hi = *std::max_element(right_ids.begin(), right_ids.end());
-                BST_CK(cudaMemsetAsync(hist_.p + (size_t)r_lo * slot_bins_, 0,
-                                       sizeof(HBin) * slot_bins_ * (size_t)(r_hi - r_lo + 1), st_));
+                BST_CK(cudaMemsetAsync(reinterpret_cast<char*>(hist_.p) + (size_t)r_lo * slot_bins_ * hbytes(), 0,
+                                       hbytes() * slot_bins_ * (size_t)(r_hi - r_lo + 1), st_));
             }
             std::vector<BExp> exps(k);
             for (size_t j = 0; j < k; ++j) {
@@ -1286,7 +1290,7 @@ class Trainer {
         root.depth = 0;
         root.count = (uint32_t)n_;
         if (n_cols_ > 0) {
-            if (n_tiles_) BST_CK(cudaMemsetAsync(hist_.p, 0, sizeof(HBin) * slot_bins_, st_));
+            if (n_tiles_) BST_CK(cudaMemsetAsync(hist_.p, 0, hbytes() * slot_bins_, st_));
             BExp e;
             std::memset(&e, 0, sizeof(e));
             e.rc = (uint32_t)n_;

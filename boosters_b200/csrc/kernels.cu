@@ -388,14 +388,31 @@ __device__ __forceinline__ void hist_add(uint32_t* s, uint32_t S, uint32_t idx, 
     }
 }
 
+// Node-histogram element access for both bin types.
+template <typename HB>
+__device__ __forceinline__ HB hb_make(long long g, long long h) {
+    HB r;
+    r.g = (decltype(r.g))g;
+    r.h = (decltype(r.h))h;
+    return r;
+}
+__device__ __forceinline__ void hb_atomic_add(HBin* p, long long g, long long h) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(&p->g), (unsigned long long)g);
+    atomicAdd(reinterpret_cast<unsigned long long*>(&p->h), (unsigned long long)h);
+}
+__device__ __forceinline__ void hb_atomic_add(HBin32* p, long long g, long long h) {
+    atomicAdd(&p->g, (int)g);
+    atomicAdd(&p->h, (int)h);
+}
+
 // One (row chunk, column tile) item: zero the shared histogram, accumulate,
 // flush to the global histogram of chunk.slot. Block-uniform; `tile` is in
 // shared memory; returns with the shared histogram free for reuse.
-template <int MODE>
+template <int MODE, typename HB = HBin>
 __device__ void hist_item(const HistChunk& chunk, const HistTile& tile, uint32_t* sm, uint32_t S,
                           const uint32_t* __restrict__ ridx, const GradLoad<MODE>& load,
                           const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16,
-                          uint32_t s16, HBin* __restrict__ hist, uint64_t slot_bins) {
+                          uint32_t s16, HB* __restrict__ hist, uint64_t slot_bins) {
     constexpr uint32_t NW = acc_words(MODE);
     for (uint32_t i = threadIdx.x; i < S * NW / 4; i += HIST_THREADS)  // S is a multiple of 4
         reinterpret_cast<uint4*>(sm)[i] = make_uint4(0, 0, 0, 0);
@@ -446,7 +463,7 @@ __device__ void hist_item(const HistChunk& chunk, const HistTile& tile, uint32_t
         }
     }
     __syncthreads();
-    HBin* out = hist + (size_t)chunk.slot * slot_bins;
+    HB* out = hist + (size_t)chunk.slot * slot_bins;
     for (uint32_t l = c0; l < c1; ++l) {
         const uint32_t so = tile.lane_smem[l], go = tile.lane_hist[l], nb = tile.lane_nbins[l];
         for (uint32_t b = threadIdx.x; b < nb; b += HIST_THREADS) {
@@ -463,8 +480,7 @@ __device__ void hist_item(const HistChunk& chunk, const HistTile& tile, uint32_t
                 g = (int32_t)gw;
                 h = (int32_t)hw;
             }
-            atomicAdd(reinterpret_cast<unsigned long long*>(&out[go + b].g), (unsigned long long)g);
-            atomicAdd(reinterpret_cast<unsigned long long*>(&out[go + b].h), (unsigned long long)h);
+            hb_atomic_add(&out[go + b], g, h);
         }
     }
     __syncthreads();
@@ -800,18 +816,17 @@ void launch_b_hist_part(const BDev& d, const LaneTile* tiles, uint32_t n_tiles, 
 // larger = parent - smaller. The parent histogram lives in slot left_pnode,
 // which becomes the left child's; the right child's is right_pnode. root:
 // no parent, the sum goes to right_pnode.
-__device__ __forceinline__ void merge_store(HBin* __restrict__ hist, uint64_t slot_bins, const BExp& e, uint32_t gb,
-                                            HBin sm, int root) {
+template <typename HB>
+__device__ __forceinline__ void merge_store(HB* __restrict__ hist, uint64_t slot_bins, const BExp& e, uint32_t gb,
+                                            HB sm, int root) {
     if (root) {
         hist[(size_t)e.right_pnode * slot_bins + gb] = sm;
         return;
     }
-    HBin* L = hist + (size_t)e.left_pnode * slot_bins + gb;
-    HBin* R = hist + (size_t)e.right_pnode * slot_bins + gb;
-    const HBin p = *L;
-    HBin lg;
-    lg.g = p.g - sm.g;
-    lg.h = p.h - sm.h;
+    HB* L = hist + (size_t)e.left_pnode * slot_bins + gb;
+    HB* R = hist + (size_t)e.right_pnode * slot_bins + gb;
+    const HB p = *L;
+    const HB lg = hb_make<HB>((long long)p.g - sm.g, (long long)p.h - sm.h);
     if (e.lc <= e.rc) {  // left child is the smaller (grower.rs:398-402)
         *L = sm;
         *R = lg;
@@ -830,9 +845,9 @@ __device__ __forceinline__ void merge_store(HBin* __restrict__ hist, uint64_t sl
 // dependent loads overlap.
 constexpr uint32_t MERGE_ILP = 2;
 
-template <int MODE>
+template <int MODE, typename HB>
 __global__ void __launch_bounds__(256, 4)
-k_b_merge(BDev d, HBin* __restrict__ hist, uint64_t slot_bins, const void* __restrict__ part, uint32_t n_tiles,
+k_b_merge(BDev d, HB* __restrict__ hist, uint64_t slot_bins, const void* __restrict__ part, uint32_t n_tiles,
           const uint2* __restrict__ ent, uint32_t n_ent, int root) {
     using E = typename PartEntry<MODE>::T;
     const E* P = reinterpret_cast<const E*>(part);
@@ -855,7 +870,7 @@ k_b_merge(BDev d, HBin* __restrict__ hist, uint64_t slot_bins, const void* __res
             ok[u] = ok[u] && m[u].x != 0xFFFFFFFFu;
         }
         long long g[MERGE_ILP], h[MERGE_ILP];
-        HBin par[MERGE_ILP];
+        HB par[MERGE_ILP];
 #pragma unroll
         for (uint32_t u = 0; u < MERGE_ILP; ++u) {
             g[u] = 0;
@@ -881,16 +896,12 @@ k_b_merge(BDev d, HBin* __restrict__ hist, uint64_t slot_bins, const void* __res
         for (uint32_t u = 0; u < MERGE_ILP; ++u) {
             if (!ok[u]) continue;
             const BExp& e = d.exp[j[u]];
-            HBin sm;
-            sm.g = g[u];
-            sm.h = h[u];
+            const HB sm = hb_make<HB>(g[u], h[u]);
             if (root) {
                 hist[(size_t)e.right_pnode * slot_bins + m[u].x] = sm;
                 continue;
             }
-            HBin lg;
-            lg.g = par[u].g - sm.g;
-            lg.h = par[u].h - sm.h;
+            const HB lg = hb_make<HB>((long long)par[u].g - g[u], (long long)par[u].h - h[u]);
             const bool left_small = e.lc <= e.rc;  // grower.rs:398-402
             hist[(size_t)e.left_pnode * slot_bins + m[u].x] = left_small ? sm : lg;
             hist[(size_t)e.right_pnode * slot_bins + m[u].x] = left_small ? lg : sm;
@@ -899,7 +910,8 @@ k_b_merge(BDev d, HBin* __restrict__ hist, uint64_t slot_bins, const void* __res
 }
 
 // Bins of general tiles (built atomically into the right slot).
-__global__ void k_b_merge_rest(BDev d, HBin* __restrict__ hist, uint64_t slot_bins, uint32_t total_bins,
+template <typename HB>
+__global__ void k_b_merge_rest(BDev d, HB* __restrict__ hist, uint64_t slot_bins, uint32_t total_bins,
                                const uint32_t* __restrict__ bin_map, int root) {
     const uint32_t n_exp = d.state->n_exp;
     const uint64_t n = (uint64_t)n_exp * total_bins;
@@ -911,17 +923,29 @@ __global__ void k_b_merge_rest(BDev d, HBin* __restrict__ hist, uint64_t slot_bi
     }
 }
 
-void launch_b_merge(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t total_bins, const void* part,
-                    uint32_t n_lane_tiles, const uint2* ent, uint32_t n_ent, const uint32_t* bin_map, bool has_rest,
-                    int root, int mode, cudaStream_t st) {
+template <typename HB>
+static void launch_b_merge_t(const BDev& d, HB* hist, uint64_t slot_bins, uint32_t total_bins, const void* part,
+                             uint32_t n_lane_tiles, const uint2* ent, uint32_t n_ent, const uint32_t* bin_map,
+                             bool has_rest, int root, int mode, cudaStream_t st) {
     const unsigned grid = 148u * 8u;
     if (n_lane_tiles) {
         if (mode == GRAD_F32)
-            k_b_merge<GRAD_F32><<<grid, 256, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles, ent, n_ent, root);
+            k_b_merge<GRAD_F32, HB><<<grid, 256, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles, ent, n_ent, root);
         else
-            k_b_merge<GRAD_Q8><<<grid, 256, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles, ent, n_ent, root);
+            k_b_merge<GRAD_Q8, HB><<<grid, 256, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles, ent, n_ent, root);
     }
-    if (has_rest) k_b_merge_rest<<<grid, 256, 0, st>>>(d, hist, slot_bins, total_bins, bin_map, root);
+    if (has_rest) k_b_merge_rest<HB><<<grid, 256, 0, st>>>(d, hist, slot_bins, total_bins, bin_map, root);
+}
+
+void launch_b_merge(const BDev& d, void* hist, uint64_t slot_bins, uint32_t total_bins, const void* part,
+                    uint32_t n_lane_tiles, const uint2* ent, uint32_t n_ent, const uint32_t* bin_map, bool has_rest,
+                    int root, int mode, cudaStream_t st, int hist32) {
+    if (hist32)
+        launch_b_merge_t(d, static_cast<HBin32*>(hist), slot_bins, total_bins, part, n_lane_tiles, ent, n_ent, bin_map,
+                         has_rest, root, mode, st);
+    else
+        launch_b_merge_t(d, static_cast<HBin*>(hist), slot_bins, total_bins, part, n_lane_tiles, ent, n_ent, bin_map,
+                         has_rest, root, mode, st);
 }
 
 // Level state for the root histogram: one "expanding node" whose smaller
@@ -1170,13 +1194,14 @@ constexpr int SORT_N = 256;  // categorical columns with <= 256 bins
 // One warp: best split of column `col` of node `node` (the node's histogram
 // lives in slot nd.slot); writes cand[node * n_cols + col] and, for column 0,
 // the node totals. key / cat: this warp's SORT_N-entry shared scratch.
+template <typename HB>
 __device__ void scan_item(const ScanNode nd, uint32_t node, uint32_t col, const ScanColumn* __restrict__ cols,
-                          uint32_t n_cols, const HBin* __restrict__ hist, uint64_t slot_bins,
+                          uint32_t n_cols, const HB* __restrict__ hist, uint64_t slot_bins,
                           const double* __restrict__ scale, const GainParamsDev& gp, ColCand* __restrict__ cand,
                           long long* __restrict__ node_tot, double* key, uint32_t* cat) {
     const int lane = threadIdx.x & 31;
     const ScanColumn cm = cols[col];
-    const HBin* h = hist + (size_t)nd.slot * slot_bins + cm.hist_off;
+    const HB* h = hist + (size_t)nd.slot * slot_bins + cm.hist_off;
     const double ig = scale[2], ih = scale[3];
     const uint32_t nb = cm.n_bins;
     const uint32_t pc = nd.count;
@@ -1367,9 +1392,10 @@ __device__ void scan_item(const ScanNode nd, uint32_t node, uint32_t col, const 
     }
 }
 
+template <typename HB>
 __global__ void __launch_bounds__(SCAN_WARPS * 32)
 k_split_scan(const ScanNode* __restrict__ nodes, const ScanColumn* __restrict__ cols,
-             uint32_t n_cols, const HBin* __restrict__ hist, uint64_t slot_bins,
+             uint32_t n_cols, const HB* __restrict__ hist, uint64_t slot_bins,
              const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
              long long* __restrict__ node_tot, uint32_t col_blocks) {
     __shared__ double s_key[SCAN_WARPS][SORT_N];
@@ -1383,15 +1409,19 @@ k_split_scan(const ScanNode* __restrict__ nodes, const ScanColumn* __restrict__ 
 }
 
 void launch_split_scan(const ScanNode* nodes, uint32_t n_nodes, const ScanColumn* cols,
-                       uint32_t n_cols, const HBin* hist, uint64_t slot_bins,
+                       uint32_t n_cols, const void* hist, uint64_t slot_bins,
                        const double* scale, GainParamsDev gp, ColCand* cand,
-                       long long* node_tot, cudaStream_t st) {
+                       long long* node_tot, cudaStream_t st, int hist32) {
     if (n_nodes == 0 || n_cols == 0) return;
     const uint32_t per = (n_cols + SCAN_WARPS - 1) / SCAN_WARPS;
     const uint64_t blocks = (uint64_t)per * n_nodes;
     if (blocks > 0x7FFFFFFFull) return;
-    k_split_scan<<<(unsigned)blocks, SCAN_WARPS * 32, 0, st>>>(nodes, cols, n_cols, hist, slot_bins, scale,
-                                                              gp, cand, node_tot, per);
+    if (hist32)
+        k_split_scan<HBin32><<<(unsigned)blocks, SCAN_WARPS * 32, 0, st>>>(
+            nodes, cols, n_cols, static_cast<const HBin32*>(hist), slot_bins, scale, gp, cand, node_tot, per);
+    else
+        k_split_scan<HBin><<<(unsigned)blocks, SCAN_WARPS * 32, 0, st>>>(
+            nodes, cols, n_cols, static_cast<const HBin*>(hist), slot_bins, scale, gp, cand, node_tot, per);
 }
 
 // Across columns (find.rs:180-212 sequential; :219-270 rayon reduce).
@@ -2095,23 +2125,27 @@ __device__ void children_body(BDev d, int a, int need_split) {
 
 
 
-__global__ void k_b_zero_right(BDev d, HBin* __restrict__ hist, uint64_t slot_bins) {
+template <typename HB>
+__global__ void k_b_zero_right(BDev d, HB* __restrict__ hist, uint64_t slot_bins) {
     const uint64_t n = (uint64_t)d.state->n_exp * slot_bins;
-    uint4* p = reinterpret_cast<uint4*>(hist + (uint64_t)d.state->first_right * slot_bins);
+    HB* p = hist + (uint64_t)d.state->first_right * slot_bins;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        p[i] = make_uint4(0, 0, 0, 0);
+        p[i] = hb_make<HB>(0, 0);
 }
 
-void launch_b_zero_right(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t grid, cudaStream_t st) {
-    k_b_zero_right<<<grid, 256, 0, st>>>(d, hist, slot_bins);
+void launch_b_zero_right(const BDev& d, void* hist, uint64_t slot_bins, uint32_t grid, cudaStream_t st, int hist32) {
+    if (hist32)
+        k_b_zero_right<HBin32><<<grid, 256, 0, st>>>(d, static_cast<HBin32*>(hist), slot_bins);
+    else
+        k_b_zero_right<HBin><<<grid, 256, 0, st>>>(d, static_cast<HBin*>(hist), slot_bins);
 }
 
 // Histograms of all smaller children of the level (one persistent launch).
-template <int MODE>
+template <int MODE, typename HB>
 __global__ void __launch_bounds__(HIST_THREADS)
 k_b_hist(BDev d, const HistTile* __restrict__ tiles, uint32_t n_tiles, uint32_t S, const uint32_t* __restrict__ ridx,
          GradRef gr, const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16,
-         HBin* __restrict__ hist, uint64_t slot_bins) {
+         HB* __restrict__ hist, uint64_t slot_bins) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);
     __shared__ HistTile tile;
@@ -2132,33 +2166,39 @@ k_b_hist(BDev d, const HistTile* __restrict__ tiles, uint32_t n_tiles, uint32_t 
             ch.begin = start + off;
             ch.count = min((uint32_t)HIST_CHUNK_MAX, seg_count - off);
             ch.flags = 0u;
-            hist_item<MODE>(ch, tile, sm, S, ridx, load, bins8, s8, bins16, s16, hist, slot_bins);
+            hist_item<MODE, HB>(ch, tile, sm, S, ridx, load, bins8, s8, bins16, s16, hist, slot_bins);
         }
     }
 }
 
 void launch_b_hist(const BDev& d, const HistTile* tiles, uint32_t n_tiles, uint32_t max_smem_bins,
                    const uint32_t* ridx, const GradRef& gr, const uint8_t* bins8, uint32_t s8,
-                   const uint16_t* bins16, uint32_t s16, HBin* hist, uint64_t slot_bins, uint32_t grid,
-                   cudaStream_t st) {
+                   const uint16_t* bins16, uint32_t s16, void* hist, uint64_t slot_bins, uint32_t grid,
+                   cudaStream_t st, int hist32) {
     if (n_tiles == 0) return;
     const uint32_t S = (max_smem_bins + 3u) & ~3u;
     const size_t smem = (size_t)S * acc_words(gr.mode) * sizeof(uint32_t);
     init_kernel_attributes();
+    HBin* h64 = static_cast<HBin*>(hist);
+    HBin32* h32 = static_cast<HBin32*>(hist);
     if (gr.mode == GRAD_Q16)
-        k_b_hist<GRAD_Q16><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16, s16,
-                                                              hist, slot_bins);
+        k_b_hist<GRAD_Q16, HBin><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16,
+                                                                    s16, h64, slot_bins);
+    else if (gr.mode == GRAD_Q8 && hist32)
+        k_b_hist<GRAD_Q8, HBin32><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16,
+                                                                     s16, h32, slot_bins);
     else if (gr.mode == GRAD_Q8)
-        k_b_hist<GRAD_Q8><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16, s16,
-                                                             hist, slot_bins);
+        k_b_hist<GRAD_Q8, HBin><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16,
+                                                                   s16, h64, slot_bins);
     else
-        k_b_hist<GRAD_F32><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16, s16,
-                                                              hist, slot_bins);
+        k_b_hist<GRAD_F32, HBin><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16,
+                                                                    s16, h64, slot_bins);
 }
 
 
+template <typename HB>
 __global__ void __launch_bounds__(SCAN_WARPS * 32)
-k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HBin* __restrict__ hist,
+k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HB* __restrict__ hist,
          uint64_t slot_bins, const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
          long long* __restrict__ node_tot) {
     __shared__ double s_key[SCAN_WARPS][SORT_N];
@@ -2175,11 +2215,16 @@ k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HBi
     }
 }
 
-void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const HBin* hist, uint64_t slot_bins,
+void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const void* hist, uint64_t slot_bins,
                    const double* scale, GainParamsDev gp, ColCand* cand, long long* node_tot, uint32_t grid,
-                   cudaStream_t st) {
+                   cudaStream_t st, int hist32) {
     if (n_cols == 0) return;
-    k_b_scan<<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, hist, slot_bins, scale, gp, cand, node_tot);
+    if (hist32)
+        k_b_scan<HBin32><<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, static_cast<const HBin32*>(hist), slot_bins,
+                                                           scale, gp, cand, node_tot);
+    else
+        k_b_scan<HBin><<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, static_cast<const HBin*>(hist), slot_bins,
+                                                         scale, gp, cand, node_tot);
 }
 
 // Reduction over columns (find.rs:180-270) straight into the next frontier.
@@ -2870,9 +2915,10 @@ void init_kernel_attributes() {
     cudaFuncSetAttribute(k_hist_build<GRAD_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
     cudaFuncSetAttribute(k_hist_build<GRAD_Q16>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
     cudaFuncSetAttribute(k_hist_build<GRAD_Q8>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
-    cudaFuncSetAttribute(k_b_hist<GRAD_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
-    cudaFuncSetAttribute(k_b_hist<GRAD_Q16>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
-    cudaFuncSetAttribute(k_b_hist<GRAD_Q8>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
+    cudaFuncSetAttribute(k_b_hist<GRAD_F32, HBin>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
+    cudaFuncSetAttribute(k_b_hist<GRAD_Q16, HBin>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
+    cudaFuncSetAttribute(k_b_hist<GRAD_Q8, HBin>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
+    cudaFuncSetAttribute(k_b_hist<GRAD_Q8, HBin32>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
     cudaFuncSetAttribute(k_bin_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
     const int lane_smem = (int)lane_smem_bytes(GRAD_F32);
     cudaFuncSetAttribute(k_b_hist_part<GRAD_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, lane_smem);

@@ -20,6 +20,11 @@ namespace bst {
 struct HBin {
     long long g, h;
 };
+// The quantised Q8 form's node histograms when every sum fits 32 bits
+// (n * 127 < 2^31): half the bytes for the merge and the split scan.
+struct HBin32 {
+    int g, h;
+};
 
 // ---- K1 bin assignment ----------------------------------------------------
 struct BinColumn {
@@ -174,10 +179,11 @@ struct NodeSplit {
     unsigned long long cats[4];
     long long tot_g, tot_h;  // exact fixed-point node totals
 };
+// hist: HBin, or HBin32 when hist32 != 0 (the same for the level kernels below)
 void launch_split_scan(const ScanNode* nodes, uint32_t n_nodes, const ScanColumn* cols,
-                       uint32_t n_cols, const HBin* hist, uint64_t slot_bins,
+                       uint32_t n_cols, const void* hist, uint64_t slot_bins,
                        const double* scale, GainParamsDev gp, ColCand* cand,
-                       long long* node_tot, cudaStream_t st);
+                       long long* node_tot, cudaStream_t st, int hist32 = 0);
 void launch_split_reduce(const ColCand* cand, const long long* node_tot, uint32_t n_nodes,
                          uint32_t n_cols, int last_wins, NodeSplit* out, cudaStream_t st);
 
@@ -306,11 +312,12 @@ void launch_transpose_bins(const uint8_t* b8, uint32_t s8, const uint16_t* b16, 
 void launch_b_partition(const BDev& d, const uint32_t* rin, uint32_t* rout, const uint8_t* bins8, uint32_t s8,
                         const uint16_t* bins16, uint32_t s16, int a, int need_split, uint32_t grid,
                         const void* qin, void* qout, int mode, const BinsFM& fm, cudaStream_t st);
-void launch_b_zero_right(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t grid, cudaStream_t st);
+void launch_b_zero_right(const BDev& d, void* hist, uint64_t slot_bins, uint32_t grid, cudaStream_t st,
+                         int hist32 = 0);
 void launch_b_hist(const BDev& d, const HistTile* tiles, uint32_t n_tiles, uint32_t max_smem_bins,
                    const uint32_t* ridx, const GradRef& gr, const uint8_t* bins8, uint32_t s8,
-                   const uint16_t* bins16, uint32_t s16, HBin* hist, uint64_t slot_bins, uint32_t grid,
-                   cudaStream_t st);
+                   const uint16_t* bins16, uint32_t s16, void* hist, uint64_t slot_bins, uint32_t grid,
+                   cudaStream_t st, int hist32 = 0);
 // Partial histograms of every (row segment, lane tile) item of the level
 // (state: n_exp, hist_chunks, hist_chunk; exp[].small_begin/small_count/
 // hist_off; seg_exp).
@@ -323,14 +330,14 @@ void launch_b_hist_part(const BDev& d, const LaneTile* tiles, uint32_t n_tiles, 
 // built atomically into the right slots.
 // ent [n_ent]: per partial entry of a node (lane tiles in order, column-major
 // inside each tile): (global bin or 0xFFFFFFFF, tile << 16 | offset).
-void launch_b_merge(const BDev& d, HBin* hist, uint64_t slot_bins, uint32_t total_bins, const void* part,
+void launch_b_merge(const BDev& d, void* hist, uint64_t slot_bins, uint32_t total_bins, const void* part,
                     uint32_t n_lane_tiles, const uint2* ent, uint32_t n_ent, const uint32_t* bin_map, bool has_rest,
-                    int root, int mode, cudaStream_t st);
+                    int root, int mode, cudaStream_t st, int hist32 = 0);
 // Level state of the root histogram: all n rows as one segment list.
 void launch_b_root_hist(const BDev& d, uint64_t n, uint32_t chunk, cudaStream_t st);
-void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const HBin* hist,
+void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const void* hist,
                    uint64_t slot_bins, const double* scale, GainParamsDev gp, ColCand* cand,
-                   long long* node_tot, uint32_t grid, cudaStream_t st);
+                   long long* node_tot, uint32_t grid, cudaStream_t st, int hist32 = 0);
 // column reduction into frontier b; decide != 0: then (last block) the
 // decisions of the next level, whose rows are in buffer buf
 void launch_b_reduce(const BDev& d, int b, const ColCand* cand, const long long* node_tot, uint32_t n_cols,
