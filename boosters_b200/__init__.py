@@ -7,6 +7,7 @@ The Python surface mirrors ``boosters`` (packages/boosters-python:
 sm_100a CUDA kernels. There is no CPU fallback.
 """
 import ctypes
+import os
 import enum
 
 import numpy as np
@@ -319,6 +320,51 @@ class GBDTModel:
         m = GBDTModel(h, config)
         m._rows = train.n_samples
         return m
+
+    # ---- model files (packages/boosters-python/src/model/gbdt.rs:259-330) ----
+    def _bytes(self, fn, *args):
+        buf, n = ctypes.c_void_p(), ctypes.c_uint64()
+        _n.check(fn(self._h, *args, ctypes.byref(buf), ctypes.byref(n)))
+        try:
+            return ctypes.string_at(buf.value, n.value) if n.value else b""
+        finally:
+            _n.lib.bst_buffer_free(buf)
+
+    def to_bytes(self):
+        """The model as a ``.bstr`` file (uncompressed MessagePack payload)."""
+        return self._bytes(_n.lib.bst_model_to_bstr)
+
+    def to_json_bytes(self, pretty=False):
+        """The model as a ``.bstr.json`` document."""
+        return self._bytes(_n.lib.bst_model_to_json, 1 if pretty else 0)
+
+    @staticmethod
+    def from_bytes(data, config=None):
+        """A model from ``.bstr`` or ``.bstr.json`` bytes."""
+        data = bytes(data)
+        h = ctypes.c_void_p()
+        _n.check(_n.lib.bst_model_from_bytes(data, len(data), ctypes.byref(h)))
+        return GBDTModel(h, config or GBDTConfig())
+
+    from_json_bytes = from_bytes
+
+    def save(self, path, pretty=False):
+        """Writes ``path``: JSON when it ends in ``.json``, else ``.bstr``."""
+        p = os.fsencode(path)
+        if p.endswith(b".json"):
+            _n.check(_n.lib.bst_model_write_json(self._h, p, 1 if pretty else 0))
+        else:
+            _n.check(_n.lib.bst_model_write_bstr(self._h, p))
+
+    @staticmethod
+    def load(path, config=None):
+        """Reads a ``.bstr`` or ``.bstr.json`` file (Model::load, persist/mod.rs:325)."""
+        h = ctypes.c_void_p()
+        _n.check(_n.lib.bst_model_load(os.fsencode(path), ctypes.byref(h)))
+        return GBDTModel(h, config or GBDTConfig())
+
+    def __reduce__(self):
+        return (GBDTModel.from_bytes, (self.to_bytes(),))
 
     @staticmethod
     def grow_tree(dataset, grad, hess, config=None, n_threads=0):

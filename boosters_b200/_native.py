@@ -120,6 +120,16 @@ SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int32,
       ctypes.c_void_p, ctypes.c_void_p]),
     ("bst_model_free", None, [ctypes.c_void_p]),
+    ("bst_model_to_json", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p),
+                                           ctypes.POINTER(ctypes.c_uint64)]),
+    ("bst_model_to_bstr", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                           ctypes.POINTER(ctypes.c_uint64)]),
+    ("bst_model_from_bytes", ctypes.c_int32, [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
+    ("bst_buffer_free", None, [ctypes.c_void_p]),
+    ("bst_model_write_json", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32]),
+    ("bst_model_write_bstr", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_char_p]),
+    ("bst_model_load", ctypes.c_int32, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
+    ("bst_crc32c", ctypes.c_uint32, [ctypes.c_char_p, ctypes.c_uint64]),
     ("bst_model_n_trees", ctypes.c_uint32, [ctypes.c_void_p]),
     ("bst_model_n_groups", ctypes.c_uint32, [ctypes.c_void_p]),
     ("bst_model_n_features", ctypes.c_uint32, [ctypes.c_void_p]),

@@ -23,7 +23,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fn
              "-Wall", "-Wno-unused-function", f"-I{CUDA}/include"]
 
 CU_SOURCES = ["kernels.cu", "noalloc.cu"]
-CPP_SOURCES = ["binning.cpp", "engine.cpp", "capi.cpp", "server.cpp", "synth.cpp"]
+CPP_SOURCES = ["binning.cpp", "engine.cpp", "capi.cpp", "server.cpp", "synth.cpp", "persist.cpp"]
 HEADERS = ["kernels.h", "binning.h", "engine.h", os.path.join("..", "..", "include", "boosters_c.h")]
 
 

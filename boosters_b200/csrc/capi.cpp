@@ -7,6 +7,8 @@
 #include <string>
 
 #include "../../include/boosters_c.h"
+#include <cstdio>
+#include <cstdlib>
 #include "engine.h"
 
 struct bst_dataset {
@@ -286,6 +288,87 @@ bst_status bst_gbdt_predict_device(const bst_model* m, const float* x, uint64_t 
 }
 
 void bst_model_free(bst_model* m) { delete m; }
+
+static bst_status copy_out(const void* src, size_t n, uint8_t** out, uint64_t* len) {
+    uint8_t* b = static_cast<uint8_t*>(std::malloc(n ? n : 1));
+    if (!b) return fail(BST_ERR_OUT_OF_MEMORY, "host allocation failed");
+    if (n) std::memcpy(b, src, n);
+    *out = b;
+    *len = n;
+    return BST_OK;
+}
+
+bst_status bst_model_to_json(const bst_model* model, int32_t pretty, uint8_t** out, uint64_t* len) {
+    if (!model || !out || !len) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    return guarded([&]() -> bst_status {
+        const std::string s = bst::model_to_json(*model->m, pretty != 0);
+        return copy_out(s.data(), s.size(), out, len);
+    });
+}
+
+bst_status bst_model_to_bstr(const bst_model* model, uint8_t** out, uint64_t* len) {
+    if (!model || !out || !len) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    return guarded([&]() -> bst_status {
+        const std::vector<uint8_t> b = bst::model_to_bstr(*model->m);
+        return copy_out(b.data(), b.size(), out, len);
+    });
+}
+
+bst_status bst_model_from_bytes(const uint8_t* data, uint64_t len, bst_model** out) {
+    if (!out || (len && !data)) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    return guarded([&]() -> bst_status {
+        std::unique_ptr<bst_model> h(new bst_model());
+        h->m = bst::model_from_bytes(data, (size_t)len);
+        *out = h.release();
+        return BST_OK;
+    });
+}
+
+void bst_buffer_free(void* p) { std::free(p); }
+
+static bst_status write_file(const char* path, const void* data, size_t n) {
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(BST_ERR_INVALID_ARGUMENT, std::string("cannot open ") + path + " for writing");
+    const size_t w = n ? std::fwrite(data, 1, n, f) : 0;
+    const int c = std::fclose(f);
+    if (w != n || c != 0) return fail(BST_ERR_INVALID_ARGUMENT, std::string("write to ") + path + " failed");
+    return BST_OK;
+}
+
+bst_status bst_model_write_json(const bst_model* model, const char* path, int32_t pretty) {
+    if (!model || !path) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    return guarded([&]() -> bst_status {
+        const std::string s = bst::model_to_json(*model->m, pretty != 0);
+        return write_file(path, s.data(), s.size());
+    });
+}
+
+bst_status bst_model_write_bstr(const bst_model* model, const char* path) {
+    if (!model || !path) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    return guarded([&]() -> bst_status {
+        const std::vector<uint8_t> b = bst::model_to_bstr(*model->m);
+        return write_file(path, b.data(), b.size());
+    });
+}
+
+bst_status bst_model_load(const char* path, bst_model** out) {
+    if (!path || !out) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    return guarded([&]() -> bst_status {
+        FILE* f = std::fopen(path, "rb");
+        if (!f) return fail(BST_ERR_INVALID_ARGUMENT, std::string("cannot open ") + path);
+        std::vector<uint8_t> buf;
+        uint8_t chunk[1 << 16];
+        size_t r;
+        while ((r = std::fread(chunk, 1, sizeof(chunk), f)) > 0) buf.insert(buf.end(), chunk, chunk + r);
+        std::fclose(f);
+        std::unique_ptr<bst_model> h(new bst_model());
+        h->m = bst::model_from_bytes(buf.data(), buf.size());
+        *out = h.release();
+        return BST_OK;
+    });
+}
+
+uint32_t bst_crc32c(const uint8_t* data, uint64_t len) { return bst::crc32c_bytes(data, (size_t)len); }
 uint32_t bst_model_n_trees(const bst_model* m) { return m ? (uint32_t)m->m->trees.size() : 0; }
 uint32_t bst_model_n_groups(const bst_model* m) { return m ? m->m->n_groups : 0; }
 uint32_t bst_model_n_features(const bst_model* m) { return m ? m->m->n_features : 0; }

@@ -156,6 +156,12 @@ void predict_host(const Model& m, const HostDataset& ds, bool raw, float* out);
 void predict_device(const Model& m, const float* x_dev_sm, uint64_t n, uint64_t F, bool raw,
                     float* out_dev, cudaStream_t st);
 int transform_of(int objective);
+// Model files (persist.cpp): .bstr.json text and .bstr bytes (uncompressed
+// MessagePack); model_from_bytes reads either (binary by its magic).
+std::string model_to_json(const Model& m, bool pretty);
+std::vector<uint8_t> model_to_bstr(const Model& m);
+std::unique_ptr<Model> model_from_bytes(const uint8_t* data, size_t len);
+uint32_t crc32c_bytes(const uint8_t* p, size_t n);
 
 // Continuous-batching prediction server (server.cpp). The model must outlive
 // the server.

@@ -348,6 +348,33 @@ bst_status bst_quantize_gradients(const float* grad, const float* hess, uint64_t
                                   int32_t* qh, double* steps);
 
 /* ------------------------------------------------------------------------ */
+/* Model files: the reference's .bstr.json (JSON envelope bstr_version /     */
+/* model_type / model, persist/json.rs:50-75) and .bstr (32-byte header,    */
+/* MessagePack named-map payload, 16-byte trailer with CRC32C;              */
+/* persist/envelope.rs:13-221, binary.rs:52-146) layouts of the model       */
+/* schema (persist/schema.rs:27-150, convert.rs:78-420). Replace            */
+/* GBDTModel::{to_bytes, to_json_bytes, from_bytes, from_json_bytes}        */
+/* (packages/boosters-python/src/model/gbdt.rs:259-330) and Model::load     */
+/* (persist/mod.rs:325).                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Library-allocated bytes: free with bst_buffer_free. .bstr payloads are
+ * written uncompressed (format byte 0x01); zstd payloads (0x02) are read
+ * as BST_ERR_UNSUPPORTED (no zstd decoder is linked). */
+bst_status bst_model_to_json(const bst_model* model, int32_t pretty, uint8_t** out, uint64_t* len);
+bst_status bst_model_to_bstr(const bst_model* model, uint8_t** out, uint64_t* len);
+/* Either layout (binary when the bytes start with "BSTR"). Malformed input:
+ * BST_ERR_INVALID_ARGUMENT with the reason; linear or multi-value leaves:
+ * BST_ERR_UNSUPPORTED. */
+bst_status bst_model_from_bytes(const uint8_t* data, uint64_t len, bst_model** out);
+void bst_buffer_free(void* p);
+bst_status bst_model_write_json(const bst_model* model, const char* path, int32_t pretty);
+bst_status bst_model_write_bstr(const bst_model* model, const char* path);
+bst_status bst_model_load(const char* path, bst_model** out);
+/* CRC32C (Castagnoli) of the .bstr trailer. */
+uint32_t bst_crc32c(const uint8_t* data, uint64_t len);
+
+/* ------------------------------------------------------------------------ */
 /* Serving: continuous batching over a device-resident forest (the engine's  */
 /* serving loop; the reference predicts one call at a time through          */
 /* Predictor::predict_into, inference/gbdt/predictor.rs:197).                */
