@@ -362,6 +362,10 @@ def run_ours(args, world, rank, local):
         except Exception as ex:  # reported, not fatal
             serving = {"error": str(ex)}
 
+    extra = None
+    if args.configs and rank == 0:
+        extra = run_configs(bst, torch)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
@@ -393,11 +397,82 @@ def run_ours(args, world, rank, local):
             "clocks": clk,
             "predict_rows_per_s": rows_pred,
             "serving": serving,
+            "configs": extra,
             "phase_ms_per_step": {k: round((t1_stats[k] - t0_stats[k]) / args.steps, 4)
                                   for k in ("gradients", "histograms", "split_scan", "partition", "leaf_update",
                                             "other")},
         }
         print(json.dumps(line), flush=True)
+
+
+def time_trees(bst, torch, ds, cfg, warm, steps):
+    """s/100 trees of `steps` timed trees after `warm` (CUDA events on the
+    engine's stream), then the rest of cfg's trees; returns (value, model)."""
+    booster = bst.Booster(ds, cfg, n_threads=0)
+    booster.update(warm)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    booster.update(steps)
+    e1.record()
+    e1.synchronize()
+    per_round = e0.elapsed_time(e1) / 1e3 / steps
+    rest = max(0, cfg.n_estimators - warm - steps)
+    if rest:
+        booster.update(rest)
+    trees_per_round = max(1, booster.model().n_trees // max(1, booster.n_rounds))
+    return 100.0 * per_round / trees_per_round, booster.model()
+
+
+def run_configs(bst, torch):
+    """The survey's other workloads, each in its plain form and its fast form
+    at equal loss: config 1 (5k x 100 regression), config 3 (10M x 200
+    leaf-wise 255 leaves, Q8 vs FP32), config 4 (2M x 50 softmax with 10
+    categorical columns, 10 classes)."""
+    out = {}
+    # config 1
+    x, y = bst.synth.regression(5_000, 100, 20, seed=1)
+    xv, yv = bst.synth.regression(1_000, 100, 20, seed=1, stream=1)
+    ds = bst.Dataset.from_feature_major(x, y)
+    kw = dict(n_estimators=50, max_depth=6, learning_rate=0.1, metric=bst.Metric.none())
+    c1 = {}
+    for form, over in (("plain", {}), ("batched_q8", dict(precision="q8", batched=True))):
+        v, m = time_trees(bst, torch, ds, bst.GBDTConfig(**kw, **over), 5, 40)
+        pv = m.predict_group_major(bst.Dataset.from_feature_major(xv))
+        c1[form] = {"s_per_100_trees": round(v, 5), "heldout_rmse": round(bst.metric("rmse", pv, yv), 6)}
+    out["config1_regression_5kx100_depth6"] = c1
+    # config 3
+    x, y = bst.synth.binary(10_000_000, 200, 20, seed=3)
+    xv, yv = bst.synth.binary(1_000_000, 200, 20, seed=3, stream=1)
+    ds = bst.Dataset.from_feature_major(x, y)
+    del x
+    kw = dict(objective=bst.Objective.logistic(), n_estimators=40, learning_rate=0.1,
+              growth_strategy=bst.GrowthStrategy.Leafwise, n_leaves=255, metric=bst.Metric.none())
+    c3 = {}
+    for form, over in (("plain_fp32", {}), ("q8", dict(precision="q8"))):
+        v, m = time_trees(bst, torch, ds, bst.GBDTConfig(**kw, **over), 3, 30)
+        pv = m.predict_group_major(bst.Dataset.from_feature_major(xv))
+        c3[form] = {"s_per_100_trees": round(v, 4), "heldout_logloss": round(bst.metric("logloss", pv, yv), 6),
+                    "trees": m.n_trees}
+    c3["loss_rel_q8_vs_fp32"] = round((c3["q8"]["heldout_logloss"] - c3["plain_fp32"]["heldout_logloss"])
+                                      / c3["plain_fp32"]["heldout_logloss"], 6)
+    out["config3_leafwise255_10Mx200"] = c3
+    del ds
+    # config 4
+    x, y = bst.synth.multiclass(2_000_000, 40, 10, 10, seed=4)
+    xv, yv = bst.synth.multiclass(400_000, 40, 10, 10, seed=4, stream=1)
+    cats = list(range(40, 50))
+    ds = bst.Dataset.from_feature_major(x, y, categorical_features=cats)
+    kw = dict(objective=bst.Objective.softmax(10), n_estimators=40, max_depth=6, learning_rate=0.1,
+              metric=bst.Metric.none())
+    c4 = {}
+    for form, over in (("plain", {}), ("batched_q8", dict(precision="q8", batched=True))):
+        v, m = time_trees(bst, torch, ds, bst.GBDTConfig(**kw, **over), 3, 20)
+        pv = m.predict_group_major(bst.Dataset.from_feature_major(xv, categorical_features=cats))
+        c4[form] = {"s_per_100_trees": round(v, 5), "heldout_mlogloss": round(bst.metric("mlogloss", pv, yv), 6),
+                    "trees": m.n_trees}
+    out["config4_softmax10_cat10_2Mx50_depth6"] = c4
+    return out
 
 
 def run_profile(args):
@@ -443,6 +518,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--profile", choices=["train", "predict"], help="run a small workload for a profiler and exit")
+    ap.add_argument("--configs", action="store_true",
+                    help="also measure the other survey workloads (configs 1, 3, 4; several minutes)")
     ap.add_argument("--form", default="batched_q8", choices=[k for k, _ in FORMS])
     ap.add_argument("--rounds", type=int, default=4)
     ap.add_argument("--trees", type=int, default=1000)
