@@ -230,7 +230,10 @@ class Dataset:
                 raise ValueError("weights must have one value per sample")
         cats = np.ascontiguousarray(sorted(set(categorical_features or [])), dtype=np.uint32)
         h = ctypes.c_void_p()
-        _n.check(_n.lib.bst_dataset_create(
+        # the engine borrows the feature array (kept alive by this object)
+        # instead of copying it
+        self._x = xfm
+        _n.check(_n.lib.bst_dataset_create_view(
             _n.ptr(xfm, ctypes.c_float), n_features, n_samples, _n.ptr(y, ctypes.c_float), n_outputs,
             _n.ptr(w, ctypes.c_float), _n.ptr(cats, ctypes.c_uint32) if len(cats) else None, len(cats),
             ctypes.byref(h)))
@@ -527,6 +530,7 @@ class Booster:
         h = ctypes.c_void_p()
         _n.check(_n.lib.bst_booster_create(train._h, ctypes.byref(c), int(n_threads), ctypes.byref(h)))
         self._h = h
+        self._train = train  # the booster reads the dataset's host arrays while it lives
         self._rows = train.n_samples
 
     def update(self, n_rounds=1):

@@ -100,6 +100,9 @@ SIGNATURES = [
     ("bst_dataset_create", ctypes.c_int32,
      [c_f32p, ctypes.c_uint64, ctypes.c_uint64, c_f32p, ctypes.c_uint32, c_f32p, c_u32p,
       ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p)]),
+    ("bst_dataset_create_view", ctypes.c_int32,
+     [c_f32p, ctypes.c_uint64, ctypes.c_uint64, c_f32p, ctypes.c_uint32, c_f32p, c_u32p,
+      ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p)]),
     ("bst_dataset_free", None, [ctypes.c_void_p]),
     ("bst_dataset_n_samples", ctypes.c_uint64, [ctypes.c_void_p]),
     ("bst_dataset_n_features", ctypes.c_uint64, [ctypes.c_void_p]),

@@ -121,8 +121,7 @@ std::vector<uint32_t> binning_sample(uint64_t n, uint64_t k) {
     std::vector<uint32_t> out;
     if (n <= k) return out;
     out.reserve(k);
-    std::unordered_set<uint32_t> seen;
-    seen.reserve(k * 2);
+    std::vector<uint64_t> seen((n + 63) / 64, 0);  // rows drawn so far
     uint64_t s = 0xD1B54A32D192ED03ULL ^ n;
     while (out.size() < k) {
         s += 0x9E3779B97F4A7C15ULL;
@@ -131,10 +130,49 @@ std::vector<uint32_t> binning_sample(uint64_t n, uint64_t k) {
         z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
         z ^= z >> 31;
         const uint32_t r = (uint32_t)(z % n);
-        if (seen.insert(r).second) out.push_back(r);
+        uint64_t& word = seen[r >> 6];
+        const uint64_t bit = 1ull << (r & 63u);
+        if (!(word & bit)) {
+            word |= bit;
+            out.push_back(r);
+        }
     }
     std::sort(out.begin(), out.end());
     return out;
+}
+
+// Ascending sort of finite floats by an LSD radix sort of order-preserving
+// keys (sign bit flipped for positives, all bits for negatives); -0.0 sorts
+// before +0.0, which compare equal and so merge in the distinct pass.
+void sort_floats(std::vector<float>& v) {
+    const size_t n = v.size();
+    if (n < 2048) {
+        std::sort(v.begin(), v.end());
+        return;
+    }
+    std::vector<uint32_t> a(n), b(n);
+    for (size_t i = 0; i < n; ++i) {
+        uint32_t u;
+        std::memcpy(&u, &v[i], 4);
+        a[i] = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    }
+    for (int shift = 0; shift < 32; shift += 11) {
+        uint32_t cnt[2048] = {0};
+        for (size_t i = 0; i < n; ++i) ++cnt[(a[i] >> shift) & 2047u];
+        uint32_t sum = 0;
+        for (uint32_t d = 0; d < 2048; ++d) {
+            const uint32_t c = cnt[d];
+            cnt[d] = sum;
+            sum += c;
+        }
+        for (size_t i = 0; i < n; ++i) b[cnt[(a[i] >> shift) & 2047u]++] = a[i];
+        a.swap(b);
+    }
+    for (size_t i = 0; i < n; ++i) {
+        const uint32_t k = a[i];
+        const uint32_t u = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
+        std::memcpy(&v[i], &u, 4);
+    }
 }
 
 // dataset.rs:683-750: quantile midpoints over the distinct finite values.
@@ -157,7 +195,7 @@ Mapper numeric_mapper(std::vector<float>& vals, uint32_t max_bins, bool has_nan)
         return m;
     }
     const uint32_t nb = (uint32_t)std::min<uint64_t>(max_bins, w);
-    std::sort(vals.begin(), vals.end());
+    sort_floats(vals);
     vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
     const size_t u = vals.size();
     if (u <= nb) {

@@ -146,8 +146,8 @@ bst_status bst_config_validate(const bst_config* c) {
     return check_config(c, false);
 }
 
-bst_status bst_dataset_create(const float* x, uint64_t F, uint64_t n, const float* y, uint32_t n_outputs,
-                              const float* w, const uint32_t* cat, uint32_t n_cat, bst_dataset** out) {
+static bst_status dataset_create(const float* x, uint64_t F, uint64_t n, const float* y, uint32_t n_outputs,
+                                 const float* w, const uint32_t* cat, uint32_t n_cat, bst_dataset** out, bool view) {
     return guarded([&]() -> bst_status {
         if (!out) return fail(BST_ERR_INVALID_ARGUMENT, "out is NULL");
         *out = nullptr;
@@ -160,7 +160,10 @@ bst_status bst_dataset_create(const float* x, uint64_t F, uint64_t n, const floa
         bst::HostDataset& d = ds->d;
         d.n = n;
         d.F = F;
-        d.x.assign(x, x + F * n);
+        if (view)
+            d.xv = x;
+        else
+            d.x.assign(x, x + F * n);
         if (y) {
             d.n_outputs = n_outputs;
             d.y.assign(y, y + (size_t)n_outputs * n);
@@ -174,6 +177,16 @@ bst_status bst_dataset_create(const float* x, uint64_t F, uint64_t n, const floa
         *out = ds;
         return BST_OK;
     });
+}
+
+bst_status bst_dataset_create(const float* x, uint64_t F, uint64_t n, const float* y, uint32_t n_outputs,
+                              const float* w, const uint32_t* cat, uint32_t n_cat, bst_dataset** out) {
+    return dataset_create(x, F, n, y, n_outputs, w, cat, n_cat, out, false);
+}
+
+bst_status bst_dataset_create_view(const float* x, uint64_t F, uint64_t n, const float* y, uint32_t n_outputs,
+                                   const float* w, const uint32_t* cat, uint32_t n_cat, bst_dataset** out) {
+    return dataset_create(x, F, n, y, n_outputs, w, cat, n_cat, out, true);
 }
 
 void bst_dataset_free(bst_dataset* ds) { delete ds; }

@@ -1470,7 +1470,7 @@ uint32_t HostTree::alloc() {
 void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, DeviceBinned& out) {
     std::string err;
     const auto t0 = std::chrono::steady_clock::now();
-    bst_status rc = plan_binning(ds.x.data(), ds.F, ds.n, ds.user_cat, cfg, out.plan, err);
+    bst_status rc = plan_binning(ds.xdata(), ds.F, ds.n, ds.user_cat, cfg, out.plan, err);
     if (rc != BST_OK) throw Error{rc, err};
     const BinPlan& p = out.plan;
     const uint32_t nc = p.n_cols();
@@ -1509,7 +1509,7 @@ void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, 
     DevArray<BinColumn> d_cols;
     x.alloc((size_t)nc * n);
     for (uint32_t c = 0; c < nc; ++c)
-        BST_CK(cudaMemcpyAsync(x.p + (size_t)c * n, ds.x.data() + (size_t)p.col_feature[c] * n, sizeof(float) * n,
+        BST_CK(cudaMemcpyAsync(x.p + (size_t)c * n, ds.xdata() + (size_t)p.col_feature[c] * n, sizeof(float) * n,
                                cudaMemcpyHostToDevice, st));
     d_cols.alloc(nc);
     BST_CK(cudaMemcpyAsync(d_cols.p, cols.data(), sizeof(BinColumn) * nc, cudaMemcpyHostToDevice, st));
@@ -1906,7 +1906,7 @@ void predict_host(const Model& m, const HostDataset& ds, bool raw, float* out) {
     DevArray<float> x, o;
     x.alloc((size_t)n * ds.F);
     o.alloc((size_t)n * m.n_groups);
-    BST_CK(cudaMemcpyAsync(x.p, ds.x.data(), sizeof(float) * n * ds.F, cudaMemcpyHostToDevice, sg.s));
+    BST_CK(cudaMemcpyAsync(x.p, ds.xdata(), sizeof(float) * n * ds.F, cudaMemcpyHostToDevice, sg.s));
     launch_predict(f.view, x.p, n, (uint32_t)ds.F, 1, o.p, sg.s);
     if (!raw) launch_transform(transform_of(m.objective), o.p, m.n_groups, n, sg.s);
     BST_CK(cudaGetLastError());

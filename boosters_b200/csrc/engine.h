@@ -55,7 +55,9 @@ struct DevArray {
 // Host copy of a feature-major dataset (data/raw/dataset.rs:139).
 struct HostDataset {
     uint64_t n = 0, F = 0;
-    std::vector<float> x;  // [F][n]
+    std::vector<float> x;  // [F][n] (owned copy), or
+    const float* xv = nullptr;  // the caller's [F][n] array (a view)
+    const float* xdata() const { return xv ? xv : x.data(); }
     std::vector<float> y;  // [n_outputs][n]
     uint32_t n_outputs = 0;
     std::vector<float> w;

@@ -144,6 +144,14 @@ bst_status bst_dataset_create(const float* features, uint64_t n_features, uint64
                               const float* targets, uint32_t n_outputs, const float* weights,
                               const uint32_t* categorical_features, uint32_t n_categorical,
                               bst_dataset** out);
+/* As bst_dataset_create, but the features stay in the caller's array (no
+ * copy): it must stay valid and unchanged while the dataset, and every
+ * booster created from it, exists. Binning reads it directly (pinned host
+ * memory gives an asynchronous device copy). Targets and weights are copied. */
+bst_status bst_dataset_create_view(const float* features, uint64_t n_features, uint64_t n_samples,
+                                   const float* targets, uint32_t n_outputs, const float* weights,
+                                   const uint32_t* categorical_features, uint32_t n_categorical,
+                                   bst_dataset** out);
 void bst_dataset_free(bst_dataset* ds);
 uint64_t bst_dataset_n_samples(const bst_dataset* ds);
 uint64_t bst_dataset_n_features(const bst_dataset* ds);
