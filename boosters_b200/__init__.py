@@ -118,7 +118,7 @@ class GBDTConfig:
                  max_bins=256, enable_bundling=True, sparsity_threshold=0.9,
                  max_categorical_cardinality=0, binning_sample_cnt=200000, cache_size=8,
                  early_stopping_rounds=None, seed=42, verbosity=0, precision="fp32",
-                 cuda_graph=False, device=0, batched=True):
+                 cuda_graph=False, device=0, batched=True, phase_timings=False):
         self.n_estimators = n_estimators
         self.learning_rate = learning_rate
         self.objective = objective if objective is not None else Objective.Squared()
@@ -144,6 +144,7 @@ class GBDTConfig:
         self.early_stopping_rounds = early_stopping_rounds
         self.seed = seed
         self.verbosity = verbosity
+        self.phase_timings = phase_timings
         if precision not in _PRECISION:
             raise ValueError(f"precision must be one of {sorted(_PRECISION)}")
         self.precision = precision
@@ -186,6 +187,7 @@ class GBDTConfig:
         c.batched = 1 if self.batched else 0
         c.device = int(self.device)
         c.record_leaves = 1 if record_leaves else 0
+        c.phase_timings = 1 if self.phase_timings else 0
         return c
 
     def __repr__(self):

@@ -70,6 +70,7 @@ class Config(ctypes.Structure):
         ("cuda_graph", ctypes.c_int32),
         ("device", ctypes.c_int32),
         ("record_leaves", ctypes.c_int32),
+        ("phase_timings", ctypes.c_int32),
     ]
 
 

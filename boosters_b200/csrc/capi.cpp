@@ -139,6 +139,7 @@ void bst_config_default(bst_config* c) {
     c->cuda_graph = 0;
     c->device = 0;
     c->record_leaves = 0;
+    c->phase_timings = 0;
 }
 
 bst_status bst_config_validate(const bst_config* c) {

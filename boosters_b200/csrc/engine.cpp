@@ -230,6 +230,7 @@ struct Timer {
     // record during capture is only an internal dependency, not a timestamp)
     bool in_graph = false;
     bool broken = false;
+    bool enabled = true;  // off: begin/end record nothing (no event nodes in graphs)
     void record(cudaEvent_t e) {
         if (in_graph)
             BST_CK(cudaEventRecordWithFlags(e, st, cudaEventRecordExternal));
@@ -237,12 +238,15 @@ struct Timer {
             BST_CK(cudaEventRecord(e, st));
     }
     size_t begin(int phase) {
+        if (!enabled) return 0;
         size_t i = used;
         record(next());
         marks.push_back({phase, i});
         return i;
     }
-    void end() { record(next()); }
+    void end() {
+        if (enabled) record(next());
+    }
     // stream must be idle
     void collect() {
         for (auto& m : marks) {
@@ -305,6 +309,7 @@ class Trainer {
         const uint32_t max_leaves = leafwise_ ? cfg.max_leaves : (1u << std::min<uint32_t>(cfg.max_depth, 31));
         max_pnodes_ = std::max<uint32_t>(1, max_leaves);
         timer_.st = st;
+        timer_.enabled = cfg.phase_timings != 0;
         gp_.lambda = (double)cfg.lambda;
         gp_.min_gain = (double)cfg.min_gain;
         gp_.min_child_weight = (double)cfg.min_child_weight;
@@ -831,6 +836,7 @@ class Trainer {
         if (!graphs_[gi]) {
             gtimers_[gi] = std::make_unique<Timer>();
             gtimers_[gi]->st = st_;
+            gtimers_[gi]->enabled = cfg_.phase_timings != 0;
             gtimers_[gi]->reserve(16 + 20 * (size_t)cfg_.max_depth);
             gtimers_[gi]->in_graph = true;
             BST_CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
