@@ -15,6 +15,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <unordered_map>
 
 namespace bst {
 
@@ -307,7 +308,8 @@ class Trainer {
         last_wins_ = (n_threads != 1) && n_cols_ >= 16;  // find.rs:125-129, utils.rs:152
         leafwise_ = cfg.growth_strategy == BST_GROWTH_LEAFWISE;
         const uint32_t max_leaves = leafwise_ ? cfg.max_leaves : (1u << std::min<uint32_t>(cfg.max_depth, 31));
-        max_pnodes_ = std::max<uint32_t>(1, max_leaves);
+        // leaf-wise: room for speculative expansions (grow_leafwise)
+        max_pnodes_ = std::max<uint32_t>(1, leafwise_ ? 2 * max_leaves : max_leaves);
         timer_.st = st;
         timer_.enabled = cfg.phase_timings != 0;
         gp_.lambda = (double)cfg.lambda;
@@ -543,7 +545,11 @@ class Trainer {
             // unnecessary with 180 GB of HBM); refuse sizes that cannot fit
             size_t free_b = 0, total_b = 0;
             BST_CK(cudaMemGetInfo(&free_b, &total_b));
-            const double need = (double)max_pnodes_ * (double)slot_bins_ * sizeof(HBin);
+            double need = (double)max_pnodes_ * (double)slot_bins_ * sizeof(HBin);
+            if (leafwise_ && need > 0.6 * (double)free_b && max_pnodes_ > cfg_.max_leaves) {
+                max_pnodes_ = std::max<uint32_t>(1, cfg_.max_leaves);  // no room to speculate
+                need = (double)max_pnodes_ * (double)slot_bins_ * sizeof(HBin);
+            }
             if (need > 0.6 * (double)free_b)
                 throw Error{BST_ERR_UNSUPPORTED, "node histograms need " + std::to_string((uint64_t)need) +
                                                      " bytes; reduce max_depth / max_leaves or max_bins"};
@@ -586,6 +592,7 @@ class Trainer {
     BDev bd_{};
     DevArray<BState> d_bstate_;
     DevArray<BNode> d_front_[2];
+    DevArray<unsigned long long> d_node_key_;
     DevArray<BExp> d_bexp_;
     DevArray<BTreeNode> d_btree_;
     DevArray<BLeaf> d_bleaves_;
@@ -681,6 +688,8 @@ class Trainer {
         max_tnodes_ = 2 * max_front;
         d_front_[0].alloc(max_front);
         d_front_[1].alloc(max_front);
+        d_node_key_.alloc(max_front);
+        BST_CK(cudaMemset(d_node_key_.p, 0, sizeof(unsigned long long) * max_front));
         d_btree_.alloc(max_tnodes_);
         d_bleaves_.alloc(max_front + 1);
         std::vector<BColumn> bc(n_cols_);
@@ -708,6 +717,7 @@ class Trainer {
         bd_.sums = d_sums_.p;
         bd_.bcols = d_bcols_.p;
         bd_.max_front = max_front;
+        bd_.node_key = d_node_key_.p;
         bd_.max_tnodes = max_tnodes_;
         graphs_.assign((size_t)G_ * RING, nullptr);
         gtimers_.resize((size_t)G_ * RING);
@@ -801,11 +811,10 @@ class Trainer {
                 enqueue_hist(gl, rout, false, tm, launches, hist_launches);
                 tm.begin(PH_SCAN);
                 launch_b_scan(bd_, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p,
-                              d_node_tot_.p, g_wide, st_, hist32_);
-                launch_b_reduce(bd_, a ^ 1, d_cand_.p, d_node_tot_.p, n_cols_, last_wins_ ? 1 : 0, 1, lp, scale,
-                                (d + 1) & 1u, g_wide, st_);  // + next level's decisions
+                              d_node_tot_.p, a ^ 1, last_wins_ ? 1 : 0, lp, (d + 1) & 1u, g_wide, st_,
+                              hist32_);  // + column reduction, next level's decisions
                 tm.end();
-                launches += 2;
+                launches += 1;
             } else {
                 tm.begin(PH_OTHER);
                 BST_CK(cudaMemsetAsync(d_sums_.p, 0, sizeof(long long) * d_sums_.n, st_));
@@ -1268,6 +1277,98 @@ class Trainer {
         }
     }
 
+    // Leaf-wise growth (expansion.rs:137-166): pop the leaf of largest
+    // (gain, node id), split it, push its children, until max_leaves.
+    //
+    // The pops are replayed here exactly, but the device expands nodes in
+    // batches: when the popped node has not been expanded yet, it is
+    // expanded together with the best other unexpanded candidates of the
+    // heap (at most as many as pops remain). A node's rows, histogram and
+    // split do not depend on when it is expanded, so a node that the replay
+    // pops later costs no device step, and one it never pops is rolled back
+    // into a leaf over its full row range. Node ids of the replay (the tie
+    // rule's "node id": left child keeps the parent's, right child takes the
+    // next) are tracked apart from the histogram slots, which are allocated
+    // in batch order; the slot pool holds 2 * max_leaves so that speculation
+    // never starves the remaining pops.
+    struct Spec {
+        Cand kids[2];
+        uint32_t right_pnode, begin, count;
+    };
+    void grow_leafwise(const Cand& root, float min_gain) {
+        struct HeapEnt {
+            Cand c;
+            uint32_t vid;
+        };
+        std::vector<HeapEnt> heap{{root, 0u}};
+        std::unordered_map<uint32_t, Spec> spec;  // expanded, not yet popped (key: pnode)
+        uint32_t n_leaves = 1, n_vid = 1;
+        auto before = [](const HeapEnt& a, const HeapEnt& b) {  // a pops before b
+            return a.c.split.gain > b.c.split.gain || (a.c.split.gain == b.c.split.gain && a.vid > b.vid);
+        };
+        auto pop = [&]() {
+            size_t bi = 0;
+            for (size_t i = 1; i < heap.size(); ++i)
+                if (before(heap[i], heap[bi])) bi = i;
+            HeapEnt e = heap[bi];
+            heap.erase(heap.begin() + bi);
+            return e;
+        };
+        while (n_leaves < cfg_.max_leaves && !heap.empty()) {
+            HeapEnt e = pop();
+            n_leaves += 1;
+            if (!expands(e.c, min_gain)) {
+                make_leaf(e.c);
+                continue;
+            }
+            if (!spec.count(e.c.node)) {
+                // slots: each later pop needs at most one more, so a batch
+                // leaves >= rem free; with rem shrinking by one per pop there
+                // is always room for at least this node
+                const uint32_t rem = cfg_.max_leaves - n_leaves;  // pops that may follow
+                const int64_t room = (int64_t)max_pnodes_ - (int64_t)n_pnodes_ - (int64_t)rem;
+                if (room < 1) throw Error{BST_ERR_OUT_OF_MEMORY, "leaf-wise growth ran out of histogram slots"};
+                const uint64_t batch = std::min<uint64_t>((uint64_t)rem + 1, (uint64_t)room);
+                std::vector<HeapEnt> more;
+                for (const HeapEnt& h : heap)
+                    if (expands(h.c, min_gain) && !spec.count(h.c.node)) more.push_back(h);
+                const size_t extra = std::min<size_t>(more.size(), (size_t)batch - 1);
+                std::partial_sort(more.begin(), more.begin() + extra, more.end(), before);
+                std::vector<Cand> par{e.c}, kids;
+                for (size_t i = 0; i < extra; ++i) par.push_back(more[i].c);
+                std::vector<std::pair<uint32_t, uint32_t>> tch(par.size(), {0xFFFFFFFFu, 0xFFFFFFFFu});
+                std::vector<uint32_t> rid(par.size());
+                std::vector<PNode> before_split(par.size());
+                for (size_t j = 0; j < par.size(); ++j) {
+                    rid[j] = n_pnodes_++;
+                    before_split[j] = pn_[par[j].node];
+                }
+                expand(par, tch, rid, n_leaves < cfg_.max_leaves, kids);
+                for (size_t j = 0; j < par.size(); ++j)
+                    spec[par[j].node] = Spec{{kids[2 * j], kids[2 * j + 1]}, rid[j], before_split[j].begin,
+                                             before_split[j].count};
+            }
+            auto it = spec.find(e.c.node);
+            Spec sp = it->second;
+            spec.erase(it);
+            const std::pair<uint32_t, uint32_t> tch = apply_split(e.c);
+            sp.kids[0].tree_node = tch.first;
+            sp.kids[1].tree_node = tch.second;
+            heap.push_back({sp.kids[0], e.vid});
+            heap.push_back({sp.kids[1], n_vid++});
+        }
+        while (!heap.empty()) {
+            const HeapEnt e = pop();
+            auto it = spec.find(e.c.node);
+            if (it != spec.end()) {  // expanded but never popped: one leaf over both children's rows
+                pn_[e.c.node] = PNode{it->second.begin, it->second.count};
+                pn_[it->second.right_pnode] = PNode{it->second.begin + it->second.count, 0u};
+                spec.erase(it);
+            }
+            make_leaf(e.c);
+        }
+    }
+
     HostTree grow(uint32_t o) {
         gr_o_ = grad_ref(o);
         gx_o_ = exact_ref(o);
@@ -1344,33 +1445,7 @@ class Trainer {
             }
             for (const Cand& c : cur) make_leaf(c);
         } else {
-            // leaf-wise (expansion.rs:137-166): max-heap by (gain, node id)
-            std::vector<Cand> heap{root};
-            uint32_t n_leaves = 1;
-            auto pop = [&]() {
-                size_t bi = 0;
-                for (size_t i = 1; i < heap.size(); ++i) {
-                    const float a = heap[i].split.gain, b = heap[bi].split.gain;
-                    if (a > b || (a == b && heap[i].node > heap[bi].node)) bi = i;
-                }
-                Cand c = heap[bi];
-                heap.erase(heap.begin() + bi);
-                return c;
-            };
-            while (n_leaves < cfg_.max_leaves && !heap.empty()) {
-                Cand c = pop();
-                n_leaves += 1;
-                if (!expands(c, min_gain)) {
-                    make_leaf(c);
-                    continue;
-                }
-                std::vector<Cand> par{c}, kids;
-                std::vector<std::pair<uint32_t, uint32_t>> tch{apply_split(c)};
-                std::vector<uint32_t> rid{n_pnodes_++};
-                expand(par, tch, rid, n_leaves < cfg_.max_leaves, kids);
-                for (auto& k : kids) heap.push_back(k);
-            }
-            while (!heap.empty()) make_leaf(pop());
+            grow_leafwise(root, min_gain);
         }
         if (qmode_ != GRAD_F32) exact_leaves(o);
         freeze_categories();

@@ -1193,9 +1193,10 @@ constexpr int SORT_N = 256;  // categorical columns with <= 256 bins
 
 // One warp: best split of column `col` of node `node` (the node's histogram
 // lives in slot nd.slot); writes cand[node * n_cols + col] and, for column 0,
-// the node totals. key / cat: this warp's SORT_N-entry shared scratch.
+// the node totals, and returns the candidate's gain (-inf: none) to every
+// lane. key / cat: this warp's SORT_N-entry shared scratch.
 template <typename HB>
-__device__ void scan_item(const ScanNode nd, uint32_t node, uint32_t col, const ScanColumn* __restrict__ cols,
+__device__ float scan_item(const ScanNode nd, uint32_t node, uint32_t col, const ScanColumn* __restrict__ cols,
                           uint32_t n_cols, const HB* __restrict__ hist, uint64_t slot_bins,
                           const double* __restrict__ scale, const GainParamsDev& gp, ColCand* __restrict__ cand,
                           long long* __restrict__ node_tot, double* key, uint32_t* cat) {
@@ -1280,7 +1281,7 @@ __device__ void scan_item(const ScanNode nd, uint32_t node, uint32_t col, const 
             out->flags = best.flags;
             out->cats[0] = out->cats[1] = out->cats[2] = out->cats[3] = 0ull;
         }
-        return;
+        return best.gain;
     }
 
     // categorical (find.rs:426-573)
@@ -1390,6 +1391,7 @@ __device__ void scan_item(const ScanNode nd, uint32_t node, uint32_t col, const 
         out->flags = best.gain > -INFINITY ? best.flags : 0u;
         for (int q = 0; q < 4; ++q) out->cats[q] = cats[q];
     }
+    return best.gain;
 }
 
 template <typename HB>
@@ -2196,104 +2198,81 @@ void launch_b_hist(const BDev& d, const HistTile* tiles, uint32_t n_tiles, uint3
 }
 
 
+// Orderable key of a column's candidate for the per-node atomicMax: larger
+// gain first, then the column the reduction over columns (find.rs:180-270)
+// keeps on a tie (the first, or the last when last_wins). 0: no candidate.
+__device__ __forceinline__ unsigned long long cand_key(float g, uint32_t col, int last_wins) {
+    if (g == 0.0f) g = 0.0f;  // -0 and +0 are the same gain
+    uint32_t u = __float_as_uint(g);
+    u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return ((unsigned long long)u << 32) | (last_wins ? col : ~col);
+}
+
+// Split finding of every node of the level (two children per expanding
+// node) and the reduction over columns: each (node, column) warp posts its
+// candidate's key to d.node_key[node]; the last block turns the winners into
+// frontier b's splits (the winner's full candidate from cand), resets the
+// keys, and derives the next level's decisions (rows in buffer buf).
 template <typename HB>
 __global__ void __launch_bounds__(SCAN_WARPS * 32)
 k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HB* __restrict__ hist,
          uint64_t slot_bins, const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
-         long long* __restrict__ node_tot) {
+         long long* __restrict__ node_tot, int b, int last_wins, LeafParams lp, uint32_t buf) {
     __shared__ double s_key[SCAN_WARPS][SORT_N];
     __shared__ uint32_t s_cat[SCAN_WARPS][SORT_N];
-    const int warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t n_nodes = 2 * d.state->n_exp;
     const uint32_t col_blocks = (n_cols + SCAN_WARPS - 1) / SCAN_WARPS;
-    const uint64_t items = (uint64_t)2 * d.state->n_exp * col_blocks;
+    const uint64_t items = (uint64_t)n_nodes * col_blocks;
     for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
         const uint32_t node = (uint32_t)(it / col_blocks);
         const uint32_t col = (uint32_t)(it % col_blocks) * SCAN_WARPS + warp;
-        if (col < n_cols)
-            scan_item(d.scan_nodes[node], node, col, cols, n_cols, hist, slot_bins, scale, gp, cand, node_tot,
-                      s_key[warp], s_cat[warp]);
+        if (col < n_cols) {
+            const float g = scan_item(d.scan_nodes[node], node, col, cols, n_cols, hist, slot_bins, scale, gp, cand,
+                                      node_tot, s_key[warp], s_cat[warp]);
+            if (lane == 0 && g > -INFINITY) atomicMax(&d.node_key[node], cand_key(g, col, last_wins));
+        }
     }
+    if (!last_block(d.state)) return;
+    BNode* B = d.front[b];
+    for (uint32_t node = threadIdx.x; node < n_nodes; node += blockDim.x) {
+        const unsigned long long key = d.node_key[node];
+        d.node_key[node] = 0ull;
+        NodeSplit sp;
+        sp.tot_g = node_tot[2 * node];
+        sp.tot_h = node_tot[2 * node + 1];
+        if (key == 0ull) {
+            sp.gain = -INFINITY;
+            sp.col = 0;
+            sp.bin = 0;
+            sp.flags = 0;
+            sp.cats[0] = sp.cats[1] = sp.cats[2] = sp.cats[3] = 0ull;
+        } else {
+            const uint32_t col = last_wins ? (uint32_t)key : ~(uint32_t)key;
+            const ColCand& w = cand[(size_t)node * n_cols + col];
+            sp.gain = w.gain;
+            sp.col = col;
+            sp.bin = w.bin;
+            sp.flags = (w.flags & 3u) | 4u;
+            for (int q = 0; q < 4; ++q) sp.cats[q] = w.cats[q];
+        }
+        B[node].split = sp;
+        B[node].G = sp.tot_g;
+        B[node].H = sp.tot_h;
+    }
+    __syncthreads();
+    decide_body(d, b, lp, scale, buf);
 }
 
 void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const void* hist, uint64_t slot_bins,
-                   const double* scale, GainParamsDev gp, ColCand* cand, long long* node_tot, uint32_t grid,
-                   cudaStream_t st, int hist32) {
-    if (n_cols == 0) return;
+                   const double* scale, GainParamsDev gp, ColCand* cand, long long* node_tot, int b, int last_wins,
+                   LeafParams lp, uint32_t buf, uint32_t grid, cudaStream_t st, int hist32) {
     if (hist32)
         k_b_scan<HBin32><<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, static_cast<const HBin32*>(hist), slot_bins,
-                                                           scale, gp, cand, node_tot);
+                                                           scale, gp, cand, node_tot, b, last_wins, lp, buf);
     else
         k_b_scan<HBin><<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, static_cast<const HBin*>(hist), slot_bins,
-                                                         scale, gp, cand, node_tot);
-}
-
-// Reduction over columns (find.rs:180-270) straight into the next frontier.
-__global__ void k_b_reduce(BDev d, int b, const ColCand* __restrict__ cand, const long long* __restrict__ node_tot,
-                           uint32_t n_cols, int last_wins, int decide, LeafParams lp,
-                           const double* __restrict__ scale, uint32_t buf) {
-    const uint32_t n_nodes = 2 * d.state->n_exp;
-    BNode* B = d.front[b];
-    const int lane = threadIdx.x;
-    for (uint32_t node = blockIdx.x; node < n_nodes; node += gridDim.x) {
-        float bg = -INFINITY;
-        uint32_t bc = 0xFFFFFFFFu;
-        const ColCand* c = cand + (size_t)node * n_cols;
-        for (uint32_t i = lane; i < n_cols; i += 32) {
-            const float g = c[i].gain;
-            if (!(g > -INFINITY)) continue;
-            if (bc == 0xFFFFFFFFu || g > bg || (last_wins && g == bg)) {
-                bg = g;
-                bc = i;
-            }
-        }
-        for (int off = 16; off > 0; off >>= 1) {
-            const float og = __shfl_xor_sync(FULL, bg, off);
-            const uint32_t oc = __shfl_xor_sync(FULL, bc, off);
-            bool take;
-            if (oc == 0xFFFFFFFFu)
-                take = false;
-            else if (bc == 0xFFFFFFFFu)
-                take = true;
-            else if (og != bg)
-                take = og > bg;
-            else
-                take = last_wins ? oc > bc : oc < bc;
-            if (take) {
-                bg = og;
-                bc = oc;
-            }
-        }
-        if (lane == 0) {
-            NodeSplit s;
-            s.tot_g = node_tot[2 * node];
-            s.tot_h = node_tot[2 * node + 1];
-            if (bc == 0xFFFFFFFFu) {
-                s.gain = -INFINITY;
-                s.col = 0;
-                s.bin = 0;
-                s.flags = 0;
-                s.cats[0] = s.cats[1] = s.cats[2] = s.cats[3] = 0ull;
-            } else {
-                const ColCand& w = c[bc];
-                s.gain = w.gain;
-                s.col = bc;
-                s.bin = w.bin;
-                s.flags = (w.flags & 3u) | 4u;
-                for (int q = 0; q < 4; ++q) s.cats[q] = w.cats[q];
-            }
-            B[node].split = s;
-            B[node].G = s.tot_g;
-            B[node].H = s.tot_h;
-        }
-    }
-    // the next level's decisions once every node of the frontier is final
-    if (decide && last_block(d.state)) decide_body(d, b, lp, scale, buf);
-}
-
-void launch_b_reduce(const BDev& d, int b, const ColCand* cand, const long long* node_tot, uint32_t n_cols,
-                     int last_wins, int decide, LeafParams lp, const double* scale, uint32_t buf, uint32_t grid,
-                     cudaStream_t st) {
-    k_b_reduce<<<grid, 32, 0, st>>>(d, b, cand, node_tot, n_cols, last_wins, decide, lp, scale, buf);
+                                                         scale, gp, cand, node_tot, b, last_wins, lp, buf);
 }
 
 // Node sums of the smaller children when the children are not split further.

@@ -283,6 +283,7 @@ struct BDev {  // device buffers of the level loop
     uint32_t max_front, max_tnodes;
     uint32_t hist_target;   // desired histogram row segments per level
     uint32_t hist_seg_max;  // largest row segment (lane_segment_max)
+    unsigned long long* node_key;  // [max_front] best candidate key per node; zero between levels
 };
 constexpr uint32_t B_PART_CHUNK = 2048;
 constexpr uint32_t B_LEAF_CHUNK = 4096;
@@ -335,14 +336,13 @@ void launch_b_merge(const BDev& d, void* hist, uint64_t slot_bins, uint32_t tota
                     int root, int mode, cudaStream_t st, int hist32 = 0);
 // Level state of the root histogram: all n rows as one segment list.
 void launch_b_root_hist(const BDev& d, uint64_t n, uint32_t chunk, cudaStream_t st);
+// split finding of the level's nodes and the reduction over columns into
+// frontier b, then (last block) the decisions of the next level, whose rows
+// are in buffer buf
 void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const void* hist,
                    uint64_t slot_bins, const double* scale, GainParamsDev gp, ColCand* cand,
-                   long long* node_tot, uint32_t grid, cudaStream_t st, int hist32 = 0);
-// column reduction into frontier b; decide != 0: then (last block) the
-// decisions of the next level, whose rows are in buffer buf
-void launch_b_reduce(const BDev& d, int b, const ColCand* cand, const long long* node_tot, uint32_t n_cols,
-                     int last_wins, int decide, LeafParams lp, const double* scale, uint32_t buf, uint32_t grid,
-                     cudaStream_t st);
+                   long long* node_tot, int b, int last_wins, LeafParams lp, uint32_t buf, uint32_t grid,
+                   cudaStream_t st, int hist32 = 0);
 void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, uint32_t grid, cudaStream_t st);
 void launch_b_children_sums(const BDev& d, int b, cudaStream_t st);
 void launch_b_finalize(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st);
