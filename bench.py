@@ -165,8 +165,9 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+PLAIN = dict(precision="fp32", batched=False)  # the reference's control flow on the GPU
 FORMS = [  # (name, GBDTConfig overrides); "plain" is the reference form on the GPU
-    ("plain", dict(precision="fp32", batched=False)),
+    ("plain", PLAIN),
     ("batched_fp32", dict(precision="fp32", batched=True)),
     ("batched_q16", dict(precision="q16", batched=True)),
     ("batched_q8", dict(precision="q8", batched=True)),
@@ -434,8 +435,8 @@ def time_trees(bst, torch, ds, cfg, warm, steps):
 def run_configs(bst, torch):
     """The survey's other workloads, each in its plain form and its fast form
     at equal loss: config 1 (5k x 100 regression), config 3 (10M x 200
-    leaf-wise 255 leaves, Q8 vs FP32), config 4 (2M x 50 softmax with 10
-    categorical columns, 10 classes)."""
+    leaf-wise 255 leaves; plain, batched FP32 and batched Q8), config 4 (2M x
+    50 softmax with 10 categorical columns, 10 classes)."""
     out = {}
     # config 1
     x, y = bst.synth.regression(5_000, 100, 20, seed=1)
@@ -443,7 +444,7 @@ def run_configs(bst, torch):
     ds = bst.Dataset.from_feature_major(x, y)
     kw = dict(n_estimators=50, max_depth=6, learning_rate=0.1, metric=bst.Metric.none())
     c1 = {}
-    for form, over in (("plain", {}), ("batched_q8", dict(precision="q8", batched=True))):
+    for form, over in (("plain", dict(PLAIN)), ("batched_q8", dict(precision="q8", batched=True))):
         v, m = time_trees(bst, torch, ds, bst.GBDTConfig(**kw, **over), 5, 40)
         pv = m.predict_group_major(bst.Dataset.from_feature_major(xv))
         c1[form] = {"s_per_100_trees": round(v, 5), "heldout_rmse": round(bst.metric("rmse", pv, yv), 6)}
@@ -456,13 +457,14 @@ def run_configs(bst, torch):
     kw = dict(objective=bst.Objective.logistic(), n_estimators=40, learning_rate=0.1,
               growth_strategy=bst.GrowthStrategy.Leafwise, n_leaves=255, metric=bst.Metric.none())
     c3 = {}
-    for form, over in (("plain_fp32", {}), ("q8", dict(precision="q8"))):
+    for form, over in (("plain", dict(PLAIN)), ("batched_fp32", dict(precision="fp32", batched=True)),
+                       ("batched_q8", dict(precision="q8", batched=True))):
         v, m = time_trees(bst, torch, ds, bst.GBDTConfig(**kw, **over), 3, 30)
         pv = m.predict_group_major(bst.Dataset.from_feature_major(xv))
         c3[form] = {"s_per_100_trees": round(v, 4), "heldout_logloss": round(bst.metric("logloss", pv, yv), 6),
                     "trees": m.n_trees}
-    c3["loss_rel_q8_vs_fp32"] = round((c3["q8"]["heldout_logloss"] - c3["plain_fp32"]["heldout_logloss"])
-                                      / c3["plain_fp32"]["heldout_logloss"], 6)
+    c3["loss_rel_q8_vs_plain"] = round((c3["batched_q8"]["heldout_logloss"] - c3["plain"]["heldout_logloss"])
+                                       / c3["plain"]["heldout_logloss"], 6)
     out["config3_leafwise255_10Mx200"] = c3
     del ds
     # config 4
@@ -473,7 +475,7 @@ def run_configs(bst, torch):
     kw = dict(objective=bst.Objective.softmax(10), n_estimators=40, max_depth=6, learning_rate=0.1,
               metric=bst.Metric.none())
     c4 = {}
-    for form, over in (("plain", {}), ("batched_q8", dict(precision="q8", batched=True))):
+    for form, over in (("plain", dict(PLAIN)), ("batched_q8", dict(precision="q8", batched=True))):
         v, m = time_trees(bst, torch, ds, bst.GBDTConfig(**kw, **over), 3, 20)
         pv = m.predict_group_major(bst.Dataset.from_feature_major(xv, categorical_features=cats))
         c4[form] = {"s_per_100_trees": round(v, 5), "heldout_mlogloss": round(bst.metric("mlogloss", pv, yv), 6),

@@ -308,8 +308,8 @@ class Trainer {
         last_wins_ = (n_threads != 1) && n_cols_ >= 16;  // find.rs:125-129, utils.rs:152
         leafwise_ = cfg.growth_strategy == BST_GROWTH_LEAFWISE;
         const uint32_t max_leaves = leafwise_ ? cfg.max_leaves : (1u << std::min<uint32_t>(cfg.max_depth, 31));
-        // leaf-wise: room for speculative expansions (grow_leafwise)
-        max_pnodes_ = std::max<uint32_t>(1, leafwise_ ? 2 * max_leaves : max_leaves);
+        // batched leaf-wise: room for speculative expansions (grow_leafwise)
+        max_pnodes_ = std::max<uint32_t>(1, leafwise_ && cfg.batched ? 2 * max_leaves : max_leaves);
         timer_.st = st;
         timer_.enabled = cfg.phase_timings != 0;
         gp_.lambda = (double)cfg.lambda;
@@ -576,8 +576,9 @@ class Trainer {
         stage_.reserve(max_chunks * 48 + (size_t)(max_pnodes_ + 4) * 256 + (1 << 20));
         if (n_cols_) setup_hist_state();
         use_batched_ = cfg_.batched && !leafwise_ && n_cols_ > 0 && cfg_.max_depth <= 14;
-        if (use_batched_) {
-            setup_batched();
+        spec_leafwise_ = cfg_.batched && leafwise_ && n_cols_ > 0;
+        if (use_batched_ || spec_leafwise_) {
+            if (use_batched_) setup_batched();
             for (auto& q : qpos_) q.alloc((size_t)n_ * grad_bytes());
             if (p_.s8) fm8_.alloc((size_t)n_ * p_.s8);
             if (p_.s16) fm16_.alloc((size_t)n_ * p_.s16);
@@ -589,6 +590,10 @@ class Trainer {
 
     // ---- device-side level loop, one CUDA graph per output (kernels.h) -------
     bool use_batched_ = false;
+    // batched leaf-wise: speculative expansion batches, gradient elements
+    // carried positionally in qpos_[0] (aligned with ridx_), split columns
+    // read from the column-major bins
+    bool spec_leafwise_ = false;
     BDev bd_{};
     DevArray<BState> d_bstate_;
     DevArray<BNode> d_front_[2];
@@ -1170,9 +1175,16 @@ class Trainer {
         std::copy(pch.begin(), pch.end(), hpc);
         upload(hpc, pch.size(), d_pchunks_);
         timer_.begin(PH_PART);
-        launch_partition(d_pworks_.p, d_pchunks_.p, (uint32_t)pch.size(), ridx_.p, tmp_.p, d_cursors_.p, b_.bins8.p,
-                         p_.s8, b_.bins16.p, p_.s16, st_);
-        launch_copy_chunks(d_pchunks_.p, d_pworks_.p, (uint32_t)pch.size(), tmp_.p, ridx_.p, st_);
+        if (spec_leafwise_) {
+            launch_partition(d_pworks_.p, d_pchunks_.p, (uint32_t)pch.size(), ridx_.p, tmp_.p, d_cursors_.p,
+                             b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, st_, qpos_[0].p, qpos_[1].p, qmode_, fm_);
+            launch_copy_chunks(d_pchunks_.p, d_pworks_.p, (uint32_t)pch.size(), tmp_.p, ridx_.p, st_, qpos_[1].p,
+                               qpos_[0].p, qmode_);
+        } else {
+            launch_partition(d_pworks_.p, d_pchunks_.p, (uint32_t)pch.size(), ridx_.p, tmp_.p, d_cursors_.p,
+                             b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, st_);
+            launch_copy_chunks(d_pchunks_.p, d_pworks_.p, (uint32_t)pch.size(), tmp_.p, ridx_.p, st_);
+        }
         timer_.end();
         m_.counters.launches += pch.empty() ? 0 : 2;
         m_.counters.partition_rows += prow;
@@ -1280,10 +1292,11 @@ class Trainer {
     // Leaf-wise growth (expansion.rs:137-166): pop the leaf of largest
     // (gain, node id), split it, push its children, until max_leaves.
     //
-    // The pops are replayed here exactly, but the device expands nodes in
-    // batches: when the popped node has not been expanded yet, it is
-    // expanded together with the best other unexpanded candidates of the
-    // heap (at most as many as pops remain). A node's rows, histogram and
+    // The pops are replayed here exactly. Plain form: the device expands
+    // each popped node on its own (the reference's order of work). Batched
+    // form: when the popped node has not been expanded yet, it is expanded
+    // together with the best other unexpanded candidates of the heap (at
+    // most as many as pops remain). A node's rows, histogram and
     // split do not depend on when it is expanded, so a node that the replay
     // pops later costs no device step, and one it never pops is rolled back
     // into a leaf over its full row range. Node ids of the replay (the tie
@@ -1328,7 +1341,7 @@ class Trainer {
                 const uint32_t rem = cfg_.max_leaves - n_leaves;  // pops that may follow
                 const int64_t room = (int64_t)max_pnodes_ - (int64_t)n_pnodes_ - (int64_t)rem;
                 if (room < 1) throw Error{BST_ERR_OUT_OF_MEMORY, "leaf-wise growth ran out of histogram slots"};
-                const uint64_t batch = std::min<uint64_t>((uint64_t)rem + 1, (uint64_t)room);
+                const uint64_t batch = spec_leafwise_ ? std::min<uint64_t>((uint64_t)rem + 1, (uint64_t)room) : 1u;
                 std::vector<HeapEnt> more;
                 for (const HeapEnt& h : heap)
                     if (expands(h.c, min_gain) && !spec.count(h.c.node)) more.push_back(h);
@@ -1371,6 +1384,7 @@ class Trainer {
 
     HostTree grow(uint32_t o) {
         gr_o_ = grad_ref(o);
+        if (spec_leafwise_) gr_o_.qpos = qpos_[0].p;  // histograms read the positional copy
         gx_o_ = exact_ref(o);
         scale_o_ = unit_scale(o);
         const std::vector<double>& hs = qmode_ == GRAD_F32 ? h_scales_ : h_qscales_;
@@ -1386,6 +1400,9 @@ class Trainer {
         stage_.reset();
         timer_.begin(PH_OTHER);
         launch_iota(ridx_.p, n_, st_);
+        if (spec_leafwise_)  // identity order: the positional copy is the row-order array
+            BST_CK(cudaMemcpyAsync(qpos_[0].p, qmode_ == GRAD_F32 ? (const void*)gr_o_.gh : gr_o_.gq,
+                                   (size_t)n_ * grad_bytes(), cudaMemcpyDeviceToDevice, st_));
         timer_.end();
         m_.counters.launches += 1;
         tree_.alloc();  // root (mutable_tree.rs:80 init_root)

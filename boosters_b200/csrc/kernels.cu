@@ -1609,36 +1609,68 @@ __device__ void part_rows(const PartWork& w, uint32_t start, uint32_t len, unsig
 
 }  // namespace
 
+template <typename Q>
 __global__ void __launch_bounds__(PART_THREADS)
 k_partition(const PartWork* __restrict__ works, const PartChunk* __restrict__ chunks,
             const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp, unsigned* __restrict__ cursors,
-            const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16) {
+            const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16,
+            const Q* __restrict__ qin, Q* __restrict__ qout, BinsFM fm) {
     const PartChunk ch = chunks[blockIdx.x];
     __shared__ PartWork w;
     if (threadIdx.x == 0) w = works[ch.work];
     __syncthreads();
-    part_rows(w, ch.start, ch.len, cursors + 2 * ch.work, ridx, tmp, bins8, s8, bins16, s16);
+    part_rows<Q>(w, ch.start, ch.len, cursors + 2 * ch.work, ridx, tmp, bins8, s8, bins16, s16, qin, qout, fm.b8,
+                 fm.b16, fm.n);
 }
 
 void launch_partition(const PartWork* works, const PartChunk* chunks, uint32_t n_chunks,
                       const uint32_t* ridx, uint32_t* tmp, unsigned* cursors,
                       const uint8_t* bins8, uint32_t s8, const uint16_t* bins16, uint32_t s16,
-                      cudaStream_t st) {
+                      cudaStream_t st, const void* qin, void* qout, int mode, const BinsFM& fm) {
     if (n_chunks == 0) return;
-    k_partition<<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16, s16);
+    if (!qin || !qout)
+        k_partition<char><<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
+                                                             s16, nullptr, nullptr, fm);
+    else if (mode == GRAD_Q8)
+        k_partition<char2><<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
+                                                              s16, static_cast<const char2*>(qin),
+                                                              static_cast<char2*>(qout), fm);
+    else if (mode == GRAD_Q16)
+        k_partition<short2><<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
+                                                               s16, static_cast<const short2*>(qin),
+                                                               static_cast<short2*>(qout), fm);
+    else
+        k_partition<float2><<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
+                                                               s16, static_cast<const float2*>(qin),
+                                                               static_cast<float2*>(qout), fm);
 }
 
+template <typename Q>
 __global__ void k_copy_chunks(const PartChunk* __restrict__ chunks, const uint32_t* __restrict__ src,
-                              uint32_t* __restrict__ dst) {
+                              uint32_t* __restrict__ dst, const Q* __restrict__ qsrc, Q* __restrict__ qdst) {
     const PartChunk ch = chunks[blockIdx.x];
-    for (uint32_t i = threadIdx.x; i < ch.len; i += blockDim.x) dst[ch.start + i] = src[ch.start + i];
+    for (uint32_t i = threadIdx.x; i < ch.len; i += blockDim.x) {
+        dst[ch.start + i] = src[ch.start + i];
+        if (qsrc) qdst[ch.start + i] = qsrc[ch.start + i];
+    }
 }
 
 void launch_copy_chunks(const PartChunk* chunks, const PartWork* works, uint32_t n_chunks,
-                        const uint32_t* src, uint32_t* dst, cudaStream_t st) {
+                        const uint32_t* src, uint32_t* dst, cudaStream_t st, const void* qsrc, void* qdst,
+                        int mode) {
     (void)works;
     if (n_chunks == 0) return;
-    k_copy_chunks<<<n_chunks, 256, 0, st>>>(chunks, src, dst);
+    if (!qsrc || !qdst)
+        k_copy_chunks<char><<<n_chunks, 256, 0, st>>>(chunks, src, dst, nullptr, nullptr);
+    else if (mode == GRAD_Q8)
+        k_copy_chunks<char2><<<n_chunks, 256, 0, st>>>(chunks, src, dst, static_cast<const char2*>(qsrc),
+                                                       static_cast<char2*>(qdst));
+    else if (mode == GRAD_Q16)
+        k_copy_chunks<short2><<<n_chunks, 256, 0, st>>>(chunks, src, dst, static_cast<const short2*>(qsrc),
+                                                        static_cast<short2*>(qdst));
+    else
+        k_copy_chunks<float2><<<n_chunks, 256, 0, st>>>(chunks, src, dst, static_cast<const float2*>(qsrc),
+                                                        static_cast<float2*>(qdst));
 }
 
 __global__ void k_iota(uint32_t* __restrict__ r, uint64_t n) {

@@ -200,14 +200,27 @@ struct PartWork {
 struct PartChunk {
     uint32_t work, start, len, pad;
 };
+// Column-major copies of the bin matrices ([column][n]), or null pointers.
+struct BinsFM {
+    const uint8_t* b8 = nullptr;
+    const uint16_t* b16 = nullptr;
+    uint64_t n = 0;
+};
 // cursors [n_work][2]: (left write cursor, right write cursor); initialised by
 // the caller to (begin, begin + count). Rows are scattered into tmp.
+// qin / qout (grad_elem_bytes(mode) each, or null): each row's gradient
+// element moves with its row id (positional copy); fm: the split column is
+// read from the column-major bins when set.
 void launch_partition(const PartWork* works, const PartChunk* chunks, uint32_t n_chunks,
                       const uint32_t* ridx, uint32_t* tmp, unsigned* cursors,
                       const uint8_t* bins8, uint32_t s8, const uint16_t* bins16, uint32_t s16,
-                      cudaStream_t st);
+                      cudaStream_t st, const void* qin = nullptr, void* qout = nullptr, int mode = 0,
+                      const BinsFM& fm = BinsFM{});
+// copies the chunks' row ids src -> dst and, when qsrc is set, their
+// positional gradient elements qsrc -> qdst
 void launch_copy_chunks(const PartChunk* chunks, const PartWork* works, uint32_t n_chunks,
-                        const uint32_t* src, uint32_t* dst, cudaStream_t st);
+                        const uint32_t* src, uint32_t* dst, cudaStream_t st, const void* qsrc = nullptr,
+                        void* qdst = nullptr, int mode = 0);
 void launch_iota(uint32_t* ridx, uint64_t n, cudaStream_t st);
 
 // ---- K8 leaf values -> predictions -----------------------------------------
@@ -299,12 +312,6 @@ void launch_b_root_set(const BDev& d, const NodeSplit* root_split, LeafParams lp
                        cudaStream_t st);
 // level kernels; `a` is the index of the current frontier buffer
 void launch_b_decide(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st);
-// Column-major copies of the bin matrices ([column][n]), or null pointers.
-struct BinsFM {
-    const uint8_t* b8 = nullptr;
-    const uint16_t* b16 = nullptr;
-    uint64_t n = 0;
-};
 void launch_transpose_bins(const uint8_t* b8, uint32_t s8, const uint16_t* b16, uint32_t s16, uint64_t n,
                            uint8_t* fm8, uint16_t* fm16, cudaStream_t st);
 // partition rin -> rout, then (last block) the children of every split;

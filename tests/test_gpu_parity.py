@@ -255,16 +255,18 @@ def test_train_parity_leafwise():
     compare_trees(gm, om, 30_000, sum_rtol=1e-6, sum_atol=1e-6)
 
 
-@pytest.mark.parametrize("n_leaves,precision", [(2, "fp32"), (5, "fp32"), (17, "fp32"), (255, "fp32"), (17, "q8")])
-def test_train_parity_leafwise_budgets(n_leaves, precision):
-    """Leaf-wise growth expands heap candidates in speculative batches and
-    replays the pops; budgets from one split to more leaves than the data
-    supports exercise rolled-back expansions, the last pop and an exhausted
-    heap."""
+@pytest.mark.parametrize("n_leaves,precision,batched", [(2, "fp32", True), (5, "fp32", True), (17, "fp32", True),
+                                                        (255, "fp32", True), (17, "q8", True), (17, "fp32", False),
+                                                        (17, "q8", False)])
+def test_train_parity_leafwise_budgets(n_leaves, precision, batched):
+    """Batched leaf-wise growth expands heap candidates in speculative
+    batches and replays the pops (plain: one node per step); budgets from one
+    split to more leaves than the data supports exercise rolled-back
+    expansions, the last pop and an exhausted heap."""
     x, y = bst.synth.regression(8000, 16, 6, seed=21)
     x[2, ::7] = np.nan
     gm, om, _ = train_both(x, y, n_estimators=4, learning_rate=0.3, growth_strategy=bst.GrowthStrategy.Leafwise,
-                           n_leaves=n_leaves, min_samples_leaf=20, precision=precision)
+                           n_leaves=n_leaves, min_samples_leaf=20, precision=precision, batched=batched)
     compare_trees(gm, om, 8000, sum_rtol=1e-9 if precision == "fp32" else 1e-6,
                   sum_atol=1e-9 if precision == "fp32" else 1e-6)
 
