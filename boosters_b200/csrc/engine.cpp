@@ -798,7 +798,7 @@ class Trainer {
             // gradient elements move with the row ids: level 0 reads them in
             // row order (the unpermuted arrays), later levels ping-pong
             const void* qin = d == 0 ? (qmode_ == GRAD_F32 ? (const void*)gh.gh : gh.gq) : (const void*)qpos_[d & 1u].p;
-            void* qout = need_split ? (void*)qpos_[(d + 1) & 1u].p : nullptr;
+            void* qout = qpos_[(d + 1) & 1u].p;  // the last level's node sums read it too
             tm.begin(PH_PART);
             launch_b_partition(bd_, R[d & 1u], rout, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, a, need_split ? 1 : 0,
                                g_wide, qin, qout, qmode_, fm_, st_);  // + children
@@ -823,7 +823,9 @@ class Trainer {
             } else {
                 tm.begin(PH_OTHER);
                 BST_CK(cudaMemsetAsync(d_sums_.p, 0, sizeof(long long) * d_sums_.n, st_));
-                launch_b_sums(bd_, rout, gh, g_wide, st_);
+                GradRef gl = gh;
+                gl.qpos = qpos_[(d + 1) & 1u].p;
+                launch_b_sums(bd_, rout, gl, g_wide, st_);
                 launch_b_children_sums(bd_, a ^ 1, st_);
                 tm.end();
                 launches += 2;

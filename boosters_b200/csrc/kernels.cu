@@ -2307,6 +2307,33 @@ void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const
                                                          scale, gp, cand, node_tot, b, last_wins, lp, buf);
 }
 
+// This thread's share of the fixed-point sums of positions [start, start +
+// len) of a row-id buffer: RANGE_ILP positions per step, all row ids loaded
+// before any gradient element, so the dependent gathers overlap.
+constexpr uint32_t RANGE_ILP = 8;
+template <int MODE>
+__device__ __forceinline__ void range_sums(uint32_t start, uint32_t len, const uint32_t* __restrict__ ridx,
+                                           const GradLoad<MODE>& load, long long& ag, long long& ah) {
+    for (uint32_t i0 = threadIdx.x; i0 < len; i0 += blockDim.x * RANGE_ILP) {
+        uint32_t rows[RANGE_ILP];
+#pragma unroll
+        for (uint32_t u = 0; u < RANGE_ILP; ++u) {
+            const uint32_t i = i0 + u * blockDim.x;
+            rows[u] = i < len ? ridx[start + i] : 0u;
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < RANGE_ILP; ++u) {
+            const uint32_t i = i0 + u * blockDim.x;
+            if (i < len) {
+                long long qg, qh;
+                load.at(start + i, rows[u], qg, qh);
+                ag += qg;
+                ah += qh;
+            }
+        }
+    }
+}
+
 // Node sums of the smaller children when the children are not split further.
 template <int MODE>
 __global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, GradRef gr) {
@@ -2318,12 +2345,7 @@ __global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, GradRef gr) 
         const uint32_t start = e.small_begin + (c - e.hist_off) * CH;
         const uint32_t len = min(CH, e.small_begin + e.small_count - start);
         long long ag = 0, ah = 0;
-        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
-            long long qg, qh;
-            load(ridx[start + i], qg, qh);
-            ag += qg;
-            ah += qh;
-        }
+        range_sums(start, len, ridx, load, ag, ah);
         for (int o = 16; o > 0; o >>= 1) {
             ag += __shfl_xor_sync(FULL, ag, o);
             ah += __shfl_xor_sync(FULL, ah, o);
@@ -2424,12 +2446,7 @@ __global__ void k_b_leaf_sums(BDev d, const uint32_t* __restrict__ r0, const uin
         const uint32_t len = min(B_LEAF_CHUNK, lf.begin + lf.count - start);
         const uint32_t* ridx = lf.buf ? r1 : r0;
         long long ag = 0, ah = 0;
-        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
-            long long qg, qh;
-            load(ridx[start + i], qg, qh);
-            ag += qg;
-            ah += qh;
-        }
+        range_sums(start, len, ridx, load, ag, ah);
         for (int o = 16; o > 0; o >>= 1) {
             ag += __shfl_xor_sync(FULL, ag, o);
             ah += __shfl_xor_sync(FULL, ah, o);
@@ -2470,10 +2487,25 @@ __global__ void k_b_leaf_update(BDev d, const uint32_t* __restrict__ r0, const u
         const uint32_t start = lf.begin + (c - lf.chunk_off) * B_LEAF_CHUNK;
         const uint32_t len = min(B_LEAF_CHUNK, lf.begin + lf.count - start);
         const uint32_t* ridx = lf.buf ? r1 : r0;
-        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
-            const uint32_t row = ridx[start + i];
-            pred[row] = pred[row] + lf.value;
-            if (row_leaf) row_leaf[row] = lf.tnode;
+        // RANGE_ILP rows per step: row ids, then predictions, then stores
+        // (a leaf's rows are distinct, so the steps do not alias)
+        for (uint32_t i0 = threadIdx.x; i0 < len; i0 += blockDim.x * RANGE_ILP) {
+            uint32_t rows[RANGE_ILP];
+            float pv[RANGE_ILP];
+#pragma unroll
+            for (uint32_t u = 0; u < RANGE_ILP; ++u) {
+                const uint32_t i = i0 + u * blockDim.x;
+                rows[u] = i < len ? ridx[start + i] : 0u;
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < RANGE_ILP; ++u)
+                pv[u] = i0 + u * blockDim.x < len ? pred[rows[u]] : 0.0f;
+#pragma unroll
+            for (uint32_t u = 0; u < RANGE_ILP; ++u)
+                if (i0 + u * blockDim.x < len) {
+                    pred[rows[u]] = pv[u] + lf.value;
+                    if (row_leaf) row_leaf[rows[u]] = lf.tnode;
+                }
         }
     }
 }
