@@ -1319,16 +1319,21 @@ __device__ float scan_item(const ScanNode nd, uint32_t node, uint32_t col, const
             }
             m += __popc(bal);
         }
-        for (uint32_t i = m + lane; i < SORT_N; i += 32) {
+        // bitonic network over the next power of two >= m entries (the
+        // (key, category) order is total, so the sorted prefix is the same
+        // for any padded size)
+        uint32_t sn = 2;
+        while (sn < m) sn <<= 1;
+        for (uint32_t i = m + lane; i < sn; i += 32) {
             key[i] = INFINITY;
             cat[i] = 0xFFFFFFFFu;
         }
         __syncwarp();
         if (m >= 2) {
-            // bitonic sort of (key, cat) over SORT_N entries
-            for (uint32_t k = 2; k <= SORT_N; k <<= 1) {
+            // bitonic sort of (key, cat) over sn entries
+            for (uint32_t k = 2; k <= sn; k <<= 1) {
                 for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-                    for (uint32_t i = lane; i < SORT_N; i += 32) {
+                    for (uint32_t i = lane; i < sn; i += 32) {
                         const uint32_t ixj = i ^ j;
                         if (ixj > i) {
                             const bool up = (i & k) == 0;
