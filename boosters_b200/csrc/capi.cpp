@@ -84,8 +84,6 @@ bst_status check_config(const bst_config* c, bool for_training) {
     if (c->objective == BST_OBJ_SOFTMAX && c->n_classes < 2) return fail(BST_ERR_CONFIG, "softmax needs n_classes >= 2");
     if (c->subsample != 1.0f || c->colsample_bytree != 1.0f || c->colsample_bylevel != 1.0f)
         return fail(BST_ERR_UNSUPPORTED, "row/column subsampling is not supported by the GPU engine");
-    if (c->early_stopping_rounds >= 0)
-        return fail(BST_ERR_UNSUPPORTED, "early stopping is not supported by the GPU engine");
     if (c->growth_strategy != BST_GROWTH_DEPTHWISE && c->growth_strategy != BST_GROWTH_LEAFWISE)
         return fail(BST_ERR_CONFIG, "unknown growth strategy");
     if (c->growth_strategy == BST_GROWTH_DEPTHWISE && c->max_depth > 24)
@@ -257,7 +255,6 @@ bst_status bst_binned_column_bins(const bst_binned* b, uint32_t col, uint16_t* o
 
 bst_status bst_gbdt_train(const bst_dataset* train, const bst_dataset* val, const bst_config* cfg,
                           uint32_t n_threads, bst_model** out) {
-    (void)val;  // only used by metrics / early stopping in the reference
     return guarded([&]() -> bst_status {
         if (!out) return fail(BST_ERR_INVALID_ARGUMENT, "out is NULL");
         *out = nullptr;
@@ -266,7 +263,17 @@ bst_status bst_gbdt_train(const bst_dataset* train, const bst_dataset* val, cons
         if (rc != BST_OK) return rc;
         if (train->d.n == 0) return fail(BST_ERR_EMPTY_DATASET, "dataset is empty");
         if (train->d.y.empty()) return fail(BST_ERR_MISSING_TARGETS, "dataset must have targets for training");
-        auto m = bst::train_model(train->d, *cfg, n_threads);
+        // the validation set is read only by early stopping's evaluation
+        // (trainer.rs:211-216: predictions only when a metric is set)
+        const bool evaluates = cfg->early_stopping_rounds > 0 &&
+                               bst::resolve_metric(cfg->metric, cfg->objective) != BST_METRIC_NONE && val;
+        if (evaluates) {
+            if (val->d.y.empty())  // eval.rs:242 ("validation set must have targets")
+                return fail(BST_ERR_MISSING_TARGETS, "validation set must have targets");
+            if (val->d.F < train->d.F)
+                return fail(BST_ERR_INVALID_ARGUMENT, "validation set has fewer features than the training set");
+        }
+        auto m = bst::train_model(train->d, *cfg, n_threads, evaluates ? &val->d : nullptr);
         *out = new bst_model{std::move(m)};
         return BST_OK;
     });
@@ -481,6 +488,8 @@ bst_status bst_booster_create(const bst_dataset* train, const bst_config* cfg, u
         *out = nullptr;
         bst_status rc = check_config(cfg, true);
         if (rc != BST_OK) return rc;
+        if (cfg->early_stopping_rounds > 0)
+            return fail(BST_ERR_UNSUPPORTED, "early stopping needs bst_gbdt_train (the booster has no validation set)");
         if (train->d.n == 0) return fail(BST_ERR_EMPTY_DATASET, "dataset is empty");
         if (train->d.y.empty()) return fail(BST_ERR_MISSING_TARGETS, "dataset must have targets for training");
         *out = new bst_booster{std::make_unique<bst::Booster>(train->d, *cfg, n_threads)};
@@ -980,43 +989,9 @@ bst_status bst_metric(int32_t metric, const float* p, uint32_t G, uint64_t n, co
                       double* out) {
     if (!out || (n && (!p || !y))) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
     *out = 0.0;
-    if (n == 0) return BST_OK;
-    const double EPS = 1e-15;
-    auto wv = [&](uint64_t i) { return w ? (double)w[i] : 1.0; };
-    auto clampd = [](double v, double lo, double hi) { return v < lo ? lo : (v > hi ? hi : v); };
-    if (metric == BST_METRIC_RMSE) {  // metrics/regression.rs:17-45
-        double sum = 0.0;
-        for (uint32_t g = 0; g < G; ++g) {
-            double ss = 0, sw = 0;
-            for (uint64_t i = 0; i < n; ++i) {
-                const double d = (double)p[(uint64_t)g * n + i] - (double)y[i];
-                ss = ss + wv(i) * d * d;
-                sw = sw + wv(i);
-            }
-            sum += sw > 0.0 ? std::sqrt(ss / sw) : 0.0;
-        }
-        *out = sum / (double)G;
-    } else if (metric == BST_METRIC_LOGLOSS) {  // metrics/classification.rs:13-40
-        double sl = 0, sw = 0;
-        for (uint64_t i = 0; i < n; ++i) {
-            const double pp = clampd((double)p[i], EPS, 1.0 - EPS), l = (double)y[i];
-            sl = sl + wv(i) * -(l * std::log(pp) + (1.0 - l) * std::log(1.0 - pp));
-            sw = sw + wv(i);
-        }
-        *out = sw > 0.0 ? sl / sw : 0.0;
-    } else if (metric == BST_METRIC_MLOGLOSS) {  // metrics/classification.rs:332-360
-        double sl = 0, sw = 0;
-        for (uint64_t i = 0; i < n; ++i) {
-            const float r = std::round(y[i]);
-            const uint64_t c = r > 0.0f ? (uint64_t)r : 0;
-            const double pp = clampd(c < G ? (double)p[c * n + i] : EPS, EPS, 1.0 - EPS);
-            sl = sl + wv(i) * -std::log(pp);
-            sw = sw + wv(i);
-        }
-        *out = sw > 0.0 ? sl / sw : 0.0;
-    } else {
+    if (metric != BST_METRIC_RMSE && metric != BST_METRIC_LOGLOSS && metric != BST_METRIC_MLOGLOSS)
         return fail(BST_ERR_INVALID_ARGUMENT, "unknown metric");
-    }
+    *out = bst::metric_value(metric, p, G, n, y, w);
     return BST_OK;
 }
 

@@ -353,10 +353,52 @@ class Trainer {
         return t;
     }
 
-    void run() {
+    void run(const HostDataset* val = nullptr) {
         setup();
-        rounds(cfg_.n_trees);
+        if (cfg_.early_stopping_rounds <= 0) {  // None or Some(0): disabled (config.rs:366)
+            rounds(cfg_.n_trees);
+            m_.rounds_run = cfg_.n_trees;
+            finish();
+            return;
+        }
+        // Early stopping (trainer.rs:344-390, callback.rs:103-136): after
+        // every round, the validation metric (the training metric without a
+        // validation set; NaN with Metric::None) against the best so far;
+        // stop once `patience` rounds passed without improvement and keep the
+        // trees up to the best round. All the engine's metrics are
+        // lower-is-better.
+        const uint32_t patience = (uint32_t)cfg_.early_stopping_rounds;
+        const int metric = resolve_metric(cfg_.metric, cfg_.objective);
+        if (metric != BST_METRIC_NONE && val) setup_validation(*val);
+        bool have_best = false;
+        double best = 0.0;
+        uint32_t best_round = 0, cur = 0;
+        size_t best_n_trees = 0;
+        for (uint32_t r = 0; r < cfg_.n_trees; ++r) {
+            const size_t before = m_.trees.size();
+            rounds(1);
+            m_.rounds_run = r + 1;
+            double value = std::numeric_limits<double>::quiet_NaN();
+            if (metric != BST_METRIC_NONE) value = val ? validation_value(metric, before) : train_value(metric);
+            const bool improved = !have_best || value < best;
+            if (improved) {
+                have_best = true;
+                best = value;
+                best_round = cur;
+            }
+            ++cur;
+            if (cur - best_round > patience) break;  // Stop
+            if (improved) best_n_trees = m_.trees.size();  // Improved
+        }
+        if (have_best) m_.rounds_kept = best_round + 1;
+        const bool truncate = best_n_trees > 0 && best_n_trees < m_.trees.size();
+        if (truncate) {
+            std::lock_guard<std::mutex> lk(m_.mu);
+            m_.trees.resize(best_n_trees);
+            m_.dev.reset();
+        }
         finish();
+        if (truncate) predict_host(m_, ds_, true, m_.train_pred.data());  // the kept trees' predictions
     }
 
     // Boosting rounds (trainer.rs:242-335): gradients of every output, then
@@ -415,6 +457,62 @@ class Trainer {
     void push_tree(HostTree&& t) {
         const uint32_t o = t.group;
         push_tree(std::move(t), o);
+    }
+
+    // ---- early-stopping evaluation -------------------------------------------
+    const HostDataset* val_ = nullptr;
+    DevArray<float> val_x_, val_pred_, eval_tmp_;
+    std::vector<float> eval_host_;
+
+    void setup_validation(const HostDataset& v) {
+        val_ = &v;
+        const uint64_t nv = v.n;
+        val_x_.alloc(std::max<uint64_t>(1, nv * v.F));
+        if (nv * v.F) BST_CK(cudaMemcpy(val_x_.p, v.xdata(), sizeof(float) * nv * v.F, cudaMemcpyHostToDevice));
+        std::vector<float> init((size_t)G_ * nv);
+        for (uint32_t g = 0; g < G_; ++g)
+            std::fill(init.begin() + (size_t)g * nv, init.begin() + (size_t)(g + 1) * nv, m_.base[g]);
+        val_pred_.alloc(std::max<size_t>(1, init.size()));
+        if (!init.empty())
+            BST_CK(cudaMemcpy(val_pred_.p, init.data(), sizeof(float) * init.size(), cudaMemcpyHostToDevice));
+    }
+
+    // Metric of [G][n] raw margins on the device against labels y / weights
+    // w (host): transformed copy (Evaluator::compute, eval.rs:150-185), read
+    // back, summed on the host.
+    double device_metric(int metric, const float* margins, uint64_t n, const float* y, const float* w) {
+        const size_t cnt = (size_t)G_ * n;
+        if (cnt == 0) return 0.0;
+        eval_tmp_.alloc(cnt);
+        BST_CK(cudaMemcpyAsync(eval_tmp_.p, margins, sizeof(float) * cnt, cudaMemcpyDeviceToDevice, st_));
+        if (metric != BST_METRIC_RMSE) launch_transform(transform_of(cfg_.objective), eval_tmp_.p, G_, n, st_);
+        eval_host_.resize(cnt);
+        BST_CK(cudaMemcpyAsync(eval_host_.data(), eval_tmp_.p, sizeof(float) * cnt, cudaMemcpyDeviceToHost, st_));
+        BST_CK(cudaStreamSynchronize(st_));
+        return metric_value(metric, eval_host_.data(), G_, n, y, w);
+    }
+
+    double train_value(int metric) {
+        return device_metric(metric, pred_.p, n_, ds_.y.data(), ds_.has_w ? ds_.w.data() : nullptr);
+    }
+
+    // Adds the trees pushed since `first` (this round's, one per output) to
+    // the validation predictions (tree.predict_into, trainer.rs:339-343),
+    // then the validation metric.
+    double validation_value(int metric, size_t first) {
+        const HostDataset& v = *val_;
+        if (v.n && m_.trees.size() > first) {
+            std::vector<const HostTree*> tp;
+            for (size_t t = first; t < m_.trees.size(); ++t) tp.push_back(&m_.trees[t]);
+            DeviceForest f;
+            upload_node_forest(tp, G_, std::vector<float>(G_, 0.0f), f);
+            eval_tmp_.alloc((size_t)G_ * v.n);
+            launch_predict(f.view, val_x_.p, v.n, (uint32_t)v.F, 1, eval_tmp_.p, st_);
+            launch_add_f32(val_pred_.p, eval_tmp_.p, (uint64_t)G_ * v.n, st_);
+            BST_CK(cudaGetLastError());
+            BST_CK(cudaStreamSynchronize(st_));  // f is freed on return
+        }
+        return device_metric(metric, val_pred_.p, v.n, v.y.data(), v.has_w ? v.w.data() : nullptr);
     }
 
     // Training predictions back to the model.
@@ -1647,7 +1745,8 @@ std::unique_ptr<Model> grow_one_tree(const HostDataset& ds, const float* g, cons
     return model;
 }
 
-std::unique_ptr<Model> train_model(const HostDataset& ds, const bst_config& cfg, uint32_t n_threads) {
+std::unique_ptr<Model> train_model(const HostDataset& ds, const bst_config& cfg, uint32_t n_threads,
+                                   const HostDataset* val) {
     BST_CK(cudaSetDevice(cfg.device));
     StreamGuard sg;
     auto model = std::make_unique<Model>();
@@ -1661,7 +1760,7 @@ std::unique_ptr<Model> train_model(const HostDataset& ds, const bst_config& cfg,
     base_scores(ds, cfg, model->n_groups, model->base);
     const auto t0 = std::chrono::steady_clock::now();
     Trainer tr(ds, binned, cfg, n_threads, sg.s, *model);
-    tr.run();
+    tr.run(val);
     model->timings[7] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return model;
 }
@@ -1723,14 +1822,15 @@ std::unique_ptr<Model> Booster::snapshot() const {
     return m;
 }
 
-const DeviceForest& Model::device_forest() const {
-    std::lock_guard<std::mutex> lk(mu);
-    if (dev) return *dev;
-    BST_CK(cudaSetDevice(device));
-    auto f = std::make_unique<DeviceForest>();
+// Node-list forest of `trees` (forest order) on the device: what
+// launch_predict walks.
+void upload_node_forest(const std::vector<const HostTree*>& trees, uint32_t n_groups, const std::vector<float>& base,
+                        DeviceForest& df) {
+    DeviceForest* f = &df;
     std::vector<ForestNode> nodes;
     std::vector<uint32_t> roots, cat_seg, cat_words, gt, goff(n_groups + 1, 0);
-    for (const HostTree& t : trees) {
+    for (const HostTree* tp : trees) {
+        const HostTree& t = *tp;
         const uint32_t base_idx = (uint32_t)nodes.size();
         const uint32_t wbase = (uint32_t)cat_words.size();
         roots.push_back(base_idx);
@@ -1751,7 +1851,7 @@ const DeviceForest& Model::device_forest() const {
     for (uint32_t g = 0; g < n_groups; ++g) {
         goff[g] = (uint32_t)gt.size();
         for (uint32_t t = 0; t < trees.size(); ++t)
-            if (trees[t].group == g) gt.push_back(t);
+            if (trees[t]->group == g) gt.push_back(t);
     }
     goff[n_groups] = (uint32_t)gt.size();
     auto up = [](auto& dst, const auto& src) {
@@ -1775,6 +1875,17 @@ const DeviceForest& Model::device_forest() const {
     f->view.base = f->base.p;
     f->view.n_trees = (uint32_t)trees.size();
     f->view.n_groups = n_groups;
+}
+
+const DeviceForest& Model::device_forest() const {
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev) return *dev;
+    BST_CK(cudaSetDevice(device));
+    auto f = std::make_unique<DeviceForest>();
+    std::vector<const HostTree*> tp;
+    tp.reserve(trees.size());
+    for (const HostTree& t : trees) tp.push_back(&t);
+    upload_node_forest(tp, n_groups, base, *f);
     build_heap_forest(*f);
     dev = std::move(f);
     return *dev;
@@ -1998,6 +2109,60 @@ void predict_device(const Model& m, const float* x, uint64_t n, uint64_t F, bool
     forest_predict_rows(f, x, n, F, out, st);
     if (!raw) launch_transform(transform_of(m.objective), out, m.n_groups, n, st);
     BST_CK(cudaGetLastError());
+}
+
+// Metric values of [G][n] predictions (already transformed for the
+// probability metrics): RMSE (metrics/regression.rs:17-45), log loss
+// (metrics/classification.rs:13-40), multiclass log loss
+// (classification.rs:332-360); f64 sums in row order.
+double metric_value(int metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w) {
+    if (n == 0) return 0.0;
+    const double EPS = 1e-15;
+    auto wv = [&](uint64_t i) { return w ? (double)w[i] : 1.0; };
+    auto clampd = [](double v, double lo, double hi) { return v < lo ? lo : (v > hi ? hi : v); };
+    if (metric == BST_METRIC_RMSE) {
+        double sum = 0.0;
+        for (uint32_t g = 0; g < G; ++g) {
+            double ss = 0, sw = 0;
+            for (uint64_t i = 0; i < n; ++i) {
+                const double d = (double)p[(uint64_t)g * n + i] - (double)y[i];
+                ss = ss + wv(i) * d * d;
+                sw = sw + wv(i);
+            }
+            sum += sw > 0.0 ? std::sqrt(ss / sw) : 0.0;
+        }
+        return sum / (double)G;
+    }
+    if (metric == BST_METRIC_LOGLOSS) {
+        double sl = 0, sw = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const double pp = clampd((double)p[i], EPS, 1.0 - EPS), l = (double)y[i];
+            sl = sl + wv(i) * -(l * std::log(pp) + (1.0 - l) * std::log(1.0 - pp));
+            sw = sw + wv(i);
+        }
+        return sw > 0.0 ? sl / sw : 0.0;
+    }
+    if (metric == BST_METRIC_MLOGLOSS) {
+        double sl = 0, sw = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const float r = std::round(y[i]);
+            const uint64_t c = r > 0.0f ? (uint64_t)r : 0;
+            const double pp = clampd(c < G ? (double)p[c * n + i] : EPS, EPS, 1.0 - EPS);
+            sl = sl + wv(i) * -std::log(pp);
+            sw = sw + wv(i);
+        }
+        return sw > 0.0 ? sl / sw : 0.0;
+    }
+    return std::numeric_limits<double>::quiet_NaN();
+}
+
+// default_metric_for_objective (training/metrics/mod.rs:213-236) for
+// BST_METRIC_DEFAULT.
+int resolve_metric(int metric, int objective) {
+    if (metric != BST_METRIC_DEFAULT) return metric;
+    if (objective == BST_OBJ_LOGISTIC) return BST_METRIC_LOGLOSS;
+    if (objective == BST_OBJ_SOFTMAX) return BST_METRIC_MLOGLOSS;
+    return BST_METRIC_RMSE;
 }
 
 void predict_host(const Model& m, const HostDataset& ds, bool raw, float* out) {

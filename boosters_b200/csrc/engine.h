@@ -107,6 +107,9 @@ struct DeviceForest {
 void forest_predict_rows(const DeviceForest& f, const float* x, uint64_t n, uint64_t F, float* out, cudaStream_t st,
                          void* scratch = nullptr, size_t scratch_bytes = 0);
 bool forest_uses_heap(const DeviceForest& f, uint64_t n, uint64_t F);
+// Node-list forest of `trees` (forest order; no heap copy) into f.
+void upload_node_forest(const std::vector<const HostTree*>& trees, uint32_t n_groups, const std::vector<float>& base,
+                        DeviceForest& f);
 // Scratch bytes enough for any batch of up to n_max rows; bin bytes per row.
 size_t forest_scratch_max(const DeviceForest& f, uint64_t n_max, uint64_t F);
 size_t forest_bin_bytes_per_row(const DeviceForest& f, uint64_t F);
@@ -126,6 +129,9 @@ struct Model {
     std::vector<float> train_pred;
     double timings[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     Counters counters;
+    // early stopping: boosting rounds run, and the round count kept (the
+    // best round + 1; 0 when early stopping was off or never improved)
+    uint32_t rounds_run = 0, rounds_kept = 0;
     int device = 0;
     mutable std::mutex mu;
     mutable std::unique_ptr<DeviceForest> dev;
@@ -151,13 +157,18 @@ class Booster {
 };
 
 void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, DeviceBinned& out);
-std::unique_ptr<Model> train_model(const HostDataset& ds, const bst_config& cfg, uint32_t n_threads);
+// val (or null): the validation set of early stopping (trainer.rs:344-390).
+std::unique_ptr<Model> train_model(const HostDataset& ds, const bst_config& cfg, uint32_t n_threads,
+                                   const HostDataset* val = nullptr);
 std::unique_ptr<Model> grow_one_tree(const HostDataset& ds, const float* grad, const float* hess,
                                      const bst_config& cfg, uint32_t n_threads);
 void predict_host(const Model& m, const HostDataset& ds, bool raw, float* out);
 void predict_device(const Model& m, const float* x_dev_sm, uint64_t n, uint64_t F, bool raw,
                     float* out_dev, cudaStream_t st);
 int transform_of(int objective);
+// Metric value of [G][n] predictions (probabilities for the log losses).
+double metric_value(int metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w);
+int resolve_metric(int metric, int objective);
 // Model files (persist.cpp): .bstr.json text and .bstr bytes (uncompressed
 // MessagePack); model_from_bytes reads either (binary by its magic).
 std::string model_to_json(const Model& m, bool pretty);

@@ -2948,6 +2948,17 @@ void launch_transform(int transform, float* out, uint32_t G, uint64_t n, cudaStr
     k_transform<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(transform, out, G, n);
 }
 
+__global__ void k_add_f32(float* __restrict__ a, const float* __restrict__ b, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        a[i] = a[i] + b[i];
+}
+
+void launch_add_f32(float* a, const float* b, uint64_t n, cudaStream_t st) {
+    if (n == 0) return;
+    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148ull * 8);
+    k_add_f32<<<(unsigned)blocks, 256, 0, st>>>(a, b, n);
+}
+
 void init_kernel_attributes() {
     static std::atomic<unsigned long long> done{0ull};
     int dev = 0;

@@ -440,5 +440,7 @@ void launch_predict_heap(const HeapForest& f, const float* x, uint64_t n, uint32
                          void* scratch, cudaStream_t st);
 // transform: 1 sigmoid, 2 softmax over [G][n]
 void launch_transform(int transform, float* out, uint32_t G, uint64_t n, cudaStream_t st);
+// a[i] = a[i] + b[i] (f32), i < n
+void launch_add_f32(float* a, const float* b, uint64_t n, cudaStream_t st);
 
 }  // namespace bst

@@ -108,7 +108,8 @@ typedef struct bst_config {
     int32_t enable_bundling;             /* default 1                       */
     uint32_t max_categorical_cardinality; /* default 0 (no auto-detect)     */
     uint64_t binning_sample_cnt;         /* default 200000                  */
-    /* early stopping: < 0 means None */
+    /* early stopping patience (model/gbdt/config.rs:210,366): < 0 means
+     * None; None and 0 disable it. Supported by bst_gbdt_train only. */
     int32_t early_stopping_rounds;
     /* resources / reproducibility */
     uint64_t cache_size; /* default 8 (host histogram LRU of the reference) */
@@ -191,7 +192,14 @@ typedef struct bst_model bst_model;
 /* n_threads keeps the reference's meaning for split tie-breaking:
  * 1 = sequential (first maximal feature wins), otherwise the rayon
  * reduction order (last maximal feature wins when >= 16 features,
- * training/gbdt/split/find.rs:125-129,266-269). val may be NULL. */
+ * training/gbdt/split/find.rs:125-129,266-269). val may be NULL; it is read
+ * only with early stopping (cfg.early_stopping_rounds > 0) and a metric:
+ * after every round the validation metric (without val: the training
+ * metric; with BST_METRIC_NONE: NaN) is compared with the best so far, and
+ * training stops once that many rounds passed without improvement, keeping
+ * the trees up to the best round (training/gbdt/trainer.rs:344-401,
+ * callback.rs:103-136). val then needs targets and at least the training
+ * set's features. */
 bst_status bst_gbdt_train(const bst_dataset* train, const bst_dataset* val,
                           const bst_config* cfg, uint32_t n_threads, bst_model** out);
 
@@ -216,7 +224,8 @@ uint32_t bst_model_n_groups(const bst_model* m);
 uint32_t bst_model_n_features(const bst_model* m);
 /* Base scores, one per group. */
 bst_status bst_model_base_scores(const bst_model* m, float* out);
-/* Training predictions [n_groups, n_samples] left after the last round. */
+/* Training predictions [n_groups, n_samples] left after the last round
+ * (after early stopping: of the trees kept). */
 bst_status bst_model_train_predictions(const bst_model* m, float* out);
 
 /* Tree introspection (repr/gbdt/tree.rs:32-47 Tree SoA). */
@@ -272,7 +281,8 @@ bst_status bst_histogram_build(const uint16_t* bins, const uint32_t* n_bins,
 /* Incremental training: the boosting loop of GBDTTrainer::train
  * (training/gbdt/trainer.rs:242-401) over a GPU-resident binned copy of
  * `train`, a caller-chosen number of rounds per update. cfg.n_trees is
- * ignored; bst_booster_model snapshots the trees trained so far. */
+ * ignored; bst_booster_model snapshots the trees trained so far. Early
+ * stopping (cfg.early_stopping_rounds > 0) is BST_ERR_UNSUPPORTED here. */
 typedef struct bst_booster bst_booster;
 bst_status bst_booster_create(const bst_dataset* train, const bst_config* cfg, uint32_t n_threads,
                               bst_booster** out);
