@@ -15,9 +15,19 @@ import numpy as np
 from . import _native as _n
 from ._native import BoostersError
 
-__all__ = ["Dataset", "GBDTConfig", "GBDTModel", "Objective", "Metric", "GrowthStrategy",
+__all__ = ["Dataset", "GBDTConfig", "GBDTModel", "Objective", "Metric", "GrowthStrategy", "ImportanceType",
            "BoostersError", "BinnedDataset", "synth", "metric"]
 __version__ = _n.lib.bst_version().decode()
+
+
+class ImportanceType(enum.Enum):
+    """Feature importance kinds (explainability/importance.rs:43-55)."""
+
+    Split = 0
+    Gain = 1
+    AverageGain = 2
+    Cover = 3
+    AverageCover = 4
 
 
 class GrowthStrategy(enum.Enum):
@@ -488,6 +498,33 @@ class GBDTModel:
         _n.check(_n.lib.bst_model_tree_train_info(self._h, i, P(t["split_bin"], ctypes.c_uint32),
                                                   P(t["grad_sum"], ctypes.c_double), P(t["hess_sum"], ctypes.c_double)))
         return t
+
+    def feature_importance(self, importance_type=ImportanceType.Split):
+        """Per-feature importance (compute_forest_importance,
+        explainability/importance.rs:199-270): split counts, gains or covers
+        of the split nodes summed in f32 in tree and node order; the Average
+        kinds divide by each feature's split count."""
+        if self.n_trees == 0:
+            raise _n.BoostersError(_n.BST_ERR_INVALID_ARGUMENT, "cannot compute importance of an empty model")
+        F = self.n_features
+        counts = np.zeros(F, np.uint64)
+        values = np.zeros(F, np.float32)
+        kind = ImportanceType(importance_type)
+        for i in range(self.n_trees):
+            t = self.tree(i)
+            split = (t["is_leaf"] == 0) & (t["split_index"] < F)
+            feats = t["split_index"][split].astype(np.intp)
+            np.add.at(counts, feats, 1)
+            if kind == ImportanceType.Split:
+                np.add.at(values, feats, np.float32(1.0))
+            elif kind in (ImportanceType.Gain, ImportanceType.AverageGain):
+                np.add.at(values, feats, t["gain"][split])
+            else:
+                np.add.at(values, feats, t["cover"][split])
+        if kind in (ImportanceType.AverageGain, ImportanceType.AverageCover):
+            used = counts > 0
+            values[used] = values[used] / counts[used].astype(np.float32)
+        return values
 
     def tree_row_leaves(self, i, n_rows):
         out = np.zeros(n_rows, dtype=np.uint32)
