@@ -843,8 +843,11 @@ class Trainer {
     // (or of all rows, root): partial histograms of the lane tiles, general
     // tiles (atomic, into zeroed right slots), then the merge with the
     // subtraction trick.
+    // wide: the level has at most WIDE_MERGE_NODES expanding nodes (the
+    // merge splits each node's many row segments over more threads)
+    static constexpr uint32_t WIDE_MERGE_NODES = 4;
     void enqueue_hist(const GradRef& gr, const uint32_t* ridx, bool root, Timer& tm, uint64_t& launches,
-                      uint64_t& hist_launches) {
+                      uint64_t& hist_launches, bool wide = false) {
         // resident general-tile blocks per SM: 64 registers x 256 threads
         // allow 4; the fixed-point form's 16 B/bin shared histograms allow 3
         const uint32_t g_hist = 148 * (qmode_ == GRAD_F32 ? 3 : 4);
@@ -858,7 +861,7 @@ class Trainer {
         tm.end();
         tm.begin(PH_OTHER);
         launch_b_merge(bd_, hist_.p, slot_bins_, p_.total_bins, d_part_.p, n_lane_tiles_, d_ent_.p, n_ent_,
-                       d_bin_map_.p, n_tiles_ > 0, root ? 1 : 0, qmode_, st_, hist32_);
+                       d_bin_map_.p, n_tiles_ > 0, root ? 1 : 0, qmode_, st_, hist32_, wide ? 1 : 0);
         tm.end();
         const uint32_t hist_kernels = (n_lane_tiles_ ? 1u : 0u) + (n_tiles_ ? 1u : 0u);
         launches += 2 * hist_kernels;  // builds and merges
@@ -880,7 +883,7 @@ class Trainer {
         if (n_tiles_) BST_CK(cudaMemsetAsync(hist_.p, 0, hbytes() * slot_bins_, st_));
         launch_b_root_hist(bd_, n_, chunk_rows(n_), st_);
         tm.end();
-        enqueue_hist(gh, ridx_.p, true, tm, launches, hist_launches);
+        enqueue_hist(gh, ridx_.p, true, tm, launches, hist_launches, true);
         tm.begin(PH_SCAN);
         launch_split_scan(d_root_scan_.p, 1, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p,
                           d_node_tot_.p, st_, hist32_);
@@ -914,7 +917,8 @@ class Trainer {
                     tm.end();
                     launches += 1;
                 }
-                enqueue_hist(gl, rout, false, tm, launches, hist_launches);
+                // level d expands at most 2^d nodes
+                enqueue_hist(gl, rout, false, tm, launches, hist_launches, (1u << std::min(d, 31u)) <= WIDE_MERGE_NODES);
                 tm.begin(PH_SCAN);
                 launch_b_scan(bd_, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p,
                               d_node_tot_.p, a ^ 1, last_wins_ ? 1 : 0, lp, (d + 1) & 1u, g_wide, st_,
@@ -1110,7 +1114,7 @@ class Trainer {
         upload(hs, 1, d_bstate_);
         upload(hseg, segs.size(), d_seg_exp_);
         uint64_t launches = 0, hist_launches = 0;
-        enqueue_hist(gr_o_, ridx_.p, root, timer_, launches, hist_launches);
+        enqueue_hist(gr_o_, ridx_.p, root, timer_, launches, hist_launches, exps.size() <= WIDE_MERGE_NODES);
         m_.counters.launches += launches;
         m_.counters.hist_launches += hist_launches;
         m_.counters.hist_rows += rows;

@@ -909,6 +909,72 @@ k_b_merge(BDev d, HB* __restrict__ hist, uint64_t slot_bins, const void* __restr
     }
 }
 
+// The same merge for levels with few expanding nodes (many row segments
+// each): a block takes MW_E consecutive entries of one node and its MW_G
+// warps sum every MW_G-th segment, then warp 0 adds the MW_G partial sums
+// (exact integers, so the result equals k_b_merge's) and stores as
+// k_b_merge does. Per-thread chains of segments / MW_G dependent loads
+// instead of segments.
+constexpr uint32_t MW_E = 32, MW_G = 8;
+
+template <int MODE, typename HB>
+__global__ void __launch_bounds__(MW_E * MW_G)
+k_b_merge_wide(BDev d, HB* __restrict__ hist, uint64_t slot_bins, const void* __restrict__ part, uint32_t n_tiles,
+               const uint2* __restrict__ ent, uint32_t n_ent, int root) {
+    using E = typename PartEntry<MODE>::T;
+    __shared__ long long s_g[MW_G][MW_E], s_h[MW_G][MW_E];
+    const E* P = reinterpret_cast<const E*>(part);
+    const uint32_t n_exp = d.state->n_exp, n_seg = d.state->hist_chunks;
+    const uint32_t tiles = (n_ent + MW_E - 1) / MW_E;
+    const uint64_t items = (uint64_t)n_exp * tiles;
+    const size_t rec = (size_t)n_tiles * LANE_PART_STRIDE;
+    const uint32_t el = threadIdx.x % MW_E, grp = threadIdx.x / MW_E;
+    for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
+        const uint32_t j = (uint32_t)(it / tiles), r = (uint32_t)(it % tiles) * MW_E + el;
+        const uint2 m = r < n_ent ? ent[r] : make_uint2(0xFFFFFFFFu, 0u);
+        const bool ok = m.x != 0xFFFFFFFFu;
+        const uint32_t c0 = d.exp[j].hist_off, c1 = j + 1 < n_exp ? d.exp[j + 1].hist_off : n_seg;
+        long long g = 0, h = 0;
+        if (ok) {
+            const E* p = P + (size_t)(m.y >> 16) * LANE_PART_STRIDE + (m.y & 0xFFFFu);
+            uint32_t c = c0 + grp;
+            for (; c + 3 * MW_G < c1; c += 4 * MW_G) {  // four segments' loads in flight
+                const E v0 = p[(size_t)c * rec], v1 = p[(size_t)(c + MW_G) * rec];
+                const E v2 = p[(size_t)(c + 2 * MW_G) * rec], v3 = p[(size_t)(c + 3 * MW_G) * rec];
+                g += (long long)v0.x + (long long)v1.x + (long long)v2.x + (long long)v3.x;
+                h += (long long)v0.y + (long long)v1.y + (long long)v2.y + (long long)v3.y;
+            }
+            for (; c < c1; c += MW_G) {
+                const E v = p[(size_t)c * rec];
+                g += v.x;
+                h += v.y;
+            }
+        }
+        s_g[grp][el] = g;
+        s_h[grp][el] = h;
+        __syncthreads();
+        if (grp == 0 && ok) {
+#pragma unroll
+            for (uint32_t q = 1; q < MW_G; ++q) {
+                g += s_g[q][el];
+                h += s_h[q][el];
+            }
+            const BExp& e = d.exp[j];
+            const HB sm = hb_make<HB>(g, h);
+            if (root) {
+                hist[(size_t)e.right_pnode * slot_bins + m.x] = sm;
+            } else {
+                const HB par = hist[(size_t)e.left_pnode * slot_bins + m.x];
+                const HB lg = hb_make<HB>((long long)par.g - g, (long long)par.h - h);
+                const bool left_small = e.lc <= e.rc;  // grower.rs:398-402
+                hist[(size_t)e.left_pnode * slot_bins + m.x] = left_small ? sm : lg;
+                hist[(size_t)e.right_pnode * slot_bins + m.x] = left_small ? lg : sm;
+            }
+        }
+        __syncthreads();  // s_g / s_h are reused by the next item
+    }
+}
+
 // Bins of general tiles (built atomically into the right slot).
 template <typename HB>
 __global__ void k_b_merge_rest(BDev d, HB* __restrict__ hist, uint64_t slot_bins, uint32_t total_bins,
@@ -926,26 +992,34 @@ __global__ void k_b_merge_rest(BDev d, HB* __restrict__ hist, uint64_t slot_bins
 template <typename HB>
 static void launch_b_merge_t(const BDev& d, HB* hist, uint64_t slot_bins, uint32_t total_bins, const void* part,
                              uint32_t n_lane_tiles, const uint2* ent, uint32_t n_ent, const uint32_t* bin_map,
-                             bool has_rest, int root, int mode, cudaStream_t st) {
+                             bool has_rest, int root, int mode, cudaStream_t st, int wide) {
     const unsigned grid = 148u * 8u;
     if (n_lane_tiles) {
-        if (mode == GRAD_F32)
+        if (wide) {
+            if (mode == GRAD_F32)
+                k_b_merge_wide<GRAD_F32, HB><<<grid, MW_E * MW_G, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles,
+                                                                          ent, n_ent, root);
+            else
+                k_b_merge_wide<GRAD_Q8, HB><<<grid, MW_E * MW_G, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles,
+                                                                         ent, n_ent, root);
+        } else if (mode == GRAD_F32) {
             k_b_merge<GRAD_F32, HB><<<grid, 256, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles, ent, n_ent, root);
-        else
+        } else {
             k_b_merge<GRAD_Q8, HB><<<grid, 256, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles, ent, n_ent, root);
+        }
     }
     if (has_rest) k_b_merge_rest<HB><<<grid, 256, 0, st>>>(d, hist, slot_bins, total_bins, bin_map, root);
 }
 
 void launch_b_merge(const BDev& d, void* hist, uint64_t slot_bins, uint32_t total_bins, const void* part,
                     uint32_t n_lane_tiles, const uint2* ent, uint32_t n_ent, const uint32_t* bin_map, bool has_rest,
-                    int root, int mode, cudaStream_t st, int hist32) {
+                    int root, int mode, cudaStream_t st, int hist32, int wide) {
     if (hist32)
         launch_b_merge_t(d, static_cast<HBin32*>(hist), slot_bins, total_bins, part, n_lane_tiles, ent, n_ent, bin_map,
-                         has_rest, root, mode, st);
+                         has_rest, root, mode, st, wide);
     else
         launch_b_merge_t(d, static_cast<HBin*>(hist), slot_bins, total_bins, part, n_lane_tiles, ent, n_ent, bin_map,
-                         has_rest, root, mode, st);
+                         has_rest, root, mode, st, wide);
 }
 
 // Level state for the root histogram: one "expanding node" whose smaller

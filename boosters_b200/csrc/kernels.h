@@ -338,9 +338,11 @@ void launch_b_hist_part(const BDev& d, const LaneTile* tiles, uint32_t n_tiles, 
 // built atomically into the right slots.
 // ent [n_ent]: per partial entry of a node (lane tiles in order, column-major
 // inside each tile): (global bin or 0xFFFFFFFF, tile << 16 | offset).
+// wide != 0: the layout for levels with few expanding nodes (many row
+// segments per node); same result.
 void launch_b_merge(const BDev& d, void* hist, uint64_t slot_bins, uint32_t total_bins, const void* part,
                     uint32_t n_lane_tiles, const uint2* ent, uint32_t n_ent, const uint32_t* bin_map, bool has_rest,
-                    int root, int mode, cudaStream_t st, int hist32 = 0);
+                    int root, int mode, cudaStream_t st, int hist32 = 0, int wide = 0);
 // Level state of the root histogram: all n rows as one segment list.
 void launch_b_root_hist(const BDev& d, uint64_t n, uint32_t chunk, cudaStream_t st);
 // split finding of the level's nodes and the reduction over columns into
