@@ -1295,6 +1295,10 @@ class Trainer {
         timer_.end();
         m_.counters.launches += pch.empty() ? 0 : 2;
         m_.counters.partition_rows += prow;
+        if (spec_leafwise_ && need_split && n_cols_ > 0) {
+            expand_children_on_device(par, tree_children, right_ids, children);
+            return;
+        }
         unsigned* hc = stage_.take<unsigned>(2 * k);
         BST_CK(cudaMemcpyAsync(hc, d_cursors_.p, sizeof(unsigned) * 2 * k, cudaMemcpyDeviceToHost, st_));
         BST_CK(cudaStreamSynchronize(st_));
@@ -1368,6 +1372,64 @@ class Trainer {
                 children.push_back(Cand{right_ids[j], tree_children[j].second, d, inv, rg, rh, rc[j]});
             }
         }
+    }
+
+    // Batched leaf-wise, after expand()'s partition: the children's counts,
+    // smaller children and histogram segments come from the partition's
+    // cursors on the device (k_lw_children), so the histograms and the
+    // children's split search follow the partition directly; one read-back
+    // (the children's splits and the cursors) per expansion batch.
+    void expand_children_on_device(const std::vector<Cand>& par,
+                                   const std::vector<std::pair<uint32_t, uint32_t>>& tree_children,
+                                   const std::vector<uint32_t>& right_ids, std::vector<Cand>& children) {
+        const size_t k = par.size();
+        if (n_tiles_) {  // general tiles add atomically into zeroed right slots
+            const uint32_t r_lo = *std::min_element(right_ids.begin(), right_ids.end());
+            const uint32_t r_hi = *std::max_element(right_ids.begin(), right_ids.end());
+            BST_CK(cudaMemsetAsync(reinterpret_cast<char*>(hist_.p) + (size_t)r_lo * slot_bins_ * hbytes(), 0,
+                                   hbytes() * slot_bins_ * (size_t)(r_hi - r_lo + 1), st_));
+        }
+        BExp* he = stage_.take<BExp>(k);
+        std::memset(he, 0, sizeof(BExp) * k);
+        for (size_t j = 0; j < k; ++j) {
+            he[j].left_pnode = par[j].node;
+            he[j].right_pnode = right_ids[j];
+        }
+        upload(he, k, d_bexp_);
+        launch_lw_children(bd_, d_pworks_.p, d_cursors_.p, (uint32_t)k, d_scan_nodes_.p, st_);
+        uint64_t launches = 1, hist_launches = 0;
+        enqueue_hist(gr_o_, ridx_.p, false, timer_, launches, hist_launches, k <= WIDE_MERGE_NODES);
+        timer_.begin(PH_SCAN);
+        launch_split_scan(d_scan_nodes_.p, (uint32_t)(2 * k), scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale_o_, gp_,
+                          d_cand_.p, d_node_tot_.p, st_, hist32_);
+        launch_split_reduce(d_cand_.p, d_node_tot_.p, (uint32_t)(2 * k), n_cols_, last_wins_ ? 1 : 0, d_splits_.p, st_);
+        timer_.end();
+        NodeSplit* hs = stage_.take<NodeSplit>(2 * k);
+        unsigned* hc = stage_.take<unsigned>(2 * k);
+        BST_CK(cudaMemcpyAsync(hs, d_splits_.p, sizeof(NodeSplit) * 2 * k, cudaMemcpyDeviceToHost, st_));
+        BST_CK(cudaMemcpyAsync(hc, d_cursors_.p, sizeof(unsigned) * 2 * k, cudaMemcpyDeviceToHost, st_));
+        BST_CK(cudaStreamSynchronize(st_));
+        m_.counters.launches += launches + 2;
+        m_.counters.hist_launches += hist_launches;
+        m_.counters.scan_launches += 1;
+        children.clear();
+        children.reserve(2 * k);
+        uint64_t rows = 0;
+        for (size_t j = 0; j < k; ++j) {
+            const PNode pn = pn_[par[j].node];
+            const uint32_t lc = hc[2 * j] - pn.begin, rc = pn.count - lc;
+            pn_[par[j].node] = PNode{pn.begin, lc};
+            pn_[right_ids[j]] = PNode{pn.begin + lc, rc};
+            rows += std::min(lc, rc);
+            const uint32_t d = par[j].depth + 1;
+            children.push_back(Cand{par[j].node, tree_children[j].first, d, hs[2 * j], hs[2 * j].tot_g,
+                                    hs[2 * j].tot_h, lc});
+            children.push_back(Cand{right_ids[j], tree_children[j].second, d, hs[2 * j + 1], hs[2 * j + 1].tot_g,
+                                    hs[2 * j + 1].tot_h, rc});
+        }
+        m_.counters.hist_rows += rows;
+        m_.counters.hist_bytes += rows * ((uint64_t)p_.f8 + 2ull * p_.f16 + grad_bytes() + 4ull);
+        stage_.reset();
     }
 
     // Quantised training: re-solve every leaf from the exact fixed-point sums

@@ -2238,6 +2238,72 @@ __device__ void children_body(BDev d, int a, int need_split) {
 
 
 
+// Children of a host-chosen expansion batch (batched leaf-wise growth):
+// from the partition's cursors, each parent's child counts and smaller child
+// (grower.rs:398-402), the level's histogram row segments (the layout the
+// host-driven loop uploads, with the same segment size rule) and the
+// children's scan nodes, so that the histograms follow the partition with no
+// read-back. d.exp[j] carries the parents' left_pnode / right_pnode on entry.
+__global__ void __launch_bounds__(1024) k_lw_children(BDev d, const PartWork* __restrict__ pw,
+                                                     const unsigned* __restrict__ cursors, uint32_t k,
+                                                     ScanNode* __restrict__ scan_nodes) {
+    __shared__ uint32_t sh[33];
+    __shared__ unsigned long long rows;
+    __shared__ uint32_t chunk, base;
+    if (threadIdx.x == 0) {
+        rows = 0;
+        base = 0;
+    }
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < k; j += blockDim.x) {
+        const PartWork w = pw[j];
+        const uint32_t lc = cursors[2 * j] - w.begin, rc = w.count - lc;
+        BExp e = d.exp[j];
+        e.lc = lc;
+        e.rc = rc;
+        const bool left_small = lc <= rc;
+        e.small_begin = left_small ? w.begin : w.begin + lc;
+        e.small_count = left_small ? lc : rc;
+        d.exp[j] = e;
+        scan_nodes[2 * j] = ScanNode{e.left_pnode, lc, 0u, 0u, 0, 0};
+        scan_nodes[2 * j + 1] = ScanNode{e.right_pnode, rc, 0u, 0u, 0, 0};
+        atomicAdd(&rows, (unsigned long long)e.small_count);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // rows per segment: about hist_target segments, a multiple of 256 in [1024, seg_max]
+        const unsigned long long tgt = d.hist_target ? d.hist_target : 1u;
+        unsigned long long want = (rows + tgt - 1) / tgt;
+        want = (want + 255ull) & ~255ull;
+        chunk = (uint32_t)(want < 1024ull ? 1024ull : (want > d.hist_seg_max ? d.hist_seg_max : want));
+    }
+    __syncthreads();
+    for (uint32_t j0 = 0; j0 < k; j0 += blockDim.x) {
+        const uint32_t j = j0 + threadIdx.x;
+        const bool valid = j < k;
+        const uint32_t nch = valid ? (d.exp[j].small_count + chunk - 1) / chunk : 0u;
+        uint32_t tc;
+        const uint32_t jc = block_excl_scan(nch, sh, &tc);
+        if (valid) d.exp[j].hist_off = base + jc;
+        __syncthreads();
+        if (threadIdx.x == 0) base += tc;
+        __syncthreads();
+    }
+    const uint32_t total = base < d.max_segs ? base : d.max_segs;
+    for (uint32_t c = threadIdx.x; c < total; c += blockDim.x)
+        d.seg_exp[c] = last_le(k, c, [&](uint32_t q) { return d.exp[q].hist_off; });
+    if (threadIdx.x == 0) {
+        d.state->n_exp = k;
+        d.state->hist_chunks = total;
+        d.state->hist_chunk = chunk;
+    }
+}
+
+void launch_lw_children(const BDev& d, const PartWork* pw, const unsigned* cursors, uint32_t k, ScanNode* scan_nodes,
+                        cudaStream_t st) {
+    if (k == 0) return;
+    k_lw_children<<<1, 1024, 0, st>>>(d, pw, cursors, k, scan_nodes);
+}
+
 template <typename HB>
 __global__ void k_b_zero_right(BDev d, HB* __restrict__ hist, uint64_t slot_bins) {
     const uint64_t n = (uint64_t)d.state->n_exp * slot_bins;

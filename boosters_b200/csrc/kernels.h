@@ -343,6 +343,11 @@ void launch_b_hist_part(const BDev& d, const LaneTile* tiles, uint32_t n_tiles, 
 void launch_b_merge(const BDev& d, void* hist, uint64_t slot_bins, uint32_t total_bins, const void* part,
                     uint32_t n_lane_tiles, const uint2* ent, uint32_t n_ent, const uint32_t* bin_map, bool has_rest,
                     int root, int mode, cudaStream_t st, int hist32 = 0, int wide = 0);
+// Batched leaf-wise growth: children counts, smaller children, histogram
+// segments and scan nodes of k partitioned parents (d.exp[j] holds their
+// slots), from the partition's cursors, on the device.
+void launch_lw_children(const BDev& d, const PartWork* pw, const unsigned* cursors, uint32_t k, ScanNode* scan_nodes,
+                        cudaStream_t st);
 // Level state of the root histogram: all n rows as one segment list.
 void launch_b_root_hist(const BDev& d, uint64_t n, uint32_t chunk, cudaStream_t st);
 // split finding of the level's nodes and the reduction over columns into
