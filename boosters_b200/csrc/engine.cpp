@@ -885,14 +885,10 @@ class Trainer {
         tm.end();
         enqueue_hist(gh, ridx_.p, true, tm, launches, hist_launches, true);
         tm.begin(PH_SCAN);
-        launch_split_scan(d_root_scan_.p, 1, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p,
-                          d_node_tot_.p, st_, hist32_);
-        launch_split_reduce(d_cand_.p, d_node_tot_.p, 1, n_cols_, last_wins_ ? 1 : 0, d_splits_.p, st_);
+        launch_b_scan(bd_, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p, d_node_tot_.p, 0,
+                      last_wins_ ? 1 : 0, lp, 0u, g_wide, st_, hist32_, d_root_scan_.p);  // + level-0 decisions
         tm.end();
-        tm.begin(PH_OTHER);
-        launch_b_root_set(bd_, d_splits_.p, lp, scale, st_);  // + level-0 decisions
-        tm.end();
-        launches += 5;
+        launches += 4;
         // row indices: level d partitions R[d & 1] into R[(d + 1) & 1]
         uint32_t* R[2] = {ridx_.p, tmp_.p};
         for (uint32_t d = 0; d < cfg_.max_depth; ++d) {
@@ -927,23 +923,19 @@ class Trainer {
                 launches += 1;
             } else {
                 tm.begin(PH_OTHER);
-                BST_CK(cudaMemsetAsync(d_sums_.p, 0, sizeof(long long) * d_sums_.n, st_));
                 GradRef gl = gh;
                 gl.qpos = qpos_[(d + 1) & 1u].p;
-                launch_b_sums(bd_, rout, gl, g_wide, st_);
-                launch_b_children_sums(bd_, a ^ 1, st_);
+                launch_b_sums(bd_, rout, gl, a ^ 1, g_wide, st_);  // + children sums
                 tm.end();
-                launches += 2;
+                launches += 1;
             }
         }
         tm.begin(PH_LEAF);
         launch_b_finalize(bd_, (int)(cfg_.max_depth & 1u), lp, scale, cfg_.max_depth & 1u, st_);
         if (qmode_ != GRAD_F32) {
-            // leaves solved from the exact sums of the f32 gradients
-            BST_CK(cudaMemsetAsync(d_sums_.p, 0, sizeof(long long) * d_sums_.n, st_));
-            launch_b_leaf_sums(bd_, R[0], R[1], exact_ref(o), g_wide, st_);
-            launch_b_leaf_values(bd_, lp, scales_.p + 4 * (size_t)o, st_);
-            launches += 2;
+            // leaves solved from the exact sums of the f32 gradients (+ values)
+            launch_b_leaf_sums(bd_, R[0], R[1], exact_ref(o), lp, scales_.p + 4 * (size_t)o, g_wide, st_);
+            launches += 1;
         }
         launch_b_leaf_update(bd_, R[0], R[1], pred, cfg_.record_leaves ? row_leaf_.p : nullptr, g_wide, st_);
         tm.end();

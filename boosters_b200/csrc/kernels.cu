@@ -2032,23 +2032,6 @@ void launch_b_decide(const BDev& d, int a, LeafParams lp, const double* scale, u
     k_b_decide<<<1, 1024, 0, st>>>(d, a, lp, scale, buf);
 }
 
-// Root split into the frontier, then the level-0 decisions.
-__global__ void __launch_bounds__(1024) k_b_root_set(BDev d, const NodeSplit* __restrict__ rs, LeafParams lp,
-                                                    const double* __restrict__ scale) {
-    if (threadIdx.x == 0) {
-        const NodeSplit s = *rs;
-        BNode& r = d.front[0][0];
-        r.split = s;
-        r.G = s.tot_g;
-        r.H = s.tot_h;
-    }
-    __syncthreads();
-    decide_body(d, 0, lp, scale, 0u);
-}
-
-void launch_b_root_set(const BDev& d, const NodeSplit* rs, LeafParams lp, const double* scale, cudaStream_t st) {
-    k_b_root_set<<<1, 1024, 0, st>>>(d, rs, lp, scale);
-}
 
 // "Last block" hand-off: every block of the launch counts itself in
 // state->done after a fence; the block that completes the count returns true
@@ -2228,6 +2211,8 @@ __device__ void children_body(BDev d, int a, int need_split) {
         for (uint32_t c = threadIdx.x; c < total; c += blockDim.x)
             d.seg_exp[c] = last_le(n_exp, c, [&](uint32_t k) { return d.exp[k].hist_off; });
     }
+    if (!need_split)  // the node sums of k_b_sums accumulate from zero
+        for (uint32_t i = threadIdx.x; i < 2 * n_exp; i += blockDim.x) d.sums[i] = 0;
     if (threadIdx.x == 0) {
         s->hist_chunks = base < d.max_segs ? base : d.max_segs;
         s->hist_chunk = chunk;
@@ -2394,19 +2379,20 @@ template <typename HB>
 __global__ void __launch_bounds__(SCAN_WARPS * 32)
 k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HB* __restrict__ hist,
          uint64_t slot_bins, const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
-         long long* __restrict__ node_tot, int b, int last_wins, LeafParams lp, uint32_t buf) {
+         long long* __restrict__ node_tot, int b, int last_wins, LeafParams lp, uint32_t buf,
+         const ScanNode* __restrict__ root) {
     __shared__ double s_key[SCAN_WARPS][SORT_N];
     __shared__ uint32_t s_cat[SCAN_WARPS][SORT_N];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t n_nodes = 2 * d.state->n_exp;
+    const uint32_t n_nodes = root ? 1u : 2 * d.state->n_exp;
     const uint32_t col_blocks = (n_cols + SCAN_WARPS - 1) / SCAN_WARPS;
     const uint64_t items = (uint64_t)n_nodes * col_blocks;
     for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
         const uint32_t node = (uint32_t)(it / col_blocks);
         const uint32_t col = (uint32_t)(it % col_blocks) * SCAN_WARPS + warp;
         if (col < n_cols) {
-            const float g = scan_item(d.scan_nodes[node], node, col, cols, n_cols, hist, slot_bins, scale, gp, cand,
-                                      node_tot, s_key[warp], s_cat[warp]);
+            const float g = scan_item(root ? root[0] : d.scan_nodes[node], node, col, cols, n_cols, hist, slot_bins,
+                                      scale, gp, cand, node_tot, s_key[warp], s_cat[warp]);
             if (lane == 0 && g > -INFINITY) atomicMax(&d.node_key[node], cand_key(g, col, last_wins));
         }
     }
@@ -2443,13 +2429,13 @@ k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HB*
 
 void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const void* hist, uint64_t slot_bins,
                    const double* scale, GainParamsDev gp, ColCand* cand, long long* node_tot, int b, int last_wins,
-                   LeafParams lp, uint32_t buf, uint32_t grid, cudaStream_t st, int hist32) {
+                   LeafParams lp, uint32_t buf, uint32_t grid, cudaStream_t st, int hist32, const ScanNode* root) {
     if (hist32)
         k_b_scan<HBin32><<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, static_cast<const HBin32*>(hist), slot_bins,
-                                                           scale, gp, cand, node_tot, b, last_wins, lp, buf);
+                                                           scale, gp, cand, node_tot, b, last_wins, lp, buf, root);
     else
         k_b_scan<HBin><<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, static_cast<const HBin*>(hist), slot_bins,
-                                                         scale, gp, cand, node_tot, b, last_wins, lp, buf);
+                                                         scale, gp, cand, node_tot, b, last_wins, lp, buf, root);
 }
 
 // This thread's share of the fixed-point sums of positions [start, start +
@@ -2479,9 +2465,13 @@ __device__ __forceinline__ void range_sums(uint32_t start, uint32_t len, const u
     }
 }
 
-// Node sums of the smaller children when the children are not split further.
+__device__ void children_sums_body(BDev d, int b);
+
+// Node sums of the smaller children when the children are not split further
+// (d.sums zeroed by the partition's last block); the last block then gives
+// both children of every expansion their sums (frontier b).
 template <int MODE>
-__global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, GradRef gr) {
+__global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, GradRef gr, int b) {
     const uint32_t total = d.state->hist_chunks, CH = d.state->hist_chunk;
     const GradLoad<MODE> load(gr);
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
@@ -2500,18 +2490,19 @@ __global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, GradRef gr) 
             atomicAdd(reinterpret_cast<unsigned long long*>(&d.sums[2 * j + 1]), (unsigned long long)ah);
         }
     }
+    if (last_block(d.state)) children_sums_body(d, b);
 }
 
-void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, uint32_t grid, cudaStream_t st) {
+void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, int b, uint32_t grid, cudaStream_t st) {
     if (gr.mode == GRAD_Q16)
-        k_b_sums<GRAD_Q16><<<grid, 256, 0, st>>>(d, ridx, gr);
+        k_b_sums<GRAD_Q16><<<grid, 256, 0, st>>>(d, ridx, gr, b);
     else if (gr.mode == GRAD_Q8)
-        k_b_sums<GRAD_Q8><<<grid, 256, 0, st>>>(d, ridx, gr);
+        k_b_sums<GRAD_Q8><<<grid, 256, 0, st>>>(d, ridx, gr, b);
     else
-        k_b_sums<GRAD_F32><<<grid, 256, 0, st>>>(d, ridx, gr);
+        k_b_sums<GRAD_F32><<<grid, 256, 0, st>>>(d, ridx, gr, b);
 }
 
-__global__ void k_b_children_sums(BDev d, int b) {
+__device__ void children_sums_body(BDev d, int b) {
     const uint32_t n_exp = d.state->n_exp;
     const BNode* A = d.front[b ^ 1];
     BNode* B = d.front[b];
@@ -2528,7 +2519,6 @@ __global__ void k_b_children_sums(BDev d, int b) {
     }
 }
 
-void launch_b_children_sums(const BDev& d, int b, cudaStream_t st) { k_b_children_sums<<<1, 1024, 0, st>>>(d, b); }
 
 // Remaining frontier -> leaves (grower.rs:484-514); leaf row chunks.
 __global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams lp, const double* __restrict__ scale,
@@ -2568,6 +2558,8 @@ __global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams l
         if (threadIdx.x == 0) base += tc;
         __syncthreads();
     }
+    // the quantised forms' leaf sums (k_b_leaf_sums) accumulate from zero
+    for (uint32_t i = threadIdx.x; i < 2 * nl; i += blockDim.x) d.sums[i] = 0;
     if (threadIdx.x == 0) {
         s->n_leaves = nl;
         s->leaf_chunks = base;
@@ -2579,9 +2571,14 @@ void launch_b_finalize(const BDev& d, int a, LeafParams lp, const double* scale,
     k_b_finalize<<<1, 1024, 0, st>>>(d, a, lp, scale, buf);
 }
 
+__device__ void leaf_values_body(BDev d, LeafParams lp, const double* __restrict__ scale);
+
 // Quantised training: every leaf is solved from the exact fixed-point sums
-// of the f32 gradients over its rows (d.sums[leaf][2], zeroed by the caller).
-__global__ void k_b_leaf_sums(BDev d, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1, GradRef gr) {
+// of the f32 gradients over its rows (d.sums[leaf][2], zeroed by
+// k_b_finalize); the last block solves the leaf values (scale: the f32
+// gradients' fixed-point scales).
+__global__ void k_b_leaf_sums(BDev d, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1, GradRef gr,
+                              LeafParams lp, const double* __restrict__ scale) {
     const uint32_t total = d.state->leaf_chunks, nl = d.state->n_leaves;
     const GradLoad<GRAD_F32> load(gr);
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
@@ -2601,14 +2598,15 @@ __global__ void k_b_leaf_sums(BDev d, const uint32_t* __restrict__ r0, const uin
             atomicAdd(reinterpret_cast<unsigned long long*>(&d.sums[2 * l + 1]), (unsigned long long)ah);
         }
     }
+    if (last_block(d.state)) leaf_values_body(d, lp, scale);
 }
 
-void launch_b_leaf_sums(const BDev& d, const uint32_t* r0, const uint32_t* r1, const GradRef& gr, uint32_t grid,
-                        cudaStream_t st) {
-    k_b_leaf_sums<<<grid, 256, 0, st>>>(d, r0, r1, gr);
+void launch_b_leaf_sums(const BDev& d, const uint32_t* r0, const uint32_t* r1, const GradRef& gr, LeafParams lp,
+                        const double* scale, uint32_t grid, cudaStream_t st) {
+    k_b_leaf_sums<<<grid, 256, 0, st>>>(d, r0, r1, gr, lp, scale);
 }
 
-__global__ void k_b_leaf_values(BDev d, LeafParams lp, const double* __restrict__ scale) {
+__device__ void leaf_values_body(BDev d, LeafParams lp, const double* __restrict__ scale) {
     const uint32_t nl = d.state->n_leaves;
     for (uint32_t l = threadIdx.x; l < nl; l += blockDim.x) {
         const long long G = d.sums[2 * l], H = d.sums[2 * l + 1];
@@ -2616,10 +2614,6 @@ __global__ void k_b_leaf_values(BDev d, LeafParams lp, const double* __restrict_
         d.leaves[l].value = v;
         write_leaf(d.tree[d.leaves[l].tnode], G, H, scale, v);
     }
-}
-
-void launch_b_leaf_values(const BDev& d, LeafParams lp, const double* scale, cudaStream_t st) {
-    k_b_leaf_values<<<1, 1024, 0, st>>>(d, lp, scale);
 }
 
 // pred[row] += leaf value over the final partition (grower.rs:208-219).

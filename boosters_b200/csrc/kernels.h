@@ -307,9 +307,6 @@ void init_kernel_attributes();
 void launch_b_root(const BDev& d, uint64_t n, cudaStream_t st);
 // Row indices alternate between two buffers: level d partitions buffer d & 1
 // into buffer (d + 1) & 1; a leaf records the buffer that holds its rows.
-// Root split into the frontier, then the level-0 decisions (rows in buffer 0).
-void launch_b_root_set(const BDev& d, const NodeSplit* root_split, LeafParams lp, const double* scale,
-                       cudaStream_t st);
 // level kernels; `a` is the index of the current frontier buffer
 void launch_b_decide(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st);
 void launch_transpose_bins(const uint8_t* b8, uint32_t s8, const uint16_t* b16, uint32_t s16, uint64_t n,
@@ -353,17 +350,20 @@ void launch_b_root_hist(const BDev& d, uint64_t n, uint32_t chunk, cudaStream_t 
 // split finding of the level's nodes and the reduction over columns into
 // frontier b, then (last block) the decisions of the next level, whose rows
 // are in buffer buf
+// root (or null): the level is the root alone, described by *root (rows in
+// buffer 0, frontier 0)
 void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const void* hist,
                    uint64_t slot_bins, const double* scale, GainParamsDev gp, ColCand* cand,
                    long long* node_tot, int b, int last_wins, LeafParams lp, uint32_t buf, uint32_t grid,
-                   cudaStream_t st, int hist32 = 0);
-void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, uint32_t grid, cudaStream_t st);
-void launch_b_children_sums(const BDev& d, int b, cudaStream_t st);
+                   cudaStream_t st, int hist32 = 0, const ScanNode* root = nullptr);
+// last level: the smaller children's sums, then (last block) both children's
+// sums into frontier b
+void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, int b, uint32_t grid, cudaStream_t st);
 void launch_b_finalize(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st);
-// quantised training: exact leaf solves from the f32 gradients (gr: GRAD_F32)
-void launch_b_leaf_sums(const BDev& d, const uint32_t* r0, const uint32_t* r1, const GradRef& gr, uint32_t grid,
-                        cudaStream_t st);
-void launch_b_leaf_values(const BDev& d, LeafParams lp, const double* scale, cudaStream_t st);
+// quantised training: exact leaf sums of the f32 gradients (gr: GRAD_F32),
+// then (last block) the leaf values with their fixed-point scale
+void launch_b_leaf_sums(const BDev& d, const uint32_t* r0, const uint32_t* r1, const GradRef& gr, LeafParams lp,
+                        const double* scale, uint32_t grid, cudaStream_t st);
 void launch_b_leaf_update(const BDev& d, const uint32_t* r0, const uint32_t* r1, float* pred, uint32_t* row_leaf,
                           uint32_t grid, cudaStream_t st);
 
