@@ -134,6 +134,46 @@ namespace {
 constexpr uint32_t PART_CHUNK_ROWS = 4096;
 constexpr uint32_t SUM_CHUNK_ROWS = 8192;
 
+// ---- column sampling (training/sampling/column.rs) -----------------------------
+// The reference seeds its column sampler from OS entropy (grower.rs:150-151,
+// column.rs:137-142), so no two of its runs draw the same columns; here the
+// draws are a splitmix64 stream keyed by (seed, round, output, depth) and
+// reproducible. The rule is the reference's: the tree's columns are
+// ceil(n * colsample_bytree) of all, each depth's ceil(|tree| *
+// colsample_bylevel) of the tree's, by a partial Fisher-Yates shuffle
+// (sample_k_inplace, column.rs:266-283), kept in ascending order; a rate
+// within 1e-6 of 1 samples nothing (column.rs:64-78).
+uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+struct ColStream {
+    uint64_t s;
+    ColStream(uint64_t seed, uint32_t round, uint32_t output, uint32_t depth) {
+        s = mix64(seed ^ (0x9E3779B97F4A7C15ull * (1ull + round)));
+        s = mix64(s ^ (0xC2B2AE3D27D4EB4Full * (1ull + output)));
+        s = mix64(s ^ (0x165667B19E3779F9ull * (1ull + depth)));
+    }
+    uint64_t next() {
+        s += 0x9E3779B97F4A7C15ull;
+        return mix64(s);
+    }
+};
+constexpr uint32_t COL_TREE_DEPTH = 0xFFFFFFFFu;  // stream of the per-tree draw
+bool col_rate_samples(float rate) { return std::fabs(rate - 1.0f) >= 1e-6f; }
+size_t col_sample_count(size_t n, float rate) {
+    const size_t k = (size_t)std::ceil((float)n * rate);
+    return std::min(std::max<size_t>(k, 1), n);
+}
+void col_sample_k(std::vector<uint32_t>& v, size_t k, ColStream& rng) {
+    const size_t n = v.size();
+    if (k >= n) return;
+    for (size_t i = 0; i < k; ++i) std::swap(v[i], v[rng.next() % (n - i) + i]);
+    v.resize(k);
+    std::sort(v.begin(), v.end());
+}
+
 float to_f32(double d) {
     const double lim = 0x1.ffffffp127;
     const double fmax = (double)std::numeric_limits<float>::max();
@@ -305,7 +345,14 @@ class Trainer {
         n_ = p_.n;
         G_ = model.n_groups;
         n_cols_ = p_.n_cols();
-        last_wins_ = (n_threads != 1) && n_cols_ >= 16;  // find.rs:125-129, utils.rs:152
+        // column sampling: every node searches the same number of columns
+        colsample_ = n_cols_ > 0 && (col_rate_samples(cfg.colsample_bytree) || col_rate_samples(cfg.colsample_bylevel));
+        size_t searched = n_cols_;
+        if (col_rate_samples(cfg.colsample_bytree)) searched = col_sample_count(searched, cfg.colsample_bytree);
+        if (col_rate_samples(cfg.colsample_bylevel)) searched = col_sample_count(searched, cfg.colsample_bylevel);
+        // the rayon reduction (last maximal column wins) only from 16 searched
+        // columns (find.rs:125-129, utils.rs:152)
+        last_wins_ = (n_threads != 1) && searched >= 16;
         leafwise_ = cfg.growth_strategy == BST_GROWTH_LEAFWISE;
         const uint32_t max_leaves = leafwise_ ? cfg.max_leaves : (1u << std::min<uint32_t>(cfg.max_depth, 31));
         // batched leaf-wise: room for speculative expansions (grow_leafwise)
@@ -415,6 +462,7 @@ class Trainer {
                 launch_quantize(qmode_, G_, gh_.p, n_, maxabs_.p, cfg_.seed, round_no_, 0u, gq_.p, qscales_.p, st_);
                 m_.counters.launches += 1;
             }
+            tree_round_ = round_no_;  // the round of this round's trees (column sampling)
             ++round_no_;
             timer_.end();
             if (use_batched_) {
@@ -531,6 +579,36 @@ class Trainer {
     uint64_t n_ = 0;
     uint32_t G_ = 1, n_cols_ = 0, max_pnodes_ = 1;
     bool last_wins_ = false, leafwise_ = false;
+    // column sampling: per-depth column masks of the tree being grown
+    // ([depth][n_cols], depth < col_levels_), on the device in d_colmask_
+    bool colsample_ = false;
+    uint32_t col_levels_ = 0;
+    uint32_t tree_round_ = 0;
+    DevArray<uint8_t> d_colmask_;
+    std::vector<std::vector<uint8_t>> h_colmask_;  // per ring slot (or [0]): host copies of the masks
+    const uint8_t* colmask() const { return colsample_ ? d_colmask_.p : nullptr; }
+    // masks of the tree (tree_round_, o) into host buffer `slot`, then to the device
+    void upload_col_masks(uint32_t o, uint32_t slot) {
+        if (!colsample_) return;
+        std::vector<uint32_t> tree_cols(n_cols_);
+        for (uint32_t c = 0; c < n_cols_; ++c) tree_cols[c] = c;
+        if (col_rate_samples(cfg_.colsample_bytree)) {
+            ColStream rng(cfg_.seed, tree_round_, o, COL_TREE_DEPTH);
+            col_sample_k(tree_cols, col_sample_count(tree_cols.size(), cfg_.colsample_bytree), rng);
+        }
+        std::vector<uint8_t>& h = h_colmask_[slot];
+        h.assign((size_t)col_levels_ * n_cols_, 0);
+        for (uint32_t d = 0; d < col_levels_; ++d) {
+            std::vector<uint32_t> lv = tree_cols;
+            if (col_rate_samples(cfg_.colsample_bylevel)) {
+                ColStream rng(cfg_.seed, tree_round_, o, d);
+                col_sample_k(lv, col_sample_count(lv.size(), cfg_.colsample_bylevel), rng);
+            }
+            for (uint32_t c : lv) h[(size_t)d * n_cols_ + c] = 1;
+        }
+        // pageable source: the copy is staged before the call returns
+        BST_CK(cudaMemcpyAsync(d_colmask_.p, h.data(), h.size(), cudaMemcpyHostToDevice, st_));
+    }
     GainParamsDev gp_{};
     Timer timer_;
     Staging stage_;
@@ -673,6 +751,11 @@ class Trainer {
         d_leaves_.alloc(max_pnodes_ + 1);
         stage_.reserve(max_chunks * 48 + (size_t)(max_pnodes_ + 4) * 256 + (1 << 20));
         if (n_cols_) setup_hist_state();
+        if (colsample_) {  // splits happen at depths < max_depth (depth-wise) or < max_leaves (leaf-wise)
+            col_levels_ = std::max<uint32_t>(1, leafwise_ ? cfg_.max_leaves : cfg_.max_depth);
+            d_colmask_.alloc((size_t)col_levels_ * n_cols_);
+            h_colmask_.resize(RING);
+        }
         use_batched_ = cfg_.batched && !leafwise_ && n_cols_ > 0 && cfg_.max_depth <= 14;
         spec_leafwise_ = cfg_.batched && leafwise_ && n_cols_ > 0;
         if (use_batched_ || spec_leafwise_) {
@@ -886,7 +969,8 @@ class Trainer {
         enqueue_hist(gh, ridx_.p, true, tm, launches, hist_launches, true);
         tm.begin(PH_SCAN);
         launch_b_scan(bd_, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p, d_node_tot_.p, 0,
-                      last_wins_ ? 1 : 0, lp, 0u, g_wide, st_, hist32_, d_root_scan_.p);  // + level-0 decisions
+                      last_wins_ ? 1 : 0, lp, 0u, g_wide, st_, hist32_, d_root_scan_.p,
+                      colmask());  // + level-0 decisions
         tm.end();
         launches += 4;
         // row indices: level d partitions R[d & 1] into R[(d + 1) & 1]
@@ -917,8 +1001,9 @@ class Trainer {
                 enqueue_hist(gl, rout, false, tm, launches, hist_launches, (1u << std::min(d, 31u)) <= WIDE_MERGE_NODES);
                 tm.begin(PH_SCAN);
                 launch_b_scan(bd_, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p,
-                              d_node_tot_.p, a ^ 1, last_wins_ ? 1 : 0, lp, (d + 1) & 1u, g_wide, st_,
-                              hist32_);  // + column reduction, next level's decisions
+                              d_node_tot_.p, a ^ 1, last_wins_ ? 1 : 0, lp, (d + 1) & 1u, g_wide, st_, hist32_,
+                              nullptr, colsample_ ? d_colmask_.p + (size_t)(d + 1) * n_cols_ : nullptr);
+                // + column reduction, next level's decisions
                 tm.end();
                 launches += 1;
             } else {
@@ -969,6 +1054,7 @@ class Trainer {
             BST_CK(e);
             graphs_[gi] = ex;
         }
+        upload_col_masks(o, si);  // read by the graph's split searches
         BST_CK(cudaEventRecord(sl.w0, st_));
         BST_CK(cudaGraphLaunch(graphs_[gi], st_));
         BST_CK(cudaEventRecord(sl.w1, st_));
@@ -1122,7 +1208,7 @@ class Trainer {
         upload(h, nodes.size(), d_scan_nodes_);
         timer_.begin(PH_SCAN);
         launch_split_scan(d_scan_nodes_.p, (uint32_t)nodes.size(), scan_cols_.p, n_cols_, hist_.p, slot_bins_,
-                          scale_o_, gp_, d_cand_.p, d_node_tot_.p, st_, hist32_);
+                          scale_o_, gp_, d_cand_.p, d_node_tot_.p, st_, hist32_, colmask());
         launch_split_reduce(d_cand_.p, d_node_tot_.p, (uint32_t)nodes.size(), n_cols_, last_wins_ ? 1 : 0,
                             d_splits_.p, st_);
         timer_.end();
@@ -1331,9 +1417,9 @@ class Trainer {
             // 3. child splits (left, right per parent)
             std::vector<ScanNode> sn;
             sn.reserve(2 * k);
-            for (size_t j = 0; j < k; ++j) {
-                sn.push_back(ScanNode{par[j].node, lc[j], 0u, 0u, 0, 0});
-                sn.push_back(ScanNode{right_ids[j], rc[j], 0u, 0u, 0, 0});
+            for (size_t j = 0; j < k; ++j) {  // pad: the children's depth (column masks)
+                sn.push_back(ScanNode{par[j].node, lc[j], 0u, par[j].depth + 1, 0, 0});
+                sn.push_back(ScanNode{right_ids[j], rc[j], 0u, par[j].depth + 1, 0, 0});
             }
             std::vector<NodeSplit> res;
             scan(sn, res);
@@ -1386,6 +1472,7 @@ class Trainer {
         for (size_t j = 0; j < k; ++j) {
             he[j].left_pnode = par[j].node;
             he[j].right_pnode = right_ids[j];
+            he[j].pad1 = par[j].depth + 1;  // the children's depth (column masks)
         }
         upload(he, k, d_bexp_);
         launch_lw_children(bd_, d_pworks_.p, d_cursors_.p, (uint32_t)k, d_scan_nodes_.p, st_);
@@ -1393,7 +1480,7 @@ class Trainer {
         enqueue_hist(gr_o_, ridx_.p, false, timer_, launches, hist_launches, k <= WIDE_MERGE_NODES);
         timer_.begin(PH_SCAN);
         launch_split_scan(d_scan_nodes_.p, (uint32_t)(2 * k), scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale_o_, gp_,
-                          d_cand_.p, d_node_tot_.p, st_, hist32_);
+                          d_cand_.p, d_node_tot_.p, st_, hist32_, colmask());
         launch_split_reduce(d_cand_.p, d_node_tot_.p, (uint32_t)(2 * k), n_cols_, last_wins_ ? 1 : 0, d_splits_.p, st_);
         timer_.end();
         NodeSplit* hs = stage_.take<NodeSplit>(2 * k);
@@ -1560,6 +1647,7 @@ class Trainer {
         n_pnodes_ = 1;
         stage_.reset();
         timer_.begin(PH_OTHER);
+        upload_col_masks(o, 0);
         launch_iota(ridx_.p, n_, st_);
         if (spec_leafwise_)  // identity order: the positional copy is the row-order array
             BST_CK(cudaMemcpyAsync(qpos_[0].p, qmode_ == GRAD_F32 ? (const void*)gr_o_.gh : gr_o_.gq,

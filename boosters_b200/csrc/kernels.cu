@@ -1268,12 +1268,15 @@ constexpr int SORT_N = 256;  // categorical columns with <= 256 bins
 // One warp: best split of column `col` of node `node` (the node's histogram
 // lives in slot nd.slot); writes cand[node * n_cols + col] and, for column 0,
 // the node totals, and returns the candidate's gain (-inf: none) to every
-// lane. key / cat: this warp's SORT_N-entry shared scratch.
+// lane. key / cat: this warp's SORT_N-entry shared scratch. cmask (or null):
+// the node's column mask (column sampling); a masked column has no
+// candidate.
 template <typename HB>
 __device__ float scan_item(const ScanNode nd, uint32_t node, uint32_t col, const ScanColumn* __restrict__ cols,
                           uint32_t n_cols, const HB* __restrict__ hist, uint64_t slot_bins,
                           const double* __restrict__ scale, const GainParamsDev& gp, ColCand* __restrict__ cand,
-                          long long* __restrict__ node_tot, double* key, uint32_t* cat) {
+                          long long* __restrict__ node_tot, double* key, uint32_t* cat,
+                          const uint8_t* __restrict__ cmask) {
     const int lane = threadIdx.x & 31;
     const ScanColumn cm = cols[col];
     const HB* h = hist + (size_t)nd.slot * slot_bins + cm.hist_off;
@@ -1297,6 +1300,17 @@ __device__ float scan_item(const ScanNode nd, uint32_t node, uint32_t col, const
         node_tot[2 * node] = tg;
         node_tot[2 * node + 1] = th;
     }
+    ColCand* out = cand + (size_t)node * n_cols + col;
+    if (cmask && !cmask[col]) {  // not among the node's sampled columns
+        if (lane == 0) {
+            out->gain = -INFINITY;
+            out->order = 0xFFFFFFFFu;
+            out->bin = 0;
+            out->flags = 0;
+            out->cats[0] = out->cats[1] = out->cats[2] = out->cats[3] = 0ull;
+        }
+        return -INFINITY;
+    }
     const double pg = (double)tg * ig, ph = (double)th * ih;
     GainCtx ctx;
     ctx.lambda = gp.lambda;
@@ -1305,7 +1319,6 @@ __device__ float scan_item(const ScanNode nd, uint32_t node, uint32_t col, const
     ctx.msl = gp.min_samples_leaf;
 
     Best best{-INFINITY, 0xFFFFFFFFu, 0u, 0u};
-    ColCand* out = cand + (size_t)node * n_cols + col;
 
     if (!cm.is_cat) {
         if (nb >= 2) {
@@ -1478,31 +1491,32 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32)
 k_split_scan(const ScanNode* __restrict__ nodes, const ScanColumn* __restrict__ cols,
              uint32_t n_cols, const HB* __restrict__ hist, uint64_t slot_bins,
              const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
-             long long* __restrict__ node_tot, uint32_t col_blocks) {
+             long long* __restrict__ node_tot, uint32_t col_blocks, const uint8_t* __restrict__ colmask) {
     __shared__ double s_key[SCAN_WARPS][SORT_N];
     __shared__ uint32_t s_cat[SCAN_WARPS][SORT_N];
     const int warp = threadIdx.x >> 5;
     const uint32_t col = (blockIdx.x % col_blocks) * SCAN_WARPS + warp;
     const uint32_t node = blockIdx.x / col_blocks;
     if (col >= n_cols) return;
-    scan_item(nodes[node], node, col, cols, n_cols, hist, slot_bins, scale, gp, cand, node_tot, s_key[warp],
-              s_cat[warp]);
+    const ScanNode nd = nodes[node];
+    scan_item(nd, node, col, cols, n_cols, hist, slot_bins, scale, gp, cand, node_tot, s_key[warp], s_cat[warp],
+              colmask ? colmask + (size_t)nd.pad * n_cols : nullptr);
 }
 
 void launch_split_scan(const ScanNode* nodes, uint32_t n_nodes, const ScanColumn* cols,
                        uint32_t n_cols, const void* hist, uint64_t slot_bins,
                        const double* scale, GainParamsDev gp, ColCand* cand,
-                       long long* node_tot, cudaStream_t st, int hist32) {
+                       long long* node_tot, cudaStream_t st, int hist32, const uint8_t* colmask) {
     if (n_nodes == 0 || n_cols == 0) return;
     const uint32_t per = (n_cols + SCAN_WARPS - 1) / SCAN_WARPS;
     const uint64_t blocks = (uint64_t)per * n_nodes;
     if (blocks > 0x7FFFFFFFull) return;
     if (hist32)
         k_split_scan<HBin32><<<(unsigned)blocks, SCAN_WARPS * 32, 0, st>>>(
-            nodes, cols, n_cols, static_cast<const HBin32*>(hist), slot_bins, scale, gp, cand, node_tot, per);
+            nodes, cols, n_cols, static_cast<const HBin32*>(hist), slot_bins, scale, gp, cand, node_tot, per, colmask);
     else
         k_split_scan<HBin><<<(unsigned)blocks, SCAN_WARPS * 32, 0, st>>>(
-            nodes, cols, n_cols, static_cast<const HBin*>(hist), slot_bins, scale, gp, cand, node_tot, per);
+            nodes, cols, n_cols, static_cast<const HBin*>(hist), slot_bins, scale, gp, cand, node_tot, per, colmask);
 }
 
 // Across columns (find.rs:180-212 sequential; :219-270 rayon reduce).
@@ -2250,8 +2264,8 @@ __global__ void __launch_bounds__(1024) k_lw_children(BDev d, const PartWork* __
         e.small_begin = left_small ? w.begin : w.begin + lc;
         e.small_count = left_small ? lc : rc;
         d.exp[j] = e;
-        scan_nodes[2 * j] = ScanNode{e.left_pnode, lc, 0u, 0u, 0, 0};
-        scan_nodes[2 * j + 1] = ScanNode{e.right_pnode, rc, 0u, 0u, 0, 0};
+        scan_nodes[2 * j] = ScanNode{e.left_pnode, lc, 0u, e.pad1, 0, 0};  // pad: the children's depth
+        scan_nodes[2 * j + 1] = ScanNode{e.right_pnode, rc, 0u, e.pad1, 0, 0};
         atomicAdd(&rows, (unsigned long long)e.small_count);
     }
     __syncthreads();
@@ -2380,7 +2394,7 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32)
 k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HB* __restrict__ hist,
          uint64_t slot_bins, const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
          long long* __restrict__ node_tot, int b, int last_wins, LeafParams lp, uint32_t buf,
-         const ScanNode* __restrict__ root) {
+         const ScanNode* __restrict__ root, const uint8_t* __restrict__ colmask) {
     __shared__ double s_key[SCAN_WARPS][SORT_N];
     __shared__ uint32_t s_cat[SCAN_WARPS][SORT_N];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -2391,8 +2405,9 @@ k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HB*
         const uint32_t node = (uint32_t)(it / col_blocks);
         const uint32_t col = (uint32_t)(it % col_blocks) * SCAN_WARPS + warp;
         if (col < n_cols) {
-            const float g = scan_item(root ? root[0] : d.scan_nodes[node], node, col, cols, n_cols, hist, slot_bins,
-                                      scale, gp, cand, node_tot, s_key[warp], s_cat[warp]);
+            const ScanNode nd = root ? root[0] : d.scan_nodes[node];
+            const float g = scan_item(nd, node, col, cols, n_cols, hist, slot_bins, scale, gp, cand, node_tot,
+                                      s_key[warp], s_cat[warp], colmask ? colmask + (size_t)nd.pad * n_cols : nullptr);
             if (lane == 0 && g > -INFINITY) atomicMax(&d.node_key[node], cand_key(g, col, last_wins));
         }
     }
@@ -2429,13 +2444,16 @@ k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HB*
 
 void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const void* hist, uint64_t slot_bins,
                    const double* scale, GainParamsDev gp, ColCand* cand, long long* node_tot, int b, int last_wins,
-                   LeafParams lp, uint32_t buf, uint32_t grid, cudaStream_t st, int hist32, const ScanNode* root) {
+                   LeafParams lp, uint32_t buf, uint32_t grid, cudaStream_t st, int hist32, const ScanNode* root,
+                   const uint8_t* colmask) {
     if (hist32)
         k_b_scan<HBin32><<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, static_cast<const HBin32*>(hist), slot_bins,
-                                                           scale, gp, cand, node_tot, b, last_wins, lp, buf, root);
+                                                           scale, gp, cand, node_tot, b, last_wins, lp, buf, root,
+                                                           colmask);
     else
         k_b_scan<HBin><<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, static_cast<const HBin*>(hist), slot_bins,
-                                                         scale, gp, cand, node_tot, b, last_wins, lp, buf, root);
+                                                         scale, gp, cand, node_tot, b, last_wins, lp, buf, root,
+                                                         colmask);
 }
 
 // This thread's share of the fixed-point sums of positions [start, start +

@@ -180,10 +180,12 @@ struct NodeSplit {
     long long tot_g, tot_h;  // exact fixed-point node totals
 };
 // hist: HBin, or HBin32 when hist32 != 0 (the same for the level kernels below)
+// colmask (or null): [depth][n_cols] column masks (column sampling), a
+// node's row chosen by its depth in ScanNode.pad
 void launch_split_scan(const ScanNode* nodes, uint32_t n_nodes, const ScanColumn* cols,
                        uint32_t n_cols, const void* hist, uint64_t slot_bins,
                        const double* scale, GainParamsDev gp, ColCand* cand,
-                       long long* node_tot, cudaStream_t st, int hist32 = 0);
+                       long long* node_tot, cudaStream_t st, int hist32 = 0, const uint8_t* colmask = nullptr);
 void launch_split_reduce(const ColCand* cand, const long long* node_tot, uint32_t n_nodes,
                          uint32_t n_cols, int last_wins, NodeSplit* out, cudaStream_t st);
 
@@ -351,11 +353,13 @@ void launch_b_root_hist(const BDev& d, uint64_t n, uint32_t chunk, cudaStream_t 
 // frontier b, then (last block) the decisions of the next level, whose rows
 // are in buffer buf
 // root (or null): the level is the root alone, described by *root (rows in
-// buffer 0, frontier 0)
+// buffer 0, frontier 0); colmask (or null): the level's column masks, a
+// node's row chosen by ScanNode.pad (0 for the device-built levels)
 void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const void* hist,
                    uint64_t slot_bins, const double* scale, GainParamsDev gp, ColCand* cand,
                    long long* node_tot, int b, int last_wins, LeafParams lp, uint32_t buf, uint32_t grid,
-                   cudaStream_t st, int hist32 = 0, const ScanNode* root = nullptr);
+                   cudaStream_t st, int hist32 = 0, const ScanNode* root = nullptr,
+                   const uint8_t* colmask = nullptr);
 // last level: the smaller children's sums, then (last block) both children's
 // sums into frontier b
 void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, int b, uint32_t grid, cudaStream_t st);

@@ -99,7 +99,11 @@ typedef struct bst_config {
     float min_gain;         /* default 0.0                                  */
     uint32_t min_samples_leaf; /* default 1                                 */
     /* sampling (only 1.0 is supported by the GPU engine)                   */
-    float subsample;
+    float subsample;         /* default 1; < 1 is BST_ERR_UNSUPPORTED (row sampling) */
+    /* column sampling (training/sampling/column.rs): ceil(n * bytree) of the
+     * columns per tree, ceil(that * bylevel) per depth, searched alone. The
+     * reference draws them from OS entropy; the engine from a stream keyed
+     * by (seed, round, output, depth), so runs repeat. Default 1 (all). */
     float colsample_bytree;
     float colsample_bylevel;
     /* binning */

@@ -642,11 +642,14 @@ struct SplitterCfg {
 };
 
 // find.rs:113-270
+// feats (or null): the node's searched columns in ascending order (column
+// sampling), n_sel of them; null: all n_feat.
 Split find_split(const HBin* hist, const uint32_t* offs, const uint32_t* nb, const uint8_t* is_cat,
                  const uint8_t* has_missing, uint32_t n_feat, double pg, double ph, uint32_t pc,
-                 const SplitterCfg& sc) {
+                 const SplitterCfg& sc, const uint32_t* feats = nullptr, uint32_t n_sel = 0) {
     NodeGainContext ctx(pg * sc.gp.sg, ph * sc.gp.sh, sc.gp);
-    bool par = sc.parallel && n_feat >= 16;  // MIN_FEATURES_PARALLEL (find.rs:18)
+    const uint32_t n_search = feats ? n_sel : n_feat;
+    bool par = sc.parallel && n_search >= 16;  // MIN_FEATURES_PARALLEL over the searched features (find.rs:18,125)
     std::vector<Split> per(n_feat);
     auto eval = [&](uint32_t f) {
         const HBin* bins = hist + offs[f];
@@ -662,14 +665,15 @@ Split find_split(const HBin* hist, const uint32_t* offs, const uint32_t* nb, con
         }
     };
 #ifdef _OPENMP
-    if (sc.omp_threads > 1 && n_feat >= 16) {
+    if (sc.omp_threads > 1 && n_search >= 16) {
 #pragma omp parallel for num_threads(sc.omp_threads) schedule(dynamic, 4)
-        for (int64_t f = 0; f < (int64_t)n_feat; ++f) eval((uint32_t)f);
+        for (int64_t i = 0; i < (int64_t)n_search; ++i) eval(feats ? feats[i] : (uint32_t)i);
     } else
 #endif
-        for (uint32_t f = 0; f < n_feat; ++f) eval(f);
+        for (uint32_t i = 0; i < n_search; ++i) eval(feats ? feats[i] : i);
     Split best;
-    for (uint32_t f = 0; f < n_feat; ++f) {
+    for (uint32_t i = 0; i < n_search; ++i) {
+        const uint32_t f = feats ? feats[i] : i;
         if (par) {
             // reduce(|a, b| if a.gain > b.gain { a } else { b }): ties go to the later item
             if (!(best.gain > per[f].gain)) best = per[f];
@@ -966,7 +970,46 @@ struct TrainCfg {
     bool leafwise = false;
     uint32_t max_depth = 6, max_leaves = 31;
     size_t cache_size = 8;
+    float colsample_bytree = 1.0f, colsample_bylevel = 1.0f;
+    uint64_t seed = 42;
 };
+
+// ---------------------------------------------------------------------------
+// Column sampling (training/sampling/column.rs): the reference seeds it from
+// OS entropy (grower.rs:150-151, column.rs:137-142), so its draws are not
+// reproducible; the engine and this restatement draw from a splitmix64
+// stream keyed by (seed, round, output, depth) and apply the reference's
+// rule: ceil(n * colsample_bytree) columns per tree, ceil(|tree| *
+// colsample_bylevel) of those per depth, by a partial Fisher-Yates shuffle
+// (sample_k_inplace, column.rs:266-283), in ascending order.
+// ---------------------------------------------------------------------------
+static uint64_t cs_mix(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+struct ColRng {
+    uint64_t s;
+    ColRng(uint64_t seed, uint32_t round, uint32_t output, uint32_t depth) {
+        s = cs_mix(seed ^ (0x9E3779B97F4A7C15ull * (1ull + round)));
+        s = cs_mix(s ^ (0xC2B2AE3D27D4EB4Full * (1ull + output)));
+        s = cs_mix(s ^ (0x165667B19E3779F9ull * (1ull + depth)));
+    }
+    uint64_t next() {
+        s += 0x9E3779B97F4A7C15ull;
+        return cs_mix(s);
+    }
+};
+static bool cs_active(float rate) { return std::fabs(rate - 1.0f) >= 1e-6f; }
+static void cs_sample(std::vector<uint32_t>& v, float rate, ColRng rng) {
+    const size_t n = v.size();
+    size_t k = (size_t)std::ceil((float)n * rate);
+    k = std::min(std::max<size_t>(k, 1), n);
+    if (k >= n) return;
+    for (size_t i = 0; i < k; ++i) std::swap(v[i], v[rng.next() % (n - i) + i]);
+    v.resize(k);
+    std::sort(v.begin(), v.end());
+}
 
 struct Grower {
     const orc_binned* ds;
@@ -1036,12 +1079,39 @@ struct Grower {
         return {g, hh};
     }
 
-    Split find(uint32_t node, double g, double h, uint32_t cnt) {  // grower.rs:733-752
+    // column sampling of the tree being grown: its round and output, the
+    // tree's columns and each depth's columns (computed on first use)
+    uint32_t cs_round = 0, cs_output = 0;
+    std::vector<uint32_t> cs_tree;
+    std::vector<std::vector<uint32_t>> cs_level;
+    void cs_begin_tree() {
+        cs_tree.clear();
+        cs_level.clear();
+        if (!cs_active(tc.colsample_bytree) && !cs_active(tc.colsample_bylevel)) return;
+        const uint32_t nc = (uint32_t)ds->col_feature.size();
+        for (uint32_t c = 0; c < nc; ++c) cs_tree.push_back(c);
+        if (cs_active(tc.colsample_bytree))
+            cs_sample(cs_tree, tc.colsample_bytree, ColRng(tc.seed, cs_round, cs_output, 0xFFFFFFFFu));
+    }
+    const std::vector<uint32_t>* cs_features(uint32_t depth) {
+        if (cs_tree.empty()) return nullptr;
+        while (cs_level.size() <= depth) {
+            std::vector<uint32_t> v = cs_tree;
+            if (cs_active(tc.colsample_bylevel))
+                cs_sample(v, tc.colsample_bylevel, ColRng(tc.seed, cs_round, cs_output, (uint32_t)cs_level.size()));
+            cs_level.push_back(std::move(v));
+        }
+        return &cs_level[depth];
+    }
+
+    Split find(uint32_t node, double g, double h, uint32_t cnt, uint32_t depth) {  // grower.rs:733-752
         int s = pool.resolve(node);
         if (s < 0) return Split();
+        const std::vector<uint32_t>* fs = cs_features(depth);
         return find_split(pool.slot_ptr(s), ds->col_offset.data(), ds->col_nbins.data(),
                           ds->col_cat.data(), ds->col_missing.data(),
-                          (uint32_t)ds->col_feature.size(), g, h, cnt, tc.sc);
+                          (uint32_t)ds->col_feature.size(), g, h, cnt, tc.sc, fs ? fs->data() : nullptr,
+                          fs ? (uint32_t)fs->size() : 0u);
     }
 
     void record_leaf(uint32_t tree_node, uint32_t pnode, float w) {  // grower.rs:238-250
@@ -1114,7 +1184,8 @@ struct Grower {
         tree.alloc();  // root = 0
         build_histogram(0);
         auto tot = sum_gradients(0);
-        Split root = find(0, tot.first, tot.second, (uint32_t)n);
+        cs_begin_tree();
+        Split root = find(0, tot.first, tot.second, (uint32_t)n, 0);
         std::vector<Candidate> cur, next, heap;
         Candidate rc{0, 0, 0, root, tot.first, tot.second, (uint32_t)n};
         uint32_t depth = 0, n_leaves = 1;
@@ -1181,8 +1252,8 @@ struct Grower {
             }
             auto ss = sum_gradients(small);
             double lg = c.g - ss.first, lh = c.h - ss.second;
-            Split s_small = find(small, ss.first, ss.second, small_cnt);
-            Split s_large = find(large, lg, lh, large_cnt);
+            Split s_small = find(small, ss.first, ss.second, small_cnt, c.depth + 1);
+            Split s_large = find(large, lg, lh, large_cnt, c.depth + 1);
             Candidate cl, cr;
             if (left_node == small)
                 cl = {left_node, lr.first, c.depth + 1, s_small, ss.first, ss.second, small_cnt};
@@ -1611,9 +1682,8 @@ int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, ui
         g_err = "dataset must have targets for training";
         return BST_ERR_MISSING_TARGETS;
     }
-    if (cfg.subsample != 1.0f || cfg.colsample_bytree != 1.0f || cfg.colsample_bylevel != 1.0f ||
-        cfg.early_stopping_rounds >= 0) {
-        g_err = "row/column sampling and early stopping are outside this restatement";
+    if (cfg.subsample != 1.0f || cfg.early_stopping_rounds >= 0) {
+        g_err = "row sampling and early stopping are outside this restatement";
         return BST_ERR_UNSUPPORTED;
     }
     if (cfg.objective == BST_OBJ_SOFTMAX && cfg.n_classes < 2) {
@@ -1644,6 +1714,9 @@ int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, ui
     tc.max_depth = cfg.max_depth;
     tc.max_leaves = cfg.max_leaves;
     tc.cache_size = cfg.cache_size;
+    tc.colsample_bytree = cfg.colsample_bytree;
+    tc.colsample_bylevel = cfg.colsample_bylevel;
+    tc.seed = cfg.seed;
     Grower gr;
     gr.init(&b, tc);
     uint32_t n_rounds = cfg.n_trees;
@@ -1676,8 +1749,12 @@ int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, ui
                 gr.kh = fixed_point_k(max_abs_finite(ho, n), n);
                 gr.rgrad = go;
                 gr.rhess = ho;
+                gr.cs_round = round;
+                gr.cs_output = o;
                 gr.grow(fqg.data(), fqh.data(), record_leaves != 0);
             } else {
+                gr.cs_round = round;
+                gr.cs_output = o;
                 gr.grow(go, ho, record_leaves != 0);
             }
             gr.update_predictions(m->train_pred.data() + (size_t)o * n);
@@ -1717,6 +1794,9 @@ int orc_grow_tree(const float* x, uint64_t F, uint64_t n, const float* grad, con
     tc.max_depth = cfg.max_depth;
     tc.max_leaves = cfg.max_leaves;
     tc.cache_size = cfg.cache_size;
+    tc.colsample_bytree = cfg.colsample_bytree;
+    tc.colsample_bylevel = cfg.colsample_bylevel;
+    tc.seed = cfg.seed;
     Grower gr;
     gr.init(&b, tc);
     gr.grow(grad, hess, true);

@@ -271,6 +271,47 @@ def test_train_parity_leafwise_budgets(n_leaves, precision, batched):
                   sum_atol=1e-9 if precision == "fp32" else 1e-6)
 
 
+COLSAMPLE_CASES = [
+    # (colsample_bytree, colsample_bylevel, growth, batched, precision, n_threads)
+    (0.5, 0.7, "depthwise", False, "fp32", 1),
+    (0.5, 0.7, "depthwise", True, "fp32", 1),
+    (0.6, 1.0, "depthwise", True, "q8", 1),
+    (1.0, 0.6, "leafwise", True, "fp32", 1),
+    (0.6, 0.8, "leafwise", False, "fp32", 1),
+    (0.9, 1.0, "depthwise", True, "fp32", 0),  # 22 of 24 columns: the parallel tie rule
+    (0.5, 1.0, "depthwise", True, "fp32", 0),  # 12 searched: sequential rule at any n_threads
+]
+
+
+@pytest.mark.parametrize("bytree,bylevel,growth,batched,precision,n_threads", COLSAMPLE_CASES)
+def test_train_parity_column_sampling(bytree, bylevel, growth, batched, precision, n_threads):
+    """Per-tree and per-depth column samples (training/sampling/column.rs)
+    drawn identically by the engine and the oracle; only the sampled
+    columns are searched."""
+    x, y = bst.synth.regression(6000, 24, 8, seed=31)
+    x[5, ::9] = np.nan
+    strat = bst.GrowthStrategy.Leafwise if growth == "leafwise" else bst.GrowthStrategy.Depthwise
+    gm, om, _ = train_both(x, y, n_threads=n_threads, n_estimators=5, learning_rate=0.3, max_depth=5,
+                           growth_strategy=strat, n_leaves=20, colsample_bytree=bytree, colsample_bylevel=bylevel,
+                           precision=precision, batched=batched, seed=7)
+    compare_trees(gm, om, 6000, sum_rtol=1e-9 if precision == "fp32" else 1e-6,
+                  sum_atol=1e-9 if precision == "fp32" else 1e-6)
+
+
+def test_column_sampling_one_column_per_tree():
+    # ceil(24 * 0.01) = 1 column per tree: every split of a tree uses it
+    x, y = bst.synth.regression(4000, 24, 8, seed=32)
+    cfg = _cfg(n_estimators=6, max_depth=4, colsample_bytree=0.01)
+    m = bst.GBDTModel.train(bst.Dataset.from_feature_major(x, y), cfg)
+    used = set()
+    for i in range(m.n_trees):
+        t = m.tree(i)
+        feats = set(t["split_index"][t["is_leaf"] == 0].tolist())
+        assert len(feats) <= 1, feats
+        used |= feats
+    assert len(used) > 1  # different trees draw different columns
+
+
 def test_train_parity_softmax_categorical():
     x, y = bst.synth.multiclass(20_000, 12, 5, 4, seed=4)
     cats = list(range(12, 17))
