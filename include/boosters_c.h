@@ -98,7 +98,7 @@ typedef struct bst_config {
     float min_child_weight; /* default 1.0                                  */
     float min_gain;         /* default 0.0                                  */
     uint32_t min_samples_leaf; /* default 1                                 */
-    /* sampling (only 1.0 is supported by the GPU engine)                   */
+    /* sampling                                                              */
     float subsample;         /* default 1; < 1 is BST_ERR_UNSUPPORTED (row sampling) */
     /* column sampling (training/sampling/column.rs): ceil(n * bytree) of the
      * columns per tree, ceil(that * bylevel) per depth, searched alone. The
