@@ -82,8 +82,6 @@ bst_status check_config(const bst_config* c, bool for_training) {
     if (c->objective < BST_OBJ_SQUARED || c->objective > BST_OBJ_SOFTMAX)
         return fail(BST_ERR_UNSUPPORTED, "objective not supported by the GPU engine");
     if (c->objective == BST_OBJ_SOFTMAX && c->n_classes < 2) return fail(BST_ERR_CONFIG, "softmax needs n_classes >= 2");
-    if (c->subsample != 1.0f)
-        return fail(BST_ERR_UNSUPPORTED, "row subsampling is not supported by the GPU engine");
     if (c->growth_strategy != BST_GROWTH_DEPTHWISE && c->growth_strategy != BST_GROWTH_LEAFWISE)
         return fail(BST_ERR_CONFIG, "unknown growth strategy");
     if (c->growth_strategy == BST_GROWTH_DEPTHWISE && c->max_depth > 24)

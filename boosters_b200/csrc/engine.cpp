@@ -174,6 +174,62 @@ void col_sample_k(std::vector<uint32_t>& v, size_t k, ColStream& rng) {
     std::sort(v.begin(), v.end());
 }
 
+// ---- uniform row sampling (training/sampling/row.rs:168-210) -------------------
+// The reference's generator, restated: rand 0.8's SmallRng on 64-bit targets
+// is Xoshiro256++, seed_from_u64 fills its state with four SplitMix64
+// outputs, and gen_range(0..=i) is UniformInt::sample_single_inclusive (a
+// 64x64 -> 128-bit multiply, rejecting low halves above the zone
+// (range << lz(range)) - 1). sample_uniform keeps k = max(1, trunc(f32(n) *
+// subsample)) rows by reservoir sampling: rows 0..k-1, then row i >= k
+// replaces slot j = gen_range(0..=i) when j < k.
+class RowSampler {
+  public:
+    explicit RowSampler(uint64_t seed) {
+        for (int i = 0; i < 4; ++i) {
+            seed += 0x9E3779B97F4A7C15ull;
+            s_[i] = mix64(seed);
+        }
+    }
+    // the sampled rows of the next call (one call per output and round) as a mask
+    uint64_t sample(uint64_t n, float rate, std::vector<uint8_t>& mask) {
+        uint64_t k = (uint64_t)((float)n * rate);
+        k = std::min<uint64_t>(std::max<uint64_t>(k, 1), n);
+        idx_.resize(k);
+        for (uint64_t i = 0; i < k; ++i) idx_[i] = (uint32_t)i;
+        for (uint64_t i = k; i < n; ++i) {
+            const uint64_t j = range_inclusive(i);
+            if (j < k) idx_[j] = (uint32_t)i;
+        }
+        mask.assign(n, 0);
+        for (uint32_t r : idx_) mask[r] = 1;
+        return k;
+    }
+
+  private:
+    uint64_t s_[4];
+    std::vector<uint32_t> idx_;
+    static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+    uint64_t next() {  // Xoshiro256++
+        const uint64_t r = rotl(s_[0] + s_[3], 23) + s_[0];
+        const uint64_t t = s_[1] << 17;
+        s_[2] ^= s_[0];
+        s_[3] ^= s_[1];
+        s_[1] ^= s_[2];
+        s_[0] ^= s_[3];
+        s_[2] ^= t;
+        s_[3] = rotl(s_[3], 45);
+        return r;
+    }
+    uint64_t range_inclusive(uint64_t high) {  // gen_range(0..=high), high < 2^64 - 1
+        const uint64_t range = high + 1;
+        const uint64_t zone = (range << __builtin_clzll(range)) - 1;
+        for (;;) {
+            const unsigned __int128 m = (unsigned __int128)next() * range;
+            if ((uint64_t)m <= zone) return (uint64_t)(m >> 64);
+        }
+    }
+};
+
 float to_f32(double d) {
     const double lim = 0x1.ffffffp127;
     const double fmax = (double)std::numeric_limits<float>::max();
@@ -456,6 +512,17 @@ class Trainer {
             timer_.begin(PH_GRAD);
             BST_CK(cudaMemsetAsync(maxabs_.p, 0, sizeof(unsigned) * 2 * G_, st_));
             launch_gradients(obj, G_, pred_.p, y_.p, w_.p, n_, gh_.p, maxabs_.p, st_);
+            if (rowsample_) {  // row.rs: per output, zero the rows outside the sample
+                for (uint32_t o = 0; o < G_; ++o) {
+                    n_sampled_[o] = (uint32_t)row_sampler_->sample(n_, cfg_.subsample, h_rowmask_);
+                    BST_CK(cudaMemcpyAsync(d_rowmask_.p + (size_t)o * n_, h_rowmask_.data(), n_, cudaMemcpyHostToDevice,
+                                           st_));  // pageable: staged before the call returns
+                    launch_zero_unsampled(gh_.p + (size_t)o * n_, d_rowmask_.p + (size_t)o * n_, n_, st_);
+                }
+                BST_CK(cudaMemsetAsync(maxabs_.p, 0, sizeof(unsigned) * 2 * G_, st_));
+                for (uint32_t o = 0; o < G_; ++o) launch_maxabs(gh_.p + (size_t)o * n_, n_, maxabs_.p + 2 * o, st_);
+                m_.counters.launches += 2 * G_;
+            }
             launch_fixed_scales(maxabs_.p, G_, n_, scales_.p, st_);
             m_.counters.launches += 2;
             if (qmode_ != GRAD_F32) {
@@ -583,6 +650,15 @@ class Trainer {
     // ([depth][n_cols], depth < col_levels_), on the device in d_colmask_
     bool colsample_ = false;
     uint32_t col_levels_ = 0;
+    // row sampling: per-output masks of the round's sampled rows and their counts
+    bool rowsample_ = false;
+    std::unique_ptr<RowSampler> row_sampler_;
+    DevArray<uint8_t> d_rowmask_;
+    std::vector<uint8_t> h_rowmask_;
+    std::vector<uint32_t> n_sampled_;
+    DevArray<unsigned> d_scnt_;
+    const uint8_t* rowmask(uint32_t o) const { return rowsample_ ? d_rowmask_.p + (size_t)o * n_ : nullptr; }
+    uint32_t tree_output_ = 0;  // the output of the host-driven tree being grown
     uint32_t tree_round_ = 0;
     DevArray<uint8_t> d_colmask_;
     std::vector<std::vector<uint8_t>> h_colmask_;  // per ring slot (or [0]): host copies of the masks
@@ -751,6 +827,15 @@ class Trainer {
         d_leaves_.alloc(max_pnodes_ + 1);
         stage_.reserve(max_chunks * 48 + (size_t)(max_pnodes_ + 4) * 256 + (1 << 20));
         if (n_cols_) setup_hist_state();
+        n_sampled_.assign(G_, (uint32_t)n_);
+        rowsample_ = std::fabs(cfg_.subsample - 1.0f) >= 1e-6f;  // config.rs:329-330
+        if (rowsample_) {
+            row_sampler_ = std::make_unique<RowSampler>(cfg_.seed);
+            d_rowmask_.alloc((size_t)G_ * n_);
+            d_scnt_.alloc(2 * ((size_t)max_pnodes_ + 1));
+            d_bscnt_.alloc(2 * ((size_t)max_pnodes_ + 1));
+            bd_.scnt = d_bscnt_.p;
+        }
         if (colsample_) {  // splits happen at depths < max_depth (depth-wise) or < max_leaves (leaf-wise)
             col_levels_ = std::max<uint32_t>(1, leafwise_ ? cfg_.max_leaves : cfg_.max_depth);
             d_colmask_.alloc((size_t)col_levels_ * n_cols_);
@@ -779,6 +864,7 @@ class Trainer {
     DevArray<BState> d_bstate_;
     DevArray<BNode> d_front_[2];
     DevArray<unsigned long long> d_node_key_;
+    DevArray<unsigned> d_bscnt_;  // row sampling: the level's sampled rows per side (BDev::scnt)
     DevArray<BExp> d_bexp_;
     DevArray<BTreeNode> d_btree_;
     DevArray<BLeaf> d_bleaves_;
@@ -1037,6 +1123,7 @@ class Trainer {
             gtimers_[gi]->enabled = cfg_.phase_timings != 0;
             gtimers_[gi]->reserve(16 + 20 * (size_t)cfg_.max_depth);
             gtimers_[gi]->in_graph = true;
+            bd_.rmask = rowmask(o);  // baked into the graph's kernels
             BST_CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
             try {
                 enqueue_tree(o, *gtimers_[gi], graph_launches_[gi], graph_hist_launches_[gi]);
@@ -1055,6 +1142,10 @@ class Trainer {
             graphs_[gi] = ex;
         }
         upload_col_masks(o, si);  // read by the graph's split searches
+        if (rowsample_) {  // the root's split search counts the sampled rows
+            const ScanNode rs{0, n_sampled_[o], 0u, 0u, 0, 0};
+            BST_CK(cudaMemcpyAsync(d_root_scan_.p, &rs, sizeof(rs), cudaMemcpyHostToDevice, st_));
+        }
         BST_CK(cudaEventRecord(sl.w0, st_));
         BST_CK(cudaGraphLaunch(graphs_[gi], st_));
         BST_CK(cudaEventRecord(sl.w1, st_));
@@ -1360,14 +1451,17 @@ class Trainer {
         std::copy(pch.begin(), pch.end(), hpc);
         upload(hpc, pch.size(), d_pchunks_);
         timer_.begin(PH_PART);
+        if (rowsample_) BST_CK(cudaMemsetAsync(d_scnt_.p, 0, sizeof(unsigned) * 2 * k, st_));
         if (spec_leafwise_) {
             launch_partition(d_pworks_.p, d_pchunks_.p, (uint32_t)pch.size(), ridx_.p, tmp_.p, d_cursors_.p,
-                             b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, st_, qpos_[0].p, qpos_[1].p, qmode_, fm_);
+                             b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, st_, qpos_[0].p, qpos_[1].p, qmode_, fm_,
+                             rowmask(tree_output_), d_scnt_.p);
             launch_copy_chunks(d_pchunks_.p, d_pworks_.p, (uint32_t)pch.size(), tmp_.p, ridx_.p, st_, qpos_[1].p,
                                qpos_[0].p, qmode_);
         } else {
             launch_partition(d_pworks_.p, d_pchunks_.p, (uint32_t)pch.size(), ridx_.p, tmp_.p, d_cursors_.p,
-                             b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, st_);
+                             b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, st_, nullptr, nullptr, 0, BinsFM{},
+                             rowmask(tree_output_), d_scnt_.p);
             launch_copy_chunks(d_pchunks_.p, d_pworks_.p, (uint32_t)pch.size(), tmp_.p, ridx_.p, st_);
         }
         timer_.end();
@@ -1378,7 +1472,10 @@ class Trainer {
             return;
         }
         unsigned* hc = stage_.take<unsigned>(2 * k);
+        unsigned* hsc = stage_.take<unsigned>(2 * k);
         BST_CK(cudaMemcpyAsync(hc, d_cursors_.p, sizeof(unsigned) * 2 * k, cudaMemcpyDeviceToHost, st_));
+        if (rowsample_)
+            BST_CK(cudaMemcpyAsync(hsc, d_scnt_.p, sizeof(unsigned) * 2 * k, cudaMemcpyDeviceToHost, st_));
         BST_CK(cudaStreamSynchronize(st_));
         std::vector<uint32_t> lc(k), rc(k);
         for (size_t j = 0; j < k; ++j) {
@@ -1417,9 +1514,9 @@ class Trainer {
             // 3. child splits (left, right per parent)
             std::vector<ScanNode> sn;
             sn.reserve(2 * k);
-            for (size_t j = 0; j < k; ++j) {  // pad: the children's depth (column masks)
-                sn.push_back(ScanNode{par[j].node, lc[j], 0u, par[j].depth + 1, 0, 0});
-                sn.push_back(ScanNode{right_ids[j], rc[j], 0u, par[j].depth + 1, 0, 0});
+            for (size_t j = 0; j < k; ++j) {  // pad: the children's depth (column masks); counts: sampled rows
+                sn.push_back(ScanNode{par[j].node, rowsample_ ? hsc[2 * j] : lc[j], 0u, par[j].depth + 1, 0, 0});
+                sn.push_back(ScanNode{right_ids[j], rowsample_ ? hsc[2 * j + 1] : rc[j], 0u, par[j].depth + 1, 0, 0});
             }
             std::vector<NodeSplit> res;
             scan(sn, res);
@@ -1475,7 +1572,8 @@ class Trainer {
             he[j].pad1 = par[j].depth + 1;  // the children's depth (column masks)
         }
         upload(he, k, d_bexp_);
-        launch_lw_children(bd_, d_pworks_.p, d_cursors_.p, (uint32_t)k, d_scan_nodes_.p, st_);
+        launch_lw_children(bd_, d_pworks_.p, d_cursors_.p, (uint32_t)k, d_scan_nodes_.p,
+                           rowsample_ ? d_scnt_.p : nullptr, st_);
         uint64_t launches = 1, hist_launches = 0;
         enqueue_hist(gr_o_, ridx_.p, false, timer_, launches, hist_launches, k <= WIDE_MERGE_NODES);
         timer_.begin(PH_SCAN);
@@ -1631,6 +1729,7 @@ class Trainer {
     }
 
     HostTree grow(uint32_t o) {
+        tree_output_ = o;
         gr_o_ = grad_ref(o);
         if (spec_leafwise_) gr_o_.qpos = qpos_[0].p;  // histograms read the positional copy
         gx_o_ = exact_ref(o);
@@ -1670,7 +1769,7 @@ class Trainer {
             e.small_count = (uint32_t)n_;
             host_hist({e}, true);
             std::vector<NodeSplit> res;
-            scan({ScanNode{0, (uint32_t)n_, 0u, 0u, 0, 0}}, res);
+            scan({ScanNode{0, n_sampled_[o], 0u, 0u, 0, 0}}, res);  // sampled rows under row sampling
             root.split = res[0];
             root.G = res[0].tot_g;
             root.H = res[0].tot_h;

@@ -1611,10 +1611,12 @@ __device__ void part_rows(const PartWork& w, uint32_t start, uint32_t len, unsig
                           const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16,
                           uint32_t s16, const Q* __restrict__ qin = nullptr, Q* __restrict__ qout = nullptr,
                           const uint8_t* __restrict__ fm8 = nullptr, const uint16_t* __restrict__ fm16 = nullptr,
-                          uint64_t n_rows = 0) {
+                          uint64_t n_rows = 0, const uint8_t* __restrict__ rmask = nullptr,
+                          unsigned* __restrict__ scnt = nullptr) {
     constexpr bool CARRY = !std::is_same<Q, char>::value;
     __shared__ uint32_t s_l[PART_PER][PART_THREADS / 32], s_r[PART_PER][PART_THREADS / 32];
     __shared__ uint32_t s_base[2];
+    __shared__ uint32_t s_sl[PART_THREADS / 32], s_sr[PART_THREADS / 32];  // sampled rows per side (row sampling)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     for (uint32_t b0 = 0; b0 < len; b0 += PART_THREADS * PART_PER) {
@@ -1654,7 +1656,30 @@ __device__ void part_rows(const PartWork& w, uint32_t start, uint32_t len, unsig
                 s_r[k][warp] = (uint32_t)__popc(rm[k]);
             }
         }
+        if (rmask) {  // row sampling: the children's sampled rows
+            uint32_t sl = 0, sr = 0;
+#pragma unroll
+            for (int k = 0; k < PART_PER; ++k) {
+                const uint32_t i = b0 + k * PART_THREADS + threadIdx.x;
+                const unsigned smp = __ballot_sync(FULL, i < len && rmask[rows[k]] != 0);
+                sl += (uint32_t)__popc(smp & lm[k]);
+                sr += (uint32_t)__popc(smp & rm[k]);
+            }
+            if (lane == 0) {
+                s_sl[warp] = sl;
+                s_sr[warp] = sr;
+            }
+        }
         __syncthreads();
+        if (rmask && warp == 1 && lane == 0) {
+            uint32_t SL = 0, SR = 0;
+            for (int q = 0; q < PART_THREADS / 32; ++q) {
+                SL += s_sl[q];
+                SR += s_sr[q];
+            }
+            if (SL) atomicAdd(&scnt[0], SL);
+            if (SR) atomicAdd(&scnt[1], SR);
+        }
         if (warp == 0) {
             // exclusive scan of the PART_PER x 8 counts in (k, warp) order:
             // lane q holds entries 2q and 2q + 1
@@ -1707,35 +1732,37 @@ __global__ void __launch_bounds__(PART_THREADS)
 k_partition(const PartWork* __restrict__ works, const PartChunk* __restrict__ chunks,
             const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp, unsigned* __restrict__ cursors,
             const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16,
-            const Q* __restrict__ qin, Q* __restrict__ qout, BinsFM fm) {
+            const Q* __restrict__ qin, Q* __restrict__ qout, BinsFM fm, const uint8_t* __restrict__ rmask,
+            unsigned* __restrict__ scnt) {
     const PartChunk ch = chunks[blockIdx.x];
     __shared__ PartWork w;
     if (threadIdx.x == 0) w = works[ch.work];
     __syncthreads();
     part_rows<Q>(w, ch.start, ch.len, cursors + 2 * ch.work, ridx, tmp, bins8, s8, bins16, s16, qin, qout, fm.b8,
-                 fm.b16, fm.n);
+                 fm.b16, fm.n, rmask, rmask ? scnt + 2 * ch.work : nullptr);
 }
 
 void launch_partition(const PartWork* works, const PartChunk* chunks, uint32_t n_chunks,
                       const uint32_t* ridx, uint32_t* tmp, unsigned* cursors,
                       const uint8_t* bins8, uint32_t s8, const uint16_t* bins16, uint32_t s16,
-                      cudaStream_t st, const void* qin, void* qout, int mode, const BinsFM& fm) {
+                      cudaStream_t st, const void* qin, void* qout, int mode, const BinsFM& fm,
+                      const uint8_t* rmask, unsigned* scnt) {
     if (n_chunks == 0) return;
     if (!qin || !qout)
         k_partition<char><<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
-                                                             s16, nullptr, nullptr, fm);
+                                                             s16, nullptr, nullptr, fm, rmask, scnt);
     else if (mode == GRAD_Q8)
         k_partition<char2><<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
                                                               s16, static_cast<const char2*>(qin),
-                                                              static_cast<char2*>(qout), fm);
+                                                              static_cast<char2*>(qout), fm, rmask, scnt);
     else if (mode == GRAD_Q16)
         k_partition<short2><<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
                                                                s16, static_cast<const short2*>(qin),
-                                                               static_cast<short2*>(qout), fm);
+                                                               static_cast<short2*>(qout), fm, rmask, scnt);
     else
         k_partition<float2><<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
                                                                s16, static_cast<const float2*>(qin),
-                                                               static_cast<float2*>(qout), fm);
+                                                               static_cast<float2*>(qout), fm, rmask, scnt);
 }
 
 template <typename Q>
@@ -2018,6 +2045,7 @@ __device__ void decide_body(BDev d, int a, LeafParams lp, const double* __restri
             d.pworks[j] = w;
             d.cursors[2 * j] = nd.begin;
             d.cursors[2 * j + 1] = nd.begin + nd.count;
+            if (d.rmask) d.scnt[2 * j] = d.scnt[2 * j + 1] = 0u;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -2087,7 +2115,7 @@ k_b_partition(BDev d, const uint32_t* __restrict__ ridx, uint32_t* __restrict__ 
         const uint32_t start = w.begin + (c - d.exp[j].part_off) * B_PART_CHUNK;
         const uint32_t len = min(B_PART_CHUNK, w.begin + w.count - start);
         part_rows<Q>(w, start, len, d.cursors + 2 * j, ridx, tmp, bins8, s8, bins16, s16, qin, qout, fm.b8, fm.b16,
-                     fm.n);
+                     fm.n, d.rmask, d.rmask ? d.scnt + 2 * j : nullptr);
     }
     if (last_block(d.state)) children_body(d, a, need_split);
 }
@@ -2186,8 +2214,10 @@ __device__ void children_body(BDev d, int a, int need_split) {
             l.split.tot_g = l.split.tot_h = r.split.tot_g = r.split.tot_h = 0;
             B[2 * j] = l;
             B[2 * j + 1] = r;
-            d.scan_nodes[2 * j] = ScanNode{nd.pnode, lc, 0u, 0u, 0, 0};
-            d.scan_nodes[2 * j + 1] = ScanNode{e.right_pnode, rc, 0u, 0u, 0, 0};
+            // row sampling: the split search counts the sampled rows
+            const uint32_t slc = d.rmask ? d.scnt[2 * j] : lc, src = d.rmask ? d.scnt[2 * j + 1] : rc;
+            d.scan_nodes[2 * j] = ScanNode{nd.pnode, slc, 0u, 0u, 0, 0};
+            d.scan_nodes[2 * j + 1] = ScanNode{e.right_pnode, src, 0u, 0u, 0, 0};
             d.exp[j] = e;
             atomicAdd(&rows, (unsigned long long)e.small_count);
         }
@@ -2245,7 +2275,8 @@ __device__ void children_body(BDev d, int a, int need_split) {
 // read-back. d.exp[j] carries the parents' left_pnode / right_pnode on entry.
 __global__ void __launch_bounds__(1024) k_lw_children(BDev d, const PartWork* __restrict__ pw,
                                                      const unsigned* __restrict__ cursors, uint32_t k,
-                                                     ScanNode* __restrict__ scan_nodes) {
+                                                     ScanNode* __restrict__ scan_nodes,
+                                                     const unsigned* __restrict__ scnt) {
     __shared__ uint32_t sh[33];
     __shared__ unsigned long long rows;
     __shared__ uint32_t chunk, base;
@@ -2264,8 +2295,9 @@ __global__ void __launch_bounds__(1024) k_lw_children(BDev d, const PartWork* __
         e.small_begin = left_small ? w.begin : w.begin + lc;
         e.small_count = left_small ? lc : rc;
         d.exp[j] = e;
-        scan_nodes[2 * j] = ScanNode{e.left_pnode, lc, 0u, e.pad1, 0, 0};  // pad: the children's depth
-        scan_nodes[2 * j + 1] = ScanNode{e.right_pnode, rc, 0u, e.pad1, 0, 0};
+        // pad: the children's depth; counts: sampled rows under row sampling
+        scan_nodes[2 * j] = ScanNode{e.left_pnode, scnt ? scnt[2 * j] : lc, 0u, e.pad1, 0, 0};
+        scan_nodes[2 * j + 1] = ScanNode{e.right_pnode, scnt ? scnt[2 * j + 1] : rc, 0u, e.pad1, 0, 0};
         atomicAdd(&rows, (unsigned long long)e.small_count);
     }
     __syncthreads();
@@ -2298,9 +2330,9 @@ __global__ void __launch_bounds__(1024) k_lw_children(BDev d, const PartWork* __
 }
 
 void launch_lw_children(const BDev& d, const PartWork* pw, const unsigned* cursors, uint32_t k, ScanNode* scan_nodes,
-                        cudaStream_t st) {
+                        const unsigned* scnt, cudaStream_t st) {
     if (k == 0) return;
-    k_lw_children<<<1, 1024, 0, st>>>(d, pw, cursors, k, scan_nodes);
+    k_lw_children<<<1, 1024, 0, st>>>(d, pw, cursors, k, scan_nodes, scnt);
 }
 
 template <typename HB>
@@ -3098,6 +3130,19 @@ void launch_transform(int transform, float* out, uint32_t G, uint64_t n, cudaStr
     if (transform == 0 || n == 0) return;
     const uint64_t total = transform == 1 ? (uint64_t)G * n : n;
     k_transform<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(transform, out, G, n);
+}
+
+// Row sampling: grad/hess of the rows outside the sample become zero
+// (sample_uniform, training/sampling/row.rs:168-210).
+__global__ void k_zero_unsampled(float2* __restrict__ gh, const uint8_t* __restrict__ mask, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (!mask[i]) gh[i] = make_float2(0.0f, 0.0f);
+}
+
+void launch_zero_unsampled(float2* gh, const uint8_t* mask, uint64_t n, cudaStream_t st) {
+    if (n == 0) return;
+    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148ull * 8);
+    k_zero_unsampled<<<(unsigned)blocks, 256, 0, st>>>(gh, mask, n);
 }
 
 __global__ void k_add_f32(float* __restrict__ a, const float* __restrict__ b, uint64_t n) {

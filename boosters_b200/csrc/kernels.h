@@ -217,7 +217,9 @@ void launch_partition(const PartWork* works, const PartChunk* chunks, uint32_t n
                       const uint32_t* ridx, uint32_t* tmp, unsigned* cursors,
                       const uint8_t* bins8, uint32_t s8, const uint16_t* bins16, uint32_t s16,
                       cudaStream_t st, const void* qin = nullptr, void* qout = nullptr, int mode = 0,
-                      const BinsFM& fm = BinsFM{});
+                      const BinsFM& fm = BinsFM{}, const uint8_t* rmask = nullptr, unsigned* scnt = nullptr);
+// rmask (or null): row-sampling mask [n]; then scnt [n_work][2] (zeroed by
+// the caller) gets each work's sampled rows going left / right.
 // copies the chunks' row ids src -> dst and, when qsrc is set, their
 // positional gradient elements qsrc -> qdst
 void launch_copy_chunks(const PartChunk* chunks, const PartWork* works, uint32_t n_chunks,
@@ -299,6 +301,8 @@ struct BDev {  // device buffers of the level loop
     uint32_t hist_target;   // desired histogram row segments per level
     uint32_t hist_seg_max;  // largest row segment (lane_segment_max)
     unsigned long long* node_key;  // [max_front] best candidate key per node; zero between levels
+    const uint8_t* rmask;  // row sampling: the tree's sampled rows [n] (or null)
+    unsigned* scnt;        // row sampling: [max_front][2] sampled rows per side of each expansion
 };
 constexpr uint32_t B_PART_CHUNK = 2048;
 constexpr uint32_t B_LEAF_CHUNK = 4096;
@@ -345,8 +349,10 @@ void launch_b_merge(const BDev& d, void* hist, uint64_t slot_bins, uint32_t tota
 // Batched leaf-wise growth: children counts, smaller children, histogram
 // segments and scan nodes of k partitioned parents (d.exp[j] holds their
 // slots), from the partition's cursors, on the device.
+// scnt (or null): the partition's sampled-row counts (row sampling), used
+// as the children's scan counts
 void launch_lw_children(const BDev& d, const PartWork* pw, const unsigned* cursors, uint32_t k, ScanNode* scan_nodes,
-                        cudaStream_t st);
+                        const unsigned* scnt, cudaStream_t st);
 // Level state of the root histogram: all n rows as one segment list.
 void launch_b_root_hist(const BDev& d, uint64_t n, uint32_t chunk, cudaStream_t st);
 // split finding of the level's nodes and the reduction over columns into
@@ -453,5 +459,7 @@ void launch_predict_heap(const HeapForest& f, const float* x, uint64_t n, uint32
 void launch_transform(int transform, float* out, uint32_t G, uint64_t n, cudaStream_t st);
 // a[i] = a[i] + b[i] (f32), i < n
 void launch_add_f32(float* a, const float* b, uint64_t n, cudaStream_t st);
+// gh[i] = (0, 0) where mask[i] == 0 (row sampling), i < n
+void launch_zero_unsampled(float2* gh, const uint8_t* mask, uint64_t n, cudaStream_t st);
 
 }  // namespace bst

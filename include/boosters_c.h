@@ -99,7 +99,10 @@ typedef struct bst_config {
     float min_gain;         /* default 0.0                                  */
     uint32_t min_samples_leaf; /* default 1                                 */
     /* sampling                                                              */
-    float subsample;         /* default 1; < 1 is BST_ERR_UNSUPPORTED (row sampling) */
+    /* uniform row sampling (training/sampling/row.rs:168-210; the reference's
+     * generator restated, seeded by `seed`): per output and round, rows
+     * outside the sample get zero grad/hess. Default 1 (all rows). */
+    float subsample;
     /* column sampling (training/sampling/column.rs): ceil(n * bytree) of the
      * columns per tree, ceil(that * bylevel) per depth, searched alone. The
      * reference draws them from OS entropy; the engine from a stream keyed

@@ -18,6 +18,7 @@
 #include <string>
 #include <unordered_map>
 #include <unordered_set>
+#include <memory>
 #include <vector>
 
 #ifdef _OPENMP
@@ -1001,6 +1002,54 @@ struct ColRng {
     }
 };
 static bool cs_active(float rate) { return std::fabs(rate - 1.0f) >= 1e-6f; }
+
+// Uniform row sampling (training/sampling/row.rs:168-210) with the
+// reference's generator: rand 0.8 SmallRng = Xoshiro256++ seeded by four
+// SplitMix64 outputs (seed_from_u64), gen_range(0..=i) by
+// UniformInt::sample_single_inclusive (128-bit multiply, zone rejection),
+// reservoir sampling of k = max(1, trunc(f32(n) * rate)) rows.
+struct OracleRowSampler {
+    uint64_t s[4];
+    explicit OracleRowSampler(uint64_t seed) {
+        for (int i = 0; i < 4; ++i) {
+            seed += 0x9E3779B97F4A7C15ull;
+            s[i] = cs_mix(seed);
+        }
+    }
+    static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+    uint64_t next() {
+        const uint64_t r = rotl(s[0] + s[3], 23) + s[0];
+        const uint64_t t = s[1] << 17;
+        s[2] ^= s[0];
+        s[3] ^= s[1];
+        s[1] ^= s[2];
+        s[0] ^= s[3];
+        s[2] ^= t;
+        s[3] = rotl(s[3], 45);
+        return r;
+    }
+    uint64_t gen_range_inclusive(uint64_t high) {
+        const uint64_t range = high + 1;
+        const uint64_t zone = (range << __builtin_clzll(range)) - 1;
+        for (;;) {
+            const unsigned __int128 m = (unsigned __int128)next() * range;
+            if ((uint64_t)m <= zone) return (uint64_t)(m >> 64);
+        }
+    }
+    uint64_t sample(uint64_t n, float rate, std::vector<uint8_t>& mask) {
+        uint64_t k = (uint64_t)((float)n * rate);
+        k = std::min<uint64_t>(std::max<uint64_t>(k, 1), n);
+        std::vector<uint32_t> idx(k);
+        for (uint64_t i = 0; i < k; ++i) idx[i] = (uint32_t)i;
+        for (uint64_t i = k; i < n; ++i) {
+            const uint64_t j = gen_range_inclusive(i);
+            if (j < k) idx[j] = (uint32_t)i;
+        }
+        mask.assign(n, 0);
+        for (uint32_t r : idx) mask[r] = 1;
+        return k;
+    }
+};
 static void cs_sample(std::vector<uint32_t>& v, float rate, ColRng rng) {
     const size_t n = v.size();
     size_t k = (size_t)std::ceil((float)n * rate);
@@ -1077,6 +1126,21 @@ struct Grower {
             hh += h[i].second;
         }
         return {g, hh};
+    }
+
+    // row sampling: the tree's sampled rows (null: all). The reference's
+    // partition holds only the sampled rows (grower.rs:275-276); here every
+    // row stays and the others carry zero grad/hess, which adds exact zeros to
+    // every f64 sum, while node counts (split validity, smaller child) count
+    // the sampled rows as the reference's do.
+    const uint8_t* rmask = nullptr;
+    uint32_t n_sampled = 0;
+    uint32_t sampled_in(uint32_t node) const {
+        const uint32_t b = part.begin[node], c = part.count[node];
+        if (!rmask) return c;
+        uint32_t k = 0;
+        for (uint32_t i = 0; i < c; ++i) k += rmask[part.indices[b + i]] != 0;
+        return k;
     }
 
     // column sampling of the tree being grown: its round and output, the
@@ -1185,9 +1249,10 @@ struct Grower {
         build_histogram(0);
         auto tot = sum_gradients(0);
         cs_begin_tree();
-        Split root = find(0, tot.first, tot.second, (uint32_t)n, 0);
+        const uint32_t root_cnt = rmask ? n_sampled : (uint32_t)n;
+        Split root = find(0, tot.first, tot.second, root_cnt, 0);
         std::vector<Candidate> cur, next, heap;
-        Candidate rc{0, 0, 0, root, tot.first, tot.second, (uint32_t)n};
+        Candidate rc{0, 0, 0, root, tot.first, tot.second, root_cnt};
         uint32_t depth = 0, n_leaves = 1;
         if (tc.leafwise)
             heap.push_back(rc);
@@ -1235,6 +1300,10 @@ struct Grower {
                 if (!s.categorical) return bin <= s.bin;
                 return std::binary_search(s.left_cats.begin(), s.left_cats.end(), bin);
             }, lc, rcnt);
+            if (rmask) {  // counts of the sampled rows
+                lc = sampled_in(c.node);
+                rcnt = sampled_in(right_node);
+            }
             uint32_t left_node = c.node, parent = c.node;
             bool left_small = lc <= rcnt;
             uint32_t small = left_small ? left_node : right_node;
@@ -1682,8 +1751,8 @@ int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, ui
         g_err = "dataset must have targets for training";
         return BST_ERR_MISSING_TARGETS;
     }
-    if (cfg.subsample != 1.0f || cfg.early_stopping_rounds >= 0) {
-        g_err = "row sampling and early stopping are outside this restatement";
+    if (cfg.early_stopping_rounds >= 0) {
+        g_err = "early stopping is outside this restatement";
         return BST_ERR_UNSUPPORTED;
     }
     if (cfg.objective == BST_OBJ_SOFTMAX && cfg.n_classes < 2) {
@@ -1724,6 +1793,10 @@ int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, ui
     const bool quant = cfg.precision != BST_PRECISION_FP32;
     std::vector<int32_t> qg, qh;
     std::vector<float> fqg, fqh;
+    // row sampling (config.rs:329-330: a rate within 1e-6 of 1 samples nothing)
+    std::unique_ptr<OracleRowSampler> row_sampler;
+    std::vector<uint8_t> row_mask;
+    if (std::fabs(cfg.subsample - 1.0f) >= 1e-6f) row_sampler = std::make_unique<OracleRowSampler>(cfg.seed);
     if (quant) {
         qg.resize(n);
         qh.resize(n);
@@ -1734,6 +1807,12 @@ int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, ui
         auto tr0 = std::chrono::steady_clock::now();
         gradients(cfg.objective, G, m->train_pred.data(), y, w, n, grad.data(), hess.data());
         for (uint32_t o = 0; o < G && built < max_trees; ++o) {
+            if (row_sampler) {  // row.rs:141-210: zero the grad/hess of the rows outside the sample
+                gr.n_sampled = (uint32_t)row_sampler->sample(n, cfg.subsample, row_mask);
+                gr.rmask = row_mask.data();
+                for (uint64_t i = 0; i < n; ++i)
+                    if (!row_mask[i]) grad[(size_t)o * n + i] = hess[(size_t)o * n + i] = 0.0f;
+            }
             const float* go = grad.data() + (size_t)o * n;
             const float* ho = hess.data() + (size_t)o * n;
             if (quant) {

@@ -119,7 +119,7 @@ def test_training_rejects_unsupported_options():
     x, y = bst.synth.regression(100, 5, 2)
     ds = bst.Dataset.from_feature_major(x, y)
     with pytest.raises(bst.BoostersError) as e:
-        bst.GBDTModel.train(ds, bst.GBDTConfig(subsample=0.5))
+        bst.GBDTModel.train(ds, bst.GBDTConfig(max_depth=30))
     assert e.value.status == n.BST_ERR_UNSUPPORTED
     with pytest.raises(bst.BoostersError) as e:
         bst.GBDTModel.train(bst.Dataset.from_feature_major(x), bst.GBDTConfig())

@@ -298,6 +298,41 @@ def test_train_parity_column_sampling(bytree, bylevel, growth, batched, precisio
                   sum_atol=1e-9 if precision == "fp32" else 1e-6)
 
 
+ROWSAMPLE_CASES = [
+    # (subsample, growth, batched, precision, objective)
+    (0.5, "depthwise", False, "fp32", "squared"),
+    (0.5, "depthwise", True, "fp32", "squared"),
+    (0.3, "depthwise", True, "q8", "logistic"),
+    (0.6, "leafwise", True, "fp32", "squared"),
+    (0.6, "leafwise", False, "fp32", "logistic"),
+    (0.7, "depthwise", True, "fp32", "softmax"),
+]
+
+
+@pytest.mark.parametrize("subsample,growth,batched,precision,objective", ROWSAMPLE_CASES)
+def test_train_parity_row_sampling(subsample, growth, batched, precision, objective):
+    """Uniform row sampling (training/sampling/row.rs): the same reservoir
+    sample per output and round in the engine and the oracle; unsampled rows
+    carry zero grad/hess and node counts are sampled counts."""
+    if objective == "softmax":
+        x, y = bst.synth.multiclass(5000, 10, 0, 3, seed=33)
+        obj = bst.Objective.softmax(3)
+    elif objective == "logistic":
+        x, y = bst.synth.binary(5000, 16, 3, seed=34)
+        obj = bst.Objective.logistic()
+    else:
+        x, y = bst.synth.regression(5000, 16, 6, seed=35)
+        obj = bst.Objective.squared()
+    strat = bst.GrowthStrategy.Leafwise if growth == "leafwise" else bst.GrowthStrategy.Depthwise
+    gm, om, _ = train_both(x, y, objective=obj, n_estimators=5, learning_rate=0.3, max_depth=5,
+                           growth_strategy=strat, n_leaves=20, subsample=subsample, min_samples_leaf=30,
+                           precision=precision, batched=batched, seed=9,
+                           colsample_bytree=0.8 if objective == "softmax" else 1.0)
+    tol = 1e-9 if (precision == "fp32" and objective == "squared") else 1e-6
+    compare_trees(gm, om, 5000, sum_rtol=tol, sum_atol=tol)
+    np.testing.assert_allclose(gm.train_predictions(), om.train_predictions(), rtol=REL, atol=1e-6)
+
+
 def test_column_sampling_one_column_per_tree():
     # ceil(24 * 0.01) = 1 column per tree: every split of a tree uses it
     x, y = bst.synth.regression(4000, 24, 8, seed=32)
