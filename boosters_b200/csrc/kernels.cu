@@ -2065,14 +2065,6 @@ __device__ void decide_body(BDev d, int a, LeafParams lp, const double* __restri
     }
 }
 
-__global__ void __launch_bounds__(1024) k_b_decide(BDev d, int a, LeafParams lp, const double* __restrict__ scale,
-                                                  uint32_t buf) {
-    decide_body(d, a, lp, scale, buf);
-}
-
-void launch_b_decide(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st) {
-    k_b_decide<<<1, 1024, 0, st>>>(d, a, lp, scale, buf);
-}
 
 
 // "Last block" hand-off: every block of the launch counts itself in

@@ -311,12 +311,12 @@ constexpr uint32_t B_LEAF_CHUNK = 4096;
 // (call once per device before any stream capture).
 void init_kernel_attributes();
 void launch_b_root(const BDev& d, uint64_t n, cudaStream_t st);
-// Row indices alternate between two buffers: level d partitions buffer d & 1
-// into buffer (d + 1) & 1; a leaf records the buffer that holds its rows.
-// level kernels; `a` is the index of the current frontier buffer
-void launch_b_decide(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st);
+// Column-major copy of the bin matrices (BinsFM).
 void launch_transpose_bins(const uint8_t* b8, uint32_t s8, const uint16_t* b16, uint32_t s16, uint64_t n,
                            uint8_t* fm8, uint16_t* fm16, cudaStream_t st);
+// Level kernels; `a` is the index of the current frontier buffer. Row indices
+// alternate between two buffers: level d partitions buffer d & 1 into buffer
+// (d + 1) & 1; a leaf records the buffer that holds its rows.
 // partition rin -> rout, then (last block) the children of every split;
 // qin / qout (grad_elem_bytes(mode) each, or null) move each row's gradient
 // element with its row id; fm: the split columns are read column-major
