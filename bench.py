@@ -150,7 +150,7 @@ def run_reference(args, world, rank):
     # bounded sample: one round estimates the cost, then as many timed rounds
     # (of the K asked for) as about a minute of CPU work allows
     probe = cpu_baseline(1, cores, x, y)[0]
-    k = max(2, min(args.steps, int(60.0 / max(probe, 1e-3))))
+    k = max(1, min(args.steps, int(60.0 / max(probe, 1e-3))))
     secs = cpu_baseline(1 + k, cores, x, y)
     timed = secs[1:]
     v = 100.0 * sum(timed) / len(timed)
