@@ -1991,3 +1991,19 @@ int orc_predict_rows(const orc_model* m, const float* x, uint64_t F, uint64_t n,
 }
 
 }  // extern "C"
+
+// Known-answer and cross-language checks of the row sampler's generator.
+extern "C" void orc_xoshiro256pp(const uint64_t state[4], uint32_t n, uint64_t* out) {
+    OracleRowSampler r(0);
+    for (int i = 0; i < 4; ++i) r.s[i] = state[i];
+    for (uint32_t i = 0; i < n; ++i) out[i] = r.next();
+}
+
+extern "C" void orc_row_sample(uint64_t seed, uint64_t n, float rate, uint32_t draws, uint8_t* masks) {
+    OracleRowSampler r(seed);
+    std::vector<uint8_t> m;
+    for (uint32_t d = 0; d < draws; ++d) {
+        r.sample(n, rate, m);
+        std::copy(m.begin(), m.end(), masks + (size_t)d * n);
+    }
+}

@@ -134,6 +134,12 @@ int orc_model_add_tree(orc_model* m, uint32_t group, uint32_t n_nodes, const uin
 
 const char* orc_last_error(void);
 
+/* Row-sampling generator (test infrastructure): n raw Xoshiro256++ outputs
+ * from `state`, and `draws` consecutive uniform row samples (masks
+ * [draws][n]) of a sampler seeded with `seed` (training/sampling/row.rs). */
+void orc_xoshiro256pp(const uint64_t state[4], uint32_t n, uint64_t* out);
+void orc_row_sample(uint64_t seed, uint64_t n, float rate, uint32_t draws, uint8_t* masks);
+
 #ifdef __cplusplus
 }
 #endif

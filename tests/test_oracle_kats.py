@@ -184,3 +184,81 @@ def test_sparse_feature_is_rejected():
     x[1, :5] = 1.0
     with pytest.raises(RuntimeError, match="sparse"):
         ob.OracleBinned(x, GBDTConfig().to_c())
+
+
+# ---- row-sampling generator (training/sampling/row.rs) ------------------------
+# The engine and the oracle each restate rand 0.8's SmallRng (Xoshiro256++
+# seeded by SplitMix64) and gen_range(0..=i); these check the oracle's copy
+# against values derived from the published algorithms and against a third,
+# pure-Python statement of the reservoir sampler.
+
+M64 = (1 << 64) - 1
+
+
+def _rotl(v, k):
+    return ((v << k) | (v >> (64 - k))) & M64
+
+
+class _PySampler:
+    def __init__(self, seed):
+        self.s = []
+        for _ in range(4):
+            seed = (seed + 0x9E3779B97F4A7C15) & M64
+            z = ((seed ^ (seed >> 30)) * 0xBF58476D1CE4E5B9) & M64
+            z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M64
+            self.s.append(z ^ (z >> 31))
+
+    def next(self):
+        s = self.s
+        r = (_rotl((s[0] + s[3]) & M64, 23) + s[0]) & M64
+        t = (s[1] << 17) & M64
+        s[2] ^= s[0]
+        s[3] ^= s[1]
+        s[1] ^= s[2]
+        s[0] ^= s[3]
+        s[2] ^= t
+        s[3] = _rotl(s[3], 45)
+        return r
+
+    def range_inclusive(self, high):
+        rng = high + 1
+        zone = ((rng << (64 - rng.bit_length())) & M64) - 1
+        while True:
+            m = self.next() * rng
+            if (m & M64) <= zone:
+                return m >> 64
+
+    def sample(self, n, rate):
+        k = min(max(int(np.float32(n) * np.float32(rate)), 1), n)
+        idx = list(range(k))
+        for i in range(k, n):
+            j = self.range_inclusive(i)
+            if j < k:
+                idx[j] = i
+        mask = np.zeros(n, np.uint8)
+        mask[idx] = 1
+        return mask
+
+
+def test_xoshiro256pp_known_answers():
+    import ctypes
+    state = (ctypes.c_uint64 * 4)(1, 2, 3, 4)
+    out = (ctypes.c_uint64 * 3)()
+    ob.lib.orc_xoshiro256pp(state, 3, out)
+    # rotl(1 + 4, 23) + 1, then the second step worked by hand
+    assert list(out) == [41943041, 58720359, 3588806011781223]
+    assert _PySampler(0).s[0] == 0xE220A8397B1DCDAF  # SplitMix64(0), first output
+
+
+@pytest.mark.parametrize("n,rate,seed", [(50, 0.2, 42), (1000, 0.5, 7), (333, 0.9, 0), (10, 0.01, 3)])
+def test_row_sampler_matches_python_statement(n, rate, seed):
+    import ctypes
+    draws = 3
+    masks = np.zeros((draws, n), np.uint8)
+    ob.lib.orc_row_sample(ctypes.c_uint64(seed), ctypes.c_uint64(n), ctypes.c_float(rate), draws,
+                          masks.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+    py = _PySampler(seed)
+    for d in range(draws):
+        want = py.sample(n, rate)
+        np.testing.assert_array_equal(masks[d], want, err_msg=f"draw {d}")
+        assert masks[d].sum() == min(max(int(np.float32(n) * np.float32(rate)), 1), n)
