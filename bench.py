@@ -12,8 +12,14 @@ copy, H2D, binning, 100 trees, D2H of the training predictions).
 With --gpus N (torchrun) every rank trains an independent replica on its own
 row stream (training does not shard; no collective on the data path).
 
+The other survey workloads (5k x 100 regression, 10M x 200 leaf-wise
+logistic, 2M x 50 softmax with categorical columns) are timed after the
+headline in every form, each with its held-out loss and equal-loss flag
+(`configs`; --no-configs skips them).
+
 --impl reference times the CPU restatement of the reference's path (the Rust
-crate cannot be built here) with all host threads, rank 0 only.
+crate cannot be built here), compiled -O3 -march=native on the host that runs
+it, with all host threads, rank 0 only; that process loads no engine library.
 """
 import argparse
 import json
@@ -31,6 +37,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "train s/100 trees, predict rows/s, p99 serve ms vs plain GPU at equal loss"
 UNIT = "s/100 trees"
+E2E_UNIT = "s/100 trees (from host arrays, binning included)"
 N_ROWS, N_FEAT, N_NAN, SEED = 1_000_000, 100, 20, 2
 WORKLOAD = "binary-logistic GBDT 1,000,000x100 f32 (20 NaN cols), depth 8, 256 bins, lr 0.1, 500 trees"
 DTYPES = {"plain": "f32 grad/hess, int64 fixed-point histograms",
@@ -131,37 +138,75 @@ def whole_job_value(world, elapsed_s, steps):
     return 100.0 * reduce_max(world, elapsed_s) / (steps * world)
 
 
-def cpu_baseline(n_rounds, n_threads, x, y):
-    """The CPU restatement on the same workload: per-tree seconds (binning excluded)."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import boosters_b200 as bst
-    import oracle_bridge as ob
-    cfg = bst.GBDTConfig(**cfg_kwargs()).to_c()
+def oracle_native():
+    """Build the CPU restatement at -O3 -march=native for this host (once per
+    host CPU) and point the checker bridge at it. Returns a description of
+    the build. Must run before `oracle_bridge` is imported."""
+    import hashlib
+    sig_src = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith(("model name", "flags")):
+                    sig_src += line
+                if line.strip() == "":
+                    break
+    except OSError:
+        pass
+    sig = hashlib.sha1(sig_src.encode()).hexdigest()[:12]
+    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "native", f"NATIVE_DIR=_native/{sig}"],
+                       capture_output=True, text=True)
+    lib = os.path.join(ROOT, "oracle", "_native", sig, "liboracle.so")
+    if r.returncode == 0 and os.path.exists(lib):
+        os.environ["BST_ORACLE_LIB"] = lib
+        return "g++ -O3 -march=native -fopenmp (built on this host)"
+    return "g++ -O3 -fopenmp (portable build; the host-tuned build failed)"
+
+
+def cpu_rounds(ob, n_rounds, n_threads, x, y, cfg):
+    """The CPU restatement on one workload: (per-tree seconds, binning
+    seconds). n_threads=0: the reference's default parallel semantics."""
     m = ob.OracleModel(x, y, cfg, n_threads=0, record_leaves=False, omp_threads=n_threads, max_trees=n_rounds)
-    return [ob.lib.orc_model_tree_seconds(m._h, t) for t in range(m.n_trees)]
+    return ([ob.lib.orc_model_tree_seconds(m._h, t) for t in range(m.n_trees)],
+            ob.lib.orc_model_binning_seconds(m._h))
+
+
+def bounded_cpu_rounds(ob, budget_s, max_rounds, n_threads, x, y, cfg):
+    """1 warm-up round plus as many timed rounds (at most max_rounds) as
+    about budget_s of CPU work allows. Returns (timed per-tree seconds,
+    binning seconds)."""
+    probe, _ = cpu_rounds(ob, 1, n_threads, x, y, cfg)
+    k = max(1, min(max_rounds, int(budget_s / max(probe[0], 1e-3))))
+    secs, bin_s = cpu_rounds(ob, 1 + k, n_threads, x, y, cfg)
+    return secs[1:], bin_s
+
+
+def oracle_cfg(ob):
+    return ob.config(objective=1, n_trees=500, learning_rate=0.1, max_depth=8, max_bins=256, metric=0)
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    import boosters_b200 as bst
-    x, y = bst.synth.binary(N_ROWS, N_FEAT, N_NAN, seed=SEED, stream=0)
+    build = oracle_native()
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bridge as ob  # noqa: E402  (after BST_ORACLE_LIB is set)
+    x, y = ob.synth.binary(N_ROWS, N_FEAT, N_NAN, seed=SEED, stream=0)
     cores = os.cpu_count() or 1
-    # bounded sample: one round estimates the cost, then as many timed rounds
-    # (of the K asked for) as about a minute of CPU work allows
-    probe = cpu_baseline(1, cores, x, y)[0]
-    k = max(1, min(args.steps, int(60.0 / max(probe, 1e-3))))
-    secs = cpu_baseline(1 + k, cores, x, y)
-    timed = secs[1:]
-    v = 100.0 * sum(timed) / len(timed)
-    sample = (f"1 warm-up + {k} timed boosting rounds (of {args.steps} asked) of the {N_ROWS}x{N_FEAT} workload, "
-              f"binning excluded, {cores} threads")
+    timed, bin_s = bounded_cpu_rounds(ob, 60.0, args.steps, cores, x, y, oracle_cfg(ob))
+    per_tree = sum(timed) / len(timed)
+    v = 100.0 * per_tree
+    sample = (f"1 warm-up + {len(timed)} timed boosting rounds (of {args.steps} asked) of the {N_ROWS}x{N_FEAT} "
+              f"workload, binning excluded, {cores} threads; {build}")
+    e2e = bin_s + v
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * sum(timed) / len(timed), 3),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * per_tree, 3),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "parallelism": "cpu threads"},
             "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
-            "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": round(e2e, 4), "unit": E2E_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                    "includes": f"binning from host arrays ({bin_s:.2f} s, measured) + 100 trees at the timed "
+                                f"per-tree rate"}}
     print(json.dumps(line), flush=True)
 
 
@@ -371,15 +416,19 @@ def run_ours(args, world, rank, local):
             serving = {"error": str(ex)}
 
     extra = None
-    if args.configs and rank == 0:
+    if not args.no_configs and rank == 0 and world == 1:
         extra = run_configs(bst, torch)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        build = oracle_native()
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_bridge as ob  # noqa: E402  (after BST_ORACLE_LIB is set)
         cores = os.cpu_count() or 1
-        secs = cpu_baseline(2, cores, x, y)
-        cpu = {"value": round(100.0 * sum(secs) / len(secs), 3), "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"2 boosting rounds of the {N_ROWS}x{N_FEAT} workload, binning excluded"}
+        timed, _ = bounded_cpu_rounds(ob, 15.0, 40, cores, x, y, oracle_cfg(ob))
+        cpu = {"value": round(100.0 * sum(timed) / len(timed), 3), "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"1 warm-up + {len(timed)} timed boosting rounds of the {N_ROWS}x{N_FEAT} workload, "
+                         f"binning excluded; {build}"}
 
     if rank == 0:
         line = {
@@ -399,8 +448,10 @@ def run_ours(args, world, rank, local):
                          "avg_launch_ms": round(hist_ms / hist_launches, 5),
                          "algorithmic_bytes_per_launch": round(hist_bytes / hist_launches)},
             "cpu_baseline": cpu,
-            "e2e": {"value": round(e2e_value, 4), "unit": "s/100 trees (host buffers, binning + H2D + D2H included)",
-                    "h2d_bytes_per_step": int(x.nbytes + y.nbytes), "d2h_bytes_per_step": int(N_ROWS * 4)},
+            "e2e": {"value": round(e2e_value, 4), "unit": E2E_UNIT,
+                    "h2d_bytes_per_step": int(x.nbytes + y.nbytes), "d2h_bytes_per_step": int(N_ROWS * 4),
+                    "includes": "public train call from pinned host arrays: dataset, binning, H2D, 100 trees, "
+                                "D2H of the training predictions"},
             "gpu_launches": int(launches),
             "clocks": clk,
             "predict_rows_per_s": rows_pred,
@@ -414,8 +465,8 @@ def run_ours(args, world, rank, local):
 
 
 def time_trees(bst, torch, ds, cfg, warm, steps):
-    """s/100 trees of `steps` timed trees after `warm` (CUDA events on the
-    engine's stream), then the rest of cfg's trees; returns (value, model)."""
+    """s/100 trees of `steps` timed rounds after `warm` (CUDA events on the
+    engine's stream), then the rest of cfg's rounds; returns (value, model)."""
     booster = bst.Booster(ds, cfg, n_threads=0)
     booster.update(warm)
     torch.cuda.synchronize()
@@ -432,55 +483,62 @@ def time_trees(bst, torch, ds, cfg, warm, steps):
     return 100.0 * per_round / trees_per_round, booster.model()
 
 
-def run_configs(bst, torch):
-    """The survey's other workloads, each in its plain form and its fast form
-    at equal loss: config 1 (5k x 100 regression), config 3 (10M x 200
-    leaf-wise 255 leaves; plain, batched FP32 and batched Q8), config 4 (2M x
-    50 softmax with 10 categorical columns, 10 classes)."""
+def config_forms(bst, torch, ds, kw, forms, warm, steps, heldout):
+    """Every form of one workload: s/100 trees, held-out loss, loss relative
+    to the plain form and the equal-loss flag (|rel| <= 1e-3); the fast form
+    is the fastest form at equal loss."""
     out = {}
-    # config 1
+    for name in forms:
+        v, m = time_trees(bst, torch, ds, bst.GBDTConfig(**kw, **dict(FORMS)[name]), warm, steps)
+        out[name] = {"s_per_100_trees": round(v, 5), "heldout_loss": round(heldout(m), 6), "trees": m.n_trees}
+        del m
+    plain = out["plain"]["heldout_loss"]
+    for r in out.values():
+        r["loss_rel_vs_plain"] = round((r["heldout_loss"] - plain) / plain, 6)
+        r["equal_loss"] = abs(r["heldout_loss"] - plain) <= EQUAL_LOSS_REL * plain
+    fast = min((k for k in out if out[k]["equal_loss"]), key=lambda k: out[k]["s_per_100_trees"])
+    return {"forms": out, "fast_form": fast,
+            "speedup_vs_plain": round(out["plain"]["s_per_100_trees"] / out[fast]["s_per_100_trees"], 3)}
+
+
+def run_configs(bst, torch):
+    """The survey's other workloads in every form, each timed on the device
+    (CUDA events) and evaluated on a held-out draw of the same generator:
+    5,000 x 100 regression (50 trees, depth 6); 10,000,000 x 200 logistic,
+    leaf-wise 255 leaves (100 trees; the workload names no tree count);
+    2,000,000 x 50 softmax with 10 categorical columns, 10 classes (200
+    rounds x 10 trees, depth 6)."""
+    all_forms = [k for k, _ in FORMS]
+    out = {}
     x, y = bst.synth.regression(5_000, 100, 20, seed=1)
     xv, yv = bst.synth.regression(1_000, 100, 20, seed=1, stream=1)
-    ds = bst.Dataset.from_feature_major(x, y)
+    dv = bst.Dataset.from_feature_major(xv)
     kw = dict(n_estimators=50, max_depth=6, learning_rate=0.1, metric=bst.Metric.none())
-    c1 = {}
-    for form, over in (("plain", dict(PLAIN)), ("batched_q8", dict(precision="q8", batched=True))):
-        v, m = time_trees(bst, torch, ds, bst.GBDTConfig(**kw, **over), 5, 40)
-        pv = m.predict_group_major(bst.Dataset.from_feature_major(xv))
-        c1[form] = {"s_per_100_trees": round(v, 5), "heldout_rmse": round(bst.metric("rmse", pv, yv), 6)}
-    out["config1_regression_5kx100_depth6"] = c1
-    # config 3
+    r = config_forms(bst, torch, bst.Dataset.from_feature_major(x, y), kw, all_forms, 5, 40,
+                     lambda m: bst.metric("rmse", m.predict_group_major(dv), yv))
+    out["regression_5kx100_depth6_50trees"] = dict(r, loss="heldout rmse, 1,000 rows")
+
     x, y = bst.synth.binary(10_000_000, 200, 20, seed=3)
-    xv, yv = bst.synth.binary(1_000_000, 200, 20, seed=3, stream=1)
+    xv, yv = bst.synth.binary(2_000_000, 200, 20, seed=3, stream=1)
     ds = bst.Dataset.from_feature_major(x, y)
-    del x
-    kw = dict(objective=bst.Objective.logistic(), n_estimators=40, learning_rate=0.1,
+    dv = bst.Dataset.from_feature_major(xv)
+    kw = dict(objective=bst.Objective.logistic(), n_estimators=100, learning_rate=0.1,
               growth_strategy=bst.GrowthStrategy.Leafwise, n_leaves=255, metric=bst.Metric.none())
-    c3 = {}
-    for form, over in (("plain", dict(PLAIN)), ("batched_fp32", dict(precision="fp32", batched=True)),
-                       ("batched_q8", dict(precision="q8", batched=True))):
-        v, m = time_trees(bst, torch, ds, bst.GBDTConfig(**kw, **over), 3, 30)
-        pv = m.predict_group_major(bst.Dataset.from_feature_major(xv))
-        c3[form] = {"s_per_100_trees": round(v, 4), "heldout_logloss": round(bst.metric("logloss", pv, yv), 6),
-                    "trees": m.n_trees}
-    c3["loss_rel_q8_vs_plain"] = round((c3["batched_q8"]["heldout_logloss"] - c3["plain"]["heldout_logloss"])
-                                       / c3["plain"]["heldout_logloss"], 6)
-    out["config3_leafwise255_10Mx200"] = c3
-    del ds
-    # config 4
+    r = config_forms(bst, torch, ds, kw, all_forms, 2, 10,
+                     lambda m: bst.metric("logloss", m.predict_group_major(dv), yv))
+    out["logistic_10Mx200_leafwise255_100trees"] = dict(r, loss="heldout logloss, 2,000,000 rows")
+    del ds, dv, x, xv
+
     x, y = bst.synth.multiclass(2_000_000, 40, 10, 10, seed=4)
     xv, yv = bst.synth.multiclass(400_000, 40, 10, 10, seed=4, stream=1)
     cats = list(range(40, 50))
     ds = bst.Dataset.from_feature_major(x, y, categorical_features=cats)
-    kw = dict(objective=bst.Objective.softmax(10), n_estimators=40, max_depth=6, learning_rate=0.1,
-              metric=bst.Metric.none())
-    c4 = {}
-    for form, over in (("plain", dict(PLAIN)), ("batched_q8", dict(precision="q8", batched=True))):
-        v, m = time_trees(bst, torch, ds, bst.GBDTConfig(**kw, **over), 3, 20)
-        pv = m.predict_group_major(bst.Dataset.from_feature_major(xv, categorical_features=cats))
-        c4[form] = {"s_per_100_trees": round(v, 5), "heldout_mlogloss": round(bst.metric("mlogloss", pv, yv), 6),
-                    "trees": m.n_trees}
-    out["config4_softmax10_cat10_2Mx50_depth6"] = c4
+    dv = bst.Dataset.from_feature_major(xv, categorical_features=cats)
+    kw = dict(objective=bst.Objective.softmax(10), n_estimators=200, max_depth=6, learning_rate=0.1,
+              max_onehot_cats=4, metric=bst.Metric.none())
+    r = config_forms(bst, torch, ds, kw, all_forms, 3, 20,
+                     lambda m: bst.metric("mlogloss", m.predict_group_major(dv), yv))
+    out["softmax10_cat10_2Mx50_depth6_200rounds"] = dict(r, loss="heldout multiclass logloss, 400,000 rows")
     return out
 
 
@@ -527,8 +585,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--profile", choices=["train", "predict"], help="run a small workload for a profiler and exit")
-    ap.add_argument("--configs", action="store_true",
-                    help="also measure the other survey workloads (configs 1, 3, 4; several minutes)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other survey workloads (5k x 100, 10M x 200 leaf-wise, 2M x 50 softmax)")
     ap.add_argument("--form", default="batched_q8", choices=[k for k, _ in FORMS])
     ap.add_argument("--rounds", type=int, default=4)
     ap.add_argument("--trees", type=int, default=1000)

@@ -24,7 +24,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fn
 
 CU_SOURCES = ["kernels.cu", "noalloc.cu"]
 CPP_SOURCES = ["binning.cpp", "engine.cpp", "capi.cpp", "server.cpp", "synth.cpp", "persist.cpp"]
-HEADERS = ["kernels.h", "binning.h", "engine.h", os.path.join("..", "..", "include", "boosters_c.h")]
+HEADERS = ["kernels.h", "binning.h", "engine.h", "synth_gen.h", "api_util.h", os.path.join("..", "..", "include", "boosters_c.h")]
 
 
 def _stale(obj, src):

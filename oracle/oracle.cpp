@@ -9,6 +9,10 @@
 
 #include "oracle.h"
 
+// The seeded workload generator, compiled into this library as its own copy
+// (a process that runs only the checker never loads the engine).
+#include "../boosters_b200/csrc/synth_gen.h"
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -300,8 +304,12 @@ struct orc_binned {
     uint32_t total_bins = 0;
 };
 
+// Per-feature work (analysis, bin mappers, bin assignment) is independent
+// across features, so `omp` threads split the features without changing any
+// result; the reference runs these loops over rayon the same way.
 static int build_binned(const float* x, uint64_t F, uint64_t n, const uint32_t* cat_idx,
-                        uint32_t n_cat, const bst_config& cfg, orc_binned& b) {
+                        uint32_t n_cat, const bst_config& cfg, orc_binned& b, int omp = 1) {
+    if (omp < 1) omp = 1;
     if (n == 0 || F == 0) {
         g_err = "dataset is empty";
         return BST_ERR_EMPTY_DATASET;
@@ -312,7 +320,8 @@ static int build_binned(const float* x, uint64_t F, uint64_t n, const uint32_t* 
     b.n = n;
     b.n_features = (uint32_t)F;
     std::vector<Analysis> an(F);
-    for (uint64_t f = 0; f < F; ++f) an[f] = analyze_feature(x + f * n, n, cfg, user_cat[f]);
+#pragma omp parallel for num_threads(omp) schedule(dynamic, 1)
+    for (int64_t f = 0; f < (int64_t)F; ++f) an[f] = analyze_feature(x + f * n, n, cfg, user_cat[f]);
     // compute_groups (feature_analysis.rs:655-751) + create_bundle_plan filter (bundling.rs:395-400):
     // sparse storage and EFB bundles are outside this restatement.
     for (uint64_t f = 0; f < F; ++f) {
@@ -326,7 +335,8 @@ static int build_binned(const float* x, uint64_t F, uint64_t n, const uint32_t* 
     // create_bin_mappers (dataset.rs:592-681)
     std::vector<uint32_t> sidx = sample_indices(n, cfg.binning_sample_cnt);
     b.mappers.resize(F);
-    for (uint64_t f = 0; f < F; ++f) {
+#pragma omp parallel for num_threads(omp) schedule(dynamic, 1)
+    for (int64_t f = 0; f < (int64_t)F; ++f) {
         const float* col = x + f * n;
         bool has_nan = an[f].n_nan > 0;
         if (an[f].is_numeric) {
@@ -360,13 +370,20 @@ static int build_binned(const float* x, uint64_t F, uint64_t n, const uint32_t* 
         b.col_default.push_back(m.default_bin);
         b.col_offset.push_back(off);
         off += m.n_bins;
-        // build_numeric_dense / build_categorical_dense (dataset.rs:782-842)
-        std::vector<uint16_t> bins(n);
-        const float* col = x + f * n;
-        for (uint64_t i = 0; i < n; ++i) bins[i] = (uint16_t)m.value_to_bin((double)col[i]);
-        b.col_bins.push_back(std::move(bins));
     }
     b.total_bins = off;
+    // build_numeric_dense / build_categorical_dense (dataset.rs:782-842)
+    const int64_t n_cols = (int64_t)b.col_feature.size();
+    b.col_bins.resize(n_cols);
+#pragma omp parallel for num_threads(omp) schedule(dynamic, 1)
+    for (int64_t c = 0; c < n_cols; ++c) {
+        const uint32_t f = b.col_feature[c];
+        const BinMapper& m = b.mappers[f];
+        std::vector<uint16_t> bins(n);
+        const float* col = x + (uint64_t)f * n;
+        for (uint64_t i = 0; i < n; ++i) bins[i] = (uint16_t)m.value_to_bin((double)col[i]);
+        b.col_bins[c] = std::move(bins);
+    }
     return 0;
 }
 
@@ -1620,6 +1637,47 @@ extern "C" {
 
 const char* orc_last_error(void) { return g_err.c_str(); }
 
+// GBDTConfig's builder defaults (model/gbdt/config.rs:111-226) and the
+// binning defaults (data/binned/feature_analysis.rs:29-63); GPU-only fields
+// are zero.
+void orc_config_default(bst_config* c) {
+    std::memset(c, 0, sizeof(*c));
+    c->objective = BST_OBJ_SQUARED;
+    c->metric = BST_METRIC_DEFAULT;
+    c->n_trees = 100;
+    c->learning_rate = 0.3f;
+    c->growth_strategy = BST_GROWTH_DEPTHWISE;
+    c->max_depth = 6;
+    c->max_leaves = 31;
+    c->max_onehot_cats = 4;
+    c->lambda = 1.0f;
+    c->min_child_weight = 1.0f;
+    c->min_samples_leaf = 1;
+    c->subsample = 1.0f;
+    c->colsample_bytree = 1.0f;
+    c->colsample_bylevel = 1.0f;
+    c->max_bins = 256;
+    c->sparsity_threshold = 0.9f;
+    c->enable_bundling = 1;
+    c->binning_sample_cnt = 200000;
+    c->early_stopping_rounds = -1;
+    c->cache_size = 8;
+    c->seed = 42;
+}
+
+int orc_synth_regression(uint64_t n, uint64_t F, uint64_t n_inf, uint64_t seed, uint64_t stream, float* x,
+                         float* y) {
+    return synthgen::regression(n, F, n_inf, seed, stream, x, y);
+}
+int orc_synth_binary(uint64_t n, uint64_t F, uint64_t n_nan_cols, uint64_t seed, uint64_t stream, float* x,
+                     float* y) {
+    return synthgen::binary(n, F, n_nan_cols, seed, stream, x, y);
+}
+int orc_synth_multiclass(uint64_t n, uint64_t n_num, uint64_t n_cat, uint64_t C, uint64_t seed, uint64_t stream,
+                         float* x, float* y) {
+    return synthgen::multiclass(n, n_num, n_cat, C, seed, stream, x, y);
+}
+
 int orc_bin(const float* x, uint64_t F, uint64_t n, const uint32_t* cat_idx, uint32_t n_cat,
             const bst_config* cfg, orc_binned** out) {
     orc_binned* b = new orc_binned();
@@ -1761,7 +1819,7 @@ int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, ui
     }
     auto t0 = std::chrono::steady_clock::now();
     orc_binned b;
-    rc = build_binned(x, F, n, cat_idx, n_cat, cfg, b);
+    rc = build_binned(x, F, n, cat_idx, n_cat, cfg, b, omp_threads);
     if (rc) return rc;
     auto t1 = std::chrono::steady_clock::now();
     orc_model* m = new orc_model();

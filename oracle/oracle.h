@@ -133,6 +133,14 @@ int orc_model_add_tree(orc_model* m, uint32_t group, uint32_t n_nodes, const uin
                        const uint32_t* words, uint32_t n_words);
 
 const char* orc_last_error(void);
+void orc_config_default(bst_config* cfg);
+/* seeded workloads (boosters_b200/csrc/synth_gen.h): 0 on success */
+int orc_synth_regression(uint64_t n, uint64_t F, uint64_t n_inf, uint64_t seed, uint64_t stream, float* x,
+                         float* y);
+int orc_synth_binary(uint64_t n, uint64_t F, uint64_t n_nan_cols, uint64_t seed, uint64_t stream, float* x,
+                     float* y);
+int orc_synth_multiclass(uint64_t n, uint64_t n_num, uint64_t n_cat, uint64_t C, uint64_t seed, uint64_t stream,
+                         float* x, float* y);
 
 /* Row-sampling generator (test infrastructure): n raw Xoshiro256++ outputs
  * from `state`, and `draws` consecutive uniform row samples (masks

@@ -1,19 +1,36 @@
 """ctypes bridge to the CPU restatement in oracle/ (the checker).
 
-Only the tests, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg
-use this module; the engine never does.
+Only the tests, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline legs
+use this module; the engine never does. It loads no engine library: the
+plain C types come from ``boosters_b200/_abi.py`` (read by path when the
+engine package is not imported), so a process that only times the checker
+maps liboracle.so alone. ``BST_ORACLE_LIB`` selects another build of the
+same source (bench.py's host-tuned build).
 """
 import ctypes
+import importlib.util
 import os
 import subprocess
+import sys
 
 import numpy as np
 
-from boosters_b200._native import Config, Split
-
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
-ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
+ORACLE_LIB = os.environ.get("BST_ORACLE_LIB") or os.path.join(ORACLE_DIR, "liboracle.so")
+
+
+def _abi_module():
+    if "boosters_b200._abi" in sys.modules:
+        return sys.modules["boosters_b200._abi"]
+    spec = importlib.util.spec_from_file_location("_bst_abi_for_oracle", os.path.join(ROOT, "boosters_b200", "_abi.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+_abi = _abi_module()
+Config, Split = _abi.Config, _abi.Split
 
 f32p = ctypes.POINTER(ctypes.c_float)
 f64p = ctypes.POINTER(ctypes.c_double)
@@ -27,7 +44,7 @@ u32 = ctypes.c_uint32
 
 _SIGS = [
     ("orc_last_error", ctypes.c_char_p, []),
-    ("orc_bin", ctypes.c_int, [f32p, u64, u64, u32p, u32, ctypes.POINTER(Config), ctypes.POINTER(vp)]),
+    ("orc_bin", ctypes.c_int, [f32p, u64, u64, u32p, u32, vp, ctypes.POINTER(vp)]),
     ("orc_binned_free", None, [vp]),
     ("orc_binned_n_columns", u32, [vp]),
     ("orc_binned_column_info", None, [vp, u32, u32p, u32p, i32p, i32p, u32p]),
@@ -40,14 +57,14 @@ _SIGS = [
      [ctypes.c_double, ctypes.c_double, u32, u32, ctypes.c_float, u32]),
     ("orc_histogram_build", None, [u16p, u32p, u32, u64, f32p, f32p, u32p, u64, f64p]),
     ("orc_find_split", None,
-     [f64p, u32p, i32p, i32p, u32, ctypes.c_double, ctypes.c_double, u32, ctypes.POINTER(Config), u32,
-      ctypes.POINTER(Split)]),
+     [f64p, u32p, i32p, i32p, u32, ctypes.c_double, ctypes.c_double, u32, vp, u32,
+      vp]),
     ("orc_gradients", None, [ctypes.c_int32, u32, f32p, f32p, f32p, u64, f32p, f32p]),
     ("orc_base_score", None, [ctypes.c_int32, u32, f32p, f32p, u64, f32p]),
     ("orc_transform", None, [ctypes.c_int32, f32p, u32, u64]),
     ("orc_metric", ctypes.c_double, [ctypes.c_int32, f32p, u32, u64, f32p, f32p]),
     ("orc_train_limited", ctypes.c_int,
-     [f32p, u64, u64, f32p, u32, f32p, u32p, u32, ctypes.POINTER(Config), u32, ctypes.c_int, ctypes.c_int, u32,
+     [f32p, u64, u64, f32p, u32, f32p, u32p, u32, vp, u32, ctypes.c_int, ctypes.c_int, u32,
       ctypes.POINTER(vp)]),
     ("orc_model_free", None, [vp]),
     ("orc_model_n_trees", u32, [vp]),
@@ -63,12 +80,16 @@ _SIGS = [
     ("orc_model_binning_seconds", ctypes.c_double, [vp]),
     ("orc_model_tree_seconds", ctypes.c_double, [vp, u32]),
     ("orc_predict", ctypes.c_int, [vp, f32p, u64, u64, ctypes.c_int, f32p]),
-    ("orc_grow_tree", ctypes.c_int, [f32p, u64, u64, f32p, f32p, ctypes.POINTER(Config), u32, ctypes.POINTER(vp)]),
+    ("orc_grow_tree", ctypes.c_int, [f32p, u64, u64, f32p, f32p, vp, u32, ctypes.POINTER(vp)]),
     ("orc_model_create", ctypes.c_int, [u32, u32, ctypes.c_int32, f32p, ctypes.POINTER(vp)]),
     ("orc_model_add_tree", ctypes.c_int,
      [vp, u32, u32, u32p, f32p, u32p, u32p, u8p, u8p, f32p, u8p, u32p, u32p, u32p, u32]),
     ("orc_predict_rows", ctypes.c_int, [vp, f32p, u64, u64, ctypes.c_int, ctypes.c_int, f32p]),
     ("orc_philox4x32_10", None, [u32p, u32p, u32p]),
+    ("orc_config_default", None, [vp]),
+    ("orc_synth_regression", ctypes.c_int, [u64, u64, u64, u64, u64, f32p, f32p]),
+    ("orc_synth_binary", ctypes.c_int, [u64, u64, u64, u64, u64, f32p, f32p]),
+    ("orc_synth_multiclass", ctypes.c_int, [u64, u64, u64, u64, u64, u64, f32p, f32p]),
     ("orc_quantize", None, [f32p, f32p, u64, ctypes.c_int32, u64, u32, u32, i32p, i32p, f64p]),
 ]
 
@@ -80,7 +101,7 @@ def build_oracle():
 
 
 def _load():
-    if not os.path.exists(ORACLE_LIB):
+    if not os.path.exists(ORACLE_LIB) and "BST_ORACLE_LIB" not in os.environ:
         build_oracle()
     lib = ctypes.CDLL(ORACLE_LIB)
     for name, res, args in _SIGS:
@@ -346,3 +367,42 @@ def quantize(grad, hess, precision, seed, rnd, output=0):
     lib.orc_quantize(P(g, ctypes.c_float), P(h, ctypes.c_float), n, precision, seed, rnd, output,
                      P(qg, ctypes.c_int32), P(qh, ctypes.c_int32), P(steps, ctypes.c_double))
     return qg, qh, steps
+
+
+def config(**fields):
+    """bst_config with the reference defaults (the oracle's own statement of
+    GBDTConfig's builder defaults) and the given fields set."""
+    c = Config()
+    lib.orc_config_default(ctypes.byref(c))
+    for k, v in fields.items():
+        setattr(c, k, v)
+    return c
+
+
+class synth:
+    """The seeded workloads from the oracle's own copy of the generator
+    (byte-identical to the engine's ``boosters_b200.synth``)."""
+
+    @staticmethod
+    def binary(n, n_features, n_nan_cols, seed, stream=0):
+        x = np.empty((n_features, n), np.float32)
+        y = np.empty(n, np.float32)
+        _check(lib.orc_synth_binary(n, n_features, n_nan_cols, seed, stream, P(x, ctypes.c_float),
+                                    P(y, ctypes.c_float)))
+        return x, y
+
+    @staticmethod
+    def regression(n, n_features, n_informative, seed, stream=0):
+        x = np.empty((n_features, n), np.float32)
+        y = np.empty(n, np.float32)
+        _check(lib.orc_synth_regression(n, n_features, n_informative, seed, stream, P(x, ctypes.c_float),
+                                        P(y, ctypes.c_float)))
+        return x, y
+
+    @staticmethod
+    def multiclass(n, n_numeric, n_categorical, n_classes, seed, stream=0):
+        x = np.empty((n_numeric + n_categorical, n), np.float32)
+        y = np.empty(n, np.float32)
+        _check(lib.orc_synth_multiclass(n, n_numeric, n_categorical, n_classes, seed, stream,
+                                        P(x, ctypes.c_float), P(y, ctypes.c_float)))
+        return x, y
