@@ -345,9 +345,11 @@ class GBDTModel:
         finally:
             _n.lib.bst_buffer_free(buf)
 
-    def to_bytes(self):
-        """The model as a ``.bstr`` file (uncompressed MessagePack payload)."""
-        return self._bytes(_n.lib.bst_model_to_bstr)
+    def to_bytes(self, compression_level=3):
+        """The model as a ``.bstr`` file: zstd-compressed MessagePack at
+        ``compression_level`` (1-22; 3 is the reference's default), or plain
+        MessagePack with 0 (persist/binary.rs:21-43)."""
+        return self._bytes(_n.lib.bst_model_to_bstr_level, int(compression_level))
 
     def to_json_bytes(self, pretty=False):
         """The model as a ``.bstr.json`` document."""
@@ -363,13 +365,14 @@ class GBDTModel:
 
     from_json_bytes = from_bytes
 
-    def save(self, path, pretty=False):
-        """Writes ``path``: JSON when it ends in ``.json``, else ``.bstr``."""
+    def save(self, path, pretty=False, compression_level=3):
+        """Writes ``path``: JSON when it ends in ``.json``, else ``.bstr``
+        (zstd at ``compression_level``, 0 for plain MessagePack)."""
         p = os.fsencode(path)
         if p.endswith(b".json"):
             _n.check(_n.lib.bst_model_write_json(self._h, p, 1 if pretty else 0))
         else:
-            _n.check(_n.lib.bst_model_write_bstr(self._h, p))
+            _n.check(_n.lib.bst_model_write_bstr_level(self._h, p, int(compression_level)))
 
     @staticmethod
     def load(path, config=None):

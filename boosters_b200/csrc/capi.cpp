@@ -9,6 +9,7 @@
 #include "../../include/boosters_c.h"
 #include <cstdio>
 #include <cstdlib>
+#include "api_util.h"
 #include "engine.h"
 
 struct bst_dataset {
@@ -95,6 +96,12 @@ bst_status check_config(const bst_config* c, bool for_training) {
 }
 
 }  // namespace
+
+namespace bst {
+bst_status api_fail(bst_status code, const char* msg) { return fail(code, msg); }
+bst_status api_check_config(const bst_config* c, bool for_training) { return check_config(c, for_training); }
+void api_clear_error() { g_err.clear(); }
+}  // namespace bst
 
 extern "C" {
 
@@ -325,12 +332,16 @@ bst_status bst_model_to_json(const bst_model* model, int32_t pretty, uint8_t** o
     });
 }
 
-bst_status bst_model_to_bstr(const bst_model* model, uint8_t** out, uint64_t* len) {
+bst_status bst_model_to_bstr_level(const bst_model* model, int32_t level, uint8_t** out, uint64_t* len) {
     if (!model || !out || !len) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
     return guarded([&]() -> bst_status {
-        const std::vector<uint8_t> b = bst::model_to_bstr(*model->m);
+        const std::vector<uint8_t> b = bst::model_to_bstr(*model->m, level);
         return copy_out(b.data(), b.size(), out, len);
     });
+}
+
+bst_status bst_model_to_bstr(const bst_model* model, uint8_t** out, uint64_t* len) {
+    return bst_model_to_bstr_level(model, BST_BSTR_DEFAULT_LEVEL, out, len);
 }
 
 bst_status bst_model_from_bytes(const uint8_t* data, uint64_t len, bst_model** out) {
@@ -362,12 +373,16 @@ bst_status bst_model_write_json(const bst_model* model, const char* path, int32_
     });
 }
 
-bst_status bst_model_write_bstr(const bst_model* model, const char* path) {
+bst_status bst_model_write_bstr_level(const bst_model* model, const char* path, int32_t level) {
     if (!model || !path) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
     return guarded([&]() -> bst_status {
-        const std::vector<uint8_t> b = bst::model_to_bstr(*model->m);
+        const std::vector<uint8_t> b = bst::model_to_bstr(*model->m, level);
         return write_file(path, b.data(), b.size());
     });
+}
+
+bst_status bst_model_write_bstr(const bst_model* model, const char* path) {
+    return bst_model_write_bstr_level(model, path, BST_BSTR_DEFAULT_LEVEL);
 }
 
 bst_status bst_model_load(const char* path, bst_model** out) {

@@ -23,6 +23,15 @@ struct Error {
 void cuda_check(cudaError_t e, const char* what);
 #define BST_CK(x) ::bst::cuda_check((x), #x)
 
+// Device-memory cap of the library's own buffers: the environment variable
+// BST_DEVICE_MEMORY_LIMIT (bytes, read once; unset or 0 = no cap) bounds
+// the bytes all live DevArrays hold together, process-wide. An allocation
+// that would pass it fails like an exhausted device (BST_ERR_OUT_OF_MEMORY)
+// without calling cudaMalloc: for sharing a GPU with other allocators, and
+// for exercising the out-of-memory paths without exhausting a device.
+void dev_bytes_reserve(size_t bytes);  // throws Error{BST_ERR_OUT_OF_MEMORY}
+void dev_bytes_release(size_t bytes);
+
 template <class T>
 struct DevArray {
     T* p = nullptr;
@@ -32,7 +41,10 @@ struct DevArray {
     DevArray& operator=(const DevArray&) = delete;
     ~DevArray() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            cudaFree(p);
+            dev_bytes_release(n * sizeof(T));
+        }
         p = nullptr;
         n = 0;
     }
@@ -40,10 +52,12 @@ struct DevArray {
         if (k <= n && p) return;
         release();
         if (k == 0) return;
+        dev_bytes_reserve(k * sizeof(T));
         cudaError_t e = cudaMalloc(&p, k * sizeof(T));
         if (e != cudaSuccess) {
             cudaGetLastError();
             p = nullptr;
+            dev_bytes_release(k * sizeof(T));
             throw Error{e == cudaErrorMemoryAllocation ? BST_ERR_OUT_OF_MEMORY : BST_ERR_CUDA,
                         std::string("cudaMalloc of ") + std::to_string(k * sizeof(T)) +
                             " bytes failed: " + cudaGetErrorString(e)};
@@ -172,7 +186,7 @@ int resolve_metric(int metric, int objective);
 // Model files (persist.cpp): .bstr.json text and .bstr bytes (uncompressed
 // MessagePack); model_from_bytes reads either (binary by its magic).
 std::string model_to_json(const Model& m, bool pretty);
-std::vector<uint8_t> model_to_bstr(const Model& m);
+std::vector<uint8_t> model_to_bstr(const Model& m, int compression_level);
 std::unique_ptr<Model> model_from_bytes(const uint8_t* data, size_t len);
 uint32_t crc32c_bytes(const uint8_t* p, size_t n);
 

@@ -12,15 +12,20 @@
 // direction, scalar leaf values), categorical splits as sorted category
 // lists of the nodes that have them, optional gains and covers; per forest
 // tree groups (only with more than one group), group count and base scores;
-// the output transform by name. Payloads written here are uncompressed
-// MessagePack (format byte 0x01); zstd payloads (0x02) are reported as
-// unsupported: no zstd decoder is linked.
+// the output transform by name. Payloads are plain MessagePack (format byte
+// 0x01) or zstd-compressed MessagePack (0x02; binary.rs:60-91, the
+// reference writes zstd level 3 by default and reads any number of
+// concatenated frames, zstd::decode_all). zstd comes from the system
+// libzstd.so.1 through its public streaming API, loaded at first use.
+#include <dlfcn.h>
+
 #include <algorithm>
 #include <charconv>
 #include <cmath>
 #include <cstring>
 #include <fstream>
 #include <limits>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -36,6 +41,104 @@ constexpr size_t HEADER_SIZE = 32, TRAILER_SIZE = 16;
 
 [[noreturn]] void bad(const std::string& msg) { throw Error{BST_ERR_INVALID_ARGUMENT, "model file: " + msg}; }
 [[noreturn]] void unsupported(const std::string& msg) { throw Error{BST_ERR_UNSUPPORTED, "model file: " + msg}; }
+
+// ---- zstd (system libzstd.so.1, public API of zstd.h) -------------------------
+// The buffer structs and entry points below are the library's documented
+// stable interface (names and signatures only).
+struct ZInBuf {
+    const void* src;
+    size_t size;
+    size_t pos;
+};
+struct ZOutBuf {
+    void* dst;
+    size_t size;
+    size_t pos;
+};
+
+struct Zstd {
+    void* h = nullptr;
+    void* (*create_dstream)() = nullptr;
+    size_t (*free_dstream)(void*) = nullptr;
+    size_t (*init_dstream)(void*) = nullptr;
+    size_t (*decompress_stream)(void*, ZOutBuf*, ZInBuf*) = nullptr;
+    size_t (*compress)(void*, size_t, const void*, size_t, int) = nullptr;
+    size_t (*compress_bound)(size_t) = nullptr;
+    unsigned (*is_error)(size_t) = nullptr;
+    const char* (*error_name)(size_t) = nullptr;
+    std::string load_error;
+};
+
+const Zstd& zstd() {
+    static Zstd z;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        z.h = dlopen("libzstd.so.1", RTLD_NOW | RTLD_LOCAL);
+        if (!z.h) {
+            const char* e = dlerror();
+            z.load_error = std::string("libzstd.so.1 could not be loaded: ") + (e ? e : "unknown error");
+            return;
+        }
+        auto sym = [&](const char* name) {
+            void* f = dlsym(z.h, name);
+            if (!f && z.load_error.empty()) z.load_error = std::string("libzstd.so.1 lacks ") + name;
+            return f;
+        };
+        z.create_dstream = reinterpret_cast<void* (*)()>(sym("ZSTD_createDStream"));
+        z.free_dstream = reinterpret_cast<size_t (*)(void*)>(sym("ZSTD_freeDStream"));
+        z.init_dstream = reinterpret_cast<size_t (*)(void*)>(sym("ZSTD_initDStream"));
+        z.decompress_stream = reinterpret_cast<size_t (*)(void*, ZOutBuf*, ZInBuf*)>(sym("ZSTD_decompressStream"));
+        z.compress = reinterpret_cast<size_t (*)(void*, size_t, const void*, size_t, int)>(sym("ZSTD_compress"));
+        z.compress_bound = reinterpret_cast<size_t (*)(size_t)>(sym("ZSTD_compressBound"));
+        z.is_error = reinterpret_cast<unsigned (*)(size_t)>(sym("ZSTD_isError"));
+        z.error_name = reinterpret_cast<const char* (*)(size_t)>(sym("ZSTD_getErrorName"));
+    });
+    if (!z.load_error.empty()) unsupported("zstd payloads need the system zstd library (" + z.load_error + ")");
+    return z;
+}
+
+// Every frame of the payload, concatenated (zstd::decode_all).
+std::vector<uint8_t> zstd_decode_all(const uint8_t* p, size_t n) {
+    const Zstd& z = zstd();
+    void* ds = z.create_dstream();
+    if (!ds) throw Error{BST_ERR_OUT_OF_MEMORY, "model file: zstd stream allocation failed"};
+    std::vector<uint8_t> out;
+    std::string err;
+    size_t r = z.init_dstream(ds);
+    if (z.is_error(r)) err = z.error_name(r);
+    ZInBuf in{p, n, 0};
+    size_t last = 0;
+    while (err.empty() && in.pos < in.size) {
+        const size_t old = out.size();
+        out.resize(old + std::max<size_t>(1 << 16, n));
+        ZOutBuf ob{out.data() + old, out.size() - old, 0};
+        last = z.decompress_stream(ds, &ob, &in);
+        out.resize(old + ob.pos);
+        if (z.is_error(last)) err = z.error_name(last);
+    }
+    // flush what the decoder still holds of the last frame
+    while (err.empty() && last != 0) {
+        const size_t old = out.size();
+        out.resize(old + (1 << 16));
+        ZOutBuf ob{out.data() + old, out.size() - old, 0};
+        last = z.decompress_stream(ds, &ob, &in);
+        out.resize(old + ob.pos);
+        if (z.is_error(last)) err = z.error_name(last);
+        else if (last != 0 && ob.pos == 0) err = "truncated zstd frame";
+    }
+    z.free_dstream(ds);
+    if (!err.empty()) bad("zstd decompression failed: " + err);
+    return out;
+}
+
+std::vector<uint8_t> zstd_compress(const std::vector<uint8_t>& src, int level) {
+    const Zstd& z = zstd();
+    std::vector<uint8_t> out(z.compress_bound(src.size()));
+    const size_t r = z.compress(out.data(), out.size(), src.data(), src.size(), level);
+    if (z.is_error(r)) throw Error{BST_ERR_INVALID_ARGUMENT, std::string("zstd compression failed: ") + z.error_name(r)};
+    out.resize(r);
+    return out;
+}
 
 // ---- CRC32C (Castagnoli, reflected polynomial 0x82F63B78) --------------------
 uint32_t crc32c(const uint8_t* p, size_t n) {
@@ -1029,13 +1132,18 @@ ModelS read_msgpack(const uint8_t* data, size_t len) {
     return m;
 }
 
-std::vector<uint8_t> write_bstr(const ModelS& m) {
-    const std::vector<uint8_t> payload = write_msgpack(m);
+// level 0: plain MessagePack (0x01); 1-22: zstd at that level (0x02)
+// (binary.rs:60-91; levels above 22 are rejected, binary.rs:56-59).
+std::vector<uint8_t> write_bstr(const ModelS& m, int level) {
+    if (level < 0 || level > 22)
+        throw Error{BST_ERR_INVALID_ARGUMENT, "compression level " + std::to_string(level) + " is outside 0-22"};
+    std::vector<uint8_t> payload = write_msgpack(m);
+    if (level > 0) payload = zstd_compress(payload, level);
     std::vector<uint8_t> out(HEADER_SIZE, 0);
     std::memcpy(out.data(), "BSTR", 4);
     for (int i = 0; i < 4; ++i) out[4 + i] = (uint8_t)(SCHEMA_VERSION >> (8 * i));
-    out[8] = 0x01;  // uncompressed MessagePack
-    out[9] = 1;     // GBDT
+    out[8] = level > 0 ? 0x02 : 0x01;
+    out[9] = 1;  // GBDT
     out.insert(out.end(), payload.begin(), payload.end());
     const uint64_t len = payload.size();
     const uint32_t crc = crc32c(payload.data(), payload.size());
@@ -1065,7 +1173,10 @@ ModelS read_bstr(const uint8_t* d, size_t n) {
     const size_t plen = n - HEADER_SIZE - TRAILER_SIZE;
     if (len != plen) bad("payload length mismatch");
     if (crc32c(payload, plen) != crc) bad("checksum mismatch");
-    if (format == 0x02) unsupported("zstd-compressed payload (write with compression level 0 to load it here)");
+    if (format == 0x02) {
+        const std::vector<uint8_t> raw = zstd_decode_all(payload, plen);
+        return read_msgpack(raw.data(), raw.size());
+    }
     return read_msgpack(payload, plen);
 }
 
@@ -1075,7 +1186,7 @@ uint32_t crc32c_bytes(const uint8_t* p, size_t n) { return crc32c(p, n); }
 
 std::string model_to_json(const Model& m, bool pretty) { return write_json(to_schema(m), pretty); }
 
-std::vector<uint8_t> model_to_bstr(const Model& m) { return write_bstr(to_schema(m)); }
+std::vector<uint8_t> model_to_bstr(const Model& m, int level) { return write_bstr(to_schema(m), level); }
 
 std::unique_ptr<Model> model_from_bytes(const uint8_t* data, size_t len) {
     ModelS s = len >= 4 && std::memcmp(data, "BSTR", 4) == 0 ? read_bstr(data, len)

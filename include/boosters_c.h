@@ -351,14 +351,19 @@ bst_status bst_find_split(const double* histogram, const uint32_t* n_bins,
  * (cudaStream_t, NULL = legacy stream) has finished. Results equal those of
  * bst_find_split on the same histogram.
  *
- * Working memory is one fixed array in device global memory (about 1.1 MiB),
- * which every GPU that loads the library holds until the process exits.
- * Limits: n_features <= 1024, sum(n_bins) <= 65536, categorical features <=
- * 256 bins; larger inputs return BST_ERR_INVALID_ARGUMENT. The first call on
- * a device looks up that array's device address (once per device); make that
- * first call before any stream capture. Every call shares the array: calls
- * that overlap on the GPU (other streams, other host threads) race and must
- * be serialised by the caller. */
+ * Working memory is one fixed array in device global memory (about 1.1 MiB).
+ * The CUDA runtime loads device code and arrays lazily: the first call on a
+ * device loads this entry point's kernels and the array onto that device
+ * and looks up the array's device address, which takes device memory once;
+ * make that first call before the device's memory is fully reserved and
+ * before any stream capture. The device then holds the array until the
+ * process exits, and later calls allocate nothing.
+ * Limits: n_features <= 1024 and sum(n_bins) <= 65536 (larger inputs return
+ * BST_ERR_INVALID_ARGUMENT); categorical features with more than 256 bins
+ * return BST_ERR_UNSUPPORTED, as in bst_find_split. Validation, n_features
+ * == 0 (BST_OK, gain -inf) and error messages follow bst_find_split. Every
+ * call shares the array: calls that overlap on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller. */
 bst_status bst_find_split_noalloc(const double* histogram_dev, const uint32_t* n_bins,
                                   const int32_t* is_categorical, const int32_t* has_missing,
                                   uint32_t n_features, double parent_grad, double parent_hess,
@@ -387,10 +392,17 @@ bst_status bst_quantize_gradients(const float* grad, const float* hess, uint64_t
 /* ------------------------------------------------------------------------ */
 
 /* Library-allocated bytes: free with bst_buffer_free. .bstr payloads are
- * written uncompressed (format byte 0x01); zstd payloads (0x02) are read
- * as BST_ERR_UNSUPPORTED (no zstd decoder is linked). */
+ * zstd-compressed MessagePack (format byte 0x02) at level 3, the reference's
+ * default (persist/binary.rs:15-31, BinaryWriteOptions::default). zstd is
+ * the system libzstd.so.1, loaded at first use; without it zstd payloads
+ * return BST_ERR_UNSUPPORTED. */
+#define BST_BSTR_DEFAULT_LEVEL 3
 bst_status bst_model_to_json(const bst_model* model, int32_t pretty, uint8_t** out, uint64_t* len);
 bst_status bst_model_to_bstr(const bst_model* model, uint8_t** out, uint64_t* len);
+/* BinaryWriteOptions { compression_level } (persist/binary.rs:21-43): 0 =
+ * plain MessagePack (format byte 0x01), 1-22 = zstd at that level (0x02);
+ * other levels: BST_ERR_INVALID_ARGUMENT. */
+bst_status bst_model_to_bstr_level(const bst_model* model, int32_t level, uint8_t** out, uint64_t* len);
 /* Either layout (binary when the bytes start with "BSTR"). Malformed input:
  * BST_ERR_INVALID_ARGUMENT with the reason; linear or multi-value leaves:
  * BST_ERR_UNSUPPORTED. */
@@ -398,6 +410,7 @@ bst_status bst_model_from_bytes(const uint8_t* data, uint64_t len, bst_model** o
 void bst_buffer_free(void* p);
 bst_status bst_model_write_json(const bst_model* model, const char* path, int32_t pretty);
 bst_status bst_model_write_bstr(const bst_model* model, const char* path);
+bst_status bst_model_write_bstr_level(const bst_model* model, const char* path, int32_t level);
 bst_status bst_model_load(const char* path, bst_model** out);
 /* CRC32C (Castagnoli) of the .bstr trailer. */
 uint32_t bst_crc32c(const uint8_t* data, uint64_t len);

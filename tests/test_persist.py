@@ -45,8 +45,19 @@ def envelope(model, version=2, kind="gbdt"):
     return json.dumps({"bstr_version": version, "model_type": kind, "model": model}).encode()
 
 
-def binary(model, fmt=1, kind=1, version=2):
-    payload = msgpack.packb(model, use_bin_type=True)
+def zstd_frames(data, parts=1):
+    """zstd frames from an independent encoder (pyarrow's bundled zstd), the
+    data split into `parts` consecutive frames."""
+    import pyarrow as pa
+    cuts = [len(data) * i // parts for i in range(parts + 1)]
+    return b"".join(pa.compress(data[a:b], codec="zstd", asbytes=True) for a, b in zip(cuts, cuts[1:]))
+
+
+def binary(model, fmt=1, kind=1, version=2, payload=None, frames=1):
+    if payload is None:
+        payload = msgpack.packb(model, use_bin_type=True)
+        if fmt == 2:
+            payload = zstd_frames(payload, frames)
     head = b"BSTR" + struct.pack("<I", version) + bytes([fmt, kind]) + bytes(22)
     return head + payload + struct.pack("<QI", len(payload), crc32c(payload)) + bytes(4)
 
@@ -55,7 +66,15 @@ def tree0(m):
     return m.tree(0)
 
 
-@pytest.mark.parametrize("encode", [envelope, binary])
+def binary_zstd(model):
+    return binary(model, fmt=2)
+
+
+def binary_zstd_two_frames(model):
+    return binary(model, fmt=2, frames=2)
+
+
+@pytest.mark.parametrize("encode", [envelope, binary, binary_zstd, binary_zstd_two_frames])
 def test_read_stump(encode):
     m = bst.GBDTModel.from_bytes(encode(stump("sigmoid")))
     assert (m.n_trees, m.n_groups, m.n_features) == (1, 1, 2)
@@ -89,8 +108,9 @@ def test_json_round_trip_and_schema():
 
 
 def test_binary_payload_decodes_independently():
+    import pyarrow as pa
     m = bst.GBDTModel.from_bytes(envelope(stump()))
-    b = m.to_bytes()
+    b = m.to_bytes(compression_level=0)
     assert b[:4] == b"BSTR" and struct.unpack("<I", b[4:8])[0] == 2 and b[8] == 1 and b[9] == 1
     assert b[10:32] == bytes(22)
     payload, trailer = b[32:-16], b[-16:]
@@ -99,8 +119,22 @@ def test_binary_payload_decodes_independently():
     doc = msgpack.unpackb(payload, raw=False)
     want = json.loads(m.to_json_bytes())["model"]
     assert doc == want
-    assert bst.GBDTModel.from_bytes(b).to_bytes() == b
-    assert pickle.loads(pickle.dumps(m)).to_bytes() == b
+    assert bst.GBDTModel.from_bytes(b).to_bytes(compression_level=0) == b
+    # the default is the reference's: zstd level 3 (format byte 0x02), whose
+    # payload an independent decoder expands to the same MessagePack bytes
+    z = m.to_bytes()
+    assert z[8] == 2 and z[9] == 1
+    zp, zt = z[32:-16], z[-16:]
+    assert struct.unpack("<QI", zt[:12]) == (len(zp), crc32c(zp))
+    assert pa.decompress(zp, decompressed_size=len(payload), codec="zstd", asbytes=True) == payload
+    assert bst.GBDTModel.from_bytes(z).to_bytes() == z
+    assert pickle.loads(pickle.dumps(m)).to_bytes() == z
+    for level in (1, 19):
+        assert bst.GBDTModel.from_bytes(m.to_bytes(compression_level=level)).to_json_bytes() == m.to_json_bytes()
+    for level in (-1, 23):
+        with pytest.raises(n.BoostersError) as e:
+            m.to_bytes(compression_level=level)
+        assert e.value.status == n.BST_ERR_INVALID_ARGUMENT
 
 
 def test_categorical_and_groups():
@@ -164,9 +198,11 @@ def test_rejections():
     corrupt[40] ^= 0xFF
     _bad(bytes(corrupt), "checksum")
     _bad(good[: len(good) // 2], "length|small|checksum")
-    with pytest.raises(n.BoostersError) as e:
-        bst.GBDTModel.from_bytes(binary(stump(), fmt=2))
-    assert e.value.status == n.BST_ERR_UNSUPPORTED and "zstd" in str(e.value)
+    # a zstd payload that is not zstd (valid checksum): a decompression error
+    _bad(binary(stump(), fmt=2, payload=b"\x28\xb5\x2f\xfd" + bytes(40)), "zstd")
+    # a truncated zstd frame
+    full = zstd_frames(msgpack.packb(stump(), use_bin_type=True))
+    _bad(binary(stump(), fmt=2, payload=full[:-3]), "zstd")
     _bad(binary(stump(), fmt=0), "0x00")
     _bad(binary(stump(), kind=2), "not gbdt")
 
