@@ -10,8 +10,10 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <map>
@@ -26,6 +28,31 @@ void cuda_check(cudaError_t e, const char* what) {
                     std::string(what) + ": " + cudaGetErrorString(e)};
     }
 }
+
+namespace {
+std::atomic<uint64_t> g_dev_bytes{0};
+
+uint64_t dev_memory_limit() {
+    static const uint64_t limit = [] {
+        const char* v = std::getenv("BST_DEVICE_MEMORY_LIMIT");
+        return v ? std::strtoull(v, nullptr, 10) : 0ull;
+    }();
+    return limit;
+}
+}  // namespace
+
+void dev_bytes_reserve(size_t bytes) {
+    const uint64_t limit = dev_memory_limit();
+    const uint64_t now = g_dev_bytes.fetch_add(bytes) + bytes;
+    if (limit && now > limit) {
+        g_dev_bytes.fetch_sub(bytes);
+        throw Error{BST_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) +
+                                               " bytes would pass BST_DEVICE_MEMORY_LIMIT=" + std::to_string(limit) +
+                                               " (" + std::to_string(now - bytes) + " bytes in use)"};
+    }
+}
+
+void dev_bytes_release(size_t bytes) { g_dev_bytes.fetch_sub(bytes); }
 
 // Column tiles of the histogram kernel: lanes of one 16-byte row vector
 // whose bins fit one shared-memory histogram (<= 4096 bins = 64 KiB).

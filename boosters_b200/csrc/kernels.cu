@@ -1580,6 +1580,13 @@ void launch_split_reduce(const ColCand* cand, const long long* node_tot, uint32_
     k_split_reduce<<<n_nodes, 32, 0, st>>>(cand, node_tot, n_cols, last_wins, out);
 }
 
+cudaError_t load_split_kernels() {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, k_split_scan<HBin>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_split_reduce);
+    return e;
+}
+
 // ============================================================================
 // K7: row partition (RowPartitioner::split, training/gbdt/partition.rs:296-382)
 // Left rows fill the node's range from the front, right rows from the back.

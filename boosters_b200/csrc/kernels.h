@@ -188,6 +188,9 @@ void launch_split_scan(const ScanNode* nodes, uint32_t n_nodes, const ScanColumn
                        long long* node_tot, cudaStream_t st, int hist32 = 0, const uint8_t* colmask = nullptr);
 void launch_split_reduce(const ColCand* cand, const long long* node_tot, uint32_t n_nodes,
                          uint32_t n_cols, int last_wins, NodeSplit* out, cudaStream_t st);
+// Loads the split-scan kernels (HBin) onto the current device now rather than
+// at their first launch (the runtime loads device code lazily).
+cudaError_t load_split_kernels();
 
 // ---- K7 partition -----------------------------------------------------------
 struct PartWork {

@@ -6,14 +6,21 @@
 // (cudaFree synchronises the whole device and stalls every other stream).
 // All working memory of this entry point lives in one file-scope
 // `static __device__` array, NOALLOC_SCRATCH_BYTES long, which the CUDA
-// runtime places on every GPU that loads the library and keeps until the
-// process exits. The caller passes the inputs (a device histogram) and the
-// output (a host bst_split).
+// runtime places on a GPU when this entry point is first called there and
+// keeps until the process exits. The caller passes the inputs (a device
+// histogram) and the output (a host bst_split).
+//
+// The CUDA runtime loads a library's device code and its `__device__` arrays
+// onto a GPU lazily, at first use. The first call on each device therefore
+// loads them (this file's kernels, the array, and the split-scan kernels it
+// launches) before doing any work, so that later calls allocate nothing; a
+// caller that reserves all device memory must make one call first.
 #include <math.h>
 
 #include <mutex>
 
 #include "../../include/boosters_c.h"
+#include "api_util.h"
 #include "kernels.h"
 
 namespace bst {
@@ -48,6 +55,11 @@ constexpr int NA_MAX_DEVICES = 64;
 NoallocScratch* g_scratch_ptr[NA_MAX_DEVICES] = {nullptr};
 std::mutex g_scratch_mu;
 
+cudaError_t load_noalloc_kernels();
+
+// First call on a device (with that device current): resolve the array's
+// device address and load every kernel a call launches, so that no later
+// call makes the runtime load (and allocate for) device code.
 cudaError_t scratch_for_current_device(NoallocScratch** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -57,6 +69,8 @@ cudaError_t scratch_for_current_device(NoallocScratch** out) {
     if (!g_scratch_ptr[dev]) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e == cudaSuccess) e = load_noalloc_kernels();
+        if (e == cudaSuccess) e = load_split_kernels();
         if (e != cudaSuccess) return e;
         g_scratch_ptr[dev] = reinterpret_cast<NoallocScratch*>(p);
     }
@@ -140,6 +154,20 @@ __global__ void k_na_quantize(const double* __restrict__ hist, uint32_t total, N
     }
 }
 
+cudaError_t load_noalloc_kernels() {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, k_na_clear);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_na_maxabs);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_na_setup);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, k_na_quantize);
+    return e;
+}
+
+bst_status cuda_fail(cudaError_t e) {
+    cudaGetLastError();
+    return api_fail(BST_ERR_CUDA, cudaGetErrorString(e));
+}
+
 }  // namespace
 }  // namespace bst
 
@@ -149,22 +177,29 @@ extern "C" bst_status bst_find_split_noalloc(const double* hist_dev, const uint3
                                              uint32_t parent_count, const bst_config* cfg, uint32_t n_threads,
                                              void* stream, bst_split* out) {
     using namespace bst;
-    if (!hist_dev || !n_bins || !is_categorical || !has_missing || !cfg || !out) return BST_ERR_INVALID_ARGUMENT;
-    if (n_features == 0 || n_features > NA_MAX_COLS) return BST_ERR_INVALID_ARGUMENT;
-    if (!(cfg->lambda >= 0.0f) || !(cfg->min_child_weight >= 0.0f) || !(cfg->min_gain >= 0.0f))
-        return BST_ERR_CONFIG;
+    api_clear_error();
+    if (!hist_dev || !n_bins || !is_categorical || !has_missing || !cfg || !out)
+        return api_fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    const bst_status rc = api_check_config(cfg, false);
+    if (rc != BST_OK) return rc;
+    *out = bst_split{};
+    out->gain = -INFINITY;
+    if (n_features == 0) return BST_OK;  // no candidate, as bst_find_split
+    if (n_features > NA_MAX_COLS)
+        return api_fail(BST_ERR_INVALID_ARGUMENT, "n_features exceeds the fixed working array's limit of 1024");
     uint64_t total = 0;
     for (uint32_t f = 0; f < n_features; ++f) {
-        if (is_categorical[f] && n_bins[f] > 256) return BST_ERR_UNSUPPORTED;
+        if (is_categorical[f] && n_bins[f] > 256)
+            return api_fail(BST_ERR_UNSUPPORTED, "categorical features need <= 256 bins");
         total += n_bins[f];
     }
-    if (total == 0 || total > NA_MAX_BINS) return BST_ERR_INVALID_ARGUMENT;
+    if (total > NA_MAX_BINS)
+        return api_fail(BST_ERR_INVALID_ARGUMENT, "sum(n_bins) exceeds the fixed working array's limit of 65536");
+    if (total == 0) return BST_OK;
     cudaStream_t st = (cudaStream_t)stream;
     NoallocScratch* s = nullptr;
-    if (scratch_for_current_device(&s) != cudaSuccess) {
-        cudaGetLastError();
-        return BST_ERR_CUDA;
-    }
+    const cudaError_t se = scratch_for_current_device(&s);
+    if (se != cudaSuccess) return cuda_fail(se);
     const double parent[2] = {parent_grad, parent_hess};
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = cudaMemcpyAsync(s->n_bins, n_bins, sizeof(uint32_t) * n_features, cudaMemcpyHostToDevice, st);
@@ -173,10 +208,7 @@ extern "C" bst_status bst_find_split_noalloc(const double* hist_dev, const uint3
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->has_missing, has_missing, sizeof(int32_t) * n_features, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(s->parent, parent, sizeof(parent), cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return BST_ERR_CUDA;
-    }
+    if (e != cudaSuccess) return cuda_fail(e);
     const uint32_t tb = (uint32_t)total;
     const unsigned blocks = (tb + 255) / 256 < 1024 ? (tb + 255) / 256 : 1024;
     k_na_clear<<<1, 32, 0, st>>>(s);
@@ -195,12 +227,7 @@ extern "C" bst_status bst_find_split_noalloc(const double* hist_dev, const uint3
     e = cudaMemcpyAsync(&res, &s->out, sizeof(res), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = cudaGetLastError();
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return BST_ERR_CUDA;
-    }
-    *out = bst_split{};
-    out->gain = -INFINITY;
+    if (e != cudaSuccess) return cuda_fail(e);
     if (res.flags & 4u) {
         out->feature = res.col;
         out->gain = res.gain;
