@@ -253,6 +253,26 @@ def serve_schedule(rng, rate, n_req, n_pool, max_rows=65536):
     return arrival, offs, sizes
 
 
+def phase_split(tr, lat):
+    """p50/p99 of each traced request phase (ms) and the achieved host->device
+    copy rate over the traced copies; `lat` (s) gives the slowest requests,
+    whose phases are listed apart (the p99 tail's make-up)."""
+    from boosters_b200 import _native as n
+    col = {k: tr[:, i].astype(np.float64) for i, k in enumerate(n.SERVER_PHASES)}
+    out = {}
+    for k in ("queue_ns", "copy_ns", "to_dispatch_ns", "kernel_ns", "d2h_ns", "dispatch_to_done_ns"):
+        v = col[k] / 1e6
+        out[k[:-3] + "_ms"] = {"p50": round(float(np.percentile(v, 50)), 3), "p99": round(float(np.percentile(v, 99)), 3)}
+    out["h2d_gb_per_s"] = round(float(col["rows"].sum() * N_FEAT * 4 / max(1.0, col["copy_ns"].sum())), 2)
+    if len(lat) == len(tr):
+        tail = np.argsort(lat)[-max(1, len(lat) // 100):]
+        out["slowest_1pct_mean_ms"] = {k[:-3]: round(float(col[k][tail].mean()) / 1e6, 3)
+                                       for k in ("queue_ns", "copy_ns", "to_dispatch_ns", "kernel_ns", "d2h_ns",
+                                                 "dispatch_to_done_ns")}
+        out["slowest_1pct_mean_rows"] = round(float(col["rows"][tail].mean()))
+    return out
+
+
 def run_serving(bst, torch, local, rank):
     """Serving on a 1000-tree depth-8 forest of the 100-feature workload,
     replayed from a native submitter thread (latency from each request's
@@ -266,19 +286,23 @@ def run_serving(bst, torch, local, rank):
     srv = bst.PredictionServer(model, mem_budget_bytes=4 << 30)
     rng = np.random.default_rng(7 + rank)
 
-    def play(rate, n_req, ring=256, rows=pool):
+    def play(rate, n_req, ring=256, rows=pool, phases=False):
         arr, offs, sizes = serve_schedule(rng, rate, n_req, pool.shape[0])
+        srv.trace()  # drop earlier records
         lat, span, _ = srv.replay(rows, arr, offs, sizes, ring=ring)
-        return {"p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
-                "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
-                "rows_per_s": round(int(sizes.sum()) / span)}
+        r = {"p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
+             "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
+             "rows_per_s": round(int(sizes.sum()) / span)}
+        if phases:
+            r["phases"] = phase_split(srv.trace(), lat)
+        return r
 
     try:
         play(10_000, 2_000)  # warm-up
         st0 = srv.stats()
-        head = play(10_000, 20_000)
+        head = play(10_000, 20_000, phases=True)
         st1 = srv.stats()
-        sweep = {str(r): play(r, 10_000) for r in (14_000, 17_000, 20_000, 23_000)}
+        sweep = {str(r): play(r, 10_000, phases=r == 17_000) for r in (14_000, 17_000, 20_000, 23_000)}
         sat = play(None, 3_000, ring=1024)
         # rows already in device memory (a GPU feature pipeline): no PCIe leg
         dev = {str(r): play(r, 10_000, rows=pool_dev) for r in (10_000, 17_000, 25_000, 34_000)}
@@ -286,11 +310,13 @@ def run_serving(bst, torch, local, rank):
     finally:
         srv.close()
     batches = st1["batches"] - st0["batches"]
+    h2d_gbs = (st1["h2d_bytes"] - st0["h2d_bytes"]) / max(1, st1["h2d_ns"] - st0["h2d_ns"])
     best = max([head["rows_per_s"]] + [v["rows_per_s"] for v in sweep.values() if v["p99_ms"] <= 2.0] + [0])
     return {"forest": "1000 trees, depth 8, 100 features (binary-logistic workload)",
             "arrivals": "Poisson, rows floor(exp(U ln 65537)) in [1, 65536], pinned host rows, native submitter",
             "requests": 20_000, "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"],
-            "rows_per_s_at_10k_req_s": head["rows_per_s"],
+            "rows_per_s_at_10k_req_s": head["rows_per_s"], "phases_at_10k_req_s": head["phases"],
+            "h2d_gb_per_s_at_10k_req_s": round(h2d_gbs, 2),
             "mean_batch_rows": round((st1["rows"] - st0["rows"]) / max(1, batches)),
             "sweep_req_per_s": sweep, "max_rows_per_s_with_p99_le_2ms": best,
             "saturation_rows_per_s": sat["rows_per_s"],

@@ -728,6 +728,15 @@ class PredictionServer:
         _n.check(_n.lib.bst_server_stats_get(self._h, ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in _n.ServerStats._fields_}
 
+    def trace(self, max_records=1 << 20):
+        """Phase records of the requests completed since the last call, as a
+        ``(k, 8)`` uint64 array with columns ``_n.SERVER_PHASES`` (ns)."""
+        out = np.zeros((int(max_records), len(_n.SERVER_PHASES)), np.uint64)
+        got = ctypes.c_uint64()
+        _n.check(_n.lib.bst_server_trace(self._h, ctypes.c_void_p(out.ctypes.data), int(max_records),
+                                         ctypes.byref(got)))
+        return out[: got.value]
+
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             _n.lib.bst_server_free(self._h)

@@ -84,4 +84,15 @@ class Split(ctypes.Structure):
 
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("batches", ctypes.c_uint64),
-                ("rows", ctypes.c_uint64), ("max_rows_seen", ctypes.c_uint64), ("max_batch_rows", ctypes.c_uint64)]
+                ("rows", ctypes.c_uint64), ("max_rows_seen", ctypes.c_uint64), ("max_batch_rows", ctypes.c_uint64),
+                ("h2d_bytes", ctypes.c_uint64), ("h2d_ns", ctypes.c_uint64)]
+
+
+SERVER_PHASES = ("rows", "batch_rows", "queue_ns", "copy_ns", "to_dispatch_ns", "kernel_ns", "d2h_ns",
+                 "dispatch_to_done_ns")
+
+
+class ServerPhase(ctypes.Structure):
+    """bst_server_phase: one completed request's phases (ns)."""
+
+    _fields_ = [(k, ctypes.c_uint64) for k in SERVER_PHASES]

@@ -109,6 +109,8 @@ SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64),
       ctypes.POINTER(ctypes.c_uint64)]),
     ("bst_server_stats_get", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
+    ("bst_server_trace", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                          ctypes.POINTER(ctypes.c_uint64)]),
     ("bst_server_replay", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),

@@ -984,6 +984,12 @@ bst_status bst_server_stats_get(bst_server* server, bst_server_stats* out) {
     return BST_OK;
 }
 
+bst_status bst_server_trace(bst_server* server, bst_server_phase* out, uint64_t max, uint64_t* n) {
+    if (!server || !n || (max && !out)) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    *n = bst::server_trace(*server->s, out, max);
+    return BST_OK;
+}
+
 bst_status bst_server_replay(bst_server* server, const float* pool, uint64_t pool_rows, uint64_t n_req,
                              const uint64_t* arrival_ns, const uint64_t* row_off, const uint64_t* n_rows, float* out,
                              uint64_t ring, uint64_t ring_stride, uint64_t* latency_ns, uint64_t* span_ns) {

@@ -947,7 +947,7 @@ class Trainer {
         // block: each item zeroes and flushes a whole shared histogram, so
         // fewer, larger items cost less (measured on B200, 1M x 100 q8: 0.95
         // ms per tree at three items per block, 0.88 at two or one)
-        const uint32_t blocks = n_lane_tiles_ ? 148u * lane_blocks_per_sm(qmode_) : 148u * 3u;
+        const uint32_t blocks = n_lane_tiles_ ? sm_count() * lane_blocks_per_sm(qmode_) : sm_count() * 3u;
         const uint32_t tiles = std::max<uint32_t>(1, n_lane_tiles_ ? n_lane_tiles_ : n_tiles_);
         bd_.hist_target = std::max<uint32_t>(1, 2u * blocks / tiles);
         bd_.hist_seg_max = n_lane_tiles_ ? lane_segment_max(qmode_) : (uint32_t)HIST_CHUNK_MAX;
@@ -1046,7 +1046,7 @@ class Trainer {
                       uint64_t& hist_launches, bool wide = false) {
         // resident general-tile blocks per SM: 64 registers x 256 threads
         // allow 4; the fixed-point form's 16 B/bin shared histograms allow 3
-        const uint32_t g_hist = 148 * (qmode_ == GRAD_F32 ? 3 : 4);
+        const uint32_t g_hist = sm_count() * (qmode_ == GRAD_F32 ? 3 : 4);
         tm.begin(PH_HIST);
         if (n_lane_tiles_)
             launch_b_hist_part(bd_, lane_tiles_.p, n_lane_tiles_, ridx, gr, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16,
@@ -1069,7 +1069,7 @@ class Trainer {
         const GradRef gh = grad_ref(o);
         const double* scale = unit_scale(o);
         float* pred = pred_.p + (size_t)o * n_;
-        const uint32_t g_wide = 148 * 8;
+        const uint32_t g_wide = sm_count() * 8;
         LeafParams lp{(double)cfg_.lambda, (double)cfg_.alpha, (double)cfg_.min_gain, cfg_.learning_rate, 0u};
         launches = 0;
         hist_launches = 0;

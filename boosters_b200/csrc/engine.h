@@ -199,6 +199,9 @@ uint64_t server_submit(Server& s, const float* rows, uint64_t n, float* out);
 int server_wait(Server& s, uint64_t id, int64_t timeout_ms, uint64_t* submit_ns, uint64_t* done_ns,
                 std::string* err);
 void server_stats(Server& s, bst_server_stats* out);
+// Moves up to `max` phase records of completed requests (oldest first) out
+// of the server's trace; returns how many.
+uint64_t server_trace(Server& s, bst_server_phase* out, uint64_t max);
 void server_replay(Server& s, const float* pool, uint64_t pool_rows, uint64_t n_req, const uint64_t* arrival_ns,
                    const uint64_t* row_off, const uint64_t* n_rows, float* out, uint64_t ring, uint64_t ring_stride,
                    uint64_t* latency_ns, uint64_t* span_ns);

@@ -16,9 +16,27 @@
 
 namespace bst {
 
+uint32_t sm_count() {
+    thread_local int dev_cached = -1;
+    thread_local uint32_t sms = 1;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return sms;
+    }
+    if (dev != dev_cached) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) cudaGetLastError();
+        sms = v > 0 ? (uint32_t)v : 1u;
+        dev_cached = dev;
+    }
+    return sms;
+}
+
 namespace {
 
 constexpr unsigned FULL = 0xFFFFFFFFu;
+
 
 __device__ __forceinline__ int32_t sat_i32(double v) {
     if (v != v) return 0;
@@ -258,7 +276,7 @@ __global__ void k_maxabs(const float2* __restrict__ gh, uint64_t n, unsigned* __
 void launch_maxabs(const float2* gh, uint64_t n, unsigned* maxabs, cudaStream_t st) {
     if (n == 0) return;
     uint64_t blocks = (n + 255) / 256;
-    if (blocks > 148ull * 8) blocks = 148ull * 8;
+    if (blocks > (uint64_t)sm_count() * 8) blocks = (uint64_t)sm_count() * 8;
     k_maxabs<<<(unsigned)blocks, 256, 0, st>>>(gh, n, maxabs);
 }
 
@@ -267,7 +285,7 @@ void launch_gradients(int objective, uint32_t G, const float* pred, const float*
                       cudaStream_t st) {
     if (n == 0) return;
     uint64_t blocks = (n + 255) / 256;
-    if (blocks > 148ull * 8) blocks = 148ull * 8;
+    if (blocks > (uint64_t)sm_count() * 8) blocks = (uint64_t)sm_count() * 8;
     k_gradients<<<(unsigned)blocks, 256, 2 * G * sizeof(unsigned), st>>>(objective, G, pred, y, w, n, gh, maxabs);
 }
 
@@ -802,7 +820,7 @@ void launch_b_hist_part(const BDev& d, const LaneTile* tiles, uint32_t n_tiles, 
                         void* part, cudaStream_t st) {
     if (n_tiles == 0) return;
     init_kernel_attributes();
-    const unsigned g = 148u * lane_blocks_per_sm(gr.mode), th = lane_threads(gr.mode);
+    const unsigned g = sm_count() * lane_blocks_per_sm(gr.mode), th = lane_threads(gr.mode);
     const size_t smem = lane_smem_bytes(gr.mode);
     if (gr.mode == GRAD_Q16)
         k_b_hist_part<GRAD_Q16><<<g, th, smem, st>>>(d, tiles, n_tiles, ridx, gr, bins8, s8, bins16, s16, part);
@@ -993,7 +1011,7 @@ template <typename HB>
 static void launch_b_merge_t(const BDev& d, HB* hist, uint64_t slot_bins, uint32_t total_bins, const void* part,
                              uint32_t n_lane_tiles, const uint2* ent, uint32_t n_ent, const uint32_t* bin_map,
                              bool has_rest, int root, int mode, cudaStream_t st, int wide) {
-    const unsigned grid = 148u * 8u;
+    const unsigned grid = sm_count() * 8u;
     if (n_lane_tiles) {
         if (wide) {
             if (mode == GRAD_F32)
@@ -1191,7 +1209,7 @@ void launch_quantize(int mode, uint32_t G, const float2* gh, uint64_t n, const u
     if (G == 0) return;
     const uint64_t total = n * G;
     uint64_t blocks = (total + 255) / 256;
-    if (blocks > 148ull * 16) blocks = 148ull * 16;
+    if (blocks > (uint64_t)sm_count() * 16) blocks = (uint64_t)sm_count() * 16;
     if (blocks == 0) blocks = 1;
     const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     if (mode == GRAD_Q8)
@@ -1809,7 +1827,7 @@ __global__ void k_iota(uint32_t* __restrict__ r, uint64_t n) {
 void launch_iota(uint32_t* ridx, uint64_t n, cudaStream_t st) {
     if (n == 0) return;
     uint64_t blocks = (n + 255) / 256;
-    if (blocks > 148ull * 16) blocks = 148ull * 16;
+    if (blocks > (uint64_t)sm_count() * 16) blocks = (uint64_t)sm_count() * 16;
     k_iota<<<(unsigned)blocks, 256, 0, st>>>(ridx, n);
 }
 
@@ -1843,7 +1861,7 @@ void launch_leaf_update(const LeafSeg* leaves, uint32_t n_leaves, const uint32_t
                         uint64_t n, float* pred, uint32_t* row_leaf, cudaStream_t st) {
     if (n == 0 || n_leaves == 0) return;
     uint64_t blocks = (n + 255) / 256;
-    if (blocks > 148ull * 16) blocks = 148ull * 16;
+    if (blocks > (uint64_t)sm_count() * 16) blocks = (uint64_t)sm_count() * 16;
     k_leaf_update<<<(unsigned)blocks, 256, 0, st>>>(leaves, n_leaves, ridx, n, pred, row_leaf);
 }
 
@@ -2803,10 +2821,10 @@ static HeapPlan heap_plan(const HeapForest& f, uint32_t F, uint64_t n) {
     uint64_t rmax = (PREDICT_SMEM - PREDICT_RING) / per_row;
     if (rmax > PREDICT_MAX_ROWS) rmax = PREDICT_MAX_ROWS;
     rmax &= ~(uint64_t)(PREDICT_MIN_ROWS - 1);
-    // whole waves of 148 tiles: as few waves as the largest tile allows, the
+    // whole waves of one tile per SM: as few waves as the largest tile allows, the
     // rows spread evenly over them (a small batch over every SM)
-    const uint64_t waves = n ? (n + 148 * rmax - 1) / (148 * rmax) : 1;
-    uint64_t r = (n + 148 * waves - 1) / (148 * waves);
+    const uint64_t waves = n ? (n + sm_count() * rmax - 1) / (sm_count() * rmax) : 1;
+    uint64_t r = (n + sm_count() * waves - 1) / (sm_count() * waves);
     r = (r + PREDICT_MIN_ROWS - 1) / PREDICT_MIN_ROWS * PREDICT_MIN_ROWS;
     if (r < PREDICT_MIN_ROWS) r = PREDICT_MIN_ROWS;
     if (r > rmax) r = rmax;
@@ -3070,7 +3088,7 @@ void launch_predict_heap(const HeapForest& f, const float* x, uint64_t n, uint32
         // warp items: row groups x feature chunks, about 32 warps per SM
         const uint32_t wr = f.bins16 ? 64u : 128u;
         const uint64_t groups = (n + wr - 1) / wr;
-        const uint64_t want = 148u * 32u;
+        const uint64_t want = sm_count() * 32u;
         const uint64_t fgs = (NF + BIN_F - 1) / BIN_F;
         uint64_t n_fc = groups >= want ? 1 : (want + groups - 1) / groups;
         if (n_fc > fgs) n_fc = fgs;
@@ -3078,14 +3096,14 @@ void launch_predict_heap(const HeapForest& f, const float* x, uint64_t n, uint32
         const uint32_t FC = (uint32_t)((fgs + n_fc - 1) / n_fc) * BIN_F;
         const uint64_t items = groups * ((NF + FC - 1) / FC);
         const uint64_t blocks = (items + BIN_THREADS / 32u - 1) / (BIN_THREADS / 32u);
-        const unsigned grid = (unsigned)(blocks < 148u * 4u ? blocks : 148u * 4u);
+        const unsigned grid = (unsigned)(blocks < sm_count() * 4u ? blocks : sm_count() * 4u);
         const size_t smem = (predict_spl_floats(NF) + (size_t)(BIN_THREADS / 32u) * wr * BIN_XS_LD) * sizeof(float);
         if (f.bins16)
             k_bin_rows<uint16_t><<<grid, BIN_THREADS, smem, st>>>(f, x, n, F, p.R, FC, static_cast<uint32_t*>(scratch));
         else
             k_bin_rows<uint8_t><<<grid, BIN_THREADS, smem, st>>>(f, x, n, F, p.R, FC, static_cast<uint32_t*>(scratch));
     }
-    const unsigned grid = (unsigned)(tiles < 148u ? tiles : 148u);
+    const unsigned grid = (unsigned)(tiles < sm_count() ? tiles : sm_count());
     const unsigned threads = p.R * p.S;
     const unsigned char* bg = static_cast<const unsigned char*>(scratch);
     if (f.has_cat)
@@ -3140,7 +3158,7 @@ __global__ void k_zero_unsampled(float2* __restrict__ gh, const uint8_t* __restr
 
 void launch_zero_unsampled(float2* gh, const uint8_t* mask, uint64_t n, cudaStream_t st) {
     if (n == 0) return;
-    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148ull * 8);
+    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 8);
     k_zero_unsampled<<<(unsigned)blocks, 256, 0, st>>>(gh, mask, n);
 }
 
@@ -3151,7 +3169,7 @@ __global__ void k_add_f32(float* __restrict__ a, const float* __restrict__ b, ui
 
 void launch_add_f32(float* a, const float* b, uint64_t n, cudaStream_t st) {
     if (n == 0) return;
-    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148ull * 8);
+    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 8);
     k_add_f32<<<(unsigned)blocks, 256, 0, st>>>(a, b, n);
 }
 

@@ -16,6 +16,10 @@
 
 namespace bst {
 
+// Streaming multiprocessors of the current device (cached per host thread
+// and device): launch grids are sized in whole waves of it.
+uint32_t sm_count();
+
 // Histogram bin: exact 64-bit fixed-point sums of grad and hess.
 struct HBin {
     long long g, h;

@@ -41,10 +41,10 @@ uint64_t now_ns() {
 
 struct Server {
     static constexpr int SLOTS = 3;
-    // Coalescing stops at one full wave of the traversal (148 SMs x 768-row
-    // tiles) unless the caller caps batches explicitly: a larger batch runs
+    // Coalescing stops at one full wave of the traversal (one 768-row tile
+    // per SM) unless the caller caps batches explicitly: a larger batch runs
     // in two waves and holds every request in it for both.
-    static constexpr uint64_t COALESCE_ROWS = 148ull * 768ull;
+    static constexpr uint64_t WAVE_TILE_ROWS = 768ull;
 
     struct Req {
         uint64_t id = 0;
@@ -52,16 +52,20 @@ struct Server {
         uint64_t n = 0;
         float* out = nullptr;
         uint64_t submit_ns = 0, done_ns = 0;
+        uint64_t admit_ns = 0, dispatch_ns = 0;  // copy issued; batch launched
         int status = -1;      // -1 pending, else bst_status
         uint64_t pos = 0;     // first ring row, once admitted
-        cudaEvent_t copied = nullptr;  // recorded after the request's copy
+        cudaEvent_t copy_start = nullptr;  // recorded before the request's copy
+        cudaEvent_t copied = nullptr;      // recorded after the request's copy
     };
     struct Slot {
         DevArray<float> d_out;
         DevArray<unsigned char> scratch;  // the traversal's bin tiles
         cudaStream_t st = nullptr;
-        cudaEvent_t done = nullptr;
+        cudaEvent_t done = nullptr;        // after the output copies
+        cudaEvent_t k0 = nullptr, k1 = nullptr;  // around binning + traversal + transform
         std::vector<uint64_t> reqs;  // ticket ids, in ring order
+        uint64_t rows = 0;
         bool busy = false;
     };
 
@@ -86,7 +90,22 @@ struct Server {
     int error = BST_OK;
     std::string error_msg;
     bst_server_stats stats{};
+    // per-request phase record of every completed request, until drained
+    // (bst_server_trace); capped so an undrained server stays bounded
+    static constexpr size_t TRACE_MAX = 1u << 20;
+    std::vector<bst_server_phase> trace;
     std::thread dispatcher, completer;
+
+    cudaEvent_t take_event() {  // caller holds mu
+        cudaEvent_t ev;
+        if (!events.empty()) {
+            ev = events.back();
+            events.pop_back();
+        } else {
+            BST_CK(cudaEventCreate(&ev));  // timing enabled: the copy's duration is traced
+        }
+        return ev;
+    }
 
     Server(const Model& model, uint64_t budget, uint64_t cap, bool raw_out) : m(model), raw(raw_out) {
         device = m.device;
@@ -101,7 +120,7 @@ struct Server {
         if (max_rows == 0)
             throw Error{BST_ERR_INVALID_ARGUMENT, "memory budget below one row per in-flight slot"};
         if (max_rows > 0xFFFFFFFFull) max_rows = 0xFFFFFFFFull;
-        coalesce_rows = cap ? max_rows : std::min(max_rows, COALESCE_ROWS);
+        coalesce_rows = cap ? max_rows : std::min(max_rows, (uint64_t)sm_count() * WAVE_TILE_ROWS);
         ring_rows = (uint64_t)SLOTS * max_rows;  // the slots' input share of the budget
         ring.alloc((size_t)ring_rows * std::max<uint64_t>(1, F));
         BST_CK(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking));
@@ -110,7 +129,9 @@ struct Server {
             s.d_out.alloc((size_t)max_rows * G);
             if (scratch) s.scratch.alloc(scratch);
             BST_CK(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
-            BST_CK(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+            BST_CK(cudaEventCreate(&s.done));
+            BST_CK(cudaEventCreate(&s.k0));
+            BST_CK(cudaEventCreate(&s.k1));
         }
         stats.max_batch_rows = max_rows;
         dispatcher = std::thread([this] { dispatch_loop(); });
@@ -139,10 +160,14 @@ struct Server {
         for (auto& s : slots) {
             if (s.st) cudaStreamSynchronize(s.st);
             if (s.done) cudaEventDestroy(s.done);
+            if (s.k0) cudaEventDestroy(s.k0);
+            if (s.k1) cudaEventDestroy(s.k1);
             if (s.st) cudaStreamDestroy(s.st);
         }
-        for (auto& kv : reqs)
+        for (auto& kv : reqs) {
+            if (kv.second.copy_start) cudaEventDestroy(kv.second.copy_start);
             if (kv.second.copied) cudaEventDestroy(kv.second.copied);
+        }
         for (cudaEvent_t e : events) cudaEventDestroy(e);
         if (cst) cudaStreamDestroy(cst);
     }
@@ -183,18 +208,14 @@ struct Server {
             Req& r = reqs[pending.front()];
             uint64_t pos;
             if (!ring_alloc(r.n, &pos)) break;
-            cudaEvent_t ev;
-            if (!events.empty()) {
-                ev = events.back();
-                events.pop_back();
-            } else {
-                BST_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-            }
-            r.copied = ev;
+            r.copy_start = take_event();
+            r.copied = take_event();
             r.pos = pos;
+            r.admit_ns = now_ns();
+            BST_CK(cudaEventRecord(r.copy_start, cst));
             if (F)
                 BST_CK(cudaMemcpyAsync(ring.p + pos * F, r.rows, sizeof(float) * r.n * F, cudaMemcpyDefault, cst));
-            BST_CK(cudaEventRecord(ev, cst));
+            BST_CK(cudaEventRecord(r.copied, cst));
             live.emplace_back(pos, r.n);
             admitted.push_back(r.id);
             pending.pop_front();
@@ -245,7 +266,10 @@ struct Server {
             return BST_ERR_TIMEOUT;
         const Req r = reqs[id];
         reqs.erase(id);
-        if (r.copied && r.status != BST_OK) cudaEventDestroy(r.copied);  // never returned to the pool
+        if (r.status != BST_OK) {  // never returned to the pool
+            if (r.copy_start) cudaEventDestroy(r.copy_start);
+            if (r.copied) cudaEventDestroy(r.copied);
+        }
         if (submit_ns) *submit_ns = r.submit_ns;
         if (done_ns) *done_ns = r.done_ns;
         return r.status;
@@ -305,7 +329,12 @@ struct Server {
                 Slot& s = slots[si];
                 s.busy = true;
                 s.reqs.clear();
-                for (auto& r : batch) s.reqs.push_back(r.id);
+                s.rows = rows;
+                const uint64_t t = now_ns();
+                for (auto& r : batch) {
+                    s.reqs.push_back(r.id);
+                    reqs[r.id].dispatch_ns = t;
+                }
                 stats.batches += 1;
                 stats.rows += rows;
                 stats.max_rows_seen = std::max<uint64_t>(stats.max_rows_seen, rows);
@@ -313,10 +342,12 @@ struct Server {
             Slot& s = slots[si];
             try {
                 BST_CK(cudaStreamWaitEvent(s.st, batch.back().copied, 0));  // copies are in order on cst
+                BST_CK(cudaEventRecord(s.k0, s.st));
                 forest_predict_rows(f, ring.p + batch.front().pos * F, rows, F, s.d_out.p, s.st, s.scratch.p,
                                     s.scratch.n);
                 if (!raw) launch_transform(tr, s.d_out.p, (uint32_t)G, rows, s.st);
                 BST_CK(cudaGetLastError());
+                BST_CK(cudaEventRecord(s.k1, s.st));
                 uint64_t off = 0;
                 for (auto& r : batch) {
                     for (uint64_t g = 0; g < G; ++g)
@@ -358,15 +389,43 @@ struct Server {
                 cudaGetLastError();
                 fail_all(BST_ERR_CUDA, std::string("batch failed: ") + cudaGetErrorString(e));
             } else {
+                float k_ms = 0.0f, d_ms = 0.0f;
+                if (cudaEventElapsedTime(&k_ms, s.k0, s.k1) != cudaSuccess ||
+                    cudaEventElapsedTime(&d_ms, s.k1, s.done) != cudaSuccess) {
+                    cudaGetLastError();
+                    k_ms = d_ms = 0.0f;
+                }
                 for (uint64_t id : s.reqs) {
                     auto it = reqs.find(id);
                     if (it == reqs.end()) continue;
-                    it->second.status = BST_OK;
-                    it->second.done_ns = t;
-                    if (it->second.copied) {
-                        events.push_back(it->second.copied);
-                        it->second.copied = nullptr;
+                    Req& r = it->second;
+                    r.status = BST_OK;
+                    r.done_ns = t;
+                    float c_ms = 0.0f;
+                    if (r.copy_start && r.copied && cudaEventElapsedTime(&c_ms, r.copy_start, r.copied) != cudaSuccess) {
+                        cudaGetLastError();
+                        c_ms = 0.0f;
                     }
+                    const uint64_t copy_ns = (uint64_t)((double)c_ms * 1e6);
+                    stats.h2d_bytes += r.n * F * sizeof(float);
+                    stats.h2d_ns += copy_ns;
+                    if (trace.size() < TRACE_MAX) {
+                        bst_server_phase ph;
+                        ph.rows = r.n;
+                        ph.batch_rows = s.rows;
+                        ph.queue_ns = r.admit_ns - r.submit_ns;
+                        ph.copy_ns = copy_ns;
+                        ph.to_dispatch_ns = r.dispatch_ns - r.admit_ns;
+                        ph.kernel_ns = (uint64_t)((double)k_ms * 1e6);
+                        ph.d2h_ns = (uint64_t)((double)d_ms * 1e6);
+                        ph.dispatch_to_done_ns = t - r.dispatch_ns;
+                        trace.push_back(ph);
+                    }
+                    for (cudaEvent_t* e : {&r.copy_start, &r.copied})
+                        if (*e) {
+                            events.push_back(*e);
+                            *e = nullptr;
+                        }
                     if (!live.empty()) live.pop_front();  // batches retire in admission order
                 }
                 stats.completed += s.reqs.size();
@@ -489,6 +548,13 @@ int server_wait(Server& s, uint64_t id, int64_t timeout_ms, uint64_t* submit_ns,
 void server_stats(Server& s, bst_server_stats* out) {
     std::lock_guard<std::mutex> lk(s.mu);
     *out = s.stats;
+}
+uint64_t server_trace(Server& s, bst_server_phase* out, uint64_t max) {
+    std::lock_guard<std::mutex> lk(s.mu);
+    const uint64_t n = std::min<uint64_t>(max, s.trace.size());
+    if (n && out) std::memcpy(out, s.trace.data(), n * sizeof(bst_server_phase));
+    s.trace.erase(s.trace.begin(), s.trace.begin() + (ptrdiff_t)n);
+    return n;
 }
 
 }  // namespace bst

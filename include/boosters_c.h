@@ -430,14 +430,30 @@ typedef struct bst_server_stats {
     uint64_t rows;           /* rows predicted                               */
     uint64_t max_rows_seen;  /* largest batch                                */
     uint64_t max_batch_rows; /* batch capacity from the memory budget        */
+    uint64_t h2d_bytes;      /* request rows copied to the device            */
+    uint64_t h2d_ns;         /* device time of those copies (CUDA events)    */
 } bst_server_stats;
+
+/* Phases of one completed request, in ns: host steady-clock intervals and
+ * device (CUDA event) durations. */
+typedef struct bst_server_phase {
+    uint64_t rows;                /* the request's rows                         */
+    uint64_t batch_rows;          /* rows of the batch it shared                */
+    uint64_t queue_ns;            /* submit -> copy issued (ring room)          */
+    uint64_t copy_ns;             /* device time of its host->device copy       */
+    uint64_t to_dispatch_ns;      /* copy issued -> its batch launched          */
+    uint64_t kernel_ns;           /* device time of the batch's binning,        */
+                                  /* traversal and transform                    */
+    uint64_t d2h_ns;              /* device time of the batch's output copies   */
+    uint64_t dispatch_to_done_ns; /* batch launched -> completion seen          */
+} bst_server_phase;
 
 /* The model stays device-resident and must outlive the server. The device
  * memory of the in-flight batches (3 slots of input + output rows) is bounded
  * by mem_budget_bytes; max_batch_rows caps a batch further (0: requests
- * coalesce up to one full wave of the traversal, 113,664 rows, and a single
- * request may fill a whole slot). raw != 0: margins; else the objective's
- * transform. */
+ * coalesce up to one full wave of the traversal, 768 rows per SM, i.e.
+ * 113,664 on a 148-SM B200, and a single request may fill a whole slot).
+ * raw != 0: margins; else the objective's transform. */
 bst_status bst_server_create(const bst_model* model, uint64_t mem_budget_bytes, uint64_t max_batch_rows,
                              int32_t raw, bst_server** out);
 /* Queues n_rows sample-major rows [n_rows, n_features] f32 for prediction
@@ -456,6 +472,9 @@ bst_status bst_server_submit(bst_server* server, const float* rows, uint64_t n_r
 bst_status bst_server_wait(bst_server* server, uint64_t ticket, int64_t timeout_ms, uint64_t* submit_ns,
                            uint64_t* done_ns);
 bst_status bst_server_stats_get(bst_server* server, bst_server_stats* out);
+/* Moves up to max phase records of completed requests (oldest first; the
+ * server keeps at most 2^20 until they are taken) into out; *n = how many. */
+bst_status bst_server_trace(bst_server* server, bst_server_phase* out, uint64_t max, uint64_t* n);
 /* Load replay (capacity planning and latency measurement): submits n_req
  * requests from a native thread at steady-clock offsets arrival_ns[i]
  * (non-decreasing, from a start 1 ms after the call), request i being rows

@@ -287,3 +287,30 @@ def test_device_resident_requests(model):
     np.testing.assert_array_equal(dout.cpu().numpy(), want[:, 100:600])
     for i in range(n_req):
         np.testing.assert_array_equal(ring[i, :, :sizes[i]], want[:, offs[i]:offs[i] + sizes[i]])
+
+
+def test_phase_trace(model):
+    """Every completed request leaves one phase record (in completion order,
+    which is submission order); copies of host rows take device time and the
+    copied bytes add up to the rows sent."""
+    rng = np.random.default_rng(5)
+    F = model.n_features
+    sizes = [3, 4000, 65536, 17, 900]
+    srv = bst.PredictionServer(model)
+    try:
+        srv.trace()
+        st0 = srv.stats()
+        tickets = [srv.submit(request_rows(rng, s, F)) for s in sizes]
+        for t in tickets:
+            srv.wait(t)
+        tr = srv.trace()
+        st1 = srv.stats()
+    finally:
+        srv.close()
+    cols = dict(zip(n.SERVER_PHASES, tr.T))
+    assert cols["rows"].tolist() == sizes
+    assert (cols["batch_rows"] >= cols["rows"]).all()
+    big = cols["rows"] >= 900  # event resolution is about 0.5 us
+    assert (cols["copy_ns"][big] > 0).all() and (cols["kernel_ns"] > 0).all()
+    assert st1["h2d_bytes"] - st0["h2d_bytes"] == sum(sizes) * F * 4
+    assert st1["h2d_ns"] - st0["h2d_ns"] == int(cols["copy_ns"].sum())
