@@ -897,6 +897,8 @@ class Trainer {
     DevArray<BLeaf> d_bleaves_;
     DevArray<BColumn> d_bcols_;
     DevArray<uint32_t> d_seg_exp_;
+    DevArray<uint2> d_part_map_;    // partition chunk -> (expansion, first row)
+    DevArray<uint2> d_leaf_map_;    // leaf chunk -> (leaf, first row)
     DevArray<uint8_t> d_part_;      // partial histograms of the lane tiles
     DevArray<uint32_t> d_bin_map_;  // global bin -> (lane tile, partial entry)
     DevArray<uint2> d_ent_;         // node partial entry -> (global bin, lane tile / offset)
@@ -943,6 +945,14 @@ class Trainer {
         d_bexp_.alloc(max_front / 2 + 1);
         bd_.state = d_bstate_.p;
         bd_.exp = d_bexp_.p;
+        const uint64_t max_pc = n_ / B_PART_CHUNK + max_front + 16;
+        d_part_map_.alloc(max_pc);
+        bd_.part_map = d_part_map_.p;
+        bd_.max_part_chunks = (uint32_t)max_pc;
+        const uint64_t max_lc = n_ / B_LEAF_CHUNK + max_front + 16;
+        d_leaf_map_.alloc(max_lc);
+        bd_.leaf_map = d_leaf_map_.p;
+        bd_.max_leaf_chunks = (uint32_t)max_lc;
         // about two (row segment, lane tile) items per resident histogram
         // block: each item zeroes and flushes a whole shared histogram, so
         // fewer, larger items cost less (measured on B200, 1M x 100 q8: 0.95

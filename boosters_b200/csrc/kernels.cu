@@ -1918,20 +1918,6 @@ __device__ float leaf_value_dev(long long G, long long H, const double* scale, c
     return w * lp.learning_rate;
 }
 
-// last index i in [0, n) with key(i) <= c (key non-decreasing, key(0) <= c)
-template <class F>
-__device__ __forceinline__ uint32_t last_le(uint32_t n, uint32_t c, F key) {
-    uint32_t lo = 0, hi = n;
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (key(mid) <= c)
-            lo = mid;
-        else
-            hi = mid;
-    }
-    return lo;
-}
-
 __device__ void write_leaf(BTreeNode& t, long long G, long long H, const double* scale, float v) {
     t.col = 0;
     t.bin = 0;
@@ -2068,6 +2054,13 @@ __device__ void decide_body(BDev d, int a, LeafParams lp, const double* __restri
             w.pad = 0;
             for (int q = 0; q < 4; ++q) w.cats[q] = nd.split.cats[q];
             d.pworks[j] = w;
+            // the partition's chunks of this node, so that each partition
+            // block finds its node with one load (capacity: rows / chunk +
+            // nodes, never exceeded)
+            for (uint32_t k = 0; k < nch; ++k) {
+                const uint32_t c = base_chunk + jc + k;
+                if (c < d.max_part_chunks) d.part_map[c] = make_uint2(j, nd.begin + k * B_PART_CHUNK);
+            }
             d.cursors[2 * j] = nd.begin;
             d.cursors[2 * j + 1] = nd.begin + nd.count;
             if (d.rmask) d.scnt[2 * j] = d.scnt[2 * j + 1] = 0u;
@@ -2119,17 +2112,16 @@ k_b_partition(BDev d, const uint32_t* __restrict__ ridx, uint32_t* __restrict__ 
               const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16,
               int a, int need_split, const Q* __restrict__ qin, Q* __restrict__ qout, BinsFM fm) {
     __shared__ PartWork w;
-    __shared__ uint32_t s_j;
-    const uint32_t total = d.state->part_chunks, n_exp = d.state->n_exp;
+    __shared__ uint2 s_m;
+    const uint32_t total = min(d.state->part_chunks, d.max_part_chunks);
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
         if (threadIdx.x == 0) {
-            const uint32_t j = last_le(n_exp, c, [&](uint32_t k) { return d.exp[k].part_off; });
-            s_j = j;
-            w = d.pworks[j];
+            const uint2 m = d.part_map[c];  // (expansion, first row)
+            s_m = m;
+            w = d.pworks[m.x];
         }
         __syncthreads();
-        const uint32_t j = s_j;
-        const uint32_t start = w.begin + (c - d.exp[j].part_off) * B_PART_CHUNK;
+        const uint32_t j = s_m.x, start = s_m.y;
         const uint32_t len = min(B_PART_CHUNK, w.begin + w.count - start);
         part_rows<Q>(w, start, len, d.cursors + 2 * j, ridx, tmp, bins8, s8, bins16, s16, qin, qout, fm.b8, fm.b16,
                      fm.n, d.rmask, d.rmask ? d.scnt + 2 * j : nullptr);
@@ -2261,16 +2253,16 @@ __device__ void children_body(BDev d, int a, int need_split) {
         const uint32_t nch = valid ? (d.exp[j].small_count + chunk - 1) / chunk : 0u;
         uint32_t tc;
         const uint32_t jc = block_excl_scan(nch, sh, &tc);
-        if (valid) d.exp[j].hist_off = base + jc;
+        if (valid) {
+            d.exp[j].hist_off = base + jc;
+            // segment -> expansion, written by the segment's owner (the
+            // buffer bound always holds)
+            for (uint32_t k = 0; k < nch; ++k)
+                if (base + jc + k < d.max_segs) d.seg_exp[base + jc + k] = j;
+        }
         __syncthreads();
         if (threadIdx.x == 0) base += tc;
         __syncthreads();
-    }
-    // segment -> expansion, all threads (the buffer bound always holds)
-    {
-        const uint32_t total = base < d.max_segs ? base : d.max_segs;
-        for (uint32_t c = threadIdx.x; c < total; c += blockDim.x)
-            d.seg_exp[c] = last_le(n_exp, c, [&](uint32_t k) { return d.exp[k].hist_off; });
     }
     if (!need_split)  // the node sums of k_b_sums accumulate from zero
         for (uint32_t i = threadIdx.x; i < 2 * n_exp; i += blockDim.x) d.sums[i] = 0;
@@ -2331,14 +2323,16 @@ __global__ void __launch_bounds__(1024) k_lw_children(BDev d, const PartWork* __
         const uint32_t nch = valid ? (d.exp[j].small_count + chunk - 1) / chunk : 0u;
         uint32_t tc;
         const uint32_t jc = block_excl_scan(nch, sh, &tc);
-        if (valid) d.exp[j].hist_off = base + jc;
+        if (valid) {
+            d.exp[j].hist_off = base + jc;
+            for (uint32_t q = 0; q < nch; ++q)  // segment -> expansion, by the owner
+                if (base + jc + q < d.max_segs) d.seg_exp[base + jc + q] = j;
+        }
         __syncthreads();
         if (threadIdx.x == 0) base += tc;
         __syncthreads();
     }
     const uint32_t total = base < d.max_segs ? base : d.max_segs;
-    for (uint32_t c = threadIdx.x; c < total; c += blockDim.x)
-        d.seg_exp[c] = last_le(k, c, [&](uint32_t q) { return d.exp[q].hist_off; });
     if (threadIdx.x == 0) {
         d.state->n_exp = k;
         d.state->hist_chunks = total;
@@ -2617,10 +2611,16 @@ __global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams l
     const uint32_t nl = n0 + nf;
     for (uint32_t l0 = 0; l0 < nl; l0 += blockDim.x) {
         const uint32_t l = l0 + threadIdx.x;
+        const uint32_t begin = l < nl ? d.leaves[l].begin : 0u;
         const uint32_t nch = l < nl ? (d.leaves[l].count + B_LEAF_CHUNK - 1) / B_LEAF_CHUNK : 0u;
         uint32_t tc;
         const uint32_t jc = block_excl_scan(nch, sh, &tc);
-        if (l < nl) d.leaves[l].chunk_off = base + jc;
+        if (l < nl) {
+            d.leaves[l].chunk_off = base + jc;
+            for (uint32_t k = 0; k < nch; ++k)  // chunk -> (leaf, first row), by the leaf's owner
+                if (base + jc + k < d.max_leaf_chunks)
+                    d.leaf_map[base + jc + k] = make_uint2(l, begin + k * B_LEAF_CHUNK);
+        }
         __syncthreads();
         if (threadIdx.x == 0) base += tc;
         __syncthreads();
@@ -2629,7 +2629,7 @@ __global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams l
     for (uint32_t i = threadIdx.x; i < 2 * nl; i += blockDim.x) d.sums[i] = 0;
     if (threadIdx.x == 0) {
         s->n_leaves = nl;
-        s->leaf_chunks = base;
+        s->leaf_chunks = base < d.max_leaf_chunks ? base : d.max_leaf_chunks;
         s->n_front = 0;
     }
 }
@@ -2646,12 +2646,12 @@ __device__ void leaf_values_body(BDev d, LeafParams lp, const double* __restrict
 // gradients' fixed-point scales).
 __global__ void k_b_leaf_sums(BDev d, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1, GradRef gr,
                               LeafParams lp, const double* __restrict__ scale) {
-    const uint32_t total = d.state->leaf_chunks, nl = d.state->n_leaves;
+    const uint32_t total = d.state->leaf_chunks;
     const GradLoad<GRAD_F32> load(gr);
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
-        const uint32_t l = last_le(nl, c, [&](uint32_t k) { return d.leaves[k].chunk_off; });
+        const uint2 m = d.leaf_map[c];
+        const uint32_t l = m.x, start = m.y;
         const BLeaf lf = d.leaves[l];
-        const uint32_t start = lf.begin + (c - lf.chunk_off) * B_LEAF_CHUNK;
         const uint32_t len = min(B_LEAF_CHUNK, lf.begin + lf.count - start);
         const uint32_t* ridx = lf.buf ? r1 : r0;
         long long ag = 0, ah = 0;
@@ -2686,11 +2686,11 @@ __device__ void leaf_values_body(BDev d, LeafParams lp, const double* __restrict
 // pred[row] += leaf value over the final partition (grower.rs:208-219).
 __global__ void k_b_leaf_update(BDev d, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1,
                                 float* __restrict__ pred, uint32_t* __restrict__ row_leaf) {
-    const uint32_t total = d.state->leaf_chunks, nl = d.state->n_leaves;
+    const uint32_t total = d.state->leaf_chunks;
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
-        const uint32_t l = last_le(nl, c, [&](uint32_t k) { return d.leaves[k].chunk_off; });
-        const BLeaf lf = d.leaves[l];
-        const uint32_t start = lf.begin + (c - lf.chunk_off) * B_LEAF_CHUNK;
+        const uint2 m = d.leaf_map[c];
+        const BLeaf lf = d.leaves[m.x];
+        const uint32_t start = m.y;
         const uint32_t len = min(B_LEAF_CHUNK, lf.begin + lf.count - start);
         const uint32_t* ridx = lf.buf ? r1 : r0;
         // RANGE_ILP rows per step: row ids, then predictions, then stores

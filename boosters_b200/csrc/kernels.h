@@ -310,6 +310,10 @@ struct BDev {  // device buffers of the level loop
     unsigned long long* node_key;  // [max_front] best candidate key per node; zero between levels
     const uint8_t* rmask;  // row sampling: the tree's sampled rows [n] (or null)
     unsigned* scnt;        // row sampling: [max_front][2] sampled rows per side of each expansion
+    uint2* part_map;       // partition chunk -> (expansion, first row), written with the decisions
+    uint32_t max_part_chunks;  // capacity of part_map
+    uint2* leaf_map;       // leaf chunk -> (leaf, first row), written by k_b_finalize
+    uint32_t max_leaf_chunks;  // capacity of leaf_map
 };
 constexpr uint32_t B_PART_CHUNK = 2048;
 constexpr uint32_t B_LEAF_CHUNK = 4096;
