@@ -324,8 +324,15 @@ bst_status plan_binning(const float* x, uint64_t F, uint64_t n,
         off += m.n_bins;
     }
     plan.total_bins = off;
-    plan.s8 = (plan.f8 + 15) / 16 * 16;
-    plan.s16 = (plan.f16 + 7) / 8 * 8;
+    // One record per row: the u8 columns, then from a 16-byte boundary the
+    // u16 columns, the whole padded to a 32-byte sector (80 u8 + 20 u16
+    // columns: 128 bytes, one cache line). Rows start on sector boundaries,
+    // so every aligned 16- or 32-byte window of a row lies in one sector and
+    // a gathered row costs exactly its sectors.
+    plan.u16_off = plan.f16 ? (plan.f8 + 15) / 16 * 16 : plan.f8;
+    plan.rec = (plan.u16_off + 2 * plan.f16 + 31) / 32 * 32;
+    plan.s8 = plan.rec;       // row stride of the u8 view, bytes
+    plan.s16 = plan.rec / 2;  // row stride of the u16 view (record + u16_off), elements
     return BST_OK;
 }
 

@@ -45,7 +45,12 @@ struct BinPlan {
     std::vector<uint32_t> col_feature, col_nbins, col_hist_off, col_default, col_matrix, col_pos;
     std::vector<uint8_t> col_cat, col_missing;
     uint32_t f8 = 0, f16 = 0;  // columns per matrix
-    uint32_t s8 = 0, s16 = 0;  // padded row strides (elements)
+    // Row record (binning.cpp): rec bytes per row, u8 columns at bytes
+    // [0, f8), u16 columns at [u16_off, u16_off + 2 f16). The two matrices
+    // are views of it: bins8 = record (stride s8 = rec bytes), bins16 =
+    // record + u16_off (stride s16 = rec / 2 elements).
+    uint32_t u16_off = 0, rec = 0;
+    uint32_t s8 = 0, s16 = 0;
     uint32_t total_bins = 0;
     uint32_t n_cols() const { return (uint32_t)col_feature.size(); }
 };

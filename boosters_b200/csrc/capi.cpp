@@ -249,10 +249,10 @@ bst_status bst_binned_column_bins(const bst_binned* b, uint32_t col, uint16_t* o
         const uint64_t n = p.n;
         if (p.col_matrix[col] == 0) {
             std::vector<uint8_t> tmp(n);
-            BST_CK(cudaMemcpy2D(tmp.data(), 1, b->b.bins8.p + p.col_pos[col], p.s8, 1, n, cudaMemcpyDeviceToHost));
+            BST_CK(cudaMemcpy2D(tmp.data(), 1, b->b.bins8 + p.col_pos[col], p.s8, 1, n, cudaMemcpyDeviceToHost));
             for (uint64_t i = 0; i < n; ++i) out[i] = tmp[i];
         } else {
-            BST_CK(cudaMemcpy2D(out, 2, b->b.bins16.p + p.col_pos[col], (size_t)p.s16 * 2, 2, n, cudaMemcpyDeviceToHost));
+            BST_CK(cudaMemcpy2D(out, 2, b->b.bins16 + p.col_pos[col], (size_t)p.s16 * 2, 2, n, cudaMemcpyDeviceToHost));
         }
         return BST_OK;
     });
@@ -668,8 +668,7 @@ bst_status bst_bin_values(const double* bounds, uint32_t n_bounds, int32_t missi
         bst::DevArray<float> dx, dthr;
         bst::DevArray<int32_t> dc;
         bst::DevArray<bst::BinColumn> dcol;
-        bst::DevArray<uint8_t> b8;
-        bst::DevArray<uint16_t> b16;
+        bst::DevArray<uint8_t> rec;
         dx.alloc(n);
         BST_CK(cudaMemcpy(dx.p, values, sizeof(float) * n, cudaMemcpyHostToDevice));
         dthr.alloc(std::max<size_t>(1, thr.size()));
@@ -678,19 +677,19 @@ bst_status bst_bin_values(const double* bounds, uint32_t n_bounds, int32_t missi
         if (!cv.empty()) BST_CK(cudaMemcpy(dc.p, cv.data(), sizeof(int32_t) * cv.size(), cudaMemcpyHostToDevice));
         dcol.alloc(1);
         BST_CK(cudaMemcpy(dcol.p, &bc, sizeof(bc), cudaMemcpyHostToDevice));
-        const uint32_t s8 = wide ? 0 : 16, s16 = wide ? 8 : 0;
-        if (s8) b8.alloc(n * s8);
-        if (s16) b16.alloc(n * s16);
-        bst::launch_bin_assign(dx.p, n, dcol.p, 1, dthr.p, dc.p, b8.p, s8, b16.p, s16, st);
+        // one column: a 32-byte record per value, the bin at byte 0
+        constexpr uint32_t REC = 32;
+        rec.alloc(n * REC);
+        bst::launch_bin_assign(dx.p, n, dcol.p, 1, dthr.p, dc.p, rec.p, REC, 0, st);
         BST_CK(cudaGetLastError());
         BST_CK(cudaDeviceSynchronize());
         if (!wide) {
             std::vector<uint8_t> t(n);
-            BST_CK(cudaMemcpy2D(t.data(), 1, b8.p, s8, 1, n, cudaMemcpyDeviceToHost));
+            BST_CK(cudaMemcpy2D(t.data(), 1, rec.p, REC, 1, n, cudaMemcpyDeviceToHost));
             for (uint64_t i = 0; i < n; ++i) out[i] = t[i];
         } else {
             std::vector<uint16_t> t(n);
-            BST_CK(cudaMemcpy2D(t.data(), 2, b16.p, (size_t)s16 * 2, 2, n, cudaMemcpyDeviceToHost));
+            BST_CK(cudaMemcpy2D(t.data(), 2, rec.p, REC, 2, n, cudaMemcpyDeviceToHost));
             for (uint64_t i = 0; i < n; ++i) out[i] = t[i];
         }
         return BST_OK;

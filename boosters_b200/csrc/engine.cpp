@@ -107,10 +107,11 @@ void build_hist_tiles(const BinPlan& p, std::vector<HistTile>& tiles, uint32_t& 
     for (auto& t : tiles) max_smem = std::max(max_smem, t.smem_bins);
 }
 
-// Column-lane tiles: aligned 32-byte windows of each matrix row (a 16-byte
-// window for a row tail of 16 bytes). A window holding a column with more
-// than max_bins bins is left to the HistTile kernel: its columns are marked
-// in `rest`.
+// Column-lane tiles: windows of each view of the row record, cut at the
+// record's 32-byte sector boundaries (32 bytes, or 16 where a view starts or
+// ends inside a sector), so that each window read touches one sector. A
+// window holding a column with more than max_bins bins is left to the
+// HistTile kernel: its columns are marked in `rest`.
 void build_lane_tiles(const BinPlan& p, uint32_t max_bins, std::vector<LaneTile>& tiles, uint32_t& tile_bins,
                       std::vector<uint8_t>& rest) {
     tiles.clear();
@@ -119,12 +120,14 @@ void build_lane_tiles(const BinPlan& p, uint32_t max_bins, std::vector<LaneTile>
     rest.assign(nc, 0);
     for (uint32_t m = 0; m < 2; ++m) {
         const uint32_t esize = m == 0 ? 1u : 2u;
-        const uint32_t row_bytes = m == 0 ? p.s8 : p.s16 * 2u;
+        const uint32_t view = m == 0 ? 0u : p.u16_off;  // the view's offset in the record (a multiple of 16)
+        const uint32_t row_bytes = ((m == 0 ? p.f8 : p.f16) * esize + 15) / 16 * 16;
         std::vector<int> col_at(row_bytes / esize, -1);
         for (uint32_t c = 0; c < nc; ++c)
             if (p.col_matrix[c] == m) col_at[p.col_pos[c]] = (int)c;
         for (uint32_t off = 0; off < row_bytes;) {
-            const uint32_t width = row_bytes - off >= 32 ? 32u : 16u;
+            const uint32_t to_sector = 32u - (view + off) % 32u;  // 16 or 32
+            const uint32_t width = std::min(to_sector, row_bytes - off);
             LaneTile t;
             std::memset(&t, 0, sizeof(t));
             t.esize = esize;
@@ -873,9 +876,9 @@ class Trainer {
         if (use_batched_ || spec_leafwise_) {
             if (use_batched_) setup_batched();
             for (auto& q : qpos_) q.alloc((size_t)n_ * grad_bytes());
-            if (p_.s8) fm8_.alloc((size_t)n_ * p_.s8);
-            if (p_.s16) fm16_.alloc((size_t)n_ * p_.s16);
-            launch_transpose_bins(b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, n_, fm8_.p, fm16_.p, st_);
+            if (p_.f8) fm8_.alloc((size_t)n_ * p_.f8);
+            if (p_.f16) fm16_.alloc((size_t)n_ * p_.f16);
+            launch_transpose_bins(b_.bins8, p_.s8, p_.f8, b_.bins16, p_.s16, p_.f16, n_, fm8_.p, fm16_.p, st_);
             BST_CK(cudaGetLastError());
             fm_ = BinsFM{fm8_.p, fm16_.p, n_};
         }
@@ -1059,10 +1062,10 @@ class Trainer {
         const uint32_t g_hist = sm_count() * (qmode_ == GRAD_F32 ? 3 : 4);
         tm.begin(PH_HIST);
         if (n_lane_tiles_)
-            launch_b_hist_part(bd_, lane_tiles_.p, n_lane_tiles_, ridx, gr, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16,
+            launch_b_hist_part(bd_, lane_tiles_.p, n_lane_tiles_, ridx, gr, b_.bins8, p_.s8, b_.bins16, p_.s16,
                                d_part_.p, st_);
         if (n_tiles_)
-            launch_b_hist(bd_, tiles_.p, n_tiles_, tile_smem_, ridx, gr, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16,
+            launch_b_hist(bd_, tiles_.p, n_tiles_, tile_smem_, ridx, gr, b_.bins8, p_.s8, b_.bins16, p_.s16,
                           hist_.p, slot_bins_, g_hist, st_, hist32_);
         tm.end();
         tm.begin(PH_OTHER);
@@ -1107,7 +1110,7 @@ class Trainer {
             const void* qin = d == 0 ? (qmode_ == GRAD_F32 ? (const void*)gh.gh : gh.gq) : (const void*)qpos_[d & 1u].p;
             void* qout = qpos_[(d + 1) & 1u].p;  // the last level's node sums read it too
             tm.begin(PH_PART);
-            launch_b_partition(bd_, R[d & 1u], rout, b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, a, need_split ? 1 : 0,
+            launch_b_partition(bd_, R[d & 1u], rout, b_.bins8, p_.s8, b_.bins16, p_.s16, a, need_split ? 1 : 0,
                                g_wide, qin, qout, qmode_, fm_, st_);  // + children
             tm.end();
             launches += 1;
@@ -1491,13 +1494,13 @@ class Trainer {
         if (rowsample_) BST_CK(cudaMemsetAsync(d_scnt_.p, 0, sizeof(unsigned) * 2 * k, st_));
         if (spec_leafwise_) {
             launch_partition(d_pworks_.p, d_pchunks_.p, (uint32_t)pch.size(), ridx_.p, tmp_.p, d_cursors_.p,
-                             b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, st_, qpos_[0].p, qpos_[1].p, qmode_, fm_,
+                             b_.bins8, p_.s8, b_.bins16, p_.s16, st_, qpos_[0].p, qpos_[1].p, qmode_, fm_,
                              rowmask(tree_output_), d_scnt_.p);
             launch_copy_chunks(d_pchunks_.p, d_pworks_.p, (uint32_t)pch.size(), tmp_.p, ridx_.p, st_, qpos_[1].p,
                                qpos_[0].p, qmode_);
         } else {
             launch_partition(d_pworks_.p, d_pchunks_.p, (uint32_t)pch.size(), ridx_.p, tmp_.p, d_cursors_.p,
-                             b_.bins8.p, p_.s8, b_.bins16.p, p_.s16, st_, nullptr, nullptr, 0, BinsFM{},
+                             b_.bins8, p_.s8, b_.bins16, p_.s16, st_, nullptr, nullptr, 0, BinsFM{},
                              rowmask(tree_output_), d_scnt_.p);
             launch_copy_chunks(d_pchunks_.p, d_pworks_.p, (uint32_t)pch.size(), tmp_.p, ridx_.p, st_);
         }
@@ -1962,7 +1965,7 @@ void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, 
         out.binning_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         return;
     }
-    if (bin_assign_rows(p.s8, p.s16) == 0) throw Error{BST_ERR_UNSUPPORTED, "too many features for one row tile"};
+    if (bin_assign_rows(p.rec) == 0) throw Error{BST_ERR_UNSUPPORTED, "too many features for one row tile"};
     std::vector<BinColumn> cols(nc);
     std::vector<float> thr;
     std::vector<int32_t> cats;
@@ -2001,9 +2004,10 @@ void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, 
     d_cats.alloc(std::max<size_t>(1, cats.size()));
     if (!cats.empty())
         BST_CK(cudaMemcpyAsync(d_cats.p, cats.data(), sizeof(int32_t) * cats.size(), cudaMemcpyHostToDevice, st));
-    if (p.s8) out.bins8.alloc((size_t)n * p.s8);
-    if (p.s16) out.bins16.alloc((size_t)n * p.s16);
-    launch_bin_assign(x.p, n, d_cols.p, nc, d_thr.p, d_cats.p, out.bins8.p, p.s8, out.bins16.p, p.s16, st);
+    if (p.rec) out.rec.alloc((size_t)n * p.rec);
+    out.bins8 = out.rec.p;
+    out.bins16 = p.f16 ? reinterpret_cast<uint16_t*>(out.rec.p + p.u16_off) : nullptr;
+    launch_bin_assign(x.p, n, d_cols.p, nc, d_thr.p, d_cats.p, out.rec.p, p.rec, p.u16_off, st);
     BST_CK(cudaGetLastError());
     BST_CK(cudaStreamSynchronize(st));
     out.binning_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

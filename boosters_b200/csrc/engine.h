@@ -82,8 +82,9 @@ struct HostDataset {
 // Binned dataset resident on the GPU.
 struct DeviceBinned {
     BinPlan plan;
-    DevArray<uint8_t> bins8;
-    DevArray<uint16_t> bins16;
+    DevArray<uint8_t> rec;        // [n][plan.rec] row records
+    uint8_t* bins8 = nullptr;     // u8 view: rec
+    uint16_t* bins16 = nullptr;   // u16 view: rec + plan.u16_off (null without u16 columns)
     double binning_ms = 0.0;
 };
 

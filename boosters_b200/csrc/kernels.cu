@@ -74,23 +74,22 @@ __device__ __forceinline__ long long shfl_up_ll(long long v, int d) {
 __global__ void __launch_bounds__(128)
 k_bin_assign(const float* __restrict__ x, uint64_t n, const BinColumn* __restrict__ cols,
              uint32_t n_cols, const float* __restrict__ thr, const int32_t* __restrict__ cats,
-             uint8_t* __restrict__ bins8, uint32_t s8, uint16_t* __restrict__ bins16,
-             uint32_t s16) {
-    // one thread per row of a tile of blockDim.x rows
+             uint8_t* __restrict__ rec_out, uint32_t rec, uint32_t u16_off) {
+    // one thread per row of a tile of blockDim.x rows; the tile's records are
+    // assembled in shared memory, then copied out as one contiguous run
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t rows = blockDim.x;
-    uint8_t* t8 = smem;
-    uint16_t* t16 = reinterpret_cast<uint16_t*>(smem + (size_t)rows * s8);
     const uint64_t r0 = (uint64_t)blockIdx.x * rows;
     const uint64_t rem = n - r0;
     const uint32_t valid = rem < (uint64_t)rows ? (uint32_t)rem : rows;
-    const uint32_t tile_bytes = rows * s8 + rows * s16 * 2u;
+    const uint32_t tile_bytes = rows * rec;  // rec is a multiple of 32
     for (uint32_t i = threadIdx.x * 16u; i < tile_bytes; i += rows * 16u)
         *reinterpret_cast<uint4*>(smem + i) = make_uint4(0, 0, 0, 0);
     __syncthreads();
     const uint32_t t = threadIdx.x;
     if (t < valid) {
         const uint64_t row = r0 + t;
+        unsigned char* my = smem + (size_t)t * rec;
         for (uint32_t c = 0; c < n_cols; ++c) {
             const BinColumn col = cols[c];
             const float v = x[(uint64_t)c * n + row];
@@ -124,45 +123,35 @@ k_bin_assign(const float* __restrict__ x, uint64_t n, const BinColumn* __restric
                 bin = lo;
             }
             if (col.matrix == 0)
-                t8[t * s8 + col.pos] = (uint8_t)bin;
+                my[col.pos] = (uint8_t)bin;
             else
-                t16[t * s16 + col.pos] = (uint16_t)bin;
+                reinterpret_cast<uint16_t*>(my + u16_off)[col.pos] = (uint16_t)bin;
         }
     }
     __syncthreads();
-    if (s8) {
-        const uint32_t nvec = valid * s8 / 16u;
-        uint4* dst = reinterpret_cast<uint4*>(bins8 + r0 * s8);
-        const uint4* src = reinterpret_cast<const uint4*>(t8);
-        for (uint32_t i = threadIdx.x; i < nvec; i += rows) dst[i] = src[i];
-    }
-    if (s16) {
-        const uint32_t nvec = valid * s16 * 2u / 16u;
-        uint4* dst = reinterpret_cast<uint4*>(bins16 + r0 * s16);
-        const uint4* src = reinterpret_cast<const uint4*>(t16);
-        for (uint32_t i = threadIdx.x; i < nvec; i += rows) dst[i] = src[i];
-    }
+    const uint32_t nvec = valid * rec / 16u;
+    uint4* dst = reinterpret_cast<uint4*>(rec_out + r0 * rec);
+    const uint4* src = reinterpret_cast<const uint4*>(smem);
+    for (uint32_t i = threadIdx.x; i < nvec; i += rows) dst[i] = src[i];
 }
 
-int bin_assign_rows(uint32_t s8, uint32_t s16) {
-    const size_t per_row = (size_t)s8 + (size_t)s16 * 2;
+int bin_assign_rows(uint32_t rec) {
     for (int rows = 128; rows >= 32; rows -= 32)
-        if ((size_t)rows * per_row <= 160 * 1024) return rows;
+        if ((size_t)rows * rec <= 160 * 1024) return rows;
     return 0;
 }
 
 void launch_bin_assign(const float* x_fm, uint64_t n, const BinColumn* cols, uint32_t n_cols,
-                       const float* thr, const int32_t* cats, uint8_t* bins8, uint32_t s8,
-                       uint16_t* bins16, uint32_t s16, cudaStream_t st) {
-    if (n == 0 || n_cols == 0) return;
-    const int rows = bin_assign_rows(s8, s16);
+                       const float* thr, const int32_t* cats, uint8_t* rec_out, uint32_t rec, uint32_t u16_off,
+                       cudaStream_t st) {
+    if (n == 0 || n_cols == 0 || rec == 0) return;
+    const int rows = bin_assign_rows(rec);
     if (rows == 0) return;
     const uint64_t blocks = (n + rows - 1) / rows;
-    const size_t smem = (size_t)rows * s8 + (size_t)rows * s16 * 2;
+    const size_t smem = (size_t)rows * rec;
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_bin_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    k_bin_assign<<<(unsigned)blocks, rows, smem, st>>>(x_fm, n, cols, n_cols, thr, cats, bins8, s8,
-                                                     bins16, s16);
+    k_bin_assign<<<(unsigned)blocks, rows, smem, st>>>(x_fm, n, cols, n_cols, thr, cats, rec_out, rec, u16_off);
 }
 
 // ============================================================================
@@ -2149,32 +2138,36 @@ void launch_b_partition(const BDev& d, const uint32_t* rin, uint32_t* rout, cons
                                                              static_cast<float2*>(qout), fm);
 }
 
-// Column-major copy of a row-major bin matrix (s columns): 32 x 32 tiles
-// through shared memory, coalesced on both sides.
+// Column-major copy [f][n] of the first f columns of a row-major bin view
+// (row stride s elements): 32 x 32 tiles through shared memory, coalesced on
+// both sides.
 template <typename T>
-__global__ void k_transpose_bins(const T* __restrict__ in, uint32_t s, uint64_t n, T* __restrict__ out) {
+__global__ void k_transpose_bins(const T* __restrict__ in, uint32_t s, uint32_t f, uint64_t n,
+                                 T* __restrict__ out) {
     __shared__ T t[32][33];
     const uint64_t r0 = (uint64_t)blockIdx.x * 32u;
     const uint32_t c0 = blockIdx.y * 32u;
     for (uint32_t k = threadIdx.y; k < 32u; k += blockDim.y) {
         const uint64_t r = r0 + k;
         const uint32_t c = c0 + threadIdx.x;
-        if (r < n && c < s) t[k][threadIdx.x] = in[r * s + c];
+        if (r < n && c < f) t[k][threadIdx.x] = in[r * s + c];
     }
     __syncthreads();
     for (uint32_t k = threadIdx.y; k < 32u; k += blockDim.y) {
         const uint32_t c = c0 + k;
         const uint64_t r = r0 + threadIdx.x;
-        if (r < n && c < s) out[(uint64_t)c * n + r] = t[threadIdx.x][k];
+        if (r < n && c < f) out[(uint64_t)c * n + r] = t[threadIdx.x][k];
     }
 }
 
-void launch_transpose_bins(const uint8_t* b8, uint32_t s8, const uint16_t* b16, uint32_t s16, uint64_t n,
-                           uint8_t* fm8, uint16_t* fm16, cudaStream_t st) {
+void launch_transpose_bins(const uint8_t* b8, uint32_t s8, uint32_t f8, const uint16_t* b16, uint32_t s16,
+                           uint32_t f16, uint64_t n, uint8_t* fm8, uint16_t* fm16, cudaStream_t st) {
     const dim3 blk(32, 8);
-    if (s8 && n) k_transpose_bins<uint8_t><<<dim3((unsigned)((n + 31) / 32), (s8 + 31) / 32), blk, 0, st>>>(b8, s8, n, fm8);
-    if (s16 && n)
-        k_transpose_bins<uint16_t><<<dim3((unsigned)((n + 31) / 32), (s16 + 31) / 32), blk, 0, st>>>(b16, s16, n, fm16);
+    if (f8 && n)
+        k_transpose_bins<uint8_t><<<dim3((unsigned)((n + 31) / 32), (f8 + 31) / 32), blk, 0, st>>>(b8, s8, f8, n, fm8);
+    if (f16 && n)
+        k_transpose_bins<uint16_t><<<dim3((unsigned)((n + 31) / 32), (f16 + 31) / 32), blk, 0, st>>>(b16, s16, f16, n,
+                                                                                               fm16);
 }
 
 // Children of every split: ranges from the partition cursors, smaller child

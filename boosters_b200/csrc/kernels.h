@@ -1,14 +1,19 @@
 // kernels.h — device data layout and launch wrappers of the B200 GBDT engine.
 //
 // HBM layout (training):
-//   bins8   row-major u8  [n_rows][s8]   columns with <= 256 logical bins
-//   bins16  row-major u16 [n_rows][s16]  columns with  > 256 logical bins
+//   rec     [n_rows][rec] bytes          one record per row: u8 bins of the
+//                                        columns with <= 256 logical bins,
+//                                        then (from a 16-byte boundary) u16
+//                                        bins of the others
+//   bins8   u8 view of rec, row stride s8 = rec bytes
+//   bins16  u16 view at rec + u16_off, row stride s16 = rec / 2 elements
 //   gh      float2 [n_outputs][n_rows]   (grad, hess) of the current round
 //   ridx    u32 [n_rows]                 row ids grouped by partition node
 //   hist    HBin [n_slots][total_bins]   one histogram per partition node,
 //                                        64-bit fixed point (exact sums)
-// s8 is a multiple of 16 and s16 a multiple of 8 so that every row starts
-// on a 16-byte boundary and is read with 128-bit loads.
+// rec is a multiple of 32 bytes: every row starts on a sector boundary and
+// its aligned 16- or 32-byte windows are read with 128-bit loads, each
+// within one sector.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -44,11 +49,11 @@ struct BinColumn {
 
 // thr holds, per numeric column, the largest f32 <= each f64 upper bound, so
 // `v <= bound` (f64) equals `v <= thr` (f32) for every f32 v.
-// Rows per bin-assignment block for these strides (0 = row too wide).
-int bin_assign_rows(uint32_t s8, uint32_t s16);
+// Rows per bin-assignment block for this record size (0 = row too wide).
+int bin_assign_rows(uint32_t rec);
 void launch_bin_assign(const float* x_fm, uint64_t n, const BinColumn* cols, uint32_t n_cols,
-                       const float* thr, const int32_t* cats, uint8_t* bins8, uint32_t s8,
-                       uint16_t* bins16, uint32_t s16, cudaStream_t st);
+                       const float* thr, const int32_t* cats, uint8_t* rec_out, uint32_t rec, uint32_t u16_off,
+                       cudaStream_t st);
 
 // ---- K3 gradients ---------------------------------------------------------
 // maxabs [G][2] receives the bit patterns of max|grad|, max|hess| (atomicMax).
@@ -323,8 +328,8 @@ constexpr uint32_t B_LEAF_CHUNK = 4096;
 void init_kernel_attributes();
 void launch_b_root(const BDev& d, uint64_t n, cudaStream_t st);
 // Column-major copy of the bin matrices (BinsFM).
-void launch_transpose_bins(const uint8_t* b8, uint32_t s8, const uint16_t* b16, uint32_t s16, uint64_t n,
-                           uint8_t* fm8, uint16_t* fm16, cudaStream_t st);
+void launch_transpose_bins(const uint8_t* b8, uint32_t s8, uint32_t f8, const uint16_t* b16, uint32_t s16,
+                           uint32_t f16, uint64_t n, uint8_t* fm8, uint16_t* fm16, cudaStream_t st);
 // Level kernels; `a` is the index of the current frontier buffer. Row indices
 // alternate between two buffers: level d partitions buffer d & 1 into buffer
 // (d + 1) & 1; a leaf records the buffer that holds its rows.
