@@ -220,9 +220,30 @@ FORMS = [  # (name, GBDTConfig overrides); "plain" is the reference form on the 
 EQUAL_LOSS_REL = 1e-3
 
 
+TUNE_CACHE = os.path.join(__import__("tempfile").gettempdir(), f"bst_bench_autotune_{os.getpid()}.txt")
+
+
+def tune_form(bst, ds, cfg):
+    """Launch-shape tuning of one form before it is timed: a throwaway
+    booster explores the candidate shapes on its first trees and stores the
+    winner in the run's cache file, which the timed booster then reads (so
+    no candidate is explored inside the timed region)."""
+    import copy
+    if not cfg.batched or bst.GrowthStrategy(cfg.growth_strategy) == bst.GrowthStrategy.Leafwise:
+        return ""  # the tuned pipeline is the batched depth-wise one
+    c = copy.copy(cfg)
+    c.autotune, c.autotune_cache = True, TUNE_CACHE
+    c.n_estimators = 16
+    b = bst.Booster(ds, c, n_threads=0)
+    b.update(16)
+    return b.model().tune_info
+
+
 def run_form(bst, torch, ds, xv, yv, cfg, args, world):
     """W warm-up rounds, K timed rounds (one update call, device events),
     then the rest of the configured trees; held-out logloss of the result."""
+    tuned = tune_form(bst, ds, cfg)
+    cfg.autotune_cache = TUNE_CACHE
     booster = bst.Booster(ds, cfg, n_threads=0)
     booster.update(args.warmup)
     t0, c0 = booster.stats()
@@ -241,7 +262,7 @@ def run_form(bst, torch, ds, xv, yv, cfg, args, world):
     model = booster.model()
     pv = model.predict_group_major(bst.Dataset.from_feature_major(xv))
     return dict(elapsed=elapsed, t0=t0, t1=t1, c0=c0, c1=c1, heldout=bst.metric("logloss", pv, yv),
-                trees=booster.n_rounds, model=model)
+                trees=booster.n_rounds, model=model, shape=model.tune_info, explored=tuned)
 
 
 def serve_schedule(rng, rate, n_req, n_pool, max_rows=65536):
@@ -369,6 +390,9 @@ def run_ours(args, world, rank, local):
         forms[name] = {"s_per_100_trees": round(r["value"], 5), "heldout_logloss": round(r["heldout"], 6),
                        "loss_rel_vs_plain": round((r["heldout"] - plain_loss) / plain_loss, 6),
                        "equal_loss": r["equal_loss"], "trees": r["trees"]}
+        if r["shape"]:
+            forms[name]["launch_shape"] = r["shape"]
+            forms[name]["autotune"] = r["explored"]
     ok = [k for k, r in res.items() if r["equal_loss"]]
     head = min(ok, key=lambda k: res[k]["value"])
     hr = res[head]
@@ -493,6 +517,8 @@ def run_ours(args, world, rank, local):
 def time_trees(bst, torch, ds, cfg, warm, steps):
     """s/100 trees of `steps` timed rounds after `warm` (CUDA events on the
     engine's stream), then the rest of cfg's rounds; returns (value, model)."""
+    tune_form(bst, ds, cfg)
+    cfg.autotune_cache = TUNE_CACHE
     booster = bst.Booster(ds, cfg, n_threads=0)
     booster.update(warm)
     torch.cuda.synchronize()
@@ -517,6 +543,8 @@ def config_forms(bst, torch, ds, kw, forms, warm, steps, heldout):
     for name in forms:
         v, m = time_trees(bst, torch, ds, bst.GBDTConfig(**kw, **dict(FORMS)[name]), warm, steps)
         out[name] = {"s_per_100_trees": round(v, 5), "heldout_loss": round(heldout(m), 6), "trees": m.n_trees}
+        if m.tune_info:
+            out[name]["launch_shape"] = m.tune_info
         del m
     plain = out["plain"]["heldout_loss"]
     for r in out.values():

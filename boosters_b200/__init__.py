@@ -119,7 +119,9 @@ class GBDTConfig:
     (packages/boosters-python/src/config.rs:160-560, model/gbdt/config.rs:111-226),
     plus GPU options: precision ("fp32", "q16", "q8"), batched (depth-wise
     trees grown by a device-side level loop replayed as one CUDA graph per
-    tree; False selects the host-driven loop), cuda_graph, device."""
+    tree; False selects the host-driven loop), cuda_graph, device, autotune
+    (time launch-shape candidates on the first trees) and autotune_cache (a
+    file keeping the chosen shapes across runs)."""
 
     def __init__(self, n_estimators=100, learning_rate=0.3, objective=None, metric=None,
                  growth_strategy=GrowthStrategy.Depthwise, max_depth=6, n_leaves=31,
@@ -128,7 +130,8 @@ class GBDTConfig:
                  max_bins=256, enable_bundling=True, sparsity_threshold=0.9,
                  max_categorical_cardinality=0, binning_sample_cnt=200000, cache_size=8,
                  early_stopping_rounds=None, seed=42, verbosity=0, precision="fp32",
-                 cuda_graph=False, device=0, batched=True, phase_timings=False):
+                 cuda_graph=False, device=0, batched=True, phase_timings=False, autotune=True,
+                 autotune_cache=None):
         self.n_estimators = n_estimators
         self.learning_rate = learning_rate
         self.objective = objective if objective is not None else Objective.Squared()
@@ -161,6 +164,8 @@ class GBDTConfig:
         self.cuda_graph = cuda_graph
         self.device = device
         self.batched = batched
+        self.autotune = autotune
+        self.autotune_cache = None if autotune_cache is None else os.fspath(autotune_cache)
         _n.check(_n.lib.bst_config_validate(ctypes.byref(self.to_c())))
 
     def to_c(self, record_leaves=False):
@@ -198,6 +203,9 @@ class GBDTConfig:
         c.device = int(self.device)
         c.record_leaves = 1 if record_leaves else 0
         c.phase_timings = 1 if self.phase_timings else 0
+        c.autotune = 1 if self.autotune else 0
+        # the struct keeps the bytes object alive as long as the struct lives
+        c.autotune_cache = None if self.autotune_cache is None else os.fsencode(self.autotune_cache)
         return c
 
     def __repr__(self):
@@ -344,6 +352,14 @@ class GBDTModel:
             return ctypes.string_at(buf.value, n.value) if n.value else b""
         finally:
             _n.lib.bst_buffer_free(buf)
+
+    @property
+    def tune_info(self):
+        """The batched pipeline's launch shape and how it was chosen."""
+        buf = ctypes.create_string_buffer(4096)
+        n = ctypes.c_uint64()
+        _n.check(_n.lib.bst_model_tune_info(self._h, buf, len(buf), ctypes.byref(n)))
+        return buf.value.decode()
 
     def to_bytes(self, compression_level=3):
         """The model as a ``.bstr`` file: zstd-compressed MessagePack at

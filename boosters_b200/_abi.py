@@ -66,6 +66,8 @@ class Config(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("record_leaves", ctypes.c_int32),
         ("phase_timings", ctypes.c_int32),
+        ("autotune", ctypes.c_int32),
+        ("autotune_cache", ctypes.c_char_p),
     ]
 
 

@@ -73,6 +73,8 @@ SIGNATURES = [
     ("bst_model_tree_row_leaves", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32, c_u32p]),
     ("bst_model_train_timings", ctypes.c_int32, [ctypes.c_void_p, c_f64p]),
     ("bst_model_train_counters", ctypes.c_int32, [ctypes.c_void_p, c_u64p, ctypes.c_uint32]),
+    ("bst_model_tune_info", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_uint64,
+                                             ctypes.POINTER(ctypes.c_uint64)]),
     ("bst_booster_create", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.POINTER(Config), ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p)]),
     ("bst_booster_update", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),

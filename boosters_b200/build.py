@@ -23,8 +23,8 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fn
              "-Wall", "-Wno-unused-function", f"-I{CUDA}/include"]
 
 CU_SOURCES = ["kernels.cu", "noalloc.cu"]
-CPP_SOURCES = ["binning.cpp", "engine.cpp", "capi.cpp", "server.cpp", "synth.cpp", "persist.cpp"]
-HEADERS = ["kernels.h", "binning.h", "engine.h", "synth_gen.h", "api_util.h", os.path.join("..", "..", "include", "boosters_c.h")]
+CPP_SOURCES = ["binning.cpp", "engine.cpp", "capi.cpp", "server.cpp", "synth.cpp", "persist.cpp", "autotune.cpp"]
+HEADERS = ["kernels.h", "binning.h", "engine.h", "synth_gen.h", "api_util.h", "autotune.h", os.path.join("..", "..", "include", "boosters_c.h")]
 
 
 def _stale(obj, src):

@@ -143,6 +143,8 @@ void bst_config_default(bst_config* c) {
     c->device = 0;
     c->record_leaves = 0;
     c->phase_timings = 0;
+    c->autotune = 1;
+    c->autotune_cache = nullptr;
 }
 
 bst_status bst_config_validate(const bst_config* c) {
@@ -491,6 +493,18 @@ bst_status bst_model_train_counters(const bst_model* m, uint64_t* out, uint32_t 
     const bst::Counters& c = m->m->counters;
     const uint64_t v[6] = {c.launches, c.hist_launches, c.hist_rows, c.hist_bytes, c.scan_launches, c.partition_rows};
     for (uint32_t i = 0; i < n && i < 6; ++i) out[i] = v[i];
+    return BST_OK;
+}
+
+bst_status bst_model_tune_info(const bst_model* m, char* out, uint64_t cap, uint64_t* len) {
+    if (!m || (cap && !out)) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
+    const std::string& s = m->m->tune_info;
+    if (len) *len = s.size();
+    if (cap) {
+        const size_t k = std::min<size_t>(s.size(), (size_t)cap - 1);
+        std::memcpy(out, s.data(), k);
+        out[k] = '\0';
+    }
     return BST_OK;
 }
 

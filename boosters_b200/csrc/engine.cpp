@@ -8,6 +8,8 @@
 // the partition counts and the chosen splits.
 #include "engine.h"
 
+#include "autotune.h"
+
 #include <algorithm>
 #include <array>
 #include <atomic>
@@ -918,6 +920,8 @@ class Trainer {
         cudaEvent_t done = nullptr, w0 = nullptr, w1 = nullptr;
         bool pending = false;
         uint32_t o = 0;
+        uint32_t cand = 0;   // tuner candidate of the tree in the slot
+        bool timed = false;  // its time counts for the tuner
         std::vector<uint32_t> row_leaf;
     };
     Slot slots_[RING];
@@ -956,18 +960,17 @@ class Trainer {
         d_leaf_map_.alloc(max_lc);
         bd_.leaf_map = d_leaf_map_.p;
         bd_.max_leaf_chunks = (uint32_t)max_lc;
-        // about two (row segment, lane tile) items per resident histogram
-        // block: each item zeroes and flushes a whole shared histogram, so
-        // fewer, larger items cost less (measured on B200, 1M x 100 q8: 0.95
-        // ms per tree at three items per block, 0.88 at two or one)
-        const uint32_t blocks = n_lane_tiles_ ? sm_count() * lane_blocks_per_sm(qmode_) : sm_count() * 3u;
-        const uint32_t tiles = std::max<uint32_t>(1, n_lane_tiles_ ? n_lane_tiles_ : n_tiles_);
-        bd_.hist_target = std::max<uint32_t>(1, 2u * blocks / tiles);
+        // launch shapes: the built-in one, or the tuner's candidates (the
+        // buffers below are sized for the candidate with the most segments)
+        setup_tuning();
+        uint32_t tgt_max = hist_target_for(shape_.items, shape_.hist);
+        for (const TuneShape& c : tune_cands_) tgt_max = std::max(tgt_max, hist_target_for(c.items, c.hist));
         bd_.hist_seg_max = n_lane_tiles_ ? lane_segment_max(qmode_) : (uint32_t)HIST_CHUNK_MAX;
+        apply_shape(shape_);
         // segments per level <= rows / segment + nodes; the segment is at least
         // min(1024, seg_max) and at least rows / hist_target rounded up
         const uint64_t min_seg = std::max<uint64_t>(
-            1024, std::min<uint64_t>(bd_.hist_seg_max, (n_ + bd_.hist_target - 1) / bd_.hist_target));
+            1024, std::min<uint64_t>(bd_.hist_seg_max, (n_ + tgt_max - 1) / tgt_max));
         const uint64_t max_segs = n_ / std::min<uint64_t>(min_seg, HIST_CHUNK_MAX) + max_front + 16;
         d_seg_exp_.alloc(max_segs);
         bd_.seg_exp = d_seg_exp_.p;
@@ -995,6 +998,101 @@ class Trainer {
             d_bin_map_.alloc(std::max<uint64_t>(1, p_.total_bins));
             BST_CK(cudaMemset(d_bin_map_.p, 0xFF, sizeof(uint32_t) * std::max<uint64_t>(1, p_.total_bins)));
         }
+    }
+
+    // ---- launch-shape autotuning (autotune.h) ----------------------------------
+    TuneShape shape_;                   // the shape the current graphs use
+    std::vector<TuneShape> tune_cands_; // exploration candidates (empty: none)
+    TuneExplorer tuner_;
+    std::string tune_key_;
+    bool tune_stored_ = false;
+    uint32_t g_wide_ = 0;               // level-kernel grid of the current shape
+
+    // (row segment, lane tile) items per resident histogram block -> the
+    // level's segment count target. Each item zeroes and flushes a whole
+    // shared histogram, so fewer, larger items cost less, while too few
+    // leave SMs idle at the end of a level.
+    uint32_t hist_target_for(uint32_t items, uint32_t variant) const {
+        const uint32_t blocks =
+            n_lane_tiles_ ? sm_count() * lane_blocks_per_sm(qmode_, (int)variant) : sm_count() * 3u;
+        const uint32_t tiles = std::max<uint32_t>(1, n_lane_tiles_ ? n_lane_tiles_ : n_tiles_);
+        return std::max<uint32_t>(1, items * blocks / tiles);
+    }
+
+    void apply_shape(const TuneShape& sh) {
+        const bool changed = !(sh == shape_) || g_wide_ == 0;
+        shape_ = sh;
+        bd_.hist_target = hist_target_for(sh.items, sh.hist);
+        g_wide_ = sm_count() * sh.grid;
+        if (changed)  // graphs bake the shape in: capture again on next use
+            for (auto& g : graphs_)
+                if (g) {
+                    BST_CK(cudaGraphExecDestroy(g));  // an in-flight launch completes first
+                    g = nullptr;
+                }
+    }
+
+    // The built-in shape (measured on B200, 1M x 100 q8: 0.95 ms per tree
+    // at three items per block, 0.88 at two or one), a cached choice, or the
+    // candidates to explore on this run's first trees (batched depth-wise).
+    void setup_tuning() {
+        shape_ = TuneShape{};
+        tune_cands_.clear();
+        const bool depthwise_batched = cfg_.batched && !leafwise_ && cfg_.max_depth <= 14;
+        if (!depthwise_batched) return;
+        uint32_t lg = 0;
+        while ((1ull << (lg + 1)) <= n_) ++lg;
+        tune_key_ = device_signature(cfg_.device) + "|mode" + std::to_string(qmode_) + "|rec=" +
+                    std::to_string(p_.rec) + "|u16=" + std::to_string(p_.u16_off) + "|tiles=" +
+                    std::to_string(n_lane_tiles_) + "+" + std::to_string(n_tiles_) + "|log2n=" + std::to_string(lg) +
+                    "|depth=" + std::to_string(cfg_.max_depth) + "|G=" + std::to_string(G_);
+        const std::string path = cfg_.autotune_cache ? cfg_.autotune_cache : "";
+        TuneShape cached;
+        if (tune_cache_lookup(path, tune_key_, cached) && cached.hist < (uint32_t)lane_variants()) {
+            shape_ = cached;
+            m_.tune_info = shape_.str() + " (cached)";
+            tune_stored_ = true;
+            return;
+        }
+        if (!cfg_.autotune) {
+            m_.tune_info = shape_.str() + " (built-in)";
+            return;
+        }
+        // the built-in shape first, then items per block x histogram kernel
+        // variant, then a half-size level-kernel grid
+        tune_cands_.push_back(shape_);
+        for (uint32_t hist = 0; hist < (uint32_t)lane_variants(); ++hist)
+            for (uint32_t items : {1u, 2u}) {
+                TuneShape c;
+                c.items = items;
+                c.hist = hist;
+                c.grid = 8;
+                if (!(c == shape_)) tune_cands_.push_back(c);
+            }
+        TuneShape half = shape_;
+        half.grid = 4;
+        tune_cands_.push_back(half);
+        tuner_ = TuneExplorer(tune_cands_, 2, 1);
+        shape_ = tune_cands_[0];
+        m_.tune_info = "exploring";
+    }
+
+    // Exploration finished: keep the winner from the next launch on, and
+    // store it.
+    void finish_tuning() {
+        if (!tuner_.done() || tune_stored_) return;
+        tune_stored_ = true;
+        const TuneShape best = tuner_.best();
+        apply_shape(best);
+        const std::vector<double> med = tuner_.medians();
+        std::string info = best.str() + " (explored:";
+        for (size_t c = 0; c < med.size(); ++c) {
+            char buf[64];
+            std::snprintf(buf, sizeof buf, " %.3f", med[c]);
+            info += " " + tune_cands_[c].str() + buf;
+        }
+        m_.tune_info = info + " ms/tree)";
+        if (cfg_.autotune_cache) tune_cache_store(cfg_.autotune_cache, tune_key_, best);
     }
 
     void setup_batched() {
@@ -1063,7 +1161,7 @@ class Trainer {
         tm.begin(PH_HIST);
         if (n_lane_tiles_)
             launch_b_hist_part(bd_, lane_tiles_.p, n_lane_tiles_, ridx, gr, b_.bins8, p_.s8, b_.bins16, p_.s16,
-                               d_part_.p, st_);
+                               d_part_.p, (int)shape_.hist, st_);
         if (n_tiles_)
             launch_b_hist(bd_, tiles_.p, n_tiles_, tile_smem_, ridx, gr, b_.bins8, p_.s8, b_.bins16, p_.s16,
                           hist_.p, slot_bins_, g_hist, st_, hist32_);
@@ -1082,7 +1180,7 @@ class Trainer {
         const GradRef gh = grad_ref(o);
         const double* scale = unit_scale(o);
         float* pred = pred_.p + (size_t)o * n_;
-        const uint32_t g_wide = sm_count() * 8;
+        const uint32_t g_wide = g_wide_;
         LeafParams lp{(double)cfg_.lambda, (double)cfg_.alpha, (double)cfg_.min_gain, cfg_.learning_rate, 0u};
         launches = 0;
         hist_launches = 0;
@@ -1157,6 +1255,14 @@ class Trainer {
     void launch_batched(uint32_t o, uint32_t si) {
         Slot& sl = slots_[si];
         const size_t gi = (size_t)o * RING + si;
+        sl.timed = false;
+        if (tuner_.active()) {
+            bool timed = false;
+            const uint32_t c = tuner_.next(&timed);
+            apply_shape(tune_cands_[c]);
+            sl.cand = c;
+            sl.timed = timed;
+        }
         if (!graphs_[gi]) {
             gtimers_[gi] = std::make_unique<Timer>();
             gtimers_[gi]->st = st_;
@@ -1209,6 +1315,13 @@ class Trainer {
         BST_CK(cudaEventSynchronize(sl.done));
         BST_CK(cudaGetLastError());
         sl.pending = false;
+        if (sl.timed) {
+            float ms = 0.0f;
+            BST_CK(cudaEventElapsedTime(&ms, sl.w0, sl.w1));
+            tuner_.record(sl.cand, ms);
+            sl.timed = false;
+            finish_tuning();
+        }
         HostTree t;
         t.group = o;
         t.row_leaf = std::move(sl.row_leaf);
@@ -2057,6 +2170,7 @@ struct Booster::Impl {
     std::unique_ptr<Model> model;
     std::unique_ptr<Trainer> tr;
     bst_config cfg;
+    std::string tune_cache;  // owned copy: the caller's string may not outlive the call
     uint32_t done = 0;
 };
 
@@ -2065,6 +2179,8 @@ Booster::Booster(const HostDataset& ds, const bst_config& cfg, uint32_t n_thread
     impl_ = std::make_unique<Impl>();
     Impl& b = *impl_;
     b.cfg = cfg;
+    if (cfg.autotune_cache) b.tune_cache = cfg.autotune_cache;
+    b.cfg.autotune_cache = cfg.autotune_cache ? b.tune_cache.c_str() : nullptr;
     b.model = std::make_unique<Model>();
     Model& m = *b.model;
     m.device = cfg.device;
@@ -2105,6 +2221,7 @@ std::unique_ptr<Model> Booster::snapshot() const {
     for (int i = 0; i < 8; ++i) m->timings[i] = s.timings[i];
     m->counters = s.counters;
     m->device = s.device;
+    m->tune_info = s.tune_info;
     return m;
 }
 

@@ -148,6 +148,8 @@ struct Model {
     // best round + 1; 0 when early stopping was off or never improved)
     uint32_t rounds_run = 0, rounds_kept = 0;
     int device = 0;
+    // launch shape of the batched pipeline and how it was chosen (autotune.h)
+    std::string tune_info;
     mutable std::mutex mu;
     mutable std::unique_ptr<DeviceForest> dev;
     const DeviceForest& device_forest() const;

@@ -498,22 +498,35 @@ __device__ void hist_item(const HistChunk& chunk, const HistTile& tile, uint32_t
 // Shared histogram of a lane tile: LANE_ROWS bins x 32 slots per accumulator
 // plane (fixed height, so plane offsets are immediates).
 constexpr uint32_t LANE_ROWS = 264;
-__host__ __device__ constexpr uint32_t lane_threads(int mode) { return mode == GRAD_F32 ? 512u : 256u; }
 constexpr uint32_t LANE_PART_STRIDE = LANE_ROWS * 32u;  // partial entries per item
 constexpr uint32_t LANE_STAGES = 3;  // cp.async ring depth per warp
 constexpr uint32_t LANE_SLOT = 48;   // bytes per lane per stage (32 + 16 pad: conflict-free 16-byte reads)
-__host__ __device__ constexpr uint32_t lane_smem_bytes(int mode) {
-    return LANE_ROWS * 32u * acc_words(mode) * 4u + (lane_threads(mode) / 32u) * LANE_STAGES * 32u * LANE_SLOT;
+constexpr uint32_t LANE_REG_STAGES = 2;  // register ring depth per lane
+
+// Variants of the lane-tile kernel (the launch-shape tuner's `hist` knob):
+//   0: each warp stages its rows' windows through a LANE_STAGES-deep cp.async
+//      ring in shared memory; 256 threads (512 for the fixed-point form)
+//   1: a LANE_REG_STAGES-deep ring of 128-bit register loads instead (no
+//      staging memory: more resident blocks per SM); 256 / 512 threads
+//   2: the register ring with 512-thread blocks
+// Every variant sums the same values into the same partials.
+constexpr int LANE_VARIANTS = 3;
+__host__ __device__ constexpr uint32_t lane_threads(int mode, int v) {
+    return v == 2 ? 512u : (mode == GRAD_F32 ? 512u : 256u);
+}
+__host__ __device__ constexpr bool lane_regs(int v) { return v != 0; }
+__host__ __device__ constexpr uint32_t lane_smem_bytes(int mode, int v) {
+    return LANE_ROWS * 32u * acc_words(mode) * 4u +
+           (lane_regs(v) ? 0u : (lane_threads(mode, v) / 32u) * LANE_STAGES * 32u * LANE_SLOT);
+}
+// minimum resident blocks per SM asked of the compiler: a register budget
+// (65536 / (threads x blocks) per thread); variant 0 keeps its 64 registers
+__host__ __device__ constexpr uint32_t lane_min_blocks(int mode, int v) {
+    return mode == GRAD_F32 ? 1u : (v == 0 ? 4u : (v == 1 ? 3u : 2u));
 }
 
 uint32_t lane_tile_max_bins(int) { return LANE_ROWS; }
-
-uint32_t lane_blocks_per_sm(int mode) {
-    uint32_t b = (227u * 1024u) / (lane_smem_bytes(mode) + 1024u);
-    const uint32_t by_threads = 2048u / lane_threads(mode);
-    if (b > by_threads) b = by_threads;
-    return b ? b : 1u;
-}
+int lane_variants() { return LANE_VARIANTS; }
 
 uint32_t lane_segment_max(int mode) { return mode == GRAD_F32 ? (uint32_t)HIST_CHUNK_MAX : 16384u; }
 uint32_t lane_part_entry_bytes(int mode) { return mode == GRAD_F32 ? 16u : 8u; }
@@ -589,12 +602,117 @@ struct LaneAdd {  // quantised: one 32-bit sum each
 // into a LANE_STAGES-deep ring of shared-memory stages with cp.async (issued
 // LANE_STAGES - 1 iterations ahead, so the gathers overlap the atomics);
 // gradients are prefetched into registers the same distance ahead.
+// The window's words, rotated left by this lane's column offset, added to
+// the lane's slots (shared by both staging forms).
+template <int MODE, int ESIZE, int WORDS>
+__device__ __forceinline__ void lane_add_window(uint32_t (&w)[WORDS], uint32_t lr, uint32_t slot0, uint32_t rq,
+                                                uint32_t rs, const LaneAdd<MODE> a, uint32_t* sm) {
+    constexpr uint32_t C = WORDS * 4 / ESIZE;
+    constexpr uint32_t plane = LANE_ROWS * 32u;
+    // rotate left by rb bytes: whole words by rq, then bytes by rs bits
+#pragma unroll
+    for (int st = 1; st < WORDS; st <<= 1) {
+        const bool take = (rq & (uint32_t)st) != 0u;
+        uint32_t t[WORDS];
+#pragma unroll
+        for (int q = 0; q < WORDS; ++q) t[q] = take ? w[(q + st) % WORDS] : w[q];
+#pragma unroll
+        for (int q = 0; q < WORDS; ++q) w[q] = t[q];
+    }
+    {
+        uint32_t t[WORDS];
+#pragma unroll
+        for (int q = 0; q < WORDS; ++q) t[q] = __funnelshift_r(w[q], w[(q + 1) % WORDS], rs);
+#pragma unroll
+        for (int q = 0; q < WORDS; ++q) w[q] = t[q];
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < C; ++j) {
+        uint32_t e;
+        if (ESIZE == 1)
+            e = (w[j >> 2] >> ((j & 3u) * 8u)) & 0xFFu;
+        else
+            e = (w[j >> 1] >> ((j & 1u) * 16u)) & 0xFFFFu;
+        a.add(sm, plane, e * 32u + slot0 + ((lr + j) & (C - 1u)));
+    }
+}
+
+// 16 bytes of a gathered row window: read-only path, no L1 allocation (each
+// window is read once), and a 128-byte L2 fetch so that the row record's
+// other windows, read by the blocks of the same row segment at about the same
+// time, hit L2.
+__device__ __forceinline__ uint4 ld_window16(const uint8_t* p) {
+    uint4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::128B.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p));
+    return v;
+}
+
+// Register-staged form: each lane keeps LANE_REG_STAGES of its rows'
+// windows in flight as 128-bit loads (the ring shifts by register moves).
+template <int MODE, int ESIZE, int WORDS>
+__device__ void lane_accumulate_regs(uint32_t first, uint32_t count, bool ident, const LaneTile& tile, uint32_t* sm,
+                                     const uint32_t* __restrict__ ridx, const GradLoad<MODE>& load,
+                                     const uint8_t* __restrict__ matrix, uint32_t stride) {
+    constexpr uint32_t C = WORDS * 4 / ESIZE;
+    constexpr uint32_t S = LANE_REG_STAGES;
+    constexpr int V = WORDS / 4;  // 128-bit loads per window
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t lr = lane % C, slot0 = (lane / C) * C;
+    const uint32_t rb = lr * ESIZE;
+    const uint32_t rq = rb >> 2, rs = (rb & 3u) * 8u;
+    const uint8_t* base = matrix + tile.byte_off;
+    const uint32_t step = nwarps * 32u;
+    const uint32_t i0 = warp * 32u + lane;
+    uint4 ring[S][V];
+    LaneAdd<MODE> gring[S];
+    auto fetch = [&](uint32_t i, uint4 (&dst)[V], LaneAdd<MODE>& g) {
+        const uint32_t p = first + i;
+        const uint32_t row = ident ? p : ridx[p];
+        const uint8_t* src = base + (size_t)row * stride;
+#pragma unroll
+        for (int v = 0; v < V; ++v) dst[v] = ld_window16(src + 16 * v);
+        long long qg, qh;
+        load.at(p, row, qg, qh);
+        g = LaneAdd<MODE>(qg, qh);
+    };
+#pragma unroll
+    for (uint32_t k = 0; k + 1 < S; ++k) {
+        const uint32_t i = i0 + k * step;
+        if (i < count) fetch(i, ring[k], gring[k]);
+    }
+    for (uint32_t k = 0; warp * 32u + k * step < count; ++k) {
+        {
+            const uint32_t i = i0 + (k + S - 1) * step;
+            if (i < count) fetch(i, ring[S - 1], gring[S - 1]);
+        }
+        const uint32_t i = i0 + k * step;
+        if (i < count) {
+            uint32_t w[WORDS];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                w[4 * v] = ring[0][v].x;
+                w[4 * v + 1] = ring[0][v].y;
+                w[4 * v + 2] = ring[0][v].z;
+                w[4 * v + 3] = ring[0][v].w;
+            }
+            lane_add_window<MODE, ESIZE, WORDS>(w, lr, slot0, rq, rs, gring[0], sm);
+        }
+#pragma unroll
+        for (uint32_t q = 0; q + 1 < S; ++q) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) ring[q][v] = ring[q + 1][v];
+            gring[q] = gring[q + 1];
+        }
+    }
+}
+
 template <int MODE, int ESIZE, int WORDS>
 __device__ void lane_accumulate(uint32_t first, uint32_t count, bool ident, const LaneTile& tile, uint32_t* sm,
                                 uint8_t* stage, const uint32_t* __restrict__ ridx, const GradLoad<MODE>& load,
                                 const uint8_t* __restrict__ matrix, uint32_t stride) {
     constexpr uint32_t C = WORDS * 4 / ESIZE;  // columns in the window
-    constexpr uint32_t plane = LANE_ROWS * 32u;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const uint32_t lr = lane % C, slot0 = (lane / C) * C;
     const uint32_t rb = lr * ESIZE;  // left rotation of the window, bytes
@@ -613,7 +731,8 @@ __device__ void lane_accumulate(uint32_t first, uint32_t count, bool ident, cons
         const uint32_t dst = my_s + s * 32u * LANE_SLOT;
 #pragma unroll
         for (int v = 0; v < WORDS / 4; ++v)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16u * v), "l"(src + 16 * v)
+            asm volatile("cp.async.cg.shared.global.L2::128B [%0], [%1], 16;" ::"r"(dst + 16u * v),
+                         "l"(src + 16 * v)
                          : "memory");
     };
     const uint32_t i0 = warp * 32u + lane;
@@ -666,33 +785,7 @@ __device__ void lane_accumulate(uint32_t first, uint32_t count, bool ident, cons
                 w[4 * v + 2] = t.z;
                 w[4 * v + 3] = t.w;
             }
-            // rotate left by rb bytes: whole words by rq, then bytes by rs bits
-#pragma unroll
-            for (int st = 1; st < WORDS; st <<= 1) {
-                const bool take = (rq & (uint32_t)st) != 0u;
-                uint32_t t[WORDS];
-#pragma unroll
-                for (int q = 0; q < WORDS; ++q) t[q] = take ? w[(q + st) % WORDS] : w[q];
-#pragma unroll
-                for (int q = 0; q < WORDS; ++q) w[q] = t[q];
-            }
-            {
-                uint32_t t[WORDS];
-#pragma unroll
-                for (int q = 0; q < WORDS; ++q) t[q] = __funnelshift_r(w[q], w[(q + 1) % WORDS], rs);
-#pragma unroll
-                for (int q = 0; q < WORDS; ++q) w[q] = t[q];
-            }
-            const LaneAdd<MODE> a = ring[0];
-#pragma unroll
-            for (uint32_t j = 0; j < C; ++j) {
-                uint32_t e;
-                if (ESIZE == 1)
-                    e = (w[j >> 2] >> ((j & 3u) * 8u)) & 0xFFu;
-                else
-                    e = (w[j >> 1] >> ((j & 1u) * 16u)) & 0xFFFFu;
-                a.add(sm, plane, e * 32u + slot0 + ((lr + j) & (C - 1u)));
-            }
+            lane_add_window<MODE, ESIZE, WORDS>(w, lr, slot0, rq, rs, ring[0], sm);
         }
 #pragma unroll
         for (uint32_t q = 0; q + 1 < LANE_STAGES; ++q) ring[q] = ring[q + 1];
@@ -702,22 +795,33 @@ __device__ void lane_accumulate(uint32_t first, uint32_t count, bool ident, cons
     asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
-template <int MODE>
+template <int MODE, int ESIZE, int WORDS, bool REGS>
+__device__ __forceinline__ void lane_accumulate_v(uint32_t first, uint32_t count, bool ident, const LaneTile& t,
+                                                  uint32_t* sm, uint8_t* stage, const uint32_t* __restrict__ ridx,
+                                                  const GradLoad<MODE>& load, const uint8_t* __restrict__ m,
+                                                  uint32_t stride) {
+    if constexpr (REGS)
+        lane_accumulate_regs<MODE, ESIZE, WORDS>(first, count, ident, t, sm, ridx, load, m, stride);
+    else
+        lane_accumulate<MODE, ESIZE, WORDS>(first, count, ident, t, sm, stage, ridx, load, m, stride);
+}
+
+template <int MODE, bool REGS>
 __device__ __forceinline__ void lane_accumulate_any(uint32_t first, uint32_t count, bool ident, const LaneTile& t,
                                                     uint32_t* sm, uint8_t* stage, const uint32_t* __restrict__ ridx,
                                                     const GradLoad<MODE>& load, const uint8_t* __restrict__ bins8,
                                                     uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16) {
     if (t.esize == 1) {
         if (t.words == 8)
-            lane_accumulate<MODE, 1, 8>(first, count, ident, t, sm, stage, ridx, load, bins8, s8);
+            lane_accumulate_v<MODE, 1, 8, REGS>(first, count, ident, t, sm, stage, ridx, load, bins8, s8);
         else
-            lane_accumulate<MODE, 1, 4>(first, count, ident, t, sm, stage, ridx, load, bins8, s8);
+            lane_accumulate_v<MODE, 1, 4, REGS>(first, count, ident, t, sm, stage, ridx, load, bins8, s8);
     } else {
         const uint8_t* m = reinterpret_cast<const uint8_t*>(bins16);
         if (t.words == 8)
-            lane_accumulate<MODE, 2, 8>(first, count, ident, t, sm, stage, ridx, load, m, s16 * 2u);
+            lane_accumulate_v<MODE, 2, 8, REGS>(first, count, ident, t, sm, stage, ridx, load, m, s16 * 2u);
         else
-            lane_accumulate<MODE, 2, 4>(first, count, ident, t, sm, stage, ridx, load, m, s16 * 2u);
+            lane_accumulate_v<MODE, 2, 4, REGS>(first, count, ident, t, sm, stage, ridx, load, m, s16 * 2u);
     }
 }
 
@@ -751,7 +855,7 @@ struct PartEntry {
     __device__ static T make(long long g, long long h) { return make_int2((int)g, (int)h); }
 };
 
-template <int MODE>
+template <int MODE, bool REGS>
 __device__ void part_item(uint32_t first, uint32_t count, const LaneTile& tile, uint32_t* sm, uint8_t* stage,
                           const uint32_t* __restrict__ ridx, const GradLoad<MODE>& load,
                           const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16,
@@ -763,7 +867,7 @@ __device__ void part_item(uint32_t first, uint32_t count, const LaneTile& tile, 
         for (uint32_t i = threadIdx.x; i < B * 8u; i += blockDim.x)
             reinterpret_cast<uint4*>(sm + w * plane)[i] = make_uint4(0, 0, 0, 0);
     __syncthreads();
-    lane_accumulate_any<MODE>(first, count, false, tile, sm, stage, ridx, load, bins8, s8, bins16, s16);
+    lane_accumulate_any<MODE, REGS>(first, count, false, tile, sm, stage, ridx, load, bins8, s8, bins16, s16);
     __syncthreads();
     // thread -> (bin b, 4 consecutive elements c4..c4+3), copies summed
     const uint32_t C = tile.words * 4u / tile.esize, K = 32u / C, G4 = C / 4u;
@@ -779,8 +883,8 @@ __device__ void part_item(uint32_t first, uint32_t count, const LaneTile& tile, 
     __syncthreads();  // shared histogram free for the next item
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(lane_threads(MODE))
+template <int MODE, int V>
+__global__ void __launch_bounds__(lane_threads(MODE, V), lane_min_blocks(MODE, V))
 k_b_hist_part(BDev d, const LaneTile* __restrict__ tiles, uint32_t n_tiles, const uint32_t* __restrict__ ridx,
               GradRef gr, const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16,
               uint32_t s16, void* __restrict__ part) {
@@ -799,24 +903,67 @@ k_b_hist_part(BDev d, const LaneTile* __restrict__ tiles, uint32_t n_tiles, cons
         const uint32_t count = min(CH, e.small_begin + e.small_count - start);
         load_lane_tile(tile, tiles[t]);
         __syncthreads();
-        part_item<MODE>(start, count, tile, sm, stage, ridx, load, bins8, s8, bins16, s16,
-                        reinterpret_cast<E*>(part) + (size_t)it * LANE_PART_STRIDE);
+        part_item<MODE, lane_regs(V)>(start, count, tile, sm, stage, ridx, load, bins8, s8, bins16, s16,
+                                      reinterpret_cast<E*>(part) + (size_t)it * LANE_PART_STRIDE);
     }
+}
+
+template <int MODE, int V>
+static const void* lane_kernel() {
+    return reinterpret_cast<const void*>(k_b_hist_part<MODE, V>);
+}
+
+static const void* lane_kernel_of(int mode, int v) {
+    if (v < 0 || v >= LANE_VARIANTS) v = 0;
+    switch (mode * LANE_VARIANTS + v) {
+        case GRAD_F32 * LANE_VARIANTS + 0: return lane_kernel<GRAD_F32, 0>();
+        case GRAD_F32 * LANE_VARIANTS + 1: return lane_kernel<GRAD_F32, 1>();
+        case GRAD_F32 * LANE_VARIANTS + 2: return lane_kernel<GRAD_F32, 2>();
+        case GRAD_Q16 * LANE_VARIANTS + 0: return lane_kernel<GRAD_Q16, 0>();
+        case GRAD_Q16 * LANE_VARIANTS + 1: return lane_kernel<GRAD_Q16, 1>();
+        case GRAD_Q16 * LANE_VARIANTS + 2: return lane_kernel<GRAD_Q16, 2>();
+        case GRAD_Q8 * LANE_VARIANTS + 0: return lane_kernel<GRAD_Q8, 0>();
+        case GRAD_Q8 * LANE_VARIANTS + 1: return lane_kernel<GRAD_Q8, 1>();
+        default: return lane_kernel<GRAD_Q8, 2>();
+    }
+}
+
+// Resident blocks per SM of a variant (occupancy of the built kernel:
+// shared memory, registers and threads), per device and host thread.
+uint32_t lane_blocks_per_sm(int mode, int v) {
+    if (v < 0 || v >= LANE_VARIANTS) v = 0;
+    thread_local int dev_cached = -1;
+    thread_local uint32_t cache[3][LANE_VARIANTS];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) cudaGetLastError();
+    if (dev != dev_cached) {
+        init_kernel_attributes();
+        for (int m = 0; m < 3; ++m)
+            for (int k = 0; k < LANE_VARIANTS; ++k) {
+                int b = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lane_kernel_of(m, k), (int)lane_threads(m, k),
+                                                                  lane_smem_bytes(m, k)) != cudaSuccess) {
+                    cudaGetLastError();
+                    b = 1;
+                }
+                cache[m][k] = b > 0 ? (uint32_t)b : 1u;
+            }
+        dev_cached = dev;
+    }
+    return cache[mode >= 0 && mode < 3 ? mode : 0][v];
 }
 
 void launch_b_hist_part(const BDev& d, const LaneTile* tiles, uint32_t n_tiles, const uint32_t* ridx,
                         const GradRef& gr, const uint8_t* bins8, uint32_t s8, const uint16_t* bins16, uint32_t s16,
-                        void* part, cudaStream_t st) {
+                        void* part, int variant, cudaStream_t st) {
     if (n_tiles == 0) return;
     init_kernel_attributes();
-    const unsigned g = sm_count() * lane_blocks_per_sm(gr.mode), th = lane_threads(gr.mode);
-    const size_t smem = lane_smem_bytes(gr.mode);
-    if (gr.mode == GRAD_Q16)
-        k_b_hist_part<GRAD_Q16><<<g, th, smem, st>>>(d, tiles, n_tiles, ridx, gr, bins8, s8, bins16, s16, part);
-    else if (gr.mode == GRAD_Q8)
-        k_b_hist_part<GRAD_Q8><<<g, th, smem, st>>>(d, tiles, n_tiles, ridx, gr, bins8, s8, bins16, s16, part);
-    else
-        k_b_hist_part<GRAD_F32><<<g, th, smem, st>>>(d, tiles, n_tiles, ridx, gr, bins8, s8, bins16, s16, part);
+    const int v = variant >= 0 && variant < LANE_VARIANTS ? variant : 0;
+    const unsigned g = sm_count() * lane_blocks_per_sm(gr.mode, v), th = lane_threads(gr.mode, v);
+    const size_t smem = lane_smem_bytes(gr.mode, v);
+    void* args[] = {(void*)&d,    (void*)&tiles, (void*)&n_tiles, (void*)&ridx,   (void*)&gr,
+                    (void*)&bins8, (void*)&s8,   (void*)&bins16,  (void*)&s16,    (void*)&part};
+    cudaLaunchKernel(lane_kernel_of(gr.mode, v), dim3(g), dim3(th), args, smem, st);  // errors: next check
 }
 
 // The subtraction trick (pool.rs:414-432) for one global bin of node e:
@@ -3186,10 +3333,10 @@ void init_kernel_attributes() {
     cudaFuncSetAttribute(k_b_hist<GRAD_Q8, HBin>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
     cudaFuncSetAttribute(k_b_hist<GRAD_Q8, HBin32>, cudaFuncAttributeMaxDynamicSharedMemorySize, hist_smem);
     cudaFuncSetAttribute(k_bin_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    const int lane_smem = (int)lane_smem_bytes(GRAD_F32);
-    cudaFuncSetAttribute(k_b_hist_part<GRAD_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, lane_smem);
-    cudaFuncSetAttribute(k_b_hist_part<GRAD_Q16>, cudaFuncAttributeMaxDynamicSharedMemorySize, lane_smem);
-    cudaFuncSetAttribute(k_b_hist_part<GRAD_Q8>, cudaFuncAttributeMaxDynamicSharedMemorySize, lane_smem);
+    for (int m = 0; m < 3; ++m)
+        for (int v = 0; v < LANE_VARIANTS; ++v)
+            cudaFuncSetAttribute(lane_kernel_of(m, v), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)lane_smem_bytes(m, v));
     done.fetch_or(bit);
 }
 

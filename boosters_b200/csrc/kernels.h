@@ -141,7 +141,9 @@ uint32_t lane_tile_max_bins(int mode);
 // Rows of a row segment at most: what one block may sum exactly in 32-bit
 // shared counters (4096 for the hi/lo fixed-point split, 16384 quantised).
 uint32_t lane_segment_max(int mode);
-uint32_t lane_blocks_per_sm(int mode);
+// Resident blocks per SM of lane-kernel variant v (0 .. lane_variants() - 1).
+uint32_t lane_blocks_per_sm(int mode, int variant);
+int lane_variants();
 // Partial histograms: one record of lane_part_stride() entries per (segment,
 // lane tile) item, entries of lane_part_entry_bytes(mode) bytes, column-major
 // (entry = element * n_bins + bin).
@@ -350,7 +352,7 @@ void launch_b_hist(const BDev& d, const HistTile* tiles, uint32_t n_tiles, uint3
 // hist_off; seg_exp).
 void launch_b_hist_part(const BDev& d, const LaneTile* tiles, uint32_t n_tiles, const uint32_t* ridx,
                         const GradRef& gr, const uint8_t* bins8, uint32_t s8, const uint16_t* bins16, uint32_t s16,
-                        void* part, cudaStream_t st);
+                        void* part, int variant, cudaStream_t st);
 // Sums each node's partials and applies the subtraction trick into slots
 // left_pnode / right_pnode (root: one node, the sum goes to right_pnode).
 // has_rest: bins of general tiles (bin_map[global bin] == 0xFFFFFFFF) were

@@ -131,6 +131,15 @@ typedef struct bst_config {
     int32_t phase_timings; /* 1: CUDA-event time of every training phase    */
                            /* (bst_model_train_timings); default 0: the     */
                            /* events cost ~0.3 ms per tree inside graphs    */
+    /* Launch-shape autotuning of the batched depth-wise pipeline (histogram
+     * items per block, histogram kernel variant, level-kernel grid): 1
+     * (default) times candidate shapes on the run's first trees, which are
+     * the same trees whatever the shape, and keeps the fastest; 0 uses the
+     * built-in shape. autotune_cache (NULL: none) names a text file of
+     * chosen shapes keyed by device, precision, bin layout and row count: a
+     * cached choice skips the exploration, a new one is added. */
+    int32_t autotune;
+    const char* autotune_cache;
 } bst_config;
 
 /* Fill *cfg with the reference defaults (GBDTConfig::default(),
@@ -263,6 +272,11 @@ bst_status bst_model_train_timings(const bst_model* m, double* out8);
  * launches, histogram row visits, histogram algorithmic bytes (rows x
  * (bin bytes per row + 12)), split-scan launches, partitioned rows]. */
 bst_status bst_model_train_counters(const bst_model* m, uint64_t* out, uint32_t n);
+/* The launch shape the batched pipeline trained with and how it was chosen
+ * ("items=2,hist=0,grid=8 (cached)", "(built-in)", or "(explored: ...)" with
+ * each candidate's median ms per tree; empty for other growth forms):
+ * NUL-terminated into out[cap] (truncated), *len = its full length. */
+bst_status bst_model_tune_info(const bst_model* m, char* out, uint64_t cap, uint64_t* len);
 
 /* ------------------------------------------------------------------------ */
 /* Component entry points (the reference's public building blocks)         */
