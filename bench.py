@@ -612,16 +612,32 @@ def run_configs(bst, torch):
 
 def run_profile(args):
     """A small fixed workload for profilers (no JSON line): `train` grows
-    --rounds trees of the 1M x 100 logistic workload in --form; `predict`
-    trains --trees trees (batched_q8) and predicts --rows rows three times."""
+    --rounds rounds of --workload (the 1M x 100 logistic depth-8 workload,
+    the 10M x 200 leaf-wise one or the 2M x 50 softmax one) in --form, after
+    a launch-shape tuning pass; `predict` trains --trees trees (batched_q8)
+    of the 1M x 100 workload and predicts --rows rows three times."""
     import ctypes
     import torch
     import boosters_b200 as bst
     from boosters_b200 import _native as n
-    x, y = bst.synth.binary(N_ROWS, N_FEAT, N_NAN, seed=SEED)
-    if args.profile == "train":
-        cfg = bst.GBDTConfig(**dict(cfg_kwargs(), **dict(FORMS)[args.form]))
+    if args.profile == "train" and args.workload == "leafwise10M":
+        # 10,000,000 x 200 logistic, leaf-wise 255 leaves
+        x, y = bst.synth.binary(10_000_000, 200, 20, seed=3)
         ds = bst.Dataset.from_feature_major(x, y)
+        cfg = bst.GBDTConfig(objective=bst.Objective.logistic(), n_estimators=100, learning_rate=0.1,
+                             growth_strategy=bst.GrowthStrategy.Leafwise, n_leaves=255, metric=bst.Metric.none(),
+                             **dict(FORMS)[args.form])
+    elif args.profile == "train" and args.workload == "softmax2M":
+        # 2,000,000 x 50 (10 categorical) softmax, 10 classes, depth 6
+        x, y = bst.synth.multiclass(2_000_000, 40, 10, 10, seed=4)
+        ds = bst.Dataset.from_feature_major(x, y, categorical_features=list(range(40, 50)))
+        cfg = bst.GBDTConfig(objective=bst.Objective.softmax(10), n_estimators=200, max_depth=6, learning_rate=0.1,
+                             max_onehot_cats=4, metric=bst.Metric.none(), **dict(FORMS)[args.form])
+    else:
+        x, y = bst.synth.binary(N_ROWS, N_FEAT, N_NAN, seed=SEED)
+        ds = bst.Dataset.from_feature_major(x, y)
+        cfg = bst.GBDTConfig(**dict(cfg_kwargs(), **dict(FORMS)[args.form]))
+    if args.profile == "train":
         # the launch shape: tuned first (16 trees, before the profiled ones),
         # or forced with --shape through the cache file
         print(f"tuning pass: {tune_form(bst, ds, cfg)}")
@@ -669,6 +685,9 @@ def main():
     ap.add_argument("--form", default="batched_q8", choices=[k for k, _ in FORMS])
     ap.add_argument("--rounds", type=int, default=4)
     ap.add_argument("--shape", default="", help="profile train: force this launch shape (items=..,hist=..,grid=..)")
+    ap.add_argument("--workload", default="1M", choices=["1M", "leafwise10M", "softmax2M"],
+                    help="profile train: the 1M x 100 depth-8 workload, the 10M x 200 leaf-wise one or the "
+                         "2M x 50 softmax one")
     ap.add_argument("--trees", type=int, default=1000)
     ap.add_argument("--rows", type=int, default=300_000)
     args = ap.parse_args()
