@@ -335,14 +335,14 @@ def run_serving(bst, torch, local, rank):
     # the link's own rate: one 256 MiB pinned host-to-device copy, best of 5
     big_h = torch.empty(64 << 20, dtype=torch.float32).pin_memory()
     big_d = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
-    best = 0.0
+    link_gbs = 0.0
     for _ in range(5):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         big_d.copy_(big_h, non_blocking=True)
         e1.record()
         e1.synchronize()
-        best = max(best, big_h.numel() * 4 / (e0.elapsed_time(e1) / 1e3) / 1e9)
+        link_gbs = max(link_gbs, big_h.numel() * 4 / (e0.elapsed_time(e1) / 1e3) / 1e9)
     del big_h, big_d
     best = max([head["rows_per_s"]] + [v["rows_per_s"] for v in sweep.values() if v["p99_ms"] <= 2.0] + [0])
     return {"forest": "1000 trees, depth 8, 100 features (binary-logistic workload)",
@@ -350,7 +350,7 @@ def run_serving(bst, torch, local, rank):
             "requests": 20_000, "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"],
             "rows_per_s_at_10k_req_s": head["rows_per_s"], "phases_at_10k_req_s": head["phases"],
             "h2d_gb_per_s_at_10k_req_s": round(h2d_gbs, 2),
-            "h2d_peak_gb_per_s": round(best, 2),
+            "h2d_peak_gb_per_s": round(link_gbs, 2),
             "h2d_needed_gb_per_s_at_1e8_rows_s": round(1e8 * N_FEAT * 4 / 1e9, 1),
             "mean_batch_rows": round((st1["rows"] - st0["rows"]) / max(1, batches)),
             "sweep_req_per_s": sweep, "max_rows_per_s_with_p99_le_2ms": best,
@@ -640,8 +640,11 @@ def run_profile(args):
     if args.profile == "train":
         # the launch shape: tuned first (16 trees, before the profiled ones),
         # or forced with --shape through the cache file
-        print(f"tuning pass: {tune_form(bst, ds, cfg)}")
-        if args.shape and os.path.exists(TUNE_CACHE):
+        if args.shape == "builtin":  # no tuning pass: the built-in shape
+            cfg.autotune = False
+        else:
+            print(f"tuning pass: {tune_form(bst, ds, cfg)}")
+        if args.shape and args.shape != "builtin" and os.path.exists(TUNE_CACHE):
             with open(TUNE_CACHE) as f:
                 key = f.read().split("\t")[0]
             with open(TUNE_CACHE, "w") as f:
@@ -684,7 +687,8 @@ def main():
                     help="skip the other survey workloads (5k x 100, 10M x 200 leaf-wise, 2M x 50 softmax)")
     ap.add_argument("--form", default="batched_q8", choices=[k for k, _ in FORMS])
     ap.add_argument("--rounds", type=int, default=4)
-    ap.add_argument("--shape", default="", help="profile train: force this launch shape (items=..,hist=..,grid=..)")
+    ap.add_argument("--shape", default="", help="profile train: force this launch shape (items=..,hist=..,grid=..; "
+                    "builtin: the built-in shape, no tuning pass)")
     ap.add_argument("--workload", default="1M", choices=["1M", "leafwise10M", "softmax2M"],
                     help="profile train: the 1M x 100 depth-8 workload, the 10M x 200 leaf-wise one or the "
                          "2M x 50 softmax one")
