@@ -135,6 +135,7 @@ void build_lane_tiles(const BinPlan& p, uint32_t max_bins, std::vector<LaneTile>
             t.esize = esize;
             t.words = width / 4;
             t.byte_off = off;
+            t.rec_off = view + off;
             bool any = false, big = false;
             for (uint32_t e = 0; e < width / esize; ++e) {
                 const int c = col_at[off / esize + e];
@@ -960,6 +961,7 @@ class Trainer {
         d_leaf_map_.alloc(max_lc);
         bd_.leaf_map = d_leaf_map_.p;
         bd_.max_leaf_chunks = (uint32_t)max_lc;
+        if (n_lane_tiles_ && p_.rec) make_record_maps(maps_, b_.rec.p, n_, p_.rec);
         // launch shapes: the built-in one, or the tuner's candidates (the
         // buffers below are sized for the candidate with the most segments)
         setup_tuning();
@@ -1001,6 +1003,7 @@ class Trainer {
     }
 
     // ---- launch-shape autotuning (autotune.h) ----------------------------------
+    RecordMaps maps_;                   // tensor maps of the row records (lane-kernel variant 3)
     TuneShape shape_;                   // the shape the current graphs use
     std::vector<TuneShape> tune_cands_; // exploration candidates (empty: none)
     TuneExplorer tuner_;
@@ -1048,7 +1051,8 @@ class Trainer {
                     "|depth=" + std::to_string(cfg_.max_depth) + "|G=" + std::to_string(G_);
         const std::string path = cfg_.autotune_cache ? cfg_.autotune_cache : "";
         TuneShape cached;
-        if (tune_cache_lookup(path, tune_key_, cached) && cached.hist < (uint32_t)lane_variants()) {
+        if (tune_cache_lookup(path, tune_key_, cached) && cached.hist < (uint32_t)lane_variants() &&
+            (cached.hist != 3 || maps_.ok)) {
             shape_ = cached;
             m_.tune_info = shape_.str() + " (cached)";
             tune_stored_ = true;
@@ -1059,16 +1063,18 @@ class Trainer {
             return;
         }
         // the built-in shape first, then items per block x histogram kernel
-        // variant, then a half-size level-kernel grid
+        // variant (the TMA form when the row records have tensor maps), then
+        // a half-size level-kernel grid
         tune_cands_.push_back(shape_);
         for (uint32_t hist = 0; hist < (uint32_t)lane_variants(); ++hist)
-            for (uint32_t items : {1u, 2u}) {
-                TuneShape c;
-                c.items = items;
-                c.hist = hist;
-                c.grid = 8;
-                if (!(c == shape_)) tune_cands_.push_back(c);
-            }
+            if (hist != 3 || maps_.ok)
+                for (uint32_t items : {1u, 2u}) {
+                    TuneShape c;
+                    c.items = items;
+                    c.hist = hist;
+                    c.grid = 8;
+                    if (!(c == shape_)) tune_cands_.push_back(c);
+                }
         TuneShape half = shape_;
         half.grid = 4;
         tune_cands_.push_back(half);
@@ -1161,7 +1167,7 @@ class Trainer {
         tm.begin(PH_HIST);
         if (n_lane_tiles_)
             launch_b_hist_part(bd_, lane_tiles_.p, n_lane_tiles_, ridx, gr, b_.bins8, p_.s8, b_.bins16, p_.s16,
-                               d_part_.p, (int)shape_.hist, st_);
+                               d_part_.p, (int)shape_.hist, &maps_, st_);
         if (n_tiles_)
             launch_b_hist(bd_, tiles_.p, n_tiles_, tile_smem_, ridx, gr, b_.bins8, p_.s8, b_.bins16, p_.s16,
                           hist_.p, slot_bins_, g_hist, st_, hist32_);
@@ -1339,6 +1345,8 @@ class Trainer {
         }
         const BState* h_bstate_ = sl.state;
         const BTreeNode* h_btree_ = sl.tree;
+        if (h_bstate_->err)
+            throw Error{BST_ERR_CUDA, "a histogram kernel's bounded wait for its row copies gave up; the tree is invalid"};
         const uint64_t rows = h_bstate_->hist_rows;
         m_.counters.launches += graph_launches_[gi];
         m_.counters.hist_launches += graph_hist_launches_[gi];

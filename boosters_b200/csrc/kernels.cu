@@ -14,6 +14,8 @@
 
 #include "kernels.h"
 
+#include <cuda.h>  // CUtensorMap and the tensor-map encoder's types (the encoder itself is fetched at run time)
+
 namespace bst {
 
 uint32_t sm_count() {
@@ -503,21 +505,29 @@ constexpr uint32_t LANE_STAGES = 3;  // cp.async ring depth per warp
 constexpr uint32_t LANE_SLOT = 48;   // bytes per lane per stage (32 + 16 pad: conflict-free 16-byte reads)
 constexpr uint32_t LANE_REG_STAGES = 2;  // register ring depth per lane
 
+constexpr uint32_t LANE_TMA_STAGES = 4;   // TMA ring depth per warp
+constexpr uint32_t LANE_TMA_STAGE = 1024;  // bytes per warp and stage: 32 rows x 32 bytes
+
 // Variants of the lane-tile kernel (the launch-shape tuner's `hist` knob):
 //   0: each warp stages its rows' windows through a LANE_STAGES-deep cp.async
 //      ring in shared memory; 256 threads (512 for the fixed-point form)
 //   1: a LANE_REG_STAGES-deep ring of 128-bit register loads instead (no
 //      staging memory: more resident blocks per SM); 256 / 512 threads
 //   2: the register ring with 512-thread blocks
+//   3: the windows gathered by the tensor memory accelerator (tile::gather4,
+//      four rows per copy, issued by eight lanes of the warp) into a
+//      LANE_TMA_STAGES-deep ring completed by mbarriers: the copies bypass
+//      the load/store pipe that the shared-memory atomics need
 // Every variant sums the same values into the same partials.
-constexpr int LANE_VARIANTS = 3;
+constexpr int LANE_VARIANTS = 4;
 __host__ __device__ constexpr uint32_t lane_threads(int mode, int v) {
     return v == 2 ? 512u : (mode == GRAD_F32 ? 512u : 256u);
 }
-__host__ __device__ constexpr bool lane_regs(int v) { return v != 0; }
+__host__ __device__ constexpr bool lane_regs(int v) { return v == 1 || v == 2; }
 __host__ __device__ constexpr uint32_t lane_smem_bytes(int mode, int v) {
     return LANE_ROWS * 32u * acc_words(mode) * 4u +
-           (lane_regs(v) ? 0u : (lane_threads(mode, v) / 32u) * LANE_STAGES * 32u * LANE_SLOT);
+           (v == 3 ? (lane_threads(mode, v) / 32u) * LANE_TMA_STAGES * (LANE_TMA_STAGE + 8u)
+                   : (lane_regs(v) ? 0u : (lane_threads(mode, v) / 32u) * LANE_STAGES * 32u * LANE_SLOT));
 }
 // minimum resident blocks per SM asked of the compiler: a register budget
 // (65536 / (threads x blocks) per thread); variant 0 keeps its 64 registers
@@ -795,6 +805,150 @@ __device__ void lane_accumulate(uint32_t first, uint32_t count, bool ident, cons
     asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
+// ---- TMA form (variant 3) ----------------------------------------------------
+// A wait on an mbarrier gives up after this many polls (far beyond any copy's
+// latency): the kernel then records the failure in BState::err, stops
+// issuing, waits (bounded) for the copies it issued and returns.
+constexpr uint32_t TMA_WAIT_POLLS = 1u << 24;
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t it = 0; it < TMA_WAIT_POLLS; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Rows [first, first + count) of a row segment: per iteration a warp's 32
+// rows are gathered by lanes 0-7 (four rows each) into stage s, whose
+// mbarrier expects the stage's bytes; each lane then reads its row's window
+// from shared memory. Stage rows are packed 4 x 32 bytes per gather, so a
+// lane of an odd group of four reads its two 16-byte halves in swapped
+// order (conflict-free 128-bit reads).
+template <int MODE, int ESIZE, int WORDS>
+__device__ bool lane_accumulate_tma(uint32_t first, uint32_t count, bool ident, const LaneTile& tile, uint32_t* sm,
+                                    uint8_t* stage, uint64_t* bars, const uint32_t* __restrict__ ridx,
+                                    const GradLoad<MODE>& load, const CUtensorMap* tmap, uint32_t n_rows,
+                                    uint32_t* err, uint32_t& parity_bits) {
+    constexpr uint32_t C = WORDS * 4 / ESIZE;
+    constexpr uint32_t S = LANE_TMA_STAGES;
+    constexpr uint32_t BOX = WORDS * 4;  // bytes per gathered row: 32 or 16
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t lr = lane % C, slot0 = (lane / C) * C;
+    const uint32_t rb = lr * ESIZE;
+    const uint32_t rq = rb >> 2, rs = (rb & 3u) * 8u;
+    const uint32_t step = nwarps * 32u;
+    const uint32_t i0 = warp * 32u + lane;
+    uint8_t* wstage = stage + (size_t)warp * S * LANE_TMA_STAGE;
+    const uint32_t wstage_s = (uint32_t)__cvta_generic_to_shared(wstage);
+    const uint32_t bar0 = (uint32_t)__cvta_generic_to_shared(bars + (size_t)warp * S);
+    const int x = (int)tile.rec_off;
+    const uint32_t grp = lane >> 2, in_grp = lane & 3u;
+    // this lane's row in a stage: a gather group of 4 rows of BOX bytes at
+    // each 128-byte boundary (the copies' destinations stay 128-byte aligned)
+    const uint32_t my_off = grp * 128u + in_grp * BOX;
+    const bool swap = (grp & 1u) != 0u && WORDS == 8;
+    bool failed = false;
+    auto row_at = [&](uint32_t i) -> uint32_t {
+        const uint32_t p = first + i;
+        return i < count ? (ident ? p : ridx[p]) : n_rows;  // n_rows: out of range, zero-filled
+    };
+    // issue iteration k (rows of all lanes) into stage s
+    auto issue = [&](uint32_t row, uint32_t s) {
+        const uint32_t r0 = __shfl_sync(FULL, row, (4u * (lane & 7u)) + 0u);
+        const uint32_t r1 = __shfl_sync(FULL, row, (4u * (lane & 7u)) + 1u);
+        const uint32_t r2 = __shfl_sync(FULL, row, (4u * (lane & 7u)) + 2u);
+        const uint32_t r3 = __shfl_sync(FULL, row, (4u * (lane & 7u)) + 3u);
+        const uint32_t bar = bar0 + s * 8u;
+        // the stage's previous contents were read by the generic proxy
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0)
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(8u * 4u * BOX)
+                         : "memory");
+        __syncwarp();
+        if (lane < 8) {
+            const uint32_t dst = wstage_s + s * LANE_TMA_STAGE + lane * 128u;
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+                " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+                "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(r0), "r"(r1), "r"(r2), "r"(r3), "r"(bar)
+                : "memory");
+        }
+    };
+    LaneAdd<MODE> ring[S];
+    const uint32_t iters = count > warp * 32u ? (count - warp * 32u + step - 1) / step : 0u;
+#pragma unroll
+    for (uint32_t k = 0; k + 1 < S; ++k) {
+        ring[k] = LaneAdd<MODE>(0, 0);
+        if (k < iters) {
+            const uint32_t i = i0 + k * step;
+            const uint32_t row = row_at(i);
+            issue(row, k);
+            if (i < count) {
+                long long qg, qh;
+                load.at(first + i, row, qg, qh);
+                ring[k] = LaneAdd<MODE>(qg, qh);
+            }
+        }
+    }
+    for (uint32_t k = 0; k < iters; ++k) {
+        const uint32_t s_cur = k % S;
+        {
+            const uint32_t kn = k + S - 1;  // issue iteration kn
+            ring[S - 1] = LaneAdd<MODE>(0, 0);
+            if (kn < iters && !failed) {
+                const uint32_t i = i0 + kn * step;
+                const uint32_t row = row_at(i);
+                issue(row, kn % S);
+                if (i < count) {
+                    long long qg, qh;
+                    load.at(first + i, row, qg, qh);
+                    ring[S - 1] = LaneAdd<MODE>(qg, qh);
+                }
+            }
+        }
+        if (!failed) {
+            const uint32_t par = (parity_bits >> s_cur) & 1u;
+            const bool ok = mbar_wait(bar0 + s_cur * 8u, par);
+            if (!__all_sync(FULL, ok)) {  // warp-uniform: the issue path shuffles across the warp
+                failed = true;
+                if (lane == 0) atomicExch(err, 1u);
+            }
+            parity_bits ^= 1u << s_cur;
+        }
+        const uint32_t i = i0 + k * step;
+        if (!failed && i < count) {
+            const uint8_t* src = wstage + s_cur * LANE_TMA_STAGE + my_off;
+            uint32_t w[WORDS];
+            if constexpr (WORDS == 8) {
+                const uint4 a = *reinterpret_cast<const uint4*>(src + (swap ? 16 : 0));
+                const uint4 b = *reinterpret_cast<const uint4*>(src + (swap ? 0 : 16));
+                const uint4 lo = swap ? b : a, hi = swap ? a : b;
+                w[0] = lo.x; w[1] = lo.y; w[2] = lo.z; w[3] = lo.w;
+                w[4] = hi.x; w[5] = hi.y; w[6] = hi.z; w[7] = hi.w;
+            } else {
+                const uint4 a = *reinterpret_cast<const uint4*>(src);
+                w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
+            }
+            lane_add_window<MODE, ESIZE, WORDS>(w, lr, slot0, rq, rs, ring[0], sm);
+        }
+#pragma unroll
+        for (uint32_t q = 0; q + 1 < S; ++q) ring[q] = ring[q + 1];
+    }
+    // after a failed wait, the copies still in flight must land before the
+    // block's shared memory is reused: wait (bounded) on every stage's
+    // pending phase, then report the failure (the caller stops)
+    if (failed)
+        for (uint32_t s = 0; s < S; ++s) mbar_wait(bar0 + s * 8u, (parity_bits >> s) & 1u);
+    return !failed;
+}
+
 template <int MODE, int ESIZE, int WORDS, bool REGS>
 __device__ __forceinline__ void lane_accumulate_v(uint32_t first, uint32_t count, bool ident, const LaneTile& t,
                                                   uint32_t* sm, uint8_t* stage, const uint32_t* __restrict__ ridx,
@@ -855,6 +1009,9 @@ struct PartEntry {
     __device__ static T make(long long g, long long h) { return make_int2((int)g, (int)h); }
 };
 
+template <int MODE>
+__device__ void part_flush(const LaneTile& tile, const uint32_t* sm, typename PartEntry<MODE>::T* __restrict__ out);
+
 template <int MODE, bool REGS>
 __device__ void part_item(uint32_t first, uint32_t count, const LaneTile& tile, uint32_t* sm, uint8_t* stage,
                           const uint32_t* __restrict__ ridx, const GradLoad<MODE>& load,
@@ -869,6 +1026,15 @@ __device__ void part_item(uint32_t first, uint32_t count, const LaneTile& tile, 
     __syncthreads();
     lane_accumulate_any<MODE, REGS>(first, count, false, tile, sm, stage, ridx, load, bins8, s8, bins16, s16);
     __syncthreads();
+    part_flush<MODE>(tile, sm, out);
+}
+
+// The tile's partial histogram, copies summed, to out (column-major);
+// returns with the shared histogram free for the next item.
+template <int MODE>
+__device__ void part_flush(const LaneTile& tile, const uint32_t* sm, typename PartEntry<MODE>::T* __restrict__ out) {
+    constexpr uint32_t plane = LANE_ROWS * 32u;
+    const uint32_t B = tile.n_bins;
     // thread -> (bin b, 4 consecutive elements c4..c4+3), copies summed
     const uint32_t C = tile.words * 4u / tile.esize, K = 32u / C, G4 = C / 4u;
     for (uint32_t t = threadIdx.x; t < B * G4; t += blockDim.x) {
@@ -908,6 +1074,70 @@ k_b_hist_part(BDev d, const LaneTile* __restrict__ tiles, uint32_t n_tiles, cons
     }
 }
 
+// Variant 3: the lane-tile partial histograms with the TMA ring. `m32` /
+// `m16`: tensor maps of the row records with 32- and 16-byte boxes.
+template <int MODE>
+__global__ void __launch_bounds__(lane_threads(MODE, 3), lane_min_blocks(MODE, 3))
+k_b_hist_part_tma(BDev d, const LaneTile* __restrict__ tiles, uint32_t n_tiles, const uint32_t* __restrict__ ridx,
+                  GradRef gr, uint32_t n_rows, void* __restrict__ part, const __grid_constant__ CUtensorMap m32,
+                  const __grid_constant__ CUtensorMap m16) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    constexpr uint32_t NW = acc_words(MODE);
+    constexpr uint32_t plane = LANE_ROWS * 32u;
+    uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);
+    const uint32_t nwarps = blockDim.x >> 5;
+    uint8_t* stage = smem_raw + NW * plane * 4u;  // 128-byte aligned (plane bytes are)
+    uint64_t* bars = reinterpret_cast<uint64_t*>(stage + (size_t)nwarps * LANE_TMA_STAGES * LANE_TMA_STAGE);
+    __shared__ LaneTile tile;
+    using E = typename PartEntry<MODE>::T;
+    const GradLoad<MODE> load(gr);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (uint32_t q = 0; q < LANE_TMA_STAGES; ++q) {
+            const uint32_t b = (uint32_t)__cvta_generic_to_shared(bars + warp * LANE_TMA_STAGES + q);
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    __syncthreads();
+    uint32_t parity_bits = 0;
+    const uint32_t CH = d.state->hist_chunk;
+    const uint64_t items = (uint64_t)d.state->hist_chunks * n_tiles;
+    __shared__ int s_fail;
+    for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
+        const uint32_t c = (uint32_t)(it / n_tiles), t = (uint32_t)(it % n_tiles);
+        const BExp e = d.exp[d.seg_exp[c]];
+        const uint32_t start = e.small_begin + (c - e.hist_off) * CH;
+        const uint32_t count = min(CH, e.small_begin + e.small_count - start);
+        load_lane_tile(tile, tiles[t]);
+        if (threadIdx.x == 0) s_fail = 0;
+        __syncthreads();
+        for (uint32_t w = 0; w < NW; ++w)
+            for (uint32_t i = threadIdx.x; i < tile.n_bins * 8u; i += blockDim.x)
+                reinterpret_cast<uint4*>(sm + w * plane)[i] = make_uint4(0, 0, 0, 0);
+        __syncthreads();
+        bool ok;
+        if (tile.words == 8) {
+            if (tile.esize == 1)
+                ok = lane_accumulate_tma<MODE, 1, 8>(start, count, false, tile, sm, stage, bars, ridx, load, &m32,
+                                                     n_rows, &d.state->err, parity_bits);
+            else
+                ok = lane_accumulate_tma<MODE, 2, 8>(start, count, false, tile, sm, stage, bars, ridx, load, &m32,
+                                                     n_rows, &d.state->err, parity_bits);
+        } else {
+            if (tile.esize == 1)
+                ok = lane_accumulate_tma<MODE, 1, 4>(start, count, false, tile, sm, stage, bars, ridx, load, &m16,
+                                                     n_rows, &d.state->err, parity_bits);
+            else
+                ok = lane_accumulate_tma<MODE, 2, 4>(start, count, false, tile, sm, stage, bars, ridx, load, &m16,
+                                                     n_rows, &d.state->err, parity_bits);
+        }
+        if (!ok) s_fail = 1;
+        __syncthreads();
+        if (s_fail) return;  // the tree is abandoned (BState::err is set)
+        part_flush<MODE>(tile, sm, reinterpret_cast<E*>(part) + (size_t)it * LANE_PART_STRIDE);
+    }
+}
+
 template <int MODE, int V>
 static const void* lane_kernel() {
     return reinterpret_cast<const void*>(k_b_hist_part<MODE, V>);
@@ -915,6 +1145,11 @@ static const void* lane_kernel() {
 
 static const void* lane_kernel_of(int mode, int v) {
     if (v < 0 || v >= LANE_VARIANTS) v = 0;
+    if (v == 3) {
+        if (mode == GRAD_F32) return reinterpret_cast<const void*>(k_b_hist_part_tma<GRAD_F32>);
+        if (mode == GRAD_Q16) return reinterpret_cast<const void*>(k_b_hist_part_tma<GRAD_Q16>);
+        return reinterpret_cast<const void*>(k_b_hist_part_tma<GRAD_Q8>);
+    }
     switch (mode * LANE_VARIANTS + v) {
         case GRAD_F32 * LANE_VARIANTS + 0: return lane_kernel<GRAD_F32, 0>();
         case GRAD_F32 * LANE_VARIANTS + 1: return lane_kernel<GRAD_F32, 1>();
@@ -953,14 +1188,68 @@ uint32_t lane_blocks_per_sm(int mode, int v) {
     return cache[mode >= 0 && mode < 3 ? mode : 0][v];
 }
 
+// cuTensorMapEncodeTiled, fetched from the driver through the runtime (no
+// link against the driver library).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+bool make_record_maps(RecordMaps& out, const uint8_t* rec, uint64_t n_rows, uint32_t rec_bytes) {
+    out.ok = false;
+    const EncodeTiledFn fn = encode_tiled();
+    // the encoder's limits: 16-byte aligned base and row stride, rows and
+    // record bytes within 32 bits
+    if (!fn || !rec || n_rows == 0 || n_rows >= (1ull << 31) || rec_bytes == 0 || rec_bytes % 16 != 0 ||
+        reinterpret_cast<uintptr_t>(rec) % 16 != 0)
+        return false;
+    const cuuint64_t dims[2] = {rec_bytes, n_rows};
+    const cuuint64_t strides[1] = {rec_bytes};
+    const cuuint32_t elem[2] = {1, 1};
+    for (int k = 0; k < 2; ++k) {
+        const cuuint32_t box[2] = {k == 0 ? 32u : 16u, 1u};
+        CUtensorMap* m = reinterpret_cast<CUtensorMap*>(k == 0 ? out.box32 : out.box16);
+        const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<uint8_t*>(rec), dims, strides, box, elem,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return false;
+    }
+    out.n_rows = (uint32_t)n_rows;
+    out.ok = true;
+    return true;
+}
+
 void launch_b_hist_part(const BDev& d, const LaneTile* tiles, uint32_t n_tiles, const uint32_t* ridx,
                         const GradRef& gr, const uint8_t* bins8, uint32_t s8, const uint16_t* bins16, uint32_t s16,
-                        void* part, int variant, cudaStream_t st) {
+                        void* part, int variant, const RecordMaps* maps, cudaStream_t st) {
     if (n_tiles == 0) return;
     init_kernel_attributes();
-    const int v = variant >= 0 && variant < LANE_VARIANTS ? variant : 0;
+    int v = variant >= 0 && variant < LANE_VARIANTS ? variant : 0;
+    if (v == 3 && !(maps && maps->ok)) v = 0;  // no tensor maps: the cp.async form
     const unsigned g = sm_count() * lane_blocks_per_sm(gr.mode, v), th = lane_threads(gr.mode, v);
     const size_t smem = lane_smem_bytes(gr.mode, v);
+    if (v == 3) {
+        const uint32_t n_rows = maps->n_rows;
+        const CUtensorMap& m32 = *reinterpret_cast<const CUtensorMap*>(maps->box32);
+        const CUtensorMap& m16 = *reinterpret_cast<const CUtensorMap*>(maps->box16);
+        void* targs[] = {(void*)&d,  (void*)&tiles, (void*)&n_tiles, (void*)&ridx, (void*)&gr,
+                         (void*)&n_rows, (void*)&part, (void*)&m32, (void*)&m16};
+        cudaLaunchKernel(lane_kernel_of(gr.mode, v), dim3(g), dim3(th), targs, smem, st);  // errors: next check
+        return;
+    }
     void* args[] = {(void*)&d,    (void*)&tiles, (void*)&n_tiles, (void*)&ridx,   (void*)&gr,
                     (void*)&bins8, (void*)&s8,   (void*)&bins16,  (void*)&s16,    (void*)&part};
     cudaLaunchKernel(lane_kernel_of(gr.mode, v), dim3(g), dim3(th), args, smem, st);  // errors: next check
@@ -2099,7 +2388,8 @@ __global__ void k_b_root(BDev d, uint64_t n) {
     s.hist_chunk = HIST_CHUNK_MAX;
     s.hist_rows = n;
     s.done = 0;
-    s.pad2[0] = s.pad2[1] = s.pad2[2] = 0;
+    s.err = 0;
+    s.pad2[0] = s.pad2[1] = 0;
     *d.state = s;
 }
 

@@ -131,7 +131,8 @@ void launch_hist_build(const HistChunk* chunks, uint32_t n_chunks, const HistTil
 struct LaneTile {
     uint32_t esize;     // 1 (u8 matrix) or 2 (u16 matrix)
     uint32_t words;     // window width in 32-bit words: 4 or 8
-    uint32_t byte_off;  // window start inside the row, bytes (multiple of 16)
+    uint32_t byte_off;  // window start inside the row of its view, bytes (multiple of 16)
+    uint32_t rec_off;   // window start inside the row record, bytes (multiple of 16)
     uint32_t n_bins;    // largest bin count of the window's columns
     uint32_t col_hist[32];   // per window element: global histogram bin offset
     uint32_t col_nbins[32];  // per window element: bins (0 = no column)
@@ -291,7 +292,8 @@ struct BState {
     uint32_t hist_chunk;           // rows per histogram work item of the level
     unsigned long long hist_rows;  // rows visited by histogram builds of this tree
     uint32_t done;                 // last-block hand-off counter (zero between launches)
-    uint32_t pad2[3];
+    uint32_t err;                  // nonzero: a bounded wait of a kernel gave up (the tree is invalid)
+    uint32_t pad2[2];
 };
 struct LeafParams {
     double lambda, alpha, min_gain;
@@ -350,9 +352,20 @@ void launch_b_hist(const BDev& d, const HistTile* tiles, uint32_t n_tiles, uint3
 // Partial histograms of every (row segment, lane tile) item of the level
 // (state: n_exp, hist_chunks, hist_chunk; exp[].small_begin/small_count/
 // hist_off; seg_exp).
+// Tensor maps of the row records for the TMA form of the lane kernel
+// (variant 3): 2D [n rows][rec bytes] u8, one-row boxes of 32 and of 16
+// bytes (tile::gather4 loads four rows per copy). Built once per binned
+// dataset; false when the driver cannot encode them (variant 3 unavailable).
+struct RecordMaps {
+    alignas(64) unsigned char box32[128];
+    alignas(64) unsigned char box16[128];
+    uint32_t n_rows = 0;  // the maps' row extent (a row id equal to it reads as zeros)
+    bool ok = false;
+};
+bool make_record_maps(RecordMaps& out, const uint8_t* rec, uint64_t n_rows, uint32_t rec_bytes);
 void launch_b_hist_part(const BDev& d, const LaneTile* tiles, uint32_t n_tiles, const uint32_t* ridx,
                         const GradRef& gr, const uint8_t* bins8, uint32_t s8, const uint16_t* bins16, uint32_t s16,
-                        void* part, int variant, cudaStream_t st);
+                        void* part, int variant, const RecordMaps* maps, cudaStream_t st);
 // Sums each node's partials and applies the subtraction trick into slots
 // left_pnode / right_pnode (root: one node, the sum goes to right_pnode).
 // has_rest: bins of general tiles (bin_map[global bin] == 0xFFFFFFFF) were
