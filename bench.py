@@ -233,9 +233,12 @@ def tune_form(bst, ds, cfg):
         return ""  # the tuned pipeline is the batched depth-wise one
     c = copy.copy(cfg)
     c.autotune, c.autotune_cache = True, TUNE_CACHE
-    c.n_estimators = 16
+    c.n_estimators = 24  # more than the exploration's 2 trees per candidate + 1
     b = bst.Booster(ds, c, n_threads=0)
-    b.update(16)
+    rounds = 0
+    while "(explored" not in b.model().tune_info and rounds < 64:
+        b.update(4)
+        rounds += 4
     return b.model().tune_info
 
 
