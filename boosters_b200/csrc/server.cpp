@@ -5,11 +5,11 @@
 // Requests (sample-major f32 rows, caller-owned input and output buffers in
 // host or device memory: the copies go by unified addressing) are admitted
 // FIFO into a device row ring as soon as it has room: the
-// admission issues the request's host-to-device copy at once on the copy
-// stream, so copies proceed while earlier batches traverse. A dispatcher
+// admission issues the request's host-to-device copy at once on one of two
+// copy streams, so copies proceed while earlier batches traverse. A dispatcher
 // coalesces admitted requests that sit contiguously in the ring into one
 // batch per free slot (SLOTS batches in flight), makes the slot's stream
-// wait for the batch's last copy, runs ONE traversal launch over the ring
+// wait for the batch's copies, runs ONE traversal launch over the ring
 // span and copies each request's outputs straight back to the caller. A
 // completion thread retires batches in order, frees their ring span, admits
 // waiting requests and wakes the waiters. A row's prediction depends on that
@@ -83,7 +83,11 @@ struct Server {
     std::deque<int> inflight;       // slot indices in issue order
     std::vector<cudaEvent_t> events;  // free copy events
     DevArray<float> ring;
-    cudaStream_t cst = nullptr;     // host-to-device copies
+    // host-to-device copies, requests alternating between the streams so
+    // that one copy's set-up overlaps another's transfer
+    static constexpr int COPY_STREAMS = 2;
+    cudaStream_t cst[COPY_STREAMS] = {nullptr, nullptr};
+    uint64_t copies_issued = 0;
     Slot slots[SLOTS];
     uint64_t next_id = 1;
     bool stop = false;
@@ -123,7 +127,7 @@ struct Server {
         coalesce_rows = cap ? max_rows : std::min(max_rows, (uint64_t)sm_count() * WAVE_TILE_ROWS);
         ring_rows = (uint64_t)SLOTS * max_rows;  // the slots' input share of the budget
         ring.alloc((size_t)ring_rows * std::max<uint64_t>(1, F));
-        BST_CK(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking));
+        for (auto& c : cst) BST_CK(cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking));
         const size_t scratch = forest_scratch_max(df, max_rows, F);
         for (auto& s : slots) {
             s.d_out.alloc((size_t)max_rows * G);
@@ -156,7 +160,8 @@ struct Server {
         if (dispatcher.joinable()) dispatcher.join();
         if (completer.joinable()) completer.join();
         cudaSetDevice(device);
-        if (cst) cudaStreamSynchronize(cst);
+        for (auto c : cst)
+            if (c) cudaStreamSynchronize(c);
         for (auto& s : slots) {
             if (s.st) cudaStreamSynchronize(s.st);
             if (s.done) cudaEventDestroy(s.done);
@@ -169,7 +174,8 @@ struct Server {
             if (kv.second.copied) cudaEventDestroy(kv.second.copied);
         }
         for (cudaEvent_t e : events) cudaEventDestroy(e);
-        if (cst) cudaStreamDestroy(cst);
+        for (auto c : cst)
+            if (c) cudaStreamDestroy(c);
     }
 
     // Ring room for n rows after the live spans (contiguous; wraps to row 0).
@@ -212,10 +218,11 @@ struct Server {
             r.copied = take_event();
             r.pos = pos;
             r.admit_ns = now_ns();
-            BST_CK(cudaEventRecord(r.copy_start, cst));
+            cudaStream_t cs = cst[copies_issued++ % COPY_STREAMS];
+            BST_CK(cudaEventRecord(r.copy_start, cs));
             if (F)
-                BST_CK(cudaMemcpyAsync(ring.p + pos * F, r.rows, sizeof(float) * r.n * F, cudaMemcpyDefault, cst));
-            BST_CK(cudaEventRecord(r.copied, cst));
+                BST_CK(cudaMemcpyAsync(ring.p + pos * F, r.rows, sizeof(float) * r.n * F, cudaMemcpyDefault, cs));
+            BST_CK(cudaEventRecord(r.copied, cs));
             live.emplace_back(pos, r.n);
             admitted.push_back(r.id);
             pending.pop_front();
@@ -280,7 +287,8 @@ struct Server {
             error = code;
             error_msg = msg;
         }
-        if (cst) cudaStreamSynchronize(cst);  // no copy still reads a caller's rows
+        for (auto c : cst)  // no copy still reads a caller's rows
+            if (c) cudaStreamSynchronize(c);
         const uint64_t t = now_ns();
         for (auto& kv : reqs)
             if (kv.second.status < 0) {
@@ -341,7 +349,8 @@ struct Server {
             }
             Slot& s = slots[si];
             try {
-                BST_CK(cudaStreamWaitEvent(s.st, batch.back().copied, 0));  // copies are in order on cst
+                for (const Req& r : batch)  // every request's copy (the copy streams run side by side)
+                    BST_CK(cudaStreamWaitEvent(s.st, r.copied, 0));
                 BST_CK(cudaEventRecord(s.k0, s.st));
                 forest_predict_rows(f, ring.p + batch.front().pos * F, rows, F, s.d_out.p, s.st, s.scratch.p,
                                     s.scratch.n);
