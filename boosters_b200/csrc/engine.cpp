@@ -878,6 +878,7 @@ class Trainer {
         spec_leafwise_ = cfg_.batched && leafwise_ && n_cols_ > 0;
         if (use_batched_ || spec_leafwise_) {
             if (use_batched_) setup_batched();
+            if (spec_leafwise_) setup_lw_device();
             for (auto& q : qpos_) q.alloc((size_t)n_ * grad_bytes());
             if (p_.f8) fm8_.alloc((size_t)n_ * p_.f8);
             if (p_.f16) fm16_.alloc((size_t)n_ * p_.f16);
@@ -933,6 +934,7 @@ class Trainer {
 
   public:
     ~Trainer() {
+        free_lw_device();
         for (auto g : graphs_)
             if (g) cudaGraphExecDestroy(g);
         for (auto& sl : slots_) {
@@ -1353,8 +1355,12 @@ class Trainer {
         m_.counters.hist_rows += rows;
         m_.counters.hist_bytes += rows * ((uint64_t)p_.f8 + 2ull * p_.f16 + grad_bytes() + 4ull);
         m_.counters.scan_launches += graph_hist_launches_[gi];
-        // host tree from the device tree (grower.rs:576-650 threshold translation)
-        const uint32_t nt = h_bstate_->n_tnodes;
+        return host_tree_from(std::move(t), h_bstate_->n_tnodes, h_btree_);
+    }
+
+    // Host tree from a device tree (grower.rs:576-650 threshold translation);
+    // t carries the tree's group and row leaves.
+    HostTree host_tree_from(HostTree&& t, uint32_t nt, const BTreeNode* h_btree_) {
         cat_nodes_.clear();
         for (uint32_t i = 0; i < nt; ++i) t.alloc();
         for (uint32_t i = 0; i < nt; ++i) {
@@ -1889,7 +1895,221 @@ class Trainer {
         }
     }
 
+    // ---- batched leaf-wise growth on the device (kernels.h, k_lw_replay) -----
+    // The replay of the heap pops runs on the device between expansion
+    // steps; the host launches LW_STEPS steps at a time as one CUDA graph and
+    // reads back only whether the tree is done.
+    static constexpr uint32_t LW_STEPS = 6;
+    DevArray<LwState> d_lw_state_;
+    DevArray<LwCand> d_lw_heap_;
+    DevArray<LwSpec> d_lw_spec_;
+    DevArray<uint2> d_lw_pn_;
+    DevArray<NodeSplit> d_lw_child_;
+    LwDev lw_{};
+    LwState* h_lw_state_ = nullptr;  // pinned
+    BState* h_lw_bstate_ = nullptr;  // pinned
+    std::vector<cudaGraphExec_t> lw_graphs_;  // [output]
+    std::vector<uint64_t> lw_launches_, lw_hist_launches_;
+    std::vector<std::unique_ptr<Timer>> lw_timers_;  // [output]: event nodes of the step graphs
+
+    void setup_lw_device() {
+        init_kernel_attributes();
+        const uint32_t mp = max_pnodes_;
+        d_lw_state_.alloc(1);
+        d_lw_heap_.alloc(2 * (size_t)cfg_.max_leaves + 4);
+        d_lw_spec_.alloc(mp);
+        d_lw_pn_.alloc(mp);
+        d_lw_child_.alloc(2 * (size_t)mp + 2);
+        lw_.st = d_lw_state_.p;
+        lw_.heap = d_lw_heap_.p;
+        lw_.spec = d_lw_spec_.p;
+        lw_.pn = d_lw_pn_.p;
+        lw_.child = d_lw_child_.p;
+        lw_.heap_cap = (uint32_t)d_lw_heap_.n;
+        lw_.max_pnodes = mp;
+        lw_.max_leaves = cfg_.max_leaves;
+        lw_.min_gain = cfg_.min_gain;
+        // the device tree, its leaves and the columns' partition facts
+        d_btree_.alloc(2 * (size_t)mp);
+        d_bleaves_.alloc((size_t)mp + 1);
+        d_node_key_.alloc(2 * (size_t)mp + 2);
+        BST_CK(cudaMemset(d_node_key_.p, 0, sizeof(unsigned long long) * d_node_key_.n));
+        std::vector<BColumn> bc(n_cols_);
+        for (uint32_t c = 0; c < n_cols_; ++c)
+            bc[c] = BColumn{p_.col_matrix[c], p_.col_pos[c], p_.col_missing[c], p_.col_default[c]};
+        d_bcols_.alloc(n_cols_);
+        BST_CK(cudaMemcpy(d_bcols_.p, bc.data(), sizeof(BColumn) * n_cols_, cudaMemcpyHostToDevice));
+        bd_.tree = d_btree_.p;
+        bd_.leaves = d_bleaves_.p;
+        bd_.bcols = d_bcols_.p;
+        bd_.node_key = d_node_key_.p;
+        bd_.pworks = d_pworks_.p;
+        bd_.cursors = d_cursors_.p;
+        bd_.scan_nodes = d_scan_nodes_.p;
+        bd_.sums = d_sums_.p;
+        bd_.scnt = rowsample_ ? d_scnt_.p : nullptr;
+        bd_.max_front = mp;
+        bd_.max_tnodes = (uint32_t)d_btree_.n;
+        if (!h_lw_state_) BST_CK(cudaMallocHost(&h_lw_state_, sizeof(LwState)));
+        if (!h_lw_bstate_) BST_CK(cudaMallocHost(&h_lw_bstate_, sizeof(BState)));
+        lw_graphs_.assign(G_, nullptr);
+        lw_launches_.assign(G_, 0);
+        lw_hist_launches_.assign(G_, 0);
+        lw_timers_.resize(G_);
+        for (auto& t : lw_timers_) {
+            t = std::make_unique<Timer>();
+            t->st = st_;
+            t->enabled = cfg_.phase_timings != 0;
+            t->in_graph = true;
+            t->reserve(LW_STEPS * 12 + 4);
+        }
+    }
+
+    void free_lw_device() {
+        for (auto g : lw_graphs_)
+            if (g) cudaGraphExecDestroy(g);
+        lw_graphs_.clear();
+        if (h_lw_state_) cudaFreeHost(h_lw_state_);
+        if (h_lw_bstate_) cudaFreeHost(h_lw_bstate_);
+        h_lw_state_ = nullptr;
+        h_lw_bstate_ = nullptr;
+    }
+
+    // LW_STEPS expansion steps of output o's tree: replay, partition (rows
+    // copied back into the one row buffer), children and histogram segments,
+    // histograms with the subtraction trick, the children's split search.
+    void enqueue_lw_steps(uint32_t o, Timer& tm, uint64_t& launches, uint64_t& hist_launches) {
+        LeafParams lp{(double)cfg_.lambda, (double)cfg_.alpha, (double)cfg_.min_gain, cfg_.learning_rate, 0u};
+        GradRef gr = grad_ref(o);
+        gr.qpos = qpos_[0].p;
+        const double* scale = unit_scale(o);
+        launches = 0;
+        hist_launches = 0;
+        for (uint32_t k = 0; k < LW_STEPS; ++k) {
+            tm.begin(PH_OTHER);
+            launch_lw_replay(bd_, lw_, lp, scale, st_);
+            tm.end();
+            tm.begin(PH_PART);
+            launch_lw_partition(bd_, ridx_.p, tmp_.p, b_.bins8, p_.s8, b_.bins16, p_.s16, g_wide_, qpos_[0].p,
+                                qpos_[1].p, qmode_, fm_, st_);
+            tm.end();
+            tm.begin(PH_OTHER);
+            launch_lw_children(bd_, d_pworks_.p, d_cursors_.p, LW_K_FROM_STATE, d_scan_nodes_.p,
+                               rowsample_ ? d_scnt_.p : nullptr, st_);
+            if (n_tiles_) launch_b_zero_right(bd_, hist_.p, slot_bins_, g_wide_, st_, hist32_);
+            tm.end();
+            enqueue_hist(gr, ridx_.p, false, tm, launches, hist_launches, false);
+            tm.begin(PH_SCAN);
+            launch_b_scan(bd_, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p, d_node_tot_.p, 0,
+                          last_wins_ ? 1 : 0, lp, 0u, g_wide_, st_, hist32_, nullptr, colmask(), lw_.child);
+            tm.end();
+            launches += 5 + (n_tiles_ ? 1 : 0);  // + replay, partition, copy-back, children, scan
+        }
+    }
+
+    HostTree grow_lw_device(uint32_t o) {
+        tree_output_ = o;
+        gr_o_ = grad_ref(o);
+        gr_o_.qpos = qpos_[0].p;  // histograms read the positional copy
+        scale_o_ = unit_scale(o);
+        bd_.rmask = rowmask(o);
+        stage_.reset();
+        timer_.begin(PH_OTHER);
+        upload_col_masks(o, 0);
+        launch_iota(ridx_.p, n_, st_);
+        // identity order: the positional copy is the row-order array
+        BST_CK(cudaMemcpyAsync(qpos_[0].p, qmode_ == GRAD_F32 ? (const void*)gr_o_.gh : gr_o_.gq,
+                               (size_t)n_ * grad_bytes(), cudaMemcpyDeviceToDevice, st_));
+        BST_CK(cudaMemsetAsync(d_lw_spec_.p, 0, sizeof(LwSpec) * d_lw_spec_.n, st_));
+        timer_.end();
+        // the root's histogram and split (grower.rs:288-308)
+        if (n_tiles_) BST_CK(cudaMemsetAsync(hist_.p, 0, hbytes() * slot_bins_, st_));
+        BExp e;
+        std::memset(&e, 0, sizeof(e));
+        e.rc = (uint32_t)n_;
+        e.small_count = (uint32_t)n_;
+        host_hist({e}, true);
+        ScanNode* rs = stage_.take<ScanNode>(1);
+        *rs = ScanNode{0, n_sampled_[o], 0u, 0u, 0, 0};  // sampled rows under row sampling
+        upload(rs, 1, d_scan_nodes_);
+        timer_.begin(PH_SCAN);
+        launch_split_scan(d_scan_nodes_.p, 1, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale_o_, gp_, d_cand_.p,
+                          d_node_tot_.p, st_, hist32_, colmask());
+        launch_split_reduce(d_cand_.p, d_node_tot_.p, 1, n_cols_, last_wins_ ? 1 : 0, lw_.child, st_);
+        timer_.end();
+        launch_lw_init(bd_, lw_, (uint32_t)n_, (uint32_t)n_, st_);
+        m_.counters.launches += 5;
+        // expansion steps, LW_STEPS per graph launch, until the replay is done
+        if (!lw_graphs_[o]) {
+            BST_CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue_lw_steps(o, *lw_timers_[o], lw_launches_[o], lw_hist_launches_[o]);
+            } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(st_, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            cudaGraph_t g = nullptr;
+            BST_CK(cudaStreamEndCapture(st_, &g));
+            cudaGraphExec_t ex = nullptr;
+            const cudaError_t ce = cudaGraphInstantiate(&ex, g, 0);
+            cudaGraphDestroy(g);
+            BST_CK(ce);
+            lw_graphs_[o] = ex;
+        }
+        // each step but the last pops at least one leaf
+        const uint32_t max_launches = cfg_.max_leaves / LW_STEPS + 4;
+        Timer& gt = *lw_timers_[o];
+        for (uint32_t it = 0;; ++it) {
+            if (it > max_launches) throw Error{BST_ERR_CUDA, "leaf-wise replay did not finish"};
+            BST_CK(cudaGraphLaunch(lw_graphs_[o], st_));
+            BST_CK(cudaMemcpyAsync(h_lw_state_, d_lw_state_.p, sizeof(LwState), cudaMemcpyDeviceToHost, st_));
+            BST_CK(cudaStreamSynchronize(st_));
+            if (gt.enabled && gt.collect_keep())
+                for (int i = 1; i < 7; ++i) {
+                    timer_.acc[i] += gt.acc[i];
+                    gt.acc[i] = 0.0;
+                }
+            m_.counters.launches += lw_launches_[o];
+            m_.counters.hist_launches += lw_hist_launches_[o];
+            m_.counters.scan_launches += LW_STEPS;
+            if (h_lw_state_->err) throw Error{BST_ERR_OUT_OF_MEMORY, "leaf-wise growth ran out of histogram slots"};
+            if (h_lw_state_->done) break;
+        }
+        // leaves: values (quantised forms: from the exact sums of the f32
+        // gradients), then the predictions of their rows (grower.rs:208-219)
+        LeafParams lp{(double)cfg_.lambda, (double)cfg_.alpha, (double)cfg_.min_gain, cfg_.learning_rate, 0u};
+        float* pred = pred_.p + (size_t)o * n_;
+        timer_.begin(PH_LEAF);
+        launch_lw_leaves(bd_, st_);
+        if (qmode_ != GRAD_F32)
+            launch_b_leaf_sums(bd_, ridx_.p, ridx_.p, exact_ref(o), lp, scales_.p + 4 * (size_t)o, g_wide_, st_);
+        launch_b_leaf_update(bd_, ridx_.p, ridx_.p, pred, cfg_.record_leaves ? row_leaf_.p : nullptr, g_wide_, st_);
+        timer_.end();
+        m_.counters.launches += qmode_ != GRAD_F32 ? 3 : 2;
+        BST_CK(cudaMemcpyAsync(h_lw_bstate_, d_bstate_.p, sizeof(BState), cudaMemcpyDeviceToHost, st_));
+        BST_CK(cudaStreamSynchronize(st_));
+        const uint32_t nt = h_lw_bstate_->n_tnodes;
+        if (nt == 0 || nt > d_btree_.n) throw Error{BST_ERR_CUDA, "device tree has an invalid node count"};
+        std::vector<BTreeNode> bt(nt);
+        BST_CK(cudaMemcpyAsync(bt.data(), d_btree_.p, sizeof(BTreeNode) * nt, cudaMemcpyDeviceToHost, st_));
+        HostTree t;
+        t.group = o;
+        if (cfg_.record_leaves) {
+            t.row_leaf.resize(n_);
+            BST_CK(cudaMemcpyAsync(t.row_leaf.data(), row_leaf_.p, sizeof(uint32_t) * n_, cudaMemcpyDeviceToHost, st_));
+        }
+        BST_CK(cudaStreamSynchronize(st_));
+        BST_CK(cudaGetLastError());
+        m_.counters.hist_rows += h_lw_bstate_->hist_rows;
+        m_.counters.hist_bytes += h_lw_bstate_->hist_rows * ((uint64_t)p_.f8 + 2ull * p_.f16 + grad_bytes() + 4ull);
+        timer_.collect();
+        return host_tree_from(std::move(t), nt, bt.data());
+    }
+
     HostTree grow(uint32_t o) {
+        if (spec_leafwise_) return grow_lw_device(o);
         tree_output_ = o;
         gr_o_ = grad_ref(o);
         if (spec_leafwise_) gr_o_.qpos = qpos_[0].p;  // histograms read the positional copy

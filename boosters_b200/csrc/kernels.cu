@@ -2719,6 +2719,12 @@ __global__ void __launch_bounds__(1024) k_lw_children(BDev d, const PartWork* __
     __shared__ uint32_t sh[33];
     __shared__ unsigned long long rows;
     __shared__ uint32_t chunk, base;
+    const bool from_state = k == LW_K_FROM_STATE;
+    if (from_state) k = d.state->n_exp;  // device-driven step (0: nothing to expand)
+    if (k == 0) {
+        if (threadIdx.x == 0) d.state->hist_chunks = 0;
+        return;
+    }
     if (threadIdx.x == 0) {
         rows = 0;
         base = 0;
@@ -2767,6 +2773,7 @@ __global__ void __launch_bounds__(1024) k_lw_children(BDev d, const PartWork* __
         d.state->n_exp = k;
         d.state->hist_chunks = total;
         d.state->hist_chunk = chunk;
+        if (from_state) d.state->hist_rows += rows;
     }
 }
 
@@ -2775,6 +2782,424 @@ void launch_lw_children(const BDev& d, const PartWork* pw, const unsigned* curso
     if (k == 0) return;
     k_lw_children<<<1, 1024, 0, st>>>(d, pw, cursors, k, scan_nodes, scnt);
 }
+
+// ============================================================================
+// Device-side leaf-wise growth (expansion.rs:129-213, grower.rs:265-342,
+// 484-514): k_lw_replay replays the reference's heap pops on one warp; the
+// level kernels expand the batches it hands out.
+// ============================================================================
+
+namespace {
+
+__device__ __forceinline__ bool lw_expands(const NodeSplit& s, float min_gain) {  // grower.rs:530-539
+    const bool valid = (s.flags & 4u) && s.gain > -INFINITY;
+    return valid && !(s.gain <= min_gain);
+}
+
+// a pops before b: larger gain, ties by higher id (expansion.rs:311-319)
+__device__ __forceinline__ bool lw_before(float ga, uint32_t va, float gb, uint32_t vb) {
+    return ga > gb || (ga == gb && va > vb);
+}
+
+// Warp argmax over heap entries [0, n) that pass `ok`: returns the index
+// (0xFFFFFFFF: none). All lanes get the result.
+template <class Ok>
+__device__ uint32_t lw_argmax(const LwCand* heap, uint32_t n, Ok ok) {
+    const uint32_t lane = threadIdx.x & 31u;
+    float bg = -INFINITY;
+    uint32_t bv = 0, bi = 0xFFFFFFFFu;
+    for (uint32_t i = lane; i < n; i += 32) {
+        if (!ok(i)) continue;
+        const float g = heap[i].split.gain;
+        const uint32_t v = heap[i].vid;
+        if (bi == 0xFFFFFFFFu || lw_before(g, v, bg, bv)) {
+            bg = g;
+            bv = v;
+            bi = i;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const float og = __shfl_xor_sync(FULL, bg, o);
+        const uint32_t ov = __shfl_xor_sync(FULL, bv, o), oi = __shfl_xor_sync(FULL, bi, o);
+        if (oi != 0xFFFFFFFFu && (bi == 0xFFFFFFFFu || lw_before(og, ov, bg, bv))) {
+            bg = og;
+            bv = ov;
+            bi = oi;
+        }
+    }
+    return __shfl_sync(FULL, bi, 0);  // one answer for the warp, whatever the gains hold
+}
+
+// make_leaf (grower.rs:484-514): the leaf's value from its exact sums (the
+// quantised forms solve it again from the f32 gradients), listed for the
+// leaf kernels with the node's final row range.
+__device__ void lw_make_leaf(const BDev& d, const LwDev& w, const LwCand& c, const double* scale, const LeafParams& lp,
+                             uint32_t slot) {
+    const float v = leaf_value_dev(c.split.tot_g, c.split.tot_h, scale, lp);
+    write_leaf(d.tree[c.tnode], c.split.tot_g, c.split.tot_h, scale, v);
+    const uint2 r = w.pn[c.pnode];
+    BLeaf lf;
+    lf.begin = r.x;
+    lf.count = r.y;
+    lf.value = v;
+    lf.tnode = c.tnode;
+    lf.chunk_off = 0;
+    lf.buf = 0;
+    d.leaves[slot] = lf;
+}
+
+}  // namespace
+
+__global__ void k_lw_init(BDev d, LwDev w, uint32_t n, uint32_t root_count) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    LwCand r;
+    r.split = w.child[0];
+    r.pnode = 0;
+    r.tnode = 0;
+    r.depth = 0;
+    r.count = root_count;
+    r.vid = 0;
+    r.pad[0] = r.pad[1] = r.pad[2] = 0;
+    w.heap[0] = r;
+    w.pn[0] = make_uint2(0u, n);
+    LwState s;
+    s.n_heap = 1;
+    s.n_leaves = 1;
+    s.n_vid = 1;
+    s.n_batch = 0;
+    s.done = 0;
+    s.err = 0;
+    s.n_leaf_out = 0;
+    s.pad = 0;
+    *w.st = s;
+    BState& b = *d.state;
+    b.n_front = 0;
+    b.n_exp = 0;
+    b.n_pnodes = 1;
+    b.n_tnodes = 1;
+    b.part_chunks = 0;
+    b.hist_chunks = 0;
+    b.n_leaves = 0;
+    b.leaf_chunks = 0;
+    b.first_right = 1;
+    b.done = 0;
+    b.err = 0;
+    b.hist_rows = n;  // the root's histogram
+}
+
+void launch_lw_init(const BDev& d, const LwDev& w, uint32_t n, uint32_t root_count, cudaStream_t st) {
+    k_lw_init<<<1, 32, 0, st>>>(d, w, n, root_count);
+}
+
+// One warp. Absorbs the last step's expansions (children counts from the
+// partition cursors, splits from the scan) into the speculation table, then
+// pops (grower.rs:265-342) until a popped leaf needs an expansion that has
+// not run: that leaf and the best other unexpanded candidates become the
+// next step's batch (level state written, BState::n_exp = its size). When
+// the budget or the heap runs out, every remaining candidate becomes a leaf
+// (an expanded one over its whole range again) and the tree is done.
+__global__ void __launch_bounds__(32) k_lw_replay(BDev d, LwDev w, LeafParams lp, const double* __restrict__ scale) {
+    const uint32_t lane = threadIdx.x & 31u;
+    LwState S = *w.st;
+    BState& B = *d.state;
+    auto no_step = [&]() {
+        if (lane == 0) {
+            B.n_exp = 0;
+            B.part_chunks = 0;
+            B.hist_chunks = 0;
+        }
+    };
+    if (S.done) {
+        no_step();
+        return;
+    }
+    // 1. the last step's children
+    for (uint32_t j = lane; j < S.n_batch; j += 32) {
+        const BExp e = d.exp[j];
+        const uint32_t P = e.left_pnode, R = e.right_pnode;
+        const uint2 pr = w.pn[P];
+        const uint32_t lc = d.cursors[2 * j] - pr.x, rc = pr.y - lc;
+        LwSpec sp;
+        sp.right_pnode = R;
+        sp.begin = pr.x;
+        sp.count = pr.y;
+        sp.valid = 1;
+        for (int q = 0; q < 2; ++q) {
+            LwCand& k = sp.kids[q];
+            k.split = w.child[2 * j + q];
+            k.pnode = q ? R : P;
+            k.tnode = 0;
+            k.depth = e.pad1;
+            k.count = q ? rc : lc;
+            k.vid = 0;
+            k.pad[0] = k.pad[1] = k.pad[2] = 0;
+        }
+        w.spec[P] = sp;
+        w.pn[P] = make_uint2(pr.x, lc);
+        w.pn[R] = make_uint2(pr.x + lc, rc);
+    }
+    S.n_batch = 0;
+    __syncwarp();
+    // 2. pops
+    for (;;) {
+        if (S.n_leaves >= w.max_leaves || S.n_heap == 0) break;
+        const uint32_t i = lw_argmax(w.heap, S.n_heap, [](uint32_t) { return true; });
+        const LwCand e = w.heap[i];
+        const bool ex = lw_expands(e.split, w.min_gain);
+        if (ex && !w.spec[e.pnode].valid) {
+            // the next step: e and the best unexpanded candidates, at most as
+            // many as pops remain (rem after e's pop) and as free slots allow
+            const uint32_t rem = w.max_leaves - (S.n_leaves + 1);
+            const int64_t room = (int64_t)w.max_pnodes - (int64_t)B.n_pnodes - (int64_t)rem;
+            if (room < 1) {
+                if (lane == 0) {
+                    S.err = 1;
+                    S.done = 1;
+                    *w.st = S;
+                }
+                no_step();
+                return;
+            }
+            const int64_t want = (int64_t)rem + 1;
+            const uint32_t batch_max = (uint32_t)(want < room ? want : room);
+            // mark e, then take the best marked-free candidates one by one;
+            // the marks live in the pad word of the heap entries
+            if (lane == 0) w.heap[i].pad[0] = 1;
+            __syncwarp();
+            uint32_t k = 0;
+            uint32_t first_right = B.n_pnodes;
+            uint32_t chunks = 0;
+            for (uint32_t sel = i; sel != 0xFFFFFFFFu && k < batch_max;) {
+                const LwCand c = w.heap[sel];
+                const uint32_t j = k++;
+                const NodeSplit& sp = c.split;
+                const bool cat = (sp.flags & 2u) != 0u;
+                const BColumn bc = d.bcols[sp.col];
+                const uint2 r = w.pn[c.pnode];
+                const uint32_t nch = (r.y + B_PART_CHUNK - 1) / B_PART_CHUNK;
+                if (lane == 0) {
+                    BExp x;
+                    x.front = 0;
+                    x.right_pnode = first_right + j;
+                    x.tl = x.tr = 0;
+                    x.lc = x.rc = x.small_begin = x.small_count = 0;
+                    x.part_off = chunks;
+                    x.hist_off = 0;
+                    x.left_pnode = c.pnode;
+                    x.pad1 = c.depth + 1;  // the children's depth (column masks)
+                    d.exp[j] = x;
+                    PartWork pw;
+                    pw.begin = r.x;
+                    pw.count = r.y;
+                    pw.matrix = bc.matrix;
+                    pw.pos = bc.pos;
+                    pw.thr_bin = sp.bin;
+                    pw.flags = (sp.flags & 1u) | (bc.has_missing ? 2u : 0u) | (cat ? 4u : 0u);
+                    pw.default_bin = bc.default_bin;
+                    pw.pad = 0;
+                    for (int q = 0; q < 4; ++q) pw.cats[q] = sp.cats[q];
+                    d.pworks[j] = pw;
+                    d.cursors[2 * j] = r.x;
+                    d.cursors[2 * j + 1] = r.x + r.y;
+                    if (d.rmask) d.scnt[2 * j] = d.scnt[2 * j + 1] = 0u;
+                }
+                for (uint32_t q = lane; q < nch; q += 32)
+                    if (chunks + q < d.max_part_chunks)
+                        d.part_map[chunks + q] = make_uint2(j, r.x + q * B_PART_CHUNK);
+                chunks += nch;
+                __syncwarp();
+                if (k >= batch_max) break;
+                sel = lw_argmax(w.heap, S.n_heap, [&](uint32_t q) {
+                    return w.heap[q].pad[0] == 0 && lw_expands(w.heap[q].split, w.min_gain) &&
+                           !w.spec[w.heap[q].pnode].valid;
+                });
+                if (sel != 0xFFFFFFFFu && lane == 0) w.heap[sel].pad[0] = 1;
+                __syncwarp();
+            }
+            for (uint32_t q = lane; q < S.n_heap; q += 32) w.heap[q].pad[0] = 0;  // clear the marks
+            if (lane == 0) {
+                S.n_batch = k;
+                *w.st = S;
+                B.n_exp = k;
+                B.first_right = first_right;
+                B.n_pnodes = first_right + k;
+                B.part_chunks = min(chunks, d.max_part_chunks);
+                B.hist_chunks = 0;
+            }
+            return;
+        }
+        // pop e
+        if (lane == 0) {
+            w.heap[i] = w.heap[S.n_heap - 1];
+        }
+        S.n_heap -= 1;
+        S.n_leaves += 1;
+        __syncwarp();
+        if (!ex) {
+            if (lane == 0) lw_make_leaf(d, w, e, scale, lp, S.n_leaf_out);
+            S.n_leaf_out += 1;
+            __syncwarp();
+            continue;
+        }
+        // apply_split (grower.rs:576-650): children tree nodes in allocation
+        // order; a categorical split sends the training-left rows to the
+        // stored right child
+        const LwSpec sp = w.spec[e.pnode];
+        const uint32_t l = B.n_tnodes, r = B.n_tnodes + 1;
+        const bool cat = (e.split.flags & 2u) != 0u;
+        if (lane == 0) {
+            w.spec[e.pnode].valid = 0;
+            BTreeNode t;
+            t.col = e.split.col;
+            t.bin = e.split.bin;
+            t.flags = (e.split.flags & 1u) | (cat ? 2u : 0u);
+            t.left = l;
+            t.right = r;
+            t.gain = e.split.gain;
+            t.leaf = 0.0f;
+            t.G = (double)e.split.tot_g * scale[2];
+            t.H = (double)e.split.tot_h * scale[3];
+            for (int q = 0; q < 4; ++q) t.cats[q] = e.split.cats[q];
+            d.tree[e.tnode] = t;
+            LwCand k0 = sp.kids[0], k1 = sp.kids[1];
+            k0.tnode = cat ? r : l;
+            k1.tnode = cat ? l : r;
+            k0.vid = e.vid;
+            k1.vid = S.n_vid;
+            w.heap[S.n_heap] = k0;
+            w.heap[S.n_heap + 1] = k1;
+            B.n_tnodes = r + 1;
+        }
+        S.n_vid += 1;
+        S.n_heap += 2;
+        __syncwarp();
+    }
+    // 3. done: every candidate left becomes a leaf, an expanded one over its
+    // whole range (its right partition node keeps no rows)
+    for (uint32_t q = 0; q < S.n_heap; ++q) {
+        const LwCand c = w.heap[q];
+        if (lane == 0) {
+            const LwSpec sp = w.spec[c.pnode];
+            if (sp.valid) {
+                w.pn[c.pnode] = make_uint2(sp.begin, sp.count);
+                w.pn[sp.right_pnode] = make_uint2(sp.begin + sp.count, 0u);
+                w.spec[c.pnode].valid = 0;
+            }
+            lw_make_leaf(d, w, c, scale, lp, S.n_leaf_out);
+        }
+        S.n_leaf_out += 1;
+        __syncwarp();
+    }
+    if (lane == 0) {
+        S.n_heap = 0;
+        S.done = 1;
+        *w.st = S;
+        B.n_leaves = S.n_leaf_out;
+        B.n_exp = 0;
+        B.part_chunks = 0;
+        B.hist_chunks = 0;
+    }
+}
+
+void launch_lw_replay(const BDev& d, const LwDev& w, LeafParams lp, const double* scale, cudaStream_t st) {
+    k_lw_replay<<<1, 32, 0, st>>>(d, w, lp, scale);
+}
+
+// Partition of the pending batch over its chunk map, rin -> rout (no
+// children derivation: k_lw_children follows).
+template <typename Q>
+__global__ void __launch_bounds__(PART_THREADS)
+k_lw_partition(BDev d, const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp,
+               const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16,
+               const Q* __restrict__ qin, Q* __restrict__ qout, BinsFM fm) {
+    __shared__ PartWork w;
+    __shared__ uint2 s_m;
+    const uint32_t total = min(d.state->part_chunks, d.max_part_chunks);
+    for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+        if (threadIdx.x == 0) {
+            const uint2 m = d.part_map[c];
+            s_m = m;
+            w = d.pworks[m.x];
+        }
+        __syncthreads();
+        const uint32_t j = s_m.x, start = s_m.y;
+        const uint32_t len = min(B_PART_CHUNK, w.begin + w.count - start);
+        part_rows<Q>(w, start, len, d.cursors + 2 * j, ridx, tmp, bins8, s8, bins16, s16, qin, qout, fm.b8, fm.b16,
+                     fm.n, d.rmask, d.rmask ? d.scnt + 2 * j : nullptr);
+    }
+}
+
+// The partitioned rows (and gradient elements) back into the row buffer:
+// chunk c copies its 2048 positions of its node's range.
+template <typename Q>
+__global__ void k_lw_copy_back(BDev d, const uint32_t* __restrict__ tmp, uint32_t* __restrict__ ridx,
+                               const Q* __restrict__ qtmp, Q* __restrict__ q) {
+    const uint32_t total = min(d.state->part_chunks, d.max_part_chunks);
+    for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+        const uint2 m = d.part_map[c];
+        const PartWork w = d.pworks[m.x];
+        const uint32_t len = min(B_PART_CHUNK, w.begin + w.count - m.y);
+        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+            ridx[m.y + i] = tmp[m.y + i];
+            if constexpr (!std::is_same<Q, char>::value) q[m.y + i] = qtmp[m.y + i];
+        }
+    }
+}
+
+template <typename Q>
+static void lw_partition_t(const BDev& d, uint32_t* rin, uint32_t* rout, const uint8_t* bins8, uint32_t s8,
+                           const uint16_t* bins16, uint32_t s16, uint32_t grid, Q* qin, Q* qout, const BinsFM& fm,
+                           cudaStream_t st) {
+    k_lw_partition<Q><<<grid, PART_THREADS, 0, st>>>(d, rin, rout, bins8, s8, bins16, s16, qin, qout, fm);
+    k_lw_copy_back<Q><<<grid, 256, 0, st>>>(d, rout, rin, qout, qin);
+}
+
+void launch_lw_partition(const BDev& d, uint32_t* rin, uint32_t* rout, const uint8_t* bins8, uint32_t s8,
+                         const uint16_t* bins16, uint32_t s16, uint32_t grid, void* qin, void* qout, int mode,
+                         const BinsFM& fm, cudaStream_t st) {
+    if (!qin || !qout)
+        lw_partition_t<char>(d, rin, rout, bins8, s8, bins16, s16, grid, nullptr, nullptr, fm, st);
+    else if (mode == GRAD_Q8)
+        lw_partition_t<char2>(d, rin, rout, bins8, s8, bins16, s16, grid, static_cast<char2*>(qin),
+                              static_cast<char2*>(qout), fm, st);
+    else if (mode == GRAD_Q16)
+        lw_partition_t<short2>(d, rin, rout, bins8, s8, bins16, s16, grid, static_cast<short2*>(qin),
+                               static_cast<short2*>(qout), fm, st);
+    else
+        lw_partition_t<float2>(d, rin, rout, bins8, s8, bins16, s16, grid, static_cast<float2*>(qin),
+                               static_cast<float2*>(qout), fm, st);
+}
+
+// Leaf chunk map of the finished tree (k_b_finalize's second half) and the
+// leaf sums zeroed for the quantised forms' exact leaf solve.
+__global__ void __launch_bounds__(1024) k_lw_leaves(BDev d) {
+    __shared__ uint32_t sh[33];
+    __shared__ uint32_t base;
+    BState* s = d.state;
+    const uint32_t nl = s->n_leaves;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    for (uint32_t l0 = 0; l0 < nl; l0 += blockDim.x) {
+        const uint32_t l = l0 + threadIdx.x;
+        const uint32_t begin = l < nl ? d.leaves[l].begin : 0u;
+        const uint32_t nch = l < nl ? (d.leaves[l].count + B_LEAF_CHUNK - 1) / B_LEAF_CHUNK : 0u;
+        uint32_t tc;
+        const uint32_t jc = block_excl_scan(nch, sh, &tc);
+        if (l < nl) {
+            d.leaves[l].chunk_off = base + jc;
+            for (uint32_t k = 0; k < nch; ++k)
+                if (base + jc + k < d.max_leaf_chunks)
+                    d.leaf_map[base + jc + k] = make_uint2(l, begin + k * B_LEAF_CHUNK);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) base += tc;
+        __syncthreads();
+    }
+    for (uint32_t i = threadIdx.x; i < 2 * nl; i += blockDim.x) d.sums[i] = 0;
+    if (threadIdx.x == 0) s->leaf_chunks = base < d.max_leaf_chunks ? base : d.max_leaf_chunks;
+}
+
+void launch_lw_leaves(const BDev& d, cudaStream_t st) { k_lw_leaves<<<1, 1024, 0, st>>>(d); }
 
 template <typename HB>
 __global__ void k_b_zero_right(BDev d, HB* __restrict__ hist, uint64_t slot_bins) {
@@ -2867,7 +3292,7 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32)
 k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HB* __restrict__ hist,
          uint64_t slot_bins, const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
          long long* __restrict__ node_tot, int b, int last_wins, LeafParams lp, uint32_t buf,
-         const ScanNode* __restrict__ root, const uint8_t* __restrict__ colmask) {
+         const ScanNode* __restrict__ root, const uint8_t* __restrict__ colmask, NodeSplit* __restrict__ lw_out) {
     __shared__ double s_key[SCAN_WARPS][SORT_N];
     __shared__ uint32_t s_cat[SCAN_WARPS][SORT_N];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -2907,10 +3332,15 @@ k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HB*
             sp.flags = (w.flags & 3u) | 4u;
             for (int q = 0; q < 4; ++q) sp.cats[q] = w.cats[q];
         }
+        if (lw_out) {
+            lw_out[node] = sp;
+            continue;
+        }
         B[node].split = sp;
         B[node].G = sp.tot_g;
         B[node].H = sp.tot_h;
     }
+    if (lw_out) return;
     __syncthreads();
     decide_body(d, b, lp, scale, buf);
 }
@@ -2918,15 +3348,15 @@ k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HB*
 void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const void* hist, uint64_t slot_bins,
                    const double* scale, GainParamsDev gp, ColCand* cand, long long* node_tot, int b, int last_wins,
                    LeafParams lp, uint32_t buf, uint32_t grid, cudaStream_t st, int hist32, const ScanNode* root,
-                   const uint8_t* colmask) {
+                   const uint8_t* colmask, NodeSplit* lw_out) {
     if (hist32)
         k_b_scan<HBin32><<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, static_cast<const HBin32*>(hist), slot_bins,
                                                            scale, gp, cand, node_tot, b, last_wins, lp, buf, root,
-                                                           colmask);
+                                                           colmask, lw_out);
     else
         k_b_scan<HBin><<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, static_cast<const HBin*>(hist), slot_bins,
                                                          scale, gp, cand, node_tot, b, last_wins, lp, buf, root,
-                                                         colmask);
+                                                         colmask, lw_out);
 }
 
 // This thread's share of the fixed-point sums of positions [start, start +

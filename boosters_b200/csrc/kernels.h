@@ -327,6 +327,50 @@ struct BDev {  // device buffers of the level loop
 constexpr uint32_t B_PART_CHUNK = 2048;
 constexpr uint32_t B_LEAF_CHUNK = 4096;
 
+// ---- device-side leaf-wise growth (expansion.rs:129-213) ---------------------
+// The reference pops the leaf of largest (gain, node id) from a max-heap,
+// splits it and pushes its children until max_leaves. The device replays
+// those pops exactly (k_lw_replay, one warp): when the popped leaf has not
+// been expanded yet it stops and hands the level kernels a batch of the
+// best unexpanded candidates (the popped one first, at most as many as pops
+// remain); their rows, histograms and splits do not depend on when they are
+// expanded (exact sums), so a later pop of a batch member costs no step.
+struct LwCand {          // a leaf that may be split
+    NodeSplit split;     // its best split; tot_g / tot_h: the node's exact sums
+    uint32_t pnode, tnode, depth, count;  // partition node, tree node, depth, rows
+    uint32_t vid;        // heap order id: gain ties pop the higher id first (expansion.rs:311-319)
+    uint32_t pad[3];
+};
+struct LwSpec {          // a partition node expanded before its pop
+    LwCand kids[2];      // training-left and training-right children
+    uint32_t right_pnode, begin, count, valid;  // range before the split; valid: not yet popped
+};
+struct LwState {
+    uint32_t n_heap, n_leaves, n_vid, n_batch;
+    uint32_t done, err, n_leaf_out, pad;
+};
+struct LwDev {
+    LwState* st;
+    LwCand* heap;        // [heap_cap]
+    LwSpec* spec;        // [max_pnodes]
+    uint2* pn;           // [max_pnodes] (begin, count) of each partition node
+    NodeSplit* child;    // [max_pnodes] split search results of the pending step's children (root: [0])
+    uint32_t heap_cap, max_pnodes, max_leaves;
+    float min_gain;
+};
+// State of a new tree: the root candidate from child[0], its rows [0, n).
+void launch_lw_init(const BDev& d, const LwDev& w, uint32_t n, uint32_t root_count, cudaStream_t st);
+// Replays pops until the next expansion is needed (writes that batch's level
+// state) or the tree is done (leaves listed in BDev::leaves, BState::n_leaves).
+void launch_lw_replay(const BDev& d, const LwDev& w, LeafParams lp, const double* scale, cudaStream_t st);
+// Partition of the pending batch (rin -> rout), then the rows copied back
+// into rin (leaf-wise keeps one row-index buffer); qin / qout likewise.
+void launch_lw_partition(const BDev& d, uint32_t* rin, uint32_t* rout, const uint8_t* bins8, uint32_t s8,
+                         const uint16_t* bins16, uint32_t s16, uint32_t grid, void* qin, void* qout, int mode,
+                         const BinsFM& fm, cudaStream_t st);
+// Leaf chunk map of the finished tree and zeroed leaf sums.
+void launch_lw_leaves(const BDev& d, cudaStream_t st);
+
 // Raises the dynamic shared-memory limits of the kernels that need > 48 KiB
 // (call once per device before any stream capture).
 void init_kernel_attributes();
@@ -382,6 +426,8 @@ void launch_b_merge(const BDev& d, void* hist, uint64_t slot_bins, uint32_t tota
 // slots), from the partition's cursors, on the device.
 // scnt (or null): the partition's sampled-row counts (row sampling), used
 // as the children's scan counts
+// k == LW_K_FROM_STATE: the batch size is BState::n_exp (device-driven steps)
+constexpr uint32_t LW_K_FROM_STATE = 0xFFFFFFFFu;
 void launch_lw_children(const BDev& d, const PartWork* pw, const unsigned* cursors, uint32_t k, ScanNode* scan_nodes,
                         const unsigned* scnt, cudaStream_t st);
 // Level state of the root histogram: all n rows as one segment list.
@@ -392,11 +438,13 @@ void launch_b_root_hist(const BDev& d, uint64_t n, uint32_t chunk, cudaStream_t 
 // root (or null): the level is the root alone, described by *root (rows in
 // buffer 0, frontier 0); colmask (or null): the level's column masks, a
 // node's row chosen by ScanNode.pad (0 for the device-built levels)
+// lw_out (or null): leaf-wise steps: the last block writes the 2 n_exp
+// children's splits there instead of a frontier and takes no decisions
 void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const void* hist,
                    uint64_t slot_bins, const double* scale, GainParamsDev gp, ColCand* cand,
                    long long* node_tot, int b, int last_wins, LeafParams lp, uint32_t buf, uint32_t grid,
                    cudaStream_t st, int hist32 = 0, const ScanNode* root = nullptr,
-                   const uint8_t* colmask = nullptr);
+                   const uint8_t* colmask = nullptr, NodeSplit* lw_out = nullptr);
 // last level: the smaller children's sums, then (last block) both children's
 // sums into frontier b
 void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, int b, uint32_t grid, cudaStream_t st);

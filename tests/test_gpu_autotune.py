@@ -60,7 +60,7 @@ def test_cache_with_unknown_or_bad_lines_is_ignored(tmp_path):
     ds = bst.Dataset.from_feature_major(x, y)
     cache = tmp_path / "tune.txt"
     cache.write_text("some other key\titems=1,hist=0,grid=4\nbroken line without tab\n")
-    kw = dict(objective=bst.Objective.logistic(), n_estimators=16, max_depth=5, precision="q8", batched=True)
+    kw = dict(objective=bst.Objective.logistic(), n_estimators=24, max_depth=5, precision="q8", batched=True)
     m = bst.GBDTModel.train(ds, bst.GBDTConfig(autotune=True, autotune_cache=cache, **kw))
     assert "(explored:" in m.tune_info
     text = cache.read_text()
