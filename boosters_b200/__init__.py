@@ -66,6 +66,58 @@ class Objective:
         def __repr__(self):
             return f"Objective.Softmax(n_classes={self.n_classes})"
 
+    class Absolute:
+        """L1 loss; leaf values renewed to the leaf's median residual."""
+        code = _n.OBJ_ABSOLUTE
+        n_outputs = 1
+
+        def __repr__(self):
+            return "Objective.Absolute()"
+
+    class Pinball:
+        """Quantile regression, one output per alpha; leaf values renewed to
+        the alpha-quantile residual."""
+        code = _n.OBJ_PINBALL
+
+        def __init__(self, alpha):
+            a = [float(v) for v in (alpha if np.ndim(alpha) else [alpha])]
+            if not a:
+                raise ValueError("alpha must have at least one quantile")
+            if any(not (0.0 < v < 1.0) for v in a):
+                raise ValueError("alpha values must be in (0, 1)")
+            self.alpha = a
+            self.n_outputs = len(a)
+
+        def __repr__(self):
+            return f"Objective.Pinball(alpha={self.alpha})"
+
+    class Huber:
+        """Pseudo-Huber loss with transition point delta."""
+        code = _n.OBJ_PSEUDO_HUBER
+        n_outputs = 1
+
+        def __init__(self, delta=1.0):
+            if not float(delta) > 0.0:
+                raise ValueError("delta must be positive")
+            self.delta = float(delta)
+
+        def __repr__(self):
+            return f"Objective.Huber(delta={self.delta})"
+
+    class Poisson:
+        code = _n.OBJ_POISSON
+        n_outputs = 1
+
+        def __repr__(self):
+            return "Objective.Poisson()"
+
+    class Hinge:
+        code = _n.OBJ_HINGE
+        n_outputs = 1
+
+        def __repr__(self):
+            return "Objective.Hinge()"
+
     @staticmethod
     def squared():
         return Objective.Squared()
@@ -77,6 +129,26 @@ class Objective:
     @staticmethod
     def softmax(n_classes):
         return Objective.Softmax(n_classes)
+
+    @staticmethod
+    def absolute():
+        return Objective.Absolute()
+
+    @staticmethod
+    def pinball(alpha):
+        return Objective.Pinball(alpha)
+
+    @staticmethod
+    def huber(delta=1.0):
+        return Objective.Huber(delta)
+
+    @staticmethod
+    def poisson():
+        return Objective.Poisson()
+
+    @staticmethod
+    def hinge():
+        return Objective.Hinge()
 
 
 class Metric:
@@ -94,9 +166,61 @@ class Metric:
     class NoMetric:
         code = _n.METRIC_NONE
 
+    class Mae:
+        code = _n.METRIC_MAE
+
+    class Mape:
+        code = _n.METRIC_MAPE
+
+    class MarginAccuracy:
+        code = _n.METRIC_MARGIN_ACCURACY
+
+    class PoissonDeviance:
+        code = _n.METRIC_POISSON
+
+    class Quantile:
+        code = _n.METRIC_QUANTILE
+
+        def __init__(self, alpha):
+            self.alpha = [float(v) for v in (alpha if np.ndim(alpha) else [alpha])]
+            if not self.alpha or any(not (0.0 < v < 1.0) for v in self.alpha):
+                raise ValueError("alpha values must be in (0, 1)")
+
+    class Huber:
+        code = _n.METRIC_HUBER
+
+        def __init__(self, delta=1.0):
+            if not float(delta) > 0.0:
+                raise ValueError("delta must be positive")
+            self.delta = float(delta)
+
     @staticmethod
     def rmse():
         return Metric.Rmse()
+
+    @staticmethod
+    def mae():
+        return Metric.Mae()
+
+    @staticmethod
+    def mape():
+        return Metric.Mape()
+
+    @staticmethod
+    def margin_accuracy():
+        return Metric.MarginAccuracy()
+
+    @staticmethod
+    def poisson_deviance():
+        return Metric.PoissonDeviance()
+
+    @staticmethod
+    def quantile(alpha):
+        return Metric.Quantile(alpha)
+
+    @staticmethod
+    def huber(delta=1.0):
+        return Metric.Huber(delta)
 
     @staticmethod
     def logloss():
@@ -131,7 +255,7 @@ class GBDTConfig:
                  max_categorical_cardinality=0, binning_sample_cnt=200000, cache_size=8,
                  early_stopping_rounds=None, seed=42, verbosity=0, precision="fp32",
                  cuda_graph=False, device=0, batched=True, phase_timings=False, autotune=True,
-                 autotune_cache=None):
+                 autotune_cache=None, goss_top_rate=0.0, goss_other_rate=0.0):
         self.n_estimators = n_estimators
         self.learning_rate = learning_rate
         self.objective = objective if objective is not None else Objective.Squared()
@@ -166,6 +290,9 @@ class GBDTConfig:
         self.batched = batched
         self.autotune = autotune
         self.autotune_cache = None if autotune_cache is None else os.fspath(autotune_cache)
+        # GOSS row sampling (training/sampling/row.rs:214-280): top_rate > 0 turns it on
+        self.goss_top_rate = goss_top_rate
+        self.goss_other_rate = goss_other_rate
         _n.check(_n.lib.bst_config_validate(ctypes.byref(self.to_c())))
 
     def to_c(self, record_leaves=False):
@@ -206,6 +333,16 @@ class GBDTConfig:
         c.autotune = 1 if self.autotune else 0
         # the struct keeps the bytes object alive as long as the struct lives
         c.autotune_cache = None if self.autotune_cache is None else os.fsencode(self.autotune_cache)
+        # objective / metric parameters (the struct keeps the array alive too)
+        alpha = getattr(self.objective, "alpha", None) or getattr(self.metric, "alpha", None)
+        if alpha:
+            c.quantile_alpha = (ctypes.c_float * len(alpha))(*alpha)
+            c.n_quantiles = len(alpha)
+        delta = getattr(self.objective, "delta", None) or getattr(self.metric, "delta", None)
+        if delta is not None:
+            c.huber_delta = float(delta)
+        c.goss_top_rate = float(self.goss_top_rate)
+        c.goss_other_rate = float(self.goss_other_rate)
         return c
 
     def __repr__(self):
@@ -618,17 +755,27 @@ class Booster:
             self._h = None
 
 
-def metric(kind, preds_group_major, labels, weights=None):
-    """Metric value (training/metrics): kind in {'rmse', 'logloss', 'mlogloss'}."""
-    codes = {"rmse": _n.METRIC_RMSE, "logloss": _n.METRIC_LOGLOSS, "mlogloss": _n.METRIC_MLOGLOSS}
+_METRIC_CODES = {"rmse": _n.METRIC_RMSE, "logloss": _n.METRIC_LOGLOSS, "mlogloss": _n.METRIC_MLOGLOSS,
+                 "mae": _n.METRIC_MAE, "mape": _n.METRIC_MAPE, "quantile": _n.METRIC_QUANTILE,
+                 "huber": _n.METRIC_HUBER, "poisson": _n.METRIC_POISSON,
+                 "margin_accuracy": _n.METRIC_MARGIN_ACCURACY}
+
+
+def metric(kind, preds_group_major, labels, weights=None, alpha=None, delta=1.0):
+    """Metric value (training/metrics) of transformed predictions (raw
+    margins for 'margin_accuracy'): kind in {'rmse', 'logloss', 'mlogloss',
+    'mae', 'mape', 'quantile' (alpha: one per output), 'huber' (delta),
+    'poisson', 'margin_accuracy'}."""
     p = _f32(preds_group_major)
     if p.ndim == 1:
         p = p.reshape(1, -1)
     y = _f32(labels).reshape(-1)
     w = None if weights is None else _f32(weights).reshape(-1)
+    a = None if alpha is None else _f32(np.atleast_1d(alpha))
     out = ctypes.c_double()
-    _n.check(_n.lib.bst_metric(codes[kind], _n.ptr(p, ctypes.c_float), p.shape[0], p.shape[1],
-                               _n.ptr(y, ctypes.c_float), _n.ptr(w, ctypes.c_float), ctypes.byref(out)))
+    _n.check(_n.lib.bst_metric_ex(_METRIC_CODES[kind], _n.ptr(p, ctypes.c_float), p.shape[0], p.shape[1],
+                                  _n.ptr(y, ctypes.c_float), _n.ptr(w, ctypes.c_float), _n.ptr(a, ctypes.c_float),
+                                  0 if a is None else a.size, float(delta), ctypes.byref(out)))
     return out.value
 
 

@@ -25,7 +25,9 @@ BST_ERR_TIMEOUT = 8
 BST_ERR_FORMAT = 9
 
 OBJ_SQUARED, OBJ_LOGISTIC, OBJ_SOFTMAX = 0, 1, 2
+OBJ_ABSOLUTE, OBJ_PINBALL, OBJ_PSEUDO_HUBER, OBJ_POISSON, OBJ_HINGE = 3, 4, 5, 6, 7
 METRIC_DEFAULT, METRIC_NONE, METRIC_RMSE, METRIC_LOGLOSS, METRIC_MLOGLOSS = -1, 0, 1, 2, 3
+METRIC_MAE, METRIC_MAPE, METRIC_QUANTILE, METRIC_HUBER, METRIC_POISSON, METRIC_MARGIN_ACCURACY = 4, 5, 6, 7, 8, 9
 GROWTH_DEPTHWISE, GROWTH_LEAFWISE = 0, 1
 PRECISION_FP32, PRECISION_Q16, PRECISION_Q8 = 0, 1, 2
 
@@ -68,6 +70,11 @@ class Config(ctypes.Structure):
         ("phase_timings", ctypes.c_int32),
         ("autotune", ctypes.c_int32),
         ("autotune_cache", ctypes.c_char_p),
+        ("quantile_alpha", c_f32p),
+        ("n_quantiles", ctypes.c_uint32),
+        ("huber_delta", ctypes.c_float),
+        ("goss_top_rate", ctypes.c_float),
+        ("goss_other_rate", ctypes.c_float),
     ]
 
 

@@ -126,6 +126,9 @@ SIGNATURES = [
       c_f32p, c_f32p]),
     ("bst_metric", ctypes.c_int32,
      [ctypes.c_int32, c_f32p, ctypes.c_uint32, ctypes.c_uint64, c_f32p, c_f32p, c_f64p]),
+    ("bst_metric_ex", ctypes.c_int32,
+     [ctypes.c_int32, c_f32p, ctypes.c_uint32, ctypes.c_uint64, c_f32p, c_f32p, c_f32p, ctypes.c_uint32,
+      ctypes.c_float, c_f64p]),
 ]
 
 

@@ -79,8 +79,27 @@ bst_status check_config(const bst_config* c, bool for_training) {
     const char* gn[4] = {"lambda", "alpha", "min_child_weight", "min_gain"};
     for (int i = 0; i < 4; ++i)
         if (*g[i] < 0.0f) return fail(BST_ERR_CONFIG, std::string(gn[i]) + " must be non-negative, got " + fmt(*g[i]));
+    // objective and sampling parameters (packages/boosters-python/src/objectives.rs
+    // constructors, training/sampling/row.rs:64-75 RowSamplingParams::goss)
+    if (c->objective == BST_OBJ_PINBALL || c->metric == BST_METRIC_QUANTILE) {
+        if (c->n_quantiles == 0 || !c->quantile_alpha)
+            return fail(BST_ERR_CONFIG, "pinball loss needs at least one quantile");
+        for (uint32_t i = 0; i < c->n_quantiles; ++i)
+            if (!(c->quantile_alpha[i] > 0.0f && c->quantile_alpha[i] < 1.0f))
+                return fail(BST_ERR_CONFIG, "quantile alpha must be in (0, 1), got " + fmt(c->quantile_alpha[i]));
+    }
+    if ((c->objective == BST_OBJ_PSEUDO_HUBER || c->metric == BST_METRIC_HUBER) && !(c->huber_delta > 0.0f))
+        return fail(BST_ERR_CONFIG, "huber_delta must be positive, got " + fmt(c->huber_delta));
+    if (c->goss_top_rate != 0.0f || c->goss_other_rate != 0.0f) {
+        if (!(c->goss_top_rate > 0.0f) || !(c->goss_other_rate > 0.0f))
+            return fail(BST_ERR_CONFIG, "GOSS top_rate and other_rate must be positive");
+        if (c->goss_top_rate + c->goss_other_rate > 1.0f)
+            return fail(BST_ERR_CONFIG, "top_rate + other_rate must be <= 1.0");
+        if (std::fabs(c->subsample - 1.0f) >= 1e-6f)
+            return fail(BST_ERR_CONFIG, "GOSS and subsample < 1 cannot be combined");
+    }
     if (!for_training) return BST_OK;
-    if (c->objective < BST_OBJ_SQUARED || c->objective > BST_OBJ_SOFTMAX)
+    if (c->objective < BST_OBJ_SQUARED || c->objective > BST_OBJ_HINGE)
         return fail(BST_ERR_UNSUPPORTED, "objective not supported by the GPU engine");
     if (c->objective == BST_OBJ_SOFTMAX && c->n_classes < 2) return fail(BST_ERR_CONFIG, "softmax needs n_classes >= 2");
     if (c->growth_strategy != BST_GROWTH_DEPTHWISE && c->growth_strategy != BST_GROWTH_LEAFWISE)
@@ -145,6 +164,11 @@ void bst_config_default(bst_config* c) {
     c->phase_timings = 0;
     c->autotune = 1;
     c->autotune_cache = nullptr;
+    c->quantile_alpha = nullptr;
+    c->n_quantiles = 0;
+    c->huber_delta = 1.0f;
+    c->goss_top_rate = 0.0f;
+    c->goss_other_rate = 0.0f;
 }
 
 bst_status bst_config_validate(const bst_config* c) {
@@ -576,7 +600,7 @@ bst_status bst_tree_grow(const bst_dataset* ds, const float* g, const float* h, 
 bst_status bst_model_create(uint32_t G, uint32_t F, int32_t objective, const float* base, bst_model** out) {
     return guarded([&]() -> bst_status {
         if (!out || G == 0 || !base) return fail(BST_ERR_INVALID_ARGUMENT, "bad argument");
-        if (objective < BST_OBJ_SQUARED || objective > BST_OBJ_SOFTMAX) return fail(BST_ERR_INVALID_ARGUMENT, "bad objective");
+        if (objective < BST_OBJ_SQUARED || objective > BST_OBJ_HINGE) return fail(BST_ERR_INVALID_ARGUMENT, "bad objective");
         auto m = std::make_unique<bst::Model>();
         m->n_groups = G;
         m->n_features = F;
@@ -1017,14 +1041,27 @@ bst_status bst_server_replay(bst_server* server, const float* pool, uint64_t poo
 
 void bst_server_free(bst_server* server) { delete server; }
 
-bst_status bst_metric(int32_t metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w,
-                      double* out) {
+bst_status bst_metric_ex(int32_t metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w,
+                         const float* alpha, uint32_t n_alpha, float delta, double* out) {
     if (!out || (n && (!p || !y))) return fail(BST_ERR_INVALID_ARGUMENT, "NULL argument");
     *out = 0.0;
-    if (metric != BST_METRIC_RMSE && metric != BST_METRIC_LOGLOSS && metric != BST_METRIC_MLOGLOSS)
+    if (metric < BST_METRIC_RMSE || metric > BST_METRIC_MARGIN_ACCURACY)
         return fail(BST_ERR_INVALID_ARGUMENT, "unknown metric");
-    *out = bst::metric_value(metric, p, G, n, y, w);
+    if (metric == BST_METRIC_QUANTILE && (!alpha || n_alpha < G))
+        return fail(BST_ERR_INVALID_ARGUMENT, "the quantile metric needs one alpha per output");
+    if (metric == BST_METRIC_HUBER && !(delta > 0.0f)) return fail(BST_ERR_INVALID_ARGUMENT, "delta must be positive");
+    bst::MetricParams mp;
+    mp.alpha = alpha;
+    mp.n_alpha = n_alpha;
+    mp.delta = delta;
+    *out = bst::metric_value(metric, p, G, n, y, w, mp);
     return BST_OK;
+}
+
+bst_status bst_metric(int32_t metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w,
+                      double* out) {
+    if (metric == BST_METRIC_QUANTILE) return fail(BST_ERR_INVALID_ARGUMENT, "the quantile metric needs bst_metric_ex");
+    return bst_metric_ex(metric, p, G, n, y, w, nullptr, 0, 1.0f, out);
 }
 
 }  // extern "C"

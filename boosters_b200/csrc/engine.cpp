@@ -237,6 +237,45 @@ class RowSampler {
         for (uint32_t r : idx_) mask[r] = 1;
         return k;
     }
+    // sample_goss (row.rs:214-280) on one output's (grad, hess) pairs: code
+    // 1 for the rows of the top_rate share by |grad x hess| (ties at the
+    // threshold included), 2 for the other_rate x n drawn from the rest with
+    // probability need / rest (rng.gen::<f32>(): the top 24 bits of the
+    // upper half of a generator output, times 2^-24), whose grad / hess
+    // are scaled by *mult; 0 for the rows left out. Returns the kept count.
+    uint64_t goss(const float* gh, uint64_t n, float top_rate, float other_rate, std::vector<uint8_t>& code,
+                  float* mult) {
+        std::vector<float> mag(n);
+        for (uint64_t i = 0; i < n; ++i) mag[i] = std::fabs(gh[2 * i] * gh[2 * i + 1]);
+        uint64_t top_k = (uint64_t)((float)n * top_rate);
+        top_k = std::min<uint64_t>(std::max<uint64_t>(top_k, 1), n - 1);
+        const uint64_t other_k = std::max<uint64_t>((uint64_t)((float)n * other_rate), 1);
+        std::vector<float> sorted(mag);
+        std::nth_element(sorted.begin(), sorted.begin() + (n - top_k), sorted.end());
+        const float threshold = sorted[n - top_k];
+        *mult = (float)(n - top_k) / (float)other_k;
+        uint64_t big = 0, small = 0;
+        code.assign(n, 0);
+        for (uint64_t i = 0; i < n; ++i) {
+            if (mag[i] >= threshold) {
+                code[i] = 1;
+                ++big;
+                continue;
+            }
+            const uint64_t need = other_k > small ? other_k - small : 0;
+            const uint64_t top_left = top_k > big ? top_k - big : 0;
+            const uint64_t rest = (n - i) > top_left ? (n - i) - top_left : 0;
+            if (rest > 0) {
+                const float prob = (float)need / (float)rest;
+                const float u = (float)((uint32_t)(next() >> 32) >> 8) * (1.0f / 16777216.0f);
+                if (u < prob) {
+                    code[i] = 2;
+                    ++small;
+                }
+            }
+        }
+        return big + small;
+    }
 
   private:
     uint64_t s_[4];
@@ -501,10 +540,11 @@ class Trainer {
         // every round, the validation metric (the training metric without a
         // validation set; NaN with Metric::None) against the best so far;
         // stop once `patience` rounds passed without improvement and keep the
-        // trees up to the best round. All the engine's metrics are
-        // lower-is-better.
+        // trees up to the best round. The margin accuracy is the one
+        // higher-is-better metric (metrics/mod.rs:288-303).
         const uint32_t patience = (uint32_t)cfg_.early_stopping_rounds;
         const int metric = resolve_metric(cfg_.metric, cfg_.objective);
+        const bool higher = metric == BST_METRIC_MARGIN_ACCURACY;
         if (metric != BST_METRIC_NONE && val) setup_validation(*val);
         bool have_best = false;
         double best = 0.0;
@@ -516,7 +556,7 @@ class Trainer {
             m_.rounds_run = r + 1;
             double value = std::numeric_limits<double>::quiet_NaN();
             if (metric != BST_METRIC_NONE) value = val ? validation_value(metric, before) : train_value(metric);
-            const bool improved = !have_best || value < best;
+            const bool improved = !have_best || (higher ? value > best : value < best);
             if (improved) {
                 have_best = true;
                 best = value;
@@ -544,13 +584,30 @@ class Trainer {
         for (uint32_t round = 0; round < k; ++round) {
             timer_.begin(PH_GRAD);
             BST_CK(cudaMemsetAsync(maxabs_.p, 0, sizeof(unsigned) * 2 * G_, st_));
-            launch_gradients(obj, G_, pred_.p, y_.p, w_.p, n_, gh_.p, maxabs_.p, st_);
+            launch_gradients(obj, G_, pred_.p, y_.p, w_.p, n_, gh_.p, maxabs_.p, st_, alpha_.p, cfg_.huber_delta);
             if (rowsample_) {  // row.rs: per output, zero the rows outside the sample
                 for (uint32_t o = 0; o < G_; ++o) {
-                    n_sampled_[o] = (uint32_t)row_sampler_->sample(n_, cfg_.subsample, h_rowmask_);
-                    BST_CK(cudaMemcpyAsync(d_rowmask_.p + (size_t)o * n_, h_rowmask_.data(), n_, cudaMemcpyHostToDevice,
-                                           st_));  // pageable: staged before the call returns
-                    launch_zero_unsampled(gh_.p + (size_t)o * n_, d_rowmask_.p + (size_t)o * n_, n_, st_);
+                    uint8_t* dm = d_rowmask_.p + (size_t)o * n_;
+                    float2* go = gh_.p + (size_t)o * n_;
+                    if (!goss_) {
+                        n_sampled_[o] = (uint32_t)row_sampler_->sample(n_, cfg_.subsample, h_rowmask_);
+                        BST_CK(cudaMemcpyAsync(dm, h_rowmask_.data(), n_, cudaMemcpyHostToDevice,
+                                               st_));  // pageable: staged before the call returns
+                        launch_zero_unsampled(go, dm, n_, st_);
+                    } else if (round_no_ < goss_warmup_) {  // GOSS starts at round floor(1 / learning_rate)
+                        n_sampled_[o] = (uint32_t)n_;
+                        BST_CK(cudaMemsetAsync(dm, 1, n_, st_));
+                    } else {
+                        h_gh_.resize(2 * (size_t)n_);
+                        BST_CK(cudaMemcpyAsync(h_gh_.data(), go, sizeof(float2) * n_, cudaMemcpyDeviceToHost, st_));
+                        BST_CK(cudaStreamSynchronize(st_));
+                        float mult = 1.0f;
+                        n_sampled_[o] = (uint32_t)row_sampler_->goss(h_gh_.data(), n_, cfg_.goss_top_rate,
+                                                                     cfg_.goss_other_rate, h_rowmask_, &mult);
+                        d_goss_code_.alloc(n_);
+                        BST_CK(cudaMemcpyAsync(d_goss_code_.p, h_rowmask_.data(), n_, cudaMemcpyHostToDevice, st_));
+                        launch_goss_apply(go, d_goss_code_.p, mult, dm, n_, st_);
+                    }
                 }
                 BST_CK(cudaMemsetAsync(maxabs_.p, 0, sizeof(unsigned) * 2 * G_, st_));
                 for (uint32_t o = 0; o < G_; ++o) launch_maxabs(gh_.p + (size_t)o * n_, n_, maxabs_.p + 2 * o, st_);
@@ -633,11 +690,14 @@ class Trainer {
         if (cnt == 0) return 0.0;
         eval_tmp_.alloc(cnt);
         BST_CK(cudaMemcpyAsync(eval_tmp_.p, margins, sizeof(float) * cnt, cudaMemcpyDeviceToDevice, st_));
-        if (metric != BST_METRIC_RMSE) launch_transform(transform_of(cfg_.objective), eval_tmp_.p, G_, n, st_);
+        // every metric but the margin accuracy reads transformed predictions
+        // (eval.rs:151, metrics/mod.rs:272-286)
+        if (metric != BST_METRIC_MARGIN_ACCURACY)
+            launch_transform(transform_of(cfg_.objective), eval_tmp_.p, G_, n, st_);
         eval_host_.resize(cnt);
         BST_CK(cudaMemcpyAsync(eval_host_.data(), eval_tmp_.p, sizeof(float) * cnt, cudaMemcpyDeviceToHost, st_));
         BST_CK(cudaStreamSynchronize(st_));
-        return metric_value(metric, eval_host_.data(), G_, n, y, w);
+        return metric_value(metric, eval_host_.data(), G_, n, y, w, metric_params(cfg_));
     }
 
     double train_value(int metric) {
@@ -686,6 +746,99 @@ class Trainer {
     // row sampling: per-output masks of the round's sampled rows and their counts
     bool rowsample_ = false;
     std::unique_ptr<RowSampler> row_sampler_;
+    DevArray<float> alpha_;  // pinball: [G] alphas
+    // GOSS row sampling: the sampler's row codes and the grad/hess read back
+    bool goss_ = false;
+    uint64_t goss_warmup_ = 0;
+    DevArray<uint8_t> d_goss_code_;
+    std::vector<float> h_gh_;
+    // leaf renewing (L1 / pinball losses)
+    bool renew_ = false;
+    RenewDev rd_{};
+    DevArray<uint32_t> rd_small_, rd_big_;
+    float quantile_alpha(uint32_t o) const {
+        return cfg_.objective == BST_OBJ_PINBALL ? quantile_alpha_of(cfg_, o) : 0.5f;
+    }
+    void setup_renew() {
+        renew_ = !external_ && (cfg_.objective == BST_OBJ_ABSOLUTE || cfg_.objective == BST_OBJ_PINBALL);
+        if (!renew_) return;
+        const uint32_t cap = max_pnodes_ + 1;
+        rd_small_.alloc((size_t)cap * (3 + 256));
+        rd_.cap = cap;
+        rd_.cnt = rd_small_.p;
+        rd_.prefix = rd_small_.p + cap;
+        rd_.rank = rd_small_.p + 2 * (size_t)cap;
+        rd_.hist = rd_small_.p + 3 * (size_t)cap;
+        if (ds_.has_w) {
+            rd_big_.alloc(4 * (size_t)n_);
+            for (int k = 0; k < 2; ++k) {
+                rd_.key[k] = rd_big_.p + (size_t)k * n_;
+                rd_.row[k] = rd_big_.p + (size_t)(2 + k) * n_;
+            }
+        }
+        if (!d_bleaves_.p) d_bleaves_.alloc((size_t)max_pnodes_ + 1);
+        bd_.leaves = d_bleaves_.p;
+        if (!bd_.state) {  // no columns: no histogram state was set up
+            d_bstate_.alloc(1);
+            bd_.state = d_bstate_.p;
+        }
+        if (!bd_.leaf_map) {
+            const uint64_t max_lc = n_ / B_LEAF_CHUNK + max_pnodes_ + 16;
+            d_leaf_map_.alloc(max_lc);
+            bd_.leaf_map = d_leaf_map_.p;
+            bd_.max_leaf_chunks = (uint32_t)max_lc;
+        }
+        if (!g_wide_) g_wide_ = sm_count() * 8;
+    }
+    // Host-driven growth: the grown tree's leaves renewed on the device
+    // (values read back into the host tree and the prediction update).
+    void renew_host_leaves(uint32_t o) {
+        std::vector<BLeaf> lv;
+        std::vector<uint32_t> pnodes;
+        std::vector<uint2> lmap;
+        for (uint32_t pnode = 0; pnode < n_pnodes_; ++pnode) {
+            if (leaf_tree_node_[pnode] == 0xFFFFFFFFu) continue;
+            BLeaf lf;
+            lf.begin = pn_[pnode].begin;
+            lf.count = pn_[pnode].count;
+            lf.value = leaf_value_[pnode];
+            lf.tnode = leaf_tree_node_[pnode];
+            lf.chunk_off = (uint32_t)lmap.size();
+            lf.buf = 0;
+            for (uint32_t s = 0; s < lf.count; s += B_LEAF_CHUNK)
+                lmap.push_back(make_uint2((uint32_t)lv.size(), lf.begin + s));
+            lv.push_back(lf);
+            pnodes.push_back(pnode);
+        }
+        if (lv.empty()) return;
+        if (lmap.size() > bd_.max_leaf_chunks) throw Error{BST_ERR_INVALID_ARGUMENT, "leaf chunk map exceeds its buffer"};
+        BState* hs = stage_.take<BState>(1);
+        std::memset(hs, 0, sizeof(BState));
+        hs->n_leaves = (uint32_t)lv.size();
+        hs->leaf_chunks = (uint32_t)lmap.size();
+        BLeaf* hl = stage_.take<BLeaf>(lv.size());
+        std::copy(lv.begin(), lv.end(), hl);
+        uint2* hm = stage_.take<uint2>(std::max<size_t>(1, lmap.size()));
+        std::copy(lmap.begin(), lmap.end(), hm);
+        upload(hs, 1, d_bstate_);
+        upload(hl, lv.size(), d_bleaves_);
+        upload(hm, lmap.size(), d_leaf_map_);
+        BDev d = bd_;
+        d.tree = nullptr;
+        d.rmask = rowmask(o);
+        timer_.begin(PH_LEAF);
+        launch_leaf_renew(d, rd_, ridx_.p, ridx_.p, y_.p, pred_.p + (size_t)o * n_, ds_.has_w ? w_.p : nullptr,
+                          quantile_alpha(o), cfg_.learning_rate, g_wide_, st_);
+        timer_.end();
+        m_.counters.launches += ds_.has_w ? 1 : 12;
+        BST_CK(cudaMemcpyAsync(hl, d_bleaves_.p, sizeof(BLeaf) * lv.size(), cudaMemcpyDeviceToHost, st_));
+        BST_CK(cudaStreamSynchronize(st_));
+        for (size_t j = 0; j < lv.size(); ++j) {
+            tree_.leaf[hl[j].tnode] = hl[j].value;
+            leaf_value_[pnodes[j]] = hl[j].value;
+        }
+        stage_.reset();
+    }
     DevArray<uint8_t> d_rowmask_;
     std::vector<uint8_t> h_rowmask_;
     std::vector<uint32_t> n_sampled_;
@@ -810,6 +963,12 @@ class Trainer {
         }
         // targets: first output row (targets.output(0) in every objective)
         BST_CK(cudaMemcpyAsync(y_.p, ds_.y.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st_));
+        if (cfg_.objective == BST_OBJ_PINBALL) {  // one alpha per output
+            std::vector<float> a(G_);
+            for (uint32_t o = 0; o < G_; ++o) a[o] = quantile_alpha_of(cfg_, o);
+            alpha_.alloc(G_);
+            BST_CK(cudaMemcpy(alpha_.p, a.data(), sizeof(float) * G_, cudaMemcpyHostToDevice));
+        }
         if (ds_.has_w) BST_CK(cudaMemcpyAsync(w_.p, ds_.w.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st_));
         std::vector<float> init((size_t)G_ * n);
         for (uint32_t g = 0; g < G_; ++g) std::fill(init.begin() + (size_t)g * n, init.begin() + (size_t)(g + 1) * n, m_.base[g]);
@@ -861,7 +1020,10 @@ class Trainer {
         stage_.reserve(max_chunks * 48 + (size_t)(max_pnodes_ + 4) * 256 + (1 << 20));
         if (n_cols_) setup_hist_state();
         n_sampled_.assign(G_, (uint32_t)n_);
-        rowsample_ = std::fabs(cfg_.subsample - 1.0f) >= 1e-6f;  // config.rs:329-330
+        goss_ = !external_ && cfg_.goss_top_rate > 0.0f;
+        goss_warmup_ = (uint64_t)(1.0f / cfg_.learning_rate);  // row.rs:112-116
+        if (goss_ && n_ < 2) throw Error{BST_ERR_CONFIG, "GOSS needs at least 2 rows"};
+        rowsample_ = std::fabs(cfg_.subsample - 1.0f) >= 1e-6f || goss_;  // config.rs:329-330
         if (rowsample_) {
             row_sampler_ = std::make_unique<RowSampler>(cfg_.seed);
             d_rowmask_.alloc((size_t)G_ * n_);
@@ -886,6 +1048,7 @@ class Trainer {
             BST_CK(cudaGetLastError());
             fm_ = BinsFM{fm8_.p, fm16_.p, n_};
         }
+        setup_renew();
     }
 
     // ---- device-side level loop, one CUDA graph per output (kernels.h) -------
@@ -1064,19 +1227,23 @@ class Trainer {
             m_.tune_info = shape_.str() + " (built-in)";
             return;
         }
-        // the built-in shape first, then items per block x histogram kernel
-        // variant (the TMA form when the row records have tensor maps), then
-        // a half-size level-kernel grid
+        // the built-in shape first; the other segment size for the cp.async
+        // form, the register and TMA forms (the latter when the row records
+        // have tensor maps) at the built-in segment size; then a half-size
+        // level-kernel grid
         tune_cands_.push_back(shape_);
-        for (uint32_t hist = 0; hist < (uint32_t)lane_variants(); ++hist)
-            if (hist != 3 || maps_.ok)
-                for (uint32_t items : {1u, 2u}) {
-                    TuneShape c;
-                    c.items = items;
-                    c.hist = hist;
-                    c.grid = 8;
-                    if (!(c == shape_)) tune_cands_.push_back(c);
-                }
+        auto cand = [&](uint32_t items, uint32_t hist) {
+            TuneShape c;
+            c.items = items;
+            c.hist = hist;
+            c.grid = 8;
+            if (hist < (uint32_t)lane_variants() && (hist != 3 || maps_.ok) && !(c == shape_))
+                tune_cands_.push_back(c);
+        };
+        cand(1, 0);
+        cand(2, 1);
+        cand(2, 2);
+        cand(2, 3);
         TuneShape half = shape_;
         half.grid = 4;
         tune_cands_.push_back(half);
@@ -1253,6 +1420,11 @@ class Trainer {
             // leaves solved from the exact sums of the f32 gradients (+ values)
             launch_b_leaf_sums(bd_, R[0], R[1], exact_ref(o), lp, scales_.p + 4 * (size_t)o, g_wide, st_);
             launches += 1;
+        }
+        if (renew_) {
+            launch_leaf_renew(bd_, rd_, R[0], R[1], y_.p, pred, ds_.has_w ? w_.p : nullptr, quantile_alpha(o),
+                              cfg_.learning_rate, g_wide, st_);
+            launches += ds_.has_w ? 1 : 12;
         }
         launch_b_leaf_update(bd_, R[0], R[1], pred, cfg_.record_leaves ? row_leaf_.p : nullptr, g_wide, st_);
         tm.end();
@@ -1905,6 +2077,8 @@ class Trainer {
     DevArray<LwSpec> d_lw_spec_;
     DevArray<uint2> d_lw_pn_;
     DevArray<NodeSplit> d_lw_child_;
+    DevArray<unsigned long long> d_lw_keys_;
+    DevArray<uint32_t> d_lw_ranks_;
     LwDev lw_{};
     LwState* h_lw_state_ = nullptr;  // pinned
     BState* h_lw_bstate_ = nullptr;  // pinned
@@ -1920,6 +2094,10 @@ class Trainer {
         d_lw_spec_.alloc(mp);
         d_lw_pn_.alloc(mp);
         d_lw_child_.alloc(2 * (size_t)mp + 2);
+        d_lw_keys_.alloc(d_lw_heap_.n);
+        d_lw_ranks_.alloc(2 * d_lw_heap_.n);
+        lw_.keys = d_lw_keys_.p;
+        lw_.ranks = d_lw_ranks_.p;
         lw_.st = d_lw_state_.p;
         lw_.heap = d_lw_heap_.p;
         lw_.spec = d_lw_spec_.p;
@@ -2085,6 +2263,11 @@ class Trainer {
         launch_lw_leaves(bd_, st_);
         if (qmode_ != GRAD_F32)
             launch_b_leaf_sums(bd_, ridx_.p, ridx_.p, exact_ref(o), lp, scales_.p + 4 * (size_t)o, g_wide_, st_);
+        if (renew_) {
+            launch_leaf_renew(bd_, rd_, ridx_.p, ridx_.p, y_.p, pred, ds_.has_w ? w_.p : nullptr, quantile_alpha(o),
+                              cfg_.learning_rate, g_wide_, st_);
+            m_.counters.launches += ds_.has_w ? 1 : 12;
+        }
         launch_b_leaf_update(bd_, ridx_.p, ridx_.p, pred, cfg_.record_leaves ? row_leaf_.p : nullptr, g_wide_, st_);
         timer_.end();
         m_.counters.launches += qmode_ != GRAD_F32 ? 3 : 2;
@@ -2194,6 +2377,7 @@ class Trainer {
             grow_leafwise(root, min_gain);
         }
         if (qmode_ != GRAD_F32) exact_leaves(o);
+        if (renew_) renew_host_leaves(o);
         freeze_categories();
 
         // prediction update from the partition (grower.rs:208-219)
@@ -2224,13 +2408,49 @@ class Trainer {
 };
 
 // Objective::compute_base_score (objectives/mod.rs:278-298).
+// compute_weighted_quantile (regression.rs:307-333): (value, weight) pairs
+// sorted stably by value; the first value whose f32 running weight reaches
+// alpha x the f32 total of the sorted weights.
+static float weighted_quantile_base(const float* y, const float* w, uint64_t n, float alpha) {
+    if (n == 0) return 0.0f;
+    std::vector<std::pair<float, float>> v(n);
+    for (uint64_t i = 0; i < n; ++i) v[i] = {y[i], w ? w[i] : 1.0f};
+    std::stable_sort(v.begin(), v.end(), [](const std::pair<float, float>& a, const std::pair<float, float>& b) {
+        return a.first < b.first;
+    });
+    float total = 0.0f;
+    for (const auto& e : v) total += e.second;
+    const float target = alpha * total;
+    float cum = 0.0f;
+    for (const auto& e : v) {
+        cum += e.second;
+        if (cum >= target) return e.first;
+    }
+    return v.back().first;
+}
+
 void base_scores(const HostDataset& ds, const bst_config& cfg, uint32_t G, std::vector<float>& out) {
     const uint64_t n = ds.n;
     const float* y = ds.y.data();
     out.assign(G, 0.0f);
     if (n == 0) return;
     auto wv = [&](uint64_t i) { return ds.has_w ? (double)ds.w[i] : 1.0; };
-    if (cfg.objective == BST_OBJ_SQUARED) {  // regression.rs:45-69
+    const float* w = ds.has_w ? ds.w.data() : nullptr;
+    if (cfg.objective == BST_OBJ_ABSOLUTE || cfg.objective == BST_OBJ_PSEUDO_HUBER) {  // regression.rs:106-118, 217-228
+        out[0] = weighted_quantile_base(y, w, n, 0.5f);
+    } else if (cfg.objective == BST_OBJ_PINBALL) {  // regression.rs:157-173
+        for (uint32_t g = 0; g < G; ++g) out[g] = weighted_quantile_base(y, w, n, quantile_alpha_of(cfg, g));
+    } else if (cfg.objective == BST_OBJ_HINGE) {  // classification.rs:119-125
+        out[0] = 0.0f;
+    } else if (cfg.objective == BST_OBJ_POISSON) {  // regression.rs:273-298
+        double sw = 0, swy = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            sw = sw + wv(i);
+            swy = swy + wv(i) * (double)y[i];
+        }
+        const double mean = sw > 0.0 ? std::fmax(swy / sw, 1e-7) : 1.0;
+        out[0] = to_f32(std::log(mean));
+    } else if (cfg.objective == BST_OBJ_SQUARED) {  // regression.rs:45-69
         double sw = 0, swy = 0;
         for (uint64_t i = 0; i < n; ++i) {
             sw = sw + wv(i);
@@ -2272,6 +2492,16 @@ struct StreamGuard {
 };
 
 }  // namespace
+
+uint32_t n_outputs_of(const bst_config& c) {
+    if (c.objective == BST_OBJ_SOFTMAX) return c.n_classes;
+    if (c.objective == BST_OBJ_PINBALL) return c.n_quantiles;
+    return 1;
+}
+
+float quantile_alpha_of(const bst_config& c, uint32_t o) {
+    return c.quantile_alpha && o < c.n_quantiles ? c.quantile_alpha[o] : 0.5f;
+}
 
 int transform_of(int objective) {
     return objective == BST_OBJ_LOGISTIC ? 1 : (objective == BST_OBJ_SOFTMAX ? 2 : 0);
@@ -2379,7 +2609,7 @@ std::unique_ptr<Model> train_model(const HostDataset& ds, const bst_config& cfg,
     auto model = std::make_unique<Model>();
     model->device = cfg.device;
     model->objective = cfg.objective;
-    model->n_groups = cfg.objective == BST_OBJ_SOFTMAX ? cfg.n_classes : 1;
+    model->n_groups = n_outputs_of(cfg);
     model->n_features = (uint32_t)ds.F;
     DeviceBinned binned;
     make_binned(ds, cfg, sg.s, binned);
@@ -2398,7 +2628,8 @@ struct Booster::Impl {
     std::unique_ptr<Model> model;
     std::unique_ptr<Trainer> tr;
     bst_config cfg;
-    std::string tune_cache;  // owned copy: the caller's string may not outlive the call
+    std::string tune_cache;  // owned copies: the caller's arrays may not outlive the call
+    std::vector<float> alphas;
     uint32_t done = 0;
 };
 
@@ -2409,11 +2640,13 @@ Booster::Booster(const HostDataset& ds, const bst_config& cfg, uint32_t n_thread
     b.cfg = cfg;
     if (cfg.autotune_cache) b.tune_cache = cfg.autotune_cache;
     b.cfg.autotune_cache = cfg.autotune_cache ? b.tune_cache.c_str() : nullptr;
+    if (cfg.quantile_alpha && cfg.n_quantiles) b.alphas.assign(cfg.quantile_alpha, cfg.quantile_alpha + cfg.n_quantiles);
+    b.cfg.quantile_alpha = b.alphas.empty() ? nullptr : b.alphas.data();
     b.model = std::make_unique<Model>();
     Model& m = *b.model;
     m.device = cfg.device;
     m.objective = cfg.objective;
-    m.n_groups = cfg.objective == BST_OBJ_SOFTMAX ? cfg.n_classes : 1;
+    m.n_groups = n_outputs_of(cfg);
     m.n_features = (uint32_t)ds.F;
     make_binned(ds, cfg, b.sg.s, b.binned);
     m.timings[PH_BIN] = b.binned.binning_ms;
@@ -2746,11 +2979,77 @@ void predict_device(const Model& m, const float* x, uint64_t n, uint64_t F, bool
 // probability metrics): RMSE (metrics/regression.rs:17-45), log loss
 // (metrics/classification.rs:13-40), multiclass log loss
 // (classification.rs:332-360); f64 sums in row order.
-double metric_value(int metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w) {
+double metric_value(int metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w,
+                    const MetricParams& mp) {
     if (n == 0) return 0.0;
     const double EPS = 1e-15;
     auto wv = [&](uint64_t i) { return w ? (double)w[i] : 1.0; };
     auto clampd = [](double v, double lo, double hi) { return v < lo ? lo : (v > hi ? hi : v); };
+    if (metric == BST_METRIC_MAE) {  // metrics/regression.rs:55-87
+        double sum = 0.0;
+        for (uint32_t g = 0; g < G; ++g) {
+            double sa = 0, sw = 0;
+            for (uint64_t i = 0; i < n; ++i) {
+                sa = sa + wv(i) * std::fabs((double)p[(uint64_t)g * n + i] - (double)y[i]);
+                sw = sw + wv(i);
+            }
+            sum += sw > 0.0 ? sa / sw : 0.0;
+        }
+        return sum / (double)G;
+    }
+    if (metric == BST_METRIC_MAPE) {  // metrics/regression.rs:89-124
+        double sa = 0, sw = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const double pp = (double)p[i], l = (double)y[i];
+            sa = sa + wv(i) * (std::fabs(pp - l) / std::fmax(std::fabs(l), EPS));
+            sw = sw + wv(i);
+        }
+        return sw > 0.0 ? (sa / sw) * 100.0 : 0.0;
+    }
+    if (metric == BST_METRIC_QUANTILE) {  // metrics/regression.rs:126-174
+        double tl = 0, tw = 0;
+        for (uint32_t q = 0; q < G; ++q) {
+            const double a = (double)(mp.alpha && q < mp.n_alpha ? mp.alpha[q] : 0.5f);
+            double l = 0, sw = 0;
+            for (uint64_t i = 0; i < n; ++i) {
+                const double r = (double)y[i] - (double)p[(uint64_t)q * n + i];
+                l = l + wv(i) * (r >= 0.0 ? a * r : (1.0 - a) * (-r));
+                sw = sw + wv(i);
+            }
+            tl = tl + l;
+            tw = tw + sw;
+        }
+        return tw > 0.0 ? tl / tw : 0.0;
+    }
+    if (metric == BST_METRIC_HUBER) {  // metrics/regression.rs:216-245
+        const double delta = (double)mp.delta;
+        double sl = 0, sw = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const double r = std::fabs((double)p[i] - (double)y[i]);
+            sl = sl + wv(i) * (r <= delta ? 0.5 * r * r : delta * (r - 0.5 * delta));
+            sw = sw + wv(i);
+        }
+        return sw > 0.0 ? sl / sw : 0.0;
+    }
+    if (metric == BST_METRIC_POISSON) {  // metrics/regression.rs:176-210
+        const double E = 1e-9;
+        double sd = 0, sw = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const double yy = (double)y[i], mu = std::fmax((double)p[i], E);
+            sd = sd + wv(i) * (yy > E ? 2.0 * (yy * std::log(yy / mu) - (yy - mu)) : 2.0 * mu);
+            sw = sw + wv(i);
+        }
+        return sw > 0.0 ? sd / sw : 0.0;
+    }
+    if (metric == BST_METRIC_MARGIN_ACCURACY) {  // metrics/classification.rs:85-118, threshold 0
+        double sc = 0, sw = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const float pc = p[i] >= 0.0f ? 1.0f : 0.0f;
+            sc = sc + wv(i) * (std::fabs(pc - y[i]) < 0.5f ? 1.0 : 0.0);
+            sw = sw + wv(i);
+        }
+        return sw > 0.0 ? sc / sw : 0.0;
+    }
     if (metric == BST_METRIC_RMSE) {
         double sum = 0.0;
         for (uint32_t g = 0; g < G; ++g) {
@@ -2793,6 +3092,8 @@ int resolve_metric(int metric, int objective) {
     if (metric != BST_METRIC_DEFAULT) return metric;
     if (objective == BST_OBJ_LOGISTIC) return BST_METRIC_LOGLOSS;
     if (objective == BST_OBJ_SOFTMAX) return BST_METRIC_MLOGLOSS;
+    if (objective == BST_OBJ_PINBALL) return BST_METRIC_QUANTILE;
+    if (objective == BST_OBJ_HINGE) return BST_METRIC_MARGIN_ACCURACY;
     return BST_METRIC_RMSE;
 }
 

@@ -184,8 +184,25 @@ void predict_device(const Model& m, const float* x_dev_sm, uint64_t n, uint64_t 
                     float* out_dev, cudaStream_t st);
 int transform_of(int objective);
 // Metric value of [G][n] predictions (probabilities for the log losses).
-double metric_value(int metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w);
+// Parameters of the quantile and Huber metrics.
+struct MetricParams {
+    const float* alpha = nullptr;
+    uint32_t n_alpha = 0;
+    float delta = 1.0f;
+};
+inline MetricParams metric_params(const bst_config& c) {
+    MetricParams m;
+    m.alpha = c.quantile_alpha;
+    m.n_alpha = c.n_quantiles;
+    m.delta = c.huber_delta;
+    return m;
+}
+double metric_value(int metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w,
+                    const MetricParams& mp = MetricParams());
 int resolve_metric(int metric, int objective);
+// Outputs (trees per round) of an objective: classes, quantiles, or one.
+uint32_t n_outputs_of(const bst_config& c);
+float quantile_alpha_of(const bst_config& c, uint32_t o);
 // Model files (persist.cpp): .bstr.json text and .bstr bytes (uncompressed
 // MessagePack); model_from_bytes reads either (binary by its magic).
 std::string model_to_json(const Model& m, bool pretty);

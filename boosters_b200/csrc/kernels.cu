@@ -177,7 +177,8 @@ __device__ __forceinline__ unsigned warp_max_u32(unsigned b) {
 // global atomic per warp on the same two words serialises in L2.
 __global__ void k_gradients(int objective, uint32_t G, const float* __restrict__ pred,
                             const float* __restrict__ y, const float* __restrict__ w, uint64_t n,
-                            float2* __restrict__ gh, unsigned* __restrict__ maxabs) {
+                            float2* __restrict__ gh, unsigned* __restrict__ maxabs,
+                            const float* __restrict__ alpha, float delta) {
     extern __shared__ unsigned smax[];  // [2G]
     const float HESS_MIN = 1e-6f;
     for (uint32_t i = threadIdx.x; i < 2 * G; i += blockDim.x) smax[i] = 0u;
@@ -208,6 +209,44 @@ __global__ void k_gradients(int objective, uint32_t G, const float* __restrict__
                 m0 = max(m0, abs_bits(g));
                 m1 = max(m1, abs_bits(h));
             }
+        } else if (objective >= 3) {
+            // absolute (regression.rs:80-104), pinball (:129-155, one output
+            // per alpha), pseudo-Huber (:183-215), Poisson (:243-271), hinge
+            // (classification.rs:88-117); targets are output 0's
+            const float inv_delta_sq = 1.0f / (delta * delta);
+            for (uint32_t o = 0; o < G; ++o) {
+                const float p = ok ? pred[(uint64_t)o * n + i] : 0.0f;
+                float g, h;
+                if (objective == 3) {
+                    const float d = p - yi;
+                    g = wi * (isnan(d) ? d : copysignf(1.0f, d));  // f32::signum
+                    h = wi;
+                } else if (objective == 4) {
+                    const float a = alpha[o];
+                    g = wi * ((p - yi) < 0.0f ? -a : 1.0f - a);
+                    h = wi;
+                } else if (objective == 5) {
+                    const float r = p - yi, r_sq = r * r;
+                    const float factor = 1.0f + r_sq * inv_delta_sq, sq = sqrtf(factor);
+                    g = wi * r / sq;
+                    h = wi / (factor * sq);
+                } else if (objective == 6) {
+                    const float pc = p < -30.0f ? -30.0f : (p > 30.0f ? 30.0f : p);
+                    const float e = exp_f32(pc);
+                    g = wi * (e - yi);
+                    h = fmaxf(wi * e, HESS_MIN);
+                } else {  // labels {0, 1} as {-1, +1}
+                    const float yy = yi > 0.5f ? 1.0f : -1.0f, margin = yy * p;
+                    g = margin < 1.0f ? -wi * yy : 0.0f;
+                    h = wi;
+                }
+                if (ok) gh[(uint64_t)o * n + i] = make_float2(g, h);
+                const unsigned bg = warp_max_u32(ok ? abs_bits(g) : 0u), bh = warp_max_u32(ok ? abs_bits(h) : 0u);
+                if ((threadIdx.x & 31) == 0) {
+                    if (bg) atomicMax(&smax[2 * o], bg);
+                    if (bh) atomicMax(&smax[2 * o + 1], bh);
+                }
+            }
         } else {  // softmax
             uint64_t label = 0;
             if (ok && yi > 0.0f) label = (uint64_t)yi;  // `f32 as usize`
@@ -230,7 +269,7 @@ __global__ void k_gradients(int objective, uint32_t G, const float* __restrict__
             }
         }
     }
-    if (objective != 2) {
+    if (objective == 0 || objective == 1) {
         m0 = warp_max_u32(m0);
         m1 = warp_max_u32(m1);
         if ((threadIdx.x & 31) == 0) {
@@ -273,11 +312,12 @@ void launch_maxabs(const float2* gh, uint64_t n, unsigned* maxabs, cudaStream_t 
 
 void launch_gradients(int objective, uint32_t G, const float* pred, const float* y,
                       const float* w, uint64_t n, float2* gh, unsigned* maxabs,
-                      cudaStream_t st) {
+                      cudaStream_t st, const float* alpha, float delta) {
     if (n == 0) return;
     uint64_t blocks = (n + 255) / 256;
     if (blocks > (uint64_t)sm_count() * 8) blocks = (uint64_t)sm_count() * 8;
-    k_gradients<<<(unsigned)blocks, 256, 2 * G * sizeof(unsigned), st>>>(objective, G, pred, y, w, n, gh, maxabs);
+    k_gradients<<<(unsigned)blocks, 256, 2 * G * sizeof(unsigned), st>>>(objective, G, pred, y, w, n, gh, maxabs,
+                                                                          alpha, delta);
 }
 
 __global__ void k_fixed_scales(const unsigned* __restrict__ maxabs, uint32_t G, uint64_t n,
@@ -2891,30 +2931,93 @@ void launch_lw_init(const BDev& d, const LwDev& w, uint32_t n, uint32_t root_cou
     k_lw_init<<<1, 32, 0, st>>>(d, w, n, root_count);
 }
 
-// One warp. Absorbs the last step's expansions (children counts from the
-// partition cursors, splits from the scan) into the speculation table, then
-// pops (grower.rs:265-342) until a popped leaf needs an expansion that has
-// not run: that leaf and the best other unexpanded candidates become the
-// next step's batch (level state written, BState::n_exp = its size). When
-// the budget or the heap runs out, every remaining candidate becomes a leaf
-// (an expanded one over its whole range again) and the tree is done.
-__global__ void __launch_bounds__(32) k_lw_replay(BDev d, LwDev w, LeafParams lp, const double* __restrict__ scale) {
-    const uint32_t lane = threadIdx.x & 31u;
-    LwState S = *w.st;
+// Absorbs the last step's expansions (children counts from the partition
+// cursors, splits from the scan) into the speculation table, then pops
+// (grower.rs:265-342) until a popped leaf needs an expansion that has not
+// run: that leaf and the best other unexpanded candidates become the next
+// step's batch (level state written, BState::n_exp = its size). When the
+// budget or the heap runs out, every remaining candidate becomes a leaf (an
+// expanded one over its whole range again) and the tree is done.
+// The block stages the heap and the speculation table in shared memory
+// (CACHED; both stay in global memory otherwise); warp 0 replays the pops,
+// the whole block ranks the batch candidates and writes the batch, and the
+// block writes heap and table back.
+constexpr uint32_t LW_REPLAY_THREADS = 512;
+constexpr size_t LW_REPLAY_SMEM_MAX = 200 * 1024;
+
+// Block copy of n records, eight 16-byte loads in flight per thread.
+template <typename T>
+__device__ __forceinline__ void lw_copy(T* dst, const T* src, uint32_t n) {
+    static_assert(sizeof(T) % 16 == 0, "16-byte records");
+    constexpr uint32_t U = 8;
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    const uint32_t words = n * (uint32_t)(sizeof(T) / 16);
+    for (uint32_t b = threadIdx.x; b < words; b += blockDim.x * U) {
+        uint4 r[U];
+#pragma unroll
+        for (uint32_t u = 0; u < U; ++u) {
+            const uint32_t i = b + u * blockDim.x;
+            if (i < words) r[u] = s[i];
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < U; ++u) {
+            const uint32_t i = b + u * blockDim.x;
+            if (i < words) d[i] = r[u];
+        }
+    }
+}
+
+// Pop-order key of an expandable candidate: a pops before b iff key(a) >
+// key(b) (larger gain, then higher id; gains are never NaN, -0 counts as 0).
+__device__ __forceinline__ unsigned long long lw_key(float g, uint32_t vid) {
+    if (g == 0.0f) g = 0.0f;
+    uint32_t u = __float_as_uint(g);
+    u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return ((unsigned long long)u << 32) | vid;
+}
+
+template <bool CACHED>
+__global__ void __launch_bounds__(LW_REPLAY_THREADS) k_lw_replay(BDev d, LwDev w, LeafParams lp,
+                                                                 const double* __restrict__ scale) {
+    extern __shared__ __align__(16) unsigned char lw_smem[];
+    __shared__ LwState sS;
+    __shared__ uint32_t s_mode, s_e, s_bmax, s_np, s_nt, s_k, s_chunk_base;
+    __shared__ uint32_t sh[33];
     BState& B = *d.state;
-    auto no_step = [&]() {
-        if (lane == 0) {
+    LwState S = *w.st;
+    if (S.done) {
+        if (threadIdx.x == 0) {
             B.n_exp = 0;
             B.part_chunks = 0;
             B.hist_chunks = 0;
         }
-    };
-    if (S.done) {
-        no_step();
         return;
     }
+    LwCand* heap = w.heap;
+    LwSpec* spec = w.spec;
+    unsigned long long* keys = w.keys;
+    uint32_t* ranks = w.ranks;  // [heap_cap] ranks, then [heap_cap] members
+    if (CACHED) {
+        unsigned char* p = lw_smem;
+        heap = reinterpret_cast<LwCand*>(p);
+        p += (size_t)w.heap_cap * sizeof(LwCand);
+        spec = reinterpret_cast<LwSpec*>(p);
+        p += (size_t)w.max_pnodes * sizeof(LwSpec);
+        keys = reinterpret_cast<unsigned long long*>(p);
+        p += (size_t)w.heap_cap * sizeof(unsigned long long);
+        ranks = reinterpret_cast<uint32_t*>(p);
+    }
+    uint32_t* members = ranks + w.heap_cap;  // ranks: then the members' first partition chunks
+    const uint32_t np0 = B.n_pnodes;
+    if (CACHED) {  // partition nodes >= np0 hold no expansion yet
+        lw_copy(heap, w.heap, S.n_heap);
+        lw_copy(spec, w.spec, np0);
+        for (uint32_t q = np0 + threadIdx.x; q < w.max_pnodes; q += blockDim.x) spec[q].valid = 0;
+        __syncthreads();
+    }
     // 1. the last step's children
-    for (uint32_t j = lane; j < S.n_batch; j += 32) {
+    for (uint32_t j = threadIdx.x; j < S.n_batch; j += blockDim.x) {
         const BExp e = d.exp[j];
         const uint32_t P = e.left_pnode, R = e.right_pnode;
         const uint2 pr = w.pn[P];
@@ -2934,175 +3037,233 @@ __global__ void __launch_bounds__(32) k_lw_replay(BDev d, LwDev w, LeafParams lp
             k.vid = 0;
             k.pad[0] = k.pad[1] = k.pad[2] = 0;
         }
-        w.spec[P] = sp;
+        spec[P] = sp;
         w.pn[P] = make_uint2(pr.x, lc);
         w.pn[R] = make_uint2(pr.x + lc, rc);
     }
     S.n_batch = 0;
-    __syncwarp();
-    // 2. pops
-    for (;;) {
-        if (S.n_leaves >= w.max_leaves || S.n_heap == 0) break;
-        const uint32_t i = lw_argmax(w.heap, S.n_heap, [](uint32_t) { return true; });
-        const LwCand e = w.heap[i];
-        const bool ex = lw_expands(e.split, w.min_gain);
-        if (ex && !w.spec[e.pnode].valid) {
-            // the next step: e and the best unexpanded candidates, at most as
-            // many as pops remain (rem after e's pop) and as free slots allow
-            const uint32_t rem = w.max_leaves - (S.n_leaves + 1);
-            const int64_t room = (int64_t)w.max_pnodes - (int64_t)B.n_pnodes - (int64_t)rem;
-            if (room < 1) {
+    __syncthreads();
+    // 2. pops (warp 0); s_mode: 0 done, 1 batch needed, 2 out of slots
+    if (threadIdx.x < 32) {
+        const uint32_t lane = threadIdx.x;
+        uint32_t n_pnodes = np0, n_tnodes = B.n_tnodes;
+        uint32_t mode = 0;
+        for (;;) {
+            if (S.n_leaves >= w.max_leaves || S.n_heap == 0) break;
+            const uint32_t i = lw_argmax(heap, S.n_heap, [](uint32_t) { return true; });
+            const LwCand e = heap[i];
+            const bool ex = lw_expands(e.split, w.min_gain);
+            if (ex && !spec[e.pnode].valid) {
+                // the next step: e and the best unexpanded candidates, at most
+                // as many as pops remain (rem after e's pop) and as free slots
+                // allow
+                const uint32_t rem = w.max_leaves - (S.n_leaves + 1);
+                const int64_t room = (int64_t)w.max_pnodes - (int64_t)n_pnodes - (int64_t)rem;
+                const int64_t want = (int64_t)rem + 1;
+                mode = room < 1 ? 2u : 1u;
                 if (lane == 0) {
-                    S.err = 1;
-                    S.done = 1;
-                    *w.st = S;
+                    s_e = i;
+                    s_bmax = room < 1 ? 0u : (uint32_t)(want < room ? want : room);
                 }
-                no_step();
-                return;
+                break;
             }
-            const int64_t want = (int64_t)rem + 1;
-            const uint32_t batch_max = (uint32_t)(want < room ? want : room);
-            // mark e, then take the best marked-free candidates one by one;
-            // the marks live in the pad word of the heap entries
-            if (lane == 0) w.heap[i].pad[0] = 1;
+            // pop e
+            if (lane == 0) heap[i] = heap[S.n_heap - 1];
+            S.n_heap -= 1;
+            S.n_leaves += 1;
             __syncwarp();
-            uint32_t k = 0;
-            uint32_t first_right = B.n_pnodes;
-            uint32_t chunks = 0;
-            for (uint32_t sel = i; sel != 0xFFFFFFFFu && k < batch_max;) {
-                const LwCand c = w.heap[sel];
-                const uint32_t j = k++;
-                const NodeSplit& sp = c.split;
+            if (!ex) {
+                if (lane == 0) lw_make_leaf(d, w, e, scale, lp, S.n_leaf_out);
+                S.n_leaf_out += 1;
+                __syncwarp();
+                continue;
+            }
+            // apply_split (grower.rs:576-650): children tree nodes in
+            // allocation order; a categorical split sends the training-left
+            // rows to the stored right child
+            const LwSpec sp = spec[e.pnode];
+            const uint32_t l = n_tnodes, r = n_tnodes + 1;
+            const bool cat = (e.split.flags & 2u) != 0u;
+            if (lane == 0) {
+                spec[e.pnode].valid = 0;
+                BTreeNode t;
+                t.col = e.split.col;
+                t.bin = e.split.bin;
+                t.flags = (e.split.flags & 1u) | (cat ? 2u : 0u);
+                t.left = l;
+                t.right = r;
+                t.gain = e.split.gain;
+                t.leaf = 0.0f;
+                t.G = (double)e.split.tot_g * scale[2];
+                t.H = (double)e.split.tot_h * scale[3];
+                for (int q = 0; q < 4; ++q) t.cats[q] = e.split.cats[q];
+                d.tree[e.tnode] = t;
+                LwCand k0 = sp.kids[0], k1 = sp.kids[1];
+                k0.tnode = cat ? r : l;
+                k1.tnode = cat ? l : r;
+                k0.vid = e.vid;
+                k1.vid = S.n_vid;
+                heap[S.n_heap] = k0;
+                heap[S.n_heap + 1] = k1;
+            }
+            n_tnodes = r + 1;
+            S.n_vid += 1;
+            S.n_heap += 2;
+            __syncwarp();
+        }
+        if (mode == 0) {
+            // 3. done: every candidate left becomes a leaf, an expanded one
+            // over its whole range (its right partition node keeps no rows)
+            for (uint32_t q = 0; q < S.n_heap; ++q) {
+                const LwCand c = heap[q];
+                if (lane == 0) {
+                    const LwSpec sp = spec[c.pnode];
+                    if (sp.valid) {
+                        w.pn[c.pnode] = make_uint2(sp.begin, sp.count);
+                        w.pn[sp.right_pnode] = make_uint2(sp.begin + sp.count, 0u);
+                        spec[c.pnode].valid = 0;
+                    }
+                    lw_make_leaf(d, w, c, scale, lp, S.n_leaf_out);
+                }
+                S.n_leaf_out += 1;
+                __syncwarp();
+            }
+            S.n_heap = 0;
+            S.done = 1;
+        } else if (mode == 2) {
+            S.err = 1;
+            S.done = 1;
+        }
+        if (lane == 0) {
+            s_mode = mode;
+            s_np = n_pnodes;
+            s_nt = n_tnodes;
+            sS = S;
+        }
+    }
+    __syncthreads();
+    const uint32_t mode = s_mode;
+    if (mode == 1) {
+        // 4. the batch: e first, then the expandable unexpanded candidates
+        // in pop order (rank = how many of them pop earlier), at most bmax
+        const uint32_t nh = sS.n_heap, ei = s_e, bmax = s_bmax, first_right = s_np;
+        for (uint32_t q = threadIdx.x; q < nh; q += blockDim.x) {
+            const LwCand& c = heap[q];
+            const bool el = q != ei && lw_expands(c.split, w.min_gain) && !spec[c.pnode].valid;
+            keys[q] = el ? lw_key(c.split.gain, c.vid) : 0ull;
+        }
+        if (threadIdx.x == 0) members[0] = ei;
+        __syncthreads();
+        uint32_t n_el = 0;
+        for (uint32_t q = threadIdx.x; q < nh; q += blockDim.x) {
+            const unsigned long long kq = keys[q];
+            if (!kq) continue;
+            uint32_t r = 0;
+            for (uint32_t t = 0; t < nh; ++t) r += keys[t] > kq ? 1u : 0u;
+            if (r + 1 < bmax) members[r + 1] = q;
+            ++n_el;
+        }
+        uint32_t tot_el;
+        block_excl_scan(n_el, sh, &tot_el);  // (synchronises: members complete)
+        const uint32_t k = 1u + min(tot_el, bmax - 1u);
+        if (threadIdx.x == 0) s_chunk_base = 0;
+        __syncthreads();
+        for (uint32_t j0 = 0; j0 < k; j0 += blockDim.x) {
+            const uint32_t j = j0 + threadIdx.x;
+            const bool valid = j < k;
+            const LwCand* c = valid ? &heap[members[j]] : nullptr;
+            const uint2 r = valid ? w.pn[c->pnode] : make_uint2(0u, 0u);
+            const uint32_t nch = (r.y + B_PART_CHUNK - 1) / B_PART_CHUNK;
+            uint32_t tc;
+            const uint32_t off = s_chunk_base + block_excl_scan(nch, sh, &tc);
+            if (valid) {
+                const NodeSplit& sp = c->split;
                 const bool cat = (sp.flags & 2u) != 0u;
                 const BColumn bc = d.bcols[sp.col];
-                const uint2 r = w.pn[c.pnode];
-                const uint32_t nch = (r.y + B_PART_CHUNK - 1) / B_PART_CHUNK;
-                if (lane == 0) {
-                    BExp x;
-                    x.front = 0;
-                    x.right_pnode = first_right + j;
-                    x.tl = x.tr = 0;
-                    x.lc = x.rc = x.small_begin = x.small_count = 0;
-                    x.part_off = chunks;
-                    x.hist_off = 0;
-                    x.left_pnode = c.pnode;
-                    x.pad1 = c.depth + 1;  // the children's depth (column masks)
-                    d.exp[j] = x;
-                    PartWork pw;
-                    pw.begin = r.x;
-                    pw.count = r.y;
-                    pw.matrix = bc.matrix;
-                    pw.pos = bc.pos;
-                    pw.thr_bin = sp.bin;
-                    pw.flags = (sp.flags & 1u) | (bc.has_missing ? 2u : 0u) | (cat ? 4u : 0u);
-                    pw.default_bin = bc.default_bin;
-                    pw.pad = 0;
-                    for (int q = 0; q < 4; ++q) pw.cats[q] = sp.cats[q];
-                    d.pworks[j] = pw;
-                    d.cursors[2 * j] = r.x;
-                    d.cursors[2 * j + 1] = r.x + r.y;
-                    if (d.rmask) d.scnt[2 * j] = d.scnt[2 * j + 1] = 0u;
-                }
-                for (uint32_t q = lane; q < nch; q += 32)
-                    if (chunks + q < d.max_part_chunks)
-                        d.part_map[chunks + q] = make_uint2(j, r.x + q * B_PART_CHUNK);
-                chunks += nch;
-                __syncwarp();
-                if (k >= batch_max) break;
-                sel = lw_argmax(w.heap, S.n_heap, [&](uint32_t q) {
-                    return w.heap[q].pad[0] == 0 && lw_expands(w.heap[q].split, w.min_gain) &&
-                           !w.spec[w.heap[q].pnode].valid;
-                });
-                if (sel != 0xFFFFFFFFu && lane == 0) w.heap[sel].pad[0] = 1;
-                __syncwarp();
+                BExp x;
+                x.front = 0;
+                x.right_pnode = first_right + j;
+                x.tl = x.tr = 0;
+                x.lc = x.rc = x.small_begin = x.small_count = 0;
+                x.part_off = off;
+                x.hist_off = 0;
+                x.left_pnode = c->pnode;
+                x.pad1 = c->depth + 1;  // the children's depth (column masks)
+                d.exp[j] = x;
+                PartWork pw;
+                pw.begin = r.x;
+                pw.count = r.y;
+                pw.matrix = bc.matrix;
+                pw.pos = bc.pos;
+                pw.thr_bin = sp.bin;
+                pw.flags = (sp.flags & 1u) | (bc.has_missing ? 2u : 0u) | (cat ? 4u : 0u);
+                pw.default_bin = bc.default_bin;
+                pw.pad = 0;
+                for (int q = 0; q < 4; ++q) pw.cats[q] = sp.cats[q];
+                d.pworks[j] = pw;
+                d.cursors[2 * j] = r.x;
+                d.cursors[2 * j + 1] = r.x + r.y;
+                if (d.rmask) d.scnt[2 * j] = d.scnt[2 * j + 1] = 0u;
+                ranks[j] = off;  // the member's first partition chunk
             }
-            for (uint32_t q = lane; q < S.n_heap; q += 32) w.heap[q].pad[0] = 0;  // clear the marks
-            if (lane == 0) {
-                S.n_batch = k;
-                *w.st = S;
-                B.n_exp = k;
-                B.first_right = first_right;
-                B.n_pnodes = first_right + k;
-                B.part_chunks = min(chunks, d.max_part_chunks);
-                B.hist_chunks = 0;
+            __syncthreads();
+            if (threadIdx.x == 0) s_chunk_base += tc;
+            __syncthreads();
+        }
+        // the chunk map, all threads: chunk c belongs to the last member whose
+        // first chunk is <= c
+        const uint32_t total = min(s_chunk_base, d.max_part_chunks);
+        for (uint32_t c = threadIdx.x; c < total; c += blockDim.x) {
+            uint32_t lo = 0, hi = k;  // ranks[lo] <= c < ranks[hi]
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (ranks[mid] <= c)
+                    lo = mid;
+                else
+                    hi = mid;
             }
-            return;
+            d.part_map[c] = make_uint2(lo, w.pn[heap[members[lo]].pnode].x + (c - ranks[lo]) * B_PART_CHUNK);
         }
-        // pop e
-        if (lane == 0) {
-            w.heap[i] = w.heap[S.n_heap - 1];
+        if (threadIdx.x == 0) {
+            sS.n_batch = k;
+            s_np = first_right + k;
+            B.n_exp = k;
+            B.first_right = first_right;
+            B.part_chunks = min(s_chunk_base, d.max_part_chunks);
+            B.hist_chunks = 0;
         }
-        S.n_heap -= 1;
-        S.n_leaves += 1;
-        __syncwarp();
-        if (!ex) {
-            if (lane == 0) lw_make_leaf(d, w, e, scale, lp, S.n_leaf_out);
-            S.n_leaf_out += 1;
-            __syncwarp();
-            continue;
-        }
-        // apply_split (grower.rs:576-650): children tree nodes in allocation
-        // order; a categorical split sends the training-left rows to the
-        // stored right child
-        const LwSpec sp = w.spec[e.pnode];
-        const uint32_t l = B.n_tnodes, r = B.n_tnodes + 1;
-        const bool cat = (e.split.flags & 2u) != 0u;
-        if (lane == 0) {
-            w.spec[e.pnode].valid = 0;
-            BTreeNode t;
-            t.col = e.split.col;
-            t.bin = e.split.bin;
-            t.flags = (e.split.flags & 1u) | (cat ? 2u : 0u);
-            t.left = l;
-            t.right = r;
-            t.gain = e.split.gain;
-            t.leaf = 0.0f;
-            t.G = (double)e.split.tot_g * scale[2];
-            t.H = (double)e.split.tot_h * scale[3];
-            for (int q = 0; q < 4; ++q) t.cats[q] = e.split.cats[q];
-            d.tree[e.tnode] = t;
-            LwCand k0 = sp.kids[0], k1 = sp.kids[1];
-            k0.tnode = cat ? r : l;
-            k1.tnode = cat ? l : r;
-            k0.vid = e.vid;
-            k1.vid = S.n_vid;
-            w.heap[S.n_heap] = k0;
-            w.heap[S.n_heap + 1] = k1;
-            B.n_tnodes = r + 1;
-        }
-        S.n_vid += 1;
-        S.n_heap += 2;
-        __syncwarp();
+        __syncthreads();
     }
-    // 3. done: every candidate left becomes a leaf, an expanded one over its
-    // whole range (its right partition node keeps no rows)
-    for (uint32_t q = 0; q < S.n_heap; ++q) {
-        const LwCand c = w.heap[q];
-        if (lane == 0) {
-            const LwSpec sp = w.spec[c.pnode];
-            if (sp.valid) {
-                w.pn[c.pnode] = make_uint2(sp.begin, sp.count);
-                w.pn[sp.right_pnode] = make_uint2(sp.begin + sp.count, 0u);
-                w.spec[c.pnode].valid = 0;
-            }
-            lw_make_leaf(d, w, c, scale, lp, S.n_leaf_out);
+    if (threadIdx.x == 0) {
+        if (mode != 1) {
+            if (mode == 0) B.n_leaves = sS.n_leaf_out;
+            B.n_exp = 0;
+            B.part_chunks = 0;
+            B.hist_chunks = 0;
         }
-        S.n_leaf_out += 1;
-        __syncwarp();
+        B.n_pnodes = s_np;
+        B.n_tnodes = s_nt;
+        *w.st = sS;
     }
-    if (lane == 0) {
-        S.n_heap = 0;
-        S.done = 1;
-        *w.st = S;
-        B.n_leaves = S.n_leaf_out;
-        B.n_exp = 0;
-        B.part_chunks = 0;
-        B.hist_chunks = 0;
+    if (CACHED && mode == 1) {  // the state the next step starts from
+        lw_copy(w.heap, heap, sS.n_heap);
+        lw_copy(w.spec, spec, s_np);
     }
 }
 
+static size_t lw_replay_smem(const LwDev& w) {
+    return (size_t)w.heap_cap * (sizeof(LwCand) + sizeof(unsigned long long) + 2 * sizeof(uint32_t)) +
+           (size_t)w.max_pnodes * sizeof(LwSpec);
+}
+
 void launch_lw_replay(const BDev& d, const LwDev& w, LeafParams lp, const double* scale, cudaStream_t st) {
-    k_lw_replay<<<1, 32, 0, st>>>(d, w, lp, scale);
+    const size_t smem = lw_replay_smem(w);
+    if (smem <= LW_REPLAY_SMEM_MAX) {  // 255 leaves: 160 KB
+        init_kernel_attributes();
+        k_lw_replay<true><<<1, LW_REPLAY_THREADS, smem, st>>>(d, w, lp, scale);
+    } else {
+        k_lw_replay<false><<<1, LW_REPLAY_THREADS, 0, st>>>(d, w, lp, scale);
+    }
 }
 
 // Partition of the pending batch over its chunk map, rin -> rout (no
@@ -3582,6 +3743,304 @@ void launch_b_leaf_update(const BDev& d, const uint32_t* r0, const uint32_t* r1,
 }
 
 // ============================================================================
+// Leaf renewing for the L1 and pinball losses (objectives/mod.rs:352-409)
+// ============================================================================
+
+namespace {
+
+constexpr uint32_t RENEW_NONE = 0xFFFFFFFFu;
+
+// Orderable key of a residual: unsigned order = value order; -0 counts as 0.
+__device__ __forceinline__ uint32_t renew_key(float r) {
+    if (r == 0.0f) r = 0.0f;
+    const uint32_t u = __float_as_uint(r);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float renew_value(uint32_t k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+}
+
+__device__ __forceinline__ bool renew_sampled(const uint8_t* rmask, uint32_t row) { return !rmask || rmask[row]; }
+
+__device__ __forceinline__ void renew_set(const BDev& d, uint32_t l, float v) {
+    d.leaves[l].value = v;
+    if (d.tree) d.tree[d.leaves[l].tnode].leaf = v;
+}
+
+}  // namespace
+
+__global__ void k_renew_start(BDev d, RenewDev r) {
+    const uint32_t nl = min(d.state->n_leaves, r.cap);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (uint64_t)nl * 256u;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        r.hist[i] = 0u;
+        if (i < nl) r.cnt[i] = 0u;
+    }
+}
+
+// Sampled rows per leaf: one block per leaf chunk, one atomic per block.
+__global__ void k_renew_count(BDev d, RenewDev r, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1) {
+    __shared__ uint32_t s_cnt;
+    const uint32_t total = d.state->leaf_chunks;
+    for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+        const uint2 m = d.leaf_map[c];
+        if (m.x >= r.cap) continue;  // block-uniform
+        const BLeaf lf = d.leaves[m.x];
+        const uint32_t len = min(B_LEAF_CHUNK, lf.begin + lf.count - m.y);
+        const uint32_t* ridx = lf.buf ? r1 : r0;
+        if (threadIdx.x == 0) s_cnt = 0;
+        __syncthreads();
+        uint32_t k = 0;
+        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) k += renew_sampled(d.rmask, ridx[m.y + i]) ? 1u : 0u;
+        for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(FULL, k, o);
+        if ((threadIdx.x & 31) == 0 && k) atomicAdd(&s_cnt, k);
+        __syncthreads();
+        if (threadIdx.x == 0 && s_cnt) atomicAdd(&r.cnt[m.x], s_cnt);
+        __syncthreads();
+    }
+}
+
+// The rank to find: ceil(alpha m) - 1 clamped to [0, m - 1] (f32 product,
+// utils.rs:42-44); none for an empty leaf.
+__global__ void k_renew_rank(BDev d, RenewDev r, float alpha) {
+    const uint32_t nl = min(d.state->n_leaves, r.cap);
+    for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nl; l += gridDim.x * blockDim.x) {
+        const uint32_t m = r.cnt[l];
+        uint32_t k = RENEW_NONE;
+        if (m > 0) {
+            const float c = ceilf(alpha * (float)m);
+            uint64_t kk = c > 0.0f ? (uint64_t)c : 0u;
+            kk = kk > 0 ? kk - 1 : 0;
+            k = (uint32_t)(kk < m - 1 ? kk : m - 1);
+        }
+        r.rank[l] = k;
+        r.prefix[l] = 0u;
+    }
+}
+
+// One radix-select pass: counts of the key byte at `shift` among the
+// sampled rows whose higher bytes match the prefix.
+__global__ void k_renew_hist(BDev d, RenewDev r, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1,
+                             const float* __restrict__ y, const float* __restrict__ pred, uint32_t shift) {
+    __shared__ uint32_t sh[256];
+    const uint32_t total = d.state->leaf_chunks;
+    const uint32_t hi_mask = shift >= 24 ? 0u : (0xFFFFFFFFu << (shift + 8));
+    for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+        const uint2 m = d.leaf_map[c];
+        if (m.x >= r.cap || r.rank[m.x] == RENEW_NONE) continue;  // block-uniform
+        const BLeaf lf = d.leaves[m.x];
+        const uint32_t len = min(B_LEAF_CHUNK, lf.begin + lf.count - m.y);
+        const uint32_t* ridx = lf.buf ? r1 : r0;
+        const uint32_t want = r.prefix[m.x] & hi_mask;
+        for (uint32_t b = threadIdx.x; b < 256; b += blockDim.x) sh[b] = 0u;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
+            const uint32_t row = ridx[m.y + i];
+            if (!renew_sampled(d.rmask, row)) continue;
+            const uint32_t k = renew_key(y[row] - pred[row]);
+            if ((k & hi_mask) == want) atomicAdd(&sh[(k >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        uint32_t* h = r.hist + (size_t)m.x * 256u;
+        for (uint32_t b = threadIdx.x; b < 256; b += blockDim.x)
+            if (sh[b]) atomicAdd(&h[b], sh[b]);
+        __syncthreads();
+    }
+}
+
+// The byte of the wanted rank (one warp per leaf; lane j owns bytes 8j ..
+// 8j + 7), then the counts cleared for the next pass.
+__global__ void k_renew_pick(BDev d, RenewDev r, uint32_t shift) {
+    const uint32_t nl = min(d.state->n_leaves, r.cap);
+    const uint32_t lane = threadIdx.x & 31u, wpb = blockDim.x >> 5;
+    for (uint32_t l = blockIdx.x * wpb + (threadIdx.x >> 5); l < nl; l += gridDim.x * wpb) {
+        const uint32_t k = r.rank[l];
+        if (k == RENEW_NONE) continue;  // warp-uniform
+        uint32_t* h = r.hist + (size_t)l * 256u;
+        uint32_t c[8], sum = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            c[q] = h[lane * 8 + q];
+            sum += c[q];
+        }
+        uint32_t incl = sum;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(FULL, incl, o);
+            if (lane >= (uint32_t)o) incl += t;
+        }
+        const uint32_t excl = incl - sum;
+        // the lane whose bytes hold rank k: excl <= k < incl
+        const unsigned owner = __ballot_sync(FULL, excl <= k && k < incl);
+        if (owner) {
+            const uint32_t src = (uint32_t)(__ffs(owner) - 1);
+            if (lane == src) {
+                uint32_t before = excl, b = 0;
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (before + c[q] <= k) {
+                        before += c[q];
+                        b = (uint32_t)q + 1u;
+                    } else {
+                        break;
+                    }
+                r.prefix[l] |= ((lane * 8u + b) & 255u) << shift;
+                r.rank[l] = k - before;
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < 8; ++q) h[lane * 8 + q] = 0u;
+    }
+}
+
+__global__ void k_renew_apply(BDev d, RenewDev r, float lr) {
+    const uint32_t nl = min(d.state->n_leaves, r.cap);
+    for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nl; l += gridDim.x * blockDim.x)
+        if (r.rank[l] != RENEW_NONE) renew_set(d, l, renew_value(r.prefix[l]) * lr);
+}
+
+// Weighted form: one block per leaf. The leaf's sampled rows are compacted
+// in partition order into key[0] / row[0] at the leaf's own positions
+// (first = its first row position in the concatenation of the leaf
+// ranges), their weights summed in that order, the keys sorted stably by
+// 32 one-bit passes (key[0] <-> key[1]), and the running weight scanned.
+constexpr uint32_t RENEW_W_THREADS = 1024;
+
+__global__ void __launch_bounds__(RENEW_W_THREADS)
+k_renew_weighted(BDev d, RenewDev r, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1,
+                 const float* __restrict__ y, const float* __restrict__ pred, const float* __restrict__ w, float alpha,
+                 float lr) {
+    __shared__ uint32_t sh[33];
+    __shared__ float s_w[RENEW_W_THREADS];
+    __shared__ uint32_t s_base, s_zero, s_hit;
+    __shared__ float s_acc;
+    const uint32_t nl = min(d.state->n_leaves, r.cap);
+    for (uint32_t l = blockIdx.x; l < nl; l += gridDim.x) {
+        const BLeaf lf = d.leaves[l];
+        const uint32_t* ridx = lf.buf ? r1 : r0;
+        const uint32_t first = lf.begin;  // the leaf's own range in the scratch arrays
+        // 1. compaction (stable) of the sampled rows
+        if (threadIdx.x == 0) s_base = 0;
+        __syncthreads();
+        for (uint32_t t0 = 0; t0 < lf.count; t0 += blockDim.x) {
+            const uint32_t i = t0 + threadIdx.x;
+            const uint32_t row = i < lf.count ? ridx[first + i] : 0u;
+            const bool keep = i < lf.count && renew_sampled(d.rmask, row);
+            uint32_t tot;
+            const uint32_t off = s_base + block_excl_scan(keep ? 1u : 0u, sh, &tot);
+            if (keep) {
+                r.key[0][first + off] = renew_key(y[row] - pred[row]);
+                r.row[0][first + off] = row;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) s_base += tot;
+            __syncthreads();
+        }
+        const uint32_t m = s_base;
+        __syncthreads();
+        if (m == 0) continue;  // block-uniform
+        // 2. the f32 total of the weights in partition order
+        if (threadIdx.x == 0) s_acc = 0.0f;
+        for (uint32_t t0 = 0; t0 < m; t0 += blockDim.x) {
+            const uint32_t i = t0 + threadIdx.x;
+            __syncthreads();
+            s_w[threadIdx.x] = i < m ? w[r.row[0][first + i]] : 0.0f;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                float acc = s_acc;
+                const uint32_t e = min(m - t0, (uint32_t)blockDim.x);
+                for (uint32_t q = 0; q < e; ++q) acc += s_w[q];
+                s_acc = acc;
+            }
+        }
+        __syncthreads();
+        const float threshold = s_acc * alpha;
+        // 3. stable sort by key: zeros of bit b first, each side in order
+        uint32_t src = 0;
+        for (uint32_t b = 0; b < 32; ++b) {
+            const uint32_t* ks = r.key[src] + first;
+            const uint32_t* rs = r.row[src] + first;
+            uint32_t* kd = r.key[src ^ 1u] + first;
+            uint32_t* rd = r.row[src ^ 1u] + first;
+            if (threadIdx.x == 0) s_zero = 0;
+            __syncthreads();
+            uint32_t z = 0;
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) z += ((ks[i] >> b) & 1u) ? 0u : 1u;
+            for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(FULL, z, o);
+            if ((threadIdx.x & 31) == 0 && z) atomicAdd(&s_zero, z);
+            if (threadIdx.x == 0) s_base = 0;
+            __syncthreads();
+            const uint32_t zeros = s_zero;
+            for (uint32_t t0 = 0; t0 < m; t0 += blockDim.x) {
+                const uint32_t i = t0 + threadIdx.x;
+                const bool valid = i < m;
+                const uint32_t k = valid ? ks[i] : 0u;
+                const bool zero = valid && !((k >> b) & 1u);
+                uint32_t tz;
+                const uint32_t rz = block_excl_scan(zero ? 1u : 0u, sh, &tz);
+                const uint32_t base = s_base;
+                if (valid) {
+                    // ones before this one in the tile: i - t0 - rz
+                    const uint32_t dst = zero ? base + rz : zeros + (t0 - base) + (i - t0 - rz);
+                    kd[dst] = k;
+                    rd[dst] = rs[i];
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) s_base += tz;
+                __syncthreads();
+            }
+            src ^= 1u;
+        }
+        // 4. the first sorted row whose running weight reaches the threshold
+        if (threadIdx.x == 0) {
+            s_acc = 0.0f;
+            s_hit = RENEW_NONE;
+        }
+        for (uint32_t t0 = 0; t0 < m; t0 += blockDim.x) {
+            const uint32_t i = t0 + threadIdx.x;
+            __syncthreads();
+            if (s_hit != RENEW_NONE) break;  // block-uniform
+            s_w[threadIdx.x] = i < m ? w[r.row[src][first + i]] : 0.0f;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                float acc = s_acc;
+                const uint32_t e = min(m - t0, (uint32_t)blockDim.x);
+                for (uint32_t q = 0; q < e; ++q) {
+                    acc += s_w[q];
+                    if (acc >= threshold) {
+                        s_hit = t0 + q;
+                        break;
+                    }
+                }
+                s_acc = acc;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const uint32_t j = s_hit != RENEW_NONE ? s_hit : m - 1;
+            renew_set(d, l, renew_value(r.key[src][first + j]) * lr);
+        }
+        __syncthreads();
+    }
+}
+
+void launch_leaf_renew(const BDev& d, const RenewDev& r, const uint32_t* r0, const uint32_t* r1, const float* y,
+                       const float* pred, const float* w, float alpha, float lr, uint32_t grid, cudaStream_t st) {
+    if (w) {
+        k_renew_weighted<<<grid, RENEW_W_THREADS, 0, st>>>(d, r, r0, r1, y, pred, w, alpha, lr);
+        return;
+    }
+    k_renew_start<<<grid, 256, 0, st>>>(d, r);
+    k_renew_count<<<grid, 256, 0, st>>>(d, r, r0, r1);
+    k_renew_rank<<<grid, 256, 0, st>>>(d, r, alpha);
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        k_renew_hist<<<grid, 256, 0, st>>>(d, r, r0, r1, y, pred, (uint32_t)shift);
+        k_renew_pick<<<grid, 256, 0, st>>>(d, r, (uint32_t)shift);
+    }
+    k_renew_apply<<<grid, 256, 0, st>>>(d, r, lr);
+}
+
+// ============================================================================
 // K9: forest traversal (tree_view.rs:119-160, predictor.rs:271-302)
 // One thread per row; trees summed in forest order per group in f32.
 // ============================================================================
@@ -4022,6 +4481,28 @@ void launch_zero_unsampled(float2* gh, const uint8_t* mask, uint64_t n, cudaStre
     k_zero_unsampled<<<(unsigned)blocks, 256, 0, st>>>(gh, mask, n);
 }
 
+// GOSS (sampling/row.rs:214-280): code 0 leaves the tree (zero grad/hess),
+// 1 is kept, 2 is kept with grad and hess scaled by `mult`; mask gets 0 / 1.
+__global__ void k_goss_apply(float2* __restrict__ gh, const uint8_t* __restrict__ code, float mult,
+                             uint8_t* __restrict__ mask, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint8_t c = code[i];
+        if (c == 0) {
+            gh[i] = make_float2(0.0f, 0.0f);
+        } else if (c == 2) {
+            const float2 v = gh[i];
+            gh[i] = make_float2(v.x * mult, v.y * mult);
+        }
+        mask[i] = c ? 1 : 0;
+    }
+}
+
+void launch_goss_apply(float2* gh, const uint8_t* code, float mult, uint8_t* mask, uint64_t n, cudaStream_t st) {
+    if (n == 0) return;
+    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 8);
+    k_goss_apply<<<(unsigned)blocks, 256, 0, st>>>(gh, code, mult, mask, n);
+}
+
 __global__ void k_add_f32(float* __restrict__ a, const float* __restrict__ b, uint64_t n) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         a[i] = a[i] + b[i];
@@ -4057,6 +4538,7 @@ void init_kernel_attributes() {
         for (int v = 0; v < LANE_VARIANTS; ++v)
             cudaFuncSetAttribute(lane_kernel_of(m, v), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)lane_smem_bytes(m, v));
+    cudaFuncSetAttribute(k_lw_replay<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LW_REPLAY_SMEM_MAX);
     done.fetch_or(bit);
 }
 

@@ -57,9 +57,10 @@ void launch_bin_assign(const float* x_fm, uint64_t n, const BinColumn* cols, uin
 
 // ---- K3 gradients ---------------------------------------------------------
 // maxabs [G][2] receives the bit patterns of max|grad|, max|hess| (atomicMax).
+// alpha: [G] pinball alphas (device); delta: the pseudo-Huber delta.
 void launch_gradients(int objective, uint32_t G, const float* pred, const float* y,
                       const float* w, uint64_t n, float2* gh, unsigned* maxabs,
-                      cudaStream_t st);
+                      cudaStream_t st, const float* alpha = nullptr, float delta = 1.0f);
 // Fixed-point resolution: every grad/hess becomes round(v * 2^k) with
 // |q| <= 2^HIST_QBITS (and n * 2^k * max < 2^62 for the int64 sums).
 constexpr int HIST_QBITS = 38;
@@ -327,14 +328,39 @@ struct BDev {  // device buffers of the level loop
 constexpr uint32_t B_PART_CHUNK = 2048;
 constexpr uint32_t B_LEAF_CHUNK = 4096;
 
+// ---- leaf renewing (trainer.rs:283-313, objectives/mod.rs:352-409) ----------
+// L1 and pinball losses: after a tree is grown, each leaf's value becomes
+// the alpha-quantile of the residuals y - pred of its (sampled) rows, times
+// the learning rate. Unweighted: the rank ceil(alpha m) - 1 element by value
+// (utils.rs:17-53), found by a 4-pass radix select over orderable residual
+// keys. Weighted: the first value, in value order (ties in partition order),
+// whose f32 running weight reaches alpha x the f32 total of the weights
+// summed in partition order (utils.rs:81-135): one block per leaf compacts,
+// sorts (32 stable 1-bit passes) and scans. The leaves come from d.leaves /
+// d.leaf_map / d.state (n_leaves, leaf_chunks); their values and, when
+// d.tree is set, the device tree's leaf values are overwritten.
+struct RenewDev {
+    uint32_t* cnt;     // [cap] sampled rows per leaf
+    uint32_t* prefix;  // [cap] key prefix found so far
+    uint32_t* rank;    // [cap] rank below the prefix still to find (0xFFFFFFFF: leaf kept)
+    uint32_t* hist;    // [cap][256]
+    uint32_t cap;
+    uint32_t* key[2];  // weighted: [n] ping-pong keys
+    uint32_t* row[2];  // weighted: [n] ping-pong row ids
+};
+void launch_leaf_renew(const BDev& d, const RenewDev& r, const uint32_t* r0, const uint32_t* r1, const float* y,
+                       const float* pred, const float* w, float alpha, float learning_rate, uint32_t grid,
+                       cudaStream_t st);
+
 // ---- device-side leaf-wise growth (expansion.rs:129-213) ---------------------
 // The reference pops the leaf of largest (gain, node id) from a max-heap,
 // splits it and pushes its children until max_leaves. The device replays
-// those pops exactly (k_lw_replay, one warp): when the popped leaf has not
-// been expanded yet it stops and hands the level kernels a batch of the
-// best unexpanded candidates (the popped one first, at most as many as pops
-// remain); their rows, histograms and splits do not depend on when they are
-// expanded (exact sums), so a later pop of a batch member costs no step.
+// those pops exactly (k_lw_replay: one warp pops, the block ranks): when
+// the popped leaf has not been expanded yet it stops and hands the level
+// kernels a batch of the best unexpanded candidates (the popped one first,
+// at most as many as pops remain); their rows, histograms and splits do not
+// depend on when they are expanded (exact sums), so a later pop of a batch
+// member costs no step.
 struct LwCand {          // a leaf that may be split
     NodeSplit split;     // its best split; tot_g / tot_h: the node's exact sums
     uint32_t pnode, tnode, depth, count;  // partition node, tree node, depth, rows
@@ -355,6 +381,8 @@ struct LwDev {
     LwSpec* spec;        // [max_pnodes]
     uint2* pn;           // [max_pnodes] (begin, count) of each partition node
     NodeSplit* child;    // [max_pnodes] split search results of the pending step's children (root: [0])
+    unsigned long long* keys;  // [heap_cap] batch selection scratch (when the heap is not staged in shared memory)
+    uint32_t* ranks;     // [2 * heap_cap] ditto
     uint32_t heap_cap, max_pnodes, max_leaves;
     float min_gain;
 };
@@ -540,5 +568,8 @@ void launch_transform(int transform, float* out, uint32_t G, uint64_t n, cudaStr
 void launch_add_f32(float* a, const float* b, uint64_t n, cudaStream_t st);
 // gh[i] = (0, 0) where mask[i] == 0 (row sampling), i < n
 void launch_zero_unsampled(float2* gh, const uint8_t* mask, uint64_t n, cudaStream_t st);
+// GOSS codes (0 out, 1 kept, 2 kept and scaled by mult) applied to one
+// output's grad/hess; mask [n] receives the kept rows.
+void launch_goss_apply(float2* gh, const uint8_t* code, float mult, uint8_t* mask, uint64_t n, cudaStream_t st);
 
 }  // namespace bst

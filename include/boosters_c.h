@@ -55,12 +55,29 @@ const char* bst_version(void);
 #define BST_OBJ_SQUARED 0  /* training/objectives/regression.rs:20       */
 #define BST_OBJ_LOGISTIC 1 /* training/objectives/classification.rs:24   */
 #define BST_OBJ_SOFTMAX 2  /* training/objectives/classification.rs:141  */
+/* L1 loss: g = w sign(p - y), h = w; base score the weighted median; leaf
+ * values renewed to the median residual of the leaf's rows
+ * (objectives/mod.rs:352-409). */
+#define BST_OBJ_ABSOLUTE 3 /* training/objectives/regression.rs:80       */
+/* Pinball (quantile) loss, one output per alpha in quantile_alpha: g = w
+ * (-alpha if p < y else 1 - alpha), h = w; base scores the weighted
+ * alpha-quantiles; leaf values renewed to the alpha-quantile residual. */
+#define BST_OBJ_PINBALL 4  /* training/objectives/regression.rs:129      */
+#define BST_OBJ_PSEUDO_HUBER 5 /* regression.rs:183 (huber_delta)          */
+#define BST_OBJ_POISSON 6  /* training/objectives/regression.rs:243      */
+#define BST_OBJ_HINGE 7    /* training/objectives/classification.rs:88   */
 
-#define BST_METRIC_DEFAULT -1 /* derived from the objective (training/metrics/mod.rs) */
+#define BST_METRIC_DEFAULT -1 /* derived from the objective (training/metrics/mod.rs:213-232) */
 #define BST_METRIC_NONE 0
 #define BST_METRIC_RMSE 1
 #define BST_METRIC_LOGLOSS 2
 #define BST_METRIC_MLOGLOSS 3
+#define BST_METRIC_MAE 4             /* metrics/regression.rs:55             */
+#define BST_METRIC_MAPE 5            /* metrics/regression.rs:89             */
+#define BST_METRIC_QUANTILE 6        /* metrics/regression.rs:126 (quantile_alpha) */
+#define BST_METRIC_HUBER 7           /* metrics/regression.rs:216 (huber_delta) */
+#define BST_METRIC_POISSON 8         /* metrics/regression.rs:176 deviance   */
+#define BST_METRIC_MARGIN_ACCURACY 9 /* metrics/classification.rs:85         */
 
 #define BST_GROWTH_DEPTHWISE 0 /* training/gbdt/expansion.rs:46 DepthWise */
 #define BST_GROWTH_LEAFWISE 1  /* training/gbdt/expansion.rs:51 LeafWise  */
@@ -140,6 +157,22 @@ typedef struct bst_config {
      * cached choice skips the exploration, a new one is added. */
     int32_t autotune;
     const char* autotune_cache;
+    /* Objective and metric parameters. quantile_alpha: n_quantiles values
+     * in (0, 1) (BST_OBJ_PINBALL: one output each; BST_METRIC_QUANTILE),
+     * copied at training; huber_delta > 0 (BST_OBJ_PSEUDO_HUBER,
+     * BST_METRIC_HUBER), default 1. */
+    const float* quantile_alpha;
+    uint32_t n_quantiles;
+    float huber_delta;
+    /* GOSS row sampling (training/sampling/row.rs:214-280, the trainer's
+     * RowSamplingParams::Goss): goss_top_rate > 0 turns it on (subsample
+     * must then be 1). From round floor(1 / learning_rate) on, per output:
+     * the top_rate share of rows by |grad x hess| are kept, other_rate x n
+     * of the rest are drawn with the reference's adaptive probability
+     * (seeded by `seed`) and their grad/hess scaled by (n - top) / other;
+     * the remaining rows leave the round's tree. Default 0 / 0 (off). */
+    float goss_top_rate;
+    float goss_other_rate;
 } bst_config;
 
 /* Fill *cfg with the reference defaults (GBDTConfig::default(),
@@ -529,9 +562,16 @@ bst_status bst_synth_multiclass(uint64_t n_samples, uint64_t n_numeric, uint64_t
 /* Metrics (training/metrics/regression.rs:17, classification.rs:13,332)    */
 /* ------------------------------------------------------------------------ */
 
-/* preds [n_groups, n_samples] (probabilities for logloss/mlogloss). */
+/* preds [n_groups, n_samples] (probabilities for logloss/mlogloss, raw
+ * margins for the margin accuracy). Metric::compute (metrics/mod.rs:238-270).
+ * BST_METRIC_QUANTILE needs bst_metric_ex. */
 bst_status bst_metric(int32_t metric, const float* preds, uint32_t n_groups, uint64_t n_samples,
                       const float* targets, const float* weights, double* out);
+/* The same with the quantile metric's alphas (one per group) and the Huber
+ * metric's delta. */
+bst_status bst_metric_ex(int32_t metric, const float* preds, uint32_t n_groups, uint64_t n_samples,
+                         const float* targets, const float* weights, const float* quantile_alpha,
+                         uint32_t n_quantiles, float huber_delta, double* out);
 
 #ifdef __cplusplus
 }

@@ -405,10 +405,64 @@ inline float exp_f32(float x) { return (float)std::exp((double)x); }
 
 namespace {
 
-// regression.rs:20-43, classification.rs:19-52, classification.rs:141-187
-void gradients(int obj, uint32_t G, const float* preds, const float* y, const float* w, uint64_t n,
+// Objective parameters: the pinball alphas (one output each) and the
+// pseudo-Huber delta.
+struct ObjP {
+    const float* alpha = nullptr;
+    uint32_t n_alpha = 0;
+    float delta = 1.0f;
+    static ObjP of(const bst_config& c) {
+        ObjP p;
+        p.alpha = c.quantile_alpha;
+        p.n_alpha = c.n_quantiles;
+        p.delta = c.huber_delta;
+        return p;
+    }
+    float alpha_at(uint32_t o) const { return alpha && o < n_alpha ? alpha[o] : 0.5f; }
+};
+
+// f32::signum: +-1 with the sign bit (so +-0 give +-1), NaN for NaN.
+inline float signum_f32(float v) { return std::isnan(v) ? v : std::copysign(1.0f, v); }
+
+// regression.rs:20-43, 80-104, 129-155, 183-215, 243-271; classification.rs:19-52, 88-117, 141-187
+void gradients(int obj, const ObjP& op, uint32_t G, const float* preds, const float* y, const float* w, uint64_t n,
                float* grad, float* hess) {
     const float HESS_MIN = 1e-6f;
+    if (obj == BST_OBJ_ABSOLUTE || obj == BST_OBJ_PINBALL || obj == BST_OBJ_PSEUDO_HUBER || obj == BST_OBJ_POISSON ||
+        obj == BST_OBJ_HINGE) {
+        const float inv_delta_sq = 1.0f / (op.delta * op.delta);
+        for (uint32_t o = 0; o < G; ++o) {
+            const float alpha = op.alpha_at(o);
+            for (uint64_t i = 0; i < n; ++i) {
+                const float wi = w_at(w, i), p = preds[o * n + i], t = y[i];
+                float g, h;
+                if (obj == BST_OBJ_ABSOLUTE) {
+                    g = wi * signum_f32(p - t);
+                    h = wi;
+                } else if (obj == BST_OBJ_PINBALL) {
+                    g = wi * ((p - t) < 0.0f ? -alpha : 1.0f - alpha);
+                    h = wi;
+                } else if (obj == BST_OBJ_PSEUDO_HUBER) {
+                    const float r = p - t, r_sq = r * r;
+                    const float factor = 1.0f + r_sq * inv_delta_sq, sq = std::sqrt(factor);
+                    g = wi * r / sq;
+                    h = wi / (factor * sq);
+                } else if (obj == BST_OBJ_POISSON) {
+                    const float pc = p < -30.0f ? -30.0f : (p > 30.0f ? 30.0f : p);
+                    const float e = exp_f32(pc);
+                    g = wi * (e - t);
+                    h = std::fmax(wi * e, HESS_MIN);
+                } else {  // hinge: labels {0, 1} as {-1, +1}
+                    const float yy = t > 0.5f ? 1.0f : -1.0f, margin = yy * p;
+                    g = margin < 1.0f ? -wi * yy : 0.0f;
+                    h = wi;
+                }
+                grad[o * n + i] = g;
+                hess[o * n + i] = h;
+            }
+        }
+        return;
+    }
     if (obj == BST_OBJ_SQUARED) {
         for (uint32_t o = 0; o < G; ++o)
             for (uint64_t i = 0; i < n; ++i) {
@@ -444,10 +498,89 @@ void gradients(int obj, uint32_t G, const float* preds, const float* y, const fl
 
 inline double clamp64(double v, double lo, double hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// regression.rs:45-69, classification.rs:54-76, classification.rs:189-222
-void base_score(int obj, uint32_t G, const float* y, const float* w, uint64_t n, float* out) {
+// compute_weighted_quantile (regression.rs:307-333): (value, weight) pairs
+// sorted stably by value; the first value whose f32 running weight reaches
+// alpha x the f32 total of the sorted weights.
+float weighted_quantile_base(const float* y, const float* w, uint64_t n, float alpha) {
+    if (n == 0) return 0.0f;
+    std::vector<std::pair<float, float>> v(n);
+    for (uint64_t i = 0; i < n; ++i) v[i] = {y[i], w_at(w, i)};
+    std::stable_sort(v.begin(), v.end(), [](const std::pair<float, float>& a, const std::pair<float, float>& b) {
+        return a.first < b.first;
+    });
+    float total = 0.0f;
+    for (const auto& e : v) total += e.second;
+    const float target = alpha * total;
+    float cum = 0.0f;
+    for (const auto& e : v) {
+        cum += e.second;
+        if (cum >= target) return e.first;
+    }
+    return v.back().first;
+}
+
+// unweighted_quantile_indexed (utils.rs:17-53): the element of rank
+// ceil(alpha n) - 1 (clamped to [0, n - 1]) by value.
+float unweighted_quantile(std::vector<float> v, float alpha) {
+    const size_t n = v.size();
+    if (n == 0) return std::numeric_limits<float>::quiet_NaN();
+    if (n == 1) return v[0];
+    const float c = std::ceil(alpha * (float)n);
+    size_t k = c > 0.0f ? (size_t)c : 0;
+    k = k > 0 ? k - 1 : 0;
+    k = std::min(k, n - 1);
+    std::nth_element(v.begin(), v.begin() + k, v.end());
+    return v[k];
+}
+
+// weighted_quantile_indexed (utils.rs:81-135): values sorted stably, the
+// f32 total of the weights in the given order, the first value whose f32
+// running weight reaches alpha x total.
+float weighted_quantile(const std::vector<float>& v, const std::vector<float>& wt, float alpha) {
+    const size_t n = v.size();
+    if (n == 0) return std::numeric_limits<float>::quiet_NaN();
+    if (n == 1) return v[0];
+    std::vector<uint32_t> ord(n);
+    for (size_t i = 0; i < n; ++i) ord[i] = (uint32_t)i;
+    std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return v[a] < v[b]; });
+    float total = 0.0f;
+    for (size_t i = 0; i < n; ++i) total += wt[i];
+    const float threshold = total * alpha;
+    float cum = 0.0f;
+    for (uint32_t i : ord) {
+        cum += wt[i];
+        if (cum >= threshold) return v[i];
+    }
+    return v[ord[n - 1]];
+}
+
+// regression.rs:45-69, 106-118, 157-173, 217-228, 273-298; classification.rs:54-76, 119-125, 189-222
+void base_score(int obj, const ObjP& op, uint32_t G, const float* y, const float* w, uint64_t n, float* out) {
     if (n == 0) {
         for (uint32_t g = 0; g < G; ++g) out[g] = 0.0f;
+        return;
+    }
+    if (obj == BST_OBJ_ABSOLUTE || obj == BST_OBJ_PSEUDO_HUBER) {
+        out[0] = weighted_quantile_base(y, w, n, 0.5f);
+        return;
+    }
+    if (obj == BST_OBJ_PINBALL) {
+        for (uint32_t g = 0; g < G; ++g) out[g] = weighted_quantile_base(y, w, n, op.alpha_at(g));
+        return;
+    }
+    if (obj == BST_OBJ_HINGE) {
+        out[0] = 0.0f;
+        return;
+    }
+    if (obj == BST_OBJ_POISSON) {
+        double sw = 0, swy = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const double wi = (double)w_at(w, i);
+            sw = sw + wi;
+            swy = swy + wi * (double)y[i];
+        }
+        const double mean = sw > 0.0 ? std::fmax(swy / sw, 1e-7) : 1.0;
+        out[0] = f64_to_f32(std::log(mean));
         return;
     }
     if (obj == BST_OBJ_SQUARED) {
@@ -1066,6 +1199,47 @@ struct OracleRowSampler {
         for (uint32_t r : idx) mask[r] = 1;
         return k;
     }
+    // rng.gen::<f32>() of rand 0.8: the top 24 bits of next_u32 (the upper
+    // half of a Xoshiro256++ output) times 2^-24
+    float gen_f32() {
+        const uint32_t u = (uint32_t)(next() >> 32);
+        return (float)(u >> 8) * (1.0f / 16777216.0f);
+    }
+    // sample_goss (row.rs:214-280) on one output's grad / hess (scaled in
+    // place for the sampled small-gradient rows); mask: 1 kept, 0 left out
+    uint64_t goss(float* g, float* h, uint64_t n, float top_rate, float other_rate, std::vector<uint8_t>& mask) {
+        std::vector<float> mag(n);
+        for (uint64_t i = 0; i < n; ++i) mag[i] = std::fabs(g[i] * h[i]);
+        uint64_t top_k = (uint64_t)((float)n * top_rate);
+        top_k = std::min<uint64_t>(std::max<uint64_t>(top_k, 1), n - 1);
+        uint64_t other_k = std::max<uint64_t>((uint64_t)((float)n * other_rate), 1);
+        std::vector<float> sorted(mag);
+        std::nth_element(sorted.begin(), sorted.begin() + (n - top_k), sorted.end());
+        const float threshold = sorted[n - top_k];
+        const float multiply = (float)(n - top_k) / (float)other_k;
+        uint64_t big = 0, small = 0;
+        mask.assign(n, 0);
+        for (uint64_t i = 0; i < n; ++i) {
+            if (mag[i] >= threshold) {
+                mask[i] = 1;
+                ++big;
+                continue;
+            }
+            const uint64_t need = other_k > small ? other_k - small : 0;
+            const uint64_t top_left = top_k > big ? top_k - big : 0;
+            const uint64_t rest = (n - i) > top_left ? (n - i) - top_left : 0;
+            if (rest > 0) {
+                const float prob = (float)need / (float)rest;
+                if (gen_f32() < prob) {
+                    mask[i] = 1;
+                    ++small;
+                    g[i] *= multiply;
+                    h[i] *= multiply;
+                }
+            }
+        }
+        return big + small;
+    }
 };
 static void cs_sample(std::vector<uint32_t>& v, float rate, ColRng rng) {
     const size_t n = v.size();
@@ -1383,6 +1557,30 @@ struct Grower {
         }
     }
 
+    // Leaf renewing (trainer.rs:283-313, objectives/mod.rs:352-409): each
+    // leaf's value becomes the alpha-quantile of the residuals y - pred of
+    // its (sampled) rows, in partition order, times the learning rate.
+    void renew_leaves(const float* y, const float* w, const float* pred, float alpha) {
+        std::vector<float> v, wt;
+        for (const auto& lm : leaf_map) {
+            const uint32_t b = part.begin[lm.second], c = part.count[lm.second];
+            v.clear();
+            wt.clear();
+            for (uint32_t i = 0; i < c; ++i) {
+                const uint32_t row = part.indices[b + i];
+                if (rmask && !rmask[row]) continue;
+                v.push_back(y[row] - pred[row]);
+                if (w) wt.push_back(w[row]);
+            }
+            if (v.empty()) continue;
+            const float q = w ? weighted_quantile(v, wt, alpha) : unweighted_quantile(v, alpha);
+            if (std::isnan(q)) continue;
+            const float sv = q * tc.learning_rate;
+            tree.leaf[lm.first] = sv;
+            last_leaf[lm.second] = sv;
+        }
+    }
+
     // grower.rs:208-219 update_predictions_from_last_tree
     void update_predictions(float* pred) {
         for (size_t node = 0; node < last_leaf.size(); ++node) {
@@ -1548,9 +1746,80 @@ void predict_impl(const orc_model* m, const float* x, uint64_t n, bool sample_ma
     if (!raw) transform(transform_of(m->objective), out, G, n);
 }
 
-double metric_impl(int metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w) {
+double metric_impl(int metric, const ObjP& op, const float* p, uint32_t G, uint64_t n, const float* y,
+                   const float* w) {
     if (n == 0) return 0.0;
     const double EPS = 1e-15;
+    if (metric == BST_METRIC_MAE) {  // metrics/regression.rs:55-87
+        double sum = 0.0;
+        for (uint32_t g = 0; g < G; ++g) {
+            double sa = 0, sw = 0;
+            for (uint64_t i = 0; i < n; ++i) {
+                const double wi = (double)w_at(w, i);
+                sa = sa + wi * std::fabs((double)p[g * n + i] - (double)y[i]);
+                sw = sw + wi;
+            }
+            sum += sw > 0.0 ? sa / sw : 0.0;
+        }
+        return sum / (double)G;
+    }
+    if (metric == BST_METRIC_MAPE) {  // metrics/regression.rs:89-124
+        double sa = 0, sw = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const double pp = (double)p[i], l = (double)y[i], wi = (double)w_at(w, i);
+            sa = sa + wi * (std::fabs(pp - l) / std::fmax(std::fabs(l), EPS));
+            sw = sw + wi;
+        }
+        return sw > 0.0 ? (sa / sw) * 100.0 : 0.0;
+    }
+    if (metric == BST_METRIC_QUANTILE) {  // metrics/regression.rs:126-174
+        double tl = 0, tw = 0;
+        for (uint32_t q = 0; q < G; ++q) {
+            const double a = (double)op.alpha_at(q);
+            double l = 0, sw = 0;
+            for (uint64_t i = 0; i < n; ++i) {
+                const double r = (double)y[i] - (double)p[q * n + i], wi = (double)w_at(w, i);
+                const double loss = r >= 0.0 ? a * r : (1.0 - a) * (-r);
+                l = l + wi * loss;
+                sw = sw + wi;
+            }
+            tl = tl + l;
+            tw = tw + sw;
+        }
+        return tw > 0.0 ? tl / tw : 0.0;
+    }
+    if (metric == BST_METRIC_HUBER) {  // metrics/regression.rs:216-245
+        const double delta = (double)op.delta;
+        double sl = 0, sw = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const double r = std::fabs((double)p[i] - (double)y[i]), wi = (double)w_at(w, i);
+            const double loss = r <= delta ? 0.5 * r * r : delta * (r - 0.5 * delta);
+            sl = sl + wi * loss;
+            sw = sw + wi;
+        }
+        return sw > 0.0 ? sl / sw : 0.0;
+    }
+    if (metric == BST_METRIC_POISSON) {  // metrics/regression.rs:176-210
+        const double E = 1e-9;
+        double sd = 0, sw = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const double yy = (double)y[i], mu = std::fmax((double)p[i], E), wi = (double)w_at(w, i);
+            const double dev = yy > E ? 2.0 * (yy * std::log(yy / mu) - (yy - mu)) : 2.0 * mu;
+            sd = sd + wi * dev;
+            sw = sw + wi;
+        }
+        return sw > 0.0 ? sd / sw : 0.0;
+    }
+    if (metric == BST_METRIC_MARGIN_ACCURACY) {  // metrics/classification.rs:85-118, threshold 0
+        double sc = 0, sw = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            const float pc = p[i] >= 0.0f ? 1.0f : 0.0f;
+            const double c = std::fabs(pc - y[i]) < 0.5f ? 1.0 : 0.0, wi = (double)w_at(w, i);
+            sc = sc + wi * c;
+            sw = sw + wi;
+        }
+        return sw > 0.0 ? sc / sw : 0.0;
+    }
     if (metric == BST_METRIC_RMSE) {  // metrics/regression.rs:17-45
         double sum = 0.0;
         for (uint32_t g = 0; g < G; ++g) {
@@ -1615,6 +1884,35 @@ int validate_cfg(const bst_config& c) {  // model/gbdt/config.rs:252-310
             g_err = std::string(gn[i]) + " must be non-negative, got " + std::to_string(*regs[i]);
             return BST_ERR_CONFIG;
         }
+    if (c.objective == BST_OBJ_PINBALL) {
+        if (c.n_quantiles == 0 || !c.quantile_alpha) {
+            g_err = "pinball loss needs at least one quantile";
+            return BST_ERR_CONFIG;
+        }
+        for (uint32_t i = 0; i < c.n_quantiles; ++i)
+            if (!(c.quantile_alpha[i] > 0.0f && c.quantile_alpha[i] < 1.0f)) {
+                g_err = "quantile alpha must be in (0, 1)";
+                return BST_ERR_CONFIG;
+            }
+    }
+    if (c.objective == BST_OBJ_PSEUDO_HUBER && !(c.huber_delta > 0.0f)) {
+        g_err = "huber_delta must be positive";
+        return BST_ERR_CONFIG;
+    }
+    if (c.goss_top_rate != 0.0f || c.goss_other_rate != 0.0f) {
+        if (!(c.goss_top_rate > 0.0f) || !(c.goss_other_rate > 0.0f)) {
+            g_err = "GOSS top_rate and other_rate must be positive";
+            return BST_ERR_CONFIG;
+        }
+        if (c.goss_top_rate + c.goss_other_rate > 1.0f) {
+            g_err = "top_rate + other_rate must be <= 1.0";
+            return BST_ERR_CONFIG;
+        }
+        if (std::fabs(c.subsample - 1.0f) >= 1e-6f) {
+            g_err = "GOSS and subsample < 1 cannot be combined";
+            return BST_ERR_CONFIG;
+        }
+    }
     return 0;
 }
 
@@ -1663,6 +1961,7 @@ void orc_config_default(bst_config* c) {
     c->early_stopping_rounds = -1;
     c->cache_size = 8;
     c->seed = 42;
+    c->huber_delta = 1.0f;
 }
 
 int orc_synth_regression(uint64_t n, uint64_t F, uint64_t n_inf, uint64_t seed, uint64_t stream, float* x,
@@ -1781,14 +2080,39 @@ void orc_find_split(const double* hist, const uint32_t* n_bins, const int32_t* i
 
 void orc_gradients(int32_t obj, uint32_t G, const float* preds, const float* y, const float* w,
                    uint64_t n, float* grad, float* hess) {
-    gradients(obj, G, preds, y, w, n, grad, hess);
+    gradients(obj, ObjP(), G, preds, y, w, n, grad, hess);
 }
 void orc_base_score(int32_t obj, uint32_t G, const float* y, const float* w, uint64_t n, float* out) {
-    base_score(obj, G, y, w, n, out);
+    base_score(obj, ObjP(), G, y, w, n, out);
+}
+void orc_gradients_cfg(const bst_config* c, uint32_t G, const float* preds, const float* y, const float* w,
+                       uint64_t n, float* grad, float* hess) {
+    gradients(c->objective, ObjP::of(*c), G, preds, y, w, n, grad, hess);
+}
+void orc_base_score_cfg(const bst_config* c, uint32_t G, const float* y, const float* w, uint64_t n, float* out) {
+    base_score(c->objective, ObjP::of(*c), G, y, w, n, out);
+}
+double orc_metric_cfg(int32_t metric, const bst_config* c, const float* p, uint32_t G, uint64_t n, const float* y,
+                      const float* w) {
+    return metric_impl(metric, ObjP::of(*c), p, G, n, y, w);
+}
+uint64_t orc_goss(float* g, float* h, uint64_t n, float top_rate, float other_rate, uint64_t seed, uint32_t calls,
+                  uint8_t* mask) {
+    OracleRowSampler rs(seed);
+    std::vector<uint8_t> m;
+    uint64_t k = 0;
+    for (uint32_t c = 0; c < calls; ++c) k = rs.goss(g, h, n, top_rate, other_rate, m);
+    std::copy(m.begin(), m.end(), mask);
+    return k;
+}
+float orc_leaf_quantile(const float* v, const float* w, uint64_t n, float alpha) {
+    std::vector<float> vv(v, v + n), ww;
+    if (w) ww.assign(w, w + n);
+    return w ? weighted_quantile(vv, ww, alpha) : unweighted_quantile(vv, alpha);
 }
 void orc_transform(int32_t t, float* p, uint32_t G, uint64_t n) { transform(t, p, G, n); }
 double orc_metric(int32_t metric, const float* p, uint32_t G, uint64_t n, const float* y, const float* w) {
-    return metric_impl(metric, p, G, n, y, w);
+    return metric_impl(metric, ObjP(), p, G, n, y, w);
 }
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
     philox4x32_10(ctr, key, out);
@@ -1817,6 +2141,12 @@ int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, ui
         g_err = "softmax needs n_classes >= 2";
         return BST_ERR_CONFIG;
     }
+    const bool goss_on = cfg.goss_top_rate > 0.0f;
+    if (goss_on && n < 2) {
+        g_err = "GOSS needs at least 2 rows";
+        return BST_ERR_CONFIG;
+    }
+    const ObjP op = ObjP::of(cfg);
     auto t0 = std::chrono::steady_clock::now();
     orc_binned b;
     rc = build_binned(x, F, n, cat_idx, n_cat, cfg, b, omp_threads);
@@ -1824,13 +2154,14 @@ int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, ui
     auto t1 = std::chrono::steady_clock::now();
     orc_model* m = new orc_model();
     m->objective = cfg.objective;
-    m->n_groups = cfg.objective == BST_OBJ_SOFTMAX ? cfg.n_classes : 1;
+    m->n_groups = cfg.objective == BST_OBJ_SOFTMAX ? cfg.n_classes
+                                                   : (cfg.objective == BST_OBJ_PINBALL ? cfg.n_quantiles : 1);
     m->n_features = (uint32_t)F;
     m->binning_seconds = std::chrono::duration<double>(t1 - t0).count();
     uint32_t G = m->n_groups;
     // trainer.rs:162-401
     m->base.resize(G);
-    base_score(cfg.objective, G, y, w, n, m->base.data());
+    base_score(cfg.objective, op, G, y, w, n, m->base.data());
     m->train_pred.resize((size_t)G * n);
     for (uint32_t g = 0; g < G; ++g) std::fill(m->train_pred.begin() + g * n, m->train_pred.begin() + (g + 1) * n, m->base[g]);
     std::vector<float> grad((size_t)G * n), hess((size_t)G * n);
@@ -1852,9 +2183,13 @@ int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, ui
     std::vector<int32_t> qg, qh;
     std::vector<float> fqg, fqh;
     // row sampling (config.rs:329-330: a rate within 1e-6 of 1 samples nothing)
+    // GOSS (row.rs:214-280) from round floor(1 / learning_rate) on
     std::unique_ptr<OracleRowSampler> row_sampler;
     std::vector<uint8_t> row_mask;
-    if (std::fabs(cfg.subsample - 1.0f) >= 1e-6f) row_sampler = std::make_unique<OracleRowSampler>(cfg.seed);
+    const bool uniform_on = std::fabs(cfg.subsample - 1.0f) >= 1e-6f;
+    if (uniform_on || goss_on) row_sampler = std::make_unique<OracleRowSampler>(cfg.seed);
+    const uint64_t goss_warmup = (uint64_t)(1.0f / cfg.learning_rate);
+    const bool renew = cfg.objective == BST_OBJ_ABSOLUTE || cfg.objective == BST_OBJ_PINBALL;
     if (quant) {
         qg.resize(n);
         qh.resize(n);
@@ -1863,10 +2198,17 @@ int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, ui
     }
     for (uint32_t round = 0; round < n_rounds && built < max_trees; ++round) {
         auto tr0 = std::chrono::steady_clock::now();
-        gradients(cfg.objective, G, m->train_pred.data(), y, w, n, grad.data(), hess.data());
+        gradients(cfg.objective, op, G, m->train_pred.data(), y, w, n, grad.data(), hess.data());
         for (uint32_t o = 0; o < G && built < max_trees; ++o) {
-            if (row_sampler) {  // row.rs:141-210: zero the grad/hess of the rows outside the sample
-                gr.n_sampled = (uint32_t)row_sampler->sample(n, cfg.subsample, row_mask);
+            gr.rmask = nullptr;
+            gr.n_sampled = (uint32_t)n;
+            const bool sampled = uniform_on || (goss_on && round >= goss_warmup);
+            if (sampled) {  // row.rs:141-280: rows outside the sample leave the tree (zero grad/hess)
+                if (goss_on)
+                    gr.n_sampled = (uint32_t)row_sampler->goss(grad.data() + (size_t)o * n, hess.data() + (size_t)o * n,
+                                                               n, cfg.goss_top_rate, cfg.goss_other_rate, row_mask);
+                else
+                    gr.n_sampled = (uint32_t)row_sampler->sample(n, cfg.subsample, row_mask);
                 gr.rmask = row_mask.data();
                 for (uint64_t i = 0; i < n; ++i)
                     if (!row_mask[i]) grad[(size_t)o * n + i] = hess[(size_t)o * n + i] = 0.0f;
@@ -1894,6 +2236,7 @@ int orc_train_limited(const float* x, uint64_t F, uint64_t n, const float* y, ui
                 gr.cs_output = o;
                 gr.grow(go, ho, record_leaves != 0);
             }
+            if (renew) gr.renew_leaves(y, w, m->train_pred.data() + (size_t)o * n, op.alpha_at(o));
             gr.update_predictions(m->train_pred.data() + (size_t)o * n);
             gr.tree.group = o;
             m->trees.push_back(std::move(gr.tree));

@@ -66,6 +66,22 @@ void orc_base_score(int32_t objective, uint32_t n_outputs, const float* y, const
 void orc_transform(int32_t transform, float* preds, uint32_t n_groups, uint64_t n);
 double orc_metric(int32_t metric, const float* preds, uint32_t n_groups, uint64_t n,
                   const float* y, const float* w);
+/* The same with the objective's parameters (pinball alphas, Huber delta)
+ * taken from cfg. */
+void orc_gradients_cfg(const bst_config* cfg, uint32_t n_outputs, const float* preds, const float* y,
+                       const float* w, uint64_t n, float* grad, float* hess);
+void orc_base_score_cfg(const bst_config* cfg, uint32_t n_outputs, const float* y, const float* w, uint64_t n,
+                        float* out);
+double orc_metric_cfg(int32_t metric, const bst_config* cfg, const float* preds, uint32_t n_groups, uint64_t n,
+                      const float* y, const float* w);
+/* GOSS (sampling/row.rs:214-280): the sampler seeded by `seed`, called
+ * `calls` times on g / h (scaled in place each call); mask of the last call,
+ * returns its sampled count. */
+uint64_t orc_goss(float* g, float* h, uint64_t n, float top_rate, float other_rate, uint64_t seed, uint32_t calls,
+                  uint8_t* mask);
+/* Leaf renewing's quantile (utils.rs:17-135): w NULL for the unweighted
+ * rank rule, else the weighted step rule. NaN for n = 0. */
+float orc_leaf_quantile(const float* v, const float* w, uint64_t n, float alpha);
 
 /* ---- quantised gradients (the engine's int8 / int16 mode; no reference
  * counterpart). Philox4x32-10 (Salmon et al., SC 2011) and the stochastic

@@ -93,6 +93,30 @@ KATS = {
         # classification.rs:276-297 logistic_weighted
         {"src": "training/objectives/classification.rs:276", "objective": 1, "preds": [[0.0, 0.0]], "y": [1.0, 0.0],
          "w": [2.0, 0.5], "grad": [[-1.0, 0.25]], "hess": None, "tol": 1e-6},
+        # regression.rs:461-473 absolute_loss_basic
+        {"src": "training/objectives/regression.rs:461", "objective": 3, "preds": [[1.0, 2.0, 3.0]],
+         "y": [0.5, 2.5, 2.5], "w": None, "grad": [[1.0, -1.0, 1.0]], "hess": None, "tol": 1e-6},
+        # regression.rs:373-407 pinball_loss_quantiles, alpha 0.1 and 0.9
+        {"src": "training/objectives/regression.rs:384", "objective": 4, "alpha": [0.1], "preds": [[1.0, 2.0]],
+         "y": [2.0, 1.0], "w": None, "grad": [[-0.1, 0.9]], "hess": [[1.0, 1.0]], "tol": 1e-6},
+        {"src": "training/objectives/regression.rs:397", "objective": 4, "alpha": [0.9], "preds": [[1.0, 2.0]],
+         "y": [2.0, 1.0], "w": None, "grad": [[-0.9, 0.1]], "hess": [[1.0, 1.0]], "tol": 1e-6},
+        # regression.rs:440-459 pinball_loss_median
+        {"src": "training/objectives/regression.rs:440", "objective": 4, "alpha": [0.5], "preds": [[1.0, 2.0, 3.0]],
+         "y": [0.5, 2.5, 2.5], "w": None, "grad": [[0.5, -0.5, 0.5]], "hess": None, "tol": 1e-6},
+        # regression.rs:476-494 pseudo_huber_near_zero (tolerances 1e-3 / 1e-2)
+        {"src": "training/objectives/regression.rs:476", "objective": 5, "delta": 1.0, "preds": [[0.01]],
+         "y": [0.0], "w": None, "grad": [[0.01]], "hess": None, "tol": 1e-3},
+        {"src": "training/objectives/regression.rs:493", "objective": 5, "delta": 1.0, "preds": [[0.01]],
+         "y": [0.0], "w": None, "grad": None, "hess": [[1.0]], "tol": 1e-2},
+        # regression.rs:496-509 poisson_loss_basic
+        {"src": "training/objectives/regression.rs:496", "objective": 6, "preds": [[0.0]], "y": [2.0], "w": None,
+         "grad": [[-1.0]], "hess": [[1.0]], "tol": 1e-6},
+        # classification.rs:300-326 hinge_loss_margin (margin 2: grad 0; margin -0.5: grad -1)
+        {"src": "training/objectives/classification.rs:314", "objective": 7, "preds": [[2.0]], "y": [1.0],
+         "w": None, "grad": [[0.0]], "hess": None, "tol": 1e-6},
+        {"src": "training/objectives/classification.rs:325", "objective": 7, "preds": [[-0.5]], "y": [1.0],
+         "w": None, "grad": [[-1.0]], "hess": None, "tol": 1e-6},
     ],
     "base_score": [
         # classification.rs:264-274 logistic_base_score: 50% positives -> 0
@@ -101,6 +125,21 @@ KATS = {
         # classification.rs:343-365 softmax_base_score: class priors 1/2, 1/4, 1/4
         {"src": "training/objectives/classification.rs:343", "objective": 2, "n_outputs": 3, "y": [0, 0, 1, 2],
          "expect": [-0.6931472, -1.3862944, -1.3862944], "tol": 1e-5},
+        # regression.rs:512-523 poisson_loss_base_score: ln(2.5)
+        {"src": "training/objectives/regression.rs:512", "objective": 6, "n_outputs": 1, "y": [1, 2, 3, 4],
+         "expect": [0.91629073], "tol": 1e-6},
+    ],
+    "leaf_quantile": [
+        # utils.rs:362-456: the unweighted rank rule and the weighted step rule
+        {"src": "utils.rs:377", "values": [], "weights": None, "alpha": 0.5, "expect": NAN},
+        {"src": "utils.rs:364", "values": [], "weights": [], "alpha": 0.5, "expect": NAN},
+        {"src": "utils.rs:384", "values": [42.0], "weights": None, "alpha": 0.5, "expect": 42.0},
+        {"src": "utils.rs:392", "values": [1.0, 2.0, 3.0, 4.0, 5.0], "weights": None, "alpha": 0.5, "expect": 3.0},
+        {"src": "utils.rs:401", "values": [1.0, 2.0, 3.0, 4.0], "weights": None, "alpha": 0.25, "expect": 1.0},
+        {"src": "utils.rs:411", "values": [1.0, 2.0, 3.0, 4.0], "weights": None, "alpha": 0.75, "expect": 3.0},
+        {"src": "utils.rs:421", "values": [5.0, 1.0, 3.0, 2.0, 4.0], "weights": None, "alpha": 0.5, "expect": 3.0},
+        {"src": "utils.rs:430", "values": [1.0, 2.0, 3.0], "weights": [1.0, 2.0, 1.0], "alpha": 0.5, "expect": 2.0},
+        {"src": "utils.rs:445", "values": [1.0, 10.0], "weights": [1.0, 9.0], "alpha": 0.5, "expect": 10.0},
     ],
     "partition": [
         # training/gbdt/partition.rs:391-463: f0 alternating, f1 halves; split f1 at bin 0, then f0 at bin 0

@@ -63,6 +63,11 @@ _SIGS = [
     ("orc_base_score", None, [ctypes.c_int32, u32, f32p, f32p, u64, f32p]),
     ("orc_transform", None, [ctypes.c_int32, f32p, u32, u64]),
     ("orc_metric", ctypes.c_double, [ctypes.c_int32, f32p, u32, u64, f32p, f32p]),
+    ("orc_gradients_cfg", None, [vp, u32, f32p, f32p, f32p, u64, f32p, f32p]),
+    ("orc_base_score_cfg", None, [vp, u32, f32p, f32p, u64, f32p]),
+    ("orc_metric_cfg", ctypes.c_double, [ctypes.c_int32, vp, f32p, u32, u64, f32p, f32p]),
+    ("orc_goss", u64, [f32p, f32p, u64, ctypes.c_float, ctypes.c_float, u64, u32, u8p]),
+    ("orc_leaf_quantile", ctypes.c_float, [f32p, f32p, u64, ctypes.c_float]),
     ("orc_train_limited", ctypes.c_int,
      [f32p, u64, u64, f32p, u32, f32p, u32p, u32, vp, u32, ctypes.c_int, ctypes.c_int, u32,
       ctypes.POINTER(vp)]),
@@ -321,32 +326,63 @@ def find_split(hist, n_bins, is_cat, has_missing, pg, ph, pc, cfg, n_threads=1):
     return s
 
 
-def gradients(objective, preds_gm, y, w=None):
+def _obj_cfg(objective, alpha, delta):
+    c = config(objective=objective, huber_delta=float(delta))
+    if alpha is not None:
+        a = [float(v) for v in np.atleast_1d(alpha)]
+        c.quantile_alpha = (ctypes.c_float * len(a))(*a)
+        c.n_quantiles = len(a)
+    return c
+
+
+def gradients(objective, preds_gm, y, w=None, alpha=None, delta=1.0):
     p = f32(preds_gm)
     if p.ndim == 1:
         p = p.reshape(1, -1)
     G, n = p.shape
     g = np.zeros((G, n), np.float32)
     h = np.zeros((G, n), np.float32)
-    lib.orc_gradients(objective, G, P(p, ctypes.c_float), P(f32(y), ctypes.c_float),
-                      P(None if w is None else f32(w), ctypes.c_float), n, P(g, ctypes.c_float), P(h, ctypes.c_float))
+    c = _obj_cfg(objective, alpha, delta)
+    lib.orc_gradients_cfg(ctypes.byref(c), G, P(p, ctypes.c_float), P(f32(y), ctypes.c_float),
+                          P(None if w is None else f32(w), ctypes.c_float), n, P(g, ctypes.c_float),
+                          P(h, ctypes.c_float))
     return g, h
 
 
-def base_score(objective, n_outputs, y, w=None):
+def base_score(objective, n_outputs, y, w=None, alpha=None):
     out = np.zeros(n_outputs, np.float32)
     yy = f32(y)
-    lib.orc_base_score(objective, n_outputs, P(yy, ctypes.c_float), P(None if w is None else f32(w), ctypes.c_float),
-                       len(yy), P(out, ctypes.c_float))
+    c = _obj_cfg(objective, alpha, 1.0)
+    lib.orc_base_score_cfg(ctypes.byref(c), n_outputs, P(yy, ctypes.c_float),
+                           P(None if w is None else f32(w), ctypes.c_float), len(yy), P(out, ctypes.c_float))
     return out
 
 
-def metric(kind, preds_gm, y, w=None):
+def metric(kind, preds_gm, y, w=None, alpha=None, delta=1.0):
     p = f32(preds_gm)
     if p.ndim == 1:
         p = p.reshape(1, -1)
-    return lib.orc_metric(kind, P(p, ctypes.c_float), p.shape[0], p.shape[1], P(f32(y), ctypes.c_float),
-                          P(None if w is None else f32(w), ctypes.c_float))
+    c = _obj_cfg(0, alpha, delta)
+    return lib.orc_metric_cfg(kind, ctypes.byref(c), P(p, ctypes.c_float), p.shape[0], p.shape[1],
+                              P(f32(y), ctypes.c_float), P(None if w is None else f32(w), ctypes.c_float))
+
+
+def goss(g, h, top_rate, other_rate, seed, calls=1):
+    """GOSS sampler (sampling/row.rs:214-280) called `calls` times on (g, h)
+    (scaled in place each call): the last call's kept mask and count, and the
+    scaled g, h."""
+    g = f32(g).copy()
+    h = f32(h).copy()
+    mask = np.zeros(g.size, np.uint8)
+    k = lib.orc_goss(P(g, ctypes.c_float), P(h, ctypes.c_float), g.size, top_rate, other_rate, seed, calls,
+                     P(mask, ctypes.c_uint8))
+    return mask, int(k), g, h
+
+
+def leaf_quantile(values, weights, alpha):
+    v = f32(values)
+    w = None if weights is None else f32(weights)
+    return float(lib.orc_leaf_quantile(P(v, ctypes.c_float), P(w, ctypes.c_float), v.size, alpha))
 
 
 def philox4x32_10(ctr, key):

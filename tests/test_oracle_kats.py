@@ -68,13 +68,24 @@ def test_find_split(kats):
 
 def test_objectives(kats):
     for c in kats["objective"]:
-        g, h = ob.gradients(c["objective"], np.array(c["preds"]), c["y"], c["w"])
-        np.testing.assert_allclose(g, np.array(c["grad"]), atol=c["tol"], err_msg=c["src"])
+        g, h = ob.gradients(c["objective"], np.array(c["preds"]), c["y"], c["w"], alpha=c.get("alpha"),
+                            delta=c.get("delta", 1.0))
+        if c["grad"] is not None:
+            np.testing.assert_allclose(g, np.array(c["grad"]), atol=c["tol"], err_msg=c["src"])
         if c["hess"] is not None:
             np.testing.assert_allclose(h, np.array(c["hess"]), atol=c["tol"], err_msg=c["src"])
     for c in kats["base_score"]:
         b = ob.base_score(c["objective"], c["n_outputs"], c["y"])
         np.testing.assert_allclose(b, c["expect"], atol=c["tol"], err_msg=c["src"])
+
+
+def test_leaf_quantile(kats):
+    for c in kats["leaf_quantile"]:
+        got = ob.leaf_quantile(c["values"], c["weights"], c["alpha"])
+        if c["expect"] == "nan":
+            assert np.isnan(got), c["src"]
+        else:
+            assert abs(got - c["expect"]) < 1e-6, c["src"]
 
 
 def test_softmax_gradient_signs():
