@@ -769,6 +769,7 @@ class Trainer {
         rd_.prefix = rd_small_.p + cap;
         rd_.rank = rd_small_.p + 2 * (size_t)cap;
         rd_.hist = rd_small_.p + 3 * (size_t)cap;
+        rd_.n_rows = (uint32_t)n_;
         if (ds_.has_w) {
             rd_big_.alloc(4 * (size_t)n_);
             for (int k = 0; k < 2; ++k) {

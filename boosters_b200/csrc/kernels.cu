@@ -3899,12 +3899,52 @@ __global__ void k_renew_apply(BDev d, RenewDev r, float lr) {
         if (r.rank[l] != RENEW_NONE) renew_set(d, l, renew_value(r.prefix[l]) * lr);
 }
 
-// Weighted form: one block per leaf. The leaf's sampled rows are compacted
-// in partition order into key[0] / row[0] at the leaf's own positions
-// (first = its first row position in the concatenation of the leaf
-// ranges), their weights summed in that order, the keys sorted stably by
-// 32 one-bit passes (key[0] <-> key[1]), and the running weight scanned.
+// Weighted form: one block per leaf. The reference's partition is stable,
+// so a leaf's rows are in ascending row order there; here they are in
+// partition-chunk order. The leaf's sampled rows are compacted into key[0]
+// / row[0] at the leaf's own positions (its range in the row buffer),
+// sorted by row id (stable one-bit passes over the id's bits), their
+// weights summed in that order, sorted stably by key (32 more passes, so
+// equal keys stay in row order) and the running weight scanned.
 constexpr uint32_t RENEW_W_THREADS = 1024;
+
+// One stable split pass of a leaf's (key, row) pairs from buffer src to
+// src ^ 1 by bit b of the key (or of the row id): zeros first, each side in
+// its order.
+__device__ void renew_split_pass(const RenewDev& r, uint32_t src, uint32_t first, uint32_t m, uint32_t b,
+                                 bool by_row, uint32_t* sh, uint32_t* s_zero, uint32_t* s_base) {
+    const uint32_t* ks = r.key[src] + first;
+    const uint32_t* rs = r.row[src] + first;
+    uint32_t* kd = r.key[src ^ 1u] + first;
+    uint32_t* rd = r.row[src ^ 1u] + first;
+    if (threadIdx.x == 0) *s_zero = 0;
+    __syncthreads();
+    uint32_t z = 0;
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) z += (((by_row ? rs[i] : ks[i]) >> b) & 1u) ? 0u : 1u;
+    for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(FULL, z, o);
+    if ((threadIdx.x & 31) == 0 && z) atomicAdd(s_zero, z);
+    if (threadIdx.x == 0) *s_base = 0;
+    __syncthreads();
+    const uint32_t zeros = *s_zero;
+    for (uint32_t t0 = 0; t0 < m; t0 += blockDim.x) {
+        const uint32_t i = t0 + threadIdx.x;
+        const bool valid = i < m;
+        const uint32_t k = valid ? ks[i] : 0u, row = valid ? rs[i] : 0u;
+        const bool zero = valid && !(((by_row ? row : k) >> b) & 1u);
+        uint32_t tz;
+        const uint32_t rz = block_excl_scan(zero ? 1u : 0u, sh, &tz);
+        const uint32_t base = *s_base;
+        if (valid) {
+            // ones before this one: (t0 - base) in earlier tiles, i - t0 - rz in this one
+            const uint32_t dst = zero ? base + rz : zeros + (t0 - base) + (i - t0 - rz);
+            kd[dst] = k;
+            rd[dst] = row;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) *s_base += tz;
+        __syncthreads();
+    }
+}
 
 __global__ void __launch_bounds__(RENEW_W_THREADS)
 k_renew_weighted(BDev d, RenewDev r, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1,
@@ -3939,12 +3979,19 @@ k_renew_weighted(BDev d, RenewDev r, const uint32_t* __restrict__ r0, const uint
         const uint32_t m = s_base;
         __syncthreads();
         if (m == 0) continue;  // block-uniform
-        // 2. the f32 total of the weights in partition order
+        // 2. row order (the reference's partition order), then the f32 total
+        // of the weights in that order
+        uint32_t src = 0;
+        const uint32_t row_bits = 32u - (uint32_t)__clz(max(r.n_rows, 2u) - 1u);  // row ids < n_rows
+        for (uint32_t b = 0; b < row_bits; ++b) {
+            renew_split_pass(r, src, first, m, b, true, sh, &s_zero, &s_base);
+            src ^= 1u;
+        }
         if (threadIdx.x == 0) s_acc = 0.0f;
         for (uint32_t t0 = 0; t0 < m; t0 += blockDim.x) {
             const uint32_t i = t0 + threadIdx.x;
             __syncthreads();
-            s_w[threadIdx.x] = i < m ? w[r.row[0][first + i]] : 0.0f;
+            s_w[threadIdx.x] = i < m ? w[r.row[src][first + i]] : 0.0f;
             __syncthreads();
             if (threadIdx.x == 0) {
                 float acc = s_acc;
@@ -3956,39 +4003,8 @@ k_renew_weighted(BDev d, RenewDev r, const uint32_t* __restrict__ r0, const uint
         __syncthreads();
         const float threshold = s_acc * alpha;
         // 3. stable sort by key: zeros of bit b first, each side in order
-        uint32_t src = 0;
         for (uint32_t b = 0; b < 32; ++b) {
-            const uint32_t* ks = r.key[src] + first;
-            const uint32_t* rs = r.row[src] + first;
-            uint32_t* kd = r.key[src ^ 1u] + first;
-            uint32_t* rd = r.row[src ^ 1u] + first;
-            if (threadIdx.x == 0) s_zero = 0;
-            __syncthreads();
-            uint32_t z = 0;
-            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) z += ((ks[i] >> b) & 1u) ? 0u : 1u;
-            for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(FULL, z, o);
-            if ((threadIdx.x & 31) == 0 && z) atomicAdd(&s_zero, z);
-            if (threadIdx.x == 0) s_base = 0;
-            __syncthreads();
-            const uint32_t zeros = s_zero;
-            for (uint32_t t0 = 0; t0 < m; t0 += blockDim.x) {
-                const uint32_t i = t0 + threadIdx.x;
-                const bool valid = i < m;
-                const uint32_t k = valid ? ks[i] : 0u;
-                const bool zero = valid && !((k >> b) & 1u);
-                uint32_t tz;
-                const uint32_t rz = block_excl_scan(zero ? 1u : 0u, sh, &tz);
-                const uint32_t base = s_base;
-                if (valid) {
-                    // ones before this one in the tile: i - t0 - rz
-                    const uint32_t dst = zero ? base + rz : zeros + (t0 - base) + (i - t0 - rz);
-                    kd[dst] = k;
-                    rd[dst] = rs[i];
-                }
-                __syncthreads();
-                if (threadIdx.x == 0) s_base += tz;
-                __syncthreads();
-            }
+            renew_split_pass(r, src, first, m, b, false, sh, &s_zero, &s_base);
             src ^= 1u;
         }
         // 4. the first sorted row whose running weight reaches the threshold

@@ -347,6 +347,7 @@ struct RenewDev {
     uint32_t cap;
     uint32_t* key[2];  // weighted: [n] ping-pong keys
     uint32_t* row[2];  // weighted: [n] ping-pong row ids
+    uint32_t n_rows;   // weighted: rows of the dataset (row ids < n_rows)
 };
 void launch_leaf_renew(const BDev& d, const RenewDev& r, const uint32_t* r0, const uint32_t* r1, const float* y,
                        const float* pred, const float* w, float alpha, float learning_rate, uint32_t grid,
