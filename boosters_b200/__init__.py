@@ -755,6 +755,12 @@ class Booster:
             self._h = None
 
 
+def release_cached_memory():
+    """Frees the device buffers the library keeps for reuse between calls
+    (bst_release_cached_memory)."""
+    _n.lib.bst_release_cached_memory()
+
+
 _METRIC_CODES = {"rmse": _n.METRIC_RMSE, "logloss": _n.METRIC_LOGLOSS, "mlogloss": _n.METRIC_MLOGLOSS,
                  "mae": _n.METRIC_MAE, "mape": _n.METRIC_MAPE, "quantile": _n.METRIC_QUANTILE,
                  "huber": _n.METRIC_HUBER, "poisson": _n.METRIC_POISSON,

@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(_HERE, "libboosters_b200.so")
 SIGNATURES = [
     ("bst_last_error", ctypes.c_char_p, []),
     ("bst_version", ctypes.c_char_p, []),
+    ("bst_release_cached_memory", None, []),
     ("bst_config_default", None, [ctypes.POINTER(Config)]),
     ("bst_config_validate", ctypes.c_int32, [ctypes.POINTER(Config)]),
     ("bst_dataset_create", ctypes.c_int32,

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <thread>
 #include <unordered_set>
 
 #ifdef _OPENMP
@@ -81,21 +82,38 @@ struct FeatureFacts {
     uint64_t n_nan = 0;
 };
 
+// v is a whole number: every float of magnitude 2^23 or more is; below
+// that, exactly when truncation to int32 and back gives v (v - trunc(v) ==
+// 0 for finite v; NaN and infinities are not whole).
+inline bool whole(float v) {
+    if (!(std::fabs(v) < 8388608.0f)) return std::isfinite(v);
+    return (float)(int32_t)v == v;
+}
+
 FeatureFacts analyze(const float* col, uint64_t n, const bst_config& cfg, bool user_cat) {
     const size_t limit = std::max<size_t>(cfg.max_categorical_cardinality, cfg.max_bins) + 10;
     DistinctFloats uniq(limit);
-    bool exceeded = false, all_int = true;
-    uint64_t nan = 0, valid = 0, nonzero = 0;
+    // three passes that each stop as early as their answer allows: the
+    // NaN and nonzero counts (branch-free), the first non-whole value, the
+    // distinct values until `limit` of them were seen
+    uint64_t nan = 0, nonzero = 0;
+#pragma omp simd reduction(+ : nan, nonzero)
     for (uint64_t i = 0; i < n; ++i) {
         const float v = col[i];
-        if (std::isnan(v)) {
-            ++nan;
-            continue;
-        }
-        ++valid;
-        nonzero += (v != 0.0f);
-        if (all_int && !(v - std::trunc(v) == 0.0f)) all_int = false;
-        if (!exceeded && uniq.probe(v, false)) {
+        nan += (v != v) ? 1u : 0u;
+        nonzero += (v != 0.0f && v == v) ? 1u : 0u;
+    }
+    const uint64_t valid = n - nan;
+    bool all_int = true;
+    for (uint64_t i = 0; i < n && all_int; ++i) {
+        const float v = col[i];
+        if (v == v && !whole(v)) all_int = false;
+    }
+    bool exceeded = false;
+    for (uint64_t i = 0; i < n && !exceeded; ++i) {
+        const float v = col[i];
+        if (v != v) continue;
+        if (uniq.probe(v, false)) {
             if (uniq.size >= limit)
                 exceeded = true;
             else
@@ -116,14 +134,14 @@ FeatureFacts analyze(const float* col, uint64_t n, const bst_config& cfg, bool u
     return f;
 }
 
-// dataset.rs:598-633: deterministic splitmix64 row sample used for bounds.
+// dataset.rs:598-633: deterministic splitmix64 row sample used for bounds,
+// in ascending row order (read off the bitmap of drawn rows).
 std::vector<uint32_t> binning_sample(uint64_t n, uint64_t k) {
     std::vector<uint32_t> out;
     if (n <= k) return out;
-    out.reserve(k);
     std::vector<uint64_t> seen((n + 63) / 64, 0);  // rows drawn so far
-    uint64_t s = 0xD1B54A32D192ED03ULL ^ n;
-    while (out.size() < k) {
+    uint64_t s = 0xD1B54A32D192ED03ULL ^ n, got = 0;
+    while (got < k) {
         s += 0x9E3779B97F4A7C15ULL;
         uint64_t z = s;
         z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
@@ -134,10 +152,12 @@ std::vector<uint32_t> binning_sample(uint64_t n, uint64_t k) {
         const uint64_t bit = 1ull << (r & 63u);
         if (!(word & bit)) {
             word |= bit;
-            out.push_back(r);
+            ++got;
         }
     }
-    std::sort(out.begin(), out.end());
+    out.reserve(k);
+    for (size_t wi = 0; wi < seen.size(); ++wi)
+        for (uint64_t w = seen[wi]; w; w &= w - 1) out.push_back((uint32_t)(wi * 64 + (uint64_t)__builtin_ctzll(w)));
     return out;
 }
 
@@ -151,21 +171,30 @@ void sort_floats(std::vector<float>& v) {
         return;
     }
     std::vector<uint32_t> a(n), b(n);
+    // 8-bit digits: the four digit counts in one pass, a pass skipped when
+    // every key has the same digit there
+    std::vector<uint32_t> cnt(4 * 256, 0);
     for (size_t i = 0; i < n; ++i) {
         uint32_t u;
         std::memcpy(&u, &v[i], 4);
-        a[i] = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+        const uint32_t k = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+        a[i] = k;
+        ++cnt[k & 255u];
+        ++cnt[256 + ((k >> 8) & 255u)];
+        ++cnt[512 + ((k >> 16) & 255u)];
+        ++cnt[768 + (k >> 24)];
     }
-    for (int shift = 0; shift < 32; shift += 11) {
-        uint32_t cnt[2048] = {0};
-        for (size_t i = 0; i < n; ++i) ++cnt[(a[i] >> shift) & 2047u];
+    for (int d = 0; d < 4; ++d) {
+        uint32_t* c = cnt.data() + 256 * d;
+        const int shift = 8 * d;
+        if (c[(a[0] >> shift) & 255u] == n) continue;
         uint32_t sum = 0;
-        for (uint32_t d = 0; d < 2048; ++d) {
-            const uint32_t c = cnt[d];
-            cnt[d] = sum;
-            sum += c;
+        for (uint32_t q = 0; q < 256; ++q) {
+            const uint32_t t = c[q];
+            c[q] = sum;
+            sum += t;
         }
-        for (size_t i = 0; i < n; ++i) b[cnt[(a[i] >> shift) & 2047u]++] = a[i];
+        for (size_t i = 0; i < n; ++i) b[c[(a[i] >> shift) & 255u]++] = a[i];
         a.swap(b);
     }
     for (size_t i = 0; i < n; ++i) {
@@ -242,14 +271,22 @@ bst_status plan_binning(const float* x, uint64_t F, uint64_t n,
     plan.mappers.resize(F);
     plan.trivial.assign(F, 0);
     std::vector<FeatureFacts> facts(F);
-    const std::vector<uint32_t> sample = binning_sample(n, cfg.binning_sample_cnt);
-
+    // the row sample (sequential draws) on one thread while the others
+    // analyse the features
+    std::vector<uint32_t> sample;
+    std::thread sampler([&] { sample = binning_sample(n, cfg.binning_sample_cnt); });
 #pragma omp parallel for schedule(dynamic, 1)
     for (int64_t f = 0; f < (int64_t)F; ++f) {
         const float* col = x + (uint64_t)f * n;
         const bool uc = (size_t)f < user_cat.size() && user_cat[f];
-        FeatureFacts ff = analyze(col, n, cfg, uc);
-        facts[f] = ff;
+        facts[f] = analyze(col, n, cfg, uc);
+    }
+    sampler.join();
+
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t f = 0; f < (int64_t)F; ++f) {
+        const float* col = x + (uint64_t)f * n;
+        const FeatureFacts& ff = facts[f];
         if (ff.trivial) continue;
         if (ff.numeric) {
             std::vector<float> vals;

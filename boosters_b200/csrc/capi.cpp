@@ -126,6 +126,7 @@ extern "C" {
 
 const char* bst_last_error(void) { return g_err.c_str(); }
 const char* bst_version(void) { return "boosters-b200 0.1.0 (sm_100a)"; }
+void bst_release_cached_memory(void) { bst::dev_cache_trim(); }
 
 void bst_config_default(bst_config* c) {
     if (!c) return;
@@ -684,6 +685,7 @@ bst_status bst_bin_values(const double* bounds, uint32_t n_bounds, int32_t missi
         bst::BinColumn bc;
         bc.matrix = wide ? 1 : 0;
         bc.pos = 0;
+        bc.src = 0;
         bc.is_cat = m.categorical;
         bc.nan_bin = m.missing == bst::MISSING_NAN ? (m.n_bins ? m.n_bins - 1 : 0) : m.default_bin;
         bc.zero_bin = m.missing == bst::MISSING_ZERO ? m.default_bin : 0xFFFFFFFFu;

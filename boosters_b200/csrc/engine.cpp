@@ -19,6 +19,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <mutex>
 #include <unordered_map>
 
 namespace bst {
@@ -55,6 +56,117 @@ void dev_bytes_reserve(size_t bytes) {
 }
 
 void dev_bytes_release(size_t bytes) { g_dev_bytes.fetch_sub(bytes); }
+
+namespace {
+
+struct DevCache {
+    std::mutex mu;
+    std::multimap<size_t, std::pair<int, void*>> blocks;  // size -> (device, pointer)
+    size_t bytes = 0;
+};
+DevCache& dev_cache() {
+    static DevCache* c = new DevCache();  // never destroyed: no cudaFree after the runtime unloads
+    return *c;
+}
+
+size_t dev_cache_max() {
+    static const size_t m = [] {
+        const char* v = std::getenv("BST_DEVICE_CACHE_BYTES");
+        return v ? (size_t)std::strtoull(v, nullptr, 10) : (size_t)8 << 30;
+    }();
+    return m;
+}
+
+// 256 B .. 1 MiB: the next power of two; above: a multiple of 2 MiB
+size_t dev_round(size_t b) {
+    if (b <= ((size_t)1 << 20)) {
+        size_t r = 256;
+        while (r < b) r <<= 1;
+        return r;
+    }
+    const size_t g = (size_t)2 << 20;
+    return (b + g - 1) / g * g;
+}
+
+}  // namespace
+
+void dev_cache_trim() {
+    DevCache& c = dev_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    for (auto& e : c.blocks) {
+        cudaFree(e.second.second);
+        dev_bytes_release(e.first);
+    }
+    cudaGetLastError();
+    c.blocks.clear();
+    c.bytes = 0;
+}
+
+void* dev_alloc(size_t bytes, size_t* block_bytes) {
+    const size_t r = dev_round(bytes);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) cudaGetLastError();
+    DevCache& c = dev_cache();
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        for (auto it = c.blocks.lower_bound(r); it != c.blocks.end() && it->first <= 2 * r; ++it)
+            if (it->second.first == dev) {
+                void* p = it->second.second;
+                *block_bytes = it->first;
+                c.bytes -= it->first;
+                c.blocks.erase(it);
+                return p;
+            }
+    }
+    try {
+        dev_bytes_reserve(r);
+    } catch (const Error&) {
+        dev_cache_trim();
+        dev_bytes_reserve(r);  // throws again if the live buffers alone pass the cap
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, r);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        dev_cache_trim();
+        e = cudaMalloc(&p, r);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        dev_bytes_release(r);
+        throw Error{e == cudaErrorMemoryAllocation ? BST_ERR_OUT_OF_MEMORY : BST_ERR_CUDA,
+                    std::string("cudaMalloc of ") + std::to_string(r) + " bytes failed: " + cudaGetErrorString(e)};
+    }
+    *block_bytes = r;
+    return p;
+}
+
+void dev_free(void* p, size_t block_bytes) {
+    if (!p) return;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) cudaGetLastError();
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) == cudaSuccess && a.type == cudaMemoryTypeDevice) dev = a.device;
+    cudaGetLastError();
+    int cur = dev;
+    cudaGetDevice(&cur);
+    if (cur != dev) cudaSetDevice(dev);
+    const cudaError_t se = cudaDeviceSynchronize();  // what cudaFree would wait for
+    if (cur != dev) cudaSetDevice(cur);
+    DevCache& c = dev_cache();
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (se == cudaSuccess && c.bytes + block_bytes <= dev_cache_max()) {
+            c.blocks.emplace(block_bytes, std::make_pair(dev, p));
+            c.bytes += block_bytes;
+            return;
+        }
+    }
+    cudaGetLastError();
+    cudaFree(p);
+    cudaGetLastError();
+    dev_bytes_release(block_bytes);
+}
 
 // Column tiles of the histogram kernel: lanes of one 16-byte row vector
 // whose bins fit one shared-memory histogram (<= 4096 bins = 64 KiB).
@@ -2528,6 +2640,20 @@ uint32_t HostTree::alloc() {
 void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, DeviceBinned& out) {
     std::string err;
     const auto t0 = std::chrono::steady_clock::now();
+    // Features in pinned host memory: every feature goes to the device
+    // while the host plans the bins (the copy overlaps the analysis);
+    // otherwise only the planned columns are copied afterwards.
+    DevArray<float> x;
+    bool staged = false;
+    {
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, ds.xdata()) == cudaSuccess && a.type == cudaMemoryTypeHost && ds.n && ds.F) {
+            x.alloc((size_t)ds.F * ds.n);
+            BST_CK(cudaMemcpyAsync(x.p, ds.xdata(), sizeof(float) * ds.F * ds.n, cudaMemcpyHostToDevice, st));
+            staged = true;
+        }
+        cudaGetLastError();
+    }
     bst_status rc = plan_binning(ds.xdata(), ds.F, ds.n, ds.user_cat, cfg, out.plan, err);
     if (rc != BST_OK) throw Error{rc, err};
     const BinPlan& p = out.plan;
@@ -2546,6 +2672,7 @@ void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, 
         BinColumn bc;
         bc.matrix = p.col_matrix[c];
         bc.pos = p.col_pos[c];
+        bc.src = staged ? p.col_feature[c] : c;
         bc.is_cat = m.categorical;
         bc.nan_bin = m.missing == MISSING_NAN ? m.n_bins - 1 : m.default_bin;
         bc.zero_bin = m.missing == MISSING_ZERO ? m.default_bin : 0xFFFFFFFFu;
@@ -2562,13 +2689,15 @@ void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, 
         }
         cols[c] = bc;
     }
-    DevArray<float> x, d_thr;
+    DevArray<float> d_thr;
     DevArray<int32_t> d_cats;
     DevArray<BinColumn> d_cols;
-    x.alloc((size_t)nc * n);
-    for (uint32_t c = 0; c < nc; ++c)
-        BST_CK(cudaMemcpyAsync(x.p + (size_t)c * n, ds.xdata() + (size_t)p.col_feature[c] * n, sizeof(float) * n,
-                               cudaMemcpyHostToDevice, st));
+    if (!staged) {
+        x.alloc((size_t)nc * n);
+        for (uint32_t c = 0; c < nc; ++c)
+            BST_CK(cudaMemcpyAsync(x.p + (size_t)c * n, ds.xdata() + (size_t)p.col_feature[c] * n, sizeof(float) * n,
+                                   cudaMemcpyHostToDevice, st));
+    }
     d_cols.alloc(nc);
     BST_CK(cudaMemcpyAsync(d_cols.p, cols.data(), sizeof(BinColumn) * nc, cudaMemcpyHostToDevice, st));
     d_thr.alloc(std::max<size_t>(1, thr.size()));

@@ -32,36 +32,39 @@ void cuda_check(cudaError_t e, const char* what);
 void dev_bytes_reserve(size_t bytes);  // throws Error{BST_ERR_OUT_OF_MEMORY}
 void dev_bytes_release(size_t bytes);
 
+// Device block cache: a released buffer is kept (per device, up to
+// BST_DEVICE_CACHE_BYTES, default 8 GiB) and handed to a later request of
+// at most its size and at least half of it, so that consecutive training
+// calls, which allocate the same buffers, skip cudaMalloc / cudaFree
+// (which maps and unmaps pages). A release waits for the device to be idle
+// first, as cudaFree does, so no kernel still in flight can see its buffer
+// reused. The cap above counts cached blocks; an allocation that would
+// pass it, or that the device refuses, first frees every cached block.
+// dev_alloc returns the block and its size (the request rounded up).
+void* dev_alloc(size_t bytes, size_t* block_bytes);  // throws Error
+void dev_free(void* p, size_t block_bytes);
+void dev_cache_trim();  // frees every cached block
+
 template <class T>
 struct DevArray {
     T* p = nullptr;
     size_t n = 0;
+    size_t block = 0;  // bytes of the underlying block
     DevArray() = default;
     DevArray(const DevArray&) = delete;
     DevArray& operator=(const DevArray&) = delete;
     ~DevArray() { release(); }
     void release() {
-        if (p) {
-            cudaFree(p);
-            dev_bytes_release(n * sizeof(T));
-        }
+        if (p) dev_free(p, block);
         p = nullptr;
         n = 0;
+        block = 0;
     }
     void alloc(size_t k) {
         if (k <= n && p) return;
         release();
         if (k == 0) return;
-        dev_bytes_reserve(k * sizeof(T));
-        cudaError_t e = cudaMalloc(&p, k * sizeof(T));
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            p = nullptr;
-            dev_bytes_release(k * sizeof(T));
-            throw Error{e == cudaErrorMemoryAllocation ? BST_ERR_OUT_OF_MEMORY : BST_ERR_CUDA,
-                        std::string("cudaMalloc of ") + std::to_string(k * sizeof(T)) +
-                            " bytes failed: " + cudaGetErrorString(e)};
-        }
+        p = static_cast<T*>(dev_alloc(k * sizeof(T), &block));
         n = k;
     }
 };

@@ -94,7 +94,7 @@ k_bin_assign(const float* __restrict__ x, uint64_t n, const BinColumn* __restric
         unsigned char* my = smem + (size_t)t * rec;
         for (uint32_t c = 0; c < n_cols; ++c) {
             const BinColumn col = cols[c];
-            const float v = x[(uint64_t)c * n + row];
+            const float v = x[(uint64_t)col.src * n + row];
             uint32_t bin;
             if (v != v) {
                 bin = col.nan_bin;

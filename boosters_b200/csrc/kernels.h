@@ -45,6 +45,7 @@ struct BinColumn {
     uint32_t n_cats;      // categorical: number of categories
     uint32_t nan_bin;     // bin of NaN
     uint32_t zero_bin;    // bin of 0.0 when missing type is Zero, else 0xFFFFFFFF
+    uint32_t src;         // the column's row in the feature-major input
 };
 
 // thr holds, per numeric column, the largest f32 <= each f64 upper bound, so

@@ -46,6 +46,12 @@ typedef int32_t bst_status;
 const char* bst_last_error(void);
 /* Library version string. */
 const char* bst_version(void);
+/* Device buffers released by the library (after a training call, a
+ * server, a prediction) are kept per device for reuse, up to the
+ * environment variable BST_DEVICE_CACHE_BYTES (default 8 GiB); this frees
+ * them, e.g. before another allocator on the same GPU needs the memory.
+ * No reference counterpart. */
+void bst_release_cached_memory(void);
 
 /* ------------------------------------------------------------------------ */
 /* Configuration  (model/gbdt/config.rs:111-226 GBDTConfig,                 */
