@@ -326,8 +326,9 @@ bst_status plan_binning(const float* x, uint64_t F, uint64_t n,
         // storage / EFB bundles, which the GPU engine does not implement.
         if (facts[f].sparse || (cfg.enable_bundling && facts[f].bundle_candidate)) {
             err = "feature " + std::to_string(f) +
-                  " has density <= 1 - sparsity_threshold and would use sparse storage, "
-                  "which the GPU engine does not support";
+                  " has density <= 1 - sparsity_threshold and would use sparse storage or a bundle, "
+                  "which the GPU engine does not support; sparsity_threshold = 1 and enable_bundling = 0 "
+                  "train it as a dense column";
             return BST_ERR_UNSUPPORTED;
         }
         const Mapper& m = plan.mappers[f];

@@ -381,3 +381,21 @@ def test_training_is_deterministic():
         for k in STRUCT_KEYS + ["threshold", "leaf_value", "gain", "grad_sum", "hess_sum"]:
             np.testing.assert_array_equal(ta[k], tb[k])
     np.testing.assert_array_equal(a.train_predictions(), b.train_predictions())
+
+
+def test_sparse_column_dense_semantics():
+    """A column of density <= 1 - sparsity_threshold would go to sparse
+    storage in the reference (feature_analysis.rs:655-751), which the engine
+    rejects; with sparsity_threshold = 1 and bundling off it is a dense
+    column, and the trees match the oracle's."""
+    from boosters_b200 import _native as n
+    rng = np.random.default_rng(71)
+    x, y = bst.synth.regression(6000, 10, 4, seed=71)
+    x[3] = np.where(rng.random(6000) < 0.05, rng.normal(size=6000), 0.0).astype(np.float32)  # 95% zeros
+    with pytest.raises(n.BoostersError) as ei:
+        bst.GBDTModel.train(bst.Dataset.from_feature_major(x, y), _cfg(n_estimators=2))
+    assert ei.value.status == n.BST_ERR_UNSUPPORTED and "sparsity_threshold" in str(ei.value)
+    gm, om, _ = train_both(x, y, n_estimators=4, learning_rate=0.3, max_depth=5, sparsity_threshold=1.0,
+                           enable_bundling=False)
+    compare_trees(gm, om, 6000)
+    assert any(3 in gm.tree(i)["split_index"][gm.tree(i)["is_leaf"] == 0] for i in range(gm.n_trees))
