@@ -1472,6 +1472,12 @@ class Trainer {
         LeafParams lp{(double)cfg_.lambda, (double)cfg_.alpha, (double)cfg_.min_gain, cfg_.learning_rate, 0u};
         launches = 0;
         hist_launches = 0;
+        // level kernels get no more blocks than their level can have work
+        // items (idle blocks would still take part in the last-block
+        // hand-off): split searches 2^(d+1) nodes x column blocks,
+        // partitions n / chunk + 2^d chunks, leaf kernels n / chunk + leaves
+        const uint64_t cb = scan_col_blocks(n_cols_);
+        auto cap = [&](uint64_t items) { return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(g_wide, items)); };
         tm.begin(PH_OTHER);
         launch_iota(ridx_.p, n_, st_);
         launch_b_root(bd_, n_, st_);
@@ -1481,7 +1487,7 @@ class Trainer {
         enqueue_hist(gh, ridx_.p, true, tm, launches, hist_launches, true);
         tm.begin(PH_SCAN);
         launch_b_scan(bd_, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p, d_node_tot_.p, 0,
-                      last_wins_ ? 1 : 0, lp, 0u, g_wide, st_, hist32_, d_root_scan_.p,
+                      last_wins_ ? 1 : 0, lp, 0u, cap(cb), st_, hist32_, d_root_scan_.p,
                       colmask());  // + level-0 decisions
         tm.end();
         launches += 4;
@@ -1497,7 +1503,7 @@ class Trainer {
             void* qout = qpos_[(d + 1) & 1u].p;  // the last level's node sums read it too
             tm.begin(PH_PART);
             launch_b_partition(bd_, R[d & 1u], rout, b_.bins8, p_.s8, b_.bins16, p_.s16, a, need_split ? 1 : 0,
-                               g_wide, qin, qout, qmode_, fm_, st_);  // + children
+                               cap(n_ / B_PART_CHUNK + (1ull << d) + 1), qin, qout, qmode_, fm_, st_);  // + children
             tm.end();
             launches += 1;
             if (need_split) {
@@ -1513,7 +1519,7 @@ class Trainer {
                 enqueue_hist(gl, rout, false, tm, launches, hist_launches, (1u << std::min(d, 31u)) <= WIDE_MERGE_NODES);
                 tm.begin(PH_SCAN);
                 launch_b_scan(bd_, scan_cols_.p, n_cols_, hist_.p, slot_bins_, scale, gp_, d_cand_.p,
-                              d_node_tot_.p, a ^ 1, last_wins_ ? 1 : 0, lp, (d + 1) & 1u, g_wide, st_, hist32_,
+                              d_node_tot_.p, a ^ 1, last_wins_ ? 1 : 0, lp, (d + 1) & 1u, cap((2ull << d) * cb), st_, hist32_,
                               nullptr, colsample_ ? d_colmask_.p + (size_t)(d + 1) * n_cols_ : nullptr);
                 // + column reduction, next level's decisions
                 tm.end();
@@ -1531,7 +1537,8 @@ class Trainer {
         launch_b_finalize(bd_, (int)(cfg_.max_depth & 1u), lp, scale, cfg_.max_depth & 1u, st_);
         if (qmode_ != GRAD_F32) {
             // leaves solved from the exact sums of the f32 gradients (+ values)
-            launch_b_leaf_sums(bd_, R[0], R[1], exact_ref(o), lp, scales_.p + 4 * (size_t)o, g_wide, st_);
+            launch_b_leaf_sums(bd_, R[0], R[1], exact_ref(o), lp, scales_.p + 4 * (size_t)o,
+                               cap(n_ / B_LEAF_CHUNK + (1ull << cfg_.max_depth) + 1), st_);
             launches += 1;
         }
         if (renew_) {
@@ -1539,7 +1546,8 @@ class Trainer {
                               cfg_.learning_rate, g_wide, st_);
             launches += ds_.has_w ? 1 : 12;
         }
-        launch_b_leaf_update(bd_, R[0], R[1], pred, cfg_.record_leaves ? row_leaf_.p : nullptr, g_wide, st_);
+        launch_b_leaf_update(bd_, R[0], R[1], pred, cfg_.record_leaves ? row_leaf_.p : nullptr,
+                             cap(n_ / B_LEAF_CHUNK + (1ull << cfg_.max_depth) + 1), st_);
         tm.end();
         launches += 2;
     }

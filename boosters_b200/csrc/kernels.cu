@@ -3506,6 +3506,8 @@ k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HB*
     decide_body(d, b, lp, scale, buf);
 }
 
+uint32_t scan_col_blocks(uint32_t n_cols) { return (n_cols + SCAN_WARPS - 1) / SCAN_WARPS; }
+
 void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const void* hist, uint64_t slot_bins,
                    const double* scale, GainParamsDev gp, ColCand* cand, long long* node_tot, int b, int last_wins,
                    LeafParams lp, uint32_t buf, uint32_t grid, cudaStream_t st, int hist32, const ScanNode* root,

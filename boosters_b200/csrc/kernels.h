@@ -478,6 +478,8 @@ void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const
 // last level: the smaller children's sums, then (last block) both children's
 // sums into frontier b
 void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, int b, uint32_t grid, cudaStream_t st);
+// work items of k_b_scan per node (column blocks of its warps)
+uint32_t scan_col_blocks(uint32_t n_cols);
 void launch_b_finalize(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st);
 // quantised training: exact leaf sums of the f32 gradients (gr: GRAD_F32),
 // then (last block) the leaf values with their fixed-point scale
