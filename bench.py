@@ -624,15 +624,16 @@ def run_profile(args):
     import boosters_b200 as bst
     from boosters_b200 import _native as n
     if args.profile == "train" and args.workload == "leafwise10M":
-        # 10,000,000 x 200 logistic, leaf-wise 255 leaves
-        x, y = bst.synth.binary(10_000_000, 200, 20, seed=3)
+        # 10,000,000 x 200 logistic, leaf-wise 255 leaves (--train-rows: a
+        # smaller row count of the same generator, for full captures)
+        x, y = bst.synth.binary(args.train_rows or 10_000_000, 200, 20, seed=3)
         ds = bst.Dataset.from_feature_major(x, y)
         cfg = bst.GBDTConfig(objective=bst.Objective.logistic(), n_estimators=100, learning_rate=0.1,
                              growth_strategy=bst.GrowthStrategy.Leafwise, n_leaves=255, metric=bst.Metric.none(),
                              **dict(FORMS)[args.form])
     elif args.profile == "train" and args.workload == "softmax2M":
         # 2,000,000 x 50 (10 categorical) softmax, 10 classes, depth 6
-        x, y = bst.synth.multiclass(2_000_000, 40, 10, 10, seed=4)
+        x, y = bst.synth.multiclass(args.train_rows or 2_000_000, 40, 10, 10, seed=4)
         ds = bst.Dataset.from_feature_major(x, y, categorical_features=list(range(40, 50)))
         cfg = bst.GBDTConfig(objective=bst.Objective.softmax(10), n_estimators=200, max_depth=6, learning_rate=0.1,
                              max_onehot_cats=4, metric=bst.Metric.none(), **dict(FORMS)[args.form])
@@ -695,6 +696,8 @@ def main():
     ap.add_argument("--workload", default="1M", choices=["1M", "leafwise10M", "softmax2M"],
                     help="profile train: the 1M x 100 depth-8 workload, the 10M x 200 leaf-wise one or the "
                          "2M x 50 softmax one")
+    ap.add_argument("--train-rows", type=int, default=0,
+                    help="profile train: rows of the leafwise10M / softmax2M workloads (0: their full size)")
     ap.add_argument("--trees", type=int, default=1000)
     ap.add_argument("--rows", type=int, default=300_000)
     args = ap.parse_args()

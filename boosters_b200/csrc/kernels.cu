@@ -3292,17 +3292,37 @@ k_lw_partition(BDev d, const uint32_t* __restrict__ ridx, uint32_t* __restrict__
 
 // The partitioned rows (and gradient elements) back into the row buffer:
 // chunk c copies its 2048 positions of its node's range.
+constexpr uint32_t LW_COPY_THREADS = 256;
+
 template <typename Q>
-__global__ void k_lw_copy_back(BDev d, const uint32_t* __restrict__ tmp, uint32_t* __restrict__ ridx,
+__global__ void __launch_bounds__(LW_COPY_THREADS) k_lw_copy_back(BDev d, const uint32_t* __restrict__ tmp, uint32_t* __restrict__ ridx,
                                const Q* __restrict__ qtmp, Q* __restrict__ q) {
     const uint32_t total = min(d.state->part_chunks, d.max_part_chunks);
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
         const uint2 m = d.part_map[c];
         const PartWork w = d.pworks[m.x];
         const uint32_t len = min(B_PART_CHUNK, w.begin + w.count - m.y);
-        for (uint32_t i = threadIdx.x; i < len; i += blockDim.x) {
-            ridx[m.y + i] = tmp[m.y + i];
-            if constexpr (!std::is_same<Q, char>::value) q[m.y + i] = qtmp[m.y + i];
+        // all of a thread's loads before its stores (launched with
+        // LW_COPY_THREADS threads: U positions per thread cover a chunk)
+        constexpr uint32_t U = B_PART_CHUNK / LW_COPY_THREADS;
+        static_assert(B_PART_CHUNK % LW_COPY_THREADS == 0, "whole chunks");
+        uint32_t rv[U];
+        Q qv[std::is_same<Q, char>::value ? 1 : U];
+#pragma unroll
+        for (uint32_t u = 0; u < U; ++u) {
+            const uint32_t i = threadIdx.x + u * LW_COPY_THREADS;
+            if (i < len) {
+                rv[u] = tmp[m.y + i];
+                if constexpr (!std::is_same<Q, char>::value) qv[u] = qtmp[m.y + i];
+            }
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < U; ++u) {
+            const uint32_t i = threadIdx.x + u * LW_COPY_THREADS;
+            if (i < len) {
+                ridx[m.y + i] = rv[u];
+                if constexpr (!std::is_same<Q, char>::value) q[m.y + i] = qv[u];
+            }
         }
     }
 }
@@ -3312,7 +3332,7 @@ static void lw_partition_t(const BDev& d, uint32_t* rin, uint32_t* rout, const u
                            const uint16_t* bins16, uint32_t s16, uint32_t grid, Q* qin, Q* qout, const BinsFM& fm,
                            cudaStream_t st) {
     k_lw_partition<Q><<<grid, PART_THREADS, 0, st>>>(d, rin, rout, bins8, s8, bins16, s16, qin, qout, fm);
-    k_lw_copy_back<Q><<<grid, 256, 0, st>>>(d, rout, rin, qout, qin);
+    k_lw_copy_back<Q><<<grid, LW_COPY_THREADS, 0, st>>>(d, rout, rin, qout, qin);
 }
 
 void launch_lw_partition(const BDev& d, uint32_t* rin, uint32_t* rout, const uint8_t* bins8, uint32_t s8,
