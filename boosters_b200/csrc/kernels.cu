@@ -2442,8 +2442,11 @@ void launch_b_root(const BDev& d, uint64_t n, cudaStream_t st) { k_b_root<<<1, 3
 // in allocation order (mutable_tree.rs:105-164), partition work lists.
 // buf: which row-index buffer holds the rows of this level's nodes (the
 // leaves made here keep their rows there).
+constexpr uint32_t DECIDE_THREADS = SCAN_WARPS * 32;  // the block size of its one caller, k_b_scan
+
 __device__ void decide_body(BDev d, int a, LeafParams lp, const double* __restrict__ scale, uint32_t buf) {
     __shared__ uint32_t sh[33];
+    __shared__ uint32_t s_jc[DECIDE_THREADS], s_j[DECIDE_THREADS], s_begin[DECIDE_THREADS];
     __shared__ uint32_t base_exp, base_leaf, base_chunk, first_right, tn0, nf;
     BState* s = d.state;
     if (threadIdx.x == 0) {
@@ -2520,16 +2523,29 @@ __device__ void decide_body(BDev d, int a, LeafParams lp, const double* __restri
             w.pad = 0;
             for (int q = 0; q < 4; ++q) w.cats[q] = nd.split.cats[q];
             d.pworks[j] = w;
-            // the partition's chunks of this node, so that each partition
-            // block finds its node with one load (capacity: rows / chunk +
-            // nodes, never exceeded)
-            for (uint32_t k = 0; k < nch; ++k) {
-                const uint32_t c = base_chunk + jc + k;
-                if (c < d.max_part_chunks) d.part_map[c] = make_uint2(j, nd.begin + k * B_PART_CHUNK);
-            }
             d.cursors[2 * j] = nd.begin;
             d.cursors[2 * j + 1] = nd.begin + nd.count;
             if (d.rmask) d.scnt[2 * j] = d.scnt[2 * j + 1] = 0u;
+        }
+        // the partition's chunks of the tile's expanding nodes, so that each
+        // partition block finds its node with one load (capacity: rows /
+        // chunk + nodes, never exceeded), written by all threads: chunk c of
+        // the tile belongs to the last thread whose first chunk is <= c
+        s_jc[threadIdx.x] = jc;
+        s_j[threadIdx.x] = base_exp + je;
+        s_begin[threadIdx.x] = valid ? nd.begin : 0u;
+        __syncthreads();
+        for (uint32_t c = threadIdx.x; c < tc; c += blockDim.x) {
+            uint32_t lo = 0, hi = blockDim.x;  // s_jc[lo] <= c < s_jc[hi]
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (s_jc[mid] <= c)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            const uint32_t g = base_chunk + c;
+            if (g < d.max_part_chunks) d.part_map[g] = make_uint2(s_j[lo], s_begin[lo] + (c - s_jc[lo]) * B_PART_CHUNK);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
