@@ -2666,8 +2666,31 @@ void launch_transpose_bins(const uint8_t* b8, uint32_t s8, uint32_t f8, const ui
 // Children of every split: ranges from the partition cursors, smaller child
 // (grower.rs:398-402), next frontier in (left, right) order, histogram or
 // node-sum work over the smaller children.
+// map[base + c] = the owner of segment c of a tile, for c < tc, written by
+// all threads: thread t owns the segments from jc (exclusive scan over the
+// tile's threads) on; the owner of c is the last thread whose jc is <= c.
+// s_jc / s_own: shared arrays of blockDim entries.
+__device__ void write_segment_owners(uint32_t* map, uint32_t cap, uint32_t base, uint32_t jc, uint32_t owner,
+                                     uint32_t tc, uint32_t* s_jc, uint32_t* s_own) {
+    s_jc[threadIdx.x] = jc;
+    s_own[threadIdx.x] = owner;
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < tc; c += blockDim.x) {
+        uint32_t lo = 0, hi = blockDim.x;  // s_jc[lo] <= c < s_jc[hi]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (s_jc[mid] <= c)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        if (base + c < cap) map[base + c] = s_own[lo];
+    }
+}
+
 __device__ void children_body(BDev d, int a, int need_split) {
     __shared__ uint32_t sh[33];
+    __shared__ uint32_t s_jc[PART_THREADS], s_own[PART_THREADS];  // block size of its caller, k_b_partition
     __shared__ uint32_t base, n_exp, chunk;
     __shared__ unsigned long long rows;
     BState* s = d.state;
@@ -2739,13 +2762,9 @@ __device__ void children_body(BDev d, int a, int need_split) {
         const uint32_t nch = valid ? (d.exp[j].small_count + chunk - 1) / chunk : 0u;
         uint32_t tc;
         const uint32_t jc = block_excl_scan(nch, sh, &tc);
-        if (valid) {
-            d.exp[j].hist_off = base + jc;
-            // segment -> expansion, written by the segment's owner (the
-            // buffer bound always holds)
-            for (uint32_t k = 0; k < nch; ++k)
-                if (base + jc + k < d.max_segs) d.seg_exp[base + jc + k] = j;
-        }
+        if (valid) d.exp[j].hist_off = base + jc;
+        // segment -> expansion (the buffer bound always holds)
+        write_segment_owners(d.seg_exp, d.max_segs, base, jc, j, tc, s_jc, s_own);
         __syncthreads();
         if (threadIdx.x == 0) base += tc;
         __syncthreads();
@@ -2773,6 +2792,7 @@ __global__ void __launch_bounds__(1024) k_lw_children(BDev d, const PartWork* __
                                                      ScanNode* __restrict__ scan_nodes,
                                                      const unsigned* __restrict__ scnt) {
     __shared__ uint32_t sh[33];
+    __shared__ uint32_t s_jc[1024], s_own[1024];
     __shared__ unsigned long long rows;
     __shared__ uint32_t chunk, base;
     const bool from_state = k == LW_K_FROM_STATE;
@@ -2815,11 +2835,8 @@ __global__ void __launch_bounds__(1024) k_lw_children(BDev d, const PartWork* __
         const uint32_t nch = valid ? (d.exp[j].small_count + chunk - 1) / chunk : 0u;
         uint32_t tc;
         const uint32_t jc = block_excl_scan(nch, sh, &tc);
-        if (valid) {
-            d.exp[j].hist_off = base + jc;
-            for (uint32_t q = 0; q < nch; ++q)  // segment -> expansion, by the owner
-                if (base + jc + q < d.max_segs) d.seg_exp[base + jc + q] = j;
-        }
+        if (valid) d.exp[j].hist_off = base + jc;
+        write_segment_owners(d.seg_exp, d.max_segs, base, jc, j, tc, s_jc, s_own);  // segment -> expansion
         __syncthreads();
         if (threadIdx.x == 0) base += tc;
         __syncthreads();
