@@ -2688,6 +2688,28 @@ __device__ void write_segment_owners(uint32_t* map, uint32_t cap, uint32_t base,
     }
 }
 
+// The same for chunk maps of rows: map[base + c] = (owner, its first row
+// + (c - its jc) x chunk rows). s_begin: a third shared array.
+__device__ void write_chunk_owners(uint2* map, uint32_t cap, uint32_t base, uint32_t jc, uint32_t owner,
+                                   uint32_t begin, uint32_t chunk, uint32_t tc, uint32_t* s_jc, uint32_t* s_own,
+                                   uint32_t* s_begin) {
+    s_jc[threadIdx.x] = jc;
+    s_own[threadIdx.x] = owner;
+    s_begin[threadIdx.x] = begin;
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < tc; c += blockDim.x) {
+        uint32_t lo = 0, hi = blockDim.x;  // s_jc[lo] <= c < s_jc[hi]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (s_jc[mid] <= c)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        if (base + c < cap) map[base + c] = make_uint2(s_own[lo], s_begin[lo] + (c - s_jc[lo]) * chunk);
+    }
+}
+
 __device__ void children_body(BDev d, int a, int need_split) {
     __shared__ uint32_t sh[33];
     __shared__ uint32_t s_jc[PART_THREADS], s_own[PART_THREADS];  // block size of its caller, k_b_partition
@@ -3388,6 +3410,7 @@ void launch_lw_partition(const BDev& d, uint32_t* rin, uint32_t* rout, const uin
 // leaf sums zeroed for the quantised forms' exact leaf solve.
 __global__ void __launch_bounds__(1024) k_lw_leaves(BDev d) {
     __shared__ uint32_t sh[33];
+    __shared__ uint32_t s_jc[1024], s_own[1024], s_begin[1024];
     __shared__ uint32_t base;
     BState* s = d.state;
     const uint32_t nl = s->n_leaves;
@@ -3399,12 +3422,9 @@ __global__ void __launch_bounds__(1024) k_lw_leaves(BDev d) {
         const uint32_t nch = l < nl ? (d.leaves[l].count + B_LEAF_CHUNK - 1) / B_LEAF_CHUNK : 0u;
         uint32_t tc;
         const uint32_t jc = block_excl_scan(nch, sh, &tc);
-        if (l < nl) {
-            d.leaves[l].chunk_off = base + jc;
-            for (uint32_t k = 0; k < nch; ++k)
-                if (base + jc + k < d.max_leaf_chunks)
-                    d.leaf_map[base + jc + k] = make_uint2(l, begin + k * B_LEAF_CHUNK);
-        }
+        if (l < nl) d.leaves[l].chunk_off = base + jc;
+        // chunk -> (leaf, first row)
+        write_chunk_owners(d.leaf_map, d.max_leaf_chunks, base, jc, l, begin, B_LEAF_CHUNK, tc, s_jc, s_own, s_begin);
         __syncthreads();
         if (threadIdx.x == 0) base += tc;
         __syncthreads();
@@ -3661,6 +3681,7 @@ __device__ void children_sums_body(BDev d, int b) {
 __global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams lp, const double* __restrict__ scale,
                                                     uint32_t buf) {
     __shared__ uint32_t sh[33];
+    __shared__ uint32_t s_jc[1024], s_own[1024], s_begin[1024];
     __shared__ uint32_t base, nf, n0;
     BState* s = d.state;
     if (threadIdx.x == 0) {
@@ -3691,12 +3712,9 @@ __global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams l
         const uint32_t nch = l < nl ? (d.leaves[l].count + B_LEAF_CHUNK - 1) / B_LEAF_CHUNK : 0u;
         uint32_t tc;
         const uint32_t jc = block_excl_scan(nch, sh, &tc);
-        if (l < nl) {
-            d.leaves[l].chunk_off = base + jc;
-            for (uint32_t k = 0; k < nch; ++k)  // chunk -> (leaf, first row), by the leaf's owner
-                if (base + jc + k < d.max_leaf_chunks)
-                    d.leaf_map[base + jc + k] = make_uint2(l, begin + k * B_LEAF_CHUNK);
-        }
+        if (l < nl) d.leaves[l].chunk_off = base + jc;
+        // chunk -> (leaf, first row)
+        write_chunk_owners(d.leaf_map, d.max_leaf_chunks, base, jc, l, begin, B_LEAF_CHUNK, tc, s_jc, s_own, s_begin);
         __syncthreads();
         if (threadIdx.x == 0) base += tc;
         __syncthreads();
