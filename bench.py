@@ -464,7 +464,7 @@ def run_ours(args, world, rank, local):
     e2e_cfg = bst.GBDTConfig(device=local, **dict(kw, n_estimators=100, **head_over))
     xh = torch.from_numpy(x).pin_memory().numpy()
     yh = torch.from_numpy(y).pin_memory().numpy()
-    e2e_steps = max(1, min(args.steps, 2))
+    e2e_steps = max(1, min(args.steps, 5))
     bst.GBDTModel.train(bst.Dataset.from_feature_major(xh, yh), e2e_cfg)  # warm-up call
     barrier(world)
     te0 = time.perf_counter()

@@ -11,6 +11,7 @@
 
 
 #include <type_traits>
+#include <utility>
 
 #include "kernels.h"
 
@@ -38,6 +39,48 @@ uint32_t sm_count() {
 namespace {
 
 constexpr unsigned FULL = 0xFFFFFFFFu;
+
+// Programmatic dependent launch. Every kernel is launched with programmatic
+// stream serialisation and begins with BST_PDL_ENTER: griddepcontrol.wait
+// holds the kernel's threads until the kernel before it in the stream has
+// completed and its memory writes are visible (for a kernel launched without
+// the attribute it returns at once), so kernel bodies still run strictly in
+// stream order. No kernel triggers its dependents early (the trigger is
+// implicit at block exit): the next kernel's launch overlaps only this
+// kernel's completion, and its blocks are placed on SMs as a whole grid
+// (the one-wave grids count on one block per SM slot).
+#define BST_PDL_ENTER() asm volatile("griddepcontrol.wait;" ::: "memory")
+
+template <typename... P, typename... A>
+inline void launch_k(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... args) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t c = {};
+    c.gridDim = grid;
+    c.blockDim = block;
+    c.dynamicSmemBytes = smem;
+    c.stream = st;
+    c.attrs = at;
+    c.numAttrs = 1;
+    cudaLaunchKernelEx(&c, k, std::forward<A>(args)...);  // errors: the caller's next check
+}
+
+// The same for a kernel chosen at run time (argument pointers as for
+// cudaLaunchKernel).
+inline void launch_kv(const void* k, dim3 grid, dim3 block, void** args, size_t smem, cudaStream_t st) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t c = {};
+    c.gridDim = grid;
+    c.blockDim = block;
+    c.dynamicSmemBytes = smem;
+    c.stream = st;
+    c.attrs = at;
+    c.numAttrs = 1;
+    cudaLaunchKernelExC(&c, k, args);
+}
 
 
 __device__ __forceinline__ int32_t sat_i32(double v) {
@@ -77,6 +120,7 @@ __global__ void __launch_bounds__(128)
 k_bin_assign(const float* __restrict__ x, uint64_t n, const BinColumn* __restrict__ cols,
              uint32_t n_cols, const float* __restrict__ thr, const int32_t* __restrict__ cats,
              uint8_t* __restrict__ rec_out, uint32_t rec, uint32_t u16_off) {
+    BST_PDL_ENTER();
     // one thread per row of a tile of blockDim.x rows; the tile's records are
     // assembled in shared memory, then copied out as one contiguous run
     extern __shared__ __align__(16) unsigned char smem[];
@@ -153,7 +197,7 @@ void launch_bin_assign(const float* x_fm, uint64_t n, const BinColumn* cols, uin
     const size_t smem = (size_t)rows * rec;
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_bin_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    k_bin_assign<<<(unsigned)blocks, rows, smem, st>>>(x_fm, n, cols, n_cols, thr, cats, rec_out, rec, u16_off);
+    launch_k(k_bin_assign, (unsigned)blocks, rows, smem, st, x_fm, n, cols, n_cols, thr, cats, rec_out, rec, u16_off);
 }
 
 // ============================================================================
@@ -179,6 +223,7 @@ __global__ void k_gradients(int objective, uint32_t G, const float* __restrict__
                             const float* __restrict__ y, const float* __restrict__ w, uint64_t n,
                             float2* __restrict__ gh, unsigned* __restrict__ maxabs,
                             const float* __restrict__ alpha, float delta) {
+    BST_PDL_ENTER();
     extern __shared__ unsigned smax[];  // [2G]
     const float HESS_MIN = 1e-6f;
     for (uint32_t i = threadIdx.x; i < 2 * G; i += blockDim.x) smax[i] = 0u;
@@ -283,6 +328,7 @@ __global__ void k_gradients(int objective, uint32_t G, const float* __restrict__
 }
 
 __global__ void k_maxabs(const float2* __restrict__ gh, uint64_t n, unsigned* __restrict__ maxabs) {
+    BST_PDL_ENTER();
     __shared__ unsigned smax[2];
     if (threadIdx.x < 2) smax[threadIdx.x] = 0u;
     __syncthreads();
@@ -307,7 +353,7 @@ void launch_maxabs(const float2* gh, uint64_t n, unsigned* maxabs, cudaStream_t 
     if (n == 0) return;
     uint64_t blocks = (n + 255) / 256;
     if (blocks > (uint64_t)sm_count() * 8) blocks = (uint64_t)sm_count() * 8;
-    k_maxabs<<<(unsigned)blocks, 256, 0, st>>>(gh, n, maxabs);
+    launch_k(k_maxabs, (unsigned)blocks, 256, 0, st, gh, n, maxabs);
 }
 
 void launch_gradients(int objective, uint32_t G, const float* pred, const float* y,
@@ -316,12 +362,13 @@ void launch_gradients(int objective, uint32_t G, const float* pred, const float*
     if (n == 0) return;
     uint64_t blocks = (n + 255) / 256;
     if (blocks > (uint64_t)sm_count() * 8) blocks = (uint64_t)sm_count() * 8;
-    k_gradients<<<(unsigned)blocks, 256, 2 * G * sizeof(unsigned), st>>>(objective, G, pred, y, w, n, gh, maxabs,
+    launch_k(k_gradients, (unsigned)blocks, 256, 2 * G * sizeof(unsigned), st, objective, G, pred, y, w, n, gh, maxabs,
                                                                           alpha, delta);
 }
 
 __global__ void k_fixed_scales(const unsigned* __restrict__ maxabs, uint32_t G, uint64_t n,
                                double* __restrict__ scales) {
+    BST_PDL_ENTER();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 2 * G) return;
     const float m = __uint_as_float(maxabs[i]);
@@ -346,7 +393,7 @@ __global__ void k_fixed_scales(const unsigned* __restrict__ maxabs, uint32_t G, 
 
 void launch_fixed_scales(const unsigned* maxabs, uint32_t G, uint64_t n, double* scales,
                          cudaStream_t st) {
-    k_fixed_scales<<<(2 * G + 63) / 64, 64, 0, st>>>(maxabs, G, n, scales);
+    launch_k(k_fixed_scales, (2 * G + 63) / 64, 64, 0, st, maxabs, G, n, scales);
 }
 
 // ============================================================================
@@ -1094,6 +1141,7 @@ __global__ void __launch_bounds__(lane_threads(MODE, V), lane_min_blocks(MODE, V
 k_b_hist_part(BDev d, const LaneTile* __restrict__ tiles, uint32_t n_tiles, const uint32_t* __restrict__ ridx,
               GradRef gr, const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16,
               uint32_t s16, void* __restrict__ part) {
+    BST_PDL_ENTER();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);
     uint8_t* stage = smem_raw + acc_words(MODE) * LANE_ROWS * 32u * 4u;
@@ -1121,6 +1169,7 @@ __global__ void __launch_bounds__(lane_threads(MODE, 3), lane_min_blocks(MODE, 3
 k_b_hist_part_tma(BDev d, const LaneTile* __restrict__ tiles, uint32_t n_tiles, const uint32_t* __restrict__ ridx,
                   GradRef gr, uint32_t n_rows, void* __restrict__ part, const __grid_constant__ CUtensorMap m32,
                   const __grid_constant__ CUtensorMap m16) {
+    BST_PDL_ENTER();
     extern __shared__ __align__(128) unsigned char smem_raw[];
     constexpr uint32_t NW = acc_words(MODE);
     constexpr uint32_t plane = LANE_ROWS * 32u;
@@ -1287,12 +1336,12 @@ void launch_b_hist_part(const BDev& d, const LaneTile* tiles, uint32_t n_tiles, 
         const CUtensorMap& m16 = *reinterpret_cast<const CUtensorMap*>(maps->box16);
         void* targs[] = {(void*)&d,  (void*)&tiles, (void*)&n_tiles, (void*)&ridx, (void*)&gr,
                          (void*)&n_rows, (void*)&part, (void*)&m32, (void*)&m16};
-        cudaLaunchKernel(lane_kernel_of(gr.mode, v), dim3(g), dim3(th), targs, smem, st);  // errors: next check
+        launch_kv(lane_kernel_of(gr.mode, v), dim3(g), dim3(th), targs, smem, st);  // errors: next check
         return;
     }
     void* args[] = {(void*)&d,    (void*)&tiles, (void*)&n_tiles, (void*)&ridx,   (void*)&gr,
                     (void*)&bins8, (void*)&s8,   (void*)&bins16,  (void*)&s16,    (void*)&part};
-    cudaLaunchKernel(lane_kernel_of(gr.mode, v), dim3(g), dim3(th), args, smem, st);  // errors: next check
+    launch_kv(lane_kernel_of(gr.mode, v), dim3(g), dim3(th), args, smem, st);  // errors: next check
 }
 
 // The subtraction trick (pool.rs:414-432) for one global bin of node e:
@@ -1332,6 +1381,7 @@ template <int MODE, typename HB>
 __global__ void __launch_bounds__(256, 4)
 k_b_merge(BDev d, HB* __restrict__ hist, uint64_t slot_bins, const void* __restrict__ part, uint32_t n_tiles,
           const uint2* __restrict__ ent, uint32_t n_ent, int root) {
+    BST_PDL_ENTER();
     using E = typename PartEntry<MODE>::T;
     const E* P = reinterpret_cast<const E*>(part);
     const uint32_t n_exp = d.state->n_exp, n_seg = d.state->hist_chunks;
@@ -1404,6 +1454,7 @@ template <int MODE, typename HB>
 __global__ void __launch_bounds__(MW_E * MW_G)
 k_b_merge_wide(BDev d, HB* __restrict__ hist, uint64_t slot_bins, const void* __restrict__ part, uint32_t n_tiles,
                const uint2* __restrict__ ent, uint32_t n_ent, int root) {
+    BST_PDL_ENTER();
     using E = typename PartEntry<MODE>::T;
     __shared__ long long s_g[MW_G][MW_E], s_h[MW_G][MW_E];
     const E* P = reinterpret_cast<const E*>(part);
@@ -1462,6 +1513,7 @@ k_b_merge_wide(BDev d, HB* __restrict__ hist, uint64_t slot_bins, const void* __
 template <typename HB>
 __global__ void k_b_merge_rest(BDev d, HB* __restrict__ hist, uint64_t slot_bins, uint32_t total_bins,
                                const uint32_t* __restrict__ bin_map, int root) {
+    BST_PDL_ENTER();
     const uint32_t n_exp = d.state->n_exp;
     const uint64_t n = (uint64_t)n_exp * total_bins;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -1480,18 +1532,18 @@ static void launch_b_merge_t(const BDev& d, HB* hist, uint64_t slot_bins, uint32
     if (n_lane_tiles) {
         if (wide) {
             if (mode == GRAD_F32)
-                k_b_merge_wide<GRAD_F32, HB><<<grid, MW_E * MW_G, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles,
+                launch_k(k_b_merge_wide<GRAD_F32, HB>, grid, MW_E * MW_G, 0, st, d, hist, slot_bins, part, n_lane_tiles,
                                                                           ent, n_ent, root);
             else
-                k_b_merge_wide<GRAD_Q8, HB><<<grid, MW_E * MW_G, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles,
+                launch_k(k_b_merge_wide<GRAD_Q8, HB>, grid, MW_E * MW_G, 0, st, d, hist, slot_bins, part, n_lane_tiles,
                                                                          ent, n_ent, root);
         } else if (mode == GRAD_F32) {
-            k_b_merge<GRAD_F32, HB><<<grid, 256, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles, ent, n_ent, root);
+            launch_k(k_b_merge<GRAD_F32, HB>, grid, 256, 0, st, d, hist, slot_bins, part, n_lane_tiles, ent, n_ent, root);
         } else {
-            k_b_merge<GRAD_Q8, HB><<<grid, 256, 0, st>>>(d, hist, slot_bins, part, n_lane_tiles, ent, n_ent, root);
+            launch_k(k_b_merge<GRAD_Q8, HB>, grid, 256, 0, st, d, hist, slot_bins, part, n_lane_tiles, ent, n_ent, root);
         }
     }
-    if (has_rest) k_b_merge_rest<HB><<<grid, 256, 0, st>>>(d, hist, slot_bins, total_bins, bin_map, root);
+    if (has_rest) launch_k(k_b_merge_rest<HB>, grid, 256, 0, st, d, hist, slot_bins, total_bins, bin_map, root);
 }
 
 void launch_b_merge(const BDev& d, void* hist, uint64_t slot_bins, uint32_t total_bins, const void* part,
@@ -1508,6 +1560,7 @@ void launch_b_merge(const BDev& d, void* hist, uint64_t slot_bins, uint32_t tota
 // Level state for the root histogram: one "expanding node" whose smaller
 // child is all n rows (ridx is the identity), segments of `chunk` rows.
 __global__ void k_b_root_hist(BDev d, uint64_t n, uint32_t chunk) {
+    BST_PDL_ENTER();
     uint32_t nseg = (uint32_t)((n + chunk - 1) / chunk);
     if (nseg > d.max_segs) nseg = d.max_segs;  // never: the buffer is sized for it
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nseg; c += gridDim.x * blockDim.x) d.seg_exp[c] = 0;
@@ -1532,7 +1585,7 @@ __global__ void k_b_root_hist(BDev d, uint64_t n, uint32_t chunk) {
 }
 
 void launch_b_root_hist(const BDev& d, uint64_t n, uint32_t chunk, cudaStream_t st) {
-    k_b_root_hist<<<4, 256, 0, st>>>(d, n, chunk);
+    launch_k(k_b_root_hist, 4, 256, 0, st, d, n, chunk);
 }
 
 template <int MODE>
@@ -1541,6 +1594,7 @@ k_hist_build(const HistChunk* __restrict__ chunks, const HistTile* __restrict__ 
              const uint32_t* __restrict__ ridx, GradRef gr, const uint8_t* __restrict__ bins8, uint32_t s8,
              const uint16_t* __restrict__ bins16, uint32_t s16, HBin* __restrict__ hist,
              uint64_t slot_bins, uint32_t n_tiles, uint32_t S) {
+    BST_PDL_ENTER();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);
     __shared__ HistTile tile;
@@ -1566,19 +1620,20 @@ void launch_hist_build(const HistChunk* chunks, uint32_t n_chunks, const HistTil
     if (blocks > 0x7FFFFFFFull) return;
     const unsigned g = (unsigned)blocks;
     if (gr.mode == GRAD_Q16)
-        k_hist_build<GRAD_Q16><<<g, HIST_THREADS, smem, st>>>(chunks, tiles, ridx, gr, bins8, s8, bins16, s16, hist,
+        launch_k(k_hist_build<GRAD_Q16>, g, HIST_THREADS, smem, st, chunks, tiles, ridx, gr, bins8, s8, bins16, s16, hist,
                                                                slot_bins, n_tiles, S);
     else if (gr.mode == GRAD_Q8)
-        k_hist_build<GRAD_Q8><<<g, HIST_THREADS, smem, st>>>(chunks, tiles, ridx, gr, bins8, s8, bins16, s16, hist,
+        launch_k(k_hist_build<GRAD_Q8>, g, HIST_THREADS, smem, st, chunks, tiles, ridx, gr, bins8, s8, bins16, s16, hist,
                                                               slot_bins, n_tiles, S);
     else
-        k_hist_build<GRAD_F32><<<g, HIST_THREADS, smem, st>>>(chunks, tiles, ridx, gr, bins8, s8, bins16, s16,
+        launch_k(k_hist_build<GRAD_F32>, g, HIST_THREADS, smem, st, chunks, tiles, ridx, gr, bins8, s8, bins16, s16,
                                                                hist, slot_bins, n_tiles, S);
 }
 
 template <int MODE>
 __global__ void k_node_sums(const HistChunk* __restrict__ chunks, const uint32_t* __restrict__ ridx, GradRef gr,
                             long long* __restrict__ sums) {
+    BST_PDL_ENTER();
     const HistChunk c = chunks[blockIdx.x];
     const GradLoad<MODE> load(gr);
     long long ag = 0, ah = 0;
@@ -1604,11 +1659,11 @@ void launch_node_sums(const HistChunk* chunks, uint32_t n_chunks, const uint32_t
                       long long* sums, cudaStream_t st) {
     if (n_chunks == 0) return;
     if (gr.mode == GRAD_Q16)
-        k_node_sums<GRAD_Q16><<<n_chunks, 256, 0, st>>>(chunks, ridx, gr, sums);
+        launch_k(k_node_sums<GRAD_Q16>, n_chunks, 256, 0, st, chunks, ridx, gr, sums);
     else if (gr.mode == GRAD_Q8)
-        k_node_sums<GRAD_Q8><<<n_chunks, 256, 0, st>>>(chunks, ridx, gr, sums);
+        launch_k(k_node_sums<GRAD_Q8>, n_chunks, 256, 0, st, chunks, ridx, gr, sums);
     else
-        k_node_sums<GRAD_F32><<<n_chunks, 256, 0, st>>>(chunks, ridx, gr, sums);
+        launch_k(k_node_sums<GRAD_F32>, n_chunks, 256, 0, st, chunks, ridx, gr, sums);
 }
 
 // ============================================================================
@@ -1645,6 +1700,7 @@ template <int MODE>
 __global__ void k_quantize(const float2* __restrict__ gh, uint64_t n, uint32_t G, const unsigned* __restrict__ maxabs,
                            uint2 key, uint32_t round, uint32_t out0, void* __restrict__ gq,
                            double* __restrict__ qscales) {
+    BST_PDL_ENTER();
     constexpr int32_t Q = MODE == GRAD_Q8 ? 127 : 32767;
     const uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i0 < 2ull * G) {
@@ -1678,9 +1734,9 @@ void launch_quantize(int mode, uint32_t G, const float2* gh, uint64_t n, const u
     if (blocks == 0) blocks = 1;
     const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     if (mode == GRAD_Q8)
-        k_quantize<GRAD_Q8><<<(unsigned)blocks, 256, 0, st>>>(gh, n, G, maxabs, key, round, out0, gq, qscales);
+        launch_k(k_quantize<GRAD_Q8>, (unsigned)blocks, 256, 0, st, gh, n, G, maxabs, key, round, out0, gq, qscales);
     else
-        k_quantize<GRAD_Q16><<<(unsigned)blocks, 256, 0, st>>>(gh, n, G, maxabs, key, round, out0, gq, qscales);
+        launch_k(k_quantize<GRAD_Q16>, (unsigned)blocks, 256, 0, st, gh, n, G, maxabs, key, round, out0, gq, qscales);
 }
 
 // ============================================================================
@@ -1975,6 +2031,7 @@ k_split_scan(const ScanNode* __restrict__ nodes, const ScanColumn* __restrict__ 
              uint32_t n_cols, const HB* __restrict__ hist, uint64_t slot_bins,
              const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
              long long* __restrict__ node_tot, uint32_t col_blocks, const uint8_t* __restrict__ colmask) {
+    BST_PDL_ENTER();
     __shared__ double s_key[SCAN_WARPS][SORT_N];
     __shared__ uint32_t s_cat[SCAN_WARPS][SORT_N];
     const int warp = threadIdx.x >> 5;
@@ -1995,16 +2052,17 @@ void launch_split_scan(const ScanNode* nodes, uint32_t n_nodes, const ScanColumn
     const uint64_t blocks = (uint64_t)per * n_nodes;
     if (blocks > 0x7FFFFFFFull) return;
     if (hist32)
-        k_split_scan<HBin32><<<(unsigned)blocks, SCAN_WARPS * 32, 0, st>>>(
+        launch_k(k_split_scan<HBin32>, (unsigned)blocks, SCAN_WARPS * 32, 0, st, 
             nodes, cols, n_cols, static_cast<const HBin32*>(hist), slot_bins, scale, gp, cand, node_tot, per, colmask);
     else
-        k_split_scan<HBin><<<(unsigned)blocks, SCAN_WARPS * 32, 0, st>>>(
+        launch_k(k_split_scan<HBin>, (unsigned)blocks, SCAN_WARPS * 32, 0, st, 
             nodes, cols, n_cols, static_cast<const HBin*>(hist), slot_bins, scale, gp, cand, node_tot, per, colmask);
 }
 
 // Across columns (find.rs:180-212 sequential; :219-270 rayon reduce).
 __global__ void k_split_reduce(const ColCand* __restrict__ cand, const long long* __restrict__ node_tot,
                                uint32_t n_cols, int last_wins, NodeSplit* __restrict__ out) {
+    BST_PDL_ENTER();
     const uint32_t node = blockIdx.x;
     const int lane = threadIdx.x;
     float bg = -INFINITY;
@@ -2060,7 +2118,7 @@ __global__ void k_split_reduce(const ColCand* __restrict__ cand, const long long
 void launch_split_reduce(const ColCand* cand, const long long* node_tot, uint32_t n_nodes,
                          uint32_t n_cols, int last_wins, NodeSplit* out, cudaStream_t st) {
     if (n_nodes == 0) return;
-    k_split_reduce<<<n_nodes, 32, 0, st>>>(cand, node_tot, n_cols, last_wins, out);
+    launch_k(k_split_reduce, n_nodes, 32, 0, st, cand, node_tot, n_cols, last_wins, out);
 }
 
 cudaError_t load_split_kernels() {
@@ -2224,6 +2282,7 @@ k_partition(const PartWork* __restrict__ works, const PartChunk* __restrict__ ch
             const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16,
             const Q* __restrict__ qin, Q* __restrict__ qout, BinsFM fm, const uint8_t* __restrict__ rmask,
             unsigned* __restrict__ scnt) {
+    BST_PDL_ENTER();
     const PartChunk ch = chunks[blockIdx.x];
     __shared__ PartWork w;
     if (threadIdx.x == 0) w = works[ch.work];
@@ -2239,18 +2298,18 @@ void launch_partition(const PartWork* works, const PartChunk* chunks, uint32_t n
                       const uint8_t* rmask, unsigned* scnt) {
     if (n_chunks == 0) return;
     if (!qin || !qout)
-        k_partition<char><<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
+        launch_k(k_partition<char>, n_chunks, PART_THREADS, 0, st, works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
                                                              s16, nullptr, nullptr, fm, rmask, scnt);
     else if (mode == GRAD_Q8)
-        k_partition<char2><<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
+        launch_k(k_partition<char2>, n_chunks, PART_THREADS, 0, st, works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
                                                               s16, static_cast<const char2*>(qin),
                                                               static_cast<char2*>(qout), fm, rmask, scnt);
     else if (mode == GRAD_Q16)
-        k_partition<short2><<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
+        launch_k(k_partition<short2>, n_chunks, PART_THREADS, 0, st, works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
                                                                s16, static_cast<const short2*>(qin),
                                                                static_cast<short2*>(qout), fm, rmask, scnt);
     else
-        k_partition<float2><<<n_chunks, PART_THREADS, 0, st>>>(works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
+        launch_k(k_partition<float2>, n_chunks, PART_THREADS, 0, st, works, chunks, ridx, tmp, cursors, bins8, s8, bins16,
                                                                s16, static_cast<const float2*>(qin),
                                                                static_cast<float2*>(qout), fm, rmask, scnt);
 }
@@ -2258,6 +2317,7 @@ void launch_partition(const PartWork* works, const PartChunk* chunks, uint32_t n
 template <typename Q>
 __global__ void k_copy_chunks(const PartChunk* __restrict__ chunks, const uint32_t* __restrict__ src,
                               uint32_t* __restrict__ dst, const Q* __restrict__ qsrc, Q* __restrict__ qdst) {
+    BST_PDL_ENTER();
     const PartChunk ch = chunks[blockIdx.x];
     for (uint32_t i = threadIdx.x; i < ch.len; i += blockDim.x) {
         dst[ch.start + i] = src[ch.start + i];
@@ -2271,19 +2331,20 @@ void launch_copy_chunks(const PartChunk* chunks, const PartWork* works, uint32_t
     (void)works;
     if (n_chunks == 0) return;
     if (!qsrc || !qdst)
-        k_copy_chunks<char><<<n_chunks, 256, 0, st>>>(chunks, src, dst, nullptr, nullptr);
+        launch_k(k_copy_chunks<char>, n_chunks, 256, 0, st, chunks, src, dst, nullptr, nullptr);
     else if (mode == GRAD_Q8)
-        k_copy_chunks<char2><<<n_chunks, 256, 0, st>>>(chunks, src, dst, static_cast<const char2*>(qsrc),
+        launch_k(k_copy_chunks<char2>, n_chunks, 256, 0, st, chunks, src, dst, static_cast<const char2*>(qsrc),
                                                        static_cast<char2*>(qdst));
     else if (mode == GRAD_Q16)
-        k_copy_chunks<short2><<<n_chunks, 256, 0, st>>>(chunks, src, dst, static_cast<const short2*>(qsrc),
+        launch_k(k_copy_chunks<short2>, n_chunks, 256, 0, st, chunks, src, dst, static_cast<const short2*>(qsrc),
                                                         static_cast<short2*>(qdst));
     else
-        k_copy_chunks<float2><<<n_chunks, 256, 0, st>>>(chunks, src, dst, static_cast<const float2*>(qsrc),
+        launch_k(k_copy_chunks<float2>, n_chunks, 256, 0, st, chunks, src, dst, static_cast<const float2*>(qsrc),
                                                         static_cast<float2*>(qdst));
 }
 
 __global__ void k_iota(uint32_t* __restrict__ r, uint64_t n) {
+    BST_PDL_ENTER();
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x)
         r[i] = (uint32_t)i;
@@ -2293,7 +2354,7 @@ void launch_iota(uint32_t* ridx, uint64_t n, cudaStream_t st) {
     if (n == 0) return;
     uint64_t blocks = (n + 255) / 256;
     if (blocks > (uint64_t)sm_count() * 16) blocks = (uint64_t)sm_count() * 16;
-    k_iota<<<(unsigned)blocks, 256, 0, st>>>(ridx, n);
+    launch_k(k_iota, (unsigned)blocks, 256, 0, st, ridx, n);
 }
 
 // ============================================================================
@@ -2303,6 +2364,7 @@ void launch_iota(uint32_t* ridx, uint64_t n, cudaStream_t st) {
 __global__ void k_leaf_update(const LeafSeg* __restrict__ leaves, uint32_t n_leaves,
                               const uint32_t* __restrict__ ridx, uint64_t n, float* __restrict__ pred,
                               uint32_t* __restrict__ row_leaf) {
+    BST_PDL_ENTER();
     for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
          p += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t lo = 0, hi = n_leaves;  // last leaf with begin <= p
@@ -2327,7 +2389,7 @@ void launch_leaf_update(const LeafSeg* leaves, uint32_t n_leaves, const uint32_t
     if (n == 0 || n_leaves == 0) return;
     uint64_t blocks = (n + 255) / 256;
     if (blocks > (uint64_t)sm_count() * 16) blocks = (uint64_t)sm_count() * 16;
-    k_leaf_update<<<(unsigned)blocks, 256, 0, st>>>(leaves, n_leaves, ridx, n, pred, row_leaf);
+    launch_k(k_leaf_update, (unsigned)blocks, 256, 0, st, leaves, n_leaves, ridx, n, pred, row_leaf);
 }
 
 // ============================================================================
@@ -2399,6 +2461,7 @@ __device__ void write_leaf(BTreeNode& t, long long G, long long H, const double*
 }  // namespace
 
 __global__ void k_b_root(BDev d, uint64_t n) {
+    BST_PDL_ENTER();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     BNode r;
     r.pnode = 0;
@@ -2433,7 +2496,7 @@ __global__ void k_b_root(BDev d, uint64_t n) {
     *d.state = s;
 }
 
-void launch_b_root(const BDev& d, uint64_t n, cudaStream_t st) { k_b_root<<<1, 32, 0, st>>>(d, n); }
+void launch_b_root(const BDev& d, uint64_t n, cudaStream_t st) { launch_k(k_b_root, 1, 32, 0, st, d, n); }
 
 
 
@@ -2593,6 +2656,7 @@ __global__ void __launch_bounds__(PART_THREADS)
 k_b_partition(BDev d, const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp,
               const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16,
               int a, int need_split, const Q* __restrict__ qin, Q* __restrict__ qout, BinsFM fm) {
+    BST_PDL_ENTER();
     __shared__ PartWork w;
     __shared__ uint2 s_m;
     const uint32_t total = min(d.state->part_chunks, d.max_part_chunks);
@@ -2615,18 +2679,18 @@ void launch_b_partition(const BDev& d, const uint32_t* rin, uint32_t* rout, cons
                         const uint16_t* bins16, uint32_t s16, int a, int need_split, uint32_t grid,
                         const void* qin, void* qout, int mode, const BinsFM& fm, cudaStream_t st) {
     if (!qin || !qout)
-        k_b_partition<char><<<grid, PART_THREADS, 0, st>>>(d, rin, rout, bins8, s8, bins16, s16, a, need_split,
+        launch_k(k_b_partition<char>, grid, PART_THREADS, 0, st, d, rin, rout, bins8, s8, bins16, s16, a, need_split,
                                                            nullptr, nullptr, fm);
     else if (mode == GRAD_Q8)
-        k_b_partition<char2><<<grid, PART_THREADS, 0, st>>>(d, rin, rout, bins8, s8, bins16, s16, a, need_split,
+        launch_k(k_b_partition<char2>, grid, PART_THREADS, 0, st, d, rin, rout, bins8, s8, bins16, s16, a, need_split,
                                                             static_cast<const char2*>(qin), static_cast<char2*>(qout),
                                                             fm);
     else if (mode == GRAD_Q16)
-        k_b_partition<short2><<<grid, PART_THREADS, 0, st>>>(d, rin, rout, bins8, s8, bins16, s16, a, need_split,
+        launch_k(k_b_partition<short2>, grid, PART_THREADS, 0, st, d, rin, rout, bins8, s8, bins16, s16, a, need_split,
                                                              static_cast<const short2*>(qin),
                                                              static_cast<short2*>(qout), fm);
     else
-        k_b_partition<float2><<<grid, PART_THREADS, 0, st>>>(d, rin, rout, bins8, s8, bins16, s16, a, need_split,
+        launch_k(k_b_partition<float2>, grid, PART_THREADS, 0, st, d, rin, rout, bins8, s8, bins16, s16, a, need_split,
                                                              static_cast<const float2*>(qin),
                                                              static_cast<float2*>(qout), fm);
 }
@@ -2637,6 +2701,7 @@ void launch_b_partition(const BDev& d, const uint32_t* rin, uint32_t* rout, cons
 template <typename T>
 __global__ void k_transpose_bins(const T* __restrict__ in, uint32_t s, uint32_t f, uint64_t n,
                                  T* __restrict__ out) {
+    BST_PDL_ENTER();
     __shared__ T t[32][33];
     const uint64_t r0 = (uint64_t)blockIdx.x * 32u;
     const uint32_t c0 = blockIdx.y * 32u;
@@ -2657,9 +2722,9 @@ void launch_transpose_bins(const uint8_t* b8, uint32_t s8, uint32_t f8, const ui
                            uint32_t f16, uint64_t n, uint8_t* fm8, uint16_t* fm16, cudaStream_t st) {
     const dim3 blk(32, 8);
     if (f8 && n)
-        k_transpose_bins<uint8_t><<<dim3((unsigned)((n + 31) / 32), (f8 + 31) / 32), blk, 0, st>>>(b8, s8, f8, n, fm8);
+        launch_k(k_transpose_bins<uint8_t>, dim3((unsigned)((n + 31) / 32), (f8 + 31) / 32), blk, 0, st, b8, s8, f8, n, fm8);
     if (f16 && n)
-        k_transpose_bins<uint16_t><<<dim3((unsigned)((n + 31) / 32), (f16 + 31) / 32), blk, 0, st>>>(b16, s16, f16, n,
+        launch_k(k_transpose_bins<uint16_t>, dim3((unsigned)((n + 31) / 32), (f16 + 31) / 32), blk, 0, st, b16, s16, f16, n,
                                                                                                fm16);
 }
 
@@ -2813,6 +2878,7 @@ __global__ void __launch_bounds__(1024) k_lw_children(BDev d, const PartWork* __
                                                      const unsigned* __restrict__ cursors, uint32_t k,
                                                      ScanNode* __restrict__ scan_nodes,
                                                      const unsigned* __restrict__ scnt) {
+    BST_PDL_ENTER();
     __shared__ uint32_t sh[33];
     __shared__ uint32_t s_jc[1024], s_own[1024];
     __shared__ unsigned long long rows;
@@ -2875,7 +2941,7 @@ __global__ void __launch_bounds__(1024) k_lw_children(BDev d, const PartWork* __
 void launch_lw_children(const BDev& d, const PartWork* pw, const unsigned* cursors, uint32_t k, ScanNode* scan_nodes,
                         const unsigned* scnt, cudaStream_t st) {
     if (k == 0) return;
-    k_lw_children<<<1, 1024, 0, st>>>(d, pw, cursors, k, scan_nodes, scnt);
+    launch_k(k_lw_children, 1, 1024, 0, st, d, pw, cursors, k, scan_nodes, scnt);
 }
 
 // ============================================================================
@@ -2946,6 +3012,7 @@ __device__ void lw_make_leaf(const BDev& d, const LwDev& w, const LwCand& c, con
 }  // namespace
 
 __global__ void k_lw_init(BDev d, LwDev w, uint32_t n, uint32_t root_count) {
+    BST_PDL_ENTER();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     LwCand r;
     r.split = w.child[0];
@@ -2983,7 +3050,7 @@ __global__ void k_lw_init(BDev d, LwDev w, uint32_t n, uint32_t root_count) {
 }
 
 void launch_lw_init(const BDev& d, const LwDev& w, uint32_t n, uint32_t root_count, cudaStream_t st) {
-    k_lw_init<<<1, 32, 0, st>>>(d, w, n, root_count);
+    launch_k(k_lw_init, 1, 32, 0, st, d, w, n, root_count);
 }
 
 // Absorbs the last step's expansions (children counts from the partition
@@ -3035,6 +3102,7 @@ __device__ __forceinline__ unsigned long long lw_key(float g, uint32_t vid) {
 template <bool CACHED>
 __global__ void __launch_bounds__(LW_REPLAY_THREADS) k_lw_replay(BDev d, LwDev w, LeafParams lp,
                                                                  const double* __restrict__ scale) {
+    BST_PDL_ENTER();
     extern __shared__ __align__(16) unsigned char lw_smem[];
     __shared__ LwState sS;
     __shared__ uint32_t s_mode, s_e, s_bmax, s_np, s_nt, s_k, s_chunk_base;
@@ -3315,9 +3383,9 @@ void launch_lw_replay(const BDev& d, const LwDev& w, LeafParams lp, const double
     const size_t smem = lw_replay_smem(w);
     if (smem <= LW_REPLAY_SMEM_MAX) {  // 255 leaves: 160 KB
         init_kernel_attributes();
-        k_lw_replay<true><<<1, LW_REPLAY_THREADS, smem, st>>>(d, w, lp, scale);
+        launch_k(k_lw_replay<true>, 1, LW_REPLAY_THREADS, smem, st, d, w, lp, scale);
     } else {
-        k_lw_replay<false><<<1, LW_REPLAY_THREADS, 0, st>>>(d, w, lp, scale);
+        launch_k(k_lw_replay<false>, 1, LW_REPLAY_THREADS, 0, st, d, w, lp, scale);
     }
 }
 
@@ -3328,6 +3396,7 @@ __global__ void __launch_bounds__(PART_THREADS)
 k_lw_partition(BDev d, const uint32_t* __restrict__ ridx, uint32_t* __restrict__ tmp,
                const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16,
                const Q* __restrict__ qin, Q* __restrict__ qout, BinsFM fm) {
+    BST_PDL_ENTER();
     __shared__ PartWork w;
     __shared__ uint2 s_m;
     const uint32_t total = min(d.state->part_chunks, d.max_part_chunks);
@@ -3352,6 +3421,7 @@ constexpr uint32_t LW_COPY_THREADS = 256;
 template <typename Q>
 __global__ void __launch_bounds__(LW_COPY_THREADS) k_lw_copy_back(BDev d, const uint32_t* __restrict__ tmp, uint32_t* __restrict__ ridx,
                                const Q* __restrict__ qtmp, Q* __restrict__ q) {
+    BST_PDL_ENTER();
     const uint32_t total = min(d.state->part_chunks, d.max_part_chunks);
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
         const uint2 m = d.part_map[c];
@@ -3386,8 +3456,8 @@ template <typename Q>
 static void lw_partition_t(const BDev& d, uint32_t* rin, uint32_t* rout, const uint8_t* bins8, uint32_t s8,
                            const uint16_t* bins16, uint32_t s16, uint32_t grid, Q* qin, Q* qout, const BinsFM& fm,
                            cudaStream_t st) {
-    k_lw_partition<Q><<<grid, PART_THREADS, 0, st>>>(d, rin, rout, bins8, s8, bins16, s16, qin, qout, fm);
-    k_lw_copy_back<Q><<<grid, LW_COPY_THREADS, 0, st>>>(d, rout, rin, qout, qin);
+    launch_k(k_lw_partition<Q>, grid, PART_THREADS, 0, st, d, rin, rout, bins8, s8, bins16, s16, qin, qout, fm);
+    launch_k(k_lw_copy_back<Q>, grid, LW_COPY_THREADS, 0, st, d, rout, rin, qout, qin);
 }
 
 void launch_lw_partition(const BDev& d, uint32_t* rin, uint32_t* rout, const uint8_t* bins8, uint32_t s8,
@@ -3409,6 +3479,7 @@ void launch_lw_partition(const BDev& d, uint32_t* rin, uint32_t* rout, const uin
 // Leaf chunk map of the finished tree (k_b_finalize's second half) and the
 // leaf sums zeroed for the quantised forms' exact leaf solve.
 __global__ void __launch_bounds__(1024) k_lw_leaves(BDev d) {
+    BST_PDL_ENTER();
     __shared__ uint32_t sh[33];
     __shared__ uint32_t s_jc[1024], s_own[1024], s_begin[1024];
     __shared__ uint32_t base;
@@ -3433,10 +3504,11 @@ __global__ void __launch_bounds__(1024) k_lw_leaves(BDev d) {
     if (threadIdx.x == 0) s->leaf_chunks = base < d.max_leaf_chunks ? base : d.max_leaf_chunks;
 }
 
-void launch_lw_leaves(const BDev& d, cudaStream_t st) { k_lw_leaves<<<1, 1024, 0, st>>>(d); }
+void launch_lw_leaves(const BDev& d, cudaStream_t st) { launch_k(k_lw_leaves, 1, 1024, 0, st, d); }
 
 template <typename HB>
 __global__ void k_b_zero_right(BDev d, HB* __restrict__ hist, uint64_t slot_bins) {
+    BST_PDL_ENTER();
     const uint64_t n = (uint64_t)d.state->n_exp * slot_bins;
     HB* p = hist + (uint64_t)d.state->first_right * slot_bins;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -3445,9 +3517,9 @@ __global__ void k_b_zero_right(BDev d, HB* __restrict__ hist, uint64_t slot_bins
 
 void launch_b_zero_right(const BDev& d, void* hist, uint64_t slot_bins, uint32_t grid, cudaStream_t st, int hist32) {
     if (hist32)
-        k_b_zero_right<HBin32><<<grid, 256, 0, st>>>(d, static_cast<HBin32*>(hist), slot_bins);
+        launch_k(k_b_zero_right<HBin32>, grid, 256, 0, st, d, static_cast<HBin32*>(hist), slot_bins);
     else
-        k_b_zero_right<HBin><<<grid, 256, 0, st>>>(d, static_cast<HBin*>(hist), slot_bins);
+        launch_k(k_b_zero_right<HBin>, grid, 256, 0, st, d, static_cast<HBin*>(hist), slot_bins);
 }
 
 // Histograms of all smaller children of the level (one persistent launch).
@@ -3456,6 +3528,7 @@ __global__ void __launch_bounds__(HIST_THREADS)
 k_b_hist(BDev d, const HistTile* __restrict__ tiles, uint32_t n_tiles, uint32_t S, const uint32_t* __restrict__ ridx,
          GradRef gr, const uint8_t* __restrict__ bins8, uint32_t s8, const uint16_t* __restrict__ bins16, uint32_t s16,
          HB* __restrict__ hist, uint64_t slot_bins) {
+    BST_PDL_ENTER();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* sm = reinterpret_cast<uint32_t*>(smem_raw);
     __shared__ HistTile tile;
@@ -3492,16 +3565,16 @@ void launch_b_hist(const BDev& d, const HistTile* tiles, uint32_t n_tiles, uint3
     HBin* h64 = static_cast<HBin*>(hist);
     HBin32* h32 = static_cast<HBin32*>(hist);
     if (gr.mode == GRAD_Q16)
-        k_b_hist<GRAD_Q16, HBin><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16,
+        launch_k(k_b_hist<GRAD_Q16, HBin>, grid, HIST_THREADS, smem, st, d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16,
                                                                     s16, h64, slot_bins);
     else if (gr.mode == GRAD_Q8 && hist32)
-        k_b_hist<GRAD_Q8, HBin32><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16,
+        launch_k(k_b_hist<GRAD_Q8, HBin32>, grid, HIST_THREADS, smem, st, d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16,
                                                                      s16, h32, slot_bins);
     else if (gr.mode == GRAD_Q8)
-        k_b_hist<GRAD_Q8, HBin><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16,
+        launch_k(k_b_hist<GRAD_Q8, HBin>, grid, HIST_THREADS, smem, st, d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16,
                                                                    s16, h64, slot_bins);
     else
-        k_b_hist<GRAD_F32, HBin><<<grid, HIST_THREADS, smem, st>>>(d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16,
+        launch_k(k_b_hist<GRAD_F32, HBin>, grid, HIST_THREADS, smem, st, d, tiles, n_tiles, S, ridx, gr, bins8, s8, bins16,
                                                                     s16, h64, slot_bins);
 }
 
@@ -3527,6 +3600,7 @@ k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HB*
          uint64_t slot_bins, const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
          long long* __restrict__ node_tot, int b, int last_wins, LeafParams lp, uint32_t buf,
          const ScanNode* __restrict__ root, const uint8_t* __restrict__ colmask, NodeSplit* __restrict__ lw_out) {
+    BST_PDL_ENTER();
     __shared__ double s_key[SCAN_WARPS][SORT_N];
     __shared__ uint32_t s_cat[SCAN_WARPS][SORT_N];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -3586,11 +3660,11 @@ void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const
                    LeafParams lp, uint32_t buf, uint32_t grid, cudaStream_t st, int hist32, const ScanNode* root,
                    const uint8_t* colmask, NodeSplit* lw_out) {
     if (hist32)
-        k_b_scan<HBin32><<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, static_cast<const HBin32*>(hist), slot_bins,
+        launch_k(k_b_scan<HBin32>, grid, SCAN_WARPS * 32, 0, st, d, cols, n_cols, static_cast<const HBin32*>(hist), slot_bins,
                                                            scale, gp, cand, node_tot, b, last_wins, lp, buf, root,
                                                            colmask, lw_out);
     else
-        k_b_scan<HBin><<<grid, SCAN_WARPS * 32, 0, st>>>(d, cols, n_cols, static_cast<const HBin*>(hist), slot_bins,
+        launch_k(k_b_scan<HBin>, grid, SCAN_WARPS * 32, 0, st, d, cols, n_cols, static_cast<const HBin*>(hist), slot_bins,
                                                          scale, gp, cand, node_tot, b, last_wins, lp, buf, root,
                                                          colmask, lw_out);
 }
@@ -3629,6 +3703,7 @@ __device__ void children_sums_body(BDev d, int b);
 // both children of every expansion their sums (frontier b).
 template <int MODE>
 __global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, GradRef gr, int b) {
+    BST_PDL_ENTER();
     const uint32_t total = d.state->hist_chunks, CH = d.state->hist_chunk;
     const GradLoad<MODE> load(gr);
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
@@ -3652,11 +3727,11 @@ __global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, GradRef gr, 
 
 void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, int b, uint32_t grid, cudaStream_t st) {
     if (gr.mode == GRAD_Q16)
-        k_b_sums<GRAD_Q16><<<grid, 256, 0, st>>>(d, ridx, gr, b);
+        launch_k(k_b_sums<GRAD_Q16>, grid, 256, 0, st, d, ridx, gr, b);
     else if (gr.mode == GRAD_Q8)
-        k_b_sums<GRAD_Q8><<<grid, 256, 0, st>>>(d, ridx, gr, b);
+        launch_k(k_b_sums<GRAD_Q8>, grid, 256, 0, st, d, ridx, gr, b);
     else
-        k_b_sums<GRAD_F32><<<grid, 256, 0, st>>>(d, ridx, gr, b);
+        launch_k(k_b_sums<GRAD_F32>, grid, 256, 0, st, d, ridx, gr, b);
 }
 
 __device__ void children_sums_body(BDev d, int b) {
@@ -3680,6 +3755,7 @@ __device__ void children_sums_body(BDev d, int b) {
 // Remaining frontier -> leaves (grower.rs:484-514); leaf row chunks.
 __global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams lp, const double* __restrict__ scale,
                                                     uint32_t buf) {
+    BST_PDL_ENTER();
     __shared__ uint32_t sh[33];
     __shared__ uint32_t s_jc[1024], s_own[1024], s_begin[1024];
     __shared__ uint32_t base, nf, n0;
@@ -3729,7 +3805,7 @@ __global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams l
 }
 
 void launch_b_finalize(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st) {
-    k_b_finalize<<<1, 1024, 0, st>>>(d, a, lp, scale, buf);
+    launch_k(k_b_finalize, 1, 1024, 0, st, d, a, lp, scale, buf);
 }
 
 __device__ void leaf_values_body(BDev d, LeafParams lp, const double* __restrict__ scale);
@@ -3740,6 +3816,7 @@ __device__ void leaf_values_body(BDev d, LeafParams lp, const double* __restrict
 // gradients' fixed-point scales).
 __global__ void k_b_leaf_sums(BDev d, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1, GradRef gr,
                               LeafParams lp, const double* __restrict__ scale) {
+    BST_PDL_ENTER();
     const uint32_t total = d.state->leaf_chunks;
     const GradLoad<GRAD_F32> load(gr);
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
@@ -3764,7 +3841,7 @@ __global__ void k_b_leaf_sums(BDev d, const uint32_t* __restrict__ r0, const uin
 
 void launch_b_leaf_sums(const BDev& d, const uint32_t* r0, const uint32_t* r1, const GradRef& gr, LeafParams lp,
                         const double* scale, uint32_t grid, cudaStream_t st) {
-    k_b_leaf_sums<<<grid, 256, 0, st>>>(d, r0, r1, gr, lp, scale);
+    launch_k(k_b_leaf_sums, grid, 256, 0, st, d, r0, r1, gr, lp, scale);
 }
 
 __device__ void leaf_values_body(BDev d, LeafParams lp, const double* __restrict__ scale) {
@@ -3780,6 +3857,7 @@ __device__ void leaf_values_body(BDev d, LeafParams lp, const double* __restrict
 // pred[row] += leaf value over the final partition (grower.rs:208-219).
 __global__ void k_b_leaf_update(BDev d, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1,
                                 float* __restrict__ pred, uint32_t* __restrict__ row_leaf) {
+    BST_PDL_ENTER();
     const uint32_t total = d.state->leaf_chunks;
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
         const uint2 m = d.leaf_map[c];
@@ -3812,7 +3890,7 @@ __global__ void k_b_leaf_update(BDev d, const uint32_t* __restrict__ r0, const u
 
 void launch_b_leaf_update(const BDev& d, const uint32_t* r0, const uint32_t* r1, float* pred, uint32_t* row_leaf,
                           uint32_t grid, cudaStream_t st) {
-    k_b_leaf_update<<<grid, 256, 0, st>>>(d, r0, r1, pred, row_leaf);
+    launch_k(k_b_leaf_update, grid, 256, 0, st, d, r0, r1, pred, row_leaf);
 }
 
 // ============================================================================
@@ -3843,6 +3921,7 @@ __device__ __forceinline__ void renew_set(const BDev& d, uint32_t l, float v) {
 }  // namespace
 
 __global__ void k_renew_start(BDev d, RenewDev r) {
+    BST_PDL_ENTER();
     const uint32_t nl = min(d.state->n_leaves, r.cap);
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (uint64_t)nl * 256u;
          i += (uint64_t)gridDim.x * blockDim.x) {
@@ -3853,6 +3932,7 @@ __global__ void k_renew_start(BDev d, RenewDev r) {
 
 // Sampled rows per leaf: one block per leaf chunk, one atomic per block.
 __global__ void k_renew_count(BDev d, RenewDev r, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1) {
+    BST_PDL_ENTER();
     __shared__ uint32_t s_cnt;
     const uint32_t total = d.state->leaf_chunks;
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
@@ -3876,6 +3956,7 @@ __global__ void k_renew_count(BDev d, RenewDev r, const uint32_t* __restrict__ r
 // The rank to find: ceil(alpha m) - 1 clamped to [0, m - 1] (f32 product,
 // utils.rs:42-44); none for an empty leaf.
 __global__ void k_renew_rank(BDev d, RenewDev r, float alpha) {
+    BST_PDL_ENTER();
     const uint32_t nl = min(d.state->n_leaves, r.cap);
     for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nl; l += gridDim.x * blockDim.x) {
         const uint32_t m = r.cnt[l];
@@ -3895,6 +3976,7 @@ __global__ void k_renew_rank(BDev d, RenewDev r, float alpha) {
 // sampled rows whose higher bytes match the prefix.
 __global__ void k_renew_hist(BDev d, RenewDev r, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1,
                              const float* __restrict__ y, const float* __restrict__ pred, uint32_t shift) {
+    BST_PDL_ENTER();
     __shared__ uint32_t sh[256];
     const uint32_t total = d.state->leaf_chunks;
     const uint32_t hi_mask = shift >= 24 ? 0u : (0xFFFFFFFFu << (shift + 8));
@@ -3924,6 +4006,7 @@ __global__ void k_renew_hist(BDev d, RenewDev r, const uint32_t* __restrict__ r0
 // The byte of the wanted rank (one warp per leaf; lane j owns bytes 8j ..
 // 8j + 7), then the counts cleared for the next pass.
 __global__ void k_renew_pick(BDev d, RenewDev r, uint32_t shift) {
+    BST_PDL_ENTER();
     const uint32_t nl = min(d.state->n_leaves, r.cap);
     const uint32_t lane = threadIdx.x & 31u, wpb = blockDim.x >> 5;
     for (uint32_t l = blockIdx.x * wpb + (threadIdx.x >> 5); l < nl; l += gridDim.x * wpb) {
@@ -3967,6 +4050,7 @@ __global__ void k_renew_pick(BDev d, RenewDev r, uint32_t shift) {
 }
 
 __global__ void k_renew_apply(BDev d, RenewDev r, float lr) {
+    BST_PDL_ENTER();
     const uint32_t nl = min(d.state->n_leaves, r.cap);
     for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nl; l += gridDim.x * blockDim.x)
         if (r.rank[l] != RENEW_NONE) renew_set(d, l, renew_value(r.prefix[l]) * lr);
@@ -4023,6 +4107,7 @@ __global__ void __launch_bounds__(RENEW_W_THREADS)
 k_renew_weighted(BDev d, RenewDev r, const uint32_t* __restrict__ r0, const uint32_t* __restrict__ r1,
                  const float* __restrict__ y, const float* __restrict__ pred, const float* __restrict__ w, float alpha,
                  float lr) {
+    BST_PDL_ENTER();
     __shared__ uint32_t sh[33];
     __shared__ float s_w[RENEW_W_THREADS];
     __shared__ uint32_t s_base, s_zero, s_hit;
@@ -4116,17 +4201,17 @@ k_renew_weighted(BDev d, RenewDev r, const uint32_t* __restrict__ r0, const uint
 void launch_leaf_renew(const BDev& d, const RenewDev& r, const uint32_t* r0, const uint32_t* r1, const float* y,
                        const float* pred, const float* w, float alpha, float lr, uint32_t grid, cudaStream_t st) {
     if (w) {
-        k_renew_weighted<<<grid, RENEW_W_THREADS, 0, st>>>(d, r, r0, r1, y, pred, w, alpha, lr);
+        launch_k(k_renew_weighted, grid, RENEW_W_THREADS, 0, st, d, r, r0, r1, y, pred, w, alpha, lr);
         return;
     }
-    k_renew_start<<<grid, 256, 0, st>>>(d, r);
-    k_renew_count<<<grid, 256, 0, st>>>(d, r, r0, r1);
-    k_renew_rank<<<grid, 256, 0, st>>>(d, r, alpha);
+    launch_k(k_renew_start, grid, 256, 0, st, d, r);
+    launch_k(k_renew_count, grid, 256, 0, st, d, r, r0, r1);
+    launch_k(k_renew_rank, grid, 256, 0, st, d, r, alpha);
     for (int shift = 24; shift >= 0; shift -= 8) {
-        k_renew_hist<<<grid, 256, 0, st>>>(d, r, r0, r1, y, pred, (uint32_t)shift);
-        k_renew_pick<<<grid, 256, 0, st>>>(d, r, (uint32_t)shift);
+        launch_k(k_renew_hist, grid, 256, 0, st, d, r, r0, r1, y, pred, (uint32_t)shift);
+        launch_k(k_renew_pick, grid, 256, 0, st, d, r, (uint32_t)shift);
     }
-    k_renew_apply<<<grid, 256, 0, st>>>(d, r, lr);
+    launch_k(k_renew_apply, grid, 256, 0, st, d, r, lr);
 }
 
 // ============================================================================
@@ -4136,6 +4221,7 @@ void launch_leaf_renew(const BDev& d, const RenewDev& r, const uint32_t* r0, con
 
 __global__ void k_predict(ForestDev f, const float* __restrict__ x,
                           uint64_t n, uint32_t n_features, int feature_major, float* __restrict__ out) {
+    BST_PDL_ENTER();
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint64_t fstride = feature_major ? n : 1;
@@ -4174,7 +4260,7 @@ __global__ void k_predict(ForestDev f, const float* __restrict__ x,
 void launch_predict(const ForestDev& f, const float* x, uint64_t n, uint32_t n_features,
                     int feature_major, float* out, cudaStream_t st) {
     if (n == 0) return;
-    k_predict<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(f, x, n, n_features, feature_major, out);
+    launch_k(k_predict, (unsigned)((n + 127) / 128), 128, 0, st, f, x, n, n_features, feature_major, out);
 }
 
 // ---- shared-memory traversal (heap-ordered trees of depth <= HEAP_DEPTH) ------
@@ -4279,6 +4365,7 @@ template <typename BinT>
 __global__ void __launch_bounds__(BIN_THREADS)
 k_bin_rows(HeapForest f, const float* __restrict__ x, uint64_t n, uint32_t F, uint32_t R, uint32_t FC,
            uint32_t* __restrict__ bins_g) {
+    BST_PDL_ENTER();
     constexpr uint32_t RPL = 4u / (uint32_t)sizeof(BinT);
     constexpr uint32_t WR = 32u * RPL;  // rows per warp
     constexpr uint32_t BITS = 8u * (uint32_t)sizeof(BinT);
@@ -4422,6 +4509,7 @@ template <bool CAT, typename BinT>
 __global__ void __launch_bounds__(PREDICT_MAX_ROWS, 1)
 k_predict_heap(HeapForest f, const unsigned char* __restrict__ bins_g, uint64_t n, uint32_t R, uint32_t S,
                float* __restrict__ out) {
+    BST_PDL_ENTER();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* ring = reinterpret_cast<uint32_t*>(smem_raw);  // [2][PREDICT_CHUNK][HEAP_NODES]
     float* lv = reinterpret_cast<float*>(smem_raw + PREDICT_RING);  // [PREDICT_CHUNK][R] when S > 1
@@ -4507,22 +4595,23 @@ void launch_predict_heap(const HeapForest& f, const float* x, uint64_t n, uint32
         const unsigned grid = (unsigned)(blocks < sm_count() * 4u ? blocks : sm_count() * 4u);
         const size_t smem = (predict_spl_floats(NF) + (size_t)(BIN_THREADS / 32u) * wr * BIN_XS_LD) * sizeof(float);
         if (f.bins16)
-            k_bin_rows<uint16_t><<<grid, BIN_THREADS, smem, st>>>(f, x, n, F, p.R, FC, static_cast<uint32_t*>(scratch));
+            launch_k(k_bin_rows<uint16_t>, grid, BIN_THREADS, smem, st, f, x, n, F, p.R, FC, static_cast<uint32_t*>(scratch));
         else
-            k_bin_rows<uint8_t><<<grid, BIN_THREADS, smem, st>>>(f, x, n, F, p.R, FC, static_cast<uint32_t*>(scratch));
+            launch_k(k_bin_rows<uint8_t>, grid, BIN_THREADS, smem, st, f, x, n, F, p.R, FC, static_cast<uint32_t*>(scratch));
     }
     const unsigned grid = (unsigned)(tiles < sm_count() ? tiles : sm_count());
     const unsigned threads = p.R * p.S;
     const unsigned char* bg = static_cast<const unsigned char*>(scratch);
     if (f.has_cat)
-        k_predict_heap<true, uint16_t><<<grid, threads, p.smem, st>>>(f, bg, n, p.R, p.S, out);
+        launch_k(k_predict_heap<true, uint16_t>, grid, threads, p.smem, st, f, bg, n, p.R, p.S, out);
     else if (f.bins16)
-        k_predict_heap<false, uint16_t><<<grid, threads, p.smem, st>>>(f, bg, n, p.R, p.S, out);
+        launch_k(k_predict_heap<false, uint16_t>, grid, threads, p.smem, st, f, bg, n, p.R, p.S, out);
     else
-        k_predict_heap<false, uint8_t><<<grid, threads, p.smem, st>>>(f, bg, n, p.R, p.S, out);
+        launch_k(k_predict_heap<false, uint8_t>, grid, threads, p.smem, st, f, bg, n, p.R, p.S, out);
 }
 
 __global__ void k_transform(int t, float* __restrict__ p, uint32_t G, uint64_t n) {
+    BST_PDL_ENTER();
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t == 1) {
         if (i >= (uint64_t)G * n) return;
@@ -4554,12 +4643,13 @@ __global__ void k_transform(int t, float* __restrict__ p, uint32_t G, uint64_t n
 void launch_transform(int transform, float* out, uint32_t G, uint64_t n, cudaStream_t st) {
     if (transform == 0 || n == 0) return;
     const uint64_t total = transform == 1 ? (uint64_t)G * n : n;
-    k_transform<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(transform, out, G, n);
+    launch_k(k_transform, (unsigned)((total + 255) / 256), 256, 0, st, transform, out, G, n);
 }
 
 // Row sampling: grad/hess of the rows outside the sample become zero
 // (sample_uniform, training/sampling/row.rs:168-210).
 __global__ void k_zero_unsampled(float2* __restrict__ gh, const uint8_t* __restrict__ mask, uint64_t n) {
+    BST_PDL_ENTER();
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         if (!mask[i]) gh[i] = make_float2(0.0f, 0.0f);
 }
@@ -4567,13 +4657,14 @@ __global__ void k_zero_unsampled(float2* __restrict__ gh, const uint8_t* __restr
 void launch_zero_unsampled(float2* gh, const uint8_t* mask, uint64_t n, cudaStream_t st) {
     if (n == 0) return;
     const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 8);
-    k_zero_unsampled<<<(unsigned)blocks, 256, 0, st>>>(gh, mask, n);
+    launch_k(k_zero_unsampled, (unsigned)blocks, 256, 0, st, gh, mask, n);
 }
 
 // GOSS (sampling/row.rs:214-280): code 0 leaves the tree (zero grad/hess),
 // 1 is kept, 2 is kept with grad and hess scaled by `mult`; mask gets 0 / 1.
 __global__ void k_goss_apply(float2* __restrict__ gh, const uint8_t* __restrict__ code, float mult,
                              uint8_t* __restrict__ mask, uint64_t n) {
+    BST_PDL_ENTER();
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint8_t c = code[i];
         if (c == 0) {
@@ -4589,10 +4680,11 @@ __global__ void k_goss_apply(float2* __restrict__ gh, const uint8_t* __restrict_
 void launch_goss_apply(float2* gh, const uint8_t* code, float mult, uint8_t* mask, uint64_t n, cudaStream_t st) {
     if (n == 0) return;
     const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 8);
-    k_goss_apply<<<(unsigned)blocks, 256, 0, st>>>(gh, code, mult, mask, n);
+    launch_k(k_goss_apply, (unsigned)blocks, 256, 0, st, gh, code, mult, mask, n);
 }
 
 __global__ void k_add_f32(float* __restrict__ a, const float* __restrict__ b, uint64_t n) {
+    BST_PDL_ENTER();
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         a[i] = a[i] + b[i];
 }
@@ -4600,7 +4692,7 @@ __global__ void k_add_f32(float* __restrict__ a, const float* __restrict__ b, ui
 void launch_add_f32(float* a, const float* b, uint64_t n, cudaStream_t st) {
     if (n == 0) return;
     const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 8);
-    k_add_f32<<<(unsigned)blocks, 256, 0, st>>>(a, b, n);
+    launch_k(k_add_f32, (unsigned)blocks, 256, 0, st, a, b, n);
 }
 
 void init_kernel_attributes() {
