@@ -22,7 +22,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", 
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fno-fast-math",
              "-Wall", "-Wno-unused-function", f"-I{CUDA}/include"]
 
-CU_SOURCES = ["kernels.cu", "noalloc.cu"]
+CU_SOURCES = ["kernels.cu", "noalloc.cu", "mappers.cu"]
 CPP_SOURCES = ["binning.cpp", "engine.cpp", "capi.cpp", "server.cpp", "synth.cpp", "persist.cpp", "autotune.cpp"]
 HEADERS = ["kernels.h", "binning.h", "engine.h", "synth_gen.h", "api_util.h", "autotune.h", os.path.join("..", "..", "include", "boosters_c.h")]
 

@@ -161,91 +161,18 @@ std::vector<uint32_t> binning_sample(uint64_t n, uint64_t k) {
     return out;
 }
 
-// Ascending sort of finite floats by an LSD radix sort of order-preserving
-// keys (sign bit flipped for positives, all bits for negatives); -0.0 sorts
-// before +0.0, which compare equal and so merge in the distinct pass.
-void sort_floats(std::vector<float>& v) {
-    const size_t n = v.size();
-    if (n < 2048) {
-        std::sort(v.begin(), v.end());
-        return;
-    }
-    std::vector<uint32_t> a(n), b(n);
-    // 8-bit digits: the four digit counts in one pass, a pass skipped when
-    // every key has the same digit there
-    std::vector<uint32_t> cnt(4 * 256, 0);
-    for (size_t i = 0; i < n; ++i) {
-        uint32_t u;
-        std::memcpy(&u, &v[i], 4);
-        const uint32_t k = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-        a[i] = k;
-        ++cnt[k & 255u];
-        ++cnt[256 + ((k >> 8) & 255u)];
-        ++cnt[512 + ((k >> 16) & 255u)];
-        ++cnt[768 + (k >> 24)];
-    }
-    for (int d = 0; d < 4; ++d) {
-        uint32_t* c = cnt.data() + 256 * d;
-        const int shift = 8 * d;
-        if (c[(a[0] >> shift) & 255u] == n) continue;
-        uint32_t sum = 0;
-        for (uint32_t q = 0; q < 256; ++q) {
-            const uint32_t t = c[q];
-            c[q] = sum;
-            sum += t;
-        }
-        for (size_t i = 0; i < n; ++i) b[c[(a[i] >> shift) & 255u]++] = a[i];
-        a.swap(b);
-    }
-    for (size_t i = 0; i < n; ++i) {
-        const uint32_t k = a[i];
-        const uint32_t u = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
-        std::memcpy(&v[i], &u, 4);
-    }
-}
+}  // namespace
 
-// dataset.rs:683-750: quantile midpoints over the distinct finite values.
-Mapper numeric_mapper(std::vector<float>& vals, uint32_t max_bins, bool has_nan) {
-    float lo = std::numeric_limits<float>::max(), hi = -std::numeric_limits<float>::max();
-    size_t w = 0;
-    for (size_t i = 0; i < vals.size(); ++i) {
-        const float v = vals[i];
-        if (std::isfinite(v)) {
-            lo = std::min(lo, v);
-            hi = std::max(hi, v);
-            vals[w++] = v;
-        }
-    }
-    vals.resize(w);
+Mapper numeric_mapper_from_bounds(const double* bounds, uint32_t n_bounds, bool has_nan) {
     Mapper m;
-    if (w == 0 || lo >= hi) {
-        m.bounds = {std::numeric_limits<double>::max()};
-        m.n_bins = 1;
-        return m;
+    m.bounds.assign(bounds, bounds + n_bounds);
+    m.n_bins = n_bounds;
+    if (n_bounds > 1 && has_nan) {  // one finite value: a single bin and no NaN bin
+        m.missing = MISSING_NAN;
+        m.default_bin = n_bounds - 1;
     }
-    const uint32_t nb = (uint32_t)std::min<uint64_t>(max_bins, w);
-    sort_floats(vals);
-    vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
-    const size_t u = vals.size();
-    if (u <= nb) {
-        for (size_t i = 0; i + 1 < u; ++i) m.bounds.push_back(((double)vals[i] + (double)vals[i + 1]) / 2.0);
-    } else {
-        for (uint32_t i = 1; i < nb; ++i) {
-            const double q = (double)i / (double)nb;
-            const size_t idx = std::min<size_t>((size_t)std::floor(q * (double)(u - 1)), u - 2);
-            const double b = ((double)vals[idx] + (double)vals[idx + 1]) / 2.0;
-            if (m.bounds.empty() || b > m.bounds.back()) m.bounds.push_back(b);
-        }
-    }
-    m.bounds.push_back(std::numeric_limits<double>::max());
-    if (has_nan) m.bounds.push_back(std::numeric_limits<double>::max());
-    m.n_bins = (uint32_t)m.bounds.size();
-    m.missing = has_nan ? MISSING_NAN : MISSING_NONE;
-    m.default_bin = has_nan ? m.n_bins - 1 : 0;
     return m;
 }
-
-}  // namespace
 
 float f32_round_down(double d) {
     float r = to_f32(d);
@@ -256,7 +183,7 @@ float f32_round_down(double d) {
 
 bst_status plan_binning(const float* x, uint64_t F, uint64_t n,
                         const std::vector<uint8_t>& user_cat, const bst_config& cfg,
-                        BinPlan& plan, std::string& err) {
+                        NumericBounds& numeric, BinPlan& plan, std::string& err) {
     if (n == 0 || F == 0) {
         err = "dataset is empty";
         return BST_ERR_EMPTY_DATASET;
@@ -283,21 +210,23 @@ bst_status plan_binning(const float* x, uint64_t F, uint64_t n,
     }
     sampler.join();
 
+    // numeric features: bounds from the sampled values off the host, while
+    // the host takes the categorical ones
+    std::vector<uint32_t> num_f;
+    std::vector<uint8_t> num_nan;
+    for (uint64_t f = 0; f < F; ++f)
+        if (!facts[f].trivial && facts[f].numeric) {
+            num_f.push_back((uint32_t)f);
+            num_nan.push_back(facts[f].n_nan > 0 ? 1 : 0);
+        }
+    if (!num_f.empty()) numeric.start(sample, num_f, num_nan, cfg.max_bins);
+
 #pragma omp parallel for schedule(dynamic, 1)
     for (int64_t f = 0; f < (int64_t)F; ++f) {
         const float* col = x + (uint64_t)f * n;
         const FeatureFacts& ff = facts[f];
-        if (ff.trivial) continue;
-        if (ff.numeric) {
-            std::vector<float> vals;
-            if (sample.empty())
-                vals.assign(col, col + n);
-            else {
-                vals.resize(sample.size());
-                for (size_t i = 0; i < sample.size(); ++i) vals[i] = col[sample[i]];
-            }
-            plan.mappers[f] = numeric_mapper(vals, cfg.max_bins, ff.n_nan > 0);
-        } else {
+        if (ff.trivial || ff.numeric) continue;
+        {
             // every finite value's category, not a sample (dataset.rs:655-672)
             std::vector<int32_t> c;
             c.reserve(1024);
@@ -316,6 +245,7 @@ bst_status plan_binning(const float* x, uint64_t F, uint64_t n,
             plan.mappers[f] = std::move(m);
         }
     }
+    if (!num_f.empty()) numeric.finish(plan.mappers);
 
     for (uint64_t f = 0; f < F; ++f) {
         if (facts[f].trivial) {

@@ -55,10 +55,28 @@ struct BinPlan {
     uint32_t n_cols() const { return (uint32_t)col_feature.size(); }
 };
 
+// Bounds of the numeric features, computed off the host (the engine's
+// device sort): start() gets the ascending row sample (empty: every row)
+// and the features with their NaN flags and may return before the bounds
+// are known; finish() stores each feature's mapper into mappers[feature].
+struct NumericBounds {
+    virtual ~NumericBounds() = default;
+    virtual void start(const std::vector<uint32_t>& sample, const std::vector<uint32_t>& features,
+                       const std::vector<uint8_t>& has_nan, uint32_t max_bins) = 0;
+    virtual void finish(std::vector<Mapper>& mappers) = 0;
+};
+
+// The numeric mapper of a feature from its bounds as NumericBounds
+// computes them (bin_mapper.rs:55-271: a NaN bin when the feature has NaN
+// and two or more distinct finite values).
+Mapper numeric_mapper_from_bounds(const double* bounds, uint32_t n_bounds, bool has_nan);
+
 // Analysis + bounds. Returns BST_OK or an error status with `err` set.
+// Numeric features' bounds come from `numeric` while the host builds the
+// categorical features' mappers.
 bst_status plan_binning(const float* x_fm, uint64_t n_features, uint64_t n,
                         const std::vector<uint8_t>& user_categorical, const bst_config& cfg,
-                        BinPlan& plan, std::string& err);
+                        NumericBounds& numeric, BinPlan& plan, std::string& err);
 
 // Largest f32 <= d (the f32 comparison key equivalent to `v <= d` in f64).
 float f32_round_down(double d);

@@ -17,9 +17,11 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <unordered_map>
 
 namespace bst {
@@ -2645,25 +2647,113 @@ uint32_t HostTree::alloc() {
     return (uint32_t)split_index.size() - 1;
 }
 
+namespace {
+
+// Numeric bounds from the device copy of the features (k_numeric_bounds):
+// the sample and the jobs go up, one block per feature sorts its sampled
+// values, the bounds come back. `ready` runs before the first launch (the
+// features' upload must be enqueued on the stream by then).
+class DeviceBounds final : public NumericBounds {
+  public:
+    DeviceBounds(const float* x, uint64_t n, cudaStream_t st, std::function<void()> ready)
+        : x_(x), n_(n), st_(st), ready_(std::move(ready)) {}
+    void start(const std::vector<uint32_t>& sample, const std::vector<uint32_t>& features,
+               const std::vector<uint8_t>& has_nan, uint32_t max_bins) override {
+        ready_();
+        feats_ = features;
+        has_nan_ = has_nan;
+        stride_ = max_bins + 2u;
+        const uint32_t nj = (uint32_t)features.size();
+        const uint32_t k = sample.empty() ? (uint32_t)n_ : (uint32_t)sample.size();
+        if (!sample.empty()) {
+            rows_.alloc(k);
+            BST_CK(cudaMemcpyAsync(rows_.p, sample.data(), sizeof(uint32_t) * k, cudaMemcpyHostToDevice, st_));
+        }
+        std::vector<MapJob> jobs(nj);
+        for (uint32_t j = 0; j < nj; ++j) jobs[j] = MapJob{features[j], has_nan[j] ? 1u : 0u};
+        jobs_.alloc(nj);
+        BST_CK(cudaMemcpyAsync(jobs_.p, jobs.data(), sizeof(MapJob) * nj, cudaMemcpyHostToDevice, st_));
+        // jobs in batches whose sort buffers (2k words each) stay within 1 GiB
+        const uint64_t per_job = 2ull * k;
+        const uint32_t batch = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(nj, (1ull << 28) / per_job));
+        scratch_.alloc((size_t)batch * per_job);
+        cand_.alloc((size_t)batch * max_bins);
+        bounds_.alloc((size_t)nj * stride_);
+        nb_.alloc(nj);
+        for (uint32_t b0 = 0; b0 < nj; b0 += batch)
+            launch_numeric_bounds(x_, n_, sample.empty() ? nullptr : rows_.p, k, jobs_.p + b0, std::min(batch, nj - b0),
+                                  max_bins, scratch_.p, cand_.p, bounds_.p + (size_t)b0 * stride_, nb_.p + b0, st_);
+        BST_CK(cudaGetLastError());
+    }
+    void finish(std::vector<Mapper>& mappers) override {
+        const uint32_t nj = (uint32_t)feats_.size();
+        std::vector<double> b((size_t)nj * stride_);
+        std::vector<uint32_t> nb(nj);
+        BST_CK(cudaMemcpyAsync(b.data(), bounds_.p, sizeof(double) * b.size(), cudaMemcpyDeviceToHost, st_));
+        BST_CK(cudaMemcpyAsync(nb.data(), nb_.p, sizeof(uint32_t) * nj, cudaMemcpyDeviceToHost, st_));
+        BST_CK(cudaStreamSynchronize(st_));
+        for (uint32_t j = 0; j < nj; ++j) {
+            if (nb[j] == 0 || nb[j] > stride_) throw Error{BST_ERR_CUDA, "device bin bounds out of range"};
+            mappers[feats_[j]] = numeric_mapper_from_bounds(b.data() + (size_t)j * stride_, nb[j], has_nan_[j] != 0);
+        }
+    }
+
+  private:
+    const float* x_;
+    uint64_t n_;
+    cudaStream_t st_;
+    std::function<void()> ready_;
+    std::vector<uint32_t> feats_;
+    std::vector<uint8_t> has_nan_;
+    uint32_t stride_ = 0;
+    DevArray<uint32_t> rows_, scratch_, nb_;
+    DevArray<MapJob> jobs_;
+    DevArray<double> cand_, bounds_;
+};
+
+}  // namespace
+
 void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, DeviceBinned& out) {
     std::string err;
     const auto t0 = std::chrono::steady_clock::now();
-    // Features in pinned host memory: every feature goes to the device
-    // while the host plans the bins (the copy overlaps the analysis);
-    // otherwise only the planned columns are copied afterwards.
+    // Every feature goes to the device while the host analyses them: from
+    // pinned memory as one asynchronous copy, from pageable memory on a
+    // helper thread (such copies hold the calling thread). The numeric
+    // features' bounds are then computed on the device from that copy.
     DevArray<float> x;
-    bool staged = false;
-    {
-        cudaPointerAttributes a{};
-        if (cudaPointerGetAttributes(&a, ds.xdata()) == cudaSuccess && a.type == cudaMemoryTypeHost && ds.n && ds.F) {
-            x.alloc((size_t)ds.F * ds.n);
-            BST_CK(cudaMemcpyAsync(x.p, ds.xdata(), sizeof(float) * ds.F * ds.n, cudaMemcpyHostToDevice, st));
-            staged = true;
+    std::thread uploader;
+    struct Joiner {
+        std::thread& t;
+        ~Joiner() {
+            if (t.joinable()) t.join();
         }
+    } joiner{uploader};
+    cudaError_t up_err = cudaSuccess;
+    if (ds.n && ds.F) {
+        x.alloc((size_t)ds.F * ds.n);
+        cudaPointerAttributes a{};
+        const bool pinned = cudaPointerGetAttributes(&a, ds.xdata()) == cudaSuccess && a.type == cudaMemoryTypeHost;
         cudaGetLastError();
+        const size_t bytes = sizeof(float) * ds.F * ds.n;
+        if (pinned) {
+            BST_CK(cudaMemcpyAsync(x.p, ds.xdata(), bytes, cudaMemcpyHostToDevice, st));
+        } else {
+            int dev = 0;
+            BST_CK(cudaGetDevice(&dev));
+            uploader = std::thread([&x, &ds, &up_err, bytes, dev, st] {
+                up_err = cudaSetDevice(dev);
+                if (up_err == cudaSuccess) up_err = cudaMemcpyAsync(x.p, ds.xdata(), bytes, cudaMemcpyHostToDevice, st);
+            });
+        }
     }
-    bst_status rc = plan_binning(ds.xdata(), ds.F, ds.n, ds.user_cat, cfg, out.plan, err);
+    DeviceBounds numeric(x.p, ds.n, st, [&] {
+        if (uploader.joinable()) uploader.join();
+        BST_CK(up_err);
+    });
+    bst_status rc = plan_binning(ds.xdata(), ds.F, ds.n, ds.user_cat, cfg, numeric, out.plan, err);
     if (rc != BST_OK) throw Error{rc, err};
+    if (uploader.joinable()) uploader.join();
+    BST_CK(up_err);
     const BinPlan& p = out.plan;
     const uint32_t nc = p.n_cols();
     const uint64_t n = p.n;
@@ -2680,7 +2770,7 @@ void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, 
         BinColumn bc;
         bc.matrix = p.col_matrix[c];
         bc.pos = p.col_pos[c];
-        bc.src = staged ? p.col_feature[c] : c;
+        bc.src = p.col_feature[c];
         bc.is_cat = m.categorical;
         bc.nan_bin = m.missing == MISSING_NAN ? m.n_bins - 1 : m.default_bin;
         bc.zero_bin = m.missing == MISSING_ZERO ? m.default_bin : 0xFFFFFFFFu;
@@ -2700,12 +2790,6 @@ void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, 
     DevArray<float> d_thr;
     DevArray<int32_t> d_cats;
     DevArray<BinColumn> d_cols;
-    if (!staged) {
-        x.alloc((size_t)nc * n);
-        for (uint32_t c = 0; c < nc; ++c)
-            BST_CK(cudaMemcpyAsync(x.p + (size_t)c * n, ds.xdata() + (size_t)p.col_feature[c] * n, sizeof(float) * n,
-                                   cudaMemcpyHostToDevice, st));
-    }
     d_cols.alloc(nc);
     BST_CK(cudaMemcpyAsync(d_cols.p, cols.data(), sizeof(BinColumn) * nc, cudaMemcpyHostToDevice, st));
     d_thr.alloc(std::max<size_t>(1, thr.size()));

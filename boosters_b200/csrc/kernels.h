@@ -56,6 +56,20 @@ void launch_bin_assign(const float* x_fm, uint64_t n, const BinColumn* cols, uin
                        const float* thr, const int32_t* cats, uint8_t* rec_out, uint32_t rec, uint32_t u16_off,
                        cudaStream_t st);
 
+// Numeric bin bounds of sampled features (dataset.rs:683-750), one block
+// per job: column `col` of x (feature-major, col_stride floats apart), its
+// rows `rows[0..k)` (ascending; null = rows 0..k-1). Per job: scratch 2k
+// words, cand max_bins doubles, bounds max_bins + 2 doubles (the upper
+// bounds, the last one DBL_MAX, then DBL_MAX again for the NaN bin when
+// has_nan and there are two or more distinct finite values) and n_bounds.
+struct MapJob {
+    uint32_t col;
+    uint32_t has_nan;
+};
+void launch_numeric_bounds(const float* x, uint64_t col_stride, const uint32_t* rows, uint32_t k, const MapJob* jobs,
+                           uint32_t n_jobs, uint32_t max_bins, uint32_t* scratch, double* cand, double* bounds,
+                           uint32_t* n_bounds, cudaStream_t st);
+
 // ---- K3 gradients ---------------------------------------------------------
 // maxabs [G][2] receives the bit patterns of max|grad|, max|hess| (atomicMax).
 // alpha: [G] pinball alphas (device); delta: the pseudo-Huber delta.
