@@ -205,6 +205,57 @@ def test_binning_parity_categorical_and_edge_columns():
     compare_binned(gb, ob.OracleBinned(x, cfg.to_c(), categorical=cats))
 
 
+def _edge_numeric_columns(n, rng):
+    """Numeric columns that reach every branch of the device bounds: signed
+    zeros (one distinct value), exactly max_bins and max_bins + 1 distinct
+    values, heavy ties, NaN and infinities mixed in, one distinct finite
+    value beside NaN, a column of every row distinct."""
+    cols = []
+    z = np.where(rng.random(n) < 0.5, np.float32(-0.0), np.float32(0.0)).astype(np.float32)
+    z[::7] = 1.5
+    cols.append(z)                                                       # -0.0 / +0.0 merge, then 1.5
+    cols.append((rng.integers(0, 32, n) * 0.25).astype(np.float32))      # 32 distinct = max_bins
+    cols.append((rng.integers(0, 33, n) * 0.25).astype(np.float32))      # 33 distinct: quantiles
+    t = rng.normal(size=n).astype(np.float32)
+    t[rng.random(n) < 0.6] = 2.0                                         # heavy ties
+    t[::11] = np.nan
+    t[::13] = np.inf
+    t[::17] = -np.inf
+    cols.append(t)
+    c = np.full(n, 4.0, np.float32)
+    c[::3] = np.nan                                                      # one value + NaN: one bin
+    cols.append(c)
+    cols.append(np.arange(n, dtype=np.float32) * np.float32(-0.5))      # all distinct, negative
+    return np.stack(cols)
+
+
+@pytest.mark.parametrize("n", [100, 3000, 9000])
+def test_binning_parity_device_bounds_edges(n):
+    rng = np.random.default_rng(n)
+    x = _edge_numeric_columns(n, rng)
+    for mb in (32, 2):
+        cfg = _cfg(max_bins=mb)
+        gb = bst.BinnedDataset(bst.Dataset.from_feature_major(x), cfg)
+        compare_binned(gb, ob.OracleBinned(x, cfg.to_c()))
+
+
+def test_binning_device_bounds_pinned_equals_pageable():
+    # pinned inputs go up as one asynchronous copy, pageable ones on a
+    # helper thread: the same bins either way
+    import torch
+
+    x, _ = bst.synth.binary(240_000, 12, n_nan_cols=4, seed=9)
+    cfg = _cfg()
+    xp = torch.from_numpy(x).pin_memory().numpy()
+    a = bst.BinnedDataset(bst.Dataset.from_feature_major(x), cfg)
+    b = bst.BinnedDataset(bst.Dataset.from_feature_major(xp), cfg)
+    assert a.n_columns == b.n_columns
+    for c in range(a.n_columns):
+        assert a.column_info(c) == b.column_info(c)
+        np.testing.assert_array_equal(a.column_bounds(c), b.column_bounds(c))
+        np.testing.assert_array_equal(a.column_bins(c), b.column_bins(c))
+
+
 # ------------------------------------------------------------------ training
 
 @pytest.mark.parametrize("n_threads", [1, 0])
