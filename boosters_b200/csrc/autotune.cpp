@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <map>
 #include <mutex>
 #include <sstream>
 
@@ -45,7 +46,16 @@ bool TuneShape::parse(const std::string& s, TuneShape& out) {
     return true;
 }
 
+// Computed once per device and process: cudaGetDeviceProperties takes
+// milliseconds, and every training call asks.
 std::string device_signature(int device) {
+    static std::mutex mu;
+    static std::map<int, std::string> known;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = known.find(device);
+        if (it != known.end()) return it->second;
+    }
     cudaDeviceProp p{};
     if (cudaGetDeviceProperties(&p, device) != cudaSuccess) {
         cudaGetLastError();
@@ -54,8 +64,10 @@ std::string device_signature(int device) {
     std::string name = p.name;
     for (char& c : name)
         if (c == '\t' || c == '\n' || c == '|') c = ' ';
-    return name + "|" + std::to_string(p.multiProcessorCount) + "|" + std::to_string(p.major) + "." +
-           std::to_string(p.minor);
+    name += "|" + std::to_string(p.multiProcessorCount) + "|" + std::to_string(p.major) + "." + std::to_string(p.minor);
+    std::lock_guard<std::mutex> lk(mu);
+    known[device] = name;
+    return name;
 }
 
 namespace {

@@ -126,7 +126,10 @@ extern "C" {
 
 const char* bst_last_error(void) { return g_err.c_str(); }
 const char* bst_version(void) { return "boosters-b200 0.1.0 (sm_100a)"; }
-void bst_release_cached_memory(void) { bst::dev_cache_trim(); }
+void bst_release_cached_memory(void) {
+    bst::dev_cache_trim();
+    bst::pinned_cache_trim();
+}
 
 void bst_config_default(bst_config* c) {
     if (!c) return;

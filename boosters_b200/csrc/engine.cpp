@@ -92,6 +92,73 @@ size_t dev_round(size_t b) {
 
 }  // namespace
 
+// Pinned host blocks, kept for reuse like the device blocks: a training
+// call's staging area and read-back slots would otherwise cost a
+// cudaMallocHost and a (device-synchronising) cudaFreeHost each.
+namespace {
+struct PinnedCache {
+    std::mutex mu;
+    std::multimap<size_t, void*> blocks;     // free: size -> pointer
+    std::unordered_map<void*, size_t> live;  // handed out: pointer -> size
+    size_t bytes = 0;                        // free bytes
+};
+PinnedCache& pinned_cache() {
+    static PinnedCache* c = new PinnedCache();  // never destroyed (see dev_cache)
+    return *c;
+}
+constexpr size_t PINNED_CACHE_MAX = (size_t)256 << 20;
+}  // namespace
+
+void* pinned_alloc(size_t bytes) {
+    const size_t r = dev_round(bytes);
+    PinnedCache& c = pinned_cache();
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        auto it = c.blocks.lower_bound(r);
+        if (it != c.blocks.end() && it->first <= 2 * r) {
+            void* p = it->second;
+            c.live[p] = it->first;
+            c.bytes -= it->first;
+            c.blocks.erase(it);
+            return p;
+        }
+    }
+    void* p = nullptr;
+    BST_CK(cudaMallocHost(&p, r));
+    std::lock_guard<std::mutex> lk(c.mu);
+    c.live[p] = r;
+    return p;
+}
+
+void pinned_free(void* p) {
+    if (!p) return;
+    cudaDeviceSynchronize();  // no copy into or out of the block is pending (cudaFreeHost would wait too)
+    cudaGetLastError();
+    PinnedCache& c = pinned_cache();
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        auto it = c.live.find(p);
+        const size_t sz = it == c.live.end() ? 0 : it->second;
+        if (it != c.live.end()) c.live.erase(it);
+        if (sz && c.bytes + sz <= PINNED_CACHE_MAX) {
+            c.blocks.emplace(sz, p);
+            c.bytes += sz;
+            return;
+        }
+    }
+    cudaFreeHost(p);
+    cudaGetLastError();
+}
+
+void pinned_cache_trim() {
+    PinnedCache& c = pinned_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    for (auto& e : c.blocks) cudaFreeHost(e.second);
+    cudaGetLastError();
+    c.blocks.clear();
+    c.bytes = 0;
+}
+
 void dev_cache_trim() {
     DevCache& c = dev_cache();
     std::lock_guard<std::mutex> lk(c.mu);
@@ -470,14 +537,12 @@ std::vector<uint32_t> bitset_words(const unsigned long long cats[4]) {  // categ
 struct Staging {
     char* p = nullptr;
     size_t cap = 0, off = 0;
-    ~Staging() {
-        if (p) cudaFreeHost(p);
-    }
+    ~Staging() { pinned_free(p); }
     void reserve(size_t bytes) {
         if (bytes <= cap) return;
-        if (p) cudaFreeHost(p);
+        pinned_free(p);
         p = nullptr;
-        BST_CK(cudaMallocHost(&p, bytes));
+        p = static_cast<char*>(pinned_alloc(bytes));
         cap = bytes;
         off = 0;
     }
@@ -1216,8 +1281,8 @@ class Trainer {
         for (auto g : graphs_)
             if (g) cudaGraphExecDestroy(g);
         for (auto& sl : slots_) {
-            if (sl.tree) cudaFreeHost(sl.tree);
-            if (sl.state) cudaFreeHost(sl.state);
+            pinned_free(sl.tree);
+            pinned_free(sl.state);
             for (auto e : {sl.done, sl.w0, sl.w1})
                 if (e) cudaEventDestroy(e);
         }
@@ -1404,8 +1469,8 @@ class Trainer {
         d_root_scan_.alloc(1);
         BST_CK(cudaMemcpy(d_root_scan_.p, &rs, sizeof(rs), cudaMemcpyHostToDevice));
         for (auto& sl : slots_) {
-            BST_CK(cudaMallocHost(&sl.tree, sizeof(BTreeNode) * max_tnodes_));
-            BST_CK(cudaMallocHost(&sl.state, sizeof(BState)));
+            sl.tree = static_cast<BTreeNode*>(pinned_alloc(sizeof(BTreeNode) * max_tnodes_));
+            sl.state = static_cast<BState*>(pinned_alloc(sizeof(BState)));
             BST_CK(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
             BST_CK(cudaEventCreate(&sl.w0));
             BST_CK(cudaEventCreate(&sl.w1));
@@ -2251,8 +2316,8 @@ class Trainer {
         bd_.scnt = rowsample_ ? d_scnt_.p : nullptr;
         bd_.max_front = mp;
         bd_.max_tnodes = (uint32_t)d_btree_.n;
-        if (!h_lw_state_) BST_CK(cudaMallocHost(&h_lw_state_, sizeof(LwState)));
-        if (!h_lw_bstate_) BST_CK(cudaMallocHost(&h_lw_bstate_, sizeof(BState)));
+        if (!h_lw_state_) h_lw_state_ = static_cast<LwState*>(pinned_alloc(sizeof(LwState)));
+        if (!h_lw_bstate_) h_lw_bstate_ = static_cast<BState*>(pinned_alloc(sizeof(BState)));
         lw_graphs_.assign(G_, nullptr);
         lw_launches_.assign(G_, 0);
         lw_hist_launches_.assign(G_, 0);
@@ -2270,8 +2335,8 @@ class Trainer {
         for (auto g : lw_graphs_)
             if (g) cudaGraphExecDestroy(g);
         lw_graphs_.clear();
-        if (h_lw_state_) cudaFreeHost(h_lw_state_);
-        if (h_lw_bstate_) cudaFreeHost(h_lw_bstate_);
+        pinned_free(h_lw_state_);
+        pinned_free(h_lw_bstate_);
         h_lw_state_ = nullptr;
         h_lw_bstate_ = nullptr;
     }

@@ -44,6 +44,11 @@ void dev_bytes_release(size_t bytes);
 void* dev_alloc(size_t bytes, size_t* block_bytes);  // throws Error
 void dev_free(void* p, size_t block_bytes);
 void dev_cache_trim();  // frees every cached block
+// Pinned host memory from a process-wide cache of blocks (pinned_free waits
+// for the device to be idle, as cudaFreeHost does, then keeps the block).
+void* pinned_alloc(size_t bytes);
+void pinned_free(void* p);
+void pinned_cache_trim();  // frees every cached pinned block
 
 template <class T>
 struct DevArray {

@@ -48,8 +48,9 @@ const char* bst_last_error(void);
 const char* bst_version(void);
 /* Device buffers released by the library (after a training call, a
  * server, a prediction) are kept per device for reuse, up to the
- * environment variable BST_DEVICE_CACHE_BYTES (default 8 GiB); this frees
- * them, e.g. before another allocator on the same GPU needs the memory.
+ * environment variable BST_DEVICE_CACHE_BYTES (default 8 GiB), and the
+ * pinned host blocks of training calls up to 256 MiB; this frees both,
+ * e.g. before another allocator on the same GPU needs the memory.
  * No reference counterpart. */
 void bst_release_cached_memory(void);
 
