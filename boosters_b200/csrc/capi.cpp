@@ -723,7 +723,8 @@ bst_status bst_bin_values(const double* bounds, uint32_t n_bounds, int32_t missi
         // one column: a 32-byte record per value, the bin at byte 0
         constexpr uint32_t REC = 32;
         rec.alloc(n * REC);
-        bst::launch_bin_assign(dx.p, n, dcol.p, 1, dthr.p, dc.p, rec.p, REC, 0, st);
+        bst::launch_bin_assign(dx.p, n, dcol.p, 1, dthr.p, dc.p, rec.p, REC, 0,
+                               (uint32_t)std::max(thr.size(), cv.size()), st);
         BST_CK(cudaGetLastError());
         BST_CK(cudaDeviceSynchronize());
         if (!wide) {

@@ -2826,7 +2826,6 @@ void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, 
         out.binning_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         return;
     }
-    if (bin_assign_rows(p.rec) == 0) throw Error{BST_ERR_UNSUPPORTED, "too many features for one row tile"};
     std::vector<BinColumn> cols(nc);
     std::vector<float> thr;
     std::vector<int32_t> cats;
@@ -2865,7 +2864,10 @@ void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, 
     if (p.rec) out.rec.alloc((size_t)n * p.rec);
     out.bins8 = out.rec.p;
     out.bins16 = p.f16 ? reinterpret_cast<uint16_t*>(out.rec.p + p.u16_off) : nullptr;
-    launch_bin_assign(x.p, n, d_cols.p, nc, d_thr.p, d_cats.p, out.rec.p, p.rec, p.u16_off, st);
+    uint32_t max_tab = 0;
+    for (const BinColumn& bc : cols) max_tab = std::max(max_tab, bc.is_cat ? bc.n_cats : bc.n_search);
+    if (bin_assign_rows(p.rec, max_tab) == 0) throw Error{BST_ERR_UNSUPPORTED, "too many features for one row tile"};
+    launch_bin_assign(x.p, n, d_cols.p, nc, d_thr.p, d_cats.p, out.rec.p, p.rec, p.u16_off, max_tab, st);
     BST_CK(cudaGetLastError());
     BST_CK(cudaStreamSynchronize(st));
     out.binning_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

@@ -116,29 +116,40 @@ __device__ __forceinline__ long long shfl_up_ll(long long v, int d) {
 // Reads the feature-major f32 matrix coalesced, writes row-major bins.
 // ============================================================================
 
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(256)
 k_bin_assign(const float* __restrict__ x, uint64_t n, const BinColumn* __restrict__ cols,
              uint32_t n_cols, const float* __restrict__ thr, const int32_t* __restrict__ cats,
-             uint8_t* __restrict__ rec_out, uint32_t rec, uint32_t u16_off) {
+             uint8_t* __restrict__ rec_out, uint32_t rec, uint32_t u16_off, uint32_t tab_cap) {
     BST_PDL_ENTER();
     // one thread per row of a tile of blockDim.x rows; the tile's records are
-    // assembled in shared memory, then copied out as one contiguous run
+    // assembled in shared memory, then copied out as one contiguous run. Each
+    // column's search table (thresholds or categories) is staged in shared
+    // memory first, two buffers alternating, so the lanes' divergent binary
+    // searches read shared memory instead of serialising in L1.
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t rows = blockDim.x;
+    uint32_t* tabs = reinterpret_cast<uint32_t*>(smem + (size_t)rows * rec);  // 2 x tab_cap words
     const uint64_t r0 = (uint64_t)blockIdx.x * rows;
     const uint64_t rem = n - r0;
     const uint32_t valid = rem < (uint64_t)rows ? (uint32_t)rem : rows;
     const uint32_t tile_bytes = rows * rec;  // rec is a multiple of 32
     for (uint32_t i = threadIdx.x * 16u; i < tile_bytes; i += rows * 16u)
         *reinterpret_cast<uint4*>(smem + i) = make_uint4(0, 0, 0, 0);
-    __syncthreads();
     const uint32_t t = threadIdx.x;
-    if (t < valid) {
-        const uint64_t row = r0 + t;
-        unsigned char* my = smem + (size_t)t * rec;
-        for (uint32_t c = 0; c < n_cols; ++c) {
-            const BinColumn col = cols[c];
-            const float v = x[(uint64_t)col.src * n + row];
+    const uint64_t row = r0 + t;
+    unsigned char* my = smem + (size_t)t * rec;
+    for (uint32_t c = 0; c < n_cols; ++c) {
+        const BinColumn col = cols[c];
+        const float v = t < valid ? x[(uint64_t)col.src * n + row] : 0.0f;
+        uint32_t* tb = tabs + (c & 1u) * tab_cap;
+        const uint32_t cnt = col.is_cat ? col.n_cats : col.n_search;
+        const uint32_t* src = col.is_cat ? reinterpret_cast<const uint32_t*>(cats + col.off)
+                                         : reinterpret_cast<const uint32_t*>(thr + col.off);
+        for (uint32_t i = t; i < cnt; i += rows) tb[i] = src[i];
+        // the table of column c - 1 (the other buffer) is no longer read
+        // once every thread passes this barrier; c + 1 overwrites it
+        __syncthreads();
+        if (t < valid) {
             uint32_t bin;
             if (v != v) {
                 bin = col.nan_bin;
@@ -146,22 +157,20 @@ k_bin_assign(const float* __restrict__ x, uint64_t n, const BinColumn* __restric
                 bin = col.zero_bin;
             } else if (col.is_cat) {
                 const int32_t key = sat_i32((double)v);
-                const int32_t* cs = cats + col.off;
                 uint32_t lo = 0, hi = col.n_cats;
                 while (lo < hi) {
                     uint32_t mid = (lo + hi) >> 1;
-                    if (cs[mid] < key)
+                    if ((int32_t)tb[mid] < key)
                         lo = mid + 1;
                     else
                         hi = mid;
                 }
-                bin = (lo < col.n_cats && cs[lo] == key) ? lo : 0u;
+                bin = (lo < col.n_cats && (int32_t)tb[lo] == key) ? lo : 0u;
             } else {
-                const float* th = thr + col.off;
                 uint32_t lo = 0, hi = col.n_search;
                 while (lo < hi) {
                     uint32_t mid = lo + ((hi - lo) >> 1);
-                    if (v <= th[mid])
+                    if (v <= __uint_as_float(tb[mid]))
                         hi = mid;
                     else
                         lo = mid + 1;
@@ -177,27 +186,35 @@ k_bin_assign(const float* __restrict__ x, uint64_t n, const BinColumn* __restric
     __syncthreads();
     const uint32_t nvec = valid * rec / 16u;
     uint4* dst = reinterpret_cast<uint4*>(rec_out + r0 * rec);
-    const uint4* src = reinterpret_cast<const uint4*>(smem);
-    for (uint32_t i = threadIdx.x; i < nvec; i += rows) dst[i] = src[i];
+    const uint4* srcv = reinterpret_cast<const uint4*>(smem);
+    for (uint32_t i = threadIdx.x; i < nvec; i += rows) dst[i] = srcv[i];
 }
 
-int bin_assign_rows(uint32_t rec) {
-    for (int rows = 128; rows >= 32; rows -= 32)
-        if ((size_t)rows * rec <= 160 * 1024) return rows;
+// Search-table words per buffer (a multiple of 4, so the tables stay 16-byte
+// aligned) and rows per block: 256 down to 32 while the record tile and the
+// two tables fit 160 KB.
+static uint32_t bin_assign_tab_cap(uint32_t max_tab) { return ((max_tab ? max_tab : 1u) + 3u) & ~3u; }
+
+int bin_assign_rows(uint32_t rec, uint32_t max_tab) {
+    const size_t tabs = 8u * (size_t)bin_assign_tab_cap(max_tab);
+    for (int rows = 256; rows >= 32; rows -= 32)
+        if ((size_t)rows * rec + tabs <= 160 * 1024) return rows;
     return 0;
 }
 
 void launch_bin_assign(const float* x_fm, uint64_t n, const BinColumn* cols, uint32_t n_cols,
                        const float* thr, const int32_t* cats, uint8_t* rec_out, uint32_t rec, uint32_t u16_off,
-                       cudaStream_t st) {
+                       uint32_t max_tab, cudaStream_t st) {
     if (n == 0 || n_cols == 0 || rec == 0) return;
-    const int rows = bin_assign_rows(rec);
+    const int rows = bin_assign_rows(rec, max_tab);
     if (rows == 0) return;
+    const uint32_t cap = bin_assign_tab_cap(max_tab);
     const uint64_t blocks = (n + rows - 1) / rows;
-    const size_t smem = (size_t)rows * rec;
+    const size_t smem = (size_t)rows * rec + 8u * (size_t)cap;
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_bin_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    launch_k(k_bin_assign, (unsigned)blocks, rows, smem, st, x_fm, n, cols, n_cols, thr, cats, rec_out, rec, u16_off);
+    launch_k(k_bin_assign, (unsigned)blocks, rows, smem, st, x_fm, n, cols, n_cols, thr, cats, rec_out, rec, u16_off,
+             cap);
 }
 
 // ============================================================================

@@ -50,11 +50,12 @@ struct BinColumn {
 
 // thr holds, per numeric column, the largest f32 <= each f64 upper bound, so
 // `v <= bound` (f64) equals `v <= thr` (f32) for every f32 v.
-// Rows per bin-assignment block for this record size (0 = row too wide).
-int bin_assign_rows(uint32_t rec);
+// Rows per bin-assignment block for this record size and largest search
+// table (the most thresholds or categories of a column; 0 = row too wide).
+int bin_assign_rows(uint32_t rec, uint32_t max_tab);
 void launch_bin_assign(const float* x_fm, uint64_t n, const BinColumn* cols, uint32_t n_cols,
                        const float* thr, const int32_t* cats, uint8_t* rec_out, uint32_t rec, uint32_t u16_off,
-                       cudaStream_t st);
+                       uint32_t max_tab, cudaStream_t st);
 
 // Numeric bin bounds of sampled features (dataset.rs:683-750), one block
 // per job: column `col` of x (feature-major, col_stride floats apart), its
