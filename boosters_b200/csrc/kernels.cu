@@ -1796,6 +1796,16 @@ __device__ __forceinline__ long long warp_incl_scan(long long v, int lane) {
     return v;
 }
 
+// 32-bit form for the HBin32 histograms (every prefix of a node's bins is
+// bounded by its exact total, which fits 31 bits there): one shuffle a step.
+__device__ __forceinline__ int warp_incl_scan(int v, int lane) {
+    for (int d = 1; d < 32; d <<= 1) {
+        const int t = __shfl_up_sync(FULL, v, d);
+        if (lane >= d) v += t;
+    }
+    return v;
+}
+
 __device__ __forceinline__ long long warp_sum_ll(long long v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
     return v;
@@ -1882,18 +1892,20 @@ __device__ float scan_item(const ScanNode nd, uint32_t node, uint32_t col, const
             // (missing left) when the column has a NaN bin (the last bin).
             const bool hm = cm.has_missing != 0;
             const long long pm_g = tg - h[nb - 1].g, pm_h = th - h[nb - 1].h;  // P[nb-2]
-            long long carry_g = 0, carry_h = 0;
+            using Acc = decltype(HB{}.g);  // int for HBin32: 32-bit prefix scans
+            Acc carry_g = 0, carry_h = 0;
             for (uint32_t base = 0; base < nb; base += 32) {
                 const uint32_t b = base + lane;
-                long long vg = 0, vh = 0;
+                Acc vg = 0, vh = 0;
                 if (b < nb) {
                     vg = h[b].g;
                     vh = h[b].h;
                 }
-                const long long Pg = warp_incl_scan(vg, lane) + carry_g;
-                const long long Ph = warp_incl_scan(vh, lane) + carry_h;
-                carry_g = __shfl_sync(FULL, Pg, 31);
-                carry_h = __shfl_sync(FULL, Ph, 31);
+                const Acc Pg_ = warp_incl_scan(vg, lane) + carry_g;
+                const Acc Ph_ = warp_incl_scan(vh, lane) + carry_h;
+                carry_g = __shfl_sync(FULL, Pg_, 31);
+                carry_h = __shfl_sync(FULL, Ph_, 31);
+                const long long Pg = Pg_, Ph = Ph_;
                 if (b + 1 < nb) {  // forward candidate: bins <= b go left
                     const double lg = (double)Pg * ig, lh = (double)Ph * ih;
                     const double rg = (double)(tg - Pg) * ig, rh = (double)(th - Ph) * ih;
@@ -1994,19 +2006,21 @@ __device__ float scan_item(const ScanNode nd, uint32_t node, uint32_t col, const
                     __syncwarp();
                 }
             }
-            long long carry_g = 0, carry_h = 0;
+            using Acc = decltype(HB{}.g);
+            Acc carry_g = 0, carry_h = 0;
             for (uint32_t base = 0; base + 1 < m; base += 32) {
                 const uint32_t i = base + lane;
-                long long vg = 0, vh = 0;
+                Acc vg = 0, vh = 0;
                 if (i + 1 < m) {
                     const uint32_t c = cat[i];
                     vg = h[c].g;
                     vh = h[c].h;
                 }
-                const long long Pg = warp_incl_scan(vg, lane) + carry_g;
-                const long long Ph = warp_incl_scan(vh, lane) + carry_h;
-                carry_g = __shfl_sync(FULL, Pg, 31);
-                carry_h = __shfl_sync(FULL, Ph, 31);
+                const Acc Pg_ = warp_incl_scan(vg, lane) + carry_g;
+                const Acc Ph_ = warp_incl_scan(vh, lane) + carry_h;
+                carry_g = __shfl_sync(FULL, Pg_, 31);
+                carry_h = __shfl_sync(FULL, Ph_, 31);
+                const long long Pg = Pg_, Ph = Ph_;
                 if (i + 1 < m) {
                     const double lg = (double)Pg * ig, lh = (double)Ph * ih;
                     const double rg = (double)(tg - Pg) * ig, rh = (double)(th - Ph) * ih;
