@@ -1,4 +1,6 @@
-// binning.cpp — per-feature analysis and bin bounds on the host.
+// binning.cpp — per-feature analysis, the row sample and the categorical
+// mappers on the host; the numeric features' bounds come from a
+// NumericBounds (the engine's device sort, mappers.cu).
 //
 // Semantics follow data/binned/feature_analysis.rs:313-569 (analysis and
 // grouping) and data/binned/dataset.rs:592-750 (bin mappers). Features are
@@ -227,16 +229,27 @@ bst_status plan_binning(const float* x, uint64_t F, uint64_t n,
         const FeatureFacts& ff = facts[f];
         if (ff.trivial || ff.numeric) continue;
         {
-            // every finite value's category, not a sample (dataset.rs:655-672)
-            std::vector<int32_t> c;
-            c.reserve(1024);
-            std::unordered_set<int32_t> seen;
-            for (uint64_t i = 0; i < n; ++i)
-                if (std::isfinite(col[i])) {
-                    const int32_t k = trunc_i32((double)col[i]);
-                    if (seen.insert(k).second) c.push_back(k);
-                }
-            std::sort(c.begin(), c.end());
+            // every finite value's category, not a sample (dataset.rs:655-672):
+            // categories in [0, 65536) in a bitmap, any others in a hash set;
+            // the sorted distinct list is the same either way
+            std::vector<uint64_t> small(1024, 0ull);
+            std::unordered_set<int32_t> other;
+            for (uint64_t i = 0; i < n; ++i) {
+                const float v = col[i];
+                if (!std::isfinite(v)) continue;
+                const int32_t k = trunc_i32((double)v);
+                if ((uint32_t)k < 65536u)
+                    small[(uint32_t)k >> 6] |= 1ull << ((uint32_t)k & 63u);
+                else
+                    other.insert(k);
+            }
+            std::vector<int32_t> c(other.begin(), other.end());
+            std::sort(c.begin(), c.end());  // negatives, then >= 65536
+            const auto split = std::lower_bound(c.begin(), c.end(), 0);
+            std::vector<int32_t> mid;
+            for (uint32_t w = 0; w < 1024; ++w)
+                for (uint64_t b = small[w]; b; b &= b - 1) mid.push_back((int32_t)(w * 64 + (uint32_t)__builtin_ctzll(b)));
+            c.insert(split, mid.begin(), mid.end());
             if (c.empty()) c.push_back(0);
             Mapper m;
             m.categorical = true;

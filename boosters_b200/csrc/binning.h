@@ -1,6 +1,7 @@
-// binning.h — host side of feature binning: per-feature analysis and bin
-// bounds (data/binned/feature_analysis.rs:313-569, data/binned/dataset.rs:592-750).
-// The bins themselves are assigned on the GPU (kernels.h, K1).
+// binning.h — the plan of feature binning: per-feature analysis, mappers and
+// the binned layout (data/binned/feature_analysis.rs:313-569,
+// data/binned/dataset.rs:592-750). Numeric bounds and the bins themselves
+// are computed on the GPU (kernels.h: launch_numeric_bounds, K1).
 #pragma once
 
 #include <stdint.h>

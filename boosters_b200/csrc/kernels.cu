@@ -1806,10 +1806,15 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane) {
     return v;
 }
 
-__device__ __forceinline__ long long warp_sum_ll(long long v) {
+__device__ __forceinline__ long long warp_sum(long long v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
     return v;
 }
+__device__ __forceinline__ int warp_sum(int v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
 
 struct GainCtx {
     double lambda, offset, mcw;
@@ -1851,13 +1856,13 @@ __device__ float scan_item(const ScanNode nd, uint32_t node, uint32_t col, const
     const uint32_t pc = nd.count;
 
     // node totals (every column's bins sum to the same exact total)
-    long long tg = 0, th = 0;
+    using TAcc = decltype(HB{}.g);  // int for HBin32: 32-bit sums
+    TAcc tg_ = 0, th_ = 0;
     for (uint32_t b = lane; b < nb; b += 32) {
-        tg += h[b].g;
-        th += h[b].h;
+        tg_ += h[b].g;
+        th_ += h[b].h;
     }
-    tg = warp_sum_ll(tg);
-    th = warp_sum_ll(th);
+    long long tg = warp_sum(tg_), th = warp_sum(th_);
     if (nd.flags & 1u) {
         tg = nd.pg;
         th = nd.ph;
@@ -3626,7 +3631,7 @@ __device__ __forceinline__ unsigned long long cand_key(float g, uint32_t col, in
 // frontier b's splits (the winner's full candidate from cand), resets the
 // keys, and derives the next level's decisions (rows in buffer buf).
 template <typename HB>
-__global__ void __launch_bounds__(SCAN_WARPS * 32)
+__global__ void __launch_bounds__(SCAN_WARPS * 32, 4)
 k_b_scan(BDev d, const ScanColumn* __restrict__ cols, uint32_t n_cols, const HB* __restrict__ hist,
          uint64_t slot_bins, const double* __restrict__ scale, GainParamsDev gp, ColCand* __restrict__ cand,
          long long* __restrict__ node_tot, int b, int last_wins, LeafParams lp, uint32_t buf,
