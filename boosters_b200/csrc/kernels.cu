@@ -126,18 +126,20 @@ k_bin_assign(const float* __restrict__ x, uint64_t n, const BinColumn* __restric
     // column's search table (thresholds or categories) is staged in shared
     // memory first, two buffers alternating, so the lanes' divergent binary
     // searches read shared memory instead of serialising in L1.
+    // records are rec + 4 bytes apart in shared memory, so the lanes'
+    // writes of one column (one row each) fall in different banks
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t rows = blockDim.x;
-    uint32_t* tabs = reinterpret_cast<uint32_t*>(smem + (size_t)rows * rec);  // 2 x tab_cap words
+    const uint32_t rs = rec + 4u;
+    uint32_t* tabs = reinterpret_cast<uint32_t*>(smem + (size_t)rows * rs);  // 2 x tab_cap words
     const uint64_t r0 = (uint64_t)blockIdx.x * rows;
     const uint64_t rem = n - r0;
     const uint32_t valid = rem < (uint64_t)rows ? (uint32_t)rem : rows;
-    const uint32_t tile_bytes = rows * rec;  // rec is a multiple of 32
-    for (uint32_t i = threadIdx.x * 16u; i < tile_bytes; i += rows * 16u)
-        *reinterpret_cast<uint4*>(smem + i) = make_uint4(0, 0, 0, 0);
+    const uint32_t tile_words = rows * rs / 4u;
+    for (uint32_t i = threadIdx.x; i < tile_words; i += rows) reinterpret_cast<uint32_t*>(smem)[i] = 0u;
     const uint32_t t = threadIdx.x;
     const uint64_t row = r0 + t;
-    unsigned char* my = smem + (size_t)t * rec;
+    unsigned char* my = smem + (size_t)t * rs;
     for (uint32_t c = 0; c < n_cols; ++c) {
         const BinColumn col = cols[c];
         const float v = t < valid ? x[(uint64_t)col.src * n + row] : 0.0f;
@@ -184,10 +186,10 @@ k_bin_assign(const float* __restrict__ x, uint64_t n, const BinColumn* __restric
         }
     }
     __syncthreads();
-    const uint32_t nvec = valid * rec / 16u;
-    uint4* dst = reinterpret_cast<uint4*>(rec_out + r0 * rec);
-    const uint4* srcv = reinterpret_cast<const uint4*>(smem);
-    for (uint32_t i = threadIdx.x; i < nvec; i += rows) dst[i] = srcv[i];
+    const uint32_t wpr = rec / 4u, nw = valid * wpr;  // rec is a multiple of 32
+    uint32_t* dst = reinterpret_cast<uint32_t*>(rec_out + r0 * rec);
+    const uint32_t* srcw = reinterpret_cast<const uint32_t*>(smem);
+    for (uint32_t i = threadIdx.x; i < nw; i += rows) dst[i] = srcw[(i / wpr) * (rs / 4u) + i % wpr];
 }
 
 // Search-table words per buffer (a multiple of 4, so the tables stay 16-byte
@@ -198,7 +200,7 @@ static uint32_t bin_assign_tab_cap(uint32_t max_tab) { return ((max_tab ? max_ta
 int bin_assign_rows(uint32_t rec, uint32_t max_tab) {
     const size_t tabs = 8u * (size_t)bin_assign_tab_cap(max_tab);
     for (int rows = 256; rows >= 32; rows -= 32)
-        if ((size_t)rows * rec + tabs <= 160 * 1024) return rows;
+        if ((size_t)rows * (rec + 4u) + tabs <= 160 * 1024) return rows;
     return 0;
 }
 
@@ -210,7 +212,7 @@ void launch_bin_assign(const float* x_fm, uint64_t n, const BinColumn* cols, uin
     if (rows == 0) return;
     const uint32_t cap = bin_assign_tab_cap(max_tab);
     const uint64_t blocks = (n + rows - 1) / rows;
-    const size_t smem = (size_t)rows * rec + 8u * (size_t)cap;
+    const size_t smem = (size_t)rows * (rec + 4u) + 8u * (size_t)cap;
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_bin_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
     launch_k(k_bin_assign, (unsigned)blocks, rows, smem, st, x_fm, n, cols, n_cols, thr, cats, rec_out, rec, u16_off,
