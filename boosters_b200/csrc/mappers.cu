@@ -22,7 +22,7 @@ namespace {
 constexpr unsigned FULL = 0xFFFFFFFFu;
 constexpr int MAP_THREADS = 1024;
 constexpr int MAP_WARPS = MAP_THREADS / 32;
-constexpr int MAP_ITEMS = 4;                                  // keys per thread and tile
+constexpr int MAP_ITEMS = 8;                                  // keys per thread and tile
 constexpr uint32_t MAP_WARP_KEYS = 32u * MAP_ITEMS;           // keys per warp and tile
 constexpr uint32_t MAP_TILE = MAP_THREADS * MAP_ITEMS;        // keys per tile
 constexpr int MAP_QUARTERS = 4;                               // cross-warp scan: 4 x 8 warps
