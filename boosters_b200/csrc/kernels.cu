@@ -1393,8 +1393,9 @@ __device__ __forceinline__ void merge_store(HB* __restrict__ hist, uint64_t slot
 // record). Consecutive threads read consecutive partial entries and touch
 // consecutive bins of the node histograms. Each thread handles MERGE_ILP
 // entries at once and loads four segments' partials at a time, so that the
-// dependent loads overlap.
-constexpr uint32_t MERGE_ILP = 2;
+// dependent loads overlap (1 entry measured faster than 2 or 4: more
+// threads in flight).
+constexpr uint32_t MERGE_ILP = 1;
 
 template <int MODE, typename HB>
 __global__ void __launch_bounds__(256, 4)
