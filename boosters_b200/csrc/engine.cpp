@@ -792,12 +792,14 @@ class Trainer {
                 for (uint32_t o = 0; o < G_; ++o) launch_maxabs(gh_.p + (size_t)o * n_, n_, maxabs_.p + 2 * o, st_);
                 m_.counters.launches += 2 * G_;
             }
-            launch_fixed_scales(maxabs_.p, G_, n_, scales_.p, st_);
-            m_.counters.launches += 2;
-            if (qmode_ != GRAD_F32) {
-                launch_quantize(qmode_, G_, gh_.p, n_, maxabs_.p, cfg_.seed, round_no_, 0u, gq_.p, qscales_.p, st_);
-                m_.counters.launches += 1;
+            m_.counters.launches += 1;
+            if (qmode_ != GRAD_F32) {  // the quantisation also writes the fixed-point scales
+                launch_quantize(qmode_, G_, gh_.p, n_, maxabs_.p, cfg_.seed, round_no_, 0u, gq_.p, qscales_.p, st_,
+                                scales_.p);
+            } else {
+                launch_fixed_scales(maxabs_.p, G_, n_, scales_.p, st_);
             }
+            m_.counters.launches += 1;
             tree_round_ = round_no_;  // the round of this round's trees (column sampling)
             ++round_no_;
             timer_.end();
@@ -1546,10 +1548,8 @@ class Trainer {
         const uint64_t cb = scan_col_blocks(n_cols_);
         auto cap = [&](uint64_t items) { return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(g_wide, items)); };
         tm.begin(PH_OTHER);
-        launch_iota(ridx_.p, n_, st_);
-        launch_b_root(bd_, n_, st_);
+        launch_b_root_init(bd_, ridx_.p, n_, chunk_rows(n_), st_);  // row ids, root node, root histogram state
         if (n_tiles_) BST_CK(cudaMemsetAsync(hist_.p, 0, hbytes() * slot_bins_, st_));
-        launch_b_root_hist(bd_, n_, chunk_rows(n_), st_);
         tm.end();
         enqueue_hist(gh, ridx_.p, true, tm, launches, hist_launches, true);
         tm.begin(PH_SCAN);
@@ -1557,7 +1557,7 @@ class Trainer {
                       last_wins_ ? 1 : 0, lp, 0u, cap(cb), st_, hist32_, d_root_scan_.p,
                       colmask());  // + level-0 decisions
         tm.end();
-        launches += 4;
+        launches += 2;  // root init, root split search
         // row indices: level d partitions R[d & 1] into R[(d + 1) & 1]
         uint32_t* R[2] = {ridx_.p, tmp_.p};
         for (uint32_t d = 0; d < cfg_.max_depth; ++d) {

@@ -385,11 +385,9 @@ void launch_gradients(int objective, uint32_t G, const float* pred, const float*
                                                                           alpha, delta);
 }
 
-__global__ void k_fixed_scales(const unsigned* __restrict__ maxabs, uint32_t G, uint64_t n,
-                               double* __restrict__ scales) {
-    BST_PDL_ENTER();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= 2 * G) return;
+// Fixed-point scale of element i (output i / 2, grad or hess i % 2).
+__device__ void write_fixed_scale(const unsigned* __restrict__ maxabs, uint32_t i, uint64_t n,
+                                  double* __restrict__ scales) {
     const float m = __uint_as_float(maxabs[i]);
     int k = 0;
     if (m > 0.0f) {
@@ -408,6 +406,13 @@ __global__ void k_fixed_scales(const unsigned* __restrict__ maxabs, uint32_t G, 
     const uint32_t o = i >> 1, which = i & 1;
     scales[4 * o + which] = ldexp(1.0, k);
     scales[4 * o + 2 + which] = ldexp(1.0, -k);
+}
+
+__global__ void k_fixed_scales(const unsigned* __restrict__ maxabs, uint32_t G, uint64_t n,
+                               double* __restrict__ scales) {
+    BST_PDL_ENTER();
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 2 * G) write_fixed_scale(maxabs, i, n, scales);
 }
 
 void launch_fixed_scales(const unsigned* maxabs, uint32_t G, uint64_t n, double* scales,
@@ -1577,36 +1582,6 @@ void launch_b_merge(const BDev& d, void* hist, uint64_t slot_bins, uint32_t tota
                          has_rest, root, mode, st, wide);
 }
 
-// Level state for the root histogram: one "expanding node" whose smaller
-// child is all n rows (ridx is the identity), segments of `chunk` rows.
-__global__ void k_b_root_hist(BDev d, uint64_t n, uint32_t chunk) {
-    BST_PDL_ENTER();
-    uint32_t nseg = (uint32_t)((n + chunk - 1) / chunk);
-    if (nseg > d.max_segs) nseg = d.max_segs;  // never: the buffer is sized for it
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nseg; c += gridDim.x * blockDim.x) d.seg_exp[c] = 0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        BExp e;
-        e.front = 0;
-        e.right_pnode = 0;
-        e.tl = e.tr = 0;
-        e.lc = 0;
-        e.rc = (uint32_t)n;
-        e.small_begin = 0;
-        e.small_count = (uint32_t)n;
-        e.part_off = 0;
-        e.hist_off = 0;
-        e.left_pnode = 0;
-        e.pad1 = 0;
-        d.exp[0] = e;
-        d.state->n_exp = 1;
-        d.state->hist_chunks = nseg;
-        d.state->hist_chunk = chunk;
-    }
-}
-
-void launch_b_root_hist(const BDev& d, uint64_t n, uint32_t chunk, cudaStream_t st) {
-    launch_k(k_b_root_hist, 4, 256, 0, st, d, n, chunk);
-}
 
 template <int MODE>
 __global__ void __launch_bounds__(HIST_THREADS)
@@ -1719,7 +1694,7 @@ __device__ __forceinline__ int32_t stochastic_round(float v, double inv, uint32_
 template <int MODE>
 __global__ void k_quantize(const float2* __restrict__ gh, uint64_t n, uint32_t G, const unsigned* __restrict__ maxabs,
                            uint2 key, uint32_t round, uint32_t out0, void* __restrict__ gq,
-                           double* __restrict__ qscales) {
+                           double* __restrict__ qscales, double* __restrict__ fscales) {
     BST_PDL_ENTER();
     constexpr int32_t Q = MODE == GRAD_Q8 ? 127 : 32767;
     const uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1728,6 +1703,7 @@ __global__ void k_quantize(const float2* __restrict__ gh, uint64_t n, uint32_t G
         const uint32_t o = (uint32_t)(i0 >> 1), which = (uint32_t)(i0 & 1);
         qscales[4 * o + which] = m > 0.0f ? (double)Q / (double)m : 0.0;
         qscales[4 * o + 2 + which] = m > 0.0f ? (double)m / (double)Q : 0.0;
+        if (fscales) write_fixed_scale(maxabs, (uint32_t)i0, n, fscales);  // the exact leaf sums' scales
     }
     const uint64_t total = n * G;
     for (uint64_t i = i0; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -1746,17 +1722,20 @@ __global__ void k_quantize(const float2* __restrict__ gh, uint64_t n, uint32_t G
 }
 
 void launch_quantize(int mode, uint32_t G, const float2* gh, uint64_t n, const unsigned* maxabs, uint64_t seed,
-                     uint32_t round, uint32_t out0, void* gq, double* qscales, cudaStream_t st) {
+                     uint32_t round, uint32_t out0, void* gq, double* qscales, cudaStream_t st,
+                     double* fscales) {
     if (G == 0) return;
     const uint64_t total = n * G;
     uint64_t blocks = (total + 255) / 256;
     if (blocks > (uint64_t)sm_count() * 16) blocks = (uint64_t)sm_count() * 16;
-    if (blocks == 0) blocks = 1;
+    if (blocks < (2ull * G + 255) / 256) blocks = (2ull * G + 255) / 256;  // a thread per scale
     const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
     if (mode == GRAD_Q8)
-        launch_k(k_quantize<GRAD_Q8>, (unsigned)blocks, 256, 0, st, gh, n, G, maxabs, key, round, out0, gq, qscales);
+        launch_k(k_quantize<GRAD_Q8>, (unsigned)blocks, 256, 0, st, gh, n, G, maxabs, key, round, out0, gq, qscales,
+                 fscales);
     else
-        launch_k(k_quantize<GRAD_Q16>, (unsigned)blocks, 256, 0, st, gh, n, G, maxabs, key, round, out0, gq, qscales);
+        launch_k(k_quantize<GRAD_Q16>, (unsigned)blocks, 256, 0, st, gh, n, G, maxabs, key, round, out0, gq, qscales,
+                 fscales);
 }
 
 // ============================================================================
@@ -2499,9 +2478,19 @@ __device__ void write_leaf(BTreeNode& t, long long G, long long H, const double*
 
 }  // namespace
 
-__global__ void k_b_root(BDev d, uint64_t n) {
+
+// Start of a depth-wise tree in one launch: row ids 0..n-1, the root node
+// as the frontier, and the level state set up for the root histogram (one
+// expanding node whose smaller child is all n rows, in `chunk`-row
+// segments).
+__global__ void k_b_root_init(BDev d, uint32_t* __restrict__ ridx, uint64_t n, uint32_t chunk) {
     BST_PDL_ENTER();
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t nseg = (uint32_t)((n + chunk - 1) / chunk);
+    if (nseg > d.max_segs) nseg = d.max_segs;  // never: the buffer is sized for it
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) ridx[i] = (uint32_t)i;
+    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nseg; c += stride) d.seg_exp[c] = 0;
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
     BNode r;
     r.pnode = 0;
     r.tnode = 0;
@@ -2517,17 +2506,30 @@ __global__ void k_b_root(BDev d, uint64_t n) {
     r.split.tot_g = 0;
     r.split.tot_h = 0;
     d.front[0][0] = r;
+    BExp e;
+    e.front = 0;
+    e.right_pnode = 0;
+    e.tl = e.tr = 0;
+    e.lc = 0;
+    e.rc = (uint32_t)n;
+    e.small_begin = 0;
+    e.small_count = (uint32_t)n;
+    e.part_off = 0;
+    e.hist_off = 0;
+    e.left_pnode = 0;
+    e.pad1 = 0;
+    d.exp[0] = e;
     BState s;
     s.n_front = 1;
-    s.n_exp = 0;
+    s.n_exp = 1;
     s.n_pnodes = 1;
     s.n_tnodes = 1;
     s.part_chunks = 0;
-    s.hist_chunks = 0;
+    s.hist_chunks = nseg;
     s.n_leaves = 0;
     s.leaf_chunks = 0;
     s.first_right = 1;
-    s.hist_chunk = HIST_CHUNK_MAX;
+    s.hist_chunk = chunk;
     s.hist_rows = n;
     s.done = 0;
     s.err = 0;
@@ -2535,7 +2537,12 @@ __global__ void k_b_root(BDev d, uint64_t n) {
     *d.state = s;
 }
 
-void launch_b_root(const BDev& d, uint64_t n, cudaStream_t st) { launch_k(k_b_root, 1, 32, 0, st, d, n); }
+void launch_b_root_init(const BDev& d, uint32_t* ridx, uint64_t n, uint32_t chunk, cudaStream_t st) {
+    if (n == 0) return;
+    uint64_t blocks = (n + 255) / 256;
+    if (blocks > (uint64_t)sm_count() * 16) blocks = (uint64_t)sm_count() * 16;
+    launch_k(k_b_root_init, (unsigned)blocks, 256, 0, st, d, ridx, n, chunk);
+}
 
 
 

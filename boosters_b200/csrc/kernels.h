@@ -112,8 +112,11 @@ constexpr uint32_t QUANT_STREAM = 0x51A7E5EDu;
 // maxabs[2] = bit patterns of max|grad|, max|hess| over finite values (atomicMax; zero it first)
 void launch_maxabs(const float2* gh, uint64_t n, unsigned* maxabs, cudaStream_t st);
 // (outputs are numbered from out0 in the counter)
+// fscales (or null): also the fixed-point scales of launch_fixed_scales,
+// which then need no launch of their own.
 void launch_quantize(int mode, uint32_t G, const float2* gh, uint64_t n, const unsigned* maxabs,
-                     uint64_t seed, uint32_t round, uint32_t out0, void* gq, double* qscales, cudaStream_t st);
+                     uint64_t seed, uint32_t round, uint32_t out0, void* gq, double* qscales, cudaStream_t st,
+                     double* fscales = nullptr);
 
 // ---- K4 histogram build -----------------------------------------------------
 struct HistChunk {
@@ -419,7 +422,9 @@ void launch_lw_leaves(const BDev& d, cudaStream_t st);
 // Raises the dynamic shared-memory limits of the kernels that need > 48 KiB
 // (call once per device before any stream capture).
 void init_kernel_attributes();
-void launch_b_root(const BDev& d, uint64_t n, cudaStream_t st);
+// Row ids 0..n-1, the root node and the root histogram's level state of a
+// depth-wise tree.
+void launch_b_root_init(const BDev& d, uint32_t* ridx, uint64_t n, uint32_t chunk, cudaStream_t st);
 // Column-major copy of the bin matrices (BinsFM).
 void launch_transpose_bins(const uint8_t* b8, uint32_t s8, uint32_t f8, const uint16_t* b16, uint32_t s16,
                            uint32_t f16, uint64_t n, uint8_t* fm8, uint16_t* fm16, cudaStream_t st);
@@ -475,8 +480,6 @@ void launch_b_merge(const BDev& d, void* hist, uint64_t slot_bins, uint32_t tota
 constexpr uint32_t LW_K_FROM_STATE = 0xFFFFFFFFu;
 void launch_lw_children(const BDev& d, const PartWork* pw, const unsigned* cursors, uint32_t k, ScanNode* scan_nodes,
                         const unsigned* scnt, cudaStream_t st);
-// Level state of the root histogram: all n rows as one segment list.
-void launch_b_root_hist(const BDev& d, uint64_t n, uint32_t chunk, cudaStream_t st);
 // split finding of the level's nodes and the reduction over columns into
 // frontier b, then (last block) the decisions of the next level, whose rows
 // are in buffer buf
