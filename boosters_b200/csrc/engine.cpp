@@ -1595,13 +1595,15 @@ class Trainer {
                 tm.begin(PH_OTHER);
                 GradRef gl = gh;
                 gl.qpos = qpos_[(d + 1) & 1u].p;
-                launch_b_sums(bd_, rout, gl, a ^ 1, g_wide, st_);  // + children sums
+                // + children sums, then the tree's leaves (k_b_finalize's work)
+                launch_b_sums(bd_, rout, gl, a ^ 1, g_wide, st_, 1, lp, scale, cfg_.max_depth & 1u);
                 tm.end();
                 launches += 1;
             }
         }
         tm.begin(PH_LEAF);
-        launch_b_finalize(bd_, (int)(cfg_.max_depth & 1u), lp, scale, cfg_.max_depth & 1u, st_);
+        if (cfg_.max_depth == 0)  // a single leaf: no level ran the last sums
+            launch_b_finalize(bd_, 0, lp, scale, 0u, st_);
         if (qmode_ != GRAD_F32) {
             // leaves solved from the exact sums of the f32 gradients (+ values)
             launch_b_leaf_sums(bd_, R[0], R[1], exact_ref(o), lp, scales_.p + 4 * (size_t)o,

@@ -3743,12 +3743,14 @@ __device__ __forceinline__ void range_sums(uint32_t start, uint32_t len, const u
 }
 
 __device__ void children_sums_body(BDev d, int b);
+__device__ void finalize_body(BDev d, int a, LeafParams lp, const double* __restrict__ scale, uint32_t buf);
 
 // Node sums of the smaller children when the children are not split further
 // (d.sums zeroed by the partition's last block); the last block then gives
 // both children of every expansion their sums (frontier b).
 template <int MODE>
-__global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, GradRef gr, int b) {
+__global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, GradRef gr, int b, int finalize, LeafParams lp,
+                         const double* __restrict__ scale, uint32_t buf) {
     BST_PDL_ENTER();
     const uint32_t total = d.state->hist_chunks, CH = d.state->hist_chunk;
     const GradLoad<MODE> load(gr);
@@ -3768,16 +3770,22 @@ __global__ void k_b_sums(BDev d, const uint32_t* __restrict__ ridx, GradRef gr, 
             atomicAdd(reinterpret_cast<unsigned long long*>(&d.sums[2 * j + 1]), (unsigned long long)ah);
         }
     }
-    if (last_block(d.state)) children_sums_body(d, b);
+    if (!last_block(d.state)) return;
+    children_sums_body(d, b);
+    if (finalize) {  // the tree's leaves (k_b_finalize) in the same block
+        __syncthreads();
+        finalize_body(d, b, lp, scale, buf);
+    }
 }
 
-void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, int b, uint32_t grid, cudaStream_t st) {
+void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, int b, uint32_t grid, cudaStream_t st,
+                   int finalize, LeafParams lp, const double* scale, uint32_t buf) {
     if (gr.mode == GRAD_Q16)
-        launch_k(k_b_sums<GRAD_Q16>, grid, 256, 0, st, d, ridx, gr, b);
+        launch_k(k_b_sums<GRAD_Q16>, grid, 256, 0, st, d, ridx, gr, b, finalize, lp, scale, buf);
     else if (gr.mode == GRAD_Q8)
-        launch_k(k_b_sums<GRAD_Q8>, grid, 256, 0, st, d, ridx, gr, b);
+        launch_k(k_b_sums<GRAD_Q8>, grid, 256, 0, st, d, ridx, gr, b, finalize, lp, scale, buf);
     else
-        launch_k(k_b_sums<GRAD_F32>, grid, 256, 0, st, d, ridx, gr, b);
+        launch_k(k_b_sums<GRAD_F32>, grid, 256, 0, st, d, ridx, gr, b, finalize, lp, scale, buf);
 }
 
 __device__ void children_sums_body(BDev d, int b) {
@@ -3799,9 +3807,7 @@ __device__ void children_sums_body(BDev d, int b) {
 
 
 // Remaining frontier -> leaves (grower.rs:484-514); leaf row chunks.
-__global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams lp, const double* __restrict__ scale,
-                                                    uint32_t buf) {
-    BST_PDL_ENTER();
+__device__ void finalize_body(BDev d, int a, LeafParams lp, const double* __restrict__ scale, uint32_t buf) {
     __shared__ uint32_t sh[33];
     __shared__ uint32_t s_jc[1024], s_own[1024], s_begin[1024];
     __shared__ uint32_t base, nf, n0;
@@ -3848,6 +3854,12 @@ __global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams l
         s->leaf_chunks = base < d.max_leaf_chunks ? base : d.max_leaf_chunks;
         s->n_front = 0;
     }
+}
+
+__global__ void __launch_bounds__(1024) k_b_finalize(BDev d, int a, LeafParams lp, const double* __restrict__ scale,
+                                                    uint32_t buf) {
+    BST_PDL_ENTER();
+    finalize_body(d, a, lp, scale, buf);
 }
 
 void launch_b_finalize(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st) {

@@ -494,8 +494,10 @@ void launch_b_scan(const BDev& d, const ScanColumn* cols, uint32_t n_cols, const
                    cudaStream_t st, int hist32 = 0, const ScanNode* root = nullptr,
                    const uint8_t* colmask = nullptr, NodeSplit* lw_out = nullptr);
 // last level: the smaller children's sums, then (last block) both children's
-// sums into frontier b
-void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, int b, uint32_t grid, cudaStream_t st);
+// sums into frontier b and, when `finalize`, the tree's leaves from frontier b
+// as launch_b_finalize(d, b, lp, scale, buf) would write them
+void launch_b_sums(const BDev& d, const uint32_t* ridx, const GradRef& gr, int b, uint32_t grid, cudaStream_t st,
+                   int finalize, LeafParams lp, const double* scale, uint32_t buf);
 // work items of k_b_scan per node (column blocks of its warps)
 uint32_t scan_col_blocks(uint32_t n_cols);
 void launch_b_finalize(const BDev& d, int a, LeafParams lp, const double* scale, uint32_t buf, cudaStream_t st);
