@@ -12,7 +12,11 @@ from ._abi import (BST_ERR_CONFIG, BST_OK, Config, ServerStats, Split, c_f32p, c
                    c_u32p, c_u64p)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libboosters_b200.so")
+# BST_LIBRARY=checked loads the bounds-checked build (libboosters_b200_checked.so)
+_VARIANT = os.environ.get("BST_LIBRARY", "")
+if _VARIANT not in ("", "checked"):
+    raise ImportError(f"BST_LIBRARY={_VARIANT!r}: expected unset or 'checked'")
+LIB_PATH = os.path.join(_HERE, "libboosters_b200_checked.so" if _VARIANT == "checked" else "libboosters_b200.so")
 
 # (name, restype, argtypes) of every exported entry point
 SIGNATURES = [
@@ -127,6 +131,9 @@ SIGNATURES = [
       c_f32p, c_f32p]),
     ("bst_metric", ctypes.c_int32,
      [ctypes.c_int32, c_f32p, ctypes.c_uint32, ctypes.c_uint64, c_f32p, c_f32p, c_f64p]),
+    ("bst_check_report", ctypes.c_int32,
+     [ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint32),
+      ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     ("bst_metric_ex", ctypes.c_int32,
      [ctypes.c_int32, c_f32p, ctypes.c_uint32, ctypes.c_uint64, c_f32p, c_f32p, c_f32p, ctypes.c_uint32,
       ctypes.c_float, c_f64p]),
@@ -136,7 +143,8 @@ SIGNATURES = [
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f"{LIB_PATH} is missing; build it with `python -m boosters_b200.build` "
+            f"{LIB_PATH} is missing; build it with `python -m boosters_b200.build`"
+            f"{' --checked' if _VARIANT else ''} "
             "(the GBDT engine has no CPU fallback)")
     lib = ctypes.CDLL(LIB_PATH)
     for name, res, args in SIGNATURES:

@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include "api_util.h"
 #include "engine.h"
+#include "nvtx_range.h"
 
 struct bst_dataset {
     bst::HostDataset d;
@@ -51,6 +52,23 @@ bst_status guarded(F&& f) {
     } catch (const std::exception& e) {
         return fail(BST_ERR_INVALID_ARGUMENT, e.what());
     }
+}
+
+// Checked build: a bounds-check violation recorded on `device` by the calls
+// before this one turns a successful result into BST_ERR_CHECK.
+bst_status check_after(int device, bst_status rc) {
+#ifdef BST_CHECKED
+    bst::CheckRecord r{};
+    if (rc == BST_OK && bst::check_take(device, &r) && r.violations) {
+        char msg[160];
+        std::snprintf(msg, sizeof msg, "bounds check failed %llu times; first at site %llu: index %llu, bound %llu",
+                      r.violations, r.site, r.index, r.bound);
+        return fail(BST_ERR_CHECK, msg);
+    }
+#else
+    (void)device;
+#endif
+    return rc;
 }
 
 bool ratio_ok(float v) { return v > 0.0f && v <= 1.0f; }
@@ -308,7 +326,10 @@ bst_status bst_gbdt_train(const bst_dataset* train, const bst_dataset* val, cons
             if (val->d.F < train->d.F)
                 return fail(BST_ERR_INVALID_ARGUMENT, "validation set has fewer features than the training set");
         }
+        BST_RANGE("bst.train");
         auto m = bst::train_model(train->d, *cfg, n_threads, evaluates ? &val->d : nullptr);
+        rc = check_after(cfg->device, BST_OK);
+        if (rc != BST_OK) return rc;
         *out = new bst_model{std::move(m)};
         return BST_OK;
     });
@@ -1071,3 +1092,20 @@ bst_status bst_metric(int32_t metric, const float* p, uint32_t G, uint64_t n, co
 }
 
 }  // extern "C"
+
+bst_status bst_check_report(int32_t device, uint64_t* violations, uint32_t* site, uint64_t* index, uint64_t* bound) {
+    return guarded([&]() -> bst_status {
+#ifdef BST_CHECKED
+        bst::CheckRecord r{};
+        if (!bst::check_take(device, &r)) return fail(BST_ERR_CUDA, "cannot read the bounds-check record");
+        if (violations) *violations = r.violations;
+        if (site) *site = (uint32_t)r.site;
+        if (index) *index = r.index;
+        if (bound) *bound = r.bound;
+        return BST_OK;
+#else
+        (void)device, (void)violations, (void)site, (void)index, (void)bound;
+        return fail(BST_ERR_UNSUPPORTED, "not a checked build (libboosters_b200_checked.so has the bounds checks)");
+#endif
+    });
+}

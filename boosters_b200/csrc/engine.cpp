@@ -7,6 +7,7 @@
 // tree under construction (a few hundred nodes) and reads back, per level,
 // the partition counts and the chosen splits.
 #include "engine.h"
+#include "nvtx_range.h"
 
 #include "autotune.h"
 
@@ -759,6 +760,7 @@ class Trainer {
     // Boosting rounds (trainer.rs:242-335): gradients of every output, then
     // one tree per output.
     void rounds(uint32_t k) {
+        BST_RANGE("bst.rounds");
         const int obj = cfg_.objective;
         for (uint32_t round = 0; round < k; ++round) {
             timer_.begin(PH_GRAD);
@@ -960,6 +962,9 @@ class Trainer {
         }
         if (!d_bleaves_.p) d_bleaves_.alloc((size_t)max_pnodes_ + 1);
         bd_.leaves = d_bleaves_.p;
+#ifdef BST_CHECKED
+        bd_.chk_rows = (uint32_t)n_;
+#endif
         if (!bd_.state) {  // no columns: no histogram state was set up
             d_bstate_.alloc(1);
             bd_.state = d_bstate_.p;
@@ -1299,6 +1304,9 @@ class Trainer {
         d_bstate_.alloc(1);
         d_bexp_.alloc(max_front / 2 + 1);
         bd_.state = d_bstate_.p;
+#ifdef BST_CHECKED
+        bd_.chk_rows = (uint32_t)n_;
+#endif
         bd_.exp = d_bexp_.p;
         const uint64_t max_pc = n_ / B_PART_CHUNK + max_front + 16;
         d_part_map_.alloc(max_pc);
@@ -2482,6 +2490,7 @@ class Trainer {
     }
 
     HostTree grow(uint32_t o) {
+        BST_RANGE("bst.tree");
         if (spec_leafwise_) return grow_lw_device(o);
         tree_output_ = o;
         gr_o_ = grad_ref(o);
@@ -2781,6 +2790,7 @@ class DeviceBounds final : public NumericBounds {
 }  // namespace
 
 void make_binned(const HostDataset& ds, const bst_config& cfg, cudaStream_t st, DeviceBinned& out) {
+    BST_RANGE("bst.binning");
     std::string err;
     const auto t0 = std::chrono::steady_clock::now();
     // Every feature goes to the device while the host analyses them: from
@@ -2949,6 +2959,7 @@ Booster::Booster(const HostDataset& ds, const bst_config& cfg, uint32_t n_thread
 Booster::~Booster() = default;
 
 void Booster::update(uint32_t rounds) {
+    BST_RANGE("bst.update");
     BST_CK(cudaSetDevice(impl_->cfg.device));
     const auto t0 = std::chrono::steady_clock::now();
     impl_->tr->rounds(rounds);
@@ -3030,6 +3041,9 @@ void upload_node_forest(const std::vector<const HostTree*>& trees, uint32_t n_gr
     f->view.base = f->base.p;
     f->view.n_trees = (uint32_t)trees.size();
     f->view.n_groups = n_groups;
+#ifdef BST_CHECKED
+    f->view.chk_nodes = (uint32_t)nodes.size();
+#endif
 }
 
 const DeviceForest& Model::device_forest() const {
@@ -3260,6 +3274,7 @@ void forest_predict_rows(const DeviceForest& f, const float* x, uint64_t n, uint
 }
 
 void predict_device(const Model& m, const float* x, uint64_t n, uint64_t F, bool raw, float* out, cudaStream_t st) {
+    BST_RANGE("bst.predict");
     const DeviceForest& f = m.device_forest();
     forest_predict_rows(f, x, n, F, out, st);
     if (!raw) launch_transform(transform_of(m.objective), out, m.n_groups, n, st);

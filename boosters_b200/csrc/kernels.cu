@@ -36,6 +36,46 @@ uint32_t sm_count() {
     return sms;
 }
 
+// Checked build: g_check holds (violations, site, index, bound) of the first
+// failed bounds test on this device. BST_IN(i, n, site) is true when i < n;
+// otherwise it records the failure and is false, and the caller skips the
+// access. In the normal build BST_IN is the constant true and every guarded
+// access compiles exactly as unguarded code.
+#ifdef BST_CHECKED
+__device__ unsigned long long g_check[4];
+
+__device__ __noinline__ bool check_fail(uint32_t site, unsigned long long i, unsigned long long n) {
+    if (atomicAdd(&g_check[0], 1ull) == 0ull) {
+        g_check[1] = site;
+        g_check[2] = i;
+        g_check[3] = n;
+    }
+    return false;
+}
+#define BST_IN(i, n, site) \
+    ((unsigned long long)(i) < (unsigned long long)(n) || check_fail((site), (unsigned long long)(i), (unsigned long long)(n)))
+
+bool check_take(int device, CheckRecord* out) {
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    unsigned long long h[4] = {0, 0, 0, 0};
+    const unsigned long long z[4] = {0, 0, 0, 0};
+    bool ok = cudaDeviceSynchronize() == cudaSuccess && cudaMemcpyFromSymbol(h, g_check, sizeof(h)) == cudaSuccess &&
+              cudaMemcpyToSymbol(g_check, z, sizeof(z)) == cudaSuccess;
+    if (!ok) cudaGetLastError();
+    cudaSetDevice(prev);
+    if (ok && out) *out = CheckRecord{h[0], h[1], h[2], h[3]};
+    return ok;
+}
+#else
+#define BST_IN(i, n, site) true
+
+bool check_take(int, CheckRecord*) { return false; }
+#endif
+
 namespace {
 
 constexpr unsigned FULL = 0xFFFFFFFFu;
@@ -967,7 +1007,12 @@ __device__ bool lane_accumulate_tma(uint32_t first, uint32_t count, bool ident, 
     bool failed = false;
     auto row_at = [&](uint32_t i) -> uint32_t {
         const uint32_t p = first + i;
+#ifdef BST_CHECKED
+        const uint32_t r = i < count ? (ident ? p : ridx[p]) : n_rows;
+        return (r == n_rows || BST_IN(r, n_rows, CHECK_HIST_ROW)) ? r : n_rows;
+#else
         return i < count ? (ident ? p : ridx[p]) : n_rows;  // n_rows: out of range, zero-filled
+#endif
     };
     // issue iteration k (rows of all lanes) into stage s
     auto issue = [&](uint32_t row, uint32_t s) {
@@ -2282,7 +2327,7 @@ __device__ void part_rows(const PartWork& w, uint32_t start, uint32_t len, unsig
                 dst = lb + s_l[k][warp] + __popc(lm[k] & lt);
             else if (rm[k] & bit)
                 dst = rbs + s_r[k][warp] + __popc(rm[k] & lt);
-            if (dst != 0xFFFFFFFFu) {
+            if (dst != 0xFFFFFFFFu && BST_IN(dst - w.begin, w.count, CHECK_PART_DST)) {
                 tmp[dst] = rows[k];
                 if constexpr (CARRY) qout[dst] = qv[k];
             }
@@ -2714,6 +2759,11 @@ k_b_partition(BDev d, const uint32_t* __restrict__ ridx, uint32_t* __restrict__ 
         }
         __syncthreads();
         const uint32_t j = s_m.x, start = s_m.y;
+#ifdef BST_CHECKED
+        const bool chunk_ok = BST_IN(start - w.begin, w.count, CHECK_PART_CHUNK);
+        __syncthreads();  // every thread has read s_m / w before a skipped chunk's next rewrite
+        if (!chunk_ok) continue;
+#endif
         const uint32_t len = min(B_PART_CHUNK, w.begin + w.count - start);
         part_rows<Q>(w, start, len, d.cursors + 2 * j, ridx, tmp, bins8, s8, bins16, s16, qin, qout, fm.b8, fm.b16,
                      fm.n, d.rmask, d.rmask ? d.scnt + 2 * j : nullptr);
@@ -3454,6 +3504,11 @@ k_lw_partition(BDev d, const uint32_t* __restrict__ ridx, uint32_t* __restrict__
         }
         __syncthreads();
         const uint32_t j = s_m.x, start = s_m.y;
+#ifdef BST_CHECKED
+        const bool chunk_ok = BST_IN(start - w.begin, w.count, CHECK_PART_CHUNK);
+        __syncthreads();  // every thread has read s_m / w before a skipped chunk's next rewrite
+        if (!chunk_ok) continue;
+#endif
         const uint32_t len = min(B_PART_CHUNK, w.begin + w.count - start);
         part_rows<Q>(w, start, len, d.cursors + 2 * j, ridx, tmp, bins8, s8, bins16, s16, qin, qout, fm.b8, fm.b16,
                      fm.n, d.rmask, d.rmask ? d.scnt + 2 * j : nullptr);
@@ -3919,6 +3974,7 @@ __global__ void k_b_leaf_update(BDev d, const uint32_t* __restrict__ r0, const u
     const uint32_t total = d.state->leaf_chunks;
     for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
         const uint2 m = d.leaf_map[c];
+        if (!BST_IN(m.x, d.state->n_leaves, CHECK_LEAF_MAP)) continue;
         const BLeaf lf = d.leaves[m.x];
         const uint32_t start = m.y;
         const uint32_t len = min(B_LEAF_CHUNK, lf.begin + lf.count - start);
@@ -3932,6 +3988,9 @@ __global__ void k_b_leaf_update(BDev d, const uint32_t* __restrict__ r0, const u
             for (uint32_t u = 0; u < RANGE_ILP; ++u) {
                 const uint32_t i = i0 + u * blockDim.x;
                 rows[u] = i < len ? ridx[start + i] : 0u;
+#ifdef BST_CHECKED
+                if (i < len && !BST_IN(rows[u], d.chk_rows, CHECK_LEAF_ROW)) rows[u] = 0u;
+#endif
             }
 #pragma unroll
             for (uint32_t u = 0; u < RANGE_ILP; ++u)
@@ -4309,6 +4368,9 @@ __global__ void k_predict(ForestDev f, const float* __restrict__ x,
                     left = v < fn.value;
                 }
                 nd = left ? fn.left : fn.right;
+#ifdef BST_CHECKED
+                if (!BST_IN(nd, f.chk_nodes, CHECK_PREDICT_NODE)) break;
+#endif
             }
         }
         out[(uint64_t)g * n + i] = acc;

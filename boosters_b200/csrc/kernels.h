@@ -25,6 +25,26 @@ namespace bst {
 // and device): launch grids are sized in whole waves of it.
 uint32_t sm_count();
 
+// Checked build (compiled with -DBST_CHECKED into libboosters_b200_checked.so):
+// device accesses whose index is read from device memory test it against its
+// bound first; a failed test is counted, the first one's site, index and
+// bound are recorded, and the access is skipped or redirected to a zero-filled
+// row, so a bad index becomes an error status on the host instead of a fault.
+enum CheckSite : uint32_t {
+    CHECK_PART_CHUNK = 1,  // partition chunk outside its expansion's rows
+    CHECK_PART_DST = 2,    // partition scatter outside the node's row range
+    CHECK_LEAF_MAP = 3,    // leaf chunk names a leaf past the tree's leaf count
+    CHECK_LEAF_ROW = 4,    // leaf update row id >= rows
+    CHECK_HIST_ROW = 5,    // histogram gather row id >= rows (tensor-map gather)
+    CHECK_PREDICT_NODE = 6,  // traversal node link >= forest nodes
+};
+struct CheckRecord {
+    unsigned long long violations, site, index, bound;
+};
+// Reads and clears the record of device `device`. False in the normal build
+// (no record exists) or on a CUDA error.
+bool check_take(int device, CheckRecord* out);
+
 // Histogram bin: exact 64-bit fixed-point sums of grad and hess.
 struct HBin {
     long long g, h;
@@ -343,6 +363,9 @@ struct BDev {  // device buffers of the level loop
     uint32_t max_part_chunks;  // capacity of part_map
     uint2* leaf_map;       // leaf chunk -> (leaf, first row), written by k_b_finalize
     uint32_t max_leaf_chunks;  // capacity of leaf_map
+#ifdef BST_CHECKED
+    uint32_t chk_rows;  // rows of the training set (bound of every row id)
+#endif
 };
 constexpr uint32_t B_PART_CHUNK = 2048;
 constexpr uint32_t B_LEAF_CHUNK = 2048;  // rows per leaf-kernel work item (2048 measured faster than 4096)
@@ -525,6 +548,9 @@ struct ForestDev {
     const uint32_t* cat_words;
     const float* base;            // [n_groups]
     uint32_t n_trees, n_groups;
+#ifdef BST_CHECKED
+    uint32_t chk_nodes;  // entries of nodes (bound of every node link)
+#endif
 };
 // feature_major != 0: x[f * n + i]; else sample-major x[i * n_features + f].
 // out [n_groups][n] raw margins (base score + trees in forest order, f32).

@@ -41,6 +41,7 @@ typedef int32_t bst_status;
 #define BST_ERR_OUT_OF_MEMORY 7
 #define BST_ERR_TIMEOUT 8
 #define BST_ERR_FORMAT 9 /* malformed model bytes                           */
+#define BST_ERR_CHECK 10 /* checked build: a device bounds check failed      */
 
 /* Message of the last failure on the calling thread ("" if none). */
 const char* bst_last_error(void);
@@ -579,6 +580,24 @@ bst_status bst_metric(int32_t metric, const float* preds, uint32_t n_groups, uin
 bst_status bst_metric_ex(int32_t metric, const float* preds, uint32_t n_groups, uint64_t n_samples,
                          const float* targets, const float* weights, const float* quantile_alpha,
                          uint32_t n_quantiles, float huber_delta, double* out);
+
+/* ------------------------------------------------------------------------ */
+/* Checked build (no counterpart in the reference, whose debug_assert region */
+/* checks in histograms/slices.rs:91-110 play this role on the CPU)          */
+/* ------------------------------------------------------------------------ */
+
+/* libboosters_b200_checked.so is the same library compiled with device-side
+ * bounds checks at the accesses whose index is read from device memory (row
+ * ids of the histogram gather and leaf update, partition chunks and scatter
+ * destinations, leaf chunks, traversal node links). A failed check is
+ * counted and its access skipped; no kernel traps. bst_gbdt_train returns
+ * BST_ERR_CHECK when its kernels recorded a violation. This reads and clears
+ * the record of `device`: the number of violations and the first one's site
+ * (1 partition chunk, 2 partition scatter, 3 leaf chunk, 4 leaf-update row,
+ * 5 histogram-gather row, 6 traversal node), index and bound. The normal
+ * library returns BST_ERR_UNSUPPORTED. */
+bst_status bst_check_report(int32_t device, uint64_t* violations, uint32_t* site, uint64_t* index,
+                            uint64_t* bound);
 
 #ifdef __cplusplus
 }

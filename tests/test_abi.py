@@ -124,3 +124,28 @@ def test_training_rejects_unsupported_options():
     with pytest.raises(bst.BoostersError) as e:
         bst.GBDTModel.train(bst.Dataset.from_feature_major(x), bst.GBDTConfig())
     assert e.value.status == n.BST_ERR_MISSING_TARGETS
+
+
+def test_checked_library_exports_and_status():
+    """The bounds-checked build exports the same entry points; the normal
+    build answers bst_check_report with BST_ERR_UNSUPPORTED (no device
+    call), the checked build without a device with BST_ERR_CUDA."""
+    checked = os.path.join(os.path.dirname(n.LIB_PATH), "libboosters_b200_checked.so")
+    if not os.path.exists(checked):
+        pytest.skip("libboosters_b200_checked.so is not built (python -m boosters_b200.build --checked)")
+    lib = ctypes.CDLL(checked)
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+    v = ctypes.c_uint64(7)
+    normal = ctypes.CDLL(n.LIB_PATH)
+    normal.bst_check_report.restype = ctypes.c_int32
+    assert normal.bst_check_report(0, ctypes.byref(v), None, None, None) == 5  # BST_ERR_UNSUPPORTED
+    assert v.value == 7
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except ImportError:
+        has_gpu = False
+    if not has_gpu:
+        lib.bst_check_report.restype = ctypes.c_int32
+        assert lib.bst_check_report(0, ctypes.byref(v), None, None, None) == 6  # BST_ERR_CUDA
