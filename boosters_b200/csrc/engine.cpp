@@ -1631,6 +1631,7 @@ class Trainer {
 
     // Enqueues the tree of output o into ring slot `si` (no host wait).
     void launch_batched(uint32_t o, uint32_t si) {
+        BST_RANGE("bst.tree");  // the tree's graph launch (its kernels run after the range closes)
         Slot& sl = slots_[si];
         const size_t gi = (size_t)o * RING + si;
         sl.timed = false;
