@@ -1224,6 +1224,14 @@ k_b_hist_part(BDev d, const LaneTile* __restrict__ tiles, uint32_t n_tiles, cons
         const BExp e = d.exp[d.seg_exp[c]];
         const uint32_t start = e.small_begin + (c - e.hist_off) * CH;
         const uint32_t count = min(CH, e.small_begin + e.small_count - start);
+#ifdef BST_CHECKED
+        // the item's rows inside the row-id buffer, and every row id < rows
+        bool rows_ok = count == 0 || BST_IN(start + count - 1, d.chk_rows, CHECK_HIST_ROW);
+        if (rows_ok)
+            for (uint32_t i = threadIdx.x; i < count; i += blockDim.x)
+                rows_ok = BST_IN(ridx[start + i], d.chk_rows, CHECK_HIST_ROW) && rows_ok;
+        if (!__syncthreads_and(rows_ok)) continue;
+#endif
         load_lane_tile(tile, tiles[t]);
         __syncthreads();
         part_item<MODE, lane_regs(V)>(start, count, tile, sm, stage, ridx, load, bins8, s8, bins16, s16,
